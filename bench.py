@@ -1,0 +1,331 @@
+#!/usr/bin/env python3
+"""Benchmark: QBVH ray queries on the 1M-triangle sphere soup.
+
+Workload (one "step"): closest-hit and any-hit queries (tmax = inf) of 2^24
+coherent primary rays (1024x1024 pinhole, 16 stratified rays per pixel) and
+2^24 incoherent rays (origins uniform in the 100^3 cube, directions uniform on
+the sphere) against 4,096 UV spheres = 1,048,576 triangles, one QBVH built by
+the reference builder's algorithm.  4 x 2^24 = 67,108,864 ray queries per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value`: ray queries per second with rays resident in HBM (whole job, all
+ranks).  `e2e`: the same queries through the host-pointer C ABI entry point
+(`tpt_traverse`) from pinned host memory, copies included.
+`--impl reference` times the CPU restatement of the reference traverser (the
+oracle) on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "toy-path-tracing_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "rays/s"
+WORKLOAD = "qbvh_traversal_1M_sphere_soup"
+ALGO_BYTES_RAY = 36  # 28 B ray in + 8 B hit out
+ALGO_BYTES_NODE = 112  # 6 x 16 B lane bounds + 4 x 4 B child words
+ALGO_BYTES_TRI = 40  # 3 x 12 B positions + 4 B primitive index
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--rays-log2", type=int, default=24, help="rays per batch = 2^k (profiling uses smaller)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def config_dict(args, world):
+    return {
+        "workload": WORKLOAD,
+        "triangles": 1048576,
+        "spheres": 4096,
+        "rays_per_batch": 1 << args.rays_log2,
+        "batches": ["coherent_1024x1024x16", "incoherent_uniform"],
+        "queries": ["closest_hit", "any_hit"],
+        "queries_per_step": 4 << args.rays_log2,
+        "tmax": "inf",
+        "l2": "inputs larger than L2 (470 MB of rays per batch); BVH+triangles (~90 MB) stay L2-resident",
+        "parallelism": f"replicas{world}",
+    }
+
+
+def make_workload(rank: int, rays_log2: int):
+    import tpt_scenes
+
+    mesh = tpt_scenes.sphere_soup(seed=1)
+    n = 1 << rays_log2
+    side = int(round((n / 16) ** 0.5))
+    coh = tpt_scenes.coherent_rays(side, side, 4, seed=2 + 100 * rank)
+    inc = tpt_scenes.incoherent_rays(n, seed=3 + 100 * rank)
+    return mesh, [coh, inc]
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(mesh, batches, target_s=8.0, max_log2=22):
+    """Oracle (CPU restatement of qbvh.rs/scene closest_hit) on all host cores:
+    grows a sample until it runs for target_s seconds; returns rays/s."""
+    import oracle as orc
+
+    g = orc.Geometry()
+    g.add_mesh(mesh["positions"], mesh["indices"])
+    g.add_instance(0, 0, np.eye(4, dtype=np.float32), np.eye(4, dtype=np.float32), np.eye(3, dtype=np.float32))
+    g.build()
+    threads = os.cpu_count() or 1
+    k = 14
+    rng = np.random.default_rng(0)
+    while True:
+        m = min(1 << k, batches[0].shape[1])
+        total = 0
+        t0 = time.perf_counter()
+        for rays in batches:
+            sel = rng.choice(rays.shape[1], m, replace=False)
+            sample = np.ascontiguousarray(rays[:, sel])
+            for mode in (0, 1):
+                g.query(sample, mode, nthreads=threads)
+                total += m
+        dt = time.perf_counter() - t0
+        if dt >= target_s or k >= max_log2 or m == batches[0].shape[1]:
+            return total / dt, threads, f"{m} rays from each batch x (closest, any) = {total} queries, {dt:.1f} s"
+        k += 1 if dt > target_s / 4 else 2
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    mesh, batches = make_workload(0, args.rays_log2)
+    rates = []
+    desc = None
+    threads = 1
+    for _ in range(args.warmup + args.steps):
+        r, threads, desc = cpu_reference_rate(mesh, batches, target_s=2.0, max_log2=20)
+        rates.append(r)
+    rate = float(np.median(rates[args.warmup:]))
+    per_step_s = (4 << args.rays_log2) / rate
+    line = {
+        "metric": METRIC, "value": rate, "unit": "rays/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sphere soup + ray batches)",
+        "config": config_dict(args, 1), "impl": "reference",
+        "cpu_baseline": {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": rate, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(device)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Not" not in r[5 + i] and r[5 + i].strip()
+                          and r[5 + i].strip() != "[N/A]"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traverse_closest_incoherent_1M.txt")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_full_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import tpt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    ctx = tpt.Context(local)
+    mesh, batches = make_workload(rank, args.rays_log2)
+    scene = tpt.Scene(ctx, [mesh], [__import__("tpt_scenes").identity_instance()])
+    n = batches[0].shape[1]
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    d_rays = [torch.from_numpy(b).to("cuda") for b in batches]
+    d_prim = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_t = torch.empty(n, dtype=torch.float32, device="cuda")
+    queries = [(b, m) for m in (tpt.CLOSEST_HIT, tpt.ANY_HIT) for b in range(2)]
+    dominant = (1, tpt.CLOSEST_HIT)  # incoherent closest hit
+
+    def step(events=None):
+        for b, m in queries:
+            if events is not None and (b, m) == dominant:
+                events[0].record(stream)
+            scene.traverse_device(d_rays[b].data_ptr(), n, m, d_prim.data_ptr(), d_t.data_ptr(), stream=sp)
+            if events is not None and (b, m) == dominant:
+                events[1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # algorithmic bytes of the dominant launch (node and triangle test counts;
+    # equal to the oracle's counts for the same rays, checked by the tests)
+    nt = torch.empty(n, dtype=torch.int32, device="cuda")
+    tt = torch.empty(n, dtype=torch.int32, device="cuda")
+    scene.traverse_stats_device(d_rays[dominant[0]].data_ptr(), n, dominant[1], d_prim.data_ptr(), d_t.data_ptr(),
+                                nt.data_ptr(), tt.data_ptr(), sp)
+    torch.cuda.synchronize()
+    nodes = int(nt.sum(dtype=torch.int64))
+    tris = int(tt.sum(dtype=torch.int64))
+    algo_bytes = ALGO_BYTES_RAY * n + ALGO_BYTES_NODE * nodes + ALGO_BYTES_TRI * tris
+
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for k in range(args.steps):
+        step(ev[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed_ms = t0.elapsed_time(t1)
+    dom_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    if world > 1:
+        tmax = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tmax.item())
+    total_rays = world * len(queries) * n * args.steps
+    value = total_rays / (elapsed_ms / 1e3)
+
+    # end to end through the host-pointer entry point, pinned host buffers
+    h_rays = [torch.from_numpy(b).pin_memory() for b in batches]
+    h_prim = torch.empty(n, dtype=torch.int32).pin_memory()
+    h_t = torch.empty(n, dtype=torch.float32).pin_memory()
+    lib = tpt.lib()
+    import ctypes as C
+
+    def e2e_step():
+        for b, m in queries:
+            st = lib.tpt_traverse(ctx.h, scene.h, C.c_void_p(h_rays[b].data_ptr()), n, m,
+                                  C.c_void_p(h_prim.data_ptr()), C.c_void_p(h_t.data_ptr()), None, None)
+            if st != 0:
+                raise RuntimeError(lib.tpt_last_error(ctx.h).decode())
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    e2e_steps = max(1, min(args.steps, 5))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - w0
+    if world > 1:
+        tm = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        e2e_s = float(tm.item())
+    e2e_value = world * len(queries) * n * e2e_steps / e2e_s
+
+    peak, peak_kind = measured_peak()
+    achieved_gbs = algo_bytes / (dom_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sphere soup + ray batches)",
+        "config": config_dict(args, world),
+        "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": len(queries) * n * 7 * 4,
+                "d2h_bytes_per_step": len(queries) * n * 8},
+        "gpu_launches": len(queries) * args.steps,
+        "roofline": {
+            "bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
+            "traffic": profiled_traffic(), "peak_kind": peak_kind,
+            "kernel": "traverse_kernel<closest,incoherent>", "launch_ms": dom_ms,
+            "algorithmic_bytes_per_launch": algo_bytes, "node_tests": nodes, "tri_tests": tris,
+            "note": "algorithmic bytes count every 4-wide node and triangle fetch; the BVH is L2-resident, "
+                    "so this rate is mostly L2 bandwidth",
+        },
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, threads, desc = cpu_reference_rate(mesh, batches)
+        line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del scene
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,198 @@
+"""Oracle: CPU restatement of the reference path tracer's per-sample hot path.
+
+Test infrastructure only.  tests/, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` load it as the checker; the shipped library
+(``toy-path-tracing_b200``) never links or calls it.
+
+The C++ sources under ``oracle/src`` restate, function by function, the Rust
+reference ``crates/renderer/src`` (file:line cited in each source).  This module
+is a thin ctypes binding over ``oracle/_build/liboracle.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+NODE_DTYPE = np.dtype(
+    [("b", "<f4", (6, 4)), ("children", "<u4", (4,)), ("valid_mask", "<u4"), ("pad", "<u4", (3,))]
+)
+assert NODE_DTYPE.itemsize == 128
+
+
+def build() -> str:
+    """Compile the oracle library (make in oracle/)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _declare(L):
+    vp, u64, u32, i64, f32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int64, C.c_float, C.c_int
+    sig = {
+        "orc_intersect_triangle": (i32, [vp, f32, vp, vp]),
+        "orc_qbvh_build": (vp, [vp, u64]),
+        "orc_qbvh_free": (None, [vp]),
+        "orc_qbvh_num_nodes": (u64, [vp]),
+        "orc_qbvh_num_prims": (u64, [vp]),
+        "orc_qbvh_copy": (None, [vp, vp, vp]),
+        "orc_qbvh_closest_box": (i64, [vp, vp, vp, vp]),
+        "orc_geometry_create": (vp, []),
+        "orc_geometry_free": (None, [vp]),
+        "orc_geometry_add_mesh": (i64, [vp, vp, u64, vp, vp, vp, u64]),
+        "orc_geometry_add_instance": (i64, [vp, u32, u32, vp, vp, vp]),
+        "orc_geometry_build": (None, [vp]),
+        "orc_geometry_mesh_qbvh_nodes": (u64, [vp, u32]),
+        "orc_geometry_mesh_qbvh_copy": (None, [vp, u32, vp, vp]),
+        "orc_geometry_tlas_nodes": (u64, [vp]),
+        "orc_geometry_tlas_copy": (None, [vp, vp, vp]),
+        "orc_geometry_query": (None, [vp, vp, u64, i32, vp, vp, vp, vp, vp, i32]),
+        "orc_sampler_vertex_randoms": (None, [u32, u32, u32, u32, u32, u32, u32, vp, vp]),
+        "orc_sampler_camera": (None, [u32, u32, u32, u32, u32, u32, vp, vp]),
+        "orc_zsobol_sample_index": (u64, [u32, u32, u32, u32, u32, u32, u32]),
+        "orc_shuffled_scrambled_sobol": (None, [u32, u32, i32, vp]),
+        "orc_uint_to_float": (f32, [u32]),
+        "orc_encode_morton_2": (u64, [u32, u32]),
+        "orc_laine_karras": (u32, [u32, u32]),
+        "orc_reverse_and_shuffle": (u32, [u32, u32]),
+        "orc_pcg_hash": (u32, [u32]),
+        "orc_pcg_state_transition": (u32, [u32]),
+        "orc_pcg_output": (u32, [u32]),
+        "orc_mix_bits": (u64, [u64]),
+        "orc_camera_ray": (None, [vp, u32, u32, u32, u32, f32, f32, u32, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+# --------------------------------------------------------------------------
+def intersect_triangle(origin, direction, t_max, v0, v1, v2):
+    ray = np.array([*origin, *direction], np.float32)
+    v = np.array([*v0, *v1, *v2], np.float32)
+    out = np.zeros(4, np.float32)
+    ok = lib().orc_intersect_triangle(_p(ray), C.c_float(t_max), _p(v), _p(out))
+    return (float(out[0]), out[1:].copy()) if ok else None
+
+
+class BoxQbvh:
+    """QBVH over axis-aligned boxes (the reference's qbvh.rs unit-test harness)."""
+
+    def __init__(self, bounds: np.ndarray):
+        self.bounds = np.ascontiguousarray(bounds, np.float32).reshape(-1, 6)
+        self.h = lib().orc_qbvh_build(_p(self.bounds), self.bounds.shape[0]) if len(self.bounds) else None
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_qbvh_free(self.h)
+
+    def arrays(self):
+        n = lib().orc_qbvh_num_nodes(self.h)
+        m = lib().orc_qbvh_num_prims(self.h)
+        nodes = np.zeros(n, NODE_DTYPE)
+        prims = np.zeros(m, np.uint32)
+        lib().orc_qbvh_copy(self.h, _p(nodes), _p(prims))
+        return nodes, prims
+
+    def closest_box(self, origin, direction):
+        ray = np.array([*origin, *direction], np.float32)
+        t = np.zeros(1, np.float32)
+        idx = lib().orc_qbvh_closest_box(self.h, _p(self.bounds), _p(ray), _p(t))
+        return (int(idx), float(t[0])) if idx >= 0 else None
+
+
+class Geometry:
+    """Two-level scene geometry (meshes + instances + TLAS), scene/mod.rs."""
+
+    def __init__(self):
+        self.h = lib().orc_geometry_create()
+        self._tri_counts = []
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_geometry_free(self.h)
+
+    def add_mesh(self, positions, indices, normals=None, uvs=None) -> int:
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        idx = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        nrm = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        uv = None if uvs is None else np.ascontiguousarray(uvs, np.float32).reshape(-1, 2)
+        self._tri_counts.append(idx.size // 3)
+        return lib().orc_geometry_add_mesh(self.h, _p(pos), pos.shape[0], _p(nrm), _p(uv), _p(idx), idx.size)
+
+    def add_instance(self, mesh: int, material: int, local_to_world, world_to_local, normal_to_world) -> int:
+        l2w = np.ascontiguousarray(local_to_world, np.float32).reshape(16)
+        w2l = np.ascontiguousarray(world_to_local, np.float32).reshape(16)
+        n2w = np.ascontiguousarray(normal_to_world, np.float32).reshape(9)
+        return lib().orc_geometry_add_instance(self.h, mesh, material, _p(l2w), _p(w2l), _p(n2w))
+
+    def build(self):
+        lib().orc_geometry_build(self.h)
+
+    def mesh_qbvh(self, mesh: int):
+        n = lib().orc_geometry_mesh_qbvh_nodes(self.h, mesh)
+        nodes = np.zeros(n, NODE_DTYPE)
+        prims = np.zeros(self._mesh_tris(mesh), np.uint32)
+        lib().orc_geometry_mesh_qbvh_copy(self.h, mesh, _p(nodes), _p(prims))
+        return nodes, prims
+
+    def _mesh_tris(self, mesh):
+        return self._tri_counts[mesh]
+
+    def query(self, rays: np.ndarray, mode: int = 0, stats: bool = False, nthreads: int | None = None):
+        """rays: float32 [7, n] planes (ox, oy, oz, dx, dy, dz, tmax)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[1]
+        prim = np.empty(n, np.int32)
+        inst = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        bary = np.empty((3, n), np.float32)
+        st = np.empty((n, 2), np.uint32) if stats else None
+        nthreads = nthreads or os.cpu_count() or 1
+        lib().orc_geometry_query(self.h, _p(rays), n, mode, _p(prim), _p(inst), _p(t), _p(bary), _p(st), nthreads)
+        out = {"prim": prim, "inst": inst, "t": t, "bary": bary}
+        if stats:
+            out["nodes"] = st[:, 0]
+            out["tris"] = st[:, 1]
+        return out
+
+
+def vertex_randoms(px, py, sample, spp, rx, ry, depth):
+    out = np.zeros(12, np.float32)
+    seed = np.zeros(1, np.uint32)
+    lib().orc_sampler_vertex_randoms(px, py, sample, spp, rx, ry, depth, _p(out), _p(seed))
+    return out, int(seed[0])
+
+
+def camera_sample(px, py, sample, spp, rx, ry):
+    out = np.zeros(2, np.float32)
+    seed = np.zeros(1, np.uint32)
+    lib().orc_sampler_camera(px, py, sample, spp, rx, ry, _p(out), _p(seed))
+    return out, int(seed[0])
+
+
+def camera_ray(params, rx, ry, px, py, ux, uy, spp):
+    p = np.ascontiguousarray(params, np.float32)
+    out = np.zeros(20, np.float32)
+    lib().orc_camera_ray(_p(p), rx, ry, px, py, C.c_float(ux), C.c_float(uy), spp, _p(out))
+    return out

@@ -1,0 +1,220 @@
+"""Parity of the device ray queries with the oracle (`Scene::closest_hit`).
+
+The bar (closest hit): triangle and instance ids and t bit-identical to the
+oracle, which visits nodes and triangles in the reference's order and keeps
+its tie rule; any hit: the same first hit as the oracle's occlusion query and
+exactly the oracle's hit/miss set.  t is also checked against a float64
+brute-force solve (1e-5 relative on non-grazing hits).
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import tpt
+import tpt_scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rand_rot(rng):
+    q = rng.standard_normal(4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def instance_from(mesh, l2w64):
+    w2l64 = np.linalg.inv(l2w64)
+    n2w = w2l64[:3, :3].T
+    return {
+        "mesh": mesh,
+        "material": 0,
+        # column-major (glam): flatten the transpose
+        "local_to_world": l2w64.T.astype(np.float32).reshape(16),
+        "world_to_local": w2l64.T.astype(np.float32).reshape(16),
+        "normal_to_world": n2w.T.astype(np.float32).reshape(9),
+    }
+
+
+def build_both(ctx, meshes, instances):
+    g = orc.Geometry()
+    for m in meshes:
+        g.add_mesh(m["positions"], m["indices"], m.get("normals"), m.get("uvs"))
+    for inst in instances:
+        g.add_instance(inst["mesh"], inst["material"], inst["local_to_world"], inst["world_to_local"],
+                       inst["normal_to_world"])
+    g.build()
+    s = tpt.Scene(ctx, meshes, instances)
+    return g, s
+
+
+def edge_rays(rng, n, lo, hi):
+    """Axis-aligned rays, rays with zero direction lanes, origins on integer planes."""
+    rays = np.zeros((7, n), np.float32)
+    rays[0:3] = rng.uniform(lo, hi, (3, n)).astype(np.float32)
+    ax = rng.integers(0, 3, n)
+    sg = rng.choice([-1.0, 1.0], n)
+    rays[3 + ax, np.arange(n)] = sg
+    half = n // 2
+    rays[0:3, :half] = np.round(rays[0:3, :half])  # origins on coordinate planes
+    rays[6] = np.inf
+    return rays
+
+
+def assert_same(dev, ref, what):
+    bad = np.nonzero((dev["prim"] != ref["prim"]) | (dev["t"].view(np.uint32) != ref["t"].view(np.uint32)))[0]
+    assert bad.size == 0, f"{what}: {bad.size} rays differ, first {bad[:5]} dev={dev['prim'][bad[:5]]} " \
+                          f"ref={ref['prim'][bad[:5]]} tdev={dev['t'][bad[:5]]} tref={ref['t'][bad[:5]]}"
+
+
+@pytest.fixture(scope="module")
+def soup(ctx):
+    mesh = tpt_scenes.sphere_soup(seed=11, n_spheres=512, cube=30.0)
+    return build_both(ctx, [mesh], [tpt_scenes.identity_instance()])
+
+
+def test_closest_hit_bit_exact_small_soup(soup):
+    g, s = soup
+    rng = np.random.default_rng(1)
+    for rays in (tpt_scenes.incoherent_rays(1 << 16, seed=4, cube=30.0),
+                 tpt_scenes.coherent_rays(128, 128, 2, seed=5, eye=(15, 15, -30), look_at=(15, 15, 15)),
+                 edge_rays(rng, 1 << 14, -1.0, 31.0)):
+        ref = g.query(rays, 0)
+        dev = s.closest_hit(rays, tpt.CLOSEST_HIT, want_instance=True, want_bary=True)
+        assert_same(dev, ref, "closest")
+        hit = ref["prim"] >= 0
+        assert np.array_equal(dev["inst"], ref["inst"])
+        assert np.array_equal(dev["bary"][:, hit].view(np.uint32), ref["bary"][:, hit].view(np.uint32))
+        assert hit.mean() > 0.05
+
+
+def test_any_hit_matches_oracle_occlusion(soup):
+    g, s = soup
+    rays = tpt_scenes.incoherent_rays(1 << 16, seed=8, cube=30.0)
+    ref = g.query(rays, 1)
+    dev = s.closest_hit(rays, tpt.ANY_HIT)
+    assert_same(dev, ref, "any")
+    ch = g.query(rays, 0)
+    assert np.array_equal(dev["prim"] >= 0, ch["prim"] >= 0)
+    # finite tmax: occluded iff the closest hit is nearer than tmax
+    rays[6] = np.float32(5.0)
+    dev = s.closest_hit(rays, tpt.ANY_HIT)
+    assert np.array_equal(dev["prim"] >= 0, ch["t"] <= 5.0)
+
+
+def test_traversal_counts_match_oracle(soup, ctx):
+    import torch
+
+    g, s = soup
+    rays = tpt_scenes.incoherent_rays(1 << 14, seed=9, cube=30.0)
+    ref = g.query(rays, 0, stats=True)
+    d = torch.from_numpy(rays).cuda()
+    n = rays.shape[1]
+    prim = torch.empty(n, dtype=torch.int32, device="cuda")
+    t = torch.empty(n, dtype=torch.float32, device="cuda")
+    nt = torch.empty(n, dtype=torch.int32, device="cuda")
+    tt = torch.empty(n, dtype=torch.int32, device="cuda")
+    s.traverse_stats_device(d.data_ptr(), n, 0, prim.data_ptr(), t.data_ptr(), nt.data_ptr(), tt.data_ptr(),
+                            torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(prim.cpu().numpy(), ref["prim"])
+    assert np.array_equal(nt.cpu().numpy().astype(np.uint32), ref["nodes"])
+    assert np.array_equal(tt.cpu().numpy().astype(np.uint32), ref["tris"])
+
+
+def test_two_level_instances_bit_exact(ctx):
+    rng = np.random.default_rng(3)
+    meshes = [tpt_scenes.sphere_soup(seed=s, n_spheres=8, cube=4.0) for s in (21, 22, 23)]
+    instances = []
+    for i in range(64):
+        l2w = np.eye(4)
+        l2w[:3, :3] = rand_rot(rng) * rng.uniform(0.5, 2.0)
+        l2w[:3, 3] = rng.uniform(-20, 20, 3)
+        instances.append(instance_from(int(rng.integers(0, 3)), l2w))
+    g, s = build_both(ctx, meshes, instances)
+    rays = tpt_scenes.incoherent_rays(1 << 15, seed=12, cube=40.0)
+    rays[0:3] -= 20.0
+    ref = g.query(rays, 0)
+    dev = s.closest_hit(rays, 0, want_instance=True)
+    assert_same(dev, ref, "two-level")
+    assert np.array_equal(dev["inst"], ref["inst"])
+    assert (ref["prim"] >= 0).mean() > 0.01
+
+
+def test_root_leaf_and_degenerate_and_empty(ctx):
+    tri = {"positions": np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [2, 0, 0]], np.float32),
+           "indices": np.array([0, 1, 2, 0, 1, 3], np.uint32)}  # second triangle is degenerate
+    g, s = build_both(ctx, [tri], [tpt_scenes.identity_instance()])
+    rays = np.zeros((7, 3), np.float32)
+    rays[0:3] = [[0.25, 1.25, 0.5], [0.25, 1.25, 0.0], [1.0, 1.0, 0.0]]
+    rays[5] = -1.0
+    rays[6] = np.inf
+    ref = g.query(rays, 0)
+    dev = s.closest_hit(rays, 0)
+    assert_same(dev, ref, "root leaf")
+    assert dev["prim"].tolist() == [0, -1, 0]
+    out = s.closest_hit(np.zeros((7, 0), np.float32))
+    assert out["prim"].size == 0
+
+
+def test_rejects_bad_scene(ctx):
+    tri = {"positions": np.zeros((3, 3), np.float32), "indices": np.array([0, 1, 5], np.uint32)}
+    with pytest.raises(tpt.TptError) as e:
+        tpt.Scene(ctx, [tri], [tpt_scenes.identity_instance()])
+    assert e.value.status == 1
+    good = {"positions": np.eye(3, dtype=np.float32), "indices": np.array([0, 1, 2], np.uint32)}
+    with pytest.raises(tpt.TptError):
+        tpt.Scene(ctx, [good], [tpt_scenes.identity_instance(mesh=3)])
+
+
+def test_fp64_brute_force_t(soup):
+    """Device t vs a float64 solve of the hit triangle (non-grazing hits)."""
+    g, s = soup
+    mesh = tpt_scenes.sphere_soup(seed=11, n_spheres=512, cube=30.0)
+    rays = tpt_scenes.incoherent_rays(1 << 14, seed=13, cube=30.0)
+    dev = s.closest_hit(rays, 0)
+    hit = np.nonzero(dev["prim"] >= 0)[0]
+    tri = mesh["positions"][mesh["indices"].reshape(-1, 3)[dev["prim"][hit]]].astype(np.float64)
+    o = rays[0:3, hit].T.astype(np.float64)
+    d = rays[3:6, hit].T.astype(np.float64)
+    e1, e2 = tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
+    n = np.cross(e1, e2)
+    t64 = np.einsum("ij,ij->i", tri[:, 0] - o, n) / np.einsum("ij,ij->i", d, n)
+    cosang = np.abs(np.einsum("ij,ij->i", d, n)) / np.linalg.norm(n, axis=1)
+    ok = cosang > 0.05
+    rel = np.abs(dev["t"][hit] - t64) / np.abs(t64)
+    assert ok.sum() > 100
+    assert np.all(rel[ok] <= 1e-5), rel[ok].max()
+
+
+def test_full_size_traversal_against_oracle_sample(ctx):
+    """Config: 1,048,576 triangles, 2^24 + 2^24 rays; every ray checked for
+    self-consistency, a 2^15 sample bit-exactly against the oracle."""
+    import torch
+
+    mesh = tpt_scenes.sphere_soup(seed=1)
+    g, s = build_both(ctx, [mesh], [tpt_scenes.identity_instance()])
+    rng = np.random.default_rng(0)
+    for rays in (tpt_scenes.incoherent_rays(1 << 24, seed=3), tpt_scenes.coherent_rays()):
+        n = rays.shape[1]
+        d = torch.from_numpy(rays).cuda()
+        prim = torch.empty(n, dtype=torch.int32, device="cuda")
+        t = torch.empty(n, dtype=torch.float32, device="cuda")
+        s.traverse_device(d.data_ptr(), n, 0, prim.data_ptr(), t.data_ptr(),
+                          stream=torch.cuda.current_stream().cuda_stream)
+        anyp = torch.empty_like(prim)
+        anyt = torch.empty_like(t)
+        s.traverse_device(d.data_ptr(), n, 1, anyp.data_ptr(), anyt.data_ptr(),
+                          stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        prim, t, anyp, anyt = prim.cpu().numpy(), t.cpu().numpy(), anyp.cpu().numpy(), anyt.cpu().numpy()
+        # properties over all rays: any-hit occludes exactly when closest-hit hits, never nearer
+        assert np.array_equal(prim >= 0, anyp >= 0)
+        assert np.all(anyt[prim >= 0] >= t[prim >= 0])
+        assert np.all(np.isinf(t[prim < 0]))
+        sample = rng.choice(n, 1 << 15, replace=False)
+        ref = g.query(np.ascontiguousarray(rays[:, sample]), 0)
+        assert np.array_equal(prim[sample], ref["prim"])
+        assert np.array_equal(t[sample].view(np.uint32), ref["t"].view(np.uint32))

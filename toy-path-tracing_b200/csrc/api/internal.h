@@ -1,0 +1,59 @@
+// Host-side objects behind the opaque C handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../../include/tpt.h"
+#include "../device/dev_types.cuh"
+#include "../host/host_types.h"
+
+struct tpt_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t* d_err = nullptr;  // device error word
+  int num_sms = 0;
+  std::string last_error;
+  // pinned staging for the host-pointer entry points
+  void* h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+  void* d_stage = nullptr;
+  size_t d_stage_bytes = 0;
+  cudaStream_t pipe[2] = {nullptr, nullptr};  // copy/compute pipeline of tpt_traverse
+  cudaEvent_t ev_slot[2] = {nullptr, nullptr};
+  cudaEvent_t ev_start = nullptr;
+};
+
+struct tpt_qbvh {
+  tpt::QbvhHost q;
+};
+
+struct tpt_scene {
+  tpt_context* ctx = nullptr;
+  tpt::DevGeometry geo{};
+  std::vector<void*> allocations;
+  uint64_t device_bytes = 0;
+  uint32_t num_meshes = 0;
+  uint32_t num_instances = 0;
+  std::vector<uint32_t> mesh_tri_counts;
+};
+
+namespace tpt {
+
+tpt_status set_error(tpt_context* ctx, tpt_status st, const std::string& msg);
+tpt_status cuda_check(tpt_context* ctx, cudaError_t e, const char* what);
+// Reads and clears the device error word (synchronising `stream`).
+tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream);
+
+// kernels (traverse_kernels.cu)
+cudaError_t launch_traverse(const DevGeometry& geo, const float* rays, uint64_t n, int mode, int32_t* prim, float* t,
+                            int32_t* inst, float* bary, uint32_t* node_tests, uint32_t* tri_tests, uint32_t* err,
+                            int num_sms, cudaStream_t stream);
+// Same, for a chunk of m rays whose planes (and bary output planes) are `stride` floats apart.
+cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t stride, uint64_t m, int mode,
+                                    int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t out_stride,
+                                    uint32_t* err, int num_sms, cudaStream_t stream);
+
+}  // namespace tpt

@@ -1,0 +1,291 @@
+"""Python binding of libtpt_cuda.so (the C ABI declared in include/tpt.h).
+
+This is the host-side mirror of the reference crate's scene/integrator API
+(`Scene::add_mesh / add_instance / build_qbvh / closest_hit`,
+`IntegratorKind::trace_radiance`) used by the tests and the benchmark.  It is a
+thin ctypes layer: every call goes through the C ABI, and there is no CPU
+fallback — loading fails loudly when the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libtpt_cuda.so")
+_lib = None
+
+TPT_OK = 0
+STATUS_NAMES = {
+    0: "TPT_OK",
+    1: "TPT_ERR_INVALID_ARG",
+    2: "TPT_ERR_OUT_OF_MEMORY",
+    3: "TPT_ERR_CUDA",
+    4: "TPT_ERR_CAPACITY",
+    5: "TPT_ERR_TIMEOUT",
+    6: "TPT_ERR_DEVICE_CHECK",
+    7: "TPT_ERR_NOT_BUILT",
+}
+CLOSEST_HIT = 0
+ANY_HIT = 1
+
+NODE_DTYPE = np.dtype(
+    [("b", "<f4", (6, 4)), ("children", "<u4", (4,)), ("valid_mask", "<u4"), ("pad", "<u4", (3,))]
+)
+
+
+class TptError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class QbvhView(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_void_p),
+        ("num_nodes", C.c_uint64),
+        ("primitive_indices", C.c_void_p),
+        ("num_primitives", C.c_uint64),
+    ]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("positions", C.c_void_p),
+        ("normals", C.c_void_p),
+        ("uvs", C.c_void_p),
+        ("num_vertices", C.c_uint64),
+        ("indices", C.c_void_p),
+        ("num_indices", C.c_uint64),
+        ("qbvh", QbvhView),
+    ]
+
+
+class InstanceDesc(C.Structure):
+    _fields_ = [
+        ("mesh_index", C.c_uint32),
+        ("material_index", C.c_uint32),
+        ("local_to_world", C.c_float * 16),
+        ("world_to_local", C.c_float * 16),
+        ("normal_to_world", C.c_float * 9),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("meshes", C.POINTER(MeshDesc)),
+        ("num_meshes", C.c_uint32),
+        ("instances", C.POINTER(InstanceDesc)),
+        ("num_instances", C.c_uint32),
+        ("tlas", QbvhView),
+    ]
+
+
+def lib():
+    """Load libtpt_cuda.so; raises when the CUDA build is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `make -C toy-path-tracing_b200` "
+                "(or __graft_entry__.build()); there is no CPU fallback"
+            )
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+EXPORTED_SYMBOLS = [
+    "tpt_context_create",
+    "tpt_context_destroy",
+    "tpt_last_error",
+    "tpt_version",
+    "tpt_qbvh_build",
+    "tpt_qbvh_view_of",
+    "tpt_qbvh_free",
+    "tpt_scene_upload",
+    "tpt_scene_release",
+    "tpt_scene_device_bytes",
+    "tpt_traverse",
+    "tpt_traverse_device",
+    "tpt_traverse_stats_device",
+]
+
+
+def _declare(L):
+    vp, u64, i32, cp = C.c_void_p, C.c_uint64, C.c_int, C.c_char_p
+    sig = {
+        "tpt_context_create": (i32, [i32, C.POINTER(vp)]),
+        "tpt_context_destroy": (i32, [vp]),
+        "tpt_last_error": (cp, [vp]),
+        "tpt_version": (cp, []),
+        "tpt_qbvh_build": (i32, [vp, u64, i32, C.POINTER(vp)]),
+        "tpt_qbvh_view_of": (i32, [vp, C.POINTER(QbvhView)]),
+        "tpt_qbvh_free": (i32, [vp]),
+        "tpt_scene_upload": (i32, [vp, C.POINTER(SceneDesc), C.POINTER(vp)]),
+        "tpt_scene_release": (i32, [vp]),
+        "tpt_scene_device_bytes": (i32, [vp, C.POINTER(u64)]),
+        "tpt_traverse": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp]),
+        "tpt_traverse_device": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp, vp]),
+        "tpt_traverse_stats_device": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(status: int, ctx=None):
+    if status != TPT_OK:
+        msg = lib().tpt_last_error(ctx.h if ctx is not None else None)
+        raise TptError(status, (msg or b"").decode())
+
+
+# --------------------------------------------------------------------------
+class Context:
+    """`tpt_context`: one CUDA device + stream."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().tpt_context_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tpt_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def build_qbvh(bounds: np.ndarray, threads: int = 0):
+    """Host builder (qbvh.rs `build_qbvh`): returns (nodes[NODE_DTYPE], primitive_indices[u32])."""
+    b = np.ascontiguousarray(bounds, np.float32).reshape(-1, 6)
+    h = C.c_void_p()
+    _check(lib().tpt_qbvh_build(_p(b), b.shape[0], threads, C.byref(h)))
+    try:
+        v = QbvhView()
+        _check(lib().tpt_qbvh_view_of(h, C.byref(v)))
+        nodes = np.zeros(v.num_nodes, NODE_DTYPE)
+        prims = np.zeros(v.num_primitives, np.uint32)
+        if v.num_nodes:
+            C.memmove(nodes.ctypes.data, v.nodes, nodes.nbytes)
+        C.memmove(prims.ctypes.data, v.primitive_indices, prims.nbytes)
+    finally:
+        lib().tpt_qbvh_free(h)
+    return nodes, prims
+
+
+def _view(q):
+    if q is None:
+        return QbvhView(None, 0, None, 0)
+    nodes, prims = q
+    return QbvhView(
+        nodes.ctypes.data if len(nodes) else None, len(nodes), prims.ctypes.data, len(prims)
+    )
+
+
+class Scene:
+    """Device-resident geometry (`tpt_scene`), uploaded from host arrays.
+
+    meshes: list of dicts with positions [V,3], indices [3T], optional normals,
+    uvs and a pre-built qbvh (nodes, prims).  instances: list of dicts with
+    mesh, material, local_to_world, world_to_local (4x4 column-major) and
+    normal_to_world (3x3)."""
+
+    def __init__(self, ctx: Context, meshes, instances, tlas=None):
+        self.ctx = ctx
+        keep = []
+        md = (MeshDesc * max(1, len(meshes)))()
+        for i, m in enumerate(meshes):
+            pos = np.ascontiguousarray(m["positions"], np.float32)
+            idx = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1)
+            nrm = m.get("normals")
+            uv = m.get("uvs")
+            nrm = None if nrm is None else np.ascontiguousarray(nrm, np.float32)
+            uv = None if uv is None else np.ascontiguousarray(uv, np.float32)
+            keep += [pos, idx, nrm, uv]
+            q = m.get("qbvh")
+            if q is not None:
+                q = (np.ascontiguousarray(q[0]), np.ascontiguousarray(q[1], np.uint32))
+                keep += list(q)
+            md[i] = MeshDesc(
+                pos.ctypes.data, None if nrm is None else nrm.ctypes.data, None if uv is None else uv.ctypes.data,
+                pos.shape[0], idx.ctypes.data, idx.size, _view(q)
+            )
+        idesc = (InstanceDesc * max(1, len(instances)))()
+        for i, inst in enumerate(instances):
+            d = InstanceDesc()
+            d.mesh_index = inst["mesh"]
+            d.material_index = inst.get("material", 0)
+            d.local_to_world[:] = np.asarray(inst["local_to_world"], np.float32).reshape(16).tolist()
+            d.world_to_local[:] = np.asarray(inst["world_to_local"], np.float32).reshape(16).tolist()
+            d.normal_to_world[:] = np.asarray(inst["normal_to_world"], np.float32).reshape(9).tolist()
+            idesc[i] = d
+        if tlas is not None:
+            tlas = (np.ascontiguousarray(tlas[0]), np.ascontiguousarray(tlas[1], np.uint32))
+            keep += list(tlas)
+        desc = SceneDesc(md, len(meshes), idesc, len(instances), _view(tlas))
+        h = C.c_void_p()
+        _check(lib().tpt_scene_upload(ctx.h, C.byref(desc), C.byref(h)), ctx)
+        self.h = h
+
+    def device_bytes(self) -> int:
+        v = C.c_uint64()
+        _check(lib().tpt_scene_device_bytes(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().tpt_scene_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- queries ----------------------------------------------------------
+    def closest_hit(self, rays: np.ndarray, mode: int = CLOSEST_HIT, want_instance=False, want_bary=False):
+        """Host arrays in/out through `tpt_traverse`. rays: float32 [7, n]."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[1]
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        inst = np.empty(n, np.int32) if want_instance else None
+        bary = np.empty((3, n), np.float32) if want_bary else None
+        _check(
+            lib().tpt_traverse(self.ctx.h, self.h, _p(rays), n, mode, _p(prim), _p(t), _p(inst), _p(bary)), self.ctx
+        )
+        out = {"prim": prim, "t": t}
+        if want_instance:
+            out["inst"] = inst
+        if want_bary:
+            out["bary"] = bary
+        return out
+
+    def traverse_device(self, rays_ptr: int, n: int, mode: int, prim_ptr: int, t_ptr: int, inst_ptr=None,
+                        bary_ptr=None, stream=None):
+        """Device pointers (e.g. torch tensor data_ptr()) and a cudaStream_t handle."""
+        _check(
+            lib().tpt_traverse_device(
+                self.ctx.h, self.h, C.c_void_p(rays_ptr), n, mode, C.c_void_p(prim_ptr), C.c_void_p(t_ptr),
+                C.c_void_p(inst_ptr) if inst_ptr else None, C.c_void_p(bary_ptr) if bary_ptr else None,
+                C.c_void_p(stream) if stream else None,
+            ),
+            self.ctx,
+        )
+
+    def traverse_stats_device(self, rays_ptr, n, mode, prim_ptr, t_ptr, nodes_ptr, tris_ptr, stream=None):
+        _check(
+            lib().tpt_traverse_stats_device(
+                self.ctx.h, self.h, C.c_void_p(rays_ptr), n, mode, C.c_void_p(prim_ptr), C.c_void_p(t_ptr),
+                C.c_void_p(nodes_ptr), C.c_void_p(tris_ptr), C.c_void_p(stream) if stream else None,
+            ),
+            self.ctx,
+        )
