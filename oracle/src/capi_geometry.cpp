@@ -251,3 +251,55 @@ void orc_camera_ray(const float* params, uint32_t rx, uint32_t ry, uint32_t px, 
 }
 
 }  // extern "C"
+
+extern "C" {
+// Step sequence of each closest-hit query in visit order: 'N' per 4-wide node
+// test, 'L' per BLAS leaf (one byte per step, zero-terminated, max_len bytes per
+// ray).  Used to model SIMT schedules of the device traversal on the CPU.
+void orc_geometry_step_sequence(void* gh, const float* rays, uint64_t n, char* out, uint32_t max_len, int nthreads) {
+  const Geometry* g = (const Geometry*)gh;
+  parallel_for(n, nthreads, [&](uint64_t i) {
+    Ray r = ray_from_soa(rays, n, i);
+    char* o = out + i * max_len;
+    uint32_t k = 0;
+    // replay Geometry::closest_hit with a recording leaf callback
+    if (g->instances.empty()) { o[0] = 0; return; }
+    float best_t = kInf;
+    traverse_qbvh(
+        g->tlas, r, kInf,
+        [&](uint32_t offset, uint32_t count, float cur) -> float {
+          float t_max = cur;
+          for (uint32_t oi = offset; oi < offset + count; ++oi) {
+            const Instance& inst = g->instances[g->tlas.primitive_indices[oi]];
+            Ray lr;
+            lr.origin = inst.world_to_local.transform_point3(r.origin);
+            lr.direction = inst.world_to_local.transform_vector3(r.direction);
+            const Mesh& mesh = g->meshes[inst.mesh_index];
+            TraversalStats st;
+            uint64_t last_nodes = 0;
+            traverse_qbvh(
+                mesh.qbvh, lr, t_max,
+                [&](uint32_t off2, uint32_t cnt2, float cur2) -> float {
+                  // node tests since the previous callback happened before this leaf
+                  for (; last_nodes < st.nodes && k + 1 < max_len; ++last_nodes) o[k++] = 'N';
+                  if (k + 1 < max_len) o[k++] = 'L';
+                  float tm = cur2;
+                  for (uint32_t q = off2; q < off2 + cnt2; ++q) {
+                    Vec3 v[3];
+                    mesh.triangle_positions(mesh.qbvh.primitive_indices[q], v);
+                    TriHit h;
+                    if (intersect_triangle(lr, tm, v[0], v[1], v[2], &h)) { tm = h.t; best_t = h.t; }
+                  }
+                  return tm;
+                },
+                nullptr, &st);
+            for (; last_nodes < st.nodes && k + 1 < max_len; ++last_nodes) o[k++] = 'N';
+            if (best_t < t_max) t_max = best_t;
+          }
+          return t_max;
+        },
+        nullptr, nullptr);
+    o[k] = 0;
+  });
+}
+}

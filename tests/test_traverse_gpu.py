@@ -154,7 +154,7 @@ def test_root_leaf_and_degenerate_and_empty(ctx):
     ref = g.query(rays, 0)
     dev = s.closest_hit(rays, 0)
     assert_same(dev, ref, "root leaf")
-    assert dev["prim"].tolist() == [0, -1, 0]
+    assert dev["prim"].tolist() == [0, -1, -1]  # third origin lies in the plane: t = 0 is rejected
     out = s.closest_hit(np.zeros((7, 0), np.float32))
     assert out["prim"].size == 0
 
@@ -170,7 +170,12 @@ def test_rejects_bad_scene(ctx):
 
 
 def test_fp64_brute_force_t(soup):
-    """Device t vs a float64 solve of the hit triangle (non-grazing hits)."""
+    """Device t vs a float64 solve of the hit triangle's plane (non-grazing hits).
+
+    Tolerance: 1e-5 relative, plus 16 ulp of the scene's coordinate scale
+    (2^-20 * 30 here): the f32 test subtracts the origin from vertices whose
+    coordinates reach 30, so its absolute t error cannot be below that scale
+    for hits close to the origin."""
     g, s = soup
     mesh = tpt_scenes.sphere_soup(seed=11, n_spheres=512, cube=30.0)
     rays = tpt_scenes.incoherent_rays(1 << 14, seed=13, cube=30.0)
@@ -184,9 +189,12 @@ def test_fp64_brute_force_t(soup):
     t64 = np.einsum("ij,ij->i", tri[:, 0] - o, n) / np.einsum("ij,ij->i", d, n)
     cosang = np.abs(np.einsum("ij,ij->i", d, n)) / np.linalg.norm(n, axis=1)
     ok = cosang > 0.05
-    rel = np.abs(dev["t"][hit] - t64) / np.abs(t64)
+    err = np.abs(dev["t"][hit] - t64)
+    tol = 1e-5 * np.abs(t64) + 2.0 ** -20 * 30.0
     assert ok.sum() > 100
-    assert np.all(rel[ok] <= 1e-5), rel[ok].max()
+    assert np.all(err[ok] <= tol[ok]), (err[ok] / tol[ok]).max()
+    far = ok & (t64 > 5.0)
+    assert np.all(err[far] <= 1e-5 * t64[far] + 2.0 ** -20 * 30.0)
 
 
 def test_full_size_traversal_against_oracle_sample(ctx):

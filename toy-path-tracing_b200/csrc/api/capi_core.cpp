@@ -47,6 +47,11 @@ tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream) {
   return set_error(ctx, TPT_ERR_DEVICE_CHECK, "device index check failed (flags " + std::to_string(h) + ")");
 }
 
+unsigned long long* next_counter(tpt_context* ctx) {
+  uint32_t k = ctx->counter_next++ % kCounterSlots;
+  return ctx->d_counters + k;
+}
+
 }  // namespace tpt
 
 using namespace tpt;
@@ -209,6 +214,12 @@ tpt_status tpt_context_create(int device, tpt_context** out) {
     return cuda_check(nullptr, e, "cudaMalloc(error word)");
   }
   cudaMemset(ctx->d_err, 0, 256);
+  if ((e = cudaMalloc(&ctx->d_counters, kCounterSlots * sizeof(unsigned long long))) != cudaSuccess) {
+    cudaFree(ctx->d_err);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return cuda_check(nullptr, e, "cudaMalloc(counters)");
+  }
   *out = ctx;
   return TPT_OK;
 }
@@ -220,6 +231,7 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->d_stage) cudaFree(ctx->d_stage);
   if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->d_counters) cudaFree(ctx->d_counters);
   for (int k = 0; k < 2; ++k) {
     if (ctx->pipe[k]) cudaStreamDestroy(ctx->pipe[k]);
     if (ctx->ev_slot[k]) cudaEventDestroy(ctx->ev_slot[k]);
@@ -458,8 +470,8 @@ tpt_status tpt_traverse_device(tpt_context* ctx, const tpt_scene* scene, const f
   if (mode != TPT_CLOSEST_HIT && mode != TPT_ANY_HIT) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad mode");
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   return cuda_check(ctx,
-                    launch_traverse(scene->geo, rays, n, mode, prim, t, instance, bary, nullptr, nullptr, ctx->d_err,
-                                    ctx->num_sms, s),
+                    launch_traverse_strided(scene->geo, rays, n, n, mode, prim, t, instance, bary, n,
+                                            next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr, nullptr),
                     "traverse kernel launch");
 }
 
@@ -472,8 +484,9 @@ tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, c
   if (mode != TPT_CLOSEST_HIT && mode != TPT_ANY_HIT) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad mode");
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   tpt_status st = cuda_check(ctx,
-                             launch_traverse(scene->geo, rays, n, mode, prim, t, nullptr, nullptr, node_tests,
-                                             tri_tests, ctx->d_err, ctx->num_sms, s),
+                             launch_traverse_strided(scene->geo, rays, n, n, mode, prim, t, nullptr, nullptr, n,
+                                                     next_counter(ctx), ctx->d_err, ctx->num_sms, s, node_tests,
+                                                     tri_tests),
                              "traverse kernel launch");
   if (st) return st;
   return check_device_errors(ctx, s);
@@ -530,7 +543,7 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
     // the kernel reads plane p of the chunk at d_rays + p*n + b: pass a view with stride n
     cudaError_t e = launch_traverse_strided(scene->geo, d_rays + b, n, m, mode, d_prim + b, d_t + b,
                                             d_inst ? d_inst + b : nullptr, d_bary ? d_bary + b : nullptr, n,
-                                            ctx->d_err, ctx->num_sms, s);
+                                            next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr, nullptr);
     if ((st = cuda_check(ctx, e, "traverse kernel launch"))) return st;
     struct Out { void* host; const void* dev; size_t planes; };
     Out outs[4] = {{prim, d_prim, 1}, {t, d_t, 1}, {instance, d_inst, 1}, {bary, d_bary, 3}};

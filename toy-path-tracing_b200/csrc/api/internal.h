@@ -24,6 +24,8 @@ struct tpt_context {
   cudaStream_t pipe[2] = {nullptr, nullptr};  // copy/compute pipeline of tpt_traverse
   cudaEvent_t ev_slot[2] = {nullptr, nullptr};
   cudaEvent_t ev_start = nullptr;
+  unsigned long long* d_counters = nullptr;  // work-distribution counters, one per in-flight launch
+  uint32_t counter_next = 0;
 };
 
 struct tpt_qbvh {
@@ -42,18 +44,22 @@ struct tpt_scene {
 
 namespace tpt {
 
+constexpr uint32_t kCounterSlots = 1024;
+
 tpt_status set_error(tpt_context* ctx, tpt_status st, const std::string& msg);
 tpt_status cuda_check(tpt_context* ctx, cudaError_t e, const char* what);
 // Reads and clears the device error word (synchronising `stream`).
 tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream);
 
-// kernels (traverse_kernels.cu)
-cudaError_t launch_traverse(const DevGeometry& geo, const float* rays, uint64_t n, int mode, int32_t* prim, float* t,
-                            int32_t* inst, float* bary, uint32_t* node_tests, uint32_t* tri_tests, uint32_t* err,
-                            int num_sms, cudaStream_t stream);
-// Same, for a chunk of m rays whose planes (and bary output planes) are `stride` floats apart.
-cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t stride, uint64_t m, int mode,
-                                    int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t out_stride,
-                                    uint32_t* err, int num_sms, cudaStream_t stream);
+// kernels (traverse_kernels.cu).  Ray plane p of ray i at rays[p * rs + i];
+// barycentric output plane p at bary[p * bs + i].  `counter` is a device word
+// the launch resets and uses for its work distribution (one per concurrent launch).
+cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
+                                    int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
+                                    unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t stream,
+                                    uint32_t* node_tests, uint32_t* tri_tests);
+
+// A work counter slot for the next launch (ring of kCounterSlots per context).
+unsigned long long* next_counter(tpt_context* ctx);
 
 }  // namespace tpt

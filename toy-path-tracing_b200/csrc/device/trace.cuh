@@ -149,33 +149,6 @@ __device__ __forceinline__ uint32_t box4(const DevNode* __restrict__ n, const Ra
   return mask;
 }
 
-// Stable ascending order of the hit lanes by entry distance; returns the
-// child words sorted far-to-near in w[0..n).  Missing lanes sort last.
-__device__ __forceinline__ int order_far_to_near(uint32_t mask, const float tmin[4], const uint32_t ch[4],
-                                                 uint32_t w[4]) {
-  float k[4];
-  int s[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    bool v = (mask >> i) & 1u;
-    k[i] = v ? tmin[i] : __int_as_float(0x7f800000);
-    s[i] = v ? i : 4 + i;
-    w[i] = ch[i];
-  }
-  // 5-comparator network on (key, lane) pairs: a total order, so any correct
-  // network reproduces the reference's stable insertion sort.
-#define TPT_CS(a, b)                                                           \
-  {                                                                            \
-    bool sw = (k[a] > k[b]) || (k[a] == k[b] && s[a] > s[b]);                  \
-    float tk = sw ? k[b] : k[a]; k[b] = sw ? k[a] : k[b]; k[a] = tk;           \
-    int ts = sw ? s[b] : s[a]; s[b] = sw ? s[a] : s[b]; s[a] = ts;             \
-    uint32_t tw = sw ? w[b] : w[a]; w[b] = sw ? w[a] : w[b]; w[a] = tw;        \
-  }
-  TPT_CS(0, 1) TPT_CS(2, 3) TPT_CS(0, 2) TPT_CS(1, 3) TPT_CS(1, 2)
-#undef TPT_CS
-  return __popc(mask);
-}
-
 struct TraceResult {
   float t;
   int32_t tri;
@@ -188,97 +161,223 @@ struct TraceCounters {
   uint32_t tris;
 };
 
-// MODE 0: closest hit.  MODE 1: stop at the first accepted triangle.
-// Returns false only on a device check failure (stack overflow), in which case
-// *err receives the flag.
-template <int MODE, bool STATS>
-__device__ __forceinline__ bool trace_ray(const DevGeometry& G, float ox, float oy, float oz, float dx, float dy,
-                                          float dz, float t_max, TraceResult& res, TraceCounters& cnt,
+// Per-thread traversal stack: the first SH entries live in shared memory
+// (entry k of thread i at base[k * blockDim.x], bank-conflict free), deeper
+// entries in a local-memory spill area.  Total depth kStackDepth (qbvh.rs:609).
+template <int SH>
+struct SplitStack {
+  uint32_t* sh;
+  uint32_t spill[kStackDepth - SH];
+  __device__ __forceinline__ void set(int k, uint32_t v) {
+    if (k < SH) sh[k * blockDim.x] = v;
+    else spill[k - SH] = v;
+  }
+  __device__ __forceinline__ uint32_t get(int k) const { return k < SH ? sh[k * blockDim.x] : spill[k - SH]; }
+};
+
+// Stack entries: interior node (bit 31 clear), BLAS/TLAS leaf (bit 31, count
+// >= 1), instance marker (bit 31, count 0, instance id), or kNone.  kNone can
+// never be a real leaf word: the upload rejects leaf ranges past 2^24.
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// Traversal of one ray, advanced one entry at a time.  `next` holds the entry
+// to process next (the would-be top of the stack kept in a register).
+struct TravState {
+  float wox, woy, woz, wdx, wdy, wdz;  // world-space ray
+  RayPre r;                            // ray of the current level (world at the TLAS, instance space in a BLAS)
+  float closest;                       // running t_max
+  TraceResult res;
+  uint32_t next;
+  int sp, floor_sp;
+  bool in_blas;
+  uint32_t node_base, tri_base, inst_id;
+};
+
+// Enter instance `id`'s BLAS with the ray transformed by world_to_local
+// (glam Mat4::transform_point3 / transform_vector3 order), scene/mod.rs:357.
+__device__ __forceinline__ void enter_instance(const DevGeometry& G, TravState& s, uint32_t id) {
+  s.inst_id = id;
+  const DevInstance* I = G.instances + id;
+  const float4 m0 = __ldg(&I->m0), m1 = __ldg(&I->m1), m2 = __ldg(&I->m2);
+  const uint4 meta = __ldg(reinterpret_cast<const uint4*>(&I->node_base));
+  const float ox = s.wox, oy = s.woy, oz = s.woz, dx = s.wdx, dy = s.wdy, dz = s.wdz;
+  float lox = m0.x * ox, loy = m0.y * ox, loz = m0.z * ox;
+  lox = m0.w * oy + lox; loy = m1.x * oy + loy; loz = m1.y * oy + loz;
+  lox = m1.z * oz + lox; loy = m1.w * oz + loy; loz = m2.x * oz + loz;
+  lox = m2.y + lox; loy = m2.z + loy; loz = m2.w + loz;
+  float ldx = m0.x * dx, ldy = m0.y * dx, ldz = m0.z * dx;
+  ldx = m0.w * dy + ldx; ldy = m1.x * dy + ldy; ldz = m1.y * dy + ldz;
+  ldx = m1.z * dz + ldx; ldy = m1.w * dz + ldy; ldz = m2.x * dz + ldz;
+  ray_setup(s.r, lox, loy, loz, ldx, ldy, ldz);
+  s.node_base = meta.x;
+  s.tri_base = meta.y;
+  s.in_blas = true;
+  s.floor_sp = s.sp;
+  s.next = meta.z;
+}
+
+template <class Stack>
+__device__ __forceinline__ void trav_pop(TravState& s, Stack& st) {
+  if (s.sp == 0) {
+    s.next = kNone;
+    return;
+  }
+  if (s.in_blas && s.sp == s.floor_sp) {
+    // the instance's BLAS is done: back to the TLAS with the world ray
+    s.in_blas = false;
+    ray_setup(s.r, s.wox, s.woy, s.woz, s.wdx, s.wdy, s.wdz);
+  }
+  s.next = st.get(--s.sp);
+}
+
+__device__ __forceinline__ void trav_init(const DevGeometry& G, TravState& s, float ox, float oy, float oz, float dx,
+                                          float dy, float dz, float t_max) {
+  s.wox = ox; s.woy = oy; s.woz = oz; s.wdx = dx; s.wdy = dy; s.wdz = dz;
+  s.closest = t_max;
+  s.res.t = __int_as_float(0x7f800000);
+  s.res.tri = -1;
+  s.res.inst = -1;
+  s.res.b0 = s.res.b1 = s.res.b2 = 0.0f;
+  s.in_blas = false;
+  s.floor_sp = 0;
+  s.sp = 0;
+  s.node_base = s.tri_base = s.inst_id = 0;
+  s.next = kNone;
+  if (G.num_instances == 0) return;
+  const uint32_t root = G.tlas_root_word;
+  if ((root & kLeafBit) && ((root >> 24) & 0x7Fu) == 1u) {
+    // TLAS is a single-instance root leaf (qbvh.rs:615-620): go straight to it
+    enter_instance(G, s, __ldg(G.tlas_prims + (root & 0xFFFFFFu)));
+  } else {
+    ray_setup(s.r, ox, oy, oz, dx, dy, dz);
+    s.next = root;
+  }
+}
+
+// Processes the interior node in `next`.  The hit children end up, bottom to
+// top, as interiors far-to-near then leaves near-to-far (qbvh.rs:640-671: leaves
+// are handled far-to-near at once, the nearest interior is popped first); the
+// would-be top becomes `next`, the rest go to the stack.
+template <bool STATS, class Stack>
+__device__ __forceinline__ void node_step(const DevGeometry& G, TravState& s, Stack& st, TraceCounters& cnt,
                                           uint32_t* err) {
-  uint32_t stack[kStackDepth];
-  int sp = 0;
-  float closest = t_max;
-  res.t = __int_as_float(0x7f800000);
-  res.tri = -1;
-  res.inst = -1;
-  res.b0 = res.b1 = res.b2 = 0.0f;
-  if (STATS) { cnt.nodes = 0; cnt.tris = 0; }
-  if (G.num_instances == 0) return true;
+  const DevNode* n = G.nodes + (s.in_blas ? s.node_base : G.tlas_node_base) + s.next;
+  if (STATS) cnt.nodes++;
+  float tmin[4];
+  uint32_t ch[4];
+  const uint32_t mask = box4(n, s.r, s.closest, tmin, ch);
+  const int nh = __popc(mask);
+  if (nh == 0) {
+    trav_pop(s, st);
+    return;
+  }
+  if (nh == 1) {
+    s.next = (mask & 1u) ? ch[0] : (mask & 2u) ? ch[1] : (mask & 4u) ? ch[2] : ch[3];
+    return;
+  }
+  if (s.sp + nh - 1 > kStackDepth) {
+    atomicOr(err, kDevErrStackOverflow);
+    s.sp = 0;
+    s.next = kNone;
+    return;
+  }
+  // before[i][j]: lane i precedes lane j in the stable ascending order by tmin
+  bool v[4], leaf[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v[i] = (mask >> i) & 1u;
+    leaf[i] = (ch[i] & kLeafBit) != 0;
+  }
+  bool pre[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = i + 1; j < 4; ++j) {
+      pre[i][j] = tmin[i] <= tmin[j];
+      pre[j][i] = !pre[i][j];
+    }
+  int n_int = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) n_int += (v[i] && !leaf[i]) ? 1 : 0;
+  const int top = nh - 1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (!v[i]) continue;
+    int pos = 0;
+    if (!leaf[i]) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j != i && v[j] && !leaf[j] && pre[i][j]) ++pos;  // interiors farther than i
+    } else {
+      pos = n_int;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j != i && v[j] && leaf[j] && pre[j][i]) ++pos;  // leaves nearer than i
+    }
+    if (pos == top) s.next = ch[i];
+    else st.set(s.sp + pos, ch[i]);
+  }
+  s.sp += nh - 1;
+}
 
-  RayPre world, local;
-  ray_setup(world, ox, oy, oz, dx, dy, dz);
-  bool in_blas = false;
-  int floor_sp = 0;
-  uint32_t node_base = 0, tri_base = 0, inst_id = 0;
-
-  stack[sp++] = G.tlas_root_word;
-  while (sp > 0) {
-    if (in_blas && sp == floor_sp) in_blas = false;
-    const uint32_t w = stack[--sp];
-    if (w & kLeafBit) {
-      const uint32_t count = (w >> 24) & 0x7Fu, off = w & 0xFFFFFFu;
-      if (!in_blas) {
-        if (count == 0) {
-          // instance marker: enter its BLAS with the ray in instance space
-          inst_id = off;
-          const DevInstance* I = G.instances + inst_id;
-          const float4 m0 = __ldg(&I->m0), m1 = __ldg(&I->m1), m2 = __ldg(&I->m2);
-          const uint4 meta = __ldg(reinterpret_cast<const uint4*>(&I->node_base));
-          // res = c0*x; res = c1*y + res; res = c2*z + res; (+ c3 for points)
-          float lox = m0.x * ox, loy = m0.y * ox, loz = m0.z * ox;
-          lox = m0.w * oy + lox; loy = m1.x * oy + loy; loz = m1.y * oy + loz;
-          lox = m1.z * oz + lox; loy = m1.w * oz + loy; loz = m2.x * oz + loz;
-          lox = m2.y + lox; loy = m2.z + loy; loz = m2.w + loz;
-          float ldx = m0.x * dx, ldy = m0.y * dx, ldz = m0.z * dx;
-          ldx = m0.w * dy + ldx; ldy = m1.x * dy + ldy; ldz = m1.y * dy + ldz;
-          ldx = m1.z * dz + ldx; ldy = m1.w * dz + ldy; ldz = m2.x * dz + ldz;
-          ray_setup(local, lox, loy, loz, ldx, ldy, ldz);
-          node_base = meta.x;
-          tri_base = meta.y;
-          in_blas = true;
-          floor_sp = sp;
-          stack[sp++] = meta.z;
-        } else {
-          // TLAS leaf: its instances in order
-          if (sp + (int)count > kStackDepth) { atomicOr(err, kDevErrStackOverflow); return false; }
-          for (int j = (int)count - 1; j >= 0; --j) stack[sp++] = kLeafBit | __ldg(G.tlas_prims + off + j);
-        }
-      } else {
-        // BLAS leaf: triangles in leaf order, t_max shrinking on each hit
-        for (uint32_t j = 0; j < count; ++j) {
-          const DevTri* T = G.tris + tri_base + off + j;
-          DevTri tri;
-          tri.v0 = __ldg(&T->v0); tri.v1 = __ldg(&T->v1); tri.v2 = __ldg(&T->v2);
-          if (STATS) cnt.tris++;
-          float t, b0, b1, b2;
-          if (tri_test(local, closest, tri, t, b0, b1, b2)) {
-            closest = t;
-            res.t = t; res.tri = __float_as_int(tri.v0.w); res.inst = (int32_t)inst_id;
-            res.b0 = b0; res.b1 = b1; res.b2 = b2;
-            if (MODE == 1) return true;
-          }
+// Processes the leaf, TLAS leaf or instance marker in `next`.
+template <int MODE, bool STATS, class Stack>
+__device__ __forceinline__ void leaf_step(const DevGeometry& G, TravState& s, Stack& st, TraceCounters& cnt,
+                                          uint32_t* err) {
+  const uint32_t w = s.next;
+  const uint32_t count = (w >> 24) & 0x7Fu, off = w & 0xFFFFFFu;
+  if (s.in_blas) {
+    // BLAS leaf: triangles in leaf order, t_max shrinking on each hit
+    const DevTri* T = G.tris + s.tri_base + off;
+    for (uint32_t j = 0; j < count; ++j) {
+      DevTri tri;
+      tri.v0 = __ldg(&T[j].v0);
+      tri.v1 = __ldg(&T[j].v1);
+      tri.v2 = __ldg(&T[j].v2);
+      if (STATS) cnt.tris++;
+      float t, b0, b1, b2;
+      if (tri_test(s.r, s.closest, tri, t, b0, b1, b2)) {
+        s.closest = t;
+        s.res.t = t;
+        s.res.tri = __float_as_int(tri.v0.w);
+        s.res.inst = (int32_t)s.inst_id;
+        s.res.b0 = b0; s.res.b1 = b1; s.res.b2 = b2;
+        if (MODE == 1) {
+          s.sp = 0;
+          s.next = kNone;
+          return;
         }
       }
-    } else {
-      const RayPre& r = in_blas ? local : world;
-      const DevNode* n = G.nodes + (in_blas ? node_base : G.tlas_node_base) + w;
-      if (STATS) cnt.nodes++;
-      float tmin[4];
-      uint32_t ch[4];
-      uint32_t mask = box4(n, r, closest, tmin, ch);
-      if (mask == 0) continue;
-      uint32_t sorted[4];
-      int nh = order_far_to_near(mask, tmin, ch, sorted);
-      if (sp + nh > kStackDepth) { atomicOr(err, kDevErrStackOverflow); return false; }
-      // interior children far-to-near (nearest on top), then leaves near-to-far
-      // (farthest on top): pops give leaves far-to-near, then nearest interior.
-      for (int k = nh - 1; k >= 0; --k)
-        if (!(sorted[k] & kLeafBit)) stack[sp++] = sorted[k];
-      for (int k = 0; k < nh; ++k)
-        if (sorted[k] & kLeafBit) stack[sp++] = sorted[k];
     }
+    trav_pop(s, st);
+  } else if (count == 0) {
+    enter_instance(G, s, off);
+  } else {
+    // TLAS leaf: its instances in order; the first is entered now
+    if (s.sp + (int)count > kStackDepth) {
+      atomicOr(err, kDevErrStackOverflow);
+      s.sp = 0;
+      s.next = kNone;
+      return;
+    }
+    for (int j = (int)count - 1; j >= 1; --j) st.set(s.sp++, kLeafBit | __ldg(G.tlas_prims + off + j));
+    enter_instance(G, s, __ldg(G.tlas_prims + off));
   }
-  return true;
+}
+
+// One thread traces one ray to the end (used where a thread owns its ray).
+template <int MODE, bool STATS, class Stack>
+__device__ __forceinline__ void trace_ray(const DevGeometry& G, Stack& st, float ox, float oy, float oz, float dx,
+                                          float dy, float dz, float t_max, TraceResult& res, TraceCounters& cnt,
+                                          uint32_t* err) {
+  TravState s;
+  trav_init(G, s, ox, oy, oz, dx, dy, dz, t_max);
+  if (STATS) { cnt.nodes = 0; cnt.tris = 0; }
+  while (s.next != kNone) {
+    if (!(s.next & kLeafBit)) node_step<STATS>(G, s, st, cnt, err);
+    else leaf_step<MODE, STATS>(G, s, st, cnt, err);
+  }
+  res = s.res;
 }
 
 }  // namespace tpt

@@ -1,36 +1,111 @@
 // Batch ray-query kernels: `Scene::closest_hit` over a structure-of-arrays
 // ray batch (scene/mod.rs:340-395), plus the any-hit occlusion variant.
+//
+// Persistent warps, "while-while" order: each warp keeps 32 rays in flight;
+// lanes step through interior nodes together until every lane faces a leaf
+// (or enough lanes have finished to be worth a refill), then all leaves are
+// tested together, then finished lanes get new rays from a global counter by
+// one warp-aggregated atomic.  Batching keeps the warp on one code path at a
+// time without changing any ray's own visit order.
+// Traversal stacks: 32 entries per thread in shared memory, spilling to local
+// memory beyond that (total depth 128, as the reference).
 #include "../api/internal.h"
 #include "../device/trace.cuh"
 
 namespace tpt {
 
+constexpr int kBlock = 128;
+constexpr int kShStack = 32;
+#ifndef TPT_TRAV_MINB
+#define TPT_TRAV_MINB 8
+#endif
+#ifndef TPT_REFILL_MIN
+#define TPT_REFILL_MIN 12  // finished lanes that end the node phase early for a refill
+#endif
+
 template <int MODE, bool STATS, bool BARY>
-__global__ void __launch_bounds__(128) traverse_kernel(DevGeometry geo, const float* __restrict__ rays, uint64_t rs, uint64_t n,
-                                                       uint64_t bs, int32_t* __restrict__ prim, float* __restrict__ tout,
-                                                       int32_t* __restrict__ inst, float* __restrict__ bary,
-                                                       uint32_t* __restrict__ node_tests,
-                                                       uint32_t* __restrict__ tri_tests, uint32_t* err) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    // plane p of ray i at rays[p * rs + i]
-    const float ox = __ldcs(rays + i), oy = __ldcs(rays + rs + i), oz = __ldcs(rays + 2 * rs + i);
-    const float dx = __ldcs(rays + 3 * rs + i), dy = __ldcs(rays + 4 * rs + i), dz = __ldcs(rays + 5 * rs + i);
-    const float tmax = MODE == 0 ? __int_as_float(0x7f800000) : __ldcs(rays + 6 * rs + i);
-    TraceResult r;
-    TraceCounters c;
-    trace_ray<MODE, STATS>(geo, ox, oy, oz, dx, dy, dz, tmax, r, c, err);
-    __stcs(prim + i, r.tri);
-    __stcs(tout + i, r.t);
-    if (inst) __stcs(inst + i, r.inst);
-    if (BARY) {
-      __stcs(bary + i, r.b0);
-      __stcs(bary + bs + i, r.b1);
-      __stcs(bary + 2 * bs + i, r.b2);
+__global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
+    traverse_kernel(DevGeometry geo, const float* __restrict__ rays, uint64_t rs, uint64_t n, uint64_t bs,
+                    int32_t* __restrict__ prim, float* __restrict__ tout, int32_t* __restrict__ inst,
+                    float* __restrict__ bary, uint32_t* __restrict__ node_tests, uint32_t* __restrict__ tri_tests,
+                    unsigned long long* __restrict__ counter, uint32_t* err) {
+  __shared__ uint32_t stack_sh[kShStack * kBlock];
+  SplitStack<kShStack> st;
+  st.sh = stack_sh + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  TravState s;
+  TraceCounters c;
+  int64_t ray = -1;  // -1: needs a ray, -2: no rays left, >= 0: active ray index
+  int stalled = 0;   // consecutive iterations in which no lane of the warp advanced
+  for (;;) {
+    bool moved = false;
+    // refill finished lanes: one warp-aggregated atomic, converged ray setup
+    const unsigned need = __ballot_sync(0xffffffffu, ray == -1);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (ray == -1) {
+        const uint64_t i = base + __popc(need & lt_mask);
+        moved = true;
+        if (i < n) {
+          ray = (int64_t)i;
+          // plane p of ray i at rays[p * rs + i]
+          const float ox = __ldcs(rays + i), oy = __ldcs(rays + rs + i), oz = __ldcs(rays + 2 * rs + i);
+          const float dx = __ldcs(rays + 3 * rs + i), dy = __ldcs(rays + 4 * rs + i), dz = __ldcs(rays + 5 * rs + i);
+          const float tmax = MODE == 0 ? __int_as_float(0x7f800000) : __ldcs(rays + 6 * rs + i);
+          trav_init(geo, s, ox, oy, oz, dx, dy, dz, tmax);
+          if (STATS) { c.nodes = 0; c.tris = 0; }
+        } else {
+          ray = -2;
+        }
+      }
     }
-    if (STATS) {
-      node_tests[i] = c.nodes;
-      tri_tests[i] = c.tris;
+    if (__all_sync(0xffffffffu, ray == -2)) break;
+    const bool active = ray >= 0;
+    // phase A: interior nodes until every active lane faces a leaf, or until
+    // enough lanes have finished their ray to be worth a refill (lanes with no
+    // ray left do not count: they can never be refilled)
+    for (;;) {
+      const bool want = active && !(s.next & kLeafBit);
+      if (!__any_sync(0xffffffffu, want)) break;
+      if (__popc(__ballot_sync(0xffffffffu, active && s.next == kNone)) >= TPT_REFILL_MIN) break;
+      if (want) {
+        node_step<STATS>(geo, s, st, c, err);
+        moved = true;
+      }
+    }
+    // phase B: one leaf / instance entry per lane
+    if (active && s.next != kNone && (s.next & kLeafBit)) {
+      leaf_step<MODE, STATS>(geo, s, st, c, err);
+      moved = true;
+    }
+    if (active && s.next == kNone) {
+      moved = true;
+      const uint64_t i = (uint64_t)ray;
+      __stcs(prim + i, s.res.tri);
+      __stcs(tout + i, s.res.t);
+      if (inst) __stcs(inst + i, s.res.inst);
+      if (BARY) {
+        __stcs(bary + i, s.res.b0);
+        __stcs(bary + bs + i, s.res.b1);
+        __stcs(bary + 2 * bs + i, s.res.b2);
+      }
+      if (STATS) {
+        node_tests[i] = c.nodes;
+        tri_tests[i] = c.tris;
+      }
+      ray = -1;
+    }
+    // watchdog: every iteration must advance some lane; if none does for a
+    // long run, flag the launch and stop instead of spinning
+    if (__any_sync(0xffffffffu, moved)) {
+      stalled = 0;
+    } else if (++stalled > 64) {
+      if (lane == 0) atomicOr(err, kDevErrTimeout);
+      break;
     }
   }
 }
@@ -38,22 +113,31 @@ __global__ void __launch_bounds__(128) traverse_kernel(DevGeometry geo, const fl
 template <int MODE, bool STATS, bool BARY>
 static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, uint64_t bs,
                             int32_t* prim, float* t, int32_t* inst, float* bary, uint32_t* nt, uint32_t* tt,
-                            uint32_t* err, int num_sms, cudaStream_t s) {
-  const int block = 128;
-  uint64_t blocks = (n + block - 1) / block;
-  const uint64_t cap = (uint64_t)num_sms * 64;  // grid-stride beyond ~64 blocks per SM
-  if (blocks > cap) blocks = cap;
-  if (blocks == 0) return cudaSuccess;
-  traverse_kernel<MODE, STATS, BARY><<<(unsigned)blocks, block, 0, s>>>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, err);
+                            unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  static int blocks_per_sm = 0;
+  if (blocks_per_sm == 0) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, traverse_kernel<MODE, STATS, BARY>,
+                                                                  kBlock, 0);
+    if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 4;
+  }
+  uint64_t blocks = (uint64_t)num_sms * blocks_per_sm;
+  const uint64_t need = (n + kBlock - 1) / kBlock;
+  if (blocks > need) blocks = need;
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  traverse_kernel<MODE, STATS, BARY>
+      <<<(unsigned)blocks, kBlock, 0, s>>>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
-                                    uint32_t* err, int num_sms, cudaStream_t s, uint32_t* nt, uint32_t* tt) {
+                                    unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
+                                    uint32_t* nt, uint32_t* tt) {
   const bool stats = nt != nullptr;
   const bool b = bary != nullptr;
-#define TPT_L(M, S, B) launch_t<M, S, B>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, err, num_sms, s)
+#define TPT_L(M, S, B) launch_t<M, S, B>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, err, num_sms, s)
   if (mode == 0) {
     if (stats) return TPT_L(0, true, false);
     if (b) return TPT_L(0, false, true);
@@ -63,18 +147,6 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
   if (b) return TPT_L(1, false, true);
   return TPT_L(1, false, false);
 #undef TPT_L
-}
-
-cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
-                                    int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
-                                    uint32_t* err, int num_sms, cudaStream_t s) {
-  return launch_traverse_strided(geo, rays, rs, n, mode, prim, t, inst, bary, bs, err, num_sms, s, nullptr, nullptr);
-}
-
-cudaError_t launch_traverse(const DevGeometry& geo, const float* rays, uint64_t n, int mode, int32_t* prim, float* t,
-                            int32_t* inst, float* bary, uint32_t* nt, uint32_t* tt, uint32_t* err, int num_sms,
-                            cudaStream_t s) {
-  return launch_traverse_strided(geo, rays, n, n, mode, prim, t, inst, bary, n, err, num_sms, s, nt, tt);
 }
 
 }  // namespace tpt

@@ -141,6 +141,14 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def _stream(handle):
+    """cudaStream_t for the C ABI: None = the context's own stream; the legacy
+    default stream (handle 0, torch's default) maps to cudaStreamLegacy."""
+    if handle is None:
+        return None
+    return C.c_void_p(1 if handle == 0 else handle)
+
+
 def _check(status: int, ctx=None):
     if status != TPT_OK:
         msg = lib().tpt_last_error(ctx.h if ctx is not None else None)
@@ -276,7 +284,7 @@ class Scene:
             lib().tpt_traverse_device(
                 self.ctx.h, self.h, C.c_void_p(rays_ptr), n, mode, C.c_void_p(prim_ptr), C.c_void_p(t_ptr),
                 C.c_void_p(inst_ptr) if inst_ptr else None, C.c_void_p(bary_ptr) if bary_ptr else None,
-                C.c_void_p(stream) if stream else None,
+                _stream(stream),
             ),
             self.ctx,
         )
@@ -285,7 +293,7 @@ class Scene:
         _check(
             lib().tpt_traverse_stats_device(
                 self.ctx.h, self.h, C.c_void_p(rays_ptr), n, mode, C.c_void_p(prim_ptr), C.c_void_p(t_ptr),
-                C.c_void_p(nodes_ptr), C.c_void_p(tris_ptr), C.c_void_p(stream) if stream else None,
+                C.c_void_p(nodes_ptr), C.c_void_p(tris_ptr), _stream(stream),
             ),
             self.ctx,
         )
