@@ -112,6 +112,45 @@ typedef struct tpt_instance_desc {
   float normal_to_world[9];
 } tpt_instance_desc;
 
+/* Materials in scope (material/mod.rs:99-115 subset). */
+typedef enum tpt_material_kind {
+  TPT_MATERIAL_NORMALIZED_LAMBERT = 0, /* NormalizedLambertMaterial::new(rho) */
+  TPT_MATERIAL_EMISSIVE = 1,           /* EmissiveMaterial::new(color, strength): two-sided pure emitter */
+  TPT_MATERIAL_OPENPBR = 2             /* OpenPbrMaterial (untextured), parameters in `openpbr` */
+} tpt_material_kind;
+
+struct tpt_openpbr_desc;
+
+typedef struct tpt_material_desc {
+  uint32_t kind;
+  float rho[3];     /* NormalizedLambert albedo */
+  float color[3];   /* Emissive colour */
+  float strength;   /* Emissive strength */
+  const struct tpt_openpbr_desc* openpbr;
+} tpt_material_desc;
+
+/* One node of the SG light tree (light_tree/mod.rs:65-86), 64 bytes:
+ * interior nodes have leaf_instance == leaf_triangle == 0xFFFFFFFF; leaves name
+ * the emissive triangle and carry its area.  Children/parent are node
+ * indices (0xFFFFFFFF = none). */
+typedef struct tpt_light_node {
+  float flux;
+  float mu[3];
+  float sigma_s2;
+  float nu[3];
+  float lambda;
+  float radius;
+  uint32_t left, right, parent;
+  uint32_t leaf_instance, leaf_triangle;
+  float area;
+} tpt_light_node;
+
+typedef struct tpt_light_tree_view {
+  const tpt_light_node* nodes;
+  uint64_t num_nodes;
+  uint32_t root;
+} tpt_light_tree_view;
+
 typedef struct tpt_scene_desc {
   const tpt_mesh_desc* meshes;
   uint32_t num_meshes;
@@ -120,6 +159,12 @@ typedef struct tpt_scene_desc {
   /* Pre-built TLAS over instance world bounds (`Scene::qbvh`, scene/mod.rs:305-317);
    * NULL arrays = build on upload. */
   tpt_qbvh_view tlas;
+  const tpt_material_desc* materials;
+  uint32_t num_materials;
+  /* Pre-built light tree (`Scene::light_tree`); NULL nodes = build on upload
+   * with the binned-SAOH builder (light_tree/builder.rs) over the emissive
+   * triangles, in the order Scene::add_instance registers them. */
+  tpt_light_tree_view light_tree;
 } tpt_scene_desc;
 
 /* Copies the scene into device memory in the B200 layout (128-byte nodes,
@@ -129,6 +174,18 @@ tpt_status tpt_scene_upload(tpt_context* ctx, const tpt_scene_desc* desc, tpt_sc
 tpt_status tpt_scene_release(tpt_scene* scene);
 /* Device bytes held by the scene. */
 tpt_status tpt_scene_device_bytes(const tpt_scene* scene, uint64_t* bytes);
+/* Host copy of the light tree the scene uses (valid while the scene lives);
+ * num_nodes == 0 when the scene has no emitter. */
+tpt_status tpt_scene_light_tree(const tpt_scene* scene, tpt_light_tree_view* view);
+
+/* Host-side light-tree builder without a device (`Scene::build_light_tree`,
+ * scene/mod.rs:300-303 -> light_tree/builder.rs:58-99): binned SAOH over the
+ * scene's emissive triangles.  `desc` needs meshes, instances and materials;
+ * fails with TPT_ERR_INVALID_ARG when nothing emits. */
+typedef struct tpt_light_tree tpt_light_tree;
+tpt_status tpt_light_tree_build(const tpt_scene_desc* desc, tpt_light_tree** out);
+tpt_status tpt_light_tree_view_of(const tpt_light_tree* tree, tpt_light_tree_view* view);
+tpt_status tpt_light_tree_free(tpt_light_tree* tree);
 
 /* ------------------------------------------------------------------------ */
 /* Ray queries (`Scene::closest_hit`, scene/mod.rs:340-395)                   */
@@ -156,6 +213,49 @@ tpt_status tpt_traverse_device(tpt_context* ctx, const tpt_scene* scene, const f
 tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n,
                                      int mode, int32_t* prim, float* t, uint32_t* node_tests,
                                      uint32_t* tri_tests, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Rendering (`IntegratorKind::trace_radiance` per sample, main.rs:99-126 loop) */
+
+typedef enum tpt_integrator {
+  TPT_INTEGRATOR_MIS = 0 /* integrator/mis.rs: BSDF sampling + light-tree NEE, balance heuristic */
+} tpt_integrator;
+
+/* PinholeCamera::new(eye, look_at, up, fov_y, exposure) (scene/camera.rs:21-39). */
+typedef struct tpt_camera_desc {
+  float eye[3];
+  float look_at[3];
+  float up[3];
+  float fov_y; /* radians */
+  float exposure;
+} tpt_camera_desc;
+
+typedef enum tpt_execution {
+  TPT_EXEC_WAVEFRONT = 0, /* stage kernels over compacted ray queues (default) */
+  TPT_EXEC_MEGAKERNEL = 1 /* one thread runs one whole path */
+} tpt_execution;
+
+typedef struct tpt_render_job {
+  const tpt_scene* scene;
+  tpt_camera_desc camera;
+  uint32_t width, height;
+  uint32_t spp;       /* samples per pixel */
+  uint32_t max_depth; /* --depth */
+  uint32_t integrator;
+  uint32_t execution; /* tpt_execution; both give the same image bit for bit */
+} tpt_render_job;
+
+/* Renders each job into out_rgb[j] (host, width*height*3 floats, row-major,
+ * pixel = y*width + x): per pixel the running mean of `spp` samples in sample
+ * order, times exposure — the raw linear buffer main.rs writes before output. */
+tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb);
+/* One job into a device buffer, asynchronous on `stream`. */
+tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream);
+/* The per-sample radiance of paths [first, first+count) in (pixel, sample)
+ * order, path = pixel * spp + sample, into a device buffer of count*3 floats
+ * (parity testing and sample-level consumers). */
+tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first, uint64_t count,
+                                     float* out_samples, void* stream);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,16 @@ def _declare(L):
         "orc_pcg_output": (u32, [u32]),
         "orc_mix_bits": (u64, [u64]),
         "orc_camera_ray": (None, [vp, u32, u32, u32, u32, f32, f32, u32, vp]),
+        "orc_render_scene_create": (vp, [vp]),
+        "orc_render_scene_free": (None, [vp]),
+        "orc_render_scene_set_materials": (None, [vp, vp, vp, vp, vp, u32]),
+        "orc_render_scene_set_light_tree": (None, [vp, vp, u64, u32]),
+        "orc_render_pixels": (None, [vp, vp, u32, u32, u32, u32, u32, u32, vp, i32]),
+        "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u64, u64, vp, i32]),
+        "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
+        "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, vp]),
+        "orc_render_emitted": (None, [vp, i32, i32, vp, vp, i32, i32, vp, vp, vp, f32, i32, vp]),
+        "orc_render_material_pdf": (f32, [vp, i32, i32, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -103,8 +113,11 @@ class BoxQbvh:
         self.h = lib().orc_qbvh_build(_p(self.bounds), self.bounds.shape[0]) if len(self.bounds) else None
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().orc_qbvh_free(self.h)
+        try:
+            if getattr(self, "h", None):
+                lib().orc_qbvh_free(self.h)
+        except Exception:
+            pass
 
     def arrays(self):
         n = lib().orc_qbvh_num_nodes(self.h)
@@ -129,8 +142,11 @@ class Geometry:
         self._tri_counts = []
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().orc_geometry_free(self.h)
+        try:
+            if getattr(self, "h", None):
+                lib().orc_geometry_free(self.h)
+        except Exception:
+            pass
 
     def add_mesh(self, positions, indices, normals=None, uvs=None) -> int:
         pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
@@ -196,3 +212,79 @@ def camera_ray(params, rx, ry, px, py, ux, uy, spp):
     out = np.zeros(20, np.float32)
     lib().orc_camera_ray(_p(p), rx, ry, px, py, C.c_float(ux), C.c_float(uy), spp, _p(out))
     return out
+
+
+class RenderScene:
+    """Oracle render scene: geometry + materials + a flattened light tree.
+
+    scene: dict with meshes, instances, materials (tpt_scenes layout);
+    light_tree: (nodes, root) in the tpt_light_node layout (the tree the
+    library built for the same scene)."""
+
+    def __init__(self, scene: dict, light_tree):
+        g = Geometry()
+        for m in scene["meshes"]:
+            g.add_mesh(m["positions"], m["indices"], m.get("normals"), m.get("uvs"))
+        for inst in scene["instances"]:
+            g.add_instance(inst["mesh"], inst.get("material", 0), inst["local_to_world"], inst["world_to_local"],
+                           inst["normal_to_world"])
+        g.build()
+        self.g = g
+        self.h = lib().orc_render_scene_create(g.h)
+        mats = scene["materials"]
+        kinds = np.array([m["kind"] for m in mats], np.uint32)
+        rho = np.array([np.asarray(m.get("rho", (0, 0, 0)), np.float32) for m in mats], np.float32)
+        col = np.array([np.asarray(m.get("color", (0, 0, 0)), np.float32) for m in mats], np.float32)
+        st = np.array([m.get("strength", 0.0) for m in mats], np.float32)
+        lib().orc_render_scene_set_materials(self.h, _p(kinds), _p(rho), _p(col), _p(st), len(mats))
+        nodes, root = light_tree
+        nodes = np.ascontiguousarray(nodes)
+        lib().orc_render_scene_set_light_tree(self.h, nodes.ctypes.data if len(nodes) else None, len(nodes), int(root))
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().orc_render_scene_free(self.h)
+        except Exception:
+            pass
+
+    @staticmethod
+    def _cam(camera):
+        return np.array([*camera["eye"], *camera["look_at"], *camera["up"], camera["fov_y"],
+                         camera.get("exposure", 1.0)], np.float32)
+
+    def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None):
+        """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3]."""
+        p0, p1 = pixels if pixels is not None else (0, width * height)
+        out = np.empty((p1 - p0, 3), np.float32)
+        cam = self._cam(camera)
+        lib().orc_render_pixels(self.h, _p(cam), width, height, spp, max_depth, p0, p1, _p(out),
+                                nthreads or os.cpu_count() or 1)
+        return out
+
+    def samples(self, camera, width, height, spp, max_depth, first, count, nthreads=None):
+        out = np.empty((count, 3), np.float32)
+        cam = self._cam(camera)
+        lib().orc_render_samples(self.h, _p(cam), width, height, spp, max_depth, first, count, _p(out),
+                                 nthreads or os.cpu_count() or 1)
+        return out
+
+    # -- unit-level queries (reference integrator unit tests) -------------------
+    def direct_light(self, inst, tri, bary, incident, u_tree, us):
+        out = np.zeros(3, np.float32)
+        b = np.asarray(bary, np.float32)
+        d = np.asarray(incident, np.float32)
+        lib().orc_render_direct_light(self.h, inst, tri, _p(b), _p(d), float(u_tree), float(us[0]), float(us[1]),
+                                      _p(out))
+        return out
+
+    def emitted(self, inst, tri, bary, incident, linst, ltri, lbary, lincident, throughput, bsdf_pdf, delta=False):
+        out = np.zeros(3, np.float32)
+        arrs = [np.asarray(a, np.float32) for a in (bary, incident, lbary, lincident, throughput)]
+        lib().orc_render_emitted(self.h, inst, tri, _p(arrs[0]), _p(arrs[1]), linst, ltri, _p(arrs[2]), _p(arrs[3]),
+                                 _p(arrs[4]), float(bsdf_pdf), int(delta), _p(out))
+        return out
+
+    def material_pdf(self, inst, tri, bary, incident, wi):
+        arrs = [np.asarray(a, np.float32) for a in (bary, incident, wi)]
+        return lib().orc_render_material_pdf(self.h, inst, tri, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]))

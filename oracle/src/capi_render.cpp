@@ -1,0 +1,62 @@
+// Oracle C entry points for rendering (test infrastructure only).
+#include <cstring>
+
+#include "render.h"
+
+using namespace orc;
+
+extern "C" {
+
+// Takes ownership of nothing: copies the geometry handle's contents.
+void* orc_render_scene_create(void* geometry) {
+  auto* s = new RenderScene();
+  s->geo = *(Geometry*)geometry;
+  return s;
+}
+void orc_render_scene_free(void* h) { delete (RenderScene*)h; }
+
+// kind, rho[3], color[3], strength per material
+void orc_render_scene_set_materials(void* h, const uint32_t* kinds, const float* rho, const float* color,
+                                    const float* strength, uint32_t n) {
+  auto* s = (RenderScene*)h;
+  s->materials.resize(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    s->materials[i].kind = kinds[i];
+    s->materials[i].rho = Vec3(rho[3 * i], rho[3 * i + 1], rho[3 * i + 2]);
+    s->materials[i].color = Vec3(color[3 * i], color[3 * i + 1], color[3 * i + 2]);
+    s->materials[i].strength = strength[i];
+  }
+}
+
+// Light tree nodes in the 64-byte tpt_light_node layout.
+void orc_render_scene_set_light_tree(void* h, const void* nodes, uint64_t n, uint32_t root) {
+  auto* s = (RenderScene*)h;
+  s->tree.resize(n);
+  if (n) std::memcpy(s->tree.data(), nodes, n * sizeof(LightNode));
+  s->root = root;
+  s->finalize();
+}
+
+static RenderJob make_job(const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth) {
+  RenderJob j;
+  j.cam = Camera::make(Vec3(cam11[0], cam11[1], cam11[2]), Vec3(cam11[3], cam11[4], cam11[5]),
+                       Vec3(cam11[6], cam11[7], cam11[8]), cam11[9], cam11[10]);
+  j.width = w;
+  j.height = hgt;
+  j.spp = spp;
+  j.max_depth = depth;
+  return j;
+}
+
+// cam11: eye(3) look_at(3) up(3) fov_y exposure
+void orc_render_pixels(void* h, const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth,
+                       uint32_t p0, uint32_t p1, float* out, int nthreads) {
+  render_pixels(*(RenderScene*)h, make_job(cam11, w, hgt, spp, depth), p0, p1, out, nthreads);
+}
+
+void orc_render_samples(void* h, const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth,
+                        uint64_t first, uint64_t count, float* out, int nthreads) {
+  render_samples(*(RenderScene*)h, make_job(cam11, w, hgt, spp, depth), first, count, out, nthreads);
+}
+
+}  // extern "C"

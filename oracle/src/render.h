@@ -1,0 +1,87 @@
+// Oracle: per-sample rendering (MIS integrator with SG light-tree NEE) for the
+// NormalizedLambert and Emissive materials.  Restates
+// crates/renderer/src/{integrator/{mod,mis}.rs, light/{mod,area}.rs,
+// light_tree/{traversal,importance,lobe}.rs, math/{sg,mod,orthonormal_basis}.rs,
+// material/{mod,normalized_lambert,emissive}.rs, bsdf/normalized_lambert.rs,
+// scene/{mod,camera}.rs, main.rs:99-126}.
+//
+// The light tree is scene preparation, not the per-sample path: the oracle takes
+// the flattened node array as input (the same one the device uses).
+#pragma once
+#include "camera.h"
+#include "geometry.h"
+#include "sampler.h"
+
+namespace orc {
+
+static constexpr float kPi = 3.14159274101257324f;
+static constexpr float kTau = 6.28318548202514648f;
+
+enum MatKind : uint32_t { kLambert = 0, kEmissive = 1, kOpenPbr = 2 };
+
+struct Material {
+  uint32_t kind = kLambert;
+  Vec3 rho;        // NormalizedLambert
+  Vec3 color;      // Emissive
+  float strength = 0;
+};
+
+// light_tree/mod.rs:65-86 flattened (64 bytes; same layout as the C ABI's tpt_light_node)
+struct LightNode {
+  float flux;
+  float mu[3];
+  float sigma_s2;
+  float nu[3];
+  float lambda;
+  float radius;
+  uint32_t left, right, parent;
+  uint32_t leaf_instance, leaf_triangle;
+  float area;
+};
+static_assert(sizeof(LightNode) == 64, "light node");
+static constexpr uint32_t kNoNode = 0xFFFFFFFFu;
+
+struct Frame {
+  Vec3 t, b, n;
+  static Frame from_normal(Vec3 n);
+  static Frame from_normal_and_tangent(Vec3 n, Vec3 hint);
+  Vec3 to_world(Vec3 d) const { return normalize(d.x * t + d.y * b + d.z * n); }
+  Vec3 to_local(Vec3 w) const { return Vec3(dot(w, t), dot(w, b), dot(w, n)); }
+};
+
+struct Vertex {
+  Vec3 p, ng, ns, wo;
+  Frame frame;
+  int32_t inst, tri;
+};
+
+struct RenderScene {
+  Geometry geo;
+  std::vector<Material> materials;
+  std::vector<LightNode> tree;
+  uint32_t root = kNoNode;
+  // (instance, triangle) -> leaf node, replacing the reference's HashMap
+  std::vector<std::vector<uint32_t>> leaf_of;  // per instance (empty if not emissive)
+  bool has_tree = false;
+  float tree_cat_pmf = 0;
+
+  void finalize();  // derived tables (after materials and tree are set)
+  const Material& mat_of(int inst) const { return materials[geo.instances[inst].material_index]; }
+  void triangle_world(int inst, int tri, Vec3* p) const;
+  Vertex shading_vertex(int inst, int tri, Vec3 bary, Vec3 incident) const;
+};
+
+struct RenderJob {
+  Camera cam;
+  uint32_t width, height, spp, max_depth;
+};
+
+// mis::trace_radiance for one sample
+Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
+
+// main.rs:99-126 for pixels [p0, p1): running mean over spp samples, times exposure.
+void render_pixels(const RenderScene& s, const RenderJob& job, uint32_t p0, uint32_t p1, float* out_rgb, int nthreads);
+// Per-sample radiance of paths [first, first + count), path = pixel * spp + sample.
+void render_samples(const RenderScene& s, const RenderJob& job, uint64_t first, uint64_t count, float* out, int nthreads);
+
+}  // namespace orc

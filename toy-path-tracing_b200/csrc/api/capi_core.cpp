@@ -232,6 +232,8 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
   if (ctx->d_stage) cudaFree(ctx->d_stage);
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
+  if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+  if (ctx->d_wf) cudaFree(ctx->d_wf);
   for (int k = 0; k < 2; ++k) {
     if (ctx->pipe[k]) cudaStreamDestroy(ctx->pipe[k]);
     if (ctx->ev_slot[k]) cudaEventDestroy(ctx->ev_slot[k]);
@@ -444,6 +446,11 @@ tpt_status tpt_scene_upload(tpt_context* ctx, const tpt_scene_desc* desc, tpt_sc
   s->geo.tlas_node_base = tlas_base;
   s->geo.tlas_root_word = tlas_root;
   s->geo.num_instances = desc->num_instances;
+  st = upload_render_data(s, desc);
+  if (st) {
+    tpt_scene_release(s);
+    return st;
+  }
   *out = s;
   return TPT_OK;
 }
@@ -453,6 +460,14 @@ tpt_status tpt_scene_release(tpt_scene* s) {
   if (s->ctx) cudaSetDevice(s->ctx->device);
   for (void* p : s->allocations) cudaFree(p);
   delete s;
+  return TPT_OK;
+}
+
+tpt_status tpt_scene_light_tree(const tpt_scene* s, tpt_light_tree_view* v) {
+  if (!s || !v) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL argument");
+  v->nodes = reinterpret_cast<const tpt_light_node*>(s->light_tree.nodes.data());
+  v->num_nodes = s->light_tree.nodes.size();
+  v->root = s->light_tree.root;
   return TPT_OK;
 }
 

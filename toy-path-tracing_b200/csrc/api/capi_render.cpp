@@ -1,0 +1,243 @@
+// C ABI: rendering (the rayon per-pixel loop of main.rs:99-126 as device launches).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+
+using namespace tpt;
+
+namespace {
+
+uint32_t log2_int(uint32_t v) { return 31u - (uint32_t)__builtin_clz(v); }
+uint32_t round_up_pow2(uint32_t v) { return v <= 1 ? 1u : 1u << (32u - (uint32_t)__builtin_clz(v - 1)); }
+
+struct F3 {
+  float x, y, z;
+};
+F3 sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+F3 cross(F3 a, F3 b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
+F3 normalize(F3 a) {
+  float r = 1.0f / std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+  return {a.x * r, a.y * r, a.z * r};
+}
+
+tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* L) {
+  if (!job || !job->scene) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL job or scene");
+  if (job->width == 0 || job->height == 0 || job->spp == 0)
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "width, height and spp must be positive");
+  if (job->integrator != TPT_INTEGRATOR_MIS) return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown integrator");
+  if (job->execution != TPT_EXEC_WAVEFRONT && job->execution != TPT_EXEC_MEGAKERNEL)
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown execution mode");
+  if (job->scene->render.num_materials == 0)
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "scene has no materials: upload materials to render");
+  if (job->spp > (1u << 24)) return set_error(ctx, TPT_ERR_INVALID_ARG, "spp above 2^24");
+  std::memset(L, 0, sizeof *L);
+  // PinholeCamera::new (scene/camera.rs:22-39)
+  const tpt_camera_desc& c = job->camera;
+  F3 eye{c.eye[0], c.eye[1], c.eye[2]}, at{c.look_at[0], c.look_at[1], c.look_at[2]}, up{c.up[0], c.up[1], c.up[2]};
+  F3 fwd = normalize(sub(at, eye));
+  F3 right = normalize(cross(fwd, up));
+  F3 iup = normalize(cross(right, fwd));
+  const float v[12] = {eye.x, eye.y, eye.z, fwd.x, fwd.y, fwd.z, right.x, right.y, right.z, iup.x, iup.y, iup.z};
+  std::memcpy(L->cam.eye, v, 12);
+  std::memcpy(L->cam.forward, v + 3, 12);
+  std::memcpy(L->cam.right, v + 6, 12);
+  std::memcpy(L->cam.up, v + 9, 12);
+  L->cam.tan_half_fov_y = std::tan(0.5f * c.fov_y);
+  L->cam.exposure = c.exposure;
+  L->width = job->width;
+  L->height = job->height;
+  L->spp = job->spp;
+  L->max_depth = job->max_depth;
+  L->integrator = job->integrator;
+  // IndexSampler::new (sampler/zsobol.rs:213-224)
+  L->log2_spp = log2_int(round_up_pow2(job->spp));
+  const uint32_t res = round_up_pow2(std::max(job->width, job->height));
+  L->n_base4_digits = log2_int(res) + (L->log2_spp + 1) / 2;
+  if (2 * L->n_base4_digits + 2 > 64) return set_error(ctx, TPT_ERR_CAPACITY, "resolution x spp beyond 64-bit Morton index");
+  return TPT_OK;
+}
+
+tpt_status ensure_scratch(tpt_context* ctx, size_t bytes) {
+  if (ctx->d_scratch_bytes >= bytes) return TPT_OK;
+  if (ctx->d_scratch) {
+    cudaDeviceSynchronize();
+    cudaFree(ctx->d_scratch);
+  }
+  ctx->d_scratch = nullptr;
+  ctx->d_scratch_bytes = 0;
+  tpt_status st = cuda_check(ctx, cudaMalloc(&ctx->d_scratch, bytes), "cudaMalloc(render scratch)");
+  if (st) return st;
+  ctx->d_scratch_bytes = bytes;
+  return TPT_OK;
+}
+
+// Carves the wavefront arena for `capacity` path slots.
+tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
+  if (ctx->wf.capacity >= capacity && ctx->d_wf) return TPT_OK;
+  const size_t C = capacity;
+  // float planes: beta 3, L 3, prev 7, q_ray 2*7, h_t 1, h_bary 3, s_ray 7, s_contrib 3, s_t 1
+  // u32 planes: prev_mat, depth, q_slot 2, h_tri, h_inst, s_slot, s_target 2, s_tri, s_inst
+  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1;
+  const size_t bytes = planes * C * 4 + 256;
+  if (ctx->d_wf) {
+    cudaDeviceSynchronize();
+    cudaFree(ctx->d_wf);
+    ctx->d_wf = nullptr;
+    ctx->d_wf_bytes = 0;
+    ctx->wf = WfBuffers{};
+  }
+  tpt_status st = cuda_check(ctx, cudaMalloc(&ctx->d_wf, bytes), "cudaMalloc(wavefront arena)");
+  if (st) return st;
+  ctx->d_wf_bytes = bytes;
+  char* p = (char*)ctx->d_wf;
+  auto take = [&](size_t n_planes) {
+    char* r = p;
+    p += n_planes * C * 4;
+    return r;
+  };
+  WfBuffers& B = ctx->wf;
+  B.capacity = capacity;
+  B.beta = (float*)take(3);
+  B.L = (float*)take(3);
+  B.prev = (float*)take(7);
+  B.prev_mat = (uint32_t*)take(1);
+  B.depth = (uint32_t*)take(1);
+  B.q_slot[0] = (uint32_t*)take(1);
+  B.q_slot[1] = (uint32_t*)take(1);
+  B.q_ray[0] = (float*)take(7);
+  B.q_ray[1] = (float*)take(7);
+  B.h_tri = (int32_t*)take(1);
+  B.h_inst = (int32_t*)take(1);
+  B.h_t = (float*)take(1);
+  B.h_bary = (float*)take(3);
+  B.s_slot = (uint32_t*)take(1);
+  B.s_ray = (float*)take(7);
+  B.s_contrib = (float*)take(3);
+  B.s_target = (uint32_t*)take(2);
+  B.s_tri = (int32_t*)take(1);
+  B.s_inst = (int32_t*)take(1);
+  B.s_t = (float*)take(1);
+  B.counts = (uint32_t*)p;
+  return TPT_OK;
+}
+
+// Paths [first, first + n) through the wavefront stages; radiance per path into samples.
+tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
+                            uint32_t n, float* samples, cudaStream_t s) {
+  tpt_status st = ensure_wavefront(ctx, n);
+  if (st) return st;
+  const WfBuffers& B = ctx->wf;
+  const DevGeometry& geo = job->scene->geo;
+  const DevRenderData& rd = job->scene->render;
+  cudaError_t e = launch_wf_generate(geo, rd, L, B, first, n, s);
+  for (uint32_t b = 0; e == cudaSuccess && b <= L.max_depth; ++b) {
+    const int cur = (int)(b & 1u);
+    e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
+    if (e == cudaSuccess)
+      e = launch_traverse_strided(geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
+                                  B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
+                                  nullptr, nullptr, B.counts + cur);
+    if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, first, cur, s);
+    if (e == cudaSuccess && b < L.max_depth)
+      e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
+                                  nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
+                                  nullptr, B.counts + 2);
+    if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s);
+  }
+  if (e == cudaSuccess) e = launch_wf_finalize(B, n, samples, s);
+  return cuda_check(ctx, e, "wavefront launch");
+}
+
+// Pixels per chunk: the per-sample buffer stays below 1 GiB and a chunk has at
+// most 2^22 paths (the wavefront arena's slot count).
+uint32_t chunk_pixels(const RenderLaunch& L) {
+  const uint64_t per_pixel = 12ull * L.spp;
+  uint64_t n = std::min<uint64_t>((1ull << 30) / per_pixel, std::max<uint64_t>(1, (1ull << 22) / L.spp));
+  const uint64_t total = (uint64_t)L.width * L.height;
+  return (uint32_t)std::max<uint64_t>(1, std::min(n, total));
+}
+
+}  // namespace
+
+extern "C" {
+
+tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  if (!out_rgb) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
+  RenderLaunch L;
+  tpt_status st = make_launch(ctx, job, &L);
+  if (st) return st;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  const uint32_t npix = L.width * L.height;
+  const uint32_t cp = chunk_pixels(L);
+  if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
+  float* samples = (float*)ctx->d_scratch;
+  for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
+    const uint32_t n = std::min(cp, npix - p0);
+    if (job->execution == TPT_EXEC_MEGAKERNEL) {
+      cudaError_t e = launch_render(job->scene->geo, job->scene->render, L, samples, (uint64_t)p0 * L.spp,
+                                    (uint64_t)n * L.spp, ctx->d_err, ctx->num_sms, s);
+      if ((st = cuda_check(ctx, e, "render kernel launch"))) return st;
+    } else {
+      if ((st = render_wavefront(ctx, job, L, (uint64_t)p0 * L.spp, n * L.spp, samples, s))) return st;
+    }
+    cudaError_t e = launch_accumulate(samples, L.spp, p0, n, L.cam.exposure, out_rgb, s);
+    if ((st = cuda_check(ctx, e, "accumulate kernel launch"))) return st;
+  }
+  return TPT_OK;
+}
+
+tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first, uint64_t count,
+                                     float* out_samples, void* stream) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  RenderLaunch L;
+  tpt_status st = make_launch(ctx, job, &L);
+  if (st) return st;
+  const uint64_t total = (uint64_t)L.width * L.height * L.spp;
+  if (first > total || count > total - first) return set_error(ctx, TPT_ERR_INVALID_ARG, "path range out of bounds");
+  if (count && !out_samples) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  if (job->execution == TPT_EXEC_MEGAKERNEL)
+    return cuda_check(ctx,
+                      launch_render(job->scene->geo, job->scene->render, L, out_samples, first, count, ctx->d_err,
+                                    ctx->num_sms, s),
+                      "render kernel launch");
+  const uint64_t step = 1ull << 22;
+  for (uint64_t b = 0; b < count; b += step) {
+    st = render_wavefront(ctx, job, L, first + b, (uint32_t)std::min(step, count - b), out_samples + 3 * b, s);
+    if (st) return st;
+  }
+  return TPT_OK;
+}
+
+tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  if (n_jobs < 0 || (n_jobs && (!jobs || !out_rgb))) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad job list");
+  cudaSetDevice(ctx->device);
+  for (int j = 0; j < n_jobs; ++j) {
+    if (!out_rgb[j]) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output image");
+    RenderLaunch L;
+    tpt_status st = make_launch(ctx, &jobs[j], &L);
+    if (st) return st;
+    const size_t img_bytes = (size_t)L.width * L.height * 12;
+    float* d_img = nullptr;
+    if ((st = cuda_check(ctx, cudaMallocAsync((void**)&d_img, img_bytes, ctx->stream), "cudaMallocAsync(image)")))
+      return st;
+    st = tpt_render_device(ctx, &jobs[j], d_img, nullptr);
+    if (!st)
+      st = cuda_check(ctx, cudaMemcpyAsync(out_rgb[j], d_img, img_bytes, cudaMemcpyDeviceToHost, ctx->stream),
+                      "D2H image");
+    cudaFreeAsync(d_img, ctx->stream);
+    if (!st) st = check_device_errors(ctx, ctx->stream);
+    if (st) return st;
+  }
+  return TPT_OK;
+}
+
+}  // extern "C"

@@ -8,6 +8,8 @@
 
 #include "../../../include/tpt.h"
 #include "../device/dev_types.cuh"
+#include "../device/render_types.h"
+#include "../host/host_scene.h"
 #include "../host/host_types.h"
 
 struct tpt_context {
@@ -26,6 +28,13 @@ struct tpt_context {
   cudaEvent_t ev_start = nullptr;
   unsigned long long* d_counters = nullptr;  // work-distribution counters, one per in-flight launch
   uint32_t counter_next = 0;
+  // device scratch for per-sample radiance of render calls (grown on demand)
+  void* d_scratch = nullptr;
+  size_t d_scratch_bytes = 0;
+  // wavefront arena (grown on demand) and its layout
+  void* d_wf = nullptr;
+  size_t d_wf_bytes = 0;
+  tpt::WfBuffers wf{};
 };
 
 struct tpt_qbvh {
@@ -40,6 +49,8 @@ struct tpt_scene {
   uint32_t num_meshes = 0;
   uint32_t num_instances = 0;
   std::vector<uint32_t> mesh_tri_counts;
+  tpt::DevRenderData render{};          // shading data for the render kernels
+  tpt::LightTreeHost light_tree;        // host copy of the light tree
 };
 
 namespace tpt {
@@ -57,9 +68,28 @@ tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream);
 cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t stream,
-                                    uint32_t* node_tests, uint32_t* tri_tests);
+                                    uint32_t* node_tests, uint32_t* tri_tests, const uint32_t* n_dev = nullptr);
 
 // A work counter slot for the next launch (ring of kCounterSlots per context).
 unsigned long long* next_counter(tpt_context* ctx);
+
+// render_kernels.cu
+cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P, float* samples,
+                          uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t stream);
+cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first_pixel, uint32_t n_pixels,
+                              float exposure, float* image, cudaStream_t stream);
+
+// wavefront_kernels.cu
+cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
+                               const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s);
+cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
+                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s);
+cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s);
+cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
+
+// scene_render_upload.cpp: materials, shading arrays, light tree, emitter map.
+tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc);
+// Device allocation owned by the scene.
+tpt_status scene_alloc(tpt_scene* s, size_t bytes, void** out);
 
 }  // namespace tpt

@@ -1,0 +1,233 @@
+// Scene upload, render half: vertex attributes, materials, per-instance
+// shading records, the SG light tree and the emitter-triangle -> leaf map that
+// replaces the reference's HashMap / linear searches (light_tree/mod.rs:101-108,
+// scene/mod.rs:583-594).
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+
+namespace tpt {
+
+tpt_status scene_alloc(tpt_scene* s, size_t bytes, void** out) {
+  bytes = std::max<size_t>(bytes, 128);
+  void* p = nullptr;
+  tpt_status st = cuda_check(s->ctx, cudaMalloc(&p, bytes), "cudaMalloc(scene)");
+  if (st) return st;
+  s->allocations.push_back(p);
+  s->device_bytes += bytes;
+  *out = p;
+  return TPT_OK;
+}
+
+namespace {
+template <class T>
+tpt_status put(tpt_scene* s, const std::vector<T>& v, const T** dst) {
+  void* p = nullptr;
+  tpt_status st = scene_alloc(s, v.size() * sizeof(T), &p);
+  if (st) return st;
+  if (!v.empty()) {
+    st = cuda_check(s->ctx, cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy(scene)");
+    if (st) return st;
+  }
+  *dst = (const T*)p;
+  return TPT_OK;
+}
+}  // namespace
+
+tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
+  tpt_context* ctx = s->ctx;
+  // materials
+  std::vector<HostMaterial> hmats(desc->num_materials);
+  std::vector<DevMaterialRec> dmats(desc->num_materials);
+  if (desc->num_materials && !desc->materials) return set_error(ctx, TPT_ERR_INVALID_ARG, "materials is NULL");
+  for (uint32_t i = 0; i < desc->num_materials; ++i) {
+    const tpt_material_desc& m = desc->materials[i];
+    if (m.kind != TPT_MATERIAL_NORMALIZED_LAMBERT && m.kind != TPT_MATERIAL_EMISSIVE)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": unsupported kind");
+    HostMaterial h{};
+    h.kind = m.kind;
+    std::memcpy(h.rho, m.rho, 12);
+    std::memcpy(h.color, m.color, 12);
+    h.strength = m.strength;
+    hmats[i] = h;
+    DevMaterialRec d{};
+    d.kind = m.kind;
+    std::memcpy(d.rho, m.rho, 12);
+    std::memcpy(d.color, m.color, 12);
+    d.strength = m.strength;
+    dmats[i] = d;
+  }
+  for (uint32_t i = 0; i < desc->num_instances; ++i)
+    if (desc->instances[i].material_index >= desc->num_materials && desc->num_materials)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "instance " + std::to_string(i) + ": material index out of range");
+
+  // vertex attributes, concatenated per mesh
+  std::vector<float> pos, nrm, uv;
+  std::vector<uint32_t> idx;
+  std::vector<DevMeshInfo> minfo(desc->num_meshes);
+  std::vector<HostMesh> hmesh(desc->num_meshes);
+  for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+    const tpt_mesh_desc& md = desc->meshes[m];
+    DevMeshInfo mi{};
+    mi.vtx_base = (uint32_t)(pos.size() / 3);
+    mi.idx_base = (uint32_t)idx.size();
+    mi.num_tris = (uint32_t)(md.num_indices / 3);
+    mi.flags = (md.normals ? 1u : 0u) | (md.uvs ? 2u : 0u);
+    pos.insert(pos.end(), md.positions, md.positions + 3 * md.num_vertices);
+    if (md.normals) nrm.resize(pos.size(), 0.0f), std::memcpy(&nrm[3 * mi.vtx_base], md.normals, 12 * md.num_vertices);
+    else nrm.resize(pos.size(), 0.0f);
+    uv.resize(2 * (pos.size() / 3), 0.0f);
+    if (md.uvs) std::memcpy(&uv[2 * mi.vtx_base], md.uvs, 8 * md.num_vertices);
+    idx.insert(idx.end(), md.indices, md.indices + md.num_indices);
+    minfo[m] = mi;
+    hmesh[m] = HostMesh{md.positions, md.normals, md.uvs, md.indices, (uint32_t)md.num_vertices, mi.num_tris};
+  }
+
+  // light tree: the caller's, or built here (builder.rs)
+  std::vector<HostInstance> hinst(desc->num_instances);
+  for (uint32_t i = 0; i < desc->num_instances; ++i) {
+    const tpt_instance_desc& id = desc->instances[i];
+    hinst[i] = HostInstance{id.mesh_index, id.material_index, id.local_to_world, id.world_to_local, id.normal_to_world};
+  }
+  if (desc->light_tree.nodes) {
+    s->light_tree.nodes.resize(desc->light_tree.num_nodes);
+    std::memcpy(s->light_tree.nodes.data(), desc->light_tree.nodes, desc->light_tree.num_nodes * 64);
+    s->light_tree.root = desc->light_tree.root;
+    const uint64_t nn = desc->light_tree.num_nodes;
+    if (nn && s->light_tree.root >= nn) return set_error(ctx, TPT_ERR_INVALID_ARG, "light tree root out of range");
+    for (uint64_t i = 0; i < nn; ++i) {
+      const LightNodeHost& n = s->light_tree.nodes[i];
+      const bool leaf = n.leaf_instance != kInvalidNode;
+      if (leaf) {
+        if (n.leaf_instance >= desc->num_instances ||
+            n.leaf_triangle >= minfo[desc->instances[n.leaf_instance].mesh_index].num_tris)
+          return set_error(ctx, TPT_ERR_INVALID_ARG, "light tree leaf names an unknown triangle");
+      } else if (n.left >= nn || n.right >= nn) {
+        return set_error(ctx, TPT_ERR_INVALID_ARG, "light tree child index out of range");
+      }
+      if (n.parent != kInvalidNode && n.parent >= nn) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad light tree parent");
+    }
+  } else if (desc->num_materials) {
+    HostSceneView view{hmesh.data(), desc->num_meshes, hinst.data(), desc->num_instances, hmats.data(),
+                       desc->num_materials};
+    build_light_tree_host(view, &s->light_tree);
+  }
+
+  // emitter map: per emissive instance, one slot per triangle
+  std::vector<DevShadeInstance> sinst(desc->num_instances);
+  uint32_t map_size = 0;
+  for (uint32_t i = 0; i < desc->num_instances; ++i) {
+    const tpt_instance_desc& id = desc->instances[i];
+    DevShadeInstance d{};
+    const float* w = id.local_to_world;
+    const float cols[12] = {w[0], w[1], w[2], w[4], w[5], w[6], w[8], w[9], w[10], w[12], w[13], w[14]};
+    std::memcpy(d.l2w, cols, sizeof cols);
+    std::memcpy(d.n2w, id.normal_to_world, 36);
+    d.mesh = id.mesh_index;
+    d.material = id.material_index;
+    d.leaf_base = kInvalidNode;
+    if (desc->num_materials && hmats[id.material_index].may_emit()) {
+      d.leaf_base = map_size;
+      map_size += minfo[id.mesh_index].num_tris;
+    }
+    sinst[i] = d;
+  }
+  std::vector<uint32_t> emap(map_size, kInvalidNode);
+  for (uint32_t k = 0; k < s->light_tree.nodes.size(); ++k) {
+    const LightNodeHost& n = s->light_tree.nodes[k];
+    if (n.leaf_instance == kInvalidNode) continue;
+    const uint32_t base = sinst[n.leaf_instance].leaf_base;
+    if (base != kInvalidNode) emap[base + n.leaf_triangle] = k;
+  }
+  std::vector<DevLightNodeRec> lnodes(s->light_tree.nodes.size());
+  if (!lnodes.empty()) std::memcpy(lnodes.data(), s->light_tree.nodes.data(), lnodes.size() * 64);
+
+  DevRenderData& R = s->render;
+  tpt_status st = TPT_OK;
+  if (!st) st = put(s, sinst, &R.inst);
+  if (!st) st = put(s, minfo, &R.meshes);
+  if (!st) st = put(s, pos, &R.pos);
+  if (!st) st = put(s, nrm, &R.nrm);
+  if (!st) st = put(s, uv, &R.uv);
+  if (!st) st = put(s, idx, &R.idx);
+  if (!st) st = put(s, dmats, &R.mats);
+  if (!st) st = put(s, lnodes, &R.ltree);
+  if (!st) st = put(s, emap, &R.emitter_leaf);
+  if (st) return st;
+  R.ltree_root = s->light_tree.root;
+  R.num_materials = desc->num_materials;
+  // LightSampler::build_from_scene (light/mod.rs:134-188) with only the Tree category
+  const float tree_w = lnodes.empty() ? 0.0f : std::fmax(lnodes[R.ltree_root].flux, 0.0f);
+  R.has_tree = tree_w > 0.0f ? 1u : 0u;
+  const float total = 0.0f + tree_w;
+  R.tree_cat_pmf = R.has_tree ? tree_w / total : 0.0f;
+  return TPT_OK;
+}
+
+}  // namespace tpt
+
+struct tpt_light_tree {
+  tpt::LightTreeHost t;
+};
+
+extern "C" {
+
+tpt_status tpt_light_tree_build(const tpt_scene_desc* desc, tpt_light_tree** out) {
+  using namespace tpt;
+  if (!desc || !out) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  if ((desc->num_meshes && !desc->meshes) || (desc->num_instances && !desc->instances) ||
+      (desc->num_materials && !desc->materials))
+    return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL array in scene description");
+  std::vector<HostMaterial> hm(desc->num_materials);
+  for (uint32_t i = 0; i < desc->num_materials; ++i) {
+    const tpt_material_desc& m = desc->materials[i];
+    hm[i] = HostMaterial{};
+    hm[i].kind = m.kind;
+    std::memcpy(hm[i].rho, m.rho, 12);
+    std::memcpy(hm[i].color, m.color, 12);
+    hm[i].strength = m.strength;
+  }
+  std::vector<HostMesh> meshes(desc->num_meshes);
+  for (uint32_t i = 0; i < desc->num_meshes; ++i) {
+    const tpt_mesh_desc& md = desc->meshes[i];
+    if (!md.positions || !md.indices || md.num_indices % 3)
+      return set_error(nullptr, TPT_ERR_INVALID_ARG, "bad mesh " + std::to_string(i));
+    for (uint64_t k = 0; k < md.num_indices; ++k)
+      if (md.indices[k] >= md.num_vertices) return set_error(nullptr, TPT_ERR_INVALID_ARG, "index out of range");
+    meshes[i] = HostMesh{md.positions, md.normals, md.uvs, md.indices, (uint32_t)md.num_vertices,
+                         (uint32_t)(md.num_indices / 3)};
+  }
+  std::vector<HostInstance> inst(desc->num_instances);
+  for (uint32_t i = 0; i < desc->num_instances; ++i) {
+    const tpt_instance_desc& id = desc->instances[i];
+    if (id.mesh_index >= desc->num_meshes || id.material_index >= desc->num_materials)
+      return set_error(nullptr, TPT_ERR_INVALID_ARG, "instance " + std::to_string(i) + " references out of range");
+    inst[i] = HostInstance{id.mesh_index, id.material_index, id.local_to_world, id.world_to_local, id.normal_to_world};
+  }
+  auto* t = new tpt_light_tree();
+  HostSceneView v{meshes.data(), desc->num_meshes, inst.data(), desc->num_instances, hm.data(), desc->num_materials};
+  if (!build_light_tree_host(v, &t->t)) {
+    delete t;
+    return set_error(nullptr, TPT_ERR_INVALID_ARG, "no emissive triangle: build_light_tree returns None");
+  }
+  *out = t;
+  return TPT_OK;
+}
+
+tpt_status tpt_light_tree_view_of(const tpt_light_tree* tree, tpt_light_tree_view* view) {
+  if (!tree || !view) return tpt::set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL argument");
+  view->nodes = reinterpret_cast<const tpt_light_node*>(tree->t.nodes.data());
+  view->num_nodes = tree->t.nodes.size();
+  view->root = tree->t.root;
+  return TPT_OK;
+}
+
+tpt_status tpt_light_tree_free(tpt_light_tree* tree) {
+  delete tree;
+  return TPT_OK;
+}
+
+}  // extern "C"

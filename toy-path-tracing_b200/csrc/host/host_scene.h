@@ -1,0 +1,88 @@
+// Host-side scene description shared by the uploader and the light-tree builder.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+namespace tpt {
+
+constexpr uint32_t kInvalidNode = 0xFFFFFFFFu;
+
+enum MaterialKind : uint32_t {
+  kMatLambert = 0,   // NormalizedLambertMaterial (material/normalized_lambert.rs)
+  kMatEmissive = 1,  // EmissiveMaterial (material/emissive.rs)
+  kMatOpenPbr = 2,   // OpenPbrMaterial (material/open_pbr.rs)
+};
+
+struct HostMaterial {
+  uint32_t kind;
+  float rho[3];       // Lambert
+  float color[3];     // Emissive colour
+  float strength;     // Emissive strength
+  bool may_emit() const { return kind == kMatEmissive; }
+  // EmissiveMaterial::max_emission (emissive.rs:87-94): max channel of colour * strength, >= 0
+  float max_emission() const {
+    if (kind != kMatEmissive) return 0.0f;
+    float a = color[0] * strength, b = color[1] * strength, c = color[2] * strength;
+    float m = std::fmax(a, std::fmax(b, c));
+    return std::fmax(m, 0.0f);
+  }
+};
+
+struct HostMesh {
+  const float* positions;
+  const float* normals;  // may be null
+  const float* uvs;      // may be null
+  const uint32_t* indices;
+  uint32_t num_vertices;
+  uint32_t num_triangles;
+};
+
+struct HostInstance {
+  uint32_t mesh, material;
+  const float* local_to_world;  // 16, column-major
+  const float* world_to_local;
+  const float* normal_to_world;  // 9, column-major
+};
+
+struct HostSceneView {
+  const HostMesh* meshes;
+  uint32_t num_meshes;
+  const HostInstance* instances;
+  uint32_t num_instances;
+  const HostMaterial* materials;
+  uint32_t num_materials;
+};
+
+// Same bytes as `tpt_light_node` in include/tpt.h (64 bytes).
+struct LightNodeHost {
+  float flux;
+  float mu[3];
+  float sigma_s2;
+  float nu[3];
+  float lambda;
+  float radius;
+  uint32_t left, right, parent;
+  uint32_t leaf_instance, leaf_triangle;  // kInvalidNode for interior nodes
+  float area;                             // emitter triangle area (leaves)
+};
+static_assert(sizeof(LightNodeHost) == 64, "light node layout");
+
+struct LightTreeHost {
+  std::vector<LightNodeHost> nodes;
+  uint32_t root = kInvalidNode;
+};
+
+// glam Mat4::transform_point3 (column-major m[16]) of p[3] into out[3].
+inline void transform_point_glam(const float* m, const float* p, float* out) {
+  float r[3];
+  for (int i = 0; i < 3; ++i) r[i] = m[0 + i] * p[0];
+  for (int i = 0; i < 3; ++i) r[i] = m[4 + i] * p[1] + r[i];
+  for (int i = 0; i < 3; ++i) r[i] = m[8 + i] * p[2] + r[i];
+  for (int i = 0; i < 3; ++i) r[i] = m[12 + i] + r[i];
+  out[0] = r[0]; out[1] = r[1]; out[2] = r[2];
+}
+
+bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out);
+
+}  // namespace tpt

@@ -28,7 +28,8 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
     traverse_kernel(DevGeometry geo, const float* __restrict__ rays, uint64_t rs, uint64_t n, uint64_t bs,
                     int32_t* __restrict__ prim, float* __restrict__ tout, int32_t* __restrict__ inst,
                     float* __restrict__ bary, uint32_t* __restrict__ node_tests, uint32_t* __restrict__ tri_tests,
-                    unsigned long long* __restrict__ counter, uint32_t* err) {
+                    unsigned long long* __restrict__ counter, const uint32_t* __restrict__ n_dev, uint32_t* err) {
+  if (n_dev) n = *n_dev;  // queue length produced on the device (wavefront stages)
   __shared__ uint32_t stack_sh[kShStack * kBlock];
   SplitStack<kShStack> st;
   st.sh = stack_sh + threadIdx.x;
@@ -113,7 +114,8 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
 template <int MODE, bool STATS, bool BARY>
 static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, uint64_t bs,
                             int32_t* prim, float* t, int32_t* inst, float* bary, uint32_t* nt, uint32_t* tt,
-                            unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s) {
+                            unsigned long long* counter, const uint32_t* n_dev, uint32_t* err, int num_sms,
+                            cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   static int blocks_per_sm = 0;
   if (blocks_per_sm == 0) {
@@ -122,22 +124,23 @@ static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t 
     if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 4;
   }
   uint64_t blocks = (uint64_t)num_sms * blocks_per_sm;
-  const uint64_t need = (n + kBlock - 1) / kBlock;
+  const uint64_t need = (n + kBlock - 1) / kBlock;  // n is an upper bound when n_dev is given
   if (blocks > need) blocks = need;
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   traverse_kernel<MODE, STATS, BARY>
-      <<<(unsigned)blocks, kBlock, 0, s>>>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, err);
+      <<<(unsigned)blocks, kBlock, 0, s>>>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
-                                    uint32_t* nt, uint32_t* tt) {
+                                    uint32_t* nt, uint32_t* tt, const uint32_t* n_dev) {
   const bool stats = nt != nullptr;
   const bool b = bary != nullptr;
-#define TPT_L(M, S, B) launch_t<M, S, B>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, err, num_sms, s)
+#define TPT_L(M, S, B) \
+  launch_t<M, S, B>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, num_sms, s)
   if (mode == 0) {
     if (stats) return TPT_L(0, true, false);
     if (b) return TPT_L(0, false, true);

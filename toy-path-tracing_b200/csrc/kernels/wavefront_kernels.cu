@@ -1,0 +1,243 @@
+// Wavefront path tracing: the MIS integrator of integrator/mis.rs split into
+// stage kernels over compacted queues of path slots,
+//
+//   generate -> [ traverse(closest) -> shade -> traverse(shadow) -> resolve ]
+//               x (max_depth + 1) -> finalize -> accumulate
+//
+// Traversal runs in the persistent-warp kernel of traverse_kernels.cu; shade
+// handles one path vertex (emission with MIS against the previous vertex, NEE
+// preparation, BSDF sampling, Russian roulette) and appends the next ray and
+// the shadow ray with warp-aggregated atomics; resolve adds the NEE
+// contribution of visible shadow rays.  Each path's radiance is updated in the
+// reference's order (emission of vertex d, then NEE of vertex d, then emission
+// of vertex d + 1), so the result equals the megakernel's bit for bit.
+// Stage launch shapes do not depend on queue lengths (those live on the
+// device), so one bounce is a fixed launch sequence that a CUDA graph replays.
+#include "../api/internal.h"
+#include "../device/render.cuh"
+
+namespace tpt {
+
+constexpr int kWfBlock = 256;
+
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+  const unsigned act = __activemask();
+  const unsigned m = __ballot_sync(act, pred);
+  const unsigned lane = threadIdx.x & 31u;
+  const int leader = __ffs(act) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader && m) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(act, base, leader);
+  return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunch P, WfBuffers B,
+                                                        uint64_t first_path, uint32_t n_paths) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    B.counts[0] = n_paths;
+    B.counts[1] = 0;
+    B.counts[2] = 0;
+  }
+  if (i >= n_paths) return;
+  const uint32_t C = B.capacity;
+  const uint64_t path = first_path + i;
+  const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
+  const uint32_t px = pixel % P.width, py = pixel / P.width;
+  PathSamplerDev ps;
+  ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+  float c0, c1;
+  ps.sample_2d(kDimCamera, c0, c1);
+  const float fx = ((float)px + 0.5f) + 0.5f * tent(c0);
+  const float fy = ((float)py + 0.5f) + 0.5f * tent(c1);
+  const V3 d = camera_dir(P.cam, P.width, P.height, fx, fy);
+  float* q = B.q_ray[0];
+  q[i] = P.cam.eye[0];
+  q[C + i] = P.cam.eye[1];
+  q[2 * C + i] = P.cam.eye[2];
+  q[3 * C + i] = d.x;
+  q[4 * C + i] = d.y;
+  q[5 * C + i] = d.z;
+  q[6 * C + i] = __int_as_float(0x7f800000);
+  B.q_slot[0][i] = i;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    B.beta[k * C + i] = 1.0f;
+    B.L[k * C + i] = 0.0f;
+  }
+  B.depth[i] = 0;
+}
+
+// One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
+__global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P, WfBuffers B, uint64_t first_path,
+                                                     int cur) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= B.counts[cur]) return;
+  const uint32_t C = B.capacity;
+  const uint32_t slot = B.q_slot[cur][j];
+  const uint32_t d = B.depth[slot];
+  bool push_next = false, push_shadow = false;
+  V3 next_o, next_d;
+  DirectPrep dp;
+  V3 beta = V3{B.beta[slot], B.beta[C + slot], B.beta[2 * C + slot]};
+  V3 L = V3{B.L[slot], B.L[C + slot], B.L[2 * C + slot]};
+  const int32_t tri = B.h_tri[j];
+  if (tri >= 0) {
+    TraceResult h;
+    h.tri = tri;
+    h.inst = B.h_inst[j];
+    h.b0 = B.h_bary[j];
+    h.b1 = B.h_bary[C + j];
+    h.b2 = B.h_bary[2 * C + j];
+    const float* qr = B.q_ray[cur];
+    const V3 rd = V3{qr[3 * C + j], qr[4 * C + j], qr[5 * C + j]};
+    const Vertex v = shade_hit<int>(S, h, rd);
+    const uint32_t mi = __ldg(&S.d.inst[v.inst].material);
+    const DevMaterialRec m = S.d.mats[mi];
+    // emission of this vertex (mis.rs:45-47 for the camera vertex, 101-117 after a bounce)
+    if (m.kind == kDevEmissive) {
+      const V3 le = emissive_le(m);
+      if (d == 0) {
+        L = L + le;
+      } else {
+        const uint32_t pm = B.prev_mat[slot];
+        if (pm >> 31) {
+          L = L + beta * le;
+        } else {
+          Vertex pv;
+          pv.p = V3{B.prev[slot], B.prev[C + slot], B.prev[2 * C + slot]};
+          pv.ns = V3{B.prev[3 * C + slot], B.prev[4 * C + slot], B.prev[5 * C + slot]};
+          const float lp = light_pdf_for_hit(S, S.d.mats[pm & 0x7FFFFFFFu], pv, v);
+          L = L + beta * le * balance_heuristic(B.prev[6 * C + slot], lp);
+        }
+      }
+    }
+    if (d < P.max_depth && m.kind != kDevEmissive) {
+      const uint64_t path = first_path + slot;
+      const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
+      PathSamplerDev ps;
+      ps.init(pixel % P.width, pixel / P.width, sample, P.log2_spp, P.n_base4_digits);
+      float us0, us1;
+      ps.sample_2d(vertex_dim(d, kOffSurface), us0, us1);
+      const float u_tree = ps.sample_1d(vertex_dim(d, kOffTree));
+      if (prepare_direct(S, m, v, u_tree, us0, us1, dp)) {
+        dp.contrib = beta * dp.contrib;
+        push_shadow = true;
+      }
+      float ud0, ud1;
+      ps.sample_2d(vertex_dim(d, kOffDir), ud0, ud1);
+      BsdfSampleOut s;
+      if (lambert_sample(m, v, ud0, ud1, s)) {
+        beta = beta * s.weight;
+        bool alive = true;
+        if (d + 1 >= 4) {
+          const float q = clampf(max_element(beta), 0.05f, 1.0f);
+          if (ps.sample_1d(vertex_dim(d, kOffRr)) > q) alive = false;
+          else beta = beta / q;
+        }
+        if (alive) {
+          push_next = true;
+          next_o = offset_origin(v.p, v.ng, s.wi);
+          next_d = s.wi;
+          B.prev[slot] = v.p.x;
+          B.prev[C + slot] = v.p.y;
+          B.prev[2 * C + slot] = v.p.z;
+          B.prev[3 * C + slot] = v.ns.x;
+          B.prev[4 * C + slot] = v.ns.y;
+          B.prev[5 * C + slot] = v.ns.z;
+          B.prev[6 * C + slot] = s.pdf;
+          B.prev_mat[slot] = mi | (s.delta ? 0x80000000u : 0u);
+          B.depth[slot] = d + 1;
+        }
+      }
+    }
+  }
+  B.L[slot] = L.x;
+  B.L[C + slot] = L.y;
+  B.L[2 * C + slot] = L.z;
+  B.beta[slot] = beta.x;
+  B.beta[C + slot] = beta.y;
+  B.beta[2 * C + slot] = beta.z;
+  const int nxt = cur ^ 1;
+  const uint32_t qn = warp_append(&B.counts[nxt], push_next);
+  const uint32_t qs = warp_append(&B.counts[2], push_shadow);
+  if (push_next) {
+    float* q = B.q_ray[nxt];
+    q[qn] = next_o.x;
+    q[C + qn] = next_o.y;
+    q[2 * C + qn] = next_o.z;
+    q[3 * C + qn] = next_d.x;
+    q[4 * C + qn] = next_d.y;
+    q[5 * C + qn] = next_d.z;
+    q[6 * C + qn] = __int_as_float(0x7f800000);
+    B.q_slot[nxt][qn] = slot;
+  }
+  if (push_shadow) {
+    float* q = B.s_ray;
+    q[qs] = dp.so.x;
+    q[C + qs] = dp.so.y;
+    q[2 * C + qs] = dp.so.z;
+    q[3 * C + qs] = dp.wi.x;
+    q[4 * C + qs] = dp.wi.y;
+    q[5 * C + qs] = dp.wi.z;
+    q[6 * C + qs] = __int_as_float(0x7f800000);
+    B.s_slot[qs] = slot;
+    B.s_target[qs] = dp.inst;
+    B.s_target[C + qs] = dp.tri;
+    B.s_contrib[qs] = dp.contrib.x;
+    B.s_contrib[C + qs] = dp.contrib.y;
+    B.s_contrib[2 * C + qs] = dp.contrib.z;
+  }
+}
+
+// unoccluded_ray (integrator/mod.rs:239-265): visible when nothing is hit or the
+// first hit is the sampled emitter triangle.
+__global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= B.counts[2]) return;
+  const uint32_t C = B.capacity;
+  const int32_t tri = B.s_tri[j];
+  const bool visible = tri < 0 || ((uint32_t)B.s_inst[j] == B.s_target[j] && (uint32_t)tri == B.s_target[C + j]);
+  if (!visible) return;
+  const uint32_t slot = B.s_slot[j];
+  B.L[slot] = B.L[slot] + B.s_contrib[j];
+  B.L[C + slot] = B.L[C + slot] + B.s_contrib[C + j];
+  B.L[2 * C + slot] = B.L[2 * C + slot] + B.s_contrib[2 * C + j];
+}
+
+__global__ void __launch_bounds__(kWfBlock) wf_finalize(WfBuffers B, uint32_t n_paths, float* samples) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_paths) return;
+  const uint32_t C = B.capacity;
+  samples[3 * (uint64_t)i] = B.L[i];
+  samples[3 * (uint64_t)i + 1] = B.L[C + i];
+  samples[3 * (uint64_t)i + 2] = B.L[2 * C + i];
+}
+
+static inline unsigned grid_for(uint32_t n) { return (n + kWfBlock - 1) / kWfBlock; }
+
+cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
+                               const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s) {
+  DevRender S{geo, rd};
+  wf_generate<<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
+                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s) {
+  DevRender S{geo, rd};
+  wf_shade<<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s) {
+  wf_resolve<<<grid_for(B.capacity), kWfBlock, 0, s>>>(B);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s) {
+  wf_finalize<<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(B, n_paths, samples);
+  return cudaGetLastError();
+}
+
+}  // namespace tpt

@@ -73,6 +73,28 @@ class InstanceDesc(C.Structure):
     ]
 
 
+class MaterialDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("rho", C.c_float * 3),
+        ("color", C.c_float * 3),
+        ("strength", C.c_float),
+        ("openpbr", C.c_void_p),
+    ]
+
+
+LIGHT_NODE_DTYPE = np.dtype(
+    [("flux", "<f4"), ("mu", "<f4", (3,)), ("sigma_s2", "<f4"), ("nu", "<f4", (3,)), ("lambda", "<f4"),
+     ("radius", "<f4"), ("left", "<u4"), ("right", "<u4"), ("parent", "<u4"), ("leaf_instance", "<u4"),
+     ("leaf_triangle", "<u4"), ("area", "<f4")]
+)
+assert LIGHT_NODE_DTYPE.itemsize == 64
+
+
+class LightTreeView(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("num_nodes", C.c_uint64), ("root", C.c_uint32)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("meshes", C.POINTER(MeshDesc)),
@@ -80,7 +102,26 @@ class SceneDesc(C.Structure):
         ("instances", C.POINTER(InstanceDesc)),
         ("num_instances", C.c_uint32),
         ("tlas", QbvhView),
+        ("materials", C.POINTER(MaterialDesc)),
+        ("num_materials", C.c_uint32),
+        ("light_tree", LightTreeView),
     ]
+
+
+class CameraDesc(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3), ("fov_y", C.c_float),
+                ("exposure", C.c_float)]
+
+
+class RenderJob(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", CameraDesc), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("spp", C.c_uint32), ("max_depth", C.c_uint32), ("integrator", C.c_uint32),
+                ("execution", C.c_uint32)]
+
+
+INTEGRATOR_MIS = 0
+EXEC_WAVEFRONT = 0
+EXEC_MEGAKERNEL = 1
 
 
 def lib():
@@ -111,6 +152,13 @@ EXPORTED_SYMBOLS = [
     "tpt_traverse",
     "tpt_traverse_device",
     "tpt_traverse_stats_device",
+    "tpt_scene_light_tree",
+    "tpt_render",
+    "tpt_render_device",
+    "tpt_render_samples_device",
+    "tpt_light_tree_build",
+    "tpt_light_tree_view_of",
+    "tpt_light_tree_free",
 ]
 
 
@@ -130,6 +178,13 @@ def _declare(L):
         "tpt_traverse": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp]),
         "tpt_traverse_device": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp, vp]),
         "tpt_traverse_stats_device": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp, vp]),
+        "tpt_scene_light_tree": (i32, [vp, C.POINTER(LightTreeView)]),
+        "tpt_render": (i32, [vp, C.POINTER(RenderJob), i32, C.POINTER(C.c_void_p)]),
+        "tpt_render_device": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
+        "tpt_render_samples_device": (i32, [vp, C.POINTER(RenderJob), u64, u64, vp, vp]),
+        "tpt_light_tree_build": (i32, [C.POINTER(SceneDesc), C.POINTER(vp)]),
+        "tpt_light_tree_view_of": (i32, [vp, C.POINTER(LightTreeView)]),
+        "tpt_light_tree_free": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -170,7 +225,10 @@ class Context:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
 
 
 def build_qbvh(bounds: np.ndarray, threads: int = 0):
@@ -200,6 +258,72 @@ def _view(q):
     )
 
 
+def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None):
+    """Build a `tpt_scene_desc` (and the list of arrays it points into)."""
+    keep = []
+    md = (MeshDesc * max(1, len(meshes)))()
+    for i, m in enumerate(meshes):
+        pos = np.ascontiguousarray(m["positions"], np.float32)
+        idx = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1)
+        nrm = m.get("normals")
+        uv = m.get("uvs")
+        nrm = None if nrm is None else np.ascontiguousarray(nrm, np.float32)
+        uv = None if uv is None else np.ascontiguousarray(uv, np.float32)
+        keep += [pos, idx, nrm, uv]
+        q = m.get("qbvh")
+        if q is not None:
+            q = (np.ascontiguousarray(q[0]), np.ascontiguousarray(q[1], np.uint32))
+            keep += list(q)
+        md[i] = MeshDesc(
+            pos.ctypes.data, None if nrm is None else nrm.ctypes.data, None if uv is None else uv.ctypes.data,
+            pos.shape[0], idx.ctypes.data, idx.size, _view(q)
+        )
+    idesc = (InstanceDesc * max(1, len(instances)))()
+    for i, inst in enumerate(instances):
+        d = InstanceDesc()
+        d.mesh_index = inst["mesh"]
+        d.material_index = inst.get("material", 0)
+        d.local_to_world[:] = np.asarray(inst["local_to_world"], np.float32).reshape(16).tolist()
+        d.world_to_local[:] = np.asarray(inst["world_to_local"], np.float32).reshape(16).tolist()
+        d.normal_to_world[:] = np.asarray(inst["normal_to_world"], np.float32).reshape(9).tolist()
+        idesc[i] = d
+    if tlas is not None:
+        tlas = (np.ascontiguousarray(tlas[0]), np.ascontiguousarray(tlas[1], np.uint32))
+        keep += list(tlas)
+    materials = materials or []
+    mdesc = (MaterialDesc * max(1, len(materials)))()
+    for i, m in enumerate(materials):
+        d = MaterialDesc()
+        d.kind = m["kind"]
+        d.rho[:] = list(np.asarray(m.get("rho", (0, 0, 0)), np.float32))
+        d.color[:] = list(np.asarray(m.get("color", (0, 0, 0)), np.float32))
+        d.strength = float(np.float32(m.get("strength", 0.0)))
+        mdesc[i] = d
+    ltv = LightTreeView(None, 0, 0)
+    if light_tree is not None:
+        nodes, root = np.ascontiguousarray(light_tree[0], LIGHT_NODE_DTYPE), int(light_tree[1])
+        keep.append(nodes)
+        ltv = LightTreeView(nodes.ctypes.data, len(nodes), root)
+    keep += [md, idesc, mdesc]
+    desc = SceneDesc(md, len(meshes), idesc, len(instances), _view(tlas), mdesc, len(materials), ltv)
+    return desc, keep
+
+
+def build_light_tree(scene: dict):
+    """Host light-tree builder (`tpt_light_tree_build`): (nodes[LIGHT_NODE_DTYPE], root)."""
+    desc, keep = scene_desc(scene["meshes"], scene["instances"], materials=scene["materials"])
+    h = C.c_void_p()
+    _check(lib().tpt_light_tree_build(C.byref(desc), C.byref(h)))
+    try:
+        v = LightTreeView()
+        _check(lib().tpt_light_tree_view_of(h, C.byref(v)))
+        nodes = np.zeros(v.num_nodes, LIGHT_NODE_DTYPE)
+        C.memmove(nodes.ctypes.data, v.nodes, nodes.nbytes)
+        return nodes, v.root
+    finally:
+        lib().tpt_light_tree_free(h)
+
+
 class Scene:
     """Device-resident geometry (`tpt_scene`), uploaded from host arrays.
 
@@ -208,42 +332,47 @@ class Scene:
     mesh, material, local_to_world, world_to_local (4x4 column-major) and
     normal_to_world (3x3)."""
 
-    def __init__(self, ctx: Context, meshes, instances, tlas=None):
+    def __init__(self, ctx: Context, meshes, instances, tlas=None, materials=None, light_tree=None):
         self.ctx = ctx
-        keep = []
-        md = (MeshDesc * max(1, len(meshes)))()
-        for i, m in enumerate(meshes):
-            pos = np.ascontiguousarray(m["positions"], np.float32)
-            idx = np.ascontiguousarray(m["indices"], np.uint32).reshape(-1)
-            nrm = m.get("normals")
-            uv = m.get("uvs")
-            nrm = None if nrm is None else np.ascontiguousarray(nrm, np.float32)
-            uv = None if uv is None else np.ascontiguousarray(uv, np.float32)
-            keep += [pos, idx, nrm, uv]
-            q = m.get("qbvh")
-            if q is not None:
-                q = (np.ascontiguousarray(q[0]), np.ascontiguousarray(q[1], np.uint32))
-                keep += list(q)
-            md[i] = MeshDesc(
-                pos.ctypes.data, None if nrm is None else nrm.ctypes.data, None if uv is None else uv.ctypes.data,
-                pos.shape[0], idx.ctypes.data, idx.size, _view(q)
-            )
-        idesc = (InstanceDesc * max(1, len(instances)))()
-        for i, inst in enumerate(instances):
-            d = InstanceDesc()
-            d.mesh_index = inst["mesh"]
-            d.material_index = inst.get("material", 0)
-            d.local_to_world[:] = np.asarray(inst["local_to_world"], np.float32).reshape(16).tolist()
-            d.world_to_local[:] = np.asarray(inst["world_to_local"], np.float32).reshape(16).tolist()
-            d.normal_to_world[:] = np.asarray(inst["normal_to_world"], np.float32).reshape(9).tolist()
-            idesc[i] = d
-        if tlas is not None:
-            tlas = (np.ascontiguousarray(tlas[0]), np.ascontiguousarray(tlas[1], np.uint32))
-            keep += list(tlas)
-        desc = SceneDesc(md, len(meshes), idesc, len(instances), _view(tlas))
+        desc, keep = scene_desc(meshes, instances, tlas, materials, light_tree)
         h = C.c_void_p()
         _check(lib().tpt_scene_upload(ctx.h, C.byref(desc), C.byref(h)), ctx)
         self.h = h
+
+    def light_tree(self):
+        """(nodes[LIGHT_NODE_DTYPE], root) of the tree the scene uses."""
+        v = LightTreeView()
+        _check(lib().tpt_scene_light_tree(self.h, C.byref(v)))
+        nodes = np.zeros(v.num_nodes, LIGHT_NODE_DTYPE)
+        if v.num_nodes:
+            C.memmove(nodes.ctypes.data, v.nodes, nodes.nbytes)
+        return nodes, v.root
+
+    def job(self, camera: dict, width: int, height: int, spp: int, max_depth: int, integrator: int = 0,
+            execution: int = EXEC_WAVEFRONT):
+        cam = CameraDesc()
+        cam.eye[:] = [float(np.float32(x)) for x in camera["eye"]]
+        cam.look_at[:] = [float(np.float32(x)) for x in camera["look_at"]]
+        cam.up[:] = [float(np.float32(x)) for x in camera["up"]]
+        cam.fov_y = float(np.float32(camera["fov_y"]))
+        cam.exposure = float(np.float32(camera.get("exposure", 1.0)))
+        return RenderJob(self.h.value, cam, width, height, spp, max_depth, integrator, execution)
+
+    def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int, integrator: int = 0,
+               execution: int = EXEC_WAVEFRONT):
+        """`tpt_render`: returns float32 [height, width, 3] (host)."""
+        j = self.job(camera, width, height, spp, max_depth, integrator, execution)
+        out = np.empty((height, width, 3), np.float32)
+        ptrs = (C.c_void_p * 1)(out.ctypes.data)
+        _check(lib().tpt_render(self.ctx.h, C.byref(j), 1, ptrs), self.ctx)
+        return out
+
+    def render_device(self, job, out_ptr: int, stream=None):
+        _check(lib().tpt_render_device(self.ctx.h, C.byref(job), C.c_void_p(out_ptr), _stream(stream)), self.ctx)
+
+    def render_samples_device(self, job, first: int, count: int, out_ptr: int, stream=None):
+        _check(lib().tpt_render_samples_device(self.ctx.h, C.byref(job), first, count, C.c_void_p(out_ptr),
+                                               _stream(stream)), self.ctx)
 
     def device_bytes(self) -> int:
         v = C.c_uint64()
@@ -256,7 +385,10 @@ class Scene:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
 
     # -- queries ----------------------------------------------------------
     def closest_hit(self, rays: np.ndarray, mode: int = CLOSEST_HIT, want_instance=False, want_bary=False):

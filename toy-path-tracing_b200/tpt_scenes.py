@@ -100,3 +100,102 @@ def incoherent_rays(n: int = 1 << 24, seed: int = 3, cube: float = 100.0):
     rays[3:6] = d
     rays[6] = np.inf
     return rays
+
+
+# ---------------------------------------------------------------------------
+# Cornell-box scene: 5 wall quads, 2 boxes rotated by U[15, 20] degrees about
+# +y (one each way), one 0.25 x 0.25 emissive quad just below the ceiling
+# (36 triangles).  Materials: one per wall/box with base colour U[0.1, 0.8]^3,
+# either NormalizedLambert (rho = colour) or OpenPBR (base_color = colour,
+# roughness 1), plus EmissiveMaterial(colour 1, strength 15).
+
+LAMBERT, EMISSIVE, OPENPBR = 0, 1, 2
+
+
+def _quad(p0, p1, p2, p3, normal):
+    pos = np.array([p0, p1, p2, p3], np.float32)
+    nrm = np.tile(np.asarray(normal, np.float32), (4, 1))
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    idx = np.array([0, 1, 2, 0, 2, 3], np.uint32)
+    return {"positions": pos, "normals": nrm, "uvs": uv, "indices": idx}
+
+
+def _unit_box():
+    """Axis-aligned box [-0.5,0.5]x[0,1]x[-0.5,0.5], 4 vertices per face (24), 12 triangles."""
+    faces = [
+        ((1, 0, 0), [(0.5, 0, -0.5), (0.5, 1, -0.5), (0.5, 1, 0.5), (0.5, 0, 0.5)]),
+        ((-1, 0, 0), [(-0.5, 0, 0.5), (-0.5, 1, 0.5), (-0.5, 1, -0.5), (-0.5, 0, -0.5)]),
+        ((0, 1, 0), [(-0.5, 1, -0.5), (-0.5, 1, 0.5), (0.5, 1, 0.5), (0.5, 1, -0.5)]),
+        ((0, -1, 0), [(-0.5, 0, 0.5), (-0.5, 0, -0.5), (0.5, 0, -0.5), (0.5, 0, 0.5)]),
+        ((0, 0, 1), [(0.5, 0, 0.5), (0.5, 1, 0.5), (-0.5, 1, 0.5), (-0.5, 0, 0.5)]),
+        ((0, 0, -1), [(-0.5, 0, -0.5), (-0.5, 1, -0.5), (0.5, 1, -0.5), (0.5, 0, -0.5)]),
+    ]
+    pos, nrm, uv, idx = [], [], [], []
+    for f, (n, corners) in enumerate(faces):
+        base = 4 * f
+        pos += corners
+        nrm += [n] * 4
+        uv += [(0, 0), (1, 0), (1, 1), (0, 1)]
+        idx += [base, base + 1, base + 2, base, base + 2, base + 3]
+    return {"positions": np.array(pos, np.float32), "normals": np.array(nrm, np.float32),
+            "uvs": np.array(uv, np.float32), "indices": np.array(idx, np.uint32)}
+
+
+def instance_matrix(mesh, material, l2w64):
+    """Instance record from a float64 4x4 local-to-world matrix (math convention)."""
+    w2l64 = np.linalg.inv(l2w64)
+    n2w = w2l64[:3, :3].T  # glam: Mat3::from_mat4(world_to_local.transpose())
+    return {
+        "mesh": mesh,
+        "material": material,
+        "local_to_world": l2w64.T.astype(np.float32).reshape(16),
+        "world_to_local": w2l64.T.astype(np.float32).reshape(16),
+        "normal_to_world": n2w.T.astype(np.float32).reshape(9),
+    }
+
+
+def _rot_y(deg):
+    a = np.radians(deg)
+    m = np.eye(4)
+    m[0, 0], m[0, 2], m[2, 0], m[2, 2] = np.cos(a), np.sin(a), -np.sin(a), np.cos(a)
+    return m
+
+
+def _trs(t, deg, s):
+    m = np.eye(4)
+    m[:3, 3] = t
+    sc = np.diag([s[0], s[1], s[2], 1.0])
+    return m @ _rot_y(deg) @ sc
+
+
+def cornell_box(seed: int = 1, material: int = OPENPBR, light_strength: float = 15.0):
+    rng = np.random.default_rng(seed)
+    L, H = 1.5, 3.0
+    meshes = [
+        _quad((-L, 0, L), (L, 0, L), (L, 0, -L), (-L, 0, -L), (0, 1, 0)),      # floor
+        _quad((-L, H, -L), (L, H, -L), (L, H, L), (-L, H, L), (0, -1, 0)),     # ceiling
+        _quad((-L, 0, -L), (L, 0, -L), (L, H, -L), (-L, H, -L), (0, 0, 1)),    # back
+        _quad((-L, 0, L), (-L, 0, -L), (-L, H, -L), (-L, H, L), (1, 0, 0)),    # left
+        _quad((L, 0, -L), (L, 0, L), (L, H, L), (L, H, -L), (-1, 0, 0)),       # right
+        _unit_box(),
+        _quad((-0.125, H - 0.01, -0.125), (0.125, H - 0.01, -0.125), (0.125, H - 0.01, 0.125),
+              (-0.125, H - 0.01, 0.125), (0, -1, 0)),                           # light
+    ]
+    colors = rng.uniform(0.1, 0.8, (7, 3)).astype(np.float32)
+    materials = []
+    for c in colors:
+        if material == LAMBERT:
+            materials.append({"kind": LAMBERT, "rho": c})
+        else:
+            materials.append({"kind": OPENPBR, "base_color": c, "base_diffuse_roughness": 1.0,
+                              "specular_roughness": 1.0})
+    materials.append({"kind": EMISSIVE, "color": np.ones(3, np.float32), "strength": np.float32(light_strength)})
+    a1, a2 = rng.uniform(15.0, 20.0, 2)
+    instances = [identity_instance(k, k) for k in range(5)]
+    instances.append(instance_matrix(5, 5, _trs((-0.55, 0.0, -0.45), a1, (0.9, 1.8, 0.9))))
+    instances.append(instance_matrix(5, 6, _trs((0.6, 0.0, 0.5), -a2, (0.9, 0.9, 0.9))))
+    instances.append(identity_instance(6, 7))
+    camera = {"eye": (0.0, 1.5, 6.8), "look_at": (0.0, 1.5, 0.0), "up": (0.0, 1.0, 0.0),
+              "fov_y": float(np.float32(np.radians(38.0))), "exposure": 1.0}
+    return {"meshes": meshes, "instances": instances, "materials": materials, "camera": camera,
+            "angles": (float(a1), float(a2)), "seed": seed}
