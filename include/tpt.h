@@ -257,6 +257,19 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
 tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first, uint64_t count,
                                      float* out_samples, void* stream);
 
+/* Allocation-free variant of tpt_render_device, for callers that cannot call
+ * cudaMalloc while they render (work recorded in a CUDA stream capture, hosts
+ * whose device memory belongs to another allocator with a fixed budget,
+ * latency-critical loops).  It has no counterpart in the reference.
+ * Runs the megakernel execution (the job's `execution` field is not read) with
+ * its per-sample scratch in a fixed array inside the library: at most
+ * width * height * spp = 2^20 paths per call (12 MiB, held on every device that
+ * loads the library until exit); larger jobs fail with TPT_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Calls share the array: two calls
+ * whose work overlaps on the GPU race.  Output equals tpt_render_device's. */
+tpt_status tpt_render_device_noalloc(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -163,6 +163,12 @@ uint32_t chunk_pixels(const RenderLaunch& L) {
 
 }  // namespace
 
+namespace tpt {
+tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* out) {
+  return make_launch(ctx, job, out);
+}
+}  // namespace tpt
+
 extern "C" {
 
 tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream) {

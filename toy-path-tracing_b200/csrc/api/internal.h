@@ -79,6 +79,9 @@ cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const
 cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first_pixel, uint32_t n_pixels,
                               float exposure, float* image, cudaStream_t stream);
 
+// capi_render.cpp: validates a job and derives its launch parameters.
+tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* out);
+
 // wavefront_kernels.cu
 cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                                const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s);

@@ -159,6 +159,7 @@ EXPORTED_SYMBOLS = [
     "tpt_light_tree_build",
     "tpt_light_tree_view_of",
     "tpt_light_tree_free",
+    "tpt_render_device_noalloc",
 ]
 
 
@@ -185,6 +186,7 @@ def _declare(L):
         "tpt_light_tree_build": (i32, [C.POINTER(SceneDesc), C.POINTER(vp)]),
         "tpt_light_tree_view_of": (i32, [vp, C.POINTER(LightTreeView)]),
         "tpt_light_tree_free": (i32, [vp]),
+        "tpt_render_device_noalloc": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
