@@ -47,6 +47,7 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--rays-log2", type=int, default=24, help="rays per batch = 2^k (profiling uses smaller)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-render", action="store_true", help="skip the render workload block")
     return p.parse_args()
 
 
@@ -77,7 +78,7 @@ def make_workload(rank: int, rays_log2: int):
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(mesh, batches, target_s=8.0, max_log2=22):
+def cpu_reference_rate(mesh, batches, target_s=8.0, max_log2=24):
     """Oracle (CPU restatement of qbvh.rs/scene closest_hit) on all host cores:
     grows a sample until it runs for target_s seconds; returns rays/s."""
     import oracle as orc
@@ -182,6 +183,63 @@ def profiled_traffic():
         return None
     m = re.search(r"dram_bytes_per_full_launch:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
+
+
+RENDER_CFG = {"scene": "cornell_box(seed=1), NormalizedLambert twin of the OpenPBR diffuse walls",
+              "width": 256, "height": 256, "spp": 64, "max_depth": 8, "triangles": 36}
+
+
+def render_block(ctx, steps, warmup, cpu=True):
+    """Cornell box 256x256, 64 spp, depth 8: wavefront vs megakernel Msamples/s
+    (identical images by construction, so equal RMSE), and the oracle on the host."""
+    import torch
+
+    import tpt
+    import tpt_scenes
+
+    sc = tpt_scenes.cornell_box(1, tpt_scenes.LAMBERT)
+    scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
+    W, H, spp, depth = RENDER_CFG["width"], RENDER_CFG["height"], RENDER_CFG["spp"], RENDER_CFG["max_depth"]
+    stream = torch.cuda.current_stream()
+    img = torch.empty(W * H * 3, device="cuda")
+    out = {"config": RENDER_CFG, "unit": "Msamples/s"}
+    for name, ex in (("wavefront", tpt.EXEC_WAVEFRONT), ("megakernel", tpt.EXEC_MEGAKERNEL)):
+        job = scene.job(sc["camera"], W, H, spp, depth, execution=ex)
+        for _ in range(warmup):
+            scene.render_device(job, img.data_ptr(), stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = max(1, steps if ex == tpt.EXEC_WAVEFRONT else min(steps, 2))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(n):
+            scene.render_device(job, img.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        out[name] = {"value": W * H * spp / ms / 1e3, "ms_per_image": ms}
+    out["wavefront_over_megakernel"] = out["wavefront"]["value"] / out["megakernel"]["value"]
+    if cpu:
+        import oracle as orc
+
+        ref = orc.RenderScene(sc, scene.light_tree())
+        threads = os.cpu_count() or 1
+        # evenly spaced rows (cost varies across the image), grown until ~5 s of CPU work
+        n_rows = 4
+        while True:
+            step = max(1, H // n_rows)
+            rows = list(range(0, H, step))
+            t0 = time.perf_counter()
+            for r in rows:
+                ref.render(sc["camera"], W, H, spp, depth, pixels=(r * W, (r + 1) * W), nthreads=threads)
+            dt = time.perf_counter() - t0
+            if dt > 5.0 or len(rows) >= H:
+                break
+            n_rows = min(H, n_rows * max(2, int(5.0 / max(dt, 1e-3))))
+        out["cpu_baseline"] = {"value": len(rows) * W * spp / dt / 1e6, "cores": threads, "kind": "port",
+                               "sample": f"{len(rows)} evenly spaced rows of {W} pixels x {spp} spp, {dt:.1f} s"}
+        out["wavefront_over_cpu"] = out["wavefront"]["value"] / out["cpu_baseline"]["value"]
+    scene.close()
+    return out
 
 
 def run_ours(args):
@@ -311,6 +369,8 @@ def run_ours(args):
     if rank == 0 and not args.no_cpu_baseline:
         rate, threads, desc = cpu_reference_rate(mesh, batches)
         line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}
+    if rank == 0 and not args.no_render:
+        line["render"] = render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del scene
