@@ -89,6 +89,21 @@ def _declare(L):
         "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, vp]),
         "orc_render_emitted": (None, [vp, i32, i32, vp, vp, i32, i32, vp, vp, vp, f32, i32, vp]),
         "orc_render_material_pdf": (f32, [vp, i32, i32, vp, vp, vp]),
+        "orc_render_scene_set_openpbr": (C.c_char_p, [vp, u32, vp]),
+        "orc_lut_dielectric_albedo": (None, [f32, vp]),
+        "orc_lut_conductor_ec": (None, [vp, vp]),
+        "orc_lut_dielectric_ec": (None, [vp, vp]),
+        "orc_lut_conductor_lookup_e": (f32, [f32, f32]),
+        "orc_openpbr_params_eval": (None, [vp, i32, f32, f32, vp, vp, i32, vp]),
+        "orc_openpbr_params_pdf": (f32, [vp, i32, f32, f32, vp, vp]),
+        "orc_openpbr_params_sample": (i32, [vp, i32, f32, f32, vp, f32, f32, f32, i32, vp]),
+        "orc_openpbr_params_eval_batch": (None, [vp, i32, f32, f32, vp, vp, u64, i32, vp, vp]),
+        "orc_eon_eval_batch": (None, [vp, f32, vp, vp, u64, vp, vp]),
+        "orc_eon_sample": (i32, [vp, f32, vp, f32, f32, vp]),
+        "orc_openpbr_unsupported": (C.c_char_p, [vp]),
+        "orc_openpbr_eval": (None, [vp, i32, vp, vp, i32, vp]),
+        "orc_openpbr_pdf": (f32, [vp, i32, vp, vp]),
+        "orc_openpbr_sample": (i32, [vp, i32, vp, f32, f32, f32, i32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -237,6 +252,11 @@ class RenderScene:
         col = np.array([np.asarray(m.get("color", (0, 0, 0)), np.float32) for m in mats], np.float32)
         st = np.array([m.get("strength", 0.0) for m in mats], np.float32)
         lib().orc_render_scene_set_materials(self.h, _p(kinds), _p(rho), _p(col), _p(st), len(mats))
+        for i, m in enumerate(mats):
+            if m["kind"] == 2:
+                why = lib().orc_render_scene_set_openpbr(self.h, i, _p(pack_openpbr(m)))
+                if why:
+                    raise ValueError(why.decode())
         nodes, root = light_tree
         nodes = np.ascontiguousarray(nodes)
         lib().orc_render_scene_set_light_tree(self.h, nodes.ctypes.data if len(nodes) else None, len(nodes), int(root))
@@ -288,3 +308,168 @@ class RenderScene:
     def material_pdf(self, inst, tri, bary, incident, wi):
         arrs = [np.asarray(a, np.float32) for a in (bary, incident, wi)]
         return lib().orc_render_material_pdf(self.h, inst, tri, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]))
+
+
+# --------------------------------------------------------------------------
+# OpenPBR (bsdf/open_pbr.rs, material/open_pbr.rs, bsdf/directional_albedo.rs)
+
+# OpenPbrMaterial's untextured parameters in the C ABI's tpt_openpbr_desc
+# layout, with the defaults of OpenPbrMaterial::new (material/open_pbr.rs:84-145).
+OPENPBR_FIELDS = [
+    ("base_weight", 1, 1.0), ("base_color", 3, 0.8), ("base_diffuse_roughness", 1, 0.0),
+    ("base_metalness", 1, 0.0), ("specular_weight", 1, 1.0), ("specular_color", 3, 1.0),
+    ("specular_roughness", 1, 0.3), ("specular_ior", 1, 1.5), ("specular_roughness_anisotropy", 1, 0.0),
+    ("transmission_weight", 1, 0.0), ("transmission_color", 3, 1.0), ("subsurface_weight", 1, 0.0),
+    ("subsurface_color", 3, 0.8), ("fuzz_weight", 1, 0.0), ("fuzz_color", 3, 1.0), ("fuzz_roughness", 1, 0.5),
+    ("coat_weight", 1, 0.0), ("coat_color", 3, 1.0), ("coat_roughness", 1, 0.0),
+    ("coat_roughness_anisotropy", 1, 0.0), ("coat_ior", 1, 1.6), ("coat_darkening", 1, 1.0),
+    ("thin_film_weight", 1, 0.0), ("thin_film_thickness", 1, 0.5), ("thin_film_ior", 1, 1.4),
+    ("emission_luminance", 1, 0.0), ("emission_color", 3, 1.0), ("geometry_opacity", 1, 1.0),
+    ("geometry_thin_walled", 1, 0),
+]
+OPENPBR_DTYPE = np.dtype([(n, "<u4" if n == "geometry_thin_walled" else "<f4", (k,) if k > 1 else ())
+                          for n, k, _ in OPENPBR_FIELDS])
+assert OPENPBR_DTYPE.itemsize == 43 * 4
+
+# OpenPbrBsdfParams as the flat float array of orc_openpbr_params_* (order of
+# the oracle's OpenPbrParams; front_face last, as 0/1).
+OPENPBR_PARAM_FIELDS = [
+    ("base_color", 3), ("base", 1), ("specular", 1), ("specular_color", 3), ("specular_alpha_x", 1),
+    ("specular_alpha_y", 1), ("specular_eta", 1), ("transmission_eta", 1), ("metalness", 1), ("coat", 1),
+    ("coat_color", 3), ("coat_darkening", 3), ("coat_alpha_x", 1), ("coat_alpha_y", 1), ("coat_eta", 1),
+    ("fuzz", 1), ("fuzz_color", 3), ("fuzz_roughness", 1), ("transmission", 1), ("transmission_color", 3),
+    ("diffuse_roughness", 1), ("subsurface", 1), ("subsurface_color", 3), ("front_face", 1),
+]
+
+
+def pack_openpbr(m: dict) -> np.ndarray:
+    """One tpt_openpbr_desc record from a material dict (missing keys: defaults)."""
+    rec = np.zeros(1, OPENPBR_DTYPE)
+    for name, k, default in OPENPBR_FIELDS:
+        rec[name] = m.get(name, default if k == 1 else (default,) * 3)
+    return rec
+
+
+def pack_openpbr_params(p: dict) -> np.ndarray:
+    out = []
+    for name, k in OPENPBR_PARAM_FIELDS:
+        v = p[name]
+        out.extend(np.broadcast_to(np.asarray(v, np.float32), (k,)).tolist() if k > 1 else [float(v)])
+    return np.asarray(out, np.float32)
+
+
+def lut_dielectric_albedo(eta: float) -> np.ndarray:
+    out = np.empty(64 * 16 * 64 * 16, np.float32)
+    lib().orc_lut_dielectric_albedo(float(eta), _p(out))
+    return out
+
+
+def lut_conductor_ec():
+    e, e_avg = np.empty(64 * 64, np.float32), np.empty(64, np.float32)
+    lib().orc_lut_conductor_ec(_p(e), _p(e_avg))
+    return e, e_avg
+
+
+def lut_dielectric_ec():
+    e, e_avg = np.empty(32 * 32 * 32, np.float32), np.empty(32 * 32, np.float32)
+    lib().orc_lut_dielectric_ec(_p(e), _p(e_avg))
+    return e, e_avg
+
+
+def _v3(a):
+    return np.ascontiguousarray(np.asarray(a, np.float32).reshape(3))
+
+
+def _unpack_sample(ok, out):
+    if not ok:
+        return None
+    return {"weight": out[0:3].copy(), "wi": out[3:6].copy(), "pdf": float(out[6]), "pdf_rev": float(out[7]),
+            "flags": int(out[8:9].view(np.uint32)[0])}
+
+
+class OpenPbrParamsBsdf:
+    """OpenPbrBsdf built from explicit OpenPbrBsdfParams (the reference's unit
+    tests construct it this way).  luts: "real" (scene tables for spec_eta /
+    coat_eta) or "const" (the tests' constant tables)."""
+
+    def __init__(self, params: dict, luts="real", spec_eta=1.5, coat_eta=1.5):
+        self.flat = pack_openpbr_params(params)
+        self.mode = 0 if luts == "real" else 1
+        self.se, self.ce = float(spec_eta), float(coat_eta)
+
+    def eval(self, wo, wi, mode=0):
+        out = np.zeros(3, np.float32)
+        lib().orc_openpbr_params_eval(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)), _p(_v3(wi)), mode,
+                                      _p(out))
+        return out
+
+    def pdf(self, wo, wi):
+        return lib().orc_openpbr_params_pdf(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)), _p(_v3(wi)))
+
+    def eval_pdf_batch(self, wo, wis, mode=0):
+        wis = np.ascontiguousarray(wis, np.float32).reshape(-1, 3)
+        f = np.zeros_like(wis)
+        pdf = np.zeros(len(wis), np.float32)
+        lib().orc_openpbr_params_eval_batch(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)), _p(wis),
+                                            len(wis), mode, _p(f), _p(pdf))
+        return f, pdf
+
+    def sample(self, wo, u_lobe, u_dir, mode=0):
+        out = np.zeros(9, np.float32)
+        ok = lib().orc_openpbr_params_sample(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)), float(u_lobe),
+                                             float(u_dir[0]), float(u_dir[1]), mode, _p(out))
+        return _unpack_sample(ok, out)
+
+
+def eon_eval_pdf_batch(rho, roughness, wo, wis):
+    """EonBsdf::eval / pdf (bsdf/eon.rs) over directions wis (n x 3)."""
+    wis = np.ascontiguousarray(wis, np.float32).reshape(-1, 3)
+    f = np.zeros_like(wis)
+    pdf = np.zeros(len(wis), np.float32)
+    lib().orc_eon_eval_batch(_p(_v3(rho)), float(roughness), _p(_v3(wo)), _p(wis), len(wis), _p(f), _p(pdf))
+    return f, pdf
+
+
+def eon_sample(rho, roughness, wo, us):
+    out = np.zeros(9, np.float32)
+    ok = lib().orc_eon_sample(_p(_v3(rho)), float(roughness), _p(_v3(wo)), float(us[0]), float(us[1]), _p(out))
+    return _unpack_sample(ok, out)
+
+
+def hemisphere_grid(n_z: int, n_phi: int):
+    """Midpoint grid over the upper hemisphere in (z, phi) with its cell
+    measure dz * dphi (bsdf/mod.rs:45-63, eon.rs tests)."""
+    dz = np.float32(1.0) / np.float32(n_z)
+    dphi = np.float32(2.0 * np.pi) / np.float32(n_phi)
+    z = (np.arange(n_z, dtype=np.float32) + np.float32(0.5)) * dz
+    phi = (np.arange(n_phi, dtype=np.float32) + np.float32(0.5)) * dphi
+    r = np.sqrt(np.maximum(np.float32(1.0) - z * z, np.float32(0.0)))
+    zz, pp = np.meshgrid(z, phi, indexing="ij")
+    rr = np.broadcast_to(r[:, None], zz.shape)
+    wis = np.stack([rr * np.cos(pp), rr * np.sin(pp), zz], -1).reshape(-1, 3).astype(np.float32)
+    return wis, float(dz) * float(dphi)
+
+
+class OpenPbrMaterial:
+    """OpenPbrMaterial::make_bsdf of an untextured material, queried in the
+    shading frame (local wo / wi)."""
+
+    def __init__(self, m: dict):
+        self.rec = pack_openpbr(m)
+        why = lib().orc_openpbr_unsupported(_p(self.rec))
+        if why:
+            raise ValueError(why.decode())
+
+    def eval(self, wo, wi, front=True, mode=0):
+        out = np.zeros(3, np.float32)
+        lib().orc_openpbr_eval(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)), mode, _p(out))
+        return out
+
+    def pdf(self, wo, wi, front=True):
+        return lib().orc_openpbr_pdf(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)))
+
+    def sample(self, wo, u_lobe, u_dir, front=True, mode=0):
+        out = np.zeros(9, np.float32)
+        ok = lib().orc_openpbr_sample(_p(self.rec), int(front), _p(_v3(wo)), float(u_lobe), float(u_dir[0]),
+                                      float(u_dir[1]), mode, _p(out))
+        return _unpack_sample(ok, out)

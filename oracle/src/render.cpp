@@ -217,12 +217,12 @@ float lambert_pdf(const Vertex& v, Vec3 wi) {
   if (wo_l.z <= 0.0f || wi_l.z <= 0.0f) return 0.0f;
   return fmax_num(wi_l.z, 0.0f) / kPi;
 }
-struct BsdfSample {
+struct MatSample {
   Vec3 weight, wi;
   float pdf;
   bool delta;
 };
-bool lambert_sample(const Material& m, const Vertex& v, Vec2 u, BsdfSample* s) {
+bool lambert_sample(const Material& m, const Vertex& v, Vec2 u, MatSample* s) {
   Vec3 wo_l = normalize_or_zero(v.frame.to_local(v.wo));
   if (wo_l.z <= 0.0f) return false;
   float r = std::sqrt(clampf(u.x, 0.0f, 1.0f));
@@ -239,6 +239,24 @@ bool lambert_sample(const Material& m, const Vertex& v, Vec2 u, BsdfSample* s) {
   return dot(s->wi, v.ng) > kGeomCosEps;
 }
 Vec3 emissive_le(const Material& m) { return m.color * m.strength; }
+
+// OpenPbrMaterial::sample (material/open_pbr.rs:489-563), radiance transport
+// (modified_bsdf_sample_weight leaves the weight unchanged).
+bool openpbr_sample(const Material& m, const Vertex& v, float u_lobe, Vec2 u_dir, MatSample* s) {
+  if (dot(v.wo, v.ng) <= 0.0f) return false;
+  Vec3 wo_l = normalize_or_zero(v.frame.to_local(v.wo));
+  if (wo_l.z <= 0.0f) return false;
+  OpenPbrBsdf b{make_openpbr_params(m.openpbr, v.front_face, wo_l), m.luts};
+  BsdfSample bs;
+  if (!b.sample(wo_l, u_lobe, u_dir, kRadiance, &bs)) return false;
+  Vec3 wi = v.frame.to_world(bs.wi);
+  if (dot(wi, v.ng) <= kGeomCosEps) return false;  // reflection only
+  s->weight = bs.weight;
+  s->wi = wi;
+  s->pdf = bs.pdf;
+  s->delta = (bs.flags & kDelta) != 0;
+  return true;
+}
 
 Vec3 offset_origin(Vec3 p, Vec3 ng, Vec3 d) {
   Vec3 n = dot(d, ng) >= 0.0f ? ng : -ng;
@@ -410,6 +428,7 @@ Vertex RenderScene::shading_vertex(int inst, int tri, Vec3 b, Vec3 incident) con
   v.p = interp(b, p[0], p[1], p[2]);
   Vec3 gn = normalize_or_zero(cross(p[1] - p[0], p[2] - p[0]));
   Vec3 sn = normalize_or_zero(interp(b, n[0], n[1], n[2]));
+  v.front_face = dot(gn, -incident) >= 0.0f;
   v.ng = face_forward(gn, -incident);
   Vec3 raw_ns = length_squared(sn) > 0.0f ? sn : v.ng;
   v.ns = face_forward(raw_ns, v.ng);
@@ -444,8 +463,10 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
     if (m->kind == kEmissive) break;
     L += beta * direct_light(s, *m, v, rnd);
-    BsdfSample bs;
-    if (!lambert_sample(*m, v, rnd.material.u_dir, &bs)) break;
+    MatSample bs;
+    bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+                                  : lambert_sample(*m, v, rnd.material.u_dir, &bs);
+    if (!ok) break;
     beta *= bs.weight;
     if (depth + 1 >= 4) {
       float q = clampf(max_element(beta), 0.05f, 1.0f);

@@ -10,6 +10,7 @@
 #pragma once
 #include "camera.h"
 #include "geometry.h"
+#include "openpbr.h"
 #include "sampler.h"
 
 namespace orc {
@@ -24,7 +25,13 @@ struct Material {
   Vec3 rho;        // NormalizedLambert
   Vec3 color;      // Emissive
   float strength = 0;
+  OpenPbrDesc openpbr{};   // OpenPbr
+  OpenPbrLuts luts{};      // the tables the scene installed for it (scene/mod.rs:164-185)
 };
+
+// Scene-level table cache (DirectionalAlbedoCache, directional_albedo.rs:38-118):
+// one albedo table per distinct eta, one of each energy-compensation table.
+OpenPbrLuts openpbr_luts_for(const OpenPbrDesc& m, int nthreads);
 
 // light_tree/mod.rs:65-86 flattened (64 bytes; same layout as the C ABI's tpt_light_node)
 struct LightNode {
@@ -53,6 +60,7 @@ struct Vertex {
   Vec3 p, ng, ns, wo;
   Frame frame;
   int32_t inst, tri;
+  bool front_face;
 };
 
 struct RenderScene {
