@@ -119,7 +119,50 @@ typedef enum tpt_material_kind {
   TPT_MATERIAL_OPENPBR = 2             /* OpenPbrMaterial (untextured), parameters in `openpbr` */
 } tpt_material_kind;
 
-struct tpt_openpbr_desc;
+/* OpenPbrMaterial's untextured parameters (material/open_pbr.rs:23-78), same
+ * names and meaning; tpt_openpbr_defaults() fills the values of
+ * OpenPbrMaterial::new (material/open_pbr.rs:84-145) with base_color 0.8.
+ * Lowered on upload into a flat device table (make_bsdf, material/open_pbr.rs:
+ * 393-487) plus directional-albedo and energy-compensation tables built on the
+ * GPU (bsdf/directional_albedo.rs).  The device path covers the base (EON
+ * diffuse), metal, specular reflection, coat and fuzz lobes with anisotropy and
+ * smooth (delta) lobes.  Upload rejects with TPT_ERR_INVALID_ARG a material
+ * with transmission_weight > 0, thin_film_weight > 0, emission_luminance > 0,
+ * geometry_opacity < 1 or geometry_thin_walled != 0.  subsurface_weight is
+ * ignored, as the reference forces it to 0 (validate_and_warn). */
+typedef struct tpt_openpbr_desc {
+  float base_weight;
+  float base_color[3];
+  float base_diffuse_roughness;
+  float base_metalness;
+  float specular_weight;
+  float specular_color[3];
+  float specular_roughness;
+  float specular_ior;
+  float specular_roughness_anisotropy;
+  float transmission_weight;
+  float transmission_color[3];
+  float subsurface_weight;
+  float subsurface_color[3];
+  float fuzz_weight;
+  float fuzz_color[3];
+  float fuzz_roughness;
+  float coat_weight;
+  float coat_color[3];
+  float coat_roughness;
+  float coat_roughness_anisotropy;
+  float coat_ior;
+  float coat_darkening;
+  float thin_film_weight;
+  float thin_film_thickness;
+  float thin_film_ior;
+  float emission_luminance;
+  float emission_color[3];
+  float geometry_opacity;
+  uint32_t geometry_thin_walled;
+} tpt_openpbr_desc;
+
+void tpt_openpbr_defaults(tpt_openpbr_desc* desc);
 
 typedef struct tpt_material_desc {
   uint32_t kind;
@@ -269,6 +312,32 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
  * first call before any stream capture.  Calls share the array: two calls
  * whose work overlaps on the GPU race.  Output equals tpt_render_device's. */
 tpt_status tpt_render_device_noalloc(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream);
+
+/* ---- OpenPBR tables and BSDF queries -------------------------------------
+ * The context builds each table on the GPU the first time a scene needs it and
+ * keeps it until destroyed (DirectionalAlbedoCache, directional_albedo.rs:
+ * 38-118): one directional-albedo table per distinct eta, one of each
+ * energy-compensation table.  These copy a table to host memory (building it
+ * first when needed); layouts and sizes are the reference's:
+ *   dielectric albedo  64 (sqrt cos) x 16 (phi) x 64 (roughness) x 16 (anisotropy)
+ *   conductor E        64 (roughness) x 64 (sqrt cos), E_avg 64
+ *   dielectric E       32 (eta) x 32 (roughness) x 32 (sqrt cos), E_avg 32 x 32 */
+tpt_status tpt_lut_dielectric_albedo(tpt_context* ctx, float eta, float* out);
+tpt_status tpt_lut_conductor_ec(tpt_context* ctx, float* e, float* e_avg);
+tpt_status tpt_lut_dielectric_ec(tpt_context* ctx, float* e, float* e_avg);
+
+/* OpenPbrBsdf::eval (radiance transport) and ::pdf of material `material` of an
+ * uploaded scene, for n direction pairs in the shading frame (device buffers:
+ * wo, wi n x 3; front_face n; f n x 3; pdf n).  The material must be OpenPBR. */
+tpt_status tpt_bsdf_eval_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
+                                const float* wo, const float* wi, const uint32_t* front_face, float* f, float* pdf,
+                                void* stream);
+/* OpenPbrBsdf::sample for n (wo, u) pairs: u n x 3 = (u_lobe, u_dir.x, u_dir.y);
+ * out n x 8 = weight (3), wi (3), pdf, flags (as uint32 bits: 1 reflection,
+ * 4 diffuse, 8 glossy, 16 delta; 0 = no sample). */
+tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
+                                  const float* wo, const float* u, const uint32_t* front_face, float* out,
+                                  void* stream);
 
 #ifdef __cplusplus
 }

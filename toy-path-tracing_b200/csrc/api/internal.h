@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -35,6 +36,11 @@ struct tpt_context {
   void* d_wf = nullptr;
   size_t d_wf_bytes = 0;
   tpt::WfBuffers wf{};
+  // OpenPBR tables (built on the GPU on first use, kept until destroy)
+  std::map<uint32_t, float*> da_tables;  // directional albedo per eta (bit pattern)
+  float* d_cec_e = nullptr;              // conductor E (64 x 64)
+  float* d_dec_e = nullptr;              // dielectric E (32 x 32 x 32)
+  std::vector<float> h_cec_e, h_cec_e_avg, h_dec_e, h_dec_e_avg;
 };
 
 struct tpt_qbvh {
@@ -51,6 +57,7 @@ struct tpt_scene {
   std::vector<uint32_t> mesh_tri_counts;
   tpt::DevRenderData render{};          // shading data for the render kernels
   tpt::LightTreeHost light_tree;        // host copy of the light tree
+  std::vector<uint32_t> material_kinds; // tpt_material_kind per material
 };
 
 namespace tpt {
@@ -89,6 +96,22 @@ cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, con
                             const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s);
 cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
+
+// capi_openpbr.cpp: the context's OpenPBR tables, built on first use.
+tpt_status ensure_ec_tables(tpt_context* ctx);
+tpt_status ensure_da_table(tpt_context* ctx, float eta, const float** out);
+
+// lut_kernels.cu: table construction (bit-exact with the reference's loops;
+// the sample tables come from lut_sample_tables).
+cudaError_t launch_lut_dielectric_albedo(float eta, const float* dirs, const float* phi_cs, float* out,
+                                         cudaStream_t s);
+cudaError_t launch_lut_conductor_e(const float* u, const float* cs, float* e, cudaStream_t s);
+cudaError_t launch_lut_dielectric_e(const float* uc, const float* ux, const float* cs, float* e, cudaStream_t s);
+// openpbr_query.cu: batched BSDF queries of one material.
+cudaError_t launch_bsdf_eval(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo, const float* wi,
+                             const uint32_t* front, float* f, float* pdf, cudaStream_t s);
+cudaError_t launch_bsdf_sample(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo,
+                               const float* u, const uint32_t* front, float* out, cudaStream_t s);
 
 // scene_render_upload.cpp: materials, shading arrays, light tree, emitter map.
 tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc);

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <string>
 
+#include "../host/openpbr_lower.h"
 #include "internal.h"
 
 namespace tpt {
@@ -42,10 +43,29 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   std::vector<HostMaterial> hmats(desc->num_materials);
   std::vector<DevMaterialRec> dmats(desc->num_materials);
   if (desc->num_materials && !desc->materials) return set_error(ctx, TPT_ERR_INVALID_ARG, "materials is NULL");
+  std::vector<DevOpenPbr> opbr;
+  s->material_kinds.assign(desc->num_materials, 0u);
   for (uint32_t i = 0; i < desc->num_materials; ++i) {
     const tpt_material_desc& m = desc->materials[i];
-    if (m.kind != TPT_MATERIAL_NORMALIZED_LAMBERT && m.kind != TPT_MATERIAL_EMISSIVE)
+    if (m.kind != TPT_MATERIAL_NORMALIZED_LAMBERT && m.kind != TPT_MATERIAL_EMISSIVE &&
+        m.kind != TPT_MATERIAL_OPENPBR)
       return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": unsupported kind");
+    s->material_kinds[i] = m.kind;
+    uint32_t opbr_index = 0;
+    if (m.kind == TPT_MATERIAL_OPENPBR) {
+      if (!m.openpbr) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": openpbr is NULL");
+      const std::string why = openpbr_unsupported(*m.openpbr);
+      if (!why.empty()) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": " + why);
+      const float *spec_da = nullptr, *coat_da = nullptr;
+      tpt_status st = ensure_ec_tables(ctx);
+      if (!st) st = ensure_da_table(ctx, openpbr_spec_table_eta(*m.openpbr), &spec_da);
+      if (!st && m.openpbr->coat_weight > 0.0f) st = ensure_da_table(ctx, openpbr_coat_table_eta(*m.openpbr), &coat_da);
+      if (st) return st;
+      DevOpenPbr rec;
+      lower_openpbr(*m.openpbr, spec_da, coat_da, ctx->h_cec_e_avg.data(), ctx->h_dec_e_avg.data(), &rec);
+      opbr_index = (uint32_t)opbr.size();
+      opbr.push_back(rec);
+    }
     HostMaterial h{};
     h.kind = m.kind;
     std::memcpy(h.rho, m.rho, 12);
@@ -57,6 +77,7 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
     std::memcpy(d.rho, m.rho, 12);
     std::memcpy(d.color, m.color, 12);
     d.strength = m.strength;
+    d.openpbr = opbr_index;
     dmats[i] = d;
   }
   for (uint32_t i = 0; i < desc->num_instances; ++i)
@@ -155,7 +176,10 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   if (!st) st = put(s, dmats, &R.mats);
   if (!st) st = put(s, lnodes, &R.ltree);
   if (!st) st = put(s, emap, &R.emitter_leaf);
+  if (!st) st = put(s, opbr, &R.openpbr);
   if (st) return st;
+  R.cec_e = ctx->d_cec_e;
+  R.dec_e = ctx->d_dec_e;
   R.ltree_root = s->light_tree.root;
   R.num_materials = desc->num_materials;
   // LightSampler::build_from_scene (light/mod.rs:134-188) with only the Tree category

@@ -8,6 +8,7 @@
 // differentials, which no material in scope reads.
 #pragma once
 #include "lights.cuh"
+#include "openpbr.cuh"
 #include "render_types.h"
 #include "sampler.cuh"
 #include "trace.cuh"
@@ -49,6 +50,7 @@ struct Vertex {
   V3 p, ng, ns, wo;
   Frame frame;
   uint32_t inst, tri;
+  bool front;  // geometric normal faces the incoming ray (ShadingVertex::front_face)
 };
 
 struct TriData {
@@ -109,6 +111,7 @@ __device__ __forceinline__ Vertex make_vertex(const TriData& T, uint32_t inst, u
   const V3 gn = normalize_or_zero(cross(T.p[1] - T.p[0], T.p[2] - T.p[0]));
   const V3 sn = normalize_or_zero(interp3(b, T.n[0], T.n[1], T.n[2]));
   const V3 minus_in = -incident;
+  v.front = dot(gn, minus_in) >= 0.0f;
   v.ng = face_forward(gn, minus_in);
   const V3 raw_ns = length_sq(sn) > 0.0f ? sn : v.ng;
   v.ns = face_forward(raw_ns, v.ng);
@@ -167,6 +170,39 @@ __device__ __forceinline__ bool lambert_sample(const DevMaterialRec& m, const Ve
   s.pdf = pdf;
   s.delta = false;
   return dot(s.wi, v.ng) > kGeomCosEps;
+}
+
+// OpenPbrMaterial::sample (material/open_pbr.rs:489-563) in radiance transport
+// (modified_bsdf_sample_weight leaves the weight unchanged there).
+static __device__ __noinline__ bool openpbr_sample(const DevRenderData& d, uint32_t opbr_index, const Vertex& v,
+                                            float u_lobe, float u0, float u1, BsdfSampleOut& s) {
+  if (dot(v.wo, v.ng) <= 0.0f) return false;
+  const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+  if (wo_l.z <= 0.0f) return false;
+  opbr::OpbrVertex ov;
+  opbr::init_vertex(ov, d.openpbr + opbr_index, d.cec_e, d.dec_e, wo_l, v.front);
+  opbr::Sample bs;
+  if (!opbr::sample(ov, u_lobe, u0, u1, bs)) return false;
+  const V3 wi = to_world(v.frame, bs.wi);
+  if (dot(wi, v.ng) <= kGeomCosEps) return false;  // reflection lobes only
+  s.wi = wi;
+  s.weight = bs.weight;
+  s.pdf = bs.pdf;
+  s.delta = (bs.flags & opbr::kFlagDelta) != 0;
+  return true;
+}
+
+// Material::sample for the BSDF materials in scope, with the vertex's
+// MaterialSampleRandoms (lobe at offset 5, direction at offset 7).
+__device__ __forceinline__ bool material_sample(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
+                                                const PathSamplerDev& ps, uint32_t depth, BsdfSampleOut& s) {
+  float ud0, ud1;
+  ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
+  if (m.kind == kDevOpenPbr) {
+    const float u_lobe = ps.sample_1d(vertex_dim(depth, kOffLobe));
+    return openpbr_sample(S.d, m.openpbr, v, u_lobe, ud0, ud1, s);
+  }
+  return lambert_sample(m, v, ud0, ud1, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -329,10 +365,8 @@ __device__ V3 trace_mis(const DevRender& S, Stack& st, const RenderLaunch& P, co
       if (!closest_hit(S, st, dp.so, dp.wi, sh, err) || ((uint32_t)sh.inst == dp.inst && (uint32_t)sh.tri == dp.tri))
         L = L + beta * dp.contrib;
     }
-    float ud0, ud1;
-    ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
     BsdfSampleOut s;
-    if (!lambert_sample(m, v, ud0, ud1, s)) break;
+    if (!material_sample(S, m, v, ps, depth, s)) break;
     beta = beta * s.weight;
     if (depth + 1 >= 4) {
       const float q = clampf(max_element(beta), 0.05f, 1.0f);

@@ -30,6 +30,61 @@ struct alignas(16) DevMaterialRec {
 };
 static_assert(sizeof(DevMaterialRec) == 64, "material record");
 
+// OpenPBR material lowered on the host (OpenPbrMaterial::make_bsdf,
+// material/open_pbr.rs:393-487, minus its per-vertex parts): the layer
+// parameters plus every constant of bsdf/open_pbr.rs that depends only on the
+// material (albedo-table axes, multiple-scattering terms, lobe weights, F82
+// terms, the view-independent half of the coat darkening), so that the device
+// evaluates the per-direction terms only.
+struct DevLerpAxis {  // compute_lut_axis_lerp (directional_albedo.rs:388-408)
+  uint32_t lo, hi;
+  float t;
+};
+struct DevMsFace {  // dielectric multiple scattering of one lobe seen from one face
+  float eta_o, one_minus_e_avg_o, ms_factor;
+  float lobe_ss, lobe_ms, lobe_total;  // dielectric_reflection_lobe_weights
+  DevLerpAxis r_axis, eta_axis;         // energy-compensation table axes at (roughness_eq, eta_o)
+};
+struct DevFresnelFace {  // base_dielectric_fresnel's weighted_fresnel_ratio arguments
+  float unc_ti, unc_tp, coat_ti, coat_tp;
+};
+enum : uint32_t {
+  kOpbrCoatRough = 1u,    // coat > 0 and not effectively smooth
+  kOpbrMetalRough = 2u,   // metalness > 0 and not smooth
+  kOpbrSpecRough = 4u,    // specular > 0 and not smooth
+  kOpbrDarkening = 8u,    // coat darkening active
+  kOpbrSpecDaSmooth = 16u,
+  kOpbrCoatDaSmooth = 32u,
+};
+struct alignas(16) DevOpenPbr {
+  float base_color[3], base;
+  float specular, specular_color[3];
+  float spec_ax, spec_ay, metalness, coat;
+  float coat_color[3], coat_ax;
+  float coat_ay, coat_eta, fuzz, fuzz_roughness;  // fuzz roughness clamped to [0.01, 1]
+  float fuzz_color[3], eon_r;
+  float eon_r_pow01;  // r^0.1 of the EON uniform-lobe probability
+  uint32_t flags;
+  float spec_da_eta, coat_da_eta;  // etas of the albedo tables
+  const float* spec_da;            // directional albedo tables (64 x 16 x 64 x 16)
+  const float* coat_da;
+  DevLerpAxis spec_da_r, coat_da_r;  // roughness axis at the roughness proxies
+  // metal (F82-tint Fresnel + conductor multiple scattering)
+  float f0[3], f82_delta[3];  // F0 and Schlick(F0, cos82) - target(cos82)
+  float f82_denom;
+  float cond_ss, cond_ms, cond_total, cond_one_minus_e_avg;
+  float cond_f_ms[3];
+  DevLerpAxis cond_r;
+  // dielectric multiple scattering: [0] specular, [1] coat; [face] 0 front, 1 back
+  DevMsFace ms[2][2];
+  DevFresnelFace fres[2];
+  float coat_clamped;  // coat weight clamped to [0, 1] for the Fresnel blend
+  // coat darkening (material/open_pbr.rs:823-858) without the view term
+  float dk_kr, dk_rb, dk_wd, dk_eta;
+  float dk_e_base[3];
+  uint32_t pad[3];
+};
+
 struct alignas(16) DevShadeInstance {
   float l2w[12];  // local_to_world affine columns c0..c3 (xyz each)
   float n2w[9];   // normal_to_world, column-major
@@ -54,7 +109,9 @@ struct DevRenderData {
   const DevMaterialRec* mats;
   const DevLightNodeRec* ltree;
   const uint32_t* emitter_leaf;
-  const void* openpbr;  // OpenPBR parameter table
+  const DevOpenPbr* openpbr;  // OpenPBR parameter table
+  const float* cec_e;         // conductor energy-compensation table (64 x 64)
+  const float* dec_e;         // dielectric energy-compensation table (32 x 32 x 32)
   uint32_t ltree_root;
   uint32_t has_tree;
   float tree_cat_pmf;  // LightSampler pmf of the Tree category

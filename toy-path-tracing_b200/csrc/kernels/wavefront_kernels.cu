@@ -124,10 +124,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
         dp.contrib = beta * dp.contrib;
         push_shadow = true;
       }
-      float ud0, ud1;
-      ps.sample_2d(vertex_dim(d, kOffDir), ud0, ud1);
       BsdfSampleOut s;
-      if (lambert_sample(m, v, ud0, ud1, s)) {
+      if (material_sample(S, m, v, ps, d, s)) {
         beta = beta * s.weight;
         bool alive = true;
         if (d + 1 >= 4) {

@@ -73,6 +73,44 @@ class InstanceDesc(C.Structure):
     ]
 
 
+# tpt_openpbr_desc: OpenPbrMaterial's untextured parameters with the defaults of
+# OpenPbrMaterial::new (material/open_pbr.rs:84-145; base_color defaults to 0.8).
+OPENPBR_FIELDS = [
+    ("base_weight", 1, 1.0), ("base_color", 3, 0.8), ("base_diffuse_roughness", 1, 0.0),
+    ("base_metalness", 1, 0.0), ("specular_weight", 1, 1.0), ("specular_color", 3, 1.0),
+    ("specular_roughness", 1, 0.3), ("specular_ior", 1, 1.5), ("specular_roughness_anisotropy", 1, 0.0),
+    ("transmission_weight", 1, 0.0), ("transmission_color", 3, 1.0), ("subsurface_weight", 1, 0.0),
+    ("subsurface_color", 3, 0.8), ("fuzz_weight", 1, 0.0), ("fuzz_color", 3, 1.0), ("fuzz_roughness", 1, 0.5),
+    ("coat_weight", 1, 0.0), ("coat_color", 3, 1.0), ("coat_roughness", 1, 0.0),
+    ("coat_roughness_anisotropy", 1, 0.0), ("coat_ior", 1, 1.6), ("coat_darkening", 1, 1.0),
+    ("thin_film_weight", 1, 0.0), ("thin_film_thickness", 1, 0.5), ("thin_film_ior", 1, 1.4),
+    ("emission_luminance", 1, 0.0), ("emission_color", 3, 1.0), ("geometry_opacity", 1, 1.0),
+    ("geometry_thin_walled", 1, 0),
+]
+
+
+class OpenPbrDesc(C.Structure):
+    _fields_ = [(n, C.c_uint32 if n == "geometry_thin_walled" else (C.c_float * 3 if k == 3 else C.c_float))
+                for n, k, _ in OPENPBR_FIELDS]
+
+
+assert C.sizeof(OpenPbrDesc) == 43 * 4
+
+
+def openpbr_desc(m: dict) -> OpenPbrDesc:
+    """A tpt_openpbr_desc from a material dict (missing keys: defaults)."""
+    d = OpenPbrDesc()
+    for name, k, default in OPENPBR_FIELDS:
+        v = m.get(name, default)
+        if k == 3:
+            getattr(d, name)[:] = [float(np.float32(x)) for x in np.broadcast_to(np.asarray(v, np.float32), (3,))]
+        elif name == "geometry_thin_walled":
+            setattr(d, name, int(v))
+        else:
+            setattr(d, name, float(np.float32(v)))
+    return d
+
+
 class MaterialDesc(C.Structure):
     _fields_ = [
         ("kind", C.c_uint32),
@@ -123,6 +161,8 @@ INTEGRATOR_MIS = 0
 EXEC_WAVEFRONT = 0
 EXEC_MEGAKERNEL = 1
 
+LAMBERT, EMISSIVE, OPENPBR = 0, 1, 2  # tpt_material_kind
+
 
 def lib():
     """Load libtpt_cuda.so; raises when the CUDA build is missing (no fallback)."""
@@ -160,6 +200,12 @@ EXPORTED_SYMBOLS = [
     "tpt_light_tree_view_of",
     "tpt_light_tree_free",
     "tpt_render_device_noalloc",
+    "tpt_openpbr_defaults",
+    "tpt_lut_dielectric_albedo",
+    "tpt_lut_conductor_ec",
+    "tpt_lut_dielectric_ec",
+    "tpt_bsdf_eval_device",
+    "tpt_bsdf_sample_device",
 ]
 
 
@@ -187,6 +233,12 @@ def _declare(L):
         "tpt_light_tree_view_of": (i32, [vp, C.POINTER(LightTreeView)]),
         "tpt_light_tree_free": (i32, [vp]),
         "tpt_render_device_noalloc": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
+        "tpt_openpbr_defaults": (None, [C.POINTER(OpenPbrDesc)]),
+        "tpt_lut_dielectric_albedo": (i32, [vp, C.c_float, vp]),
+        "tpt_lut_conductor_ec": (i32, [vp, vp, vp]),
+        "tpt_lut_dielectric_ec": (i32, [vp, vp, vp]),
+        "tpt_bsdf_eval_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, vp, vp, vp]),
+        "tpt_bsdf_sample_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -225,6 +277,22 @@ class Context:
         if getattr(self, "h", None):
             lib().tpt_context_destroy(self.h)
             self.h = None
+
+    # -- OpenPBR tables (built on the GPU on first use) -------------------------
+    def lut_dielectric_albedo(self, eta: float) -> np.ndarray:
+        out = np.empty(64 * 16 * 64 * 16, np.float32)
+        _check(lib().tpt_lut_dielectric_albedo(self.h, float(eta), _p(out)), self)
+        return out
+
+    def lut_conductor_ec(self):
+        e, e_avg = np.empty(64 * 64, np.float32), np.empty(64, np.float32)
+        _check(lib().tpt_lut_conductor_ec(self.h, _p(e), _p(e_avg)), self)
+        return e, e_avg
+
+    def lut_dielectric_ec(self):
+        e, e_avg = np.empty(32 * 32 * 32, np.float32), np.empty(32 * 32, np.float32)
+        _check(lib().tpt_lut_dielectric_ec(self.h, _p(e), _p(e_avg)), self)
+        return e, e_avg
 
     def __del__(self):
         try:
@@ -300,6 +368,10 @@ def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None):
         d.rho[:] = list(np.asarray(m.get("rho", (0, 0, 0)), np.float32))
         d.color[:] = list(np.asarray(m.get("color", (0, 0, 0)), np.float32))
         d.strength = float(np.float32(m.get("strength", 0.0)))
+        if d.kind == OPENPBR:
+            od = openpbr_desc(m)
+            keep.append(od)
+            d.openpbr = C.addressof(od)
         mdesc[i] = d
     ltv = LightTreeView(None, 0, 0)
     if light_tree is not None:
@@ -375,6 +447,19 @@ class Scene:
     def render_samples_device(self, job, first: int, count: int, out_ptr: int, stream=None):
         _check(lib().tpt_render_samples_device(self.ctx.h, C.byref(job), first, count, C.c_void_p(out_ptr),
                                                _stream(stream)), self.ctx)
+
+    def bsdf_eval_device(self, material: int, n: int, wo_ptr: int, wi_ptr: int, front_ptr: int, f_ptr: int,
+                         pdf_ptr: int, stream=None):
+        """`tpt_bsdf_eval_device`: OpenPBR eval + pdf of n direction pairs (device buffers)."""
+        _check(lib().tpt_bsdf_eval_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr), C.c_void_p(wi_ptr),
+                                          C.c_void_p(front_ptr), C.c_void_p(f_ptr), C.c_void_p(pdf_ptr),
+                                          _stream(stream)), self.ctx)
+
+    def bsdf_sample_device(self, material: int, n: int, wo_ptr: int, u_ptr: int, front_ptr: int, out_ptr: int,
+                           stream=None):
+        """`tpt_bsdf_sample_device`: OpenPBR samples (weight, wi, pdf, flags) for n (wo, u)."""
+        _check(lib().tpt_bsdf_sample_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr), C.c_void_p(u_ptr),
+                                            C.c_void_p(front_ptr), C.c_void_p(out_ptr), _stream(stream)), self.ctx)
 
     def device_bytes(self) -> int:
         v = C.c_uint64()
