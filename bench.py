@@ -185,24 +185,41 @@ def profiled_traffic():
     return float(m.group(1)) if m else None
 
 
-RENDER_CFG = {"scene": "cornell_box(seed=1), NormalizedLambert twin of the OpenPBR diffuse walls",
-              "width": 256, "height": 256, "spp": 64, "max_depth": 8, "triangles": 36}
+RENDER_CFG = {"width": 256, "height": 256, "spp": 64, "max_depth": 8, "triangles": 36}
+RENDER_SCENES = {
+    # the Cornell box of the plain-MIS configuration: OpenPBR walls and boxes
+    # (base_color U[0.1, 0.8], diffuse and specular roughness 1), emissive quad
+    "cornell_openpbr": "cornell_box(seed=1): OpenPBR diffuse walls/boxes, 0.25^2 light of radiance 15",
+    # the same box with NormalizedLambert walls: exercises light-tree NEE
+    "cornell_lambert": "cornell_box(seed=1) with NormalizedLambert walls/boxes (rho = the OpenPBR base_color)",
+}
 
 
 def render_block(ctx, steps, warmup, cpu=True):
-    """Cornell box 256x256, 64 spp, depth 8: wavefront vs megakernel Msamples/s
-    (identical images by construction, so equal RMSE), and the oracle on the host."""
+    """Both Cornell boxes at 256x256, 64 spp, depth 8."""
+    import tpt_scenes
+
+    out = {"config": RENDER_CFG, "unit": "Msamples/s"}
+    for key, kind in (("cornell_openpbr", tpt_scenes.OPENPBR), ("cornell_lambert", tpt_scenes.LAMBERT)):
+        out[key] = render_scene_block(ctx, kind, steps, warmup, cpu)
+        out[key]["scene"] = RENDER_SCENES[key]
+    return out
+
+
+def render_scene_block(ctx, kind, steps, warmup, cpu=True):
+    """Wavefront vs megakernel Msamples/s (identical images by construction, so
+    equal RMSE), and the oracle on the host cores."""
     import torch
 
     import tpt
     import tpt_scenes
 
-    sc = tpt_scenes.cornell_box(1, tpt_scenes.LAMBERT)
+    sc = tpt_scenes.cornell_box(1, kind)
     scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
     W, H, spp, depth = RENDER_CFG["width"], RENDER_CFG["height"], RENDER_CFG["spp"], RENDER_CFG["max_depth"]
     stream = torch.cuda.current_stream()
     img = torch.empty(W * H * 3, device="cuda")
-    out = {"config": RENDER_CFG, "unit": "Msamples/s"}
+    out = {}
     for name, ex in (("wavefront", tpt.EXEC_WAVEFRONT), ("megakernel", tpt.EXEC_MEGAKERNEL)):
         job = scene.job(sc["camera"], W, H, spp, depth, execution=ex)
         for _ in range(warmup):
