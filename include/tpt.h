@@ -261,7 +261,13 @@ tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, c
 /* Rendering (`IntegratorKind::trace_radiance` per sample, main.rs:99-126 loop) */
 
 typedef enum tpt_integrator {
-  TPT_INTEGRATOR_MIS = 0 /* integrator/mis.rs: BSDF sampling + light-tree NEE, balance heuristic */
+  TPT_INTEGRATOR_MIS = 0, /* integrator/mis.rs: BSDF sampling + light-tree NEE, balance heuristic */
+  /* integrator/bdpt.rs: camera and light subpaths, every connection between
+   * them, balance-heuristic MIS over the strategies (area lights picked by
+   * power).  Runs as one thread per sample whatever `execution` says; the
+   * device keeps both subpaths on chip, so max_depth is limited to 16
+   * (TPT_ERR_CAPACITY above). */
+  TPT_INTEGRATOR_BDPT = 1
 } tpt_integrator;
 
 /* PinholeCamera::new(eye, look_at, up, fov_y, exposure) (scene/camera.rs:21-39). */
@@ -326,18 +332,19 @@ tpt_status tpt_lut_dielectric_albedo(tpt_context* ctx, float eta, float* out);
 tpt_status tpt_lut_conductor_ec(tpt_context* ctx, float* e, float* e_avg);
 tpt_status tpt_lut_dielectric_ec(tpt_context* ctx, float* e, float* e_avg);
 
-/* OpenPbrBsdf::eval (radiance transport) and ::pdf of material `material` of an
- * uploaded scene, for n direction pairs in the shading frame (device buffers:
- * wo, wi n x 3; front_face n; f n x 3; pdf n).  The material must be OpenPBR. */
+/* OpenPbrBsdf::eval and ::pdf of material `material` of an uploaded scene, for
+ * n direction pairs in the shading frame (device buffers: wo, wi n x 3;
+ * front_face n; f n x 3; pdf n).  mode: 0 radiance, 1 importance transport
+ * (TransportMode).  The material must be OpenPBR. */
 tpt_status tpt_bsdf_eval_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
-                                const float* wo, const float* wi, const uint32_t* front_face, float* f, float* pdf,
-                                void* stream);
+                                const float* wo, const float* wi, const uint32_t* front_face, uint32_t mode, float* f,
+                                float* pdf, void* stream);
 /* OpenPbrBsdf::sample for n (wo, u) pairs: u n x 3 = (u_lobe, u_dir.x, u_dir.y);
- * out n x 8 = weight (3), wi (3), pdf, flags (as uint32 bits: 1 reflection,
- * 4 diffuse, 8 glossy, 16 delta; 0 = no sample). */
+ * out n x 9 = weight (3), wi (3), pdf, pdf_rev, flags (as uint32 bits:
+ * 1 reflection, 4 diffuse, 8 glossy, 16 delta; 0 = no sample). */
 tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
-                                  const float* wo, const float* u, const uint32_t* front_face, float* out,
-                                  void* stream);
+                                  const float* wo, const float* u, const uint32_t* front_face, uint32_t mode,
+                                  float* out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -83,8 +83,8 @@ def _declare(L):
         "orc_render_scene_free": (None, [vp]),
         "orc_render_scene_set_materials": (None, [vp, vp, vp, vp, vp, u32]),
         "orc_render_scene_set_light_tree": (None, [vp, vp, u64, u32]),
-        "orc_render_pixels": (None, [vp, vp, u32, u32, u32, u32, u32, u32, vp, i32]),
-        "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u64, u64, vp, i32]),
+        "orc_render_pixels": (None, [vp, vp, u32, u32, u32, u32, u32, u32, u32, vp, i32]),
+        "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u32, u64, u64, vp, i32]),
         "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
         "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, vp]),
         "orc_render_emitted": (None, [vp, i32, i32, vp, vp, i32, i32, vp, vp, vp, f32, i32, vp]),
@@ -273,19 +273,20 @@ class RenderScene:
         return np.array([*camera["eye"], *camera["look_at"], *camera["up"], camera["fov_y"],
                          camera.get("exposure", 1.0)], np.float32)
 
-    def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None):
-        """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3]."""
+    def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0):
+        """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3].
+        integrator: 0 MIS (integrator/mis.rs), 1 BDPT (integrator/bdpt.rs)."""
         p0, p1 = pixels if pixels is not None else (0, width * height)
         out = np.empty((p1 - p0, 3), np.float32)
         cam = self._cam(camera)
-        lib().orc_render_pixels(self.h, _p(cam), width, height, spp, max_depth, p0, p1, _p(out),
+        lib().orc_render_pixels(self.h, _p(cam), width, height, spp, max_depth, integrator, p0, p1, _p(out),
                                 nthreads or os.cpu_count() or 1)
         return out
 
-    def samples(self, camera, width, height, spp, max_depth, first, count, nthreads=None):
+    def samples(self, camera, width, height, spp, max_depth, first, count, nthreads=None, integrator=0):
         out = np.empty((count, 3), np.float32)
         cam = self._cam(camera)
-        lib().orc_render_samples(self.h, _p(cam), width, height, spp, max_depth, first, count, _p(out),
+        lib().orc_render_samples(self.h, _p(cam), width, height, spp, max_depth, integrator, first, count, _p(out),
                                  nthreads or os.cpu_count() or 1)
         return out
 

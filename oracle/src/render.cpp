@@ -397,6 +397,26 @@ void RenderScene::finalize() {
   for (uint32_t k = 0; k < tree.size(); ++k)
     if (tree[k].leaf_instance != kNoNode && !leaf_of[tree[k].leaf_instance].empty())
       leaf_of[tree[k].leaf_instance][tree[k].leaf_triangle] = k;
+  // Scene::register_area_light_triangles (scene/mod.rs:649-684), per instance in order
+  area_lights.clear();
+  area_light_weight_sum = 0.0f;
+  for (size_t i = 0; i < geo.instances.size(); ++i) {
+    const Material& m = materials[geo.instances[i].material_index];
+    if (m.kind != kEmissive) continue;  // may_emit
+    Vec3 e = m.color * m.strength;
+    float max_emission = fmax_num(fmax_num(fmax_num(e.x, e.y), e.z), 0.0f);
+    if (max_emission <= 0.0f) continue;
+    int ntri = (int)geo.meshes[geo.instances[i].mesh_index].triangle_count();
+    for (int t = 0; t < ntri; ++t) {
+      Vec3 p[3];
+      triangle_world((int)i, t, p);
+      float area = 0.5f * length(cross(p[1] - p[0], p[2] - p[0]));
+      float weight = area * max_emission;
+      if (weight <= 0.0f) continue;
+      area_light_weight_sum += weight;
+      area_lights.push_back(AreaLight{(int32_t)i, t, area, weight, area_light_weight_sum});
+    }
+  }
   float w = tree.empty() ? 0.0f : fmax_num(tree[root].flux, 0.0f);
   has_tree = w > 0.0f;
   float total = 0.0f + w;
@@ -494,7 +514,7 @@ Vec3 one_sample(const RenderScene& s, const RenderJob& job, uint32_t pixel, uint
   PathSampler ps(px, py, sample, job.spp, job.width, job.height);
   Vec2 us = ps.camera_sample();
   Ray r = job.cam.generate_ray_differential(job.width, job.height, px, py, us, job.spp);
-  return trace_mis(s, r, ps, job.max_depth);
+  return job.integrator == 1 ? trace_bdpt(s, r, ps, job.max_depth) : trace_mis(s, r, ps, job.max_depth);
 }
 }  // namespace
 

@@ -63,9 +63,18 @@ struct Vertex {
   bool front_face;
 };
 
+// scene/mod.rs:48-54: an emissive triangle with its selection weight
+// (area * max_emission) and the running prefix of the weights.
+struct AreaLight {
+  int32_t inst, tri;
+  float area, weight, prefix_weight;
+};
+
 struct RenderScene {
   Geometry geo;
   std::vector<Material> materials;
+  std::vector<AreaLight> area_lights;  // Scene::area_light_triangles, instance order
+  float area_light_weight_sum = 0.0f;
   std::vector<LightNode> tree;
   uint32_t root = kNoNode;
   // (instance, triangle) -> leaf node, replacing the reference's HashMap
@@ -82,10 +91,27 @@ struct RenderScene {
 struct RenderJob {
   Camera cam;
   uint32_t width, height, spp, max_depth;
+  uint32_t integrator = 0;  // 0 MIS, 1 BDPT
 };
+
+// Material interface (material/mod.rs:251-502) for the kinds in scope, with
+// the transport mode (material.rs modified_bsdf_eval / _sample_weight).
+struct MatSampleOut {
+  Vec3 weight, wi;
+  float pdf = 0, pdf_rev = 0;
+  bool delta = false;
+};
+Vec3 material_eval(const Material& m, const Vertex& v, Vec3 wi, TransportMode mode);
+float material_pdf(const Material& m, const Vertex& v, Vec3 wi);
+bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& r, TransportMode mode,
+                     MatSampleOut* s);
+bool material_le(const Material& m, Vec3* le);  // Emissive only (two-sided)
+inline bool is_pure_emitter(const Material& m) { return m.kind == kEmissive; }
 
 // mis::trace_radiance for one sample
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
+// bdpt::trace_radiance for one sample (integrator/bdpt.rs:70-131)
+Vec3 trace_bdpt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
 
 // main.rs:99-126 for pixels [p0, p1): running mean over spp samples, times exposure.
 void render_pixels(const RenderScene& s, const RenderJob& job, uint32_t p0, uint32_t p1, float* out_rgb, int nthreads);

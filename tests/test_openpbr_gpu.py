@@ -81,11 +81,12 @@ def _assert_close(dev, ref, what):
     assert np.all((r <= 1e-3) | (np.abs(np.asarray(dev, np.float64) - ref) <= 1e-7)), (what, r.max())
 
 
+@pytest.mark.parametrize("mode", [0, 1], ids=["radiance", "importance"])
 @pytest.mark.parametrize("mi", range(len(MATERIALS)))
-def test_bsdf_eval_pdf_match_oracle(bsdf_scene, mi):
+def test_bsdf_eval_pdf_match_oracle(bsdf_scene, mi, mode):
     import torch
 
-    rng = np.random.default_rng(100 + mi)
+    rng = np.random.default_rng(100 + mi + 50 * mode)
     n = 2000
     wo = _dirs(rng, n)
     wi = _dirs(rng, n, below=0.1)
@@ -94,11 +95,11 @@ def test_bsdf_eval_pdf_match_oracle(bsdf_scene, mi):
     f = torch.empty((n, 3), dtype=torch.float32, device="cuda")
     pdf = torch.empty(n, dtype=torch.float32, device="cuda")
     bsdf_scene.bsdf_eval_device(mi, n, t["wo"].data_ptr(), t["wi"].data_ptr(), t["front"].data_ptr(), f.data_ptr(),
-                                pdf.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
+                                pdf.data_ptr(), stream=torch.cuda.current_stream().cuda_stream, mode=mode)
     torch.cuda.synchronize()
     f, pdf = f.cpu().numpy(), pdf.cpu().numpy()
     m = orc.OpenPbrMaterial(MATERIALS[mi])
-    rf = np.array([m.eval(wo[k], wi[k], front=bool(front[k])) for k in range(n)])
+    rf = np.array([m.eval(wo[k], wi[k], front=bool(front[k]), mode=mode) for k in range(n)])
     rp = np.array([m.pdf(wo[k], wi[k], front=bool(front[k])) for k in range(n)], np.float32)
     assert np.all(np.isfinite(f)) and np.all(np.isfinite(pdf))
     assert (rp > 0).mean() > 0.5 and (rf.max(1) > 0).mean() > 0.5
@@ -106,24 +107,25 @@ def test_bsdf_eval_pdf_match_oracle(bsdf_scene, mi):
     _assert_close(pdf, rp, "pdf")
 
 
+@pytest.mark.parametrize("mode", [0, 1], ids=["radiance", "importance"])
 @pytest.mark.parametrize("mi", range(len(MATERIALS)))
-def test_bsdf_sample_matches_oracle(bsdf_scene, mi):
+def test_bsdf_sample_matches_oracle(bsdf_scene, mi, mode):
     import torch
 
-    rng = np.random.default_rng(200 + mi)
+    rng = np.random.default_rng(200 + mi + 50 * mode)
     n = 2000
     wo = _dirs(rng, n)
     u = rng.random((n, 3)).astype(np.float32)
     front = (rng.random(n) < 0.7).astype(np.uint32)
     tw, tu, tf = (torch.from_numpy(a).cuda() for a in (wo, u, front.view(np.int32)))
-    out = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+    out = torch.empty((n, 9), dtype=torch.float32, device="cuda")
     bsdf_scene.bsdf_sample_device(mi, n, tw.data_ptr(), tu.data_ptr(), tf.data_ptr(), out.data_ptr(),
-                                  stream=torch.cuda.current_stream().cuda_stream)
+                                  stream=torch.cuda.current_stream().cuda_stream, mode=mode)
     torch.cuda.synchronize()
     out = out.cpu().numpy()
-    flags = out[:, 7].view(np.uint32)
+    flags = out[:, 8].view(np.uint32)
     m = orc.OpenPbrMaterial(MATERIALS[mi])
-    ref = [m.sample(wo[k], u[k, 0], u[k, 1:], front=bool(front[k])) for k in range(n)]
+    ref = [m.sample(wo[k], u[k, 0], u[k, 1:], front=bool(front[k]), mode=mode) for k in range(n)]
     rflags = np.array([0 if s is None else s["flags"] for s in ref], np.uint32)
     assert (flags == rflags).mean() >= 0.999
     both = np.nonzero((flags == rflags) & (rflags != 0))[0]
@@ -131,9 +133,11 @@ def test_bsdf_sample_matches_oracle(bsdf_scene, mi):
     rw = np.array([ref[k]["weight"] for k in both])
     rwi = np.array([ref[k]["wi"] for k in both])
     rpdf = np.array([ref[k]["pdf"] for k in both], np.float32)
+    rrev = np.array([ref[k]["pdf_rev"] for k in both], np.float32)
     _assert_close(out[both, 0:3], rw, "weight")
     _assert_close(out[both, 3:6], rwi, "wi")
     _assert_close(out[both, 6], rpdf, "pdf")
+    _assert_close(out[both, 7], rrev, "pdf_rev")
 
 
 @pytest.fixture(scope="module")

@@ -132,24 +132,26 @@ static tpt_status check_query(tpt_context* ctx, const tpt_scene* scene, uint32_t
 }
 
 tpt_status tpt_bsdf_eval_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
-                                const float* wo, const float* wi, const uint32_t* front_face, float* f, float* pdf,
-                                void* stream) {
+                                const float* wo, const float* wi, const uint32_t* front_face, uint32_t mode, float* f,
+                                float* pdf, void* stream) {
   tpt_status st = check_query(ctx, scene, material);
   if (st) return st;
   if (n && (!wo || !wi || !front_face || !f || !pdf)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
+  if (mode > 1) return set_error(ctx, TPT_ERR_INVALID_ARG, "mode must be 0 (radiance) or 1 (importance)");
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  return cuda_check(ctx, launch_bsdf_eval(scene->render, material, n, wo, wi, front_face, f, pdf, s),
+  return cuda_check(ctx, launch_bsdf_eval(scene->render, material, n, wo, wi, front_face, mode, f, pdf, s),
                     "bsdf eval launch");
 }
 
 tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
-                                  const float* wo, const float* u, const uint32_t* front_face, float* out,
-                                  void* stream) {
+                                  const float* wo, const float* u, const uint32_t* front_face, uint32_t mode,
+                                  float* out, void* stream) {
   tpt_status st = check_query(ctx, scene, material);
   if (st) return st;
   if (n && (!wo || !u || !front_face || !out)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
+  if (mode > 1) return set_error(ctx, TPT_ERR_INVALID_ARG, "mode must be 0 (radiance) or 1 (importance)");
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  return cuda_check(ctx, launch_bsdf_sample(scene->render, material, n, wo, u, front_face, out, s),
+  return cuda_check(ctx, launch_bsdf_sample(scene->render, material, n, wo, u, front_face, mode, out, s),
                     "bsdf sample launch");
 }
 

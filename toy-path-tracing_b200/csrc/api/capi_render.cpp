@@ -27,7 +27,12 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
   if (!job || !job->scene) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL job or scene");
   if (job->width == 0 || job->height == 0 || job->spp == 0)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "width, height and spp must be positive");
-  if (job->integrator != TPT_INTEGRATOR_MIS) return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown integrator");
+  if (job->integrator != TPT_INTEGRATOR_MIS && job->integrator != TPT_INTEGRATOR_BDPT)
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown integrator");
+  if (job->integrator == TPT_INTEGRATOR_BDPT && job->max_depth > kBdptMaxDepthApi)
+    return set_error(ctx, TPT_ERR_CAPACITY,
+                     "BDPT max_depth " + std::to_string(job->max_depth) + " above the device limit of " +
+                         std::to_string(kBdptMaxDepthApi));
   if (job->execution != TPT_EXEC_WAVEFRONT && job->execution != TPT_EXEC_MEGAKERNEL)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown execution mode");
   if (job->scene->render.num_materials == 0)
@@ -185,7 +190,7 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
   float* samples = (float*)ctx->d_scratch;
   for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
     const uint32_t n = std::min(cp, npix - p0);
-    if (job->execution == TPT_EXEC_MEGAKERNEL) {
+    if (job->execution == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
       cudaError_t e = launch_render(job->scene->geo, job->scene->render, L, samples, (uint64_t)p0 * L.spp,
                                     (uint64_t)n * L.spp, ctx->d_err, ctx->num_sms, s);
       if ((st = cuda_check(ctx, e, "render kernel launch"))) return st;
@@ -209,7 +214,7 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
   if (count && !out_samples) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  if (job->execution == TPT_EXEC_MEGAKERNEL)
+  if (job->execution == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT)
     return cuda_check(ctx,
                       launch_render(job->scene->geo, job->scene->render, L, out_samples, first, count, ctx->d_err,
                                     ctx->num_sms, s),

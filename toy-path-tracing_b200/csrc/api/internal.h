@@ -85,6 +85,9 @@ cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const
                           uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t stream);
 cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first_pixel, uint32_t n_pixels,
                               float exposure, float* image, cudaStream_t stream);
+// bdpt_kernels.cu (launch_render dispatches to it for TPT_INTEGRATOR_BDPT)
+cudaError_t launch_render_bdpt(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P, float* samples,
+                               uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t stream);
 
 // capi_render.cpp: validates a job and derives its launch parameters.
 tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* out);
@@ -109,9 +112,9 @@ cudaError_t launch_lut_conductor_e(const float* u, const float* cs, float* e, cu
 cudaError_t launch_lut_dielectric_e(const float* uc, const float* ux, const float* cs, float* e, cudaStream_t s);
 // openpbr_query.cu: batched BSDF queries of one material.
 cudaError_t launch_bsdf_eval(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo, const float* wi,
-                             const uint32_t* front, float* f, float* pdf, cudaStream_t s);
+                             const uint32_t* front, uint32_t mode, float* f, float* pdf, cudaStream_t s);
 cudaError_t launch_bsdf_sample(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo,
-                               const float* u, const uint32_t* front, float* out, cudaStream_t s);
+                               const float* u, const uint32_t* front, uint32_t mode, float* out, cudaStream_t s);
 
 // scene_render_upload.cpp: materials, shading arrays, light tree, emitter map.
 tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc);

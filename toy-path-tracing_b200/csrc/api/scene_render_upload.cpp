@@ -162,6 +162,21 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
     const uint32_t base = sinst[n.leaf_instance].leaf_base;
     if (base != kInvalidNode) emap[base + n.leaf_triangle] = k;
   }
+  // area-light registry (BDPT light subpaths) and its emitter-map index
+  std::vector<HostAreaLight> hal;
+  float al_sum = 0.0f;
+  {
+    HostSceneView view{hmesh.data(), desc->num_meshes, hinst.data(), desc->num_instances, hmats.data(),
+                       desc->num_materials};
+    if (desc->num_materials) register_area_lights(view, &hal, &al_sum);
+  }
+  std::vector<DevAreaLight> dal(hal.size());
+  std::vector<uint32_t> al_of(map_size, kInvalidNode);
+  for (size_t k = 0; k < hal.size(); ++k) {
+    dal[k] = DevAreaLight{hal[k].inst, hal[k].tri, hal[k].area, hal[k].weight, hal[k].prefix_weight, {0, 0, 0}};
+    const uint32_t base = sinst[hal[k].inst].leaf_base;
+    if (base != kInvalidNode) al_of[base + hal[k].tri] = (uint32_t)k;
+  }
   std::vector<DevLightNodeRec> lnodes(s->light_tree.nodes.size());
   if (!lnodes.empty()) std::memcpy(lnodes.data(), s->light_tree.nodes.data(), lnodes.size() * 64);
 
@@ -177,7 +192,11 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   if (!st) st = put(s, lnodes, &R.ltree);
   if (!st) st = put(s, emap, &R.emitter_leaf);
   if (!st) st = put(s, opbr, &R.openpbr);
+  if (!st) st = put(s, dal, &R.area_lights);
+  if (!st) st = put(s, al_of, &R.area_light_of);
   if (st) return st;
+  R.num_area_lights = (uint32_t)dal.size();
+  R.area_light_weight_sum = al_sum;
   R.cec_e = ctx->d_cec_e;
   R.dec_e = ctx->d_dec_e;
   R.ltree_root = s->light_tree.root;

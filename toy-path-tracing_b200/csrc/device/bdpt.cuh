@@ -1,0 +1,417 @@
+// Bidirectional path tracing on the device, integrator/bdpt.rs:70-791, for
+// area lights (the light type in scope): camera subpath, light subpath from an
+// emissive triangle picked by power, and every connection between their
+// connectible vertices with a visibility ray and the reference's MIS weight.
+// Both subpaths live in the thread's local memory (interleaved across the warp
+// by the hardware, so vertex k of every lane is one coalesced line).
+#pragma once
+#include "render.cuh"
+
+namespace tpt {
+
+constexpr uint32_t kBdptMaxDepth = kBdptMaxDepthApi;
+constexpr float kShadowTolerance = 1.0e-3f;
+
+// ---- material interface with transport modes (material/mod.rs:33-79) --------
+__device__ __forceinline__ V3 modified_eval(const Vertex& v, V3 wi, V3 f, bool importance) {
+  if (length_sq(f) == 0.0f) return V3{0.0f, 0.0f, 0.0f};
+  const V3 dir = importance ? v.wo : wi;
+  const float cos_geom = fabsf(dot(dir, v.ng));
+  if (cos_geom <= kGeomCosEps) return V3{0.0f, 0.0f, 0.0f};
+  return f * (fabsf(dot(dir, v.ns)) / cos_geom);
+}
+__device__ __forceinline__ V3 modified_weight(const Vertex& v, V3 wi, V3 w, bool delta, bool importance) {
+  if (!importance || delta || length_sq(w) == 0.0f) return w;
+  const float cos_wo_geom = fabsf(dot(v.wo, v.ng)), cos_wo_sh = fabsf(dot(v.wo, v.ns));
+  const float cos_wi_geom = fabsf(dot(wi, v.ng)), cos_wi_sh = fabsf(dot(wi, v.ns));
+  if (cos_wo_geom <= kGeomCosEps || cos_wi_sh <= kGeomCosEps) return V3{0.0f, 0.0f, 0.0f};
+  return w * (cos_wo_sh / cos_wo_geom) * (cos_wi_geom / cos_wi_sh);
+}
+__device__ __forceinline__ float lambert_bsdf_pdf(V3 wo, V3 wi) {
+  if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
+  return fmaxf(wi.z, 0.0f) / kPiF;
+}
+
+// Material::eval (NormalizedLambert, OpenPbr; zero for the pure emitter)
+static __device__ __noinline__ V3 material_eval(const DevRender& S, const DevMaterialRec& m, const Vertex& v, V3 wi,
+                                               bool importance) {
+  if (m.kind == kDevLambert) {
+    if (dot(v.wo, v.ng) <= 0.0f || dot(wi, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
+    V3 f = V3{0.0f, 0.0f, 0.0f};
+    if (!(wo_l.z <= 0.0f || wi_l.z <= 0.0f)) f = V3{m.rho[0], m.rho[1], m.rho[2]} / kPiF;
+    return modified_eval(v, wi, f, importance);
+  }
+  if (m.kind == kDevOpenPbr) {
+    if (dot(v.wo, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
+    if (wo_l.z <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const DevOpenPbr* mp = S.d.openpbr + m.openpbr;
+    opbr::OpbrVertex s;
+    opbr::init_vertex(s, mp, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    V3 f;
+    float pdf;
+    if (importance) {
+      opbr::OpbrVertex lay;
+      opbr::init_vertex(lay, mp, S.d.cec_e, S.d.dec_e, wi_l, v.front, fabsf(wo_l.z));
+      opbr::eval_pdf(s, lay, wi_l, f, pdf);
+    } else {
+      opbr::eval_pdf(s, s, wi_l, f, pdf);
+    }
+    return modified_eval(v, wi, f, importance);
+  }
+  return V3{0.0f, 0.0f, 0.0f};
+}
+
+// Material::pdf
+static __device__ __noinline__ float material_pdf(const DevRender& S, const DevMaterialRec& m, const Vertex& v, V3 wi) {
+  if (m.kind == kDevLambert) {
+    if (dot(v.wo, v.ng) <= 0.0f || dot(wi, v.ng) <= 0.0f) return 0.0f;
+    return lambert_bsdf_pdf(normalize_or_zero(to_local(v.frame, v.wo)), normalize_or_zero(to_local(v.frame, wi)));
+  }
+  if (m.kind == kDevOpenPbr) {
+    if (dot(v.wo, v.ng) <= 0.0f) return 0.0f;
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
+    if (wo_l.z <= 0.0f) return 0.0f;
+    opbr::OpbrVertex s;
+    opbr::init_vertex(s, S.d.openpbr + m.openpbr, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    V3 f;
+    float pdf;
+    opbr::eval_pdf(s, s, wi_l, f, pdf);
+    return pdf;
+  }
+  return 0.0f;
+}
+
+struct MatSample {
+  V3 weight, wi;
+  float pdf, pdf_rev;
+  bool delta;
+};
+
+// Material::sample with pdf_rev
+static __device__ __noinline__ bool material_sample_rev(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
+                                                       float u_lobe, float u0, float u1, bool importance,
+                                                       MatSample& s) {
+  if (m.kind == kDevLambert) {
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    if (wo_l.z <= 0.0f) return false;
+    const V3 wi_l = opbr::sample_cosine_hemisphere(u0, u1);
+    const float pdf = lambert_bsdf_pdf(wo_l, wi_l);
+    if (pdf <= 0.0f) return false;
+    const V3 wi = to_world(v.frame, wi_l);
+    s.weight = modified_weight(v, wi, V3{m.rho[0], m.rho[1], m.rho[2]}, false, importance);
+    s.wi = wi;
+    s.pdf = pdf;
+    s.pdf_rev = lambert_bsdf_pdf(wi_l, wo_l);
+    s.delta = false;
+    return dot(wi, v.ng) > kGeomCosEps;
+  }
+  if (m.kind == kDevOpenPbr) {
+    if (dot(v.wo, v.ng) <= 0.0f) return false;
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    if (wo_l.z <= 0.0f) return false;
+    opbr::OpbrVertex ov;
+    opbr::init_vertex(ov, S.d.openpbr + m.openpbr, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    opbr::Sample bs;
+    if (!opbr::sample(ov, u_lobe, u0, u1, bs, importance, true)) return false;
+    const V3 wi = to_world(v.frame, bs.wi);
+    if (dot(wi, v.ng) <= kGeomCosEps) return false;
+    s.delta = (bs.flags & opbr::kFlagDelta) != 0;
+    s.weight = modified_weight(v, wi, bs.weight, s.delta, importance);
+    s.wi = wi;
+    s.pdf = bs.pdf;
+    s.pdf_rev = bs.pdf_rev;
+    return true;
+  }
+  return false;  // pure emitter
+}
+
+// ---- path vertices ---------------------------------------------------------
+constexpr uint32_t kBdLight = 1u, kBdDelta = 2u, kBdConnectible = 4u;
+
+struct BdVertex {
+  Vertex v;
+  V3 beta;
+  float pdf_fwd, pdf_rev;
+  uint32_t flags;
+};
+
+__device__ __forceinline__ float remap0(float x) { return x == 0.0f ? 1.0f : x; }
+
+// bdpt.rs:626-642
+__device__ __forceinline__ float solid_angle_to_area(float pdf, V3 from, V3 to, V3 to_ng) {
+  if (pdf <= 0.0f) return 0.0f;
+  const V3 d = to - from;
+  const float dist2 = length_sq(d);
+  if (dist2 <= 0.0f) return 0.0f;
+  const V3 wi = normalize_or_zero(d);
+  const float cos_to = fabsf(dot(to_ng, -wi));
+  if (cos_to <= 0.0f) return 0.0f;
+  return pdf * cos_to / dist2;
+}
+// bdpt.rs:644-659 through the emitter map instead of a linear search
+__device__ __forceinline__ float area_light_origin_pdf(const DevRender& S, const BdVertex& v) {
+  const uint32_t base = __ldg(&S.d.inst[v.v.inst].leaf_base);
+  if (base == 0xFFFFFFFFu) return 0.0f;
+  const uint32_t k = __ldg(S.d.area_light_of + base + v.v.tri);
+  if (k == 0xFFFFFFFFu) return 0.0f;
+  const float area = __ldg(&S.d.area_lights[k].area);
+  if (S.d.area_light_weight_sum <= 0.0f || area <= 0.0f) return 0.0f;
+  return __ldg(&S.d.area_lights[k].weight) / S.d.area_light_weight_sum / area;
+}
+// bdpt.rs:661-675
+__device__ __forceinline__ float light_emission_pdf(const BdVertex& light, const BdVertex& target) {
+  const V3 d = target.v.p - light.v.p;
+  const float dist2 = length_sq(d);
+  if (dist2 <= 0.0f) return 0.0f;
+  const V3 dir = d / sqrtf(dist2);
+  const float cos_emit = fmaxf(dot(light.v.ng, dir), 0.0f);
+  if (cos_emit <= 0.0f) return 0.0f;
+  return solid_angle_to_area(cos_emit / kPiF, light.v.p, target.v.p, target.v.ng);
+}
+// bdpt.rs:677-715
+__device__ __forceinline__ float vertex_pdf_area(const DevRender& S, const BdVertex& from, const BdVertex* prev,
+                                                 const BdVertex& target) {
+  if (from.flags & kBdLight) return light_emission_pdf(from, target);
+  const V3 d = target.v.p - from.v.p;
+  if (length_sq(d) <= 0.0f) return 0.0f;
+  Vertex v = from.v;
+  if (prev) {
+    const V3 tp = prev->v.p - from.v.p;
+    if (length_sq(tp) <= 0.0f) return 0.0f;
+    v.wo = normalize_or_zero(tp);
+  }
+  const V3 wi = normalize_or_zero(d);
+  const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[from.v.inst].material)];
+  return solid_angle_to_area(material_pdf(S, m, v, wi), from.v.p, target.v.p, target.v.ng);
+}
+
+// bdpt.rs:717-746
+__device__ __noinline__ float camera_light_hit_mis(const DevRender& S, const BdVertex* cp, uint32_t n) {
+  if (n <= 1) return 1.0f;
+  const uint32_t pt = n - 1, ptm = pt - 1;
+  const float pt_rev = area_light_origin_pdf(S, cp[pt]);
+  const float ptm_rev = light_emission_pdf(cp[pt], cp[ptm]);
+  float sum = 0.0f, ri = 1.0f;
+  for (uint32_t i = n - 1; i >= 1; --i) {
+    const float pr = i == pt ? pt_rev : (i == ptm ? ptm_rev : cp[i].pdf_rev);
+    ri *= remap0(pr) / remap0(cp[i].pdf_fwd);
+    if (!(cp[i].flags & kBdDelta) && !(cp[i - 1].flags & kBdDelta)) sum += ri;
+  }
+  return 1.0f / (1.0f + fmaxf(sum, 0.0f));
+}
+
+// bdpt.rs:748-817 for light_path[0..ns), camera_path[0..nt)
+static __device__ __noinline__ float bdpt_mis(const DevRender& S, const BdVertex* lp, uint32_t ns, const BdVertex* cp,
+                                              uint32_t nt) {
+  if (ns + nt <= 2) return 1.0f;
+  const uint32_t qs = ns - 1, pt = nt - 1;
+  const BdVertex* qsm = qs >= 1 ? &lp[qs - 1] : nullptr;
+  const BdVertex* ptm = pt >= 1 ? &cp[pt - 1] : nullptr;
+  const float pt_rev = vertex_pdf_area(S, lp[qs], qsm, cp[pt]);
+  const float ptm_rev = ptm ? vertex_pdf_area(S, cp[pt], &lp[qs], *ptm) : 0.0f;
+  const float qs_rev = vertex_pdf_area(S, cp[pt], ptm, lp[qs]);
+  const float qsm_rev = qsm ? vertex_pdf_area(S, lp[qs], &cp[pt], *qsm) : 0.0f;
+  float sum = 0.0f, ri = 1.0f;
+  for (uint32_t i = nt - 1; i >= 1; --i) {
+    const float pr = i == pt ? pt_rev : ((pt >= 1 && i == pt - 1) ? ptm_rev : cp[i].pdf_rev);
+    ri *= remap0(pr) / remap0(cp[i].pdf_fwd);
+    if (!(cp[i].flags & kBdDelta) && !(cp[i - 1].flags & kBdDelta)) sum += ri;
+  }
+  ri = 1.0f;
+  for (uint32_t k = ns; k-- > 0;) {
+    const float pr = k == qs ? qs_rev : ((qs >= 1 && k == qs - 1) ? qsm_rev : lp[k].pdf_rev);
+    ri *= remap0(pr) / remap0(lp[k].pdf_fwd);
+    const bool prev_delta = k > 0 && (lp[k - 1].flags & kBdDelta);
+    if (!(lp[k].flags & kBdDelta) && !prev_delta) sum += ri;
+  }
+  return 1.0f / (1.0f + fmaxf(sum, 0.0f));
+}
+
+// connect_vertices (bdpt.rs:488-538) with visible_between (577-602)
+template <class Stack>
+__device__ __forceinline__ V3 bdpt_connect(const DevRender& S, Stack& st, const BdVertex& lv, const BdVertex& cv,
+                                           uint32_t* err) {
+  const V3 zero = V3{0.0f, 0.0f, 0.0f};
+  const V3 delta = cv.v.p - lv.v.p;
+  const float dist2 = length_sq(delta);
+  if (dist2 <= 0.0f) return zero;
+  const float dist = sqrtf(dist2);
+  const V3 w_lc = delta / dist;
+  const V3 w_cl = -w_lc;
+  TraceResult h;
+  if (closest_hit(S, st, offset_origin(lv.v.p, lv.v.ng, w_lc), w_lc, h, err)) {
+    const bool target = (uint32_t)h.inst == cv.v.inst && (uint32_t)h.tri == cv.v.tri;
+    if (!target && !(h.t >= dist * (1.0f - kShadowTolerance))) return zero;
+  }
+  const DevMaterialRec cm = S.d.mats[__ldg(&S.d.inst[cv.v.inst].material)];
+  const V3 f_cam = material_eval(S, cm, cv.v, w_cl, false);
+  if (length_sq(f_cam) == 0.0f) return zero;
+  V3 f_light;
+  if (lv.flags & kBdLight) {
+    if (dot(lv.v.ng, w_lc) <= 0.0f) return zero;
+    f_light = V3{1.0f, 1.0f, 1.0f};
+  } else {
+    const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[lv.v.inst].material)];
+    f_light = material_eval(S, lm, lv.v, w_lc, true);
+  }
+  if (length_sq(f_light) == 0.0f) return zero;
+  const float g = fabsf(dot(lv.v.ng, w_lc)) * fabsf(dot(cv.v.ng, w_cl)) / dist2;
+  if (g <= 0.0f) return zero;
+  return lv.beta * f_light * g * f_cam * cv.beta;
+}
+
+// bdpt.rs:135-262 (no environment or non-area lights in scope)
+template <class Stack>
+__device__ __noinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& st, const RenderLaunch& P,
+                                                     const PathSamplerDev& ps, V3 ro, V3 rd, BdVertex* vs, V3& L,
+                                                     uint32_t* err) {
+  uint32_t n = 0;
+  V3 beta = V3{1.0f, 1.0f, 1.0f};
+  bool count_emission = true, have_pending = false;
+  V3 pending_from = V3{0.0f, 0.0f, 0.0f};
+  float pending_pdf = 0.0f;
+  for (uint32_t depth = 0; depth < P.max_depth; ++depth) {
+    TraceResult h;
+    if (!closest_hit(S, st, ro, rd, h, err)) break;
+    const Vertex v = shade_hit<Stack>(S, h, rd);
+    const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
+    BdVertex& pv = vs[n];
+    pv.v = v;
+    pv.beta = beta;
+    pv.pdf_fwd = have_pending ? solid_angle_to_area(pending_pdf, pending_from, v.p, v.ng) : 0.0f;
+    pv.pdf_rev = 0.0f;
+    pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
+    ++n;
+    if (m.kind == kDevEmissive) {
+      const float w = count_emission ? 1.0f : camera_light_hit_mis(S, vs, n);
+      L = L + beta * emissive_le(m) * w;
+      break;  // pure emitter: sample() is None
+    }
+    float ud0, ud1;
+    ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
+    const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
+    MatSample s;
+    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, false, s)) break;
+    pv.flags = s.delta ? kBdDelta : kBdConnectible;
+    if (n >= 2) vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
+    ro = offset_origin(v.p, v.ng, s.wi);
+    rd = s.wi;
+    beta = beta * s.weight;
+    if (depth + 1 >= 4) {
+      const float q = clampf(max_element(beta), 0.05f, 1.0f);
+      if (ps.sample_1d(vertex_dim(depth, kOffRr)) > q) break;
+      beta = beta / q;
+    }
+    have_pending = true;
+    pending_from = v.p;
+    pending_pdf = s.pdf;
+    count_emission = s.delta;
+  }
+  return n;
+}
+
+// bdpt.rs:264-385
+template <class Stack>
+__device__ __noinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& st, const RenderLaunch& P,
+                                                    const PathSamplerDev& ps, BdVertex* vs, uint32_t* err) {
+  if (P.max_depth == 0 || S.d.num_area_lights == 0 || S.d.area_light_weight_sum <= 0.0f) return 0;
+  // sample_area_light_triangle (bdpt.rs:540-553): first prefix >= u * sum
+  const float target = clampf(ps.sample_1d(vertex_dim(0, kOffCategory)), 0.0f, 1.0f) * S.d.area_light_weight_sum;
+  uint32_t lo = 0, hi = S.d.num_area_lights;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(&S.d.area_lights[mid].prefix_weight) < target) lo = mid + 1;
+    else hi = mid;
+  }
+  const uint32_t k = min(lo, S.d.num_area_lights - 1);
+  const DevAreaLight al = S.d.area_lights[k];
+  const float pmf = al.weight / S.d.area_light_weight_sum;
+  TriData T;
+  fetch_triangle(S, al.inst, al.tri, T, true);
+  float us0, us1;
+  ps.sample_2d(vertex_dim(0, kOffSurface), us0, us1);
+  const float su0 = sqrtf(clampf(us0, 0.0f, 1.0f));
+  const float u1 = clampf(us1, 0.0f, 1.0f);
+  const float b0 = 1.0f - su0, b1 = u1 * su0, b2 = (1.0f - u1) * su0;
+  const float area = 0.5f * length(cross(T.p[1] - T.p[0], T.p[2] - T.p[0]));
+  const float pdf_point = area > 0.0f ? 1.0f / area : 0.0f;
+  const float pdf_area = pmf * pdf_point;
+  if (pdf_area <= 0.0f) return 0;
+  const V3 gn = normalize_or_zero(cross(T.p[1] - T.p[0], T.p[2] - T.p[0]));
+  const Frame fr = frame_from_normal(gn);
+  float ud0, ud1;
+  ps.sample_2d(vertex_dim(0, kOffDir), ud0, ud1);
+  const V3 ld = opbr::sample_cosine_hemisphere(ud0, ud1);
+  const V3 emit = normalize_or_zero(to_world(fr, ld));
+  const float pdf_dir = fmaxf(ld.z, 0.0f) / kPiF;
+  if (length_sq(emit) == 0.0f || pdf_dir <= 0.0f) return 0;
+  Vertex lvx = make_vertex(T, al.inst, al.tri, b0, b1, b2, -emit);
+  lvx.wo = emit;
+  const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[al.inst].material)];
+  if (lm.kind != kDevEmissive) return 0;  // le() is None
+  const float cos_emit = fmaxf(dot(lvx.ng, emit), 0.0f);
+  if (cos_emit <= 0.0f) return 0;
+  const V3 endpoint_beta = emissive_le(lm) / pdf_area;
+  uint32_t n = 0;
+  vs[0].v = lvx;
+  vs[0].beta = endpoint_beta;
+  vs[0].pdf_fwd = pdf_area;
+  vs[0].pdf_rev = 0.0f;
+  vs[0].flags = kBdLight | kBdConnectible;
+  n = 1;
+  V3 ro = offset_origin(lvx.p, lvx.ng, emit), rd = emit;
+  V3 beta = endpoint_beta * (cos_emit / pdf_dir);
+  V3 pending_from = lvx.p;
+  float pending_pdf = pdf_dir;
+  for (uint32_t depth = 1; depth < P.max_depth; ++depth) {
+    TraceResult h;
+    if (!closest_hit(S, st, ro, rd, h, err)) break;
+    const Vertex v = shade_hit<Stack>(S, h, rd);
+    const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
+    BdVertex& pv = vs[n];
+    pv.v = v;
+    pv.beta = beta;
+    pv.pdf_fwd = solid_angle_to_area(pending_pdf, pending_from, v.p, v.ng);
+    pv.pdf_rev = 0.0f;
+    pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
+    ++n;
+    if (m.kind == kDevEmissive) break;
+    float ud0, ud1;
+    ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
+    const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
+    MatSample s;
+    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, true, s)) break;
+    pv.flags = s.delta ? kBdDelta : kBdConnectible;
+    vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
+    ro = offset_origin(v.p, v.ng, s.wi);
+    rd = s.wi;
+    beta = beta * s.weight;
+    pending_from = v.p;
+    pending_pdf = s.pdf;
+  }
+  return n;
+}
+
+// bdpt::trace_radiance for one sample (bdpt.rs:70-131)
+template <class Stack>
+__device__ V3 trace_bdpt(const DevRender& S, Stack& st, const RenderLaunch& P, const PathSamplerDev& ps, V3 ro, V3 rd,
+                         uint32_t* err) {
+  BdVertex cam[kBdptMaxDepth], lig[kBdptMaxDepth];
+  V3 L = V3{0.0f, 0.0f, 0.0f};
+  const uint32_t nc = bdpt_camera_subpath(S, st, P, ps, ro, rd, cam, L, err);
+  const uint32_t nl = bdpt_light_subpath(S, st, P, ps, lig, err);
+  for (uint32_t li = 0; li < nl; ++li)
+    for (uint32_t ci = 0; ci < nc; ++ci) {
+      if (!(lig[li].flags & kBdConnectible) || !(cam[ci].flags & kBdConnectible)) continue;
+      const float w = bdpt_mis(S, lig, li + 1, cam, ci + 1);
+      L = L + w * bdpt_connect(S, st, lig[li], cam[ci], err);
+    }
+  return L;
+}
+
+}  // namespace tpt

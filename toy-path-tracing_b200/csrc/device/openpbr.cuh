@@ -381,6 +381,7 @@ struct OpbrVertex {
   const float* dec_e;
   V3 wo;
   uint32_t face;       // 0 front, 1 back
+  float dk_cos;        // |wo.z| of the vertex the BSDF was built for
   float below_fuzz_s;  // max(1 - fuzz * E_fuzz, 0)
   float e_coat;        // coat albedo (with multiple scattering)
   float e_spec;        // specular albedo (with multiple scattering)
@@ -420,19 +421,23 @@ __device__ __forceinline__ float albedo_with_ms(const OpbrVertex& s, int lobe, b
 }
 
 // Builds the per-vertex state (make_bsdf's view-dependent part, the albedos,
-// layer weights without wi and the lobe probabilities).
-static __device__ __noinline__ void init_vertex(OpbrVertex& s, const DevOpenPbr* mp, const float* cec_e, const float* dec_e,
-                                         V3 wo, bool front_face) {
+// layer weights without wi and the lobe probabilities) for outgoing direction
+// `wo`.  `dk_cos` is |wo.z| of the shading vertex the BSDF was built for (the
+// coat darkening reads it); it differs from |wo.z| only when the state is
+// evaluated at another direction of the same BSDF (pdf_rev, importance layers).
+static __device__ __noinline__ void init_vertex(OpbrVertex& s, const DevOpenPbr* mp, const float* cec_e,
+                                                const float* dec_e, V3 wo, bool front_face, float dk_cos) {
   const DevOpenPbr& m = *mp;
   s.m = mp;
   s.cec_e = cec_e;
   s.dec_e = dec_e;
   s.wo = wo;
   s.face = front_face ? 0u : 1u;
+  s.dk_cos = dk_cos;
   // coat_darkening_factor's view term (material/open_pbr.rs:836-857)
   s.darkening = V3{1.0f, 1.0f, 1.0f};
   if (m.flags & kOpbrDarkening) {
-    const float ks = fresnel_dielectric(clampf(fabsf(wo.z), 0.0f, 1.0f), 1.0f, m.dk_eta);
+    const float ks = fresnel_dielectric(clampf(dk_cos, 0.0f, 1.0f), 1.0f, m.dk_eta);
     const float k = clampf(ks + (m.dk_kr - ks) * m.dk_rb, 0.0f, 1.0f);
     const V3 cc = ld3(m.coat_color);
     const V3 denom = vmaxv(V3{1.0f, 1.0f, 1.0f} - ld3(m.dk_e_base) * (k * cc), splat(1.0e-4f));
@@ -487,8 +492,20 @@ __device__ __forceinline__ float refl_ms(const OpbrVertex& s, int lobe, float wi
   return f.ms_factor * (1.0f - s.dec_eo[lobe]) * (1.0f - e_i) / (kPiF * f.one_minus_e_avg_o);
 }
 
-// OpenPbrBsdf::eval (radiance transport) and ::pdf for one direction pair.
-static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, V3 wi, V3& f_out, float& pdf_out) {
+// coat_absorb_tint (open_pbr.rs:453-464) for a (layer wo, wi) pair, wi.z > 0
+__device__ __forceinline__ V3 coat_tint(const DevOpenPbr& m, V3 wo, V3 wi) {
+  if (wo.z <= 0.0f || wi.z <= 0.0f) return V3{1.0f, 1.0f, 1.0f};
+  const float mu_o = refracted_cos(wo.z, m.coat_eta), mu_i = refracted_cos(wi.z, m.coat_eta);
+  const float e = 0.5f * (1.0f / fmaxf(mu_i, 1.0e-4f) + 1.0f / fmaxf(mu_o, 1.0e-4f));
+  return V3{powf(fmaxf(m.coat_color[0], 0.0f), e), powf(fmaxf(m.coat_color[1], 0.0f), e),
+            powf(fmaxf(m.coat_color[2], 0.0f), e)};
+}
+
+// OpenPbrBsdf::eval and ::pdf for one direction pair.  `lay` is the state of
+// the direction the layer weights are taken at: the vertex itself in radiance
+// transport, wi in importance transport (open_pbr.rs:228-233).
+static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVertex& lay, V3 wi, V3& f_out,
+                                             float& pdf_out) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
   V3 total = V3{0.0f, 0.0f, 0.0f};
@@ -500,15 +517,9 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, V3 wi, V3& f_o
   V3 wm;
   const bool has_wm = half_vector(wo, wi, wm);
   // layer weights with this wi (the coat tint depends on it)
-  V3 tint = V3{1.0f, 1.0f, 1.0f};
-  if (m.coat > 0.0f) {
-    const float mu_o = refracted_cos(wo.z, m.coat_eta), mu_i = refracted_cos(wi.z, m.coat_eta);
-    const float e = 0.5f * (1.0f / fmaxf(mu_i, 1.0e-4f) + 1.0f / fmaxf(mu_o, 1.0e-4f));
-    tint = V3{powf(fmaxf(m.coat_color[0], 0.0f), e), powf(fmaxf(m.coat_color[1], 0.0f), e),
-              powf(fmaxf(m.coat_color[2], 0.0f), e)};
-  }
-  const Below b = weights_below(s, tint);
-  const float coat_w = m.coat * s.below_fuzz_s;
+  const V3 tint = m.coat > 0.0f ? coat_tint(m, lay.wo, wi) : V3{1.0f, 1.0f, 1.0f};
+  const Below b = weights_below(lay, tint);
+  const float coat_w = m.coat * lay.below_fuzz_s;
   const float inv4 = 4.0f * wo.z * wi.z;
   // specular GGX terms shared by the metal and dielectric lobes
   const bool need_spec = (m.flags & (kOpbrMetalRough | kOpbrSpecRough)) != 0;
@@ -586,13 +597,19 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, V3 wi, V3& f_o
 struct Sample {
   V3 weight, wi;
   float pdf;
+  float pdf_rev;  // pdf(wi -> wo), computed when requested (0 for delta samples)
   uint32_t flags;
 };
 
-__device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t flags, Sample& out) {
+// finalize_rough_sample_with_wavelength (open_pbr.rs:1997-2027).  `importance`
+// selects the transport mode of the evaluation; `want_rev` computes pdf_rev.
+__device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t flags, bool importance, bool want_rev,
+                                         Sample& out) {
   V3 f;
   float pdf;
-  eval_pdf(s, wi, f, pdf);
+  OpbrVertex at_wi;  // the same BSDF seen from wi
+  if (importance || want_rev) init_vertex(at_wi, s.m, s.cec_e, s.dec_e, wi, s.face == 0u, s.dk_cos);
+  eval_pdf(s, importance ? at_wi : s, wi, f, pdf);
   if (pdf <= 0.0f) return false;
   if (length_sq(f) == 0.0f) return false;
   const float c = fabsf(wi.z);
@@ -601,11 +618,17 @@ __device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t fl
   out.wi = wi;
   out.pdf = pdf;
   out.flags = flags;
+  out.pdf_rev = 0.0f;
+  if (want_rev) {
+    V3 f_rev;
+    eval_pdf(at_wi, at_wi, s.wo, f_rev, out.pdf_rev);
+  }
   return true;
 }
 
 // OpenPbrBsdf::sample (open_pbr.rs:298-332) in the shading frame.
-static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, float u0, float u1, Sample& out) {
+static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, float u0, float u1, Sample& out,
+                                           bool importance = false, bool want_rev = false) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
   if (!(wo.z > 0.0f) || s.q_total <= 0.0f) return false;
@@ -640,20 +663,16 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
     const bool ok = lobe == 3 ? fuzz_sample_dir(m.fuzz_roughness, wo, u0, u1, wi)
                               : eon_sample_dir(m.eon_r, m.eon_r_pow01, wo, u0, u1, wi);
     if (!ok) return false;
-    return finalize(s, wi, lobe == 3 ? (kFlagGlossy | kFlagReflection) : (kFlagDiffuse | kFlagReflection), out);
+    return finalize(s, wi, lobe == 3 ? (kFlagGlossy | kFlagReflection) : (kFlagDiffuse | kFlagReflection),
+                    importance, want_rev, out);
   }
   const bool rough = lobe == 0 ? (m.flags & kOpbrCoatRough) != 0
                                : (lobe == 1 ? (m.flags & kOpbrMetalRough) != 0 : (m.flags & kOpbrSpecRough) != 0);
   if (!rough) {
     // smooth lobe: mirror direction, delta sample
     const V3 wi = V3{-wo.x, -wo.y, wo.z};
-    V3 tint = V3{1.0f, 1.0f, 1.0f};
-    if (m.coat > 0.0f) {
-      const float mu_o = refracted_cos(wo.z, m.coat_eta), mu_i = refracted_cos(wi.z, m.coat_eta);
-      const float e = 0.5f * (1.0f / fmaxf(mu_i, 1.0e-4f) + 1.0f / fmaxf(mu_o, 1.0e-4f));
-      tint = V3{powf(fmaxf(m.coat_color[0], 0.0f), e), powf(fmaxf(m.coat_color[1], 0.0f), e),
-                powf(fmaxf(m.coat_color[2], 0.0f), e)};
-    }
+    const V3 tint = m.coat > 0.0f ? coat_tint(m, wo, wi) : V3{1.0f, 1.0f, 1.0f};
+    out.pdf_rev = 0.0f;
     if (lobe == 0) {
       const float fr = fresnel_dielectric(fabsf(wi.z), 1.0f, m.coat_eta);
       out.weight = splat(m.coat * s.below_fuzz_s * fr / p_lobe);
@@ -693,7 +712,7 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
     wi = reflect_local(wo, wm);
     if (wi.z <= 0.0f) return false;
   }
-  return finalize(s, wi, kFlagGlossy | kFlagReflection, out);
+  return finalize(s, wi, kFlagGlossy | kFlagReflection, importance, want_rev, out);
 }
 
 }  // namespace opbr

@@ -180,7 +180,7 @@ static __device__ __noinline__ bool openpbr_sample(const DevRenderData& d, uint3
   const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
   if (wo_l.z <= 0.0f) return false;
   opbr::OpbrVertex ov;
-  opbr::init_vertex(ov, d.openpbr + opbr_index, d.cec_e, d.dec_e, wo_l, v.front);
+  opbr::init_vertex(ov, d.openpbr + opbr_index, d.cec_e, d.dec_e, wo_l, v.front, fabsf(wo_l.z));
   opbr::Sample bs;
   if (!opbr::sample(ov, u_lobe, u0, u1, bs)) return false;
   const V3 wi = to_world(v.frame, bs.wi);

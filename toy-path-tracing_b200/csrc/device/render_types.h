@@ -20,6 +20,9 @@ static_assert(sizeof(DevLightNodeRec) == 64, "light node layout");
 
 enum DevMatKind : uint32_t { kDevLambert = 0, kDevEmissive = 1, kDevOpenPbr = 2 };
 
+// Longest BDPT subpath the device keeps on chip (vertices per subpath).
+constexpr uint32_t kBdptMaxDepthApi = 16;
+
 struct alignas(16) DevMaterialRec {
   uint32_t kind;
   float rho[3];
@@ -95,6 +98,15 @@ struct alignas(16) DevShadeInstance {
 };
 static_assert(sizeof(DevShadeInstance) == 128, "shade instance record");
 
+// Scene::area_light_triangles entry (scene/mod.rs:48-54): emissive triangle,
+// its area, selection weight (area * max_emission) and the running prefix.
+struct alignas(16) DevAreaLight {
+  uint32_t inst, tri;
+  float area, weight, prefix_weight;
+  uint32_t pad[3];
+};
+static_assert(sizeof(DevAreaLight) == 32, "area light record");
+
 struct DevMeshInfo {
   uint32_t vtx_base, idx_base, num_tris, flags;  // flags bit 0: normals, bit 1: uvs
 };
@@ -112,6 +124,10 @@ struct DevRenderData {
   const DevOpenPbr* openpbr;  // OpenPBR parameter table
   const float* cec_e;         // conductor energy-compensation table (64 x 64)
   const float* dec_e;         // dielectric energy-compensation table (32 x 32 x 32)
+  const DevAreaLight* area_lights;  // in registration (instance, triangle) order
+  const uint32_t* area_light_of;    // emitter-map slot -> area light index (or 0xFFFFFFFF)
+  uint32_t num_area_lights;
+  float area_light_weight_sum;
   uint32_t ltree_root;
   uint32_t has_tree;
   float tree_cat_pmf;  // LightSampler pmf of the Tree category

@@ -85,4 +85,10 @@ inline void transform_point_glam(const float* m, const float* p, float* out) {
 
 bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out);
 
+struct HostAreaLight {
+  uint32_t inst, tri;
+  float area, weight, prefix_weight;
+};
+void register_area_lights(const HostSceneView& s, std::vector<HostAreaLight>* out, float* weight_sum);
+
 }  // namespace tpt

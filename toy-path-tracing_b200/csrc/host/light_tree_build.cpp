@@ -281,6 +281,36 @@ class TreeBuilder {
 
 }  // namespace
 
+// Scene::register_area_light_triangles (scene/mod.rs:649-683): the area-light
+// registry BDPT samples its light subpaths from.
+void register_area_lights(const HostSceneView& s, std::vector<HostAreaLight>* out, float* weight_sum) {
+  out->clear();
+  float sum = 0.0f;
+  for (uint32_t ii = 0; ii < s.num_instances; ++ii) {
+    const HostInstance& inst = s.instances[ii];
+    const HostMaterial& mat = s.materials[inst.material];
+    if (!mat.may_emit()) continue;
+    const float max_em = mat.max_emission();
+    if (max_em <= 0.0f) continue;
+    const HostMesh& m = s.meshes[inst.mesh];
+    for (uint32_t t = 0; t < m.num_triangles; ++t) {
+      V3 p[3];
+      for (int k = 0; k < 3; ++k) {
+        const float* v = m.positions + 3 * (size_t)m.indices[3 * (size_t)t + k];
+        float w[3];
+        transform_point_glam(inst.local_to_world, v, w);
+        p[k] = V3{w[0], w[1], w[2]};
+      }
+      const float area = 0.5f * length(cross(sub(p[1], p[0]), sub(p[2], p[0])));
+      const float weight = area * max_em;
+      if (weight <= 0.0f) continue;
+      sum += weight;
+      out->push_back(HostAreaLight{ii, t, area, weight, sum});
+    }
+  }
+  *weight_sum = sum;
+}
+
 // Scene::register_area_light_triangles (scene/mod.rs:649-683) + build_light_tree
 // (builder.rs:58-99): emitters in instance/triangle order, leaves with flux > 0.
 bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out) {

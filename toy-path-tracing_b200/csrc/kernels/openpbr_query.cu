@@ -12,16 +12,24 @@ constexpr int kQueryBlock = 128;
 __global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(DevRenderData rd, uint32_t material, uint64_t n,
                                                                 const float* __restrict__ wo,
                                                                 const float* __restrict__ wi,
-                                                                const uint32_t* __restrict__ front,
+                                                                const uint32_t* __restrict__ front, uint32_t mode,
                                                                 float* __restrict__ f, float* __restrict__ pdf) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const DevOpenPbr* m = rd.openpbr + rd.mats[material].openpbr;
   opbr::OpbrVertex s;
-  opbr::init_vertex(s, m, rd.cec_e, rd.dec_e, V3{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]}, front[i] != 0);
+  const V3 o = V3{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]};
+  const V3 w = V3{wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
+  opbr::init_vertex(s, m, rd.cec_e, rd.dec_e, o, front[i] != 0, fabsf(o.z));
   V3 fv;
   float p;
-  opbr::eval_pdf(s, V3{wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]}, fv, p);
+  if (mode == 1) {  // importance transport: layer weights at wi
+    opbr::OpbrVertex lay;
+    opbr::init_vertex(lay, m, rd.cec_e, rd.dec_e, w, front[i] != 0, fabsf(o.z));
+    opbr::eval_pdf(s, lay, w, fv, p);
+  } else {
+    opbr::eval_pdf(s, s, w, fv, p);
+  }
   f[3 * i] = fv.x;
   f[3 * i + 1] = fv.y;
   f[3 * i + 2] = fv.z;
@@ -31,17 +39,18 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(DevRenderData rd
 __global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(DevRenderData rd, uint32_t material, uint64_t n,
                                                                   const float* __restrict__ wo,
                                                                   const float* __restrict__ u,
-                                                                  const uint32_t* __restrict__ front,
+                                                                  const uint32_t* __restrict__ front, uint32_t mode,
                                                                   float* __restrict__ out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const DevOpenPbr* m = rd.openpbr + rd.mats[material].openpbr;
   opbr::OpbrVertex s;
-  opbr::init_vertex(s, m, rd.cec_e, rd.dec_e, V3{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]}, front[i] != 0);
+  const V3 w = V3{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]};
+  opbr::init_vertex(s, m, rd.cec_e, rd.dec_e, w, front[i] != 0, fabsf(w.z));
   opbr::Sample smp;
-  float* o = out + 8 * i;
-  if (!opbr::sample(s, u[3 * i], u[3 * i + 1], u[3 * i + 2], smp)) {
-    for (int k = 0; k < 8; ++k) o[k] = 0.0f;
+  float* o = out + 9 * i;
+  if (!opbr::sample(s, u[3 * i], u[3 * i + 1], u[3 * i + 2], smp, mode == 1, true)) {
+    for (int k = 0; k < 9; ++k) o[k] = 0.0f;
     return;
   }
   o[0] = smp.weight.x;
@@ -51,23 +60,24 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(DevRenderData 
   o[4] = smp.wi.y;
   o[5] = smp.wi.z;
   o[6] = smp.pdf;
-  o[7] = __uint_as_float(smp.flags);
+  o[7] = smp.pdf_rev;
+  o[8] = __uint_as_float(smp.flags);
 }
 }  // namespace
 
 cudaError_t launch_bsdf_eval(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo, const float* wi,
-                             const uint32_t* front, float* f, float* pdf, cudaStream_t s) {
+                             const uint32_t* front, uint32_t mode, float* f, float* pdf, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   bsdf_eval_kernel<<<(unsigned)((n + kQueryBlock - 1) / kQueryBlock), kQueryBlock, 0, s>>>(rd, material, n, wo, wi,
-                                                                                          front, f, pdf);
+                                                                                          front, mode, f, pdf);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bsdf_sample(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo,
-                               const float* u, const uint32_t* front, float* out, cudaStream_t s) {
+                               const float* u, const uint32_t* front, uint32_t mode, float* out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   bsdf_sample_kernel<<<(unsigned)((n + kQueryBlock - 1) / kQueryBlock), kQueryBlock, 0, s>>>(rd, material, n, wo, u,
-                                                                                            front, out);
+                                                                                            front, mode, out);
   return cudaGetLastError();
 }
 

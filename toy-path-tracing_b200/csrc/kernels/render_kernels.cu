@@ -59,6 +59,8 @@ __global__ void accumulate_kernel(const float* __restrict__ samples, uint32_t sp
 cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P, float* samples,
                           uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t s) {
   if (n_paths == 0) return cudaSuccess;
+  if (P.integrator == TPT_INTEGRATOR_BDPT)
+    return launch_render_bdpt(geo, rd, P, samples, first_path, n_paths, err, num_sms, s);
   DevRender S;
   S.geo = geo;
   S.d = rd;

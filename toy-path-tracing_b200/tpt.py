@@ -162,6 +162,7 @@ EXEC_WAVEFRONT = 0
 EXEC_MEGAKERNEL = 1
 
 LAMBERT, EMISSIVE, OPENPBR = 0, 1, 2  # tpt_material_kind
+INTEGRATOR_MIS, INTEGRATOR_BDPT = 0, 1  # tpt_integrator
 
 
 def lib():
@@ -237,8 +238,8 @@ def _declare(L):
         "tpt_lut_dielectric_albedo": (i32, [vp, C.c_float, vp]),
         "tpt_lut_conductor_ec": (i32, [vp, vp, vp]),
         "tpt_lut_dielectric_ec": (i32, [vp, vp, vp]),
-        "tpt_bsdf_eval_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, vp, vp, vp]),
-        "tpt_bsdf_sample_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, vp, vp]),
+        "tpt_bsdf_eval_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp, vp]),
+        "tpt_bsdf_sample_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -449,17 +450,19 @@ class Scene:
                                                _stream(stream)), self.ctx)
 
     def bsdf_eval_device(self, material: int, n: int, wo_ptr: int, wi_ptr: int, front_ptr: int, f_ptr: int,
-                         pdf_ptr: int, stream=None):
-        """`tpt_bsdf_eval_device`: OpenPBR eval + pdf of n direction pairs (device buffers)."""
+                         pdf_ptr: int, stream=None, mode: int = 0):
+        """`tpt_bsdf_eval_device`: OpenPBR eval + pdf of n direction pairs (device buffers);
+        mode 0 radiance, 1 importance transport."""
         _check(lib().tpt_bsdf_eval_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr), C.c_void_p(wi_ptr),
-                                          C.c_void_p(front_ptr), C.c_void_p(f_ptr), C.c_void_p(pdf_ptr),
+                                          C.c_void_p(front_ptr), mode, C.c_void_p(f_ptr), C.c_void_p(pdf_ptr),
                                           _stream(stream)), self.ctx)
 
     def bsdf_sample_device(self, material: int, n: int, wo_ptr: int, u_ptr: int, front_ptr: int, out_ptr: int,
-                           stream=None):
-        """`tpt_bsdf_sample_device`: OpenPBR samples (weight, wi, pdf, flags) for n (wo, u)."""
+                           stream=None, mode: int = 0):
+        """`tpt_bsdf_sample_device`: OpenPBR samples (weight, wi, pdf, pdf_rev, flags) for n (wo, u)."""
         _check(lib().tpt_bsdf_sample_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr), C.c_void_p(u_ptr),
-                                            C.c_void_p(front_ptr), C.c_void_p(out_ptr), _stream(stream)), self.ctx)
+                                            C.c_void_p(front_ptr), mode, C.c_void_p(out_ptr), _stream(stream)),
+               self.ctx)
 
     def device_bytes(self) -> int:
         v = C.c_uint64()
