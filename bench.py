@@ -48,6 +48,12 @@ def parse_args():
     p.add_argument("--rays-log2", type=int, default=24, help="rays per batch = 2^k (profiling uses smaller)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-render", action="store_true", help="skip the render workload block")
+    # profiling shapes of the render block (defaults: the plain-MIS configuration)
+    p.add_argument("--render-only", action="store_true", help="run the render block alone")
+    p.add_argument("--render-res", type=int, default=256)
+    p.add_argument("--render-spp", type=int, default=64)
+    p.add_argument("--render-exec", choices=["both", "wavefront", "megakernel"], default="both")
+    p.add_argument("--render-scene", choices=["both", "openpbr", "lambert"], default="both")
     return p.parse_args()
 
 
@@ -195,18 +201,25 @@ RENDER_SCENES = {
 }
 
 
-def render_block(ctx, steps, warmup, cpu=True):
-    """Both Cornell boxes at 256x256, 64 spp, depth 8."""
+def render_block(ctx, steps, warmup, cpu=True, args=None):
+    """Both Cornell boxes at 256x256, 64 spp, depth 8 (other shapes for profiling)."""
     import tpt_scenes
 
-    out = {"config": RENDER_CFG, "unit": "Msamples/s"}
+    cfg = dict(RENDER_CFG)
+    if args is not None:
+        cfg.update(width=args.render_res, height=args.render_res, spp=args.render_spp)
+    which = "both" if args is None else args.render_scene
+    execs = "both" if args is None else args.render_exec
+    out = {"config": cfg, "unit": "Msamples/s"}
     for key, kind in (("cornell_openpbr", tpt_scenes.OPENPBR), ("cornell_lambert", tpt_scenes.LAMBERT)):
-        out[key] = render_scene_block(ctx, kind, steps, warmup, cpu)
+        if which != "both" and not key.endswith(which):
+            continue
+        out[key] = render_scene_block(ctx, kind, steps, warmup, cpu, cfg, execs)
         out[key]["scene"] = RENDER_SCENES[key]
     return out
 
 
-def render_scene_block(ctx, kind, steps, warmup, cpu=True):
+def render_scene_block(ctx, kind, steps, warmup, cpu=True, cfg=RENDER_CFG, execs="both"):
     """Wavefront vs megakernel Msamples/s (identical images by construction, so
     equal RMSE), and the oracle on the host cores."""
     import torch
@@ -216,11 +229,13 @@ def render_scene_block(ctx, kind, steps, warmup, cpu=True):
 
     sc = tpt_scenes.cornell_box(1, kind)
     scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
-    W, H, spp, depth = RENDER_CFG["width"], RENDER_CFG["height"], RENDER_CFG["spp"], RENDER_CFG["max_depth"]
+    W, H, spp, depth = cfg["width"], cfg["height"], cfg["spp"], cfg["max_depth"]
     stream = torch.cuda.current_stream()
     img = torch.empty(W * H * 3, device="cuda")
     out = {}
     for name, ex in (("wavefront", tpt.EXEC_WAVEFRONT), ("megakernel", tpt.EXEC_MEGAKERNEL)):
+        if execs not in ("both", name):
+            continue
         job = scene.job(sc["camera"], W, H, spp, depth, execution=ex)
         for _ in range(warmup):
             scene.render_device(job, img.data_ptr(), stream.cuda_stream)
@@ -234,8 +249,9 @@ def render_scene_block(ctx, kind, steps, warmup, cpu=True):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / n
         out[name] = {"value": W * H * spp / ms / 1e3, "ms_per_image": ms}
-    out["wavefront_over_megakernel"] = out["wavefront"]["value"] / out["megakernel"]["value"]
-    if cpu:
+    if execs == "both":
+        out["wavefront_over_megakernel"] = out["wavefront"]["value"] / out["megakernel"]["value"]
+    if cpu and "wavefront" in out:
         import oracle as orc
 
         ref = orc.RenderScene(sc, scene.light_tree())
@@ -274,6 +290,12 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     ctx = tpt.Context(local)
+    if args.render_only:
+        if rank == 0:
+            line = {"render": render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline, args=args)}
+            print(json.dumps(line), flush=True)
+        ctx.close()
+        return 0
     mesh, batches = make_workload(rank, args.rays_log2)
     scene = tpt.Scene(ctx, [mesh], [__import__("tpt_scenes").identity_instance()])
     n = batches[0].shape[1]
@@ -387,7 +409,7 @@ def run_ours(args):
         rate, threads, desc = cpu_reference_rate(mesh, batches)
         line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0 and not args.no_render:
-        line["render"] = render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline)
+        line["render"] = render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline, args=args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del scene
