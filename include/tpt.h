@@ -346,6 +346,65 @@ tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint
                                   const float* wo, const float* u, const uint32_t* front_face, uint32_t mode,
                                   float* out, void* stream);
 
+/* ---- Material updates and the path-replay adjoint -------------------------
+ * Neither has a counterpart in the reference: its materials are fixed once
+ * added to a Scene, and its renderer is not differentiable.  They give the
+ * renderer a forward/backward pair for inverse rendering of OpenPBR materials:
+ * forward = tpt_render_device, backward = tpt_adjoint_device. */
+
+/* Replaces the parameters of OpenPBR materials of an uploaded scene (count
+ * entries: scene material index, new parameters).  The new records are lowered
+ * on the host and copied on `stream` (NULL = the context's stream), ordered
+ * after the work already queued there; renders on other streams that read the
+ * scene must have finished.  Fails with TPT_ERR_INVALID_ARG for a material that
+ * is not OpenPBR or for parameters upload would reject. */
+tpt_status tpt_scene_set_openpbr(tpt_context* ctx, tpt_scene* scene, uint32_t count, const uint32_t* material_ids,
+                                 const tpt_openpbr_desc* descs, void* stream);
+
+/* Gradient layout: per scene material, TPT_GRAD_PARAMS doubles in this order. */
+enum {
+  TPT_GRAD_BASE_COLOR_R = 0,
+  TPT_GRAD_BASE_COLOR_G = 1,
+  TPT_GRAD_BASE_COLOR_B = 2,
+  TPT_GRAD_SPECULAR_ROUGHNESS = 3,
+  TPT_GRAD_BASE_METALNESS = 4,
+  TPT_GRAD_SPECULAR_IOR = 5,
+  TPT_GRAD_COAT_WEIGHT = 6,
+  TPT_GRAD_PARAMS = 7
+};
+/* Parameter groups (bits of tpt_adjoint_desc.param_mask). */
+enum {
+  TPT_GRAD_MASK_BASE_COLOR = 1,
+  TPT_GRAD_MASK_ROUGHNESS = 2,
+  TPT_GRAD_MASK_METALNESS = 4,
+  TPT_GRAD_MASK_IOR = 8,
+  TPT_GRAD_MASK_COAT = 16,
+  TPT_GRAD_ALL = 31
+};
+
+typedef struct tpt_adjoint_desc {
+  uint32_t param_mask; /* groups to differentiate; 0 = TPT_GRAD_ALL */
+  float fd_step;       /* parameter step of the BSDF central differences; 0 = 1e-3 */
+} tpt_adjoint_desc;
+
+/* dLoss/d(material parameters) of the image tpt_render_device produces for
+ * `job` (MIS integrator; `execution` is not read), given d_image = dLoss/dimage
+ * (device, width*height*3 floats).  grad (device, num_materials x
+ * TPT_GRAD_PARAMS doubles) is overwritten; non-OpenPBR materials get zeros.
+ * Path replay with detached sampling: per chunk of paths the forward wavefront
+ * is run again for the paths' radiance, then replayed from the same streams,
+ * and every rough OpenPBR vertex adds dLoss/dL * R * (df/dtheta) / f, R being
+ * the radiance the path collects after the vertex and df/dtheta a central
+ * difference of the BSDF at the sampled direction between host-lowered
+ * theta -/+ fd_step copies of the material (clipped to [0, 1], the IOR to
+ * [1, 10]).  Accumulation is FP64 atomics, so the sums' order (and last bits)
+ * vary between runs.  adesc may be NULL (all groups, step 1e-3). */
+tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const tpt_adjoint_desc* adesc,
+                              const float* d_image, double* grad, void* stream);
+/* Host-buffer variant (synchronous). */
+tpt_status tpt_adjoint(tpt_context* ctx, const tpt_render_job* job, const tpt_adjoint_desc* adesc,
+                       const float* d_image, double* grad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,7 @@ def _declare(L):
         "orc_render_scene_set_light_tree": (None, [vp, vp, u64, u32]),
         "orc_render_pixels": (None, [vp, vp, u32, u32, u32, u32, u32, u32, u32, vp, i32]),
         "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u32, u64, u64, vp, i32]),
+        "orc_render_adjoint": (None, [vp, vp, u32, u32, u32, u32, vp, u32, C.c_float, vp, i32]),
         "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
         "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, vp]),
         "orc_render_emitted": (None, [vp, i32, i32, vp, vp, i32, i32, vp, vp, vp, f32, i32, vp]),
@@ -247,6 +248,7 @@ class RenderScene:
         self.g = g
         self.h = lib().orc_render_scene_create(g.h)
         mats = scene["materials"]
+        self.n_materials = len(mats)
         kinds = np.array([m["kind"] for m in mats], np.uint32)
         rho = np.array([np.asarray(m.get("rho", (0, 0, 0)), np.float32) for m in mats], np.float32)
         col = np.array([np.asarray(m.get("color", (0, 0, 0)), np.float32) for m in mats], np.float32)
@@ -287,6 +289,18 @@ class RenderScene:
         out = np.empty((count, 3), np.float32)
         cam = self._cam(camera)
         lib().orc_render_samples(self.h, _p(cam), width, height, spp, max_depth, integrator, first, count, _p(out),
+                                 nthreads or os.cpu_count() or 1)
+        return out
+
+    def adjoint(self, camera, width, height, spp, max_depth, d_image, mask=31, step=1e-3, nthreads=None):
+        """Path-replay adjoint (MIS): dLoss/d(OpenPBR parameters) per material,
+        float64 [n_materials, 7] = base_color rgb, specular_roughness,
+        base_metalness, specular_ior, coat_weight; d_image = dLoss/dimage."""
+        d = np.ascontiguousarray(d_image, np.float32).reshape(-1)
+        assert d.size == width * height * 3
+        out = np.zeros((self.n_materials, 7), np.float64)
+        cam = self._cam(camera)
+        lib().orc_render_adjoint(self.h, _p(cam), width, height, spp, max_depth, _p(d), mask, float(step), _p(out),
                                  nthreads or os.cpu_count() or 1)
         return out
 

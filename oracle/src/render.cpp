@@ -508,6 +508,45 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
   return L;
 }
 
+void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth, Vec3 L,
+                AdjointVertexSink& sink) {
+  Vec3 R = L, beta(1, 1, 1);
+  SceneHit h;
+  if (!closest(s, ray.origin, ray.direction, &h)) return;
+  Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
+  const Material* m = &s.mat_of(h.instance);
+  uint32_t mi = s.geo.instances[h.instance].material_index;
+  if (m->kind == kEmissive) R = R - emissive_le(*m);
+  for (uint32_t depth = 0; depth < max_depth; ++depth) {
+    VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    if (m->kind == kEmissive) break;
+    R = R - beta * direct_light(s, *m, v, rnd);
+    MatSample bs;
+    bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+                                  : lambert_sample(*m, v, rnd.material.u_dir, &bs);
+    if (!ok) break;
+    beta *= bs.weight;
+    if (depth + 1 >= 4) {
+      float q = clampf(max_element(beta), 0.05f, 1.0f);
+      if (rnd.u_rr > q) break;
+      beta /= q;
+    }
+    if (m->kind == kOpenPbr && !bs.delta) sink.vertex(mi, v, bs.wi, R);
+    SceneHit nh;
+    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) break;
+    Vertex nv = s.shading_vertex(nh.instance, nh.triangle, nh.bary, bs.wi);
+    const Material* nm = &s.mat_of(nh.instance);
+    if (nm->kind == kEmissive) {
+      Vec3 le = emissive_le(*nm);
+      if (bs.delta) R = R - beta * le;
+      else R = R - beta * le * balance(bs.pdf, light_pdf_for_hit(s, *m, v, nv));
+    }
+    v = nv;
+    m = nm;
+    mi = s.geo.instances[nh.instance].material_index;
+  }
+}
+
 namespace {
 Vec3 one_sample(const RenderScene& s, const RenderJob& job, uint32_t pixel, uint32_t sample) {
   uint32_t px = pixel % job.width, py = pixel / job.width;

@@ -113,6 +113,18 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
 // bdpt::trace_radiance for one sample (integrator/bdpt.rs:70-131)
 Vec3 trace_bdpt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
 
+// Path-replay adjoint (no counterpart in the reference): replays the path of
+// trace_mis with the same streams, given its radiance L, and calls `vertex` at
+// every rough (non-delta) OpenPBR scattering vertex with the sampled direction
+// and R = the part of L the path collects after that vertex (emission and NEE
+// of later vertices).  OpenPBR vertices do no NEE, so R is exact there.
+struct AdjointVertexSink {
+  virtual ~AdjointVertexSink() = default;
+  virtual void vertex(uint32_t material_index, const Vertex& v, Vec3 wi, Vec3 R) = 0;
+};
+void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth, Vec3 L,
+                AdjointVertexSink& sink);
+
 // main.rs:99-126 for pixels [p0, p1): running mean over spp samples, times exposure.
 void render_pixels(const RenderScene& s, const RenderJob& job, uint32_t p0, uint32_t p1, float* out_rgb, int nthreads);
 // Per-sample radiance of paths [first, first + count), path = pixel * spp + sample.

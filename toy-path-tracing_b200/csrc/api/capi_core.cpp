@@ -462,6 +462,7 @@ tpt_status tpt_scene_release(tpt_scene* s) {
   if (!s) return TPT_OK;
   if (s->ctx) cudaSetDevice(s->ctx->device);
   for (void* p : s->allocations) cudaFree(p);
+  if (s->d_adj) cudaFree(s->d_adj);
   delete s;
   return TPT_OK;
 }

@@ -65,6 +65,9 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
   return TPT_OK;
 }
 
+}  // namespace
+
+namespace tpt {
 tpt_status ensure_scratch(tpt_context* ctx, size_t bytes) {
   if (ctx->d_scratch_bytes >= bytes) return TPT_OK;
   if (ctx->d_scratch) {
@@ -129,15 +132,17 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   return TPT_OK;
 }
 
-// Paths [first, first + n) through the wavefront stages; radiance per path into samples.
+// Paths [first, first + n) through the wavefront stages; radiance per path into
+// samples.  With A, the adjoint replay instead: samples holds the paths'
+// radiance from a forward pass and the gradients go to A->grad.
 tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
-                            uint32_t n, float* samples, cudaStream_t s) {
+                            uint32_t n, float* samples, cudaStream_t s, const DevAdjoint* A) {
   tpt_status st = ensure_wavefront(ctx, n);
   if (st) return st;
   const WfBuffers& B = ctx->wf;
   const DevGeometry& geo = job->scene->geo;
   const DevRenderData& rd = job->scene->render;
-  cudaError_t e = launch_wf_generate(geo, rd, L, B, first, n, s);
+  cudaError_t e = launch_wf_generate(geo, rd, L, B, first, n, s, A ? samples : nullptr);
   for (uint32_t b = 0; e == cudaSuccess && b <= L.max_depth; ++b) {
     const int cur = (int)(b & 1u);
     e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
@@ -146,14 +151,14 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
       e = launch_traverse_strided(geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
                                   B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
                                   nullptr, nullptr, B.counts + cur);
-    if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, first, cur, s);
+    if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, first, cur, s, A);
     if (e == cudaSuccess && b < L.max_depth)
       e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
                                   nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
                                   nullptr, B.counts + 2);
-    if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s);
+    if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s, A != nullptr);
   }
-  if (e == cudaSuccess) e = launch_wf_finalize(B, n, samples, s);
+  if (e == cudaSuccess && !A) e = launch_wf_finalize(B, n, samples, s);
   return cuda_check(ctx, e, "wavefront launch");
 }
 
@@ -166,9 +171,7 @@ uint32_t chunk_pixels(const RenderLaunch& L) {
   return (uint32_t)std::max<uint64_t>(1, std::min(n, total));
 }
 
-}  // namespace
 
-namespace tpt {
 tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* out) {
   return make_launch(ctx, job, out);
 }

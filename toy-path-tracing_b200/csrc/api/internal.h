@@ -58,6 +58,16 @@ struct tpt_scene {
   tpt::DevRenderData render{};          // shading data for the render kernels
   tpt::LightTreeHost light_tree;        // host copy of the light tree
   std::vector<uint32_t> material_kinds; // tpt_material_kind per material
+  // OpenPBR materials: host copy of each table entry's parameters and the
+  // material -> table index map (0xFFFFFFFF: not OpenPBR)
+  std::vector<tpt_openpbr_desc> opbr_desc;
+  std::vector<uint32_t> opbr_of_material;
+  uint32_t mat_version = 0;  // bumped by tpt_scene_set_openpbr
+  // adjoint perturbation tables (lowered on demand, owned by the scene)
+  void* d_adj = nullptr;
+  size_t d_adj_bytes = 0;
+  uint32_t adj_version = 0xFFFFFFFFu, adj_mask = 0;
+  float adj_step = 0.0f;
 };
 
 namespace tpt {
@@ -91,13 +101,26 @@ cudaError_t launch_render_bdpt(const DevGeometry& geo, const DevRenderData& rd, 
 
 // capi_render.cpp: validates a job and derives its launch parameters.
 tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* out);
+// The context's per-sample scratch (grown on demand) and wavefront arena.
+tpt_status ensure_scratch(tpt_context* ctx, size_t bytes);
+tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity);
+// Pixels per chunk of a job: at most 2^22 paths and 1 GiB of samples.
+uint32_t chunk_pixels(const RenderLaunch& L);
+// Paths [first, first + n) through the wavefront stages (forward: radiance into
+// samples; with A: the adjoint replay of samples' paths, gradients to A->grad).
+tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
+                            uint32_t n, float* samples, cudaStream_t s, const DevAdjoint* A = nullptr);
 
 // wavefront_kernels.cu
+// primal != NULL / A != NULL / adjoint: the adjoint instantiation (path replay
+// with R; primal = per-sample radiance of the forward pass, path order).
 cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                               const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s);
+                               const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s,
+                               const float* primal = nullptr);
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s);
-cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s);
+                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s,
+                            const DevAdjoint* A = nullptr);
+cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint = false);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
 
 // capi_openpbr.cpp: the context's OpenPBR tables, built on first use.
@@ -118,6 +141,9 @@ cudaError_t launch_bsdf_sample(const DevRenderData& rd, uint32_t material, uint6
 
 // scene_render_upload.cpp: materials, shading arrays, light tree, emitter map.
 tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc);
+// One OpenPBR material lowered for the device (make_bsdf's material part),
+// building the tables it reads on first use.
+tpt_status lower_openpbr_material(tpt_context* ctx, const tpt_openpbr_desc& d, DevOpenPbr* out);
 // Device allocation owned by the scene.
 tpt_status scene_alloc(tpt_scene* s, size_t bytes, void** out);
 

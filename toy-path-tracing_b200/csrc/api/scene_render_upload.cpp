@@ -37,6 +37,16 @@ tpt_status put(tpt_scene* s, const std::vector<T>& v, const T** dst) {
 }
 }  // namespace
 
+tpt_status lower_openpbr_material(tpt_context* ctx, const tpt_openpbr_desc& d, DevOpenPbr* out) {
+  const float *spec_da = nullptr, *coat_da = nullptr;
+  tpt_status st = ensure_ec_tables(ctx);
+  if (!st) st = ensure_da_table(ctx, openpbr_spec_table_eta(d), &spec_da);
+  if (!st && d.coat_weight > 0.0f) st = ensure_da_table(ctx, openpbr_coat_table_eta(d), &coat_da);
+  if (st) return st;
+  lower_openpbr(d, spec_da, coat_da, ctx->h_cec_e_avg.data(), ctx->h_dec_e_avg.data(), out);
+  return TPT_OK;
+}
+
 tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   tpt_context* ctx = s->ctx;
   // materials
@@ -45,6 +55,8 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   if (desc->num_materials && !desc->materials) return set_error(ctx, TPT_ERR_INVALID_ARG, "materials is NULL");
   std::vector<DevOpenPbr> opbr;
   s->material_kinds.assign(desc->num_materials, 0u);
+  s->opbr_desc.clear();
+  s->opbr_of_material.clear();
   for (uint32_t i = 0; i < desc->num_materials; ++i) {
     const tpt_material_desc& m = desc->materials[i];
     if (m.kind != TPT_MATERIAL_NORMALIZED_LAMBERT && m.kind != TPT_MATERIAL_EMISSIVE &&
@@ -56,16 +68,14 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
       if (!m.openpbr) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": openpbr is NULL");
       const std::string why = openpbr_unsupported(*m.openpbr);
       if (!why.empty()) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": " + why);
-      const float *spec_da = nullptr, *coat_da = nullptr;
-      tpt_status st = ensure_ec_tables(ctx);
-      if (!st) st = ensure_da_table(ctx, openpbr_spec_table_eta(*m.openpbr), &spec_da);
-      if (!st && m.openpbr->coat_weight > 0.0f) st = ensure_da_table(ctx, openpbr_coat_table_eta(*m.openpbr), &coat_da);
-      if (st) return st;
       DevOpenPbr rec;
-      lower_openpbr(*m.openpbr, spec_da, coat_da, ctx->h_cec_e_avg.data(), ctx->h_dec_e_avg.data(), &rec);
+      tpt_status st = lower_openpbr_material(ctx, *m.openpbr, &rec);
+      if (st) return st;
       opbr_index = (uint32_t)opbr.size();
       opbr.push_back(rec);
+      s->opbr_desc.push_back(*m.openpbr);
     }
+    s->opbr_of_material.push_back(m.kind == TPT_MATERIAL_OPENPBR ? opbr_index : kInvalidNode);
     HostMaterial h{};
     h.kind = m.kind;
     std::memcpy(h.rho, m.rho, 12);

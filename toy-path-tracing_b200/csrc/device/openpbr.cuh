@@ -503,9 +503,10 @@ __device__ __forceinline__ V3 coat_tint(const DevOpenPbr& m, V3 wo, V3 wi) {
 
 // OpenPbrBsdf::eval and ::pdf for one direction pair.  `lay` is the state of
 // the direction the layer weights are taken at: the vertex itself in radiance
-// transport, wi in importance transport (open_pbr.rs:228-233).
+// transport, wi in importance transport (open_pbr.rs:228-233).  want_pdf =
+// false leaves pdf_out at 0 (callers that need f only).
 static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVertex& lay, V3 wi, V3& f_out,
-                                             float& pdf_out) {
+                                             float& pdf_out, bool want_pdf = true) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
   V3 total = V3{0.0f, 0.0f, 0.0f};
@@ -569,7 +570,7 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVert
   }
   f_out = total;
   // pdf (open_pbr.rs:262-296)
-  if (s.q_total <= 0.0f) return;
+  if (!want_pdf || s.q_total <= 0.0f) return;
   if (s.q_coat > 0.0f && (m.flags & kOpbrCoatRough)) {
     const DevMsFace& f = m.ms[1][s.face];
     float p;

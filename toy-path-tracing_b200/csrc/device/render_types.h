@@ -149,6 +149,23 @@ struct RenderLaunch {
   uint32_t pad;
 };
 
+// Path-replay adjoint (no counterpart in the reference): inputs of the adjoint
+// instantiation of the wavefront stages.  Gradients are per scene material,
+// kGradParams doubles each: base_color r, g, b, specular_roughness,
+// base_metalness, specular_ior, coat_weight.  The BSDF partials are central
+// differences between two host-lowered copies of each OpenPBR material, one
+// pair per parameter group (base colour, roughness, metalness, ior, coat).
+constexpr uint32_t kGradParams = 7;
+constexpr uint32_t kGradGroups = 5;
+struct DevAdjoint {
+  const DevOpenPbr* pert;  // [OpenPBR table index][group][lo, hi]
+  const float* span;       // [OpenPBR table index][group][3]: hi - lo per channel
+  const float* d_image;    // dLoss/dimage: width * height * 3
+  double* grad;            // [material][kGradParams]
+  float scale;             // exposure / spp: d image / d sample radiance
+  uint32_t mask;           // parameter groups to differentiate (bit g = group g)
+};
+
 // Wavefront state: per path slot of a chunk (capacity slots), two ray queues,
 // the hit records of the current queue and the shadow queue.  Planes of a
 // structured array are `capacity` elements apart.

@@ -13,7 +13,14 @@
 // of vertex d + 1), so the result equals the megakernel's bit for bit.
 // Stage launch shapes do not depend on queue lengths (those live on the
 // device), so one bounce is a fixed launch sequence that a CUDA graph replays.
+//
+// The adjoint instantiation (ADJ = true) replays the same paths with the
+// radiance planes holding R, the part of the path's radiance still to come:
+// generate starts R at the path's radiance from the forward pass, shade and
+// resolve subtract what each vertex collects, and shade adds, at every rough
+// OpenPBR vertex, dLoss/dL * R * (df/dtheta) / f to the per-material gradients.
 #include "../api/internal.h"
+#include "../device/adjoint.cuh"
 #include "../device/render.cuh"
 
 namespace tpt {
@@ -31,8 +38,10 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
+template <bool ADJ>
 __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunch P, WfBuffers B,
-                                                        uint64_t first_path, uint32_t n_paths) {
+                                                        uint64_t first_path, uint32_t n_paths,
+                                                        const float* __restrict__ primal) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
     B.counts[0] = n_paths;
@@ -63,16 +72,21 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunc
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     B.beta[k * C + i] = 1.0f;
-    B.L[k * C + i] = 0.0f;
+    B.L[k * C + i] = ADJ ? primal[3 * (uint64_t)i + k] : 0.0f;
   }
   B.depth[i] = 0;
 }
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
+template <bool ADJ>
 __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P, WfBuffers B, uint64_t first_path,
-                                                     int cur) {
+                                                     int cur, DevAdjoint A) {
+  __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[cur]) return;
+  const float sgn = ADJ ? -1.0f : 1.0f;  // the adjoint takes collected radiance off R
+  uint32_t grad_key = 0xFFFFFFFFu;
+  float grad_v[ADJ ? kGradParams : 1];
   const uint32_t C = B.capacity;
   const uint32_t slot = B.q_slot[cur][j];
   const uint32_t d = B.depth[slot];
@@ -98,17 +112,17 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
     if (m.kind == kDevEmissive) {
       const V3 le = emissive_le(m);
       if (d == 0) {
-        L = L + le;
+        L = L + sgn * le;
       } else {
         const uint32_t pm = B.prev_mat[slot];
         if (pm >> 31) {
-          L = L + beta * le;
+          L = L + sgn * (beta * le);
         } else {
           Vertex pv;
           pv.p = V3{B.prev[slot], B.prev[C + slot], B.prev[2 * C + slot]};
           pv.ns = V3{B.prev[3 * C + slot], B.prev[4 * C + slot], B.prev[5 * C + slot]};
           const float lp = light_pdf_for_hit(S, S.d.mats[pm & 0x7FFFFFFFu], pv, v);
-          L = L + beta * le * balance_heuristic(B.prev[6 * C + slot], lp);
+          L = L + sgn * (beta * le * balance_heuristic(B.prev[6 * C + slot], lp));
         }
       }
     }
@@ -135,6 +149,14 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
         }
         if (alive) {
           push_next = true;
+          if (ADJ && m.kind == kDevOpenPbr && !s.delta) {
+            // OpenPBR vertices do no NEE, so R (= L here) is what the path collects after this vertex
+            const uint32_t pixel = (uint32_t)(path / P.spp);
+            const V3 dl = V3{A.d_image[3 * (uint64_t)pixel], A.d_image[3 * (uint64_t)pixel + 1],
+                             A.d_image[3 * (uint64_t)pixel + 2]} * A.scale;
+            openpbr_vertex_grads(S, A, m.openpbr, v, s.wi, dl * L, grad_v);
+            grad_key = mi;
+          }
           next_o = offset_origin(v.p, v.ng, s.wi);
           next_d = s.wi;
           B.prev[slot] = v.p.x;
@@ -186,10 +208,12 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
     B.s_contrib[C + qs] = dp.contrib.y;
     B.s_contrib[2 * C + qs] = dp.contrib.z;
   }
+  if (ADJ) warp_accumulate_grads(A.grad, grad_key, grad_v, grad_sh + (threadIdx.x & ~31u) * kGradParams);
 }
 
 // unoccluded_ray (integrator/mod.rs:239-265): visible when nothing is hit or the
 // first hit is the sampled emitter triangle.
+template <bool ADJ>
 __global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[2]) return;
@@ -198,9 +222,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B) {
   const bool visible = tri < 0 || ((uint32_t)B.s_inst[j] == B.s_target[j] && (uint32_t)tri == B.s_target[C + j]);
   if (!visible) return;
   const uint32_t slot = B.s_slot[j];
-  B.L[slot] = B.L[slot] + B.s_contrib[j];
-  B.L[C + slot] = B.L[C + slot] + B.s_contrib[C + j];
-  B.L[2 * C + slot] = B.L[2 * C + slot] + B.s_contrib[2 * C + j];
+  const float sgn = ADJ ? -1.0f : 1.0f;
+  B.L[slot] = B.L[slot] + sgn * B.s_contrib[j];
+  B.L[C + slot] = B.L[C + slot] + sgn * B.s_contrib[C + j];
+  B.L[2 * C + slot] = B.L[2 * C + slot] + sgn * B.s_contrib[2 * C + j];
 }
 
 __global__ void __launch_bounds__(kWfBlock) wf_finalize(WfBuffers B, uint32_t n_paths, float* samples) {
@@ -215,21 +240,29 @@ __global__ void __launch_bounds__(kWfBlock) wf_finalize(WfBuffers B, uint32_t n_
 static inline unsigned grid_for(uint32_t n) { return (n + kWfBlock - 1) / kWfBlock; }
 
 cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                               const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s) {
+                               const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s,
+                               const float* primal) {
   DevRender S{geo, rd};
-  wf_generate<<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths);
+  if (primal)
+    wf_generate<true><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths, primal);
+  else
+    wf_generate<false><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s) {
+                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s, const DevAdjoint* A) {
   DevRender S{geo, rd};
-  wf_shade<<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur);
+  if (A)
+    wf_shade<true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, *A);
+  else
+    wf_shade<false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, DevAdjoint{});
   return cudaGetLastError();
 }
 
-cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s) {
-  wf_resolve<<<grid_for(B.capacity), kWfBlock, 0, s>>>(B);
+cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint) {
+  if (adjoint) wf_resolve<true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(B);
+  else wf_resolve<false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(B);
   return cudaGetLastError();
 }
 

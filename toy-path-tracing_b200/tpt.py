@@ -157,6 +157,17 @@ class RenderJob(C.Structure):
                 ("execution", C.c_uint32)]
 
 
+class AdjointDesc(C.Structure):
+    _fields_ = [("param_mask", C.c_uint32), ("fd_step", C.c_float)]
+
+
+# gradient layout per material (tpt.h TPT_GRAD_*) and parameter-group bits
+GRAD_PARAMS = 7
+GRAD_NAMES = ["base_color_r", "base_color_g", "base_color_b", "specular_roughness", "base_metalness",
+              "specular_ior", "coat_weight"]
+GRAD_MASK_BASE_COLOR, GRAD_MASK_ROUGHNESS, GRAD_MASK_METALNESS, GRAD_MASK_IOR, GRAD_MASK_COAT = 1, 2, 4, 8, 16
+GRAD_ALL = 31
+
 INTEGRATOR_MIS = 0
 EXEC_WAVEFRONT = 0
 EXEC_MEGAKERNEL = 1
@@ -207,6 +218,9 @@ EXPORTED_SYMBOLS = [
     "tpt_lut_dielectric_ec",
     "tpt_bsdf_eval_device",
     "tpt_bsdf_sample_device",
+    "tpt_scene_set_openpbr",
+    "tpt_adjoint_device",
+    "tpt_adjoint",
 ]
 
 
@@ -240,6 +254,9 @@ def _declare(L):
         "tpt_lut_dielectric_ec": (i32, [vp, vp, vp]),
         "tpt_bsdf_eval_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp, vp]),
         "tpt_bsdf_sample_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp]),
+        "tpt_scene_set_openpbr": (i32, [vp, vp, C.c_uint32, vp, vp, vp]),
+        "tpt_adjoint_device": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp, vp]),
+        "tpt_adjoint": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -413,6 +430,7 @@ class Scene:
         h = C.c_void_p()
         _check(lib().tpt_scene_upload(ctx.h, C.byref(desc), C.byref(h)), ctx)
         self.h = h
+        self.n_materials = len(materials or [])
 
     def light_tree(self):
         """(nodes[LIGHT_NODE_DTYPE], root) of the tree the scene uses."""
@@ -463,6 +481,33 @@ class Scene:
         _check(lib().tpt_bsdf_sample_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr), C.c_void_p(u_ptr),
                                             C.c_void_p(front_ptr), mode, C.c_void_p(out_ptr), _stream(stream)),
                self.ctx)
+
+    # -- material updates and the adjoint (no counterpart in the reference) ----
+    def set_openpbr(self, material_ids, materials, stream=None):
+        """`tpt_scene_set_openpbr`: new parameters (dicts) for OpenPBR materials."""
+        ids = np.ascontiguousarray(material_ids, np.uint32)
+        descs = (OpenPbrDesc * max(1, len(ids)))()
+        for k, m in enumerate(materials):
+            descs[k] = openpbr_desc(m)
+        _check(lib().tpt_scene_set_openpbr(self.ctx.h, self.h, len(ids), _p(ids), descs, _stream(stream)), self.ctx)
+
+    def adjoint_device(self, job, d_image_ptr: int, grad_ptr: int, mask: int = 0, fd_step: float = 0.0,
+                       stream=None):
+        """`tpt_adjoint_device`: dLoss/d(material parameters) (float64 [n_materials, 7]
+        at grad_ptr, n_materials = self.n_materials) from dLoss/dimage (float32
+        [h*w*3] at d_image_ptr)."""
+        ad = AdjointDesc(mask, fd_step)
+        _check(lib().tpt_adjoint_device(self.ctx.h, C.byref(job), C.byref(ad), C.c_void_p(d_image_ptr),
+                                        C.c_void_p(grad_ptr), _stream(stream)), self.ctx)
+
+    def adjoint(self, job, d_image: np.ndarray, mask: int = 0, fd_step: float = 0.0):
+        """`tpt_adjoint` with host arrays; returns float64 [n_materials, 7]."""
+        d = np.ascontiguousarray(d_image, np.float32).reshape(-1)
+        assert d.size == job.width * job.height * 3
+        out = np.zeros((self.n_materials, GRAD_PARAMS), np.float64)
+        ad = AdjointDesc(mask, fd_step)
+        _check(lib().tpt_adjoint(self.ctx.h, C.byref(job), C.byref(ad), _p(d), _p(out)), self.ctx)
+        return out
 
     def device_bytes(self) -> int:
         v = C.c_uint64()
@@ -519,3 +564,47 @@ class Scene:
             ),
             self.ctx,
         )
+
+
+# --------------------------------------------------------------------------
+def render_function():
+    """The forward/backward pair as a torch.autograd.Function (torch is only the
+    caller's tensor plumbing here; both passes run through the C ABI):
+
+        image = RenderFunction.apply(params, scene, job, material_ids, materials_of, mask)
+
+    params: float32 [n, k] tensor of material parameters (any layout the caller's
+    `materials_of(params_row) -> dict` maps to OpenPBR parameters); forward sets
+    the materials and renders; backward runs the path-replay adjoint and maps
+    the [n_materials, 7] gradient back through `grad_of(g7, row)` (default:
+    base_color rgb, roughness, metalness -> the first five slots)."""
+    import torch
+
+    class RenderFunction(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, params, scene, job, material_ids, materials_of, mask=0, fd_step=0.0):
+            rows = params.detach().cpu().numpy()
+            stream = torch.cuda.current_stream().cuda_stream
+            scene.set_openpbr(material_ids, [materials_of(r) for r in rows], stream=stream)
+            img = torch.empty(job.height * job.width * 3, dtype=torch.float32, device="cuda")
+            scene.render_device(job, img.data_ptr(), stream)
+            fctx.scene, fctx.job, fctx.ids, fctx.mask, fctx.step = scene, job, material_ids, mask, fd_step
+            fctx.k = params.shape[1]
+            fctx.device, fctx.dtype = params.device, params.dtype
+            return img.view(job.height, job.width, 3)
+
+        @staticmethod
+        def backward(fctx, grad_img):
+            import torch
+
+            scene, job = fctx.scene, fctx.job
+            g = grad_img.contiguous().float().view(-1)
+            n_mat = scene.n_materials
+            grad = torch.zeros(n_mat * GRAD_PARAMS, dtype=torch.float64, device="cuda")
+            scene.adjoint_device(job, g.data_ptr(), grad.data_ptr(), fctx.mask, fctx.step,
+                                 stream=torch.cuda.current_stream().cuda_stream)
+            grad = grad.view(n_mat, GRAD_PARAMS)[torch.as_tensor(fctx.ids, device="cuda").long()]
+            out = grad[:, :fctx.k].to(device=fctx.device, dtype=fctx.dtype)
+            return (out, None, None, None, None, None, None)
+
+    return RenderFunction

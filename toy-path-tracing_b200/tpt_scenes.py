@@ -199,3 +199,125 @@ def cornell_box(seed: int = 1, material: int = OPENPBR, light_strength: float = 
               "fov_y": float(np.float32(np.radians(38.0))), "exposure": 1.0}
     return {"meshes": meshes, "instances": instances, "materials": materials, "camera": camera,
             "angles": (float(a1), float(a2)), "seed": seed}
+
+
+# ---------------------------------------------------------------------------
+# Differentiable-render scene: the Cornell box with its five walls split into
+# 3 x 4 patches each (60 patches, every patch a 4 x 4 grid of quads) and each
+# box split into its sides and its caps (4 patches, faces 2 x 2 quads): 64
+# OpenPBR materials, one per patch, ~2k triangles, plus the emissive quad.
+# Parameters per material: base_color (3), specular_roughness, base_metalness
+# (base_diffuse_roughness 1, the other OpenPBR inputs at their defaults).
+
+N_PATCH_MATERIALS = 64
+
+
+def _grid_quad(p0, du, dv, n_u, n_v, normal):
+    """A planar patch p0 + s*du + t*dv, s, t in [0, 1], as an n_u x n_v grid of quads."""
+    p0, du, dv = (np.asarray(a, np.float64) for a in (p0, du, dv))
+    s = np.linspace(0.0, 1.0, n_u + 1)
+    t = np.linspace(0.0, 1.0, n_v + 1)
+    S, T = np.meshgrid(s, t, indexing="ij")
+    pos = p0[None, None] + S[..., None] * du + T[..., None] * dv
+    uv = np.stack([S, T], -1)
+    idx = []
+    for i in range(n_u):
+        for j in range(n_v):
+            a, b, c, d = i * (n_v + 1) + j, (i + 1) * (n_v + 1) + j, (i + 1) * (n_v + 1) + j + 1, i * (n_v + 1) + j + 1
+            idx += [a, b, c, a, c, d]
+    n = pos.reshape(-1, 3).shape[0]
+    return {"positions": pos.reshape(-1, 3).astype(np.float32),
+            "normals": np.tile(np.asarray(normal, np.float32), (n, 1)),
+            "uvs": uv.reshape(-1, 2).astype(np.float32), "indices": np.asarray(idx, np.uint32)}
+
+
+def _merge(meshes):
+    pos, nrm, uv, idx, base = [], [], [], [], 0
+    for m in meshes:
+        pos.append(m["positions"])
+        nrm.append(m["normals"])
+        uv.append(m["uvs"])
+        idx.append(m["indices"].astype(np.int64) + base)
+        base += m["positions"].shape[0]
+    return {"positions": np.concatenate(pos), "normals": np.concatenate(nrm), "uvs": np.concatenate(uv),
+            "indices": np.concatenate(idx).astype(np.uint32)}
+
+
+def patch_params(seed: int = 5, start: bool = False, perturb: float = 0.2):
+    """float32 [64, 5]: base_color rgb, specular_roughness, base_metalness.  The
+    true parameters are base_color U[0.1, 0.9]^3, roughness U[0.1, 1],
+    metalness U[0, 1]; start = true + U[-perturb, perturb], clipped."""
+    rng = np.random.default_rng(seed)
+    p = np.empty((N_PATCH_MATERIALS, 5), np.float64)
+    p[:, 0:3] = rng.uniform(0.1, 0.9, (N_PATCH_MATERIALS, 3))
+    p[:, 3] = rng.uniform(0.1, 1.0, N_PATCH_MATERIALS)
+    p[:, 4] = rng.uniform(0.0, 1.0, N_PATCH_MATERIALS)
+    if start:
+        p = p + np.random.default_rng(seed + 1).uniform(-perturb, perturb, p.shape)
+        p[:, 0:3] = np.clip(p[:, 0:3], 0.02, 0.98)
+        p[:, 3] = np.clip(p[:, 3], 0.05, 1.0)
+        p[:, 4] = np.clip(p[:, 4], 0.0, 1.0)
+    return p.astype(np.float32)
+
+
+def patch_material(p) -> dict:
+    return {"kind": OPENPBR, "base_color": np.asarray(p[0:3], np.float32), "specular_roughness": float(p[3]),
+            "base_metalness": float(p[4]), "base_diffuse_roughness": 1.0}
+
+
+def cornell_patches(seed: int = 5, params=None, light_strength: float = 15.0):
+    """The 64-patch Cornell box; `params` [64, 5] (default: the true ones)."""
+    if params is None:
+        params = patch_params(seed)
+    L, H = 1.5, 3.0
+    walls = [  # (corner, u edge, v edge, normal)
+        ((-L, 0, L), (2 * L, 0, 0), (0, 0, -2 * L), (0, 1, 0)),      # floor
+        ((-L, H, -L), (2 * L, 0, 0), (0, 0, 2 * L), (0, -1, 0)),     # ceiling
+        ((-L, 0, -L), (2 * L, 0, 0), (0, H, 0), (0, 0, 1)),          # back
+        ((-L, 0, L), (0, 0, -2 * L), (0, H, 0), (1, 0, 0)),          # left
+        ((L, 0, -L), (0, 0, 2 * L), (0, H, 0), (-1, 0, 0)),          # right
+    ]
+    meshes, instances = [], []
+    for w, (corner, du, dv, n) in enumerate(walls):
+        corner, du, dv = (np.asarray(a, np.float64) for a in (corner, du, dv))
+        for i in range(3):
+            for j in range(4):
+                p0 = corner + du * (i / 3.0) + dv * (j / 4.0)
+                meshes.append(_grid_quad(p0, du / 3.0, dv / 4.0, 4, 4, n))
+                instances.append(identity_instance(len(meshes) - 1, len(instances)))
+    # unit box [-0.5, 0.5] x [0, 1] x [-0.5, 0.5]: sides and caps, faces 2 x 2 quads
+    sides = _merge([
+        _grid_quad((0.5, 0, -0.5), (0, 0, 1), (0, 1, 0), 2, 2, (1, 0, 0)),
+        _grid_quad((-0.5, 0, 0.5), (0, 0, -1), (0, 1, 0), 2, 2, (-1, 0, 0)),
+        _grid_quad((0.5, 0, 0.5), (-1, 0, 0), (0, 1, 0), 2, 2, (0, 0, 1)),
+        _grid_quad((-0.5, 0, -0.5), (1, 0, 0), (0, 1, 0), 2, 2, (0, 0, -1)),
+    ])
+    caps = _merge([
+        _grid_quad((-0.5, 1, -0.5), (0, 0, 1), (1, 0, 0), 2, 2, (0, 1, 0)),
+        _grid_quad((-0.5, 0, 0.5), (0, 0, -1), (1, 0, 0), 2, 2, (0, -1, 0)),
+    ])
+    rng = np.random.default_rng(seed)
+    a1, a2 = rng.uniform(15.0, 20.0, 2)
+    meshes += [sides, caps]
+    ms, mc = len(meshes) - 2, len(meshes) - 1
+    for trs in (_trs((-0.55, 0.0, -0.45), a1, (0.9, 1.8, 0.9)), _trs((0.6, 0.0, 0.5), -a2, (0.9, 0.9, 0.9))):
+        instances.append(instance_matrix(ms, len(instances), trs))
+        instances.append(instance_matrix(mc, len(instances), trs))
+    assert len(instances) == N_PATCH_MATERIALS
+    meshes.append(_quad((-0.125, H - 0.01, -0.125), (0.125, H - 0.01, -0.125), (0.125, H - 0.01, 0.125),
+                        (-0.125, H - 0.01, 0.125), (0, -1, 0)))
+    instances.append(identity_instance(len(meshes) - 1, N_PATCH_MATERIALS))
+    materials = [patch_material(p) for p in params]
+    materials.append({"kind": EMISSIVE, "color": np.ones(3, np.float32), "strength": np.float32(light_strength)})
+    camera = {"eye": (0.0, 1.5, 6.8), "look_at": (0.0, 1.5, 0.0), "up": (0.0, 1.0, 0.0),
+              "fov_y": float(np.float32(np.radians(38.0))), "exposure": 1.0}
+    return {"meshes": meshes, "instances": instances, "materials": materials, "camera": camera,
+            "angles": (float(a1), float(a2)), "seed": seed, "params": np.asarray(params, np.float32)}
+
+
+def with_patch_params(scene: dict, params) -> dict:
+    """The same scene with its 64 patch materials set to `params` [64, 5]."""
+    out = dict(scene)
+    out["materials"] = [patch_material(p) for p in params] + [scene["materials"][-1]]
+    out["params"] = np.asarray(params, np.float32)
+    return out
