@@ -195,7 +195,7 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
     const uint32_t n = std::min(cp, npix - p0);
     if (job->execution == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
       cudaError_t e = launch_render(job->scene->geo, job->scene->render, L, samples, (uint64_t)p0 * L.spp,
-                                    (uint64_t)n * L.spp, ctx->d_err, ctx->num_sms, s);
+                                    (uint64_t)n * L.spp, ctx->d_err, ctx->num_sms, s, next_counter(ctx));
       if ((st = cuda_check(ctx, e, "render kernel launch"))) return st;
     } else {
       if ((st = render_wavefront(ctx, job, L, (uint64_t)p0 * L.spp, n * L.spp, samples, s))) return st;
@@ -220,7 +220,7 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
   if (job->execution == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT)
     return cuda_check(ctx,
                       launch_render(job->scene->geo, job->scene->render, L, out_samples, first, count, ctx->d_err,
-                                    ctx->num_sms, s),
+                                    ctx->num_sms, s, next_counter(ctx)),
                       "render kernel launch");
   const uint64_t step = 1ull << 22;
   for (uint64_t b = 0; b < count; b += step) {

@@ -91,8 +91,10 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
 unsigned long long* next_counter(tpt_context* ctx);
 
 // render_kernels.cu
+// `counter`: a work-distribution word (next_counter) the launch resets.
 cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P, float* samples,
-                          uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t stream);
+                          uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t stream,
+                          unsigned long long* counter);
 cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first_pixel, uint32_t n_pixels,
                               float exposure, float* image, cudaStream_t stream);
 // bdpt_kernels.cu (launch_render dispatches to it for TPT_INTEGRATOR_BDPT)

@@ -380,4 +380,27 @@ __device__ __forceinline__ void trace_ray(const DevGeometry& G, Stack& st, float
   res = s.res;
 }
 
+// trace_ray for lanes that trace together: the lanes in `act` (all of which
+// call this) step through interior nodes together until each faces a leaf,
+// then test their leaves together ("while-while"), so the warp runs one code
+// path at a time.  Each ray's own visit order is unchanged.
+template <int MODE, class Stack>
+__device__ __forceinline__ void trace_ray_ww(const DevGeometry& G, Stack& st, unsigned act, float ox, float oy,
+                                             float oz, float dx, float dy, float dz, float t_max, TraceResult& res,
+                                             uint32_t* err) {
+  TravState s;
+  TraceCounters c;
+  trav_init(G, s, ox, oy, oz, dx, dy, dz, t_max);
+  for (;;) {
+    for (;;) {
+      const bool want = !(s.next & kLeafBit);
+      if (!__any_sync(act, want)) break;
+      if (want) node_step<false>(G, s, st, c, err);
+    }
+    if (s.next != kNone) leaf_step<MODE, false>(G, s, st, c, err);
+    if (!__any_sync(act, s.next != kNone)) break;
+  }
+  res = s.res;
+}
+
 }  // namespace tpt

@@ -71,7 +71,8 @@ extern "C" tpt_status tpt_render_device_noalloc(tpt_context* ctx, const tpt_rend
   float* scratch = nullptr;
   if ((st = scratch_for(ctx, ctx->device, &scratch))) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  e = launch_render(job->scene->geo, job->scene->render, L, scratch, 0, n_paths, ctx->d_err, ctx->num_sms, s);
+  e = launch_render(job->scene->geo, job->scene->render, L, scratch, 0, n_paths, ctx->d_err, ctx->num_sms, s,
+                    next_counter(ctx));
   if ((st = cuda_check(ctx, e, "render kernel launch"))) return st;
   e = launch_accumulate(scratch, L.spp, 0, L.width * L.height, L.cam.exposure, out_rgb, s);
   return cuda_check(ctx, e, "accumulate kernel launch");
