@@ -294,6 +294,14 @@ typedef struct tpt_render_job {
   uint32_t execution; /* tpt_execution; both give the same image bit for bit */
 } tpt_render_job;
 
+/* Path slots of the wavefront pipeline's queues: a render is processed in
+ * chunks of at most this many paths (0 = the default 2^22; otherwise
+ * [1024, 2^24]).  Larger chunks fill the GPU better, smaller ones hold less
+ * device memory (about 250 bytes per slot).  tpt_autotune picks it per
+ * workload.  Results do not depend on it. */
+tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots);
+uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx);
+
 /* Renders each job into out_rgb[j] (host, width*height*3 floats, row-major,
  * pixel = y*width + x): per pixel the running mean of `spp` samples in sample
  * order, times exposure — the raw linear buffer main.rs writes before output. */
@@ -305,6 +313,15 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
  * (parity testing and sample-level consumers). */
 tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first, uint64_t count,
                                      float* out_samples, void* stream);
+
+/* Batched rendering: n_jobs MIS jobs (any mix of scenes, cameras,
+ * resolutions, spp and depths; `execution` is not read) through one wavefront
+ * launch sequence, job j into the device image out_rgb[j] (width*height*3
+ * floats), asynchronous on `stream`.  Each image equals tpt_render_device's for
+ * the same job bit for bit.  No counterpart in the reference, which renders one
+ * image per run (main.rs:99-126). */
+tpt_status tpt_render_batch_device(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb,
+                                   void* stream);
 
 /* Allocation-free variant of tpt_render_device, for callers that cannot call
  * cudaMalloc while they render (work recorded in a CUDA stream capture, hosts

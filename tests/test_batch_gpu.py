@@ -1,0 +1,78 @@
+"""Batched rendering (tpt_render_batch_device): many jobs of different scenes,
+cameras, resolutions, spp and depths through one wavefront launch sequence.
+
+Bar: every job's image equals tpt_render_device's for the same job bit for bit
+(the per-path arithmetic and the in-order per-pixel accumulation are the same),
+with the default capacity and with a small capacity that splits jobs across
+chunks and puts several jobs in one chunk.
+"""
+import numpy as np
+import pytest
+
+import tpt
+import tpt_scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mixed(ctx):
+    scenes = []
+    for sc in (tpt_scenes.cornell_box(1, tpt_scenes.LAMBERT), tpt_scenes.cornell_box(2, tpt_scenes.OPENPBR),
+               tpt_scenes.grid_scene(seed=7, n_side=6, tris_per_object=200, n_materials=12, n_emissive_tris=40)):
+        scenes.append((sc, tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])))
+    shapes = [(0, 40, 30, 8, 8), (1, 33, 17, 4, 5), (2, 64, 48, 16, 12), (0, 16, 16, 1, 3), (2, 25, 31, 3, 16),
+              (1, 48, 48, 32, 8)]
+    jobs = [scenes[i][1].job(scenes[i][0]["camera"], w, h, spp, depth) for i, w, h, spp, depth in shapes]
+    yield jobs
+    for _, s in scenes:
+        s.close()
+
+
+def _render_each(ctx, jobs):
+    import torch
+
+    outs = []
+    st = torch.cuda.current_stream().cuda_stream
+    for j in jobs:
+        img = torch.empty(j.width * j.height * 3, device="cuda")
+        tpt.lib().tpt_render_device(ctx.h, tpt.C.byref(j), tpt.C.c_void_p(img.data_ptr()), tpt.C.c_void_p(st))
+        outs.append(img)
+    torch.cuda.synchronize()
+    return [o.cpu().numpy() for o in outs]
+
+
+def _render_batch(ctx, jobs):
+    import torch
+
+    outs = [torch.full((j.width * j.height * 3,), -1.0, device="cuda") for j in jobs]
+    ctx.render_batch_device(jobs, [o.data_ptr() for o in outs], torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return [o.cpu().numpy() for o in outs]
+
+
+@pytest.mark.parametrize("capacity", [0, 4096], ids=["default", "small_chunks"])
+def test_batch_equals_single_jobs(ctx, mixed, capacity):
+    ctx.wavefront_capacity = 0
+    ref = _render_each(ctx, mixed)
+    ctx.wavefront_capacity = capacity
+    try:
+        got = _render_batch(ctx, mixed)
+    finally:
+        ctx.wavefront_capacity = 0
+    for a, b in zip(got, ref):
+        assert np.all(np.isfinite(a)) and b.max() > 0
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_capacity_does_not_change_single_renders(ctx, mixed):
+    ref = _render_each(ctx, mixed[:3])
+    ctx.wavefront_capacity = 2048
+    try:
+        got = _render_each(ctx, mixed[:3])
+    finally:
+        ctx.wavefront_capacity = 0
+    for a, b in zip(got, ref):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    with pytest.raises(tpt.TptError):
+        ctx.wavefront_capacity = 100

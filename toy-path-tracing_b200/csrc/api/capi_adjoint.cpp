@@ -153,7 +153,7 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   A.scale = L.cam.exposure / (float)L.spp;
   A.mask = mask;
   const uint32_t npix = L.width * L.height;
-  const uint32_t cp = chunk_pixels(L);
+  const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
   if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
   float* samples = (float*)ctx->d_scratch;
   for (uint32_t p0 = 0; p0 < npix; p0 += cp) {

@@ -87,8 +87,9 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   if (ctx->wf.capacity >= capacity && ctx->d_wf) return TPT_OK;
   const size_t C = capacity;
   // float planes: beta 3, L 3, prev 7, q_ray 2*7, h_t 1, h_bary 3, s_ray 7, s_contrib 3, s_t 1
-  // u32 planes: prev_mat, depth, q_slot 2, h_tri, h_inst, s_slot, s_target 2, s_tri, s_inst
-  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1;
+  // u32 planes: prev_mat, depth, q_slot 2, h_tri, h_inst, s_slot, s_target 2, s_tri, s_inst,
+  // job, q_job 2, s_job
+  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4;
   const size_t bytes = planes * C * 4 + 256;
   if (ctx->d_wf) {
     cudaDeviceSynchronize();
@@ -128,6 +129,10 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   B.s_tri = (int32_t*)take(1);
   B.s_inst = (int32_t*)take(1);
   B.s_t = (float*)take(1);
+  B.job = (uint32_t*)take(1);
+  B.q_job[0] = (uint32_t*)take(1);
+  B.q_job[1] = (uint32_t*)take(1);
+  B.s_job = (uint32_t*)take(1);
   B.counts = (uint32_t*)p;
   return TPT_OK;
 }
@@ -163,10 +168,11 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
 }
 
 // Pixels per chunk: the per-sample buffer stays below 1 GiB and a chunk has at
-// most 2^22 paths (the wavefront arena's slot count).
-uint32_t chunk_pixels(const RenderLaunch& L) {
+// most `capacity` paths (the wavefront arena's slot count; 0 = 2^22).
+uint32_t chunk_pixels(const RenderLaunch& L, uint32_t capacity) {
+  if (capacity == 0) capacity = 1u << 22;
   const uint64_t per_pixel = 12ull * L.spp;
-  uint64_t n = std::min<uint64_t>((1ull << 30) / per_pixel, std::max<uint64_t>(1, (1ull << 22) / L.spp));
+  uint64_t n = std::min<uint64_t>((1ull << 30) / per_pixel, std::max<uint64_t>(1, (uint64_t)capacity / L.spp));
   const uint64_t total = (uint64_t)L.width * L.height;
   return (uint32_t)std::max<uint64_t>(1, std::min(n, total));
 }
@@ -179,6 +185,18 @@ tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, Ren
 
 extern "C" {
 
+tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  if (slots != 0 && (slots < 1024 || slots > (1u << 24)))
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "wavefront capacity must be 0 or in [1024, 2^24]");
+  ctx->batch_capacity = slots;
+  return TPT_OK;
+}
+
+uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx) {
+  return ctx ? (ctx->batch_capacity ? ctx->batch_capacity : (1u << 22)) : 0u;
+}
+
 tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (!out_rgb) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
@@ -188,7 +206,7 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   const uint32_t npix = L.width * L.height;
-  const uint32_t cp = chunk_pixels(L);
+  const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
   if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
   float* samples = (float*)ctx->d_scratch;
   for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
@@ -222,7 +240,7 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
                       launch_render(job->scene->geo, job->scene->render, L, out_samples, first, count, ctx->d_err,
                                     ctx->num_sms, s, next_counter(ctx)),
                       "render kernel launch");
-  const uint64_t step = 1ull << 22;
+  const uint64_t step = ctx->batch_capacity ? ctx->batch_capacity : 1ull << 22;
   for (uint64_t b = 0; b < count; b += step) {
     st = render_wavefront(ctx, job, L, first + b, (uint32_t)std::min(step, count - b), out_samples + 3 * b, s);
     if (st) return st;

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../../include/tpt.h"
+#include "../device/batch_types.h"
 #include "../device/dev_types.cuh"
 #include "../device/render_types.h"
 #include "../host/host_scene.h"
@@ -36,6 +37,11 @@ struct tpt_context {
   void* d_wf = nullptr;
   size_t d_wf_bytes = 0;
   tpt::WfBuffers wf{};
+  // batched renders: device job table (grown on demand) and the wavefront
+  // capacity (path slots per chunk; 0 = 2^22)
+  tpt::DevJob* d_jobs = nullptr;
+  size_t d_jobs_cap = 0;
+  uint32_t batch_capacity = 0;
   // OpenPBR tables (built on the GPU on first use, kept until destroy)
   std::map<uint32_t, float*> da_tables;  // directional albedo per eta (bit pattern)
   float* d_cec_e = nullptr;              // conductor E (64 x 64)
@@ -85,7 +91,8 @@ tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream);
 cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t stream,
-                                    uint32_t* node_tests, uint32_t* tri_tests, const uint32_t* n_dev = nullptr);
+                                    uint32_t* node_tests, uint32_t* tri_tests, const uint32_t* n_dev = nullptr,
+                                    const DevJob* jobs = nullptr, const uint32_t* ray_job = nullptr);
 
 // A work counter slot for the next launch (ring of kCounterSlots per context).
 unsigned long long* next_counter(tpt_context* ctx);
@@ -106,8 +113,8 @@ tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, Ren
 // The context's per-sample scratch (grown on demand) and wavefront arena.
 tpt_status ensure_scratch(tpt_context* ctx, size_t bytes);
 tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity);
-// Pixels per chunk of a job: at most 2^22 paths and 1 GiB of samples.
-uint32_t chunk_pixels(const RenderLaunch& L);
+// Pixels per chunk of a job: at most `capacity` paths (0 = 2^22) and 1 GiB of samples.
+uint32_t chunk_pixels(const RenderLaunch& L, uint32_t capacity);
 // Paths [first, first + n) through the wavefront stages (forward: radiance into
 // samples; with A: the adjoint replay of samples' paths, gradients to A->grad).
 tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
@@ -123,7 +130,17 @@ cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, con
                             const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s,
                             const DevAdjoint* A = nullptr);
 cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint = false);
+// Batched stages: slot i is global path first_path + i of the jobs' index space.
+cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const WfBuffers& B, uint64_t first_path,
+                                     uint32_t n_paths, cudaStream_t s);
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, uint64_t first_path, int cur,
+                                  cudaStream_t s);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
+
+// capi_batch.cpp: jobs (MIS) through one wavefront launch sequence; out_rgb are
+// device images; capacity = path slots per chunk (0 = 2^22).
+tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb,
+                        cudaStream_t s, uint32_t capacity);
 
 // capi_openpbr.cpp: the context's OpenPBR tables, built on first use.
 tpt_status ensure_ec_tables(tpt_context* ctx);

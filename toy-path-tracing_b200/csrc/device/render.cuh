@@ -7,6 +7,7 @@
 // cones are not carried: they only feed texture filtering and specular
 // differentials, which no material in scope reads.
 #pragma once
+#include "batch_types.h"
 #include "lights.cuh"
 #include "openpbr.cuh"
 #include "render_types.h"
@@ -15,11 +16,6 @@
 #include "vmath.cuh"
 
 namespace tpt {
-
-struct DevRender {
-  DevGeometry geo;
-  DevRenderData d;
-};
 
 struct Ray3 {
   V3 o, d;

@@ -190,6 +190,11 @@ struct WfBuffers {
   int32_t* s_inst;
   float* s_t;
   uint32_t* counts;   // [0], [1]: ray queue lengths, [2]: shadow queue length
+  // batched renders only: the job of each slot, of each queued ray and of
+  // each shadow ray (index into the batch's DevJob array)
+  uint32_t* job;
+  uint32_t* q_job[2];
+  uint32_t* s_job;
 };
 
 }  // namespace tpt

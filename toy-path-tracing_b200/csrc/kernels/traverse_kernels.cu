@@ -9,6 +9,9 @@
 // time without changing any ray's own visit order.
 // Traversal stacks: 32 entries per thread in shared memory, spilling to local
 // memory beyond that (total depth 128, as the reference).
+// The batched instantiation (BATCH) serves rays of many scenes in one launch:
+// ray i belongs to job ray_job[i], and a lane loads that job's geometry record
+// when it takes the ray.
 #include "../api/internal.h"
 #include "../device/trace.cuh"
 
@@ -23,13 +26,16 @@ constexpr int kShStack = 32;
 #define TPT_REFILL_MIN 12  // finished lanes that end the node phase early for a refill
 #endif
 
-template <int MODE, bool STATS, bool BARY>
+template <int MODE, bool STATS, bool BARY, bool BATCH>
 __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
     traverse_kernel(DevGeometry geo, const float* __restrict__ rays, uint64_t rs, uint64_t n, uint64_t bs,
                     int32_t* __restrict__ prim, float* __restrict__ tout, int32_t* __restrict__ inst,
                     float* __restrict__ bary, uint32_t* __restrict__ node_tests, uint32_t* __restrict__ tri_tests,
-                    unsigned long long* __restrict__ counter, const uint32_t* __restrict__ n_dev, uint32_t* err) {
+                    unsigned long long* __restrict__ counter, const uint32_t* __restrict__ n_dev, uint32_t* err,
+                    const DevJob* __restrict__ jobs, const uint32_t* __restrict__ ray_job) {
   if (n_dev) n = *n_dev;  // queue length produced on the device (wavefront stages)
+  DevGeometry lane_geo;  // BATCH: the scene of this lane's ray
+  const DevGeometry& G = BATCH ? lane_geo : geo;
   __shared__ uint32_t stack_sh[kShStack * kBlock];
   SplitStack<kShStack> st;
   st.sh = stack_sh + threadIdx.x;
@@ -57,7 +63,8 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
           const float ox = __ldcs(rays + i), oy = __ldcs(rays + rs + i), oz = __ldcs(rays + 2 * rs + i);
           const float dx = __ldcs(rays + 3 * rs + i), dy = __ldcs(rays + 4 * rs + i), dz = __ldcs(rays + 5 * rs + i);
           const float tmax = MODE == 0 ? __int_as_float(0x7f800000) : __ldcs(rays + 6 * rs + i);
-          trav_init(geo, s, ox, oy, oz, dx, dy, dz, tmax);
+          if (BATCH) lane_geo = jobs[__ldg(ray_job + i)].render.geo;
+          trav_init(G, s, ox, oy, oz, dx, dy, dz, tmax);
           if (STATS) { c.nodes = 0; c.tris = 0; }
         } else {
           ray = -2;
@@ -74,13 +81,13 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
       if (!__any_sync(0xffffffffu, want)) break;
       if (__popc(__ballot_sync(0xffffffffu, active && s.next == kNone)) >= TPT_REFILL_MIN) break;
       if (want) {
-        node_step<STATS>(geo, s, st, c, err);
+        node_step<STATS>(G, s, st, c, err);
         moved = true;
       }
     }
     // phase B: one leaf / instance entry per lane
     if (active && s.next != kNone && (s.next & kLeafBit)) {
-      leaf_step<MODE, STATS>(geo, s, st, c, err);
+      leaf_step<MODE, STATS>(G, s, st, c, err);
       moved = true;
     }
     if (active && s.next == kNone) {
@@ -111,16 +118,16 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
   }
 }
 
-template <int MODE, bool STATS, bool BARY>
+template <int MODE, bool STATS, bool BARY, bool BATCH>
 static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, uint64_t bs,
                             int32_t* prim, float* t, int32_t* inst, float* bary, uint32_t* nt, uint32_t* tt,
                             unsigned long long* counter, const uint32_t* n_dev, uint32_t* err, int num_sms,
-                            cudaStream_t s) {
+                            cudaStream_t s, const DevJob* jobs, const uint32_t* ray_job) {
   if (n == 0) return cudaSuccess;
   static int blocks_per_sm = 0;
   if (blocks_per_sm == 0) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, traverse_kernel<MODE, STATS, BARY>,
-                                                                  kBlock, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &blocks_per_sm, traverse_kernel<MODE, STATS, BARY, BATCH>, kBlock, 0);
     if (e != cudaSuccess || blocks_per_sm <= 0) blocks_per_sm = 4;
   }
   uint64_t blocks = (uint64_t)num_sms * blocks_per_sm;
@@ -128,27 +135,33 @@ static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t 
   if (blocks > need) blocks = need;
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
-  traverse_kernel<MODE, STATS, BARY>
-      <<<(unsigned)blocks, kBlock, 0, s>>>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err);
+  traverse_kernel<MODE, STATS, BARY, BATCH><<<(unsigned)blocks, kBlock, 0, s>>>(
+      geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, jobs, ray_job);
   return cudaGetLastError();
 }
 
 cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, int mode,
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
-                                    uint32_t* nt, uint32_t* tt, const uint32_t* n_dev) {
+                                    uint32_t* nt, uint32_t* tt, const uint32_t* n_dev, const DevJob* jobs,
+                                    const uint32_t* ray_job) {
   const bool stats = nt != nullptr;
   const bool b = bary != nullptr;
-#define TPT_L(M, S, B) \
-  launch_t<M, S, B>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, num_sms, s)
-  if (mode == 0) {
-    if (stats) return TPT_L(0, true, false);
-    if (b) return TPT_L(0, false, true);
-    return TPT_L(0, false, false);
+#define TPT_L(M, S, B, J) \
+  launch_t<M, S, B, J>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, num_sms, s, jobs, ray_job)
+  if (jobs) {  // batched wavefront: closest hit, with or without barycentrics
+    if (mode != 0 || stats) return cudaErrorInvalidValue;
+    if (b) return TPT_L(0, false, true, true);
+    return TPT_L(0, false, false, true);
   }
-  if (stats) return TPT_L(1, true, false);
-  if (b) return TPT_L(1, false, true);
-  return TPT_L(1, false, false);
+  if (mode == 0) {
+    if (stats) return TPT_L(0, true, false, false);
+    if (b) return TPT_L(0, false, true, false);
+    return TPT_L(0, false, false, false);
+  }
+  if (stats) return TPT_L(1, true, false, false);
+  if (b) return TPT_L(1, false, true, false);
+  return TPT_L(1, false, false, false);
 #undef TPT_L
 }
 

@@ -14,6 +14,13 @@
 // Stage launch shapes do not depend on queue lengths (those live on the
 // device), so one bounce is a fixed launch sequence that a CUDA graph replays.
 //
+// The batched instantiation (BATCH = true) runs many jobs (scenes, cameras,
+// resolutions, spp, depths) through one launch sequence: slot i of a chunk is
+// global path first_path + i of the batch, whose job is found by binary search
+// over the jobs' path bases; every slot, queued ray and shadow ray carries its
+// job index, and each stage reads the job's scene and launch record from the
+// DevJob array instead of its kernel parameters.
+//
 // The adjoint instantiation (ADJ = true) replays the same paths with the
 // radiance planes holding R, the part of the path's radiance still to come:
 // generate starts R at the path's radiance from the forward pass, shade and
@@ -38,10 +45,22 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
-template <bool ADJ>
-__global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunch P, WfBuffers B,
+// Job of global path g: the last job whose path_base <= g (jobs sorted by path_base).
+__device__ __forceinline__ uint32_t job_of_path(const DevJob* __restrict__ jobs, uint32_t n_jobs, uint64_t g) {
+  uint32_t lo = 0, hi = n_jobs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].path_base <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <bool ADJ, bool BATCH>
+__global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaunch P0, WfBuffers B,
                                                         uint64_t first_path, uint32_t n_paths,
-                                                        const float* __restrict__ primal) {
+                                                        const float* __restrict__ primal,
+                                                        const DevJob* __restrict__ jobs, uint32_t n_jobs) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
     B.counts[0] = n_paths;
@@ -50,7 +69,9 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunc
   }
   if (i >= n_paths) return;
   const uint32_t C = B.capacity;
-  const uint64_t path = first_path + i;
+  const uint32_t jb = BATCH ? job_of_path(jobs, n_jobs, first_path + i) : 0u;
+  const RenderLaunch& P = BATCH ? jobs[jb].P : P0;
+  const uint64_t path = first_path + i - (BATCH ? jobs[jb].path_base : 0ull);
   const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
   const uint32_t px = pixel % P.width, py = pixel / P.width;
   PathSamplerDev ps;
@@ -69,6 +90,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunc
   q[5 * C + i] = d.z;
   q[6 * C + i] = __int_as_float(0x7f800000);
   B.q_slot[0][i] = i;
+  if (BATCH) {
+    B.job[i] = jb;
+    B.q_job[0][i] = jb;
+  }
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     B.beta[k * C + i] = 1.0f;
@@ -78,9 +103,9 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S, RenderLaunc
 }
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
-template <bool ADJ>
-__global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P, WfBuffers B, uint64_t first_path,
-                                                     int cur, DevAdjoint A) {
+template <bool ADJ, bool BATCH>
+__global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, uint64_t first_path,
+                                                     int cur, DevAdjoint A, const DevJob* __restrict__ jobs) {
   __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[cur]) return;
@@ -89,6 +114,9 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
   float grad_v[ADJ ? kGradParams : 1];
   const uint32_t C = B.capacity;
   const uint32_t slot = B.q_slot[cur][j];
+  const uint32_t jb = BATCH ? B.job[slot] : 0u;
+  const DevRender& S = BATCH ? jobs[jb].render : S0;
+  const RenderLaunch& P = BATCH ? jobs[jb].P : P0;
   const uint32_t d = B.depth[slot];
   bool push_next = false, push_shadow = false;
   V3 next_o, next_d;
@@ -127,7 +155,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
       }
     }
     if (d < P.max_depth && m.kind != kDevEmissive) {
-      const uint64_t path = first_path + slot;
+      const uint64_t path = first_path + slot - (BATCH ? jobs[jb].path_base : 0ull);
       const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
       PathSamplerDev ps;
       ps.init(pixel % P.width, pixel / P.width, sample, P.log2_spp, P.n_base4_digits);
@@ -191,6 +219,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
     q[5 * C + qn] = next_d.z;
     q[6 * C + qn] = __int_as_float(0x7f800000);
     B.q_slot[nxt][qn] = slot;
+    if (BATCH) B.q_job[nxt][qn] = jb;
   }
   if (push_shadow) {
     float* q = B.s_ray;
@@ -202,6 +231,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S, RenderLaunch P
     q[5 * C + qs] = dp.wi.z;
     q[6 * C + qs] = __int_as_float(0x7f800000);
     B.s_slot[qs] = slot;
+    if (BATCH) B.s_job[qs] = jb;
     B.s_target[qs] = dp.inst;
     B.s_target[C + qs] = dp.tri;
     B.s_contrib[qs] = dp.contrib.x;
@@ -244,9 +274,11 @@ cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, 
                                const float* primal) {
   DevRender S{geo, rd};
   if (primal)
-    wf_generate<true><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths, primal);
+    wf_generate<true, false><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths,
+                                                                                  primal, nullptr, 0);
   else
-    wf_generate<false><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths, nullptr);
+    wf_generate<false, false><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(S, P, B, first_path, n_paths,
+                                                                                   nullptr, nullptr, 0);
   return cudaGetLastError();
 }
 
@@ -254,9 +286,23 @@ cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, con
                             const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s, const DevAdjoint* A) {
   DevRender S{geo, rd};
   if (A)
-    wf_shade<true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, *A);
+    wf_shade<true, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, *A, nullptr);
   else
-    wf_shade<false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, DevAdjoint{});
+    wf_shade<false, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, DevAdjoint{}, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const WfBuffers& B, uint64_t first_path,
+                                     uint32_t n_paths, cudaStream_t s) {
+  wf_generate<false, true><<<grid_for(std::max(n_paths, 1u)), kWfBlock, 0, s>>>(
+      DevRender{}, RenderLaunch{}, B, first_path, n_paths, nullptr, jobs, n_jobs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, uint64_t first_path, int cur,
+                                  cudaStream_t s) {
+  wf_shade<false, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(DevRender{}, RenderLaunch{}, B, first_path, cur,
+                                                                  DevAdjoint{}, jobs);
   return cudaGetLastError();
 }
 

@@ -219,6 +219,9 @@ EXPORTED_SYMBOLS = [
     "tpt_bsdf_eval_device",
     "tpt_bsdf_sample_device",
     "tpt_scene_set_openpbr",
+    "tpt_render_batch_device",
+    "tpt_context_set_wavefront_capacity",
+    "tpt_context_wavefront_capacity",
     "tpt_adjoint_device",
     "tpt_adjoint",
 ]
@@ -255,6 +258,9 @@ def _declare(L):
         "tpt_bsdf_eval_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp, vp]),
         "tpt_bsdf_sample_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp]),
         "tpt_scene_set_openpbr": (i32, [vp, vp, C.c_uint32, vp, vp, vp]),
+        "tpt_render_batch_device": (i32, [vp, vp, i32, vp, vp]),
+        "tpt_context_set_wavefront_capacity": (i32, [vp, C.c_uint32]),
+        "tpt_context_wavefront_capacity": (C.c_uint32, [vp]),
         "tpt_adjoint_device": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp, vp]),
         "tpt_adjoint": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp]),
     }
@@ -295,6 +301,20 @@ class Context:
         if getattr(self, "h", None):
             lib().tpt_context_destroy(self.h)
             self.h = None
+
+    @property
+    def wavefront_capacity(self) -> int:
+        return int(lib().tpt_context_wavefront_capacity(self.h))
+
+    @wavefront_capacity.setter
+    def wavefront_capacity(self, slots: int):
+        _check(lib().tpt_context_set_wavefront_capacity(self.h, int(slots)), self)
+
+    def render_batch_device(self, jobs, out_ptrs, stream=None):
+        """`tpt_render_batch_device`: jobs (RenderJob list) into device images."""
+        arr = (RenderJob * max(1, len(jobs)))(*jobs)
+        outs = (C.c_void_p * max(1, len(jobs)))(*[C.c_void_p(p) for p in out_ptrs])
+        _check(lib().tpt_render_batch_device(self.h, arr, len(jobs), outs, _stream(stream)), self)
 
     # -- OpenPBR tables (built on the GPU on first use) -------------------------
     def lut_dielectric_albedo(self, eta: float) -> np.ndarray:

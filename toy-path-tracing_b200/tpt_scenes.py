@@ -321,3 +321,127 @@ def with_patch_params(scene: dict, params) -> dict:
     out["materials"] = [patch_material(p) for p in params] + [scene["materials"][-1]]
     out["params"] = np.asarray(params, np.float32)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Large instanced scene: an n_side x n_side grid of tessellated spheres, boxes
+# and tori on a ground plane, lit by small emissive quads.  Each object is an
+# instance of one of three prototype meshes (about tris_per_object triangles
+# each) with its own scale and rotation, and one of n_materials OpenPBR
+# materials (base_color U[0,1]^3, specular_roughness U[0.05,1], metalness
+# Bernoulli(0.3), specular_ior 1.5, coat_weight U[0,1], coat_roughness
+# U[0,0.3]).  Emitters: n_emissive_tris / 2 downward-facing quads above the
+# grid, each with one of 64 emissive materials of strength log-U[1, 100].
+# The defaults give ~2.1M triangles, 10,000 emissive triangles and 256
+# materials; smaller settings give the batched-render variants.
+
+def _uv_sphere_mesh(n_theta: int):
+    n_phi = 2 * n_theta
+    pos, uv, idx = uv_sphere(n_phi, n_theta)
+    return {"positions": pos.astype(np.float32), "normals": pos.astype(np.float32), "uvs": uv.astype(np.float32),
+            "indices": idx}
+
+
+def _torus_mesh(n_v: int, R: float = 0.7, r: float = 0.3):
+    n_u = 2 * n_v
+    u = np.linspace(0.0, 2 * np.pi, n_u + 1)
+    v = np.linspace(0.0, 2 * np.pi, n_v + 1)
+    U, V = np.meshgrid(u, v, indexing="ij")
+    pos = np.stack([(R + r * np.cos(V)) * np.cos(U), r * np.sin(V) + r, (R + r * np.cos(V)) * np.sin(U)], -1)
+    nrm = np.stack([np.cos(V) * np.cos(U), np.sin(V), np.cos(V) * np.sin(U)], -1)
+    uv = np.stack([U / (2 * np.pi), V / (2 * np.pi)], -1)
+    idx = []
+    w = n_v + 1
+    for i in range(n_u):
+        for j in range(n_v):
+            a, b, c, d = i * w + j, (i + 1) * w + j, (i + 1) * w + j + 1, i * w + j + 1
+            idx += [a, c, b, a, d, c]
+    return {"positions": pos.reshape(-1, 3).astype(np.float32), "normals": nrm.reshape(-1, 3).astype(np.float32),
+            "uvs": uv.reshape(-1, 2).astype(np.float32), "indices": np.asarray(idx, np.uint32)}
+
+
+def _box_mesh(k: int):
+    faces = []
+    for axis in range(3):
+        for sgn in (1.0, -1.0):
+            n = np.zeros(3)
+            n[axis] = sgn
+            a, b = [(axis + 1) % 3, (axis + 2) % 3]
+            du, dv = np.zeros(3), np.zeros(3)
+            du[a], dv[b] = 1.0, 1.0
+            if sgn < 0:
+                du, dv = dv, du
+            corner = 0.5 * n - 0.5 * du - 0.5 * dv + np.array([0.0, 0.5, 0.0])
+            faces.append(_grid_quad(corner, du, dv, k, k, n))
+    return _merge(faces)
+
+
+def grid_scene(seed: int = 3, n_side: int = 32, tris_per_object: int = 2048, n_materials: int = 256,
+               n_emissive_tris: int = 10000, ground: bool = True):
+    rng = np.random.default_rng(seed)
+    nt = max(2, int(round(np.sqrt(tris_per_object / 4.0))))
+    kb = max(1, int(round(np.sqrt(tris_per_object / 12.0))))
+    meshes = [_uv_sphere_mesh(nt), _box_mesh(kb), _torus_mesh(nt)]
+    spacing = 3.0
+    extent = n_side * spacing
+    materials = []
+    for _ in range(n_materials):
+        materials.append({"kind": OPENPBR, "base_color": rng.uniform(0.0, 1.0, 3).astype(np.float32),
+                          "specular_roughness": float(rng.uniform(0.05, 1.0)),
+                          "base_metalness": float(rng.random() < 0.3), "specular_ior": 1.5,
+                          "coat_weight": float(rng.uniform(0.0, 1.0)), "coat_roughness": float(rng.uniform(0.0, 0.3))})
+    n_emit_mats = 64
+    emit0 = len(materials)
+    for _ in range(n_emit_mats):
+        materials.append({"kind": EMISSIVE, "color": np.ones(3, np.float32),
+                          "strength": np.float32(np.exp(rng.uniform(np.log(1.0), np.log(100.0))))})
+    instances = []
+    for i in range(n_side):
+        for j in range(n_side):
+            proto = int(rng.integers(0, 3))
+            s = float(rng.uniform(0.8, 1.4))
+            c = np.array([(i + 0.5) * spacing - 0.5 * extent, 0.0, (j + 0.5) * spacing - 0.5 * extent])
+            if proto == 0:
+                c[1] = s  # unit sphere centred at the origin: rest it on the ground
+            instances.append(instance_matrix(proto, int(rng.integers(0, n_materials)),
+                                             _trs(c, float(rng.uniform(0, 360)), (s, s, s))))
+    # emitters: 0.5 x 0.5 quads facing down, 6 to 10 units above the ground
+    meshes.append(_quad((-0.25, 0, -0.25), (0.25, 0, -0.25), (0.25, 0, 0.25), (-0.25, 0, 0.25), (0, -1, 0)))
+    quad = len(meshes) - 1
+    for _ in range(max(1, n_emissive_tris // 2)):
+        c = np.array([rng.uniform(-0.5, 0.5) * extent, rng.uniform(6.0, 10.0), rng.uniform(-0.5, 0.5) * extent])
+        instances.append(instance_matrix(quad, emit0 + int(rng.integers(0, n_emit_mats)), _trs(c, 0.0, (1, 1, 1))))
+    if ground:
+        g = 0.5 * extent + 10.0
+        meshes.append(_quad((-g, 0, g), (g, 0, g), (g, 0, -g), (-g, 0, -g), (0, 1, 0)))
+        instances.append(identity_instance(len(meshes) - 1, int(rng.integers(0, n_materials))))
+    tris = sum(meshes[inst["mesh"]]["indices"].size // 3 for inst in instances)
+    camera = {"eye": (0.55 * extent, 0.35 * extent + 4.0, 0.75 * extent), "look_at": (0.0, 0.0, 0.0),
+              "up": (0.0, 1.0, 0.0), "fov_y": float(np.float32(np.radians(45.0))), "exposure": 1.0}
+    return {"meshes": meshes, "instances": instances, "materials": materials, "camera": camera, "triangles": tris,
+            "emissive_triangles": 2 * max(1, n_emissive_tris // 2), "seed": seed}
+
+
+BATCH_RESOLUTIONS = [(128, 128), (256, 192), (512, 384), (640, 480), (1024, 768)]
+BATCH_SPP = [16, 64, 256]
+
+
+def batch_jobs(seed: int = 4, n_jobs: int = 64, spp_scale: float = 1.0):
+    """The batched-render workload: n_jobs seeded grid_scene variants with
+    10k-500k triangles (log-uniform), 4-1024 emissive triangles, 8-64
+    materials, a resolution from BATCH_RESOLUTIONS, spp from BATCH_SPP (times
+    spp_scale, at least 1) and max depth 8-16.  Returns (scene dicts, job specs)."""
+    rng = np.random.default_rng(seed)
+    scenes, specs = [], []
+    for k in range(n_jobs):
+        tris = float(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
+        n_side = int(rng.integers(4, 17))
+        per = max(24, int(tris / (n_side * n_side)))
+        emis = int(np.exp(rng.uniform(np.log(4), np.log(1024))))
+        sc = grid_scene(seed=1000 + k, n_side=n_side, tris_per_object=per, n_materials=int(rng.integers(8, 65)),
+                        n_emissive_tris=emis)
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+        spp = max(1, int(round(BATCH_SPP[int(rng.integers(0, len(BATCH_SPP)))] * spp_scale)))
+        scenes.append(sc)
+        specs.append({"width": w, "height": h, "spp": spp, "max_depth": int(rng.integers(8, 17))})
+    return scenes, specs
