@@ -280,8 +280,9 @@ typedef struct tpt_camera_desc {
 } tpt_camera_desc;
 
 typedef enum tpt_execution {
-  TPT_EXEC_WAVEFRONT = 0, /* stage kernels over compacted ray queues (default) */
-  TPT_EXEC_MEGAKERNEL = 1 /* one thread runs one whole path */
+  TPT_EXEC_WAVEFRONT = 0,  /* stage kernels over compacted ray queues (default) */
+  TPT_EXEC_MEGAKERNEL = 1, /* one persistent kernel: each thread carries one path at a time */
+  TPT_EXEC_AUTO = 2        /* the execution tpt_autotune last picked on this context (wavefront before) */
 } tpt_execution;
 
 typedef struct tpt_render_job {
@@ -301,6 +302,12 @@ typedef struct tpt_render_job {
  * workload.  Results do not depend on it. */
 tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots);
 uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx);
+/* Wavefront bounces are replayed from captured CUDA graphs (one per bounce
+ * shape, cached per scene, camera and arena; default on).  enable = 0 launches
+ * every stage directly.  Inside a caller's own stream capture the stages are
+ * always launched directly (they join the caller's graph).  Results do not
+ * depend on it. */
+tpt_status tpt_context_set_graphs(tpt_context* ctx, int enable);
 
 /* Renders each job into out_rgb[j] (host, width*height*3 floats, row-major,
  * pixel = y*width + x): per pixel the running mean of `spp` samples in sample
@@ -313,6 +320,25 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
  * (parity testing and sample-level consumers). */
 tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first, uint64_t count,
                                      float* out_samples, void* stream);
+
+/* Autotuner (no counterpart in the reference): times the candidate settings
+ * on a pilot of `jobs` (each job's rows scaled down until the pilot holds at
+ * most 2^24 paths) and applies the fastest to the context: the execution used
+ * by jobs whose `execution` is TPT_EXEC_AUTO, and, when that is the wavefront,
+ * its queue capacity (tpt_context_set_wavefront_capacity) and graph replay
+ * (tpt_context_set_graphs).  Candidates: the megakernel, and the wavefront
+ * (batched when n_jobs > 1) at capacities 2^18 .. 2^23, with and without graph
+ * replay.  MIS jobs only.  Results do not depend on the settings. */
+typedef struct tpt_tune_result {
+  uint32_t execution;          /* TPT_EXEC_WAVEFRONT or TPT_EXEC_MEGAKERNEL */
+  uint32_t wavefront_capacity; /* path slots per chunk */
+  uint32_t graphs;             /* 1: bounces replayed from captured graphs */
+  float ms;                    /* pilot time of the chosen settings */
+  float ms_megakernel;         /* pilot time of the megakernel */
+  float ms_wavefront_default;  /* pilot time of the wavefront at 2^22 slots with graphs */
+  uint64_t pilot_paths;
+} tpt_tune_result;
+tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, tpt_tune_result* out);
 
 /* Batched rendering: n_jobs MIS jobs (any mix of scenes, cameras,
  * resolutions, spp and depths; `execution` is not read) through one wavefront

@@ -76,3 +76,45 @@ def test_capacity_does_not_change_single_renders(ctx, mixed):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     with pytest.raises(tpt.TptError):
         ctx.wavefront_capacity = 100
+
+
+def test_graph_replay_equals_direct_launches(ctx, mixed):
+    """Bounces replayed from captured graphs give the same bits as direct launches,
+    on the legacy default stream, on a side stream, and batched."""
+    import torch
+
+    ctx.set_graphs(False)
+    try:
+        direct = _render_each(ctx, mixed)
+        direct_b = _render_batch(ctx, mixed)
+    finally:
+        ctx.set_graphs(True)
+    for _ in range(2):  # the first pass captures, the second replays
+        graphs = _render_each(ctx, mixed)
+        graphs_b = _render_batch(ctx, mixed)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        graphs_s = _render_each(ctx, mixed)
+    for a, b, c, d, e in zip(direct, graphs, direct_b, graphs_b, graphs_s):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        assert np.array_equal(c.view(np.uint32), d.view(np.uint32))
+        assert np.array_equal(a.view(np.uint32), e.view(np.uint32))
+
+
+def test_autotune_applies_a_setting_that_renders_the_same(ctx, mixed):
+    import torch
+
+    ref = _render_each(ctx, mixed)
+    try:
+        r = ctx.autotune(mixed)
+        assert r["execution"] in (tpt.EXEC_WAVEFRONT, tpt.EXEC_MEGAKERNEL)
+        assert r["ms"] > 0 and r["ms"] <= r["ms_megakernel"] * 1.0001
+        assert r["pilot_paths"] == sum(j.width * j.height * j.spp for j in mixed)  # small: the whole workload
+        auto = [tpt.RenderJob(j.scene, j.camera, j.width, j.height, j.spp, j.max_depth, j.integrator, tpt.EXEC_AUTO)
+                for j in mixed]
+        got = _render_each(ctx, auto)
+        for a, b in zip(got, ref):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    finally:
+        ctx.wavefront_capacity = 0
+        ctx.set_graphs(True)

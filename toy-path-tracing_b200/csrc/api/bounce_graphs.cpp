@@ -1,0 +1,144 @@
+// One captured CUDA graph per wavefront bounce.
+//
+// A bounce is a fixed sequence: clear the next ray-queue and shadow-queue
+// lengths, closest-hit traversal of the current queue, shade, then (except on
+// the last bounce) the shadow traversal and resolve.  Its launch shapes depend
+// on the arena capacity only (queue lengths live on the device) and every
+// chunk-specific value is read from the device (the chunk's first path is
+// written by generate), so the same four graphs (current queue 0 or 1, with or
+// without the shadow stage) serve every chunk and every bounce of a given
+// (scene, camera, arena) and are replayed instead of re-launching ~8
+// operations per bounce.  Graphs are captured on a private non-blocking stream
+// and launched on the caller's stream; a stream that is itself being captured
+// gets the plain launches (they join the caller's graph).
+#include <cstring>
+
+#include "internal.h"
+
+namespace tpt {
+
+namespace {
+
+constexpr size_t kMaxGraphSets = kGraphCounterSlots / 2;
+
+struct BounceKey {
+  DevRender S;
+  RenderLaunch P;
+  WfBuffers B;
+  const DevJob* jobs;
+  uint32_t* err;
+  int num_sms;
+  int pad;
+};
+
+// The operations of one bounce (the shared body of the direct and the captured path).
+cudaError_t bounce_ops(const BounceKey& k, int cur, bool last, unsigned long long* c0, unsigned long long* c1,
+                       cudaStream_t s) {
+  const WfBuffers& B = k.B;
+  cudaError_t e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
+  if (e == cudaSuccess)
+    e = launch_traverse_strided(k.S.geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
+                                B.h_inst, B.h_bary, B.capacity, c0, k.err, k.num_sms, s, nullptr, nullptr,
+                                B.counts + cur, k.jobs, k.jobs ? B.q_job[cur] : nullptr);
+  if (e == cudaSuccess)
+    e = k.jobs ? launch_wf_shade_batch(k.jobs, B, cur, s) : launch_wf_shade(k.S.geo, k.S.d, k.P, B, cur, s);
+  if (e == cudaSuccess && !last)
+    e = launch_traverse_strided(k.S.geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
+                                nullptr, B.capacity, c1, k.err, k.num_sms, s, nullptr, nullptr, B.counts + 2, k.jobs,
+                                k.jobs ? B.s_job : nullptr);
+  if (e == cudaSuccess && !last) e = launch_wf_resolve(B, s);
+  return e;
+}
+
+}  // namespace
+
+struct BounceGraphSet {
+  BounceKey key;
+  cudaGraphExec_t exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  bool failed = false;
+  uint64_t last_use = 0;
+  uint32_t slot = 0;  // index of its two dedicated work counters
+};
+
+void destroy_bounce_graphs(tpt_context* ctx) {
+  for (BounceGraphSet* g : ctx->graphs) {
+    for (auto& row : g->exec)
+      for (cudaGraphExec_t x : row)
+        if (x) cudaGraphExecDestroy(x);
+    delete g;
+  }
+  ctx->graphs.clear();
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  ctx->cap_stream = nullptr;
+}
+
+cudaError_t enqueue_bounce(tpt_context* ctx, cudaStream_t s, const DevGeometry& geo, const DevRenderData& rd,
+                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last) {
+  BounceKey key;
+  std::memset(&key, 0, sizeof key);
+  if (!jobs) {
+    std::memcpy(&key.S.geo, &geo, sizeof geo);
+    std::memcpy(&key.S.d, &rd, sizeof rd);
+    std::memcpy(&key.P, &P, sizeof P);
+  }
+  std::memcpy(&key.B, &B, sizeof B);
+  key.jobs = jobs;
+  key.err = ctx->d_err;
+  key.num_sms = ctx->num_sms;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  const bool capturing = cudaStreamIsCapturing(s, &cap) == cudaSuccess && cap != cudaStreamCaptureStatusNone;
+  if (!ctx->use_graphs || capturing) return bounce_ops(key, cur, last, next_counter(ctx), next_counter(ctx), s);
+  BounceGraphSet* g = nullptr;
+  for (BounceGraphSet* x : ctx->graphs)
+    if (std::memcmp(&x->key, &key, sizeof key) == 0) g = x;
+  if (!g) {
+    uint32_t slot = (uint32_t)ctx->graphs.size();
+    if (ctx->graphs.size() >= kMaxGraphSets) {  // evict the least recently used set
+      size_t lru = 0;
+      for (size_t i = 1; i < ctx->graphs.size(); ++i)
+        if (ctx->graphs[i]->last_use < ctx->graphs[lru]->last_use) lru = i;
+      BounceGraphSet* old = ctx->graphs[lru];
+      slot = old->slot;
+      for (auto& row : old->exec)
+        for (cudaGraphExec_t x : row)
+          if (x) cudaGraphExecDestroy(x);  // an in-flight launch completes first
+      delete old;
+      ctx->graphs.erase(ctx->graphs.begin() + lru);
+    }
+    g = new BounceGraphSet();
+    g->key = key;
+    g->slot = slot;
+    ctx->graphs.push_back(g);
+  }
+  g->last_use = ++ctx->graph_clock;
+  unsigned long long* c0 = ctx->d_counters + kCounterSlots - 2 * kMaxGraphSets + 2 * g->slot;
+  if (g->failed) return bounce_ops(key, cur, last, c0, c0 + 1, s);
+  cudaGraphExec_t& x = g->exec[cur][last ? 1 : 0];
+  if (!x) {
+    if (!ctx->cap_stream && cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      ctx->cap_stream = nullptr;
+      g->failed = true;
+      cudaGetLastError();
+      return bounce_ops(key, cur, last, c0, c0 + 1, s);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const cudaError_t e_ops = bounce_ops(key, cur, last, c0, c0 + 1, ctx->cap_stream);
+      e = cudaStreamEndCapture(ctx->cap_stream, &graph);
+      if (e == cudaSuccess) e = e_ops;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      x = nullptr;
+      g->failed = true;
+      cudaGetLastError();  // capture errors are not sticky; fall back to plain launches
+      return bounce_ops(key, cur, last, c0, c0 + 1, s);
+    }
+  }
+  return cudaGraphLaunch(x, s);
+}
+
+}  // namespace tpt

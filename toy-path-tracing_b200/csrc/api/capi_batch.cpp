@@ -116,21 +116,9 @@ tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   const DevGeometry no_geo{};
   for (const Chunk& c : plan_chunks(L, path_base, capacity)) {
     cudaError_t e = launch_wf_generate_batch(ctx->d_jobs, (uint32_t)n_jobs, B, c.first_path, c.n_paths, s);
-    for (uint32_t b = 0; e == cudaSuccess && b <= c.max_depth; ++b) {
-      const int cur = (int)(b & 1u);
-      e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
-      if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
-      if (e == cudaSuccess)
-        e = launch_traverse_strided(no_geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
-                                    B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
-                                    nullptr, nullptr, B.counts + cur, ctx->d_jobs, B.q_job[cur]);
-      if (e == cudaSuccess) e = launch_wf_shade_batch(ctx->d_jobs, B, c.first_path, cur, s);
-      if (e == cudaSuccess && b < c.max_depth)
-        e = launch_traverse_strided(no_geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t,
-                                    B.s_inst, nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
-                                    nullptr, nullptr, B.counts + 2, ctx->d_jobs, B.s_job);
-      if (e == cudaSuccess && b < c.max_depth) e = launch_wf_resolve(B, s);
-    }
+    for (uint32_t b = 0; e == cudaSuccess && b <= c.max_depth; ++b)
+      e = enqueue_bounce(ctx, s, no_geo, DevRenderData{}, RenderLaunch{}, B, ctx->d_jobs, (int)(b & 1u),
+                         b == c.max_depth);
     if (e == cudaSuccess) e = launch_wf_finalize(B, c.n_paths, samples, s);
     for (const Segment& g : c.segs) {
       if (e != cudaSuccess) break;

@@ -48,7 +48,7 @@ tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream) {
 }
 
 unsigned long long* next_counter(tpt_context* ctx) {
-  uint32_t k = ctx->counter_next++ % kCounterSlots;
+  uint32_t k = ctx->counter_next++ % (kCounterSlots - kGraphCounterSlots);
   return ctx->d_counters + k;
 }
 
@@ -231,6 +231,7 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->d_stage) cudaFree(ctx->d_stage);
   if (ctx->d_err) cudaFree(ctx->d_err);
+  destroy_bounce_graphs(ctx);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   if (ctx->d_scratch) cudaFree(ctx->d_scratch);
   if (ctx->d_wf) cudaFree(ctx->d_wf);

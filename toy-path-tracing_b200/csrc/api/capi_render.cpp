@@ -33,7 +33,8 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
     return set_error(ctx, TPT_ERR_CAPACITY,
                      "BDPT max_depth " + std::to_string(job->max_depth) + " above the device limit of " +
                          std::to_string(kBdptMaxDepthApi));
-  if (job->execution != TPT_EXEC_WAVEFRONT && job->execution != TPT_EXEC_MEGAKERNEL)
+  if (job->execution != TPT_EXEC_WAVEFRONT && job->execution != TPT_EXEC_MEGAKERNEL &&
+      job->execution != TPT_EXEC_AUTO)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown execution mode");
   if (job->scene->render.num_materials == 0)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "scene has no materials: upload materials to render");
@@ -148,7 +149,9 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
   const DevGeometry& geo = job->scene->geo;
   const DevRenderData& rd = job->scene->render;
   cudaError_t e = launch_wf_generate(geo, rd, L, B, first, n, s, A ? samples : nullptr);
-  for (uint32_t b = 0; e == cudaSuccess && b <= L.max_depth; ++b) {
+  for (uint32_t b = 0; !A && e == cudaSuccess && b <= L.max_depth; ++b)
+    e = enqueue_bounce(ctx, s, geo, rd, L, B, nullptr, (int)(b & 1u), b == L.max_depth);
+  for (uint32_t b = 0; A && e == cudaSuccess && b <= L.max_depth; ++b) {
     const int cur = (int)(b & 1u);
     e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
@@ -156,7 +159,7 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
       e = launch_traverse_strided(geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
                                   B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
                                   nullptr, nullptr, B.counts + cur);
-    if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, first, cur, s, A);
+    if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, cur, s, A);
     if (e == cudaSuccess && b < L.max_depth)
       e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
                                   nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
@@ -193,6 +196,12 @@ tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots) 
   return TPT_OK;
 }
 
+tpt_status tpt_context_set_graphs(tpt_context* ctx, int enable) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  ctx->use_graphs = enable != 0;
+  return TPT_OK;
+}
+
 uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx) {
   return ctx ? (ctx->batch_capacity ? ctx->batch_capacity : (1u << 22)) : 0u;
 }
@@ -209,9 +218,10 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
   const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
   if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
   float* samples = (float*)ctx->d_scratch;
+  const uint32_t exec = job->execution == TPT_EXEC_AUTO ? ctx->tuned_execution : job->execution;
   for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
     const uint32_t n = std::min(cp, npix - p0);
-    if (job->execution == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
+    if (exec == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
       cudaError_t e = launch_render(job->scene->geo, job->scene->render, L, samples, (uint64_t)p0 * L.spp,
                                     (uint64_t)n * L.spp, ctx->d_err, ctx->num_sms, s, next_counter(ctx));
       if ((st = cuda_check(ctx, e, "render kernel launch"))) return st;
@@ -235,7 +245,8 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
   if (count && !out_samples) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  if (job->execution == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT)
+  const uint32_t exec = job->execution == TPT_EXEC_AUTO ? ctx->tuned_execution : job->execution;
+  if (exec == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT)
     return cuda_check(ctx,
                       launch_render(job->scene->geo, job->scene->render, L, out_samples, first, count, ctx->d_err,
                                     ctx->num_sms, s, next_counter(ctx)),

@@ -14,6 +14,10 @@
 #include "../host/host_scene.h"
 #include "../host/host_types.h"
 
+namespace tpt {
+struct BounceGraphSet;
+}
+
 struct tpt_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -42,6 +46,12 @@ struct tpt_context {
   tpt::DevJob* d_jobs = nullptr;
   size_t d_jobs_cap = 0;
   uint32_t batch_capacity = 0;
+  // per-bounce CUDA graphs of the wavefront (bounce_graphs.cpp)
+  bool use_graphs = true;
+  uint32_t tuned_execution = 0;  // what TPT_EXEC_AUTO means (tpt_autotune)
+  std::vector<tpt::BounceGraphSet*> graphs;
+  uint64_t graph_clock = 0;
+  cudaStream_t cap_stream = nullptr;
   // OpenPBR tables (built on the GPU on first use, kept until destroy)
   std::map<uint32_t, float*> da_tables;  // directional albedo per eta (bit pattern)
   float* d_cec_e = nullptr;              // conductor E (64 x 64)
@@ -79,6 +89,7 @@ struct tpt_scene {
 namespace tpt {
 
 constexpr uint32_t kCounterSlots = 1024;
+constexpr uint32_t kGraphCounterSlots = 32;  // the last slots: two per cached bounce-graph set
 
 tpt_status set_error(tpt_context* ctx, tpt_status st, const std::string& msg);
 tpt_status cuda_check(tpt_context* ctx, cudaError_t e, const char* what);
@@ -126,16 +137,21 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
 cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                                const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s,
                                const float* primal = nullptr);
+// shade reads the chunk's first path from the queue counters (written by generate)
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s,
-                            const DevAdjoint* A = nullptr);
+                            const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A = nullptr);
 cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint = false);
 // Batched stages: slot i is global path first_path + i of the jobs' index space.
 cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const WfBuffers& B, uint64_t first_path,
                                      uint32_t n_paths, cudaStream_t s);
-cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, uint64_t first_path, int cur,
-                                  cudaStream_t s);
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
+
+// bounce_graphs.cpp: one wavefront bounce (single job when jobs == nullptr,
+// else batched) on `s`, replayed from a cached CUDA graph when possible.
+cudaError_t enqueue_bounce(tpt_context* ctx, cudaStream_t s, const DevGeometry& geo, const DevRenderData& rd,
+                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last);
+void destroy_bounce_graphs(tpt_context* ctx);
 
 // capi_batch.cpp: jobs (MIS) through one wavefront launch sequence; out_rgb are
 // device images; capacity = path slots per chunk (0 = 2^22).

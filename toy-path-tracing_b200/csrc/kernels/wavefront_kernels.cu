@@ -66,6 +66,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaun
     B.counts[0] = n_paths;
     B.counts[1] = 0;
     B.counts[2] = 0;
+    // the chunk's first path, for the later stages (which a graph replays
+    // unchanged from chunk to chunk)
+    B.counts[4] = (uint32_t)first_path;
+    B.counts[5] = (uint32_t)(first_path >> 32);
   }
   if (i >= n_paths) return;
   const uint32_t C = B.capacity;
@@ -104,11 +108,12 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaun
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
 template <bool ADJ, bool BATCH>
-__global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, uint64_t first_path,
-                                                     int cur, DevAdjoint A, const DevJob* __restrict__ jobs) {
+__global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, int cur,
+                                                     DevAdjoint A, const DevJob* __restrict__ jobs) {
   __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[cur]) return;
+  const uint64_t first_path = (uint64_t)B.counts[4] | ((uint64_t)B.counts[5] << 32);
   const float sgn = ADJ ? -1.0f : 1.0f;  // the adjoint takes collected radiance off R
   uint32_t grad_key = 0xFFFFFFFFu;
   float grad_v[ADJ ? kGradParams : 1];
@@ -283,12 +288,12 @@ cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, 
 }
 
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                            const WfBuffers& B, uint64_t first_path, int cur, cudaStream_t s, const DevAdjoint* A) {
+                            const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A) {
   DevRender S{geo, rd};
   if (A)
-    wf_shade<true, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, *A, nullptr);
+    wf_shade<true, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, *A, nullptr);
   else
-    wf_shade<false, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, first_path, cur, DevAdjoint{}, nullptr);
+    wf_shade<false, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, DevAdjoint{}, nullptr);
   return cudaGetLastError();
 }
 
@@ -299,9 +304,8 @@ cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, uint64_t first_path, int cur,
-                                  cudaStream_t s) {
-  wf_shade<false, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(DevRender{}, RenderLaunch{}, B, first_path, cur,
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s) {
+  wf_shade<false, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(DevRender{}, RenderLaunch{}, B, cur,
                                                                   DevAdjoint{}, jobs);
   return cudaGetLastError();
 }

@@ -168,7 +168,14 @@ GRAD_NAMES = ["base_color_r", "base_color_g", "base_color_b", "specular_roughnes
 GRAD_MASK_BASE_COLOR, GRAD_MASK_ROUGHNESS, GRAD_MASK_METALNESS, GRAD_MASK_IOR, GRAD_MASK_COAT = 1, 2, 4, 8, 16
 GRAD_ALL = 31
 
+class TuneResult(C.Structure):
+    _fields_ = [("execution", C.c_uint32), ("wavefront_capacity", C.c_uint32), ("graphs", C.c_uint32),
+                ("ms", C.c_float), ("ms_megakernel", C.c_float), ("ms_wavefront_default", C.c_float),
+                ("pilot_paths", C.c_uint64)]
+
+
 INTEGRATOR_MIS = 0
+EXEC_AUTO = 2
 EXEC_WAVEFRONT = 0
 EXEC_MEGAKERNEL = 1
 
@@ -222,6 +229,8 @@ EXPORTED_SYMBOLS = [
     "tpt_render_batch_device",
     "tpt_context_set_wavefront_capacity",
     "tpt_context_wavefront_capacity",
+    "tpt_context_set_graphs",
+    "tpt_autotune",
     "tpt_adjoint_device",
     "tpt_adjoint",
 ]
@@ -261,6 +270,8 @@ def _declare(L):
         "tpt_render_batch_device": (i32, [vp, vp, i32, vp, vp]),
         "tpt_context_set_wavefront_capacity": (i32, [vp, C.c_uint32]),
         "tpt_context_wavefront_capacity": (C.c_uint32, [vp]),
+        "tpt_context_set_graphs": (i32, [vp, i32]),
+        "tpt_autotune": (i32, [vp, vp, i32, C.POINTER(TuneResult)]),
         "tpt_adjoint_device": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp, vp]),
         "tpt_adjoint": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp]),
     }
@@ -309,6 +320,17 @@ class Context:
     @wavefront_capacity.setter
     def wavefront_capacity(self, slots: int):
         _check(lib().tpt_context_set_wavefront_capacity(self.h, int(slots)), self)
+
+    def set_graphs(self, enable: bool):
+        """`tpt_context_set_graphs`: replay wavefront bounces from CUDA graphs."""
+        _check(lib().tpt_context_set_graphs(self.h, int(bool(enable))), self)
+
+    def autotune(self, jobs) -> dict:
+        """`tpt_autotune`: times candidate settings on a pilot of `jobs` and applies the fastest."""
+        arr = (RenderJob * len(jobs))(*jobs)
+        r = TuneResult()
+        _check(lib().tpt_autotune(self.h, arr, len(jobs), C.byref(r)), self)
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_}
 
     def render_batch_device(self, jobs, out_ptrs, stream=None):
         """`tpt_render_batch_device`: jobs (RenderJob list) into device images."""
