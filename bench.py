@@ -54,6 +54,11 @@ def parse_args():
     p.add_argument("--render-spp", type=int, default=64)
     p.add_argument("--render-exec", choices=["both", "wavefront", "megakernel"], default="both")
     p.add_argument("--render-scene", choices=["both", "openpbr", "lambert"], default="both")
+    p.add_argument("--no-large", action="store_true", help="skip the large-scene render block")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched-render block")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-render block")
+    p.add_argument("--large-spp", type=int, default=16, help="spp timed on the large scene")
+    p.add_argument("--batch-spp-scale", type=float, default=0.25, help="spp scale of the batched workload")
     return p.parse_args()
 
 
@@ -275,6 +280,201 @@ def render_scene_block(ctx, kind, steps, warmup, cpu=True, cfg=RENDER_CFG, execs
     return out
 
 
+
+def _time_ms(fn, reps=1):
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def large_block(ctx, args, cpu=True):
+    """The plain large render: ~2.1M triangles (1024 instanced spheres, boxes and
+    tori + ground), 256 OpenPBR materials, 10,000 emissive triangles, 1920x1080,
+    depth 16 (MIS) and path length 10 (BDPT).  Msamples/s is timed at
+    --large-spp samples per pixel (the per-sample cost does not depend on spp)."""
+    import torch
+
+    import tpt
+    import tpt_scenes
+
+    t0 = time.perf_counter()
+    sc = tpt_scenes.grid_scene()
+    scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
+    setup_s = time.perf_counter() - t0
+    W, H, spp = 1920, 1080, args.large_spp
+    st = torch.cuda.current_stream().cuda_stream
+    img = torch.empty(W * H * 3, device="cuda")
+    out = {"config": {"triangles": sc["triangles"], "emissive_triangles": sc["emissive_triangles"],
+                      "materials": 256, "width": W, "height": H, "spp_timed": spp, "spp_configured": 256,
+                      "mis_max_depth": 16, "bdpt_max_path_length": 10},
+           "unit": "Msamples/s", "upload_s": setup_s}
+    for name, ex, integ, depth, s_spp in (("mis_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_MIS, 16, spp),
+                                          ("mis_megakernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_MIS, 16, spp),
+                                          ("bdpt", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_BDPT, 10, 1)):
+        job = scene.job(sc["camera"], W, H, s_spp, depth, integrator=integ, execution=ex)
+        ms = _time_ms(lambda: scene.render_device(job, img.data_ptr(), st))
+        out[name] = {"value": W * H * s_spp / ms / 1e3, "ms_per_image": ms, "spp": s_spp}
+    out["wavefront_over_megakernel"] = out["mis_wavefront"]["value"] / out["mis_megakernel"]["value"]
+    if cpu:
+        import oracle as orc
+
+        ref = orc.RenderScene(sc, scene.light_tree())
+        threads = os.cpu_count() or 1
+        n_rows = 8
+        while True:  # evenly spaced rows, grown until ~5 s of CPU work
+            rows = [int(r) for r in np.linspace(0, H - 1, n_rows)]
+            t0 = time.perf_counter()
+            for r in rows:
+                ref.render(sc["camera"], W, H, 1, 16, pixels=(r * W, (r + 1) * W), nthreads=threads)
+            dt = time.perf_counter() - t0
+            if dt > 3.0 or n_rows >= H:
+                break
+            n_rows = min(H, n_rows * max(2, int(5.0 / max(dt, 1e-3))))
+        out["cpu_baseline"] = {"value": len(rows) * W / dt / 1e6, "cores": threads, "kind": "port",
+                               "sample": f"MIS: {len(rows)} evenly spaced rows of {W} pixels x 1 spp, {dt:.1f} s"}
+        out["wavefront_over_cpu"] = out["mis_wavefront"]["value"] / out["cpu_baseline"]["value"]
+    scene.close()
+    return out
+
+
+def batch_block(ctx, args):
+    """Batched uneven renders: 64 seeded variants of the large-scene generator
+    (10k-500k triangles, 4-1024 emissive triangles, 8-64 materials), resolutions
+    from {128^2, 256x192, 512x384, 640x480, 1024x768}, spp from {16, 64, 256}
+    times --batch-spp-scale, depth 8-16; one batched wavefront (autotuned) vs
+    the megakernel job by job.  Both executions produce the same images bit for
+    bit, so the comparison is at equal RMSE."""
+    import torch
+
+    import tpt
+    import tpt_scenes
+
+    t0 = time.perf_counter()
+    scs, specs = tpt_scenes.batch_jobs(spp_scale=args.batch_spp_scale)
+    scenes = [tpt.Scene(ctx, s["meshes"], s["instances"], materials=s["materials"]) for s in scs]
+    setup_s = time.perf_counter() - t0
+    st = torch.cuda.current_stream().cuda_stream
+    total = sum(p["width"] * p["height"] * p["spp"] for p in specs)
+
+    def jobs(ex):
+        return [sc.job(s["camera"], p["width"], p["height"], p["spp"], p["max_depth"], execution=ex)
+                for sc, s, p in zip(scenes, scs, specs)]
+
+    outs = [torch.empty(p["width"] * p["height"] * 3, device="cuda") for p in specs]
+    ptrs = [o.data_ptr() for o in outs]
+    jw, jm = jobs(tpt.EXEC_WAVEFRONT), jobs(tpt.EXEC_MEGAKERNEL)
+    out = {"config": {"jobs": len(specs), "samples": total, "spp_scale": args.batch_spp_scale,
+                      "triangles_min": min(s["triangles"] for s in scs),
+                      "triangles_max": max(s["triangles"] for s in scs)},
+           "unit": "Msamples/s", "upload_s": setup_s}
+    t0 = time.perf_counter()
+    tune = ctx.autotune(jw)
+    out["autotune"] = dict(tune, seconds=time.perf_counter() - t0)
+    ms = _time_ms(lambda: ctx.render_batch_device(jw, ptrs, st))
+    out["batched_wavefront"] = {"value": total / ms / 1e3, "ms": ms}
+    ctx.wavefront_capacity = 0
+    ctx.set_graphs(True)
+    ms = _time_ms(lambda: [sc.render_device(j, p, st) for sc, j, p in zip(scenes, jw, ptrs)])
+    out["per_job_wavefront"] = {"value": total / ms / 1e3, "ms": ms}
+    ms = _time_ms(lambda: [sc.render_device(j, p, st) for sc, j, p in zip(scenes, jm, ptrs)])
+    out["per_job_megakernel"] = {"value": total / ms / 1e3, "ms": ms}
+    out["batched_over_megakernel"] = out["batched_wavefront"]["value"] / out["per_job_megakernel"]["value"]
+    for sc in scenes:
+        sc.close()
+    return out
+
+
+def adjoint_block(ctx, args, cpu=True):
+    """Differentiable render: the Cornell box split into 64 OpenPBR patches,
+    128x128, 16 spp forward and adjoint, depth 6; gradients of an L2 image loss
+    with respect to base_color (3), specular_roughness and base_metalness of
+    every material (5 x 64 = 320 parameters) by the path-replay adjoint; then
+    200 Adam steps of inverse rendering from a perturbed start against a
+    1024-spp target."""
+    import torch
+
+    import tpt
+    import tpt_scenes
+
+    sc = tpt_scenes.cornell_patches()
+    W, spp, depth = 128, 16, 6
+    scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
+    st = torch.cuda.current_stream().cuda_stream
+    job = scene.job(sc["camera"], W, W, spp, depth)
+    img = torch.empty(W * W * 3, device="cuda")
+    d_img = torch.rand(W * W * 3, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    grad = torch.zeros(scene.n_materials * tpt.GRAD_PARAMS, dtype=torch.float64, device="cuda")
+    mask = tpt.GRAD_MASK_BASE_COLOR | tpt.GRAD_MASK_ROUGHNESS | tpt.GRAD_MASK_METALNESS
+    fwd = _time_ms(lambda: scene.render_device(job, img.data_ptr(), st), reps=5)
+    bwd = _time_ms(lambda: scene.adjoint_device(job, d_img.data_ptr(), grad.data_ptr(), mask, 0.0, st), reps=5)
+    n_params = 64 * 5
+    out = {"config": {"materials": 64, "params_per_material": 5, "width": W, "height": W, "spp": spp,
+                      "max_depth": depth, "fd_step": 1e-3},
+           "unit": "grads/s", "forward_ms": fwd, "adjoint_ms": bwd, "adjoint_over_forward": bwd / fwd,
+           "value": n_params / (bwd / 1e3), "samples_per_s_adjoint": W * W * spp / (bwd / 1e3)}
+    # inverse rendering
+    tscene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
+    tjob = tscene.job(sc["camera"], W, W, 1024, depth)
+    target = torch.empty(W * W * 3, device="cuda")
+    tscene.render_device(tjob, target.data_ptr(), st)
+    target = target.view(W, W, 3)
+    start = tpt_scenes.patch_params(5, start=True)
+    params = torch.tensor(start, requires_grad=True)
+    opt = torch.optim.Adam([params], lr=0.01)
+    lo = torch.tensor([0.02, 0.02, 0.02, 0.05, 0.0])
+    hi = torch.tensor([0.98, 0.98, 0.98, 1.0, 1.0])
+    RenderFunction = tpt.render_function()
+    # the backward pass replays 2 x spp paths: samples independent of the forward
+    # image's, so the L2 loss gradient is not biased by their correlation
+    adj_job = scene.job(sc["camera"], W, W, 2 * spp, depth)
+    losses = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(200):
+        opt.zero_grad()
+        im = RenderFunction.apply(params, scene, job, list(range(64)), tpt_scenes.patch_material, mask, 0.0,
+                                  adj_job)
+        loss = ((im - target) ** 2).sum()
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            params.copy_(torch.maximum(torch.minimum(params, hi), lo))
+        losses.append(float(loss.detach()))
+    adam_s = time.perf_counter() - t0
+    out["inverse_rendering"] = {"steps": 200, "adjoint_spp": 2 * spp, "loss_first": losses[0], "loss_last": losses[-1],
+                                "loss_min": min(losses), "seconds": adam_s,
+                                "param_mae_start": float(np.abs(start - sc["params"]).mean()),
+                                "param_mae_end": float(np.abs(params.detach().numpy() - sc["params"]).mean())}
+    if cpu:
+        import oracle as orc
+
+        ref = orc.RenderScene(sc, scene.light_tree())
+        threads = os.cpu_count() or 1
+        Wc = 32
+        while True:  # a centred Wc x Wc window of the image, grown until ~3 s of CPU work
+            dc = np.random.default_rng(0).uniform(0, 1, Wc * Wc * 3).astype(np.float32)
+            ref.adjoint(sc["camera"], Wc, Wc, spp, depth, dc, mask=mask)  # builds the perturbed tables
+            t0 = time.perf_counter()
+            ref.adjoint(sc["camera"], Wc, Wc, spp, depth, dc, mask=mask)
+            dt = time.perf_counter() - t0
+            if dt > 2.0 or Wc >= W:
+                break
+            Wc = min(W, 2 * Wc)
+        out["cpu_baseline"] = {"value": n_params / (dt * (W * W) / (Wc * Wc)), "cores": threads, "kind": "port",
+                               "sample": f"oracle adjoint at {Wc}x{Wc}x{spp}, {dt:.2f} s, scaled to {W}x{W}"}
+    scene.close()
+    tscene.close()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -410,6 +610,12 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0 and not args.no_render:
         line["render"] = render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline, args=args)
+    if rank == 0 and not args.no_large:
+        line["render_large"] = large_block(ctx, args, cpu=not args.no_cpu_baseline)
+    if rank == 0 and not args.no_batch:
+        line["render_batch"] = batch_block(ctx, args)
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = adjoint_block(ctx, args, cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del scene

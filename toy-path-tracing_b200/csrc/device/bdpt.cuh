@@ -243,11 +243,8 @@ __device__ __forceinline__ V3 bdpt_connect(const DevRender& S, Stack& st, const 
   const float dist = sqrtf(dist2);
   const V3 w_lc = delta / dist;
   const V3 w_cl = -w_lc;
-  TraceResult h;
-  if (closest_hit(S, st, offset_origin(lv.v.p, lv.v.ng, w_lc), w_lc, h, err)) {
-    const bool target = (uint32_t)h.inst == cv.v.inst && (uint32_t)h.tri == cv.v.tri;
-    if (!target && !(h.t >= dist * (1.0f - kShadowTolerance))) return zero;
-  }
+  // The reference tests visibility first; every test below returns zero on its
+  // own, so the cheap ones go first and the shadow ray is traced last.
   const DevMaterialRec cm = S.d.mats[__ldg(&S.d.inst[cv.v.inst].material)];
   const V3 f_cam = material_eval(S, cm, cv.v, w_cl, false);
   if (length_sq(f_cam) == 0.0f) return zero;
@@ -262,6 +259,11 @@ __device__ __forceinline__ V3 bdpt_connect(const DevRender& S, Stack& st, const 
   if (length_sq(f_light) == 0.0f) return zero;
   const float g = fabsf(dot(lv.v.ng, w_lc)) * fabsf(dot(cv.v.ng, w_cl)) / dist2;
   if (g <= 0.0f) return zero;
+  TraceResult h;
+  if (closest_hit(S, st, offset_origin(lv.v.p, lv.v.ng, w_lc), w_lc, h, err)) {
+    const bool target = (uint32_t)h.inst == cv.v.inst && (uint32_t)h.tri == cv.v.tri;
+    if (!target && !(h.t >= dist * (1.0f - kShadowTolerance))) return zero;
+  }
   return lv.beta * f_light * g * f_cam * cv.beta;
 }
 
@@ -408,8 +410,12 @@ __device__ V3 trace_bdpt(const DevRender& S, Stack& st, const RenderLaunch& P, c
   for (uint32_t li = 0; li < nl; ++li)
     for (uint32_t ci = 0; ci < nc; ++ci) {
       if (!(lig[li].flags & kBdConnectible) || !(cam[ci].flags & kBdConnectible)) continue;
+      // the MIS weight is finite (in [0, 1]), so a zero connection adds exactly
+      // zero whatever it is: skip its four pdf evaluations
+      const V3 c = bdpt_connect(S, st, lig[li], cam[ci], err);
+      if (c.x == 0.0f && c.y == 0.0f && c.z == 0.0f) continue;
       const float w = bdpt_mis(S, lig, li + 1, cam, ci + 1);
-      L = L + w * bdpt_connect(S, st, lig[li], cam[ci], err);
+      L = L + w * c;
     }
   return L;
 }

@@ -613,24 +613,30 @@ def render_function():
     """The forward/backward pair as a torch.autograd.Function (torch is only the
     caller's tensor plumbing here; both passes run through the C ABI):
 
-        image = RenderFunction.apply(params, scene, job, material_ids, materials_of, mask)
+        image = RenderFunction.apply(params, scene, job, material_ids, materials_of, mask, fd_step, adjoint_job)
 
     params: float32 [n, k] tensor of material parameters (any layout the caller's
     `materials_of(params_row) -> dict` maps to OpenPBR parameters); forward sets
-    the materials and renders; backward runs the path-replay adjoint and maps
-    the [n_materials, 7] gradient back through `grad_of(g7, row)` (default:
-    base_color rgb, roughness, metalness -> the first five slots)."""
+    the materials and renders; backward runs the path-replay adjoint and returns
+    the first k = params.shape[1] columns of the [n_materials, 7] gradient for
+    the listed materials (the TPT_GRAD_* order: base_color rgb, roughness,
+    metalness, specular_ior, coat_weight), so params rows must follow that
+    order up to k.  adjoint_job
+    (optional): the job the backward pass replays, e.g. the same image at another
+    spp, so that its paths are independent of the forward image's (an L2 loss
+    gradient from correlated samples is biased)."""
     import torch
 
     class RenderFunction(torch.autograd.Function):
         @staticmethod
-        def forward(fctx, params, scene, job, material_ids, materials_of, mask=0, fd_step=0.0):
+        def forward(fctx, params, scene, job, material_ids, materials_of, mask=0, fd_step=0.0, adjoint_job=None):
             rows = params.detach().cpu().numpy()
             stream = torch.cuda.current_stream().cuda_stream
             scene.set_openpbr(material_ids, [materials_of(r) for r in rows], stream=stream)
             img = torch.empty(job.height * job.width * 3, dtype=torch.float32, device="cuda")
             scene.render_device(job, img.data_ptr(), stream)
-            fctx.scene, fctx.job, fctx.ids, fctx.mask, fctx.step = scene, job, material_ids, mask, fd_step
+            fctx.scene, fctx.ids, fctx.mask, fctx.step = scene, material_ids, mask, fd_step
+            fctx.job = adjoint_job if adjoint_job is not None else job
             fctx.k = params.shape[1]
             fctx.device, fctx.dtype = params.device, params.dtype
             return img.view(job.height, job.width, 3)
@@ -647,6 +653,6 @@ def render_function():
                                  stream=torch.cuda.current_stream().cuda_stream)
             grad = grad.view(n_mat, GRAD_PARAMS)[torch.as_tensor(fctx.ids, device="cuda").long()]
             out = grad[:, :fctx.k].to(device=fctx.device, dtype=fctx.dtype)
-            return (out, None, None, None, None, None, None)
+            return (out, None, None, None, None, None, None, None)
 
     return RenderFunction
