@@ -232,54 +232,71 @@ static __device__ __noinline__ float bdpt_mis(const DevRender& S, const BdVertex
   return 1.0f / (1.0f + fmaxf(sum, 0.0f));
 }
 
-// connect_vertices (bdpt.rs:488-538) with visible_between (577-602)
-template <class Stack>
-__device__ __forceinline__ V3 bdpt_connect(const DevRender& S, Stack& st, const BdVertex& lv, const BdVertex& cv,
-                                           uint32_t* err) {
-  const V3 zero = V3{0.0f, 0.0f, 0.0f};
+// connect_vertices (bdpt.rs:488-538) up to visible_between (577-602): the
+// contribution c if the two vertices see each other (zero when any other test
+// already makes it zero), and the visibility ray.  The reference tests
+// visibility first; each test here returns zero on its own, so the order does
+// not change the result and the shadow ray is traced only for non-zero c.
+struct BdConnection {
+  V3 c, origin, dir;
+  float dist;
+};
+__device__ __forceinline__ bool bdpt_connect_prepare(const DevRender& S, const BdVertex& lv, const BdVertex& cv,
+                                                     BdConnection& out) {
   const V3 delta = cv.v.p - lv.v.p;
   const float dist2 = length_sq(delta);
-  if (dist2 <= 0.0f) return zero;
+  if (dist2 <= 0.0f) return false;
   const float dist = sqrtf(dist2);
   const V3 w_lc = delta / dist;
   const V3 w_cl = -w_lc;
-  // The reference tests visibility first; every test below returns zero on its
-  // own, so the cheap ones go first and the shadow ray is traced last.
   const DevMaterialRec cm = S.d.mats[__ldg(&S.d.inst[cv.v.inst].material)];
   const V3 f_cam = material_eval(S, cm, cv.v, w_cl, false);
-  if (length_sq(f_cam) == 0.0f) return zero;
+  if (length_sq(f_cam) == 0.0f) return false;
   V3 f_light;
   if (lv.flags & kBdLight) {
-    if (dot(lv.v.ng, w_lc) <= 0.0f) return zero;
+    if (dot(lv.v.ng, w_lc) <= 0.0f) return false;
     f_light = V3{1.0f, 1.0f, 1.0f};
   } else {
     const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[lv.v.inst].material)];
     f_light = material_eval(S, lm, lv.v, w_lc, true);
   }
-  if (length_sq(f_light) == 0.0f) return zero;
+  if (length_sq(f_light) == 0.0f) return false;
   const float g = fabsf(dot(lv.v.ng, w_lc)) * fabsf(dot(cv.v.ng, w_cl)) / dist2;
-  if (g <= 0.0f) return zero;
-  TraceResult h;
-  if (closest_hit(S, st, offset_origin(lv.v.p, lv.v.ng, w_lc), w_lc, h, err)) {
-    const bool target = (uint32_t)h.inst == cv.v.inst && (uint32_t)h.tri == cv.v.tri;
-    if (!target && !(h.t >= dist * (1.0f - kShadowTolerance))) return zero;
-  }
-  return lv.beta * f_light * g * f_cam * cv.beta;
+  if (g <= 0.0f) return false;
+  out.c = lv.beta * f_light * g * f_cam * cv.beta;
+  out.origin = offset_origin(lv.v.p, lv.v.ng, w_lc);
+  out.dir = w_lc;
+  out.dist = dist;
+  return true;
 }
+
+// The subpaths and connections below are warp-synchronous: every lane of the
+// warp calls them (`valid` = the lane holds a sample), lanes step through
+// their loops together, and each step traces the rays of the lanes that need
+// one at a single call site with the while-while traversal (lanes step through
+// interior nodes together before testing leaves).  Each lane's own arithmetic
+// and order are those of bdpt.rs.
 
 // bdpt.rs:135-262 (no environment or non-area lights in scope)
 template <class Stack>
-__device__ __noinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& st, const RenderLaunch& P,
-                                                     const PathSamplerDev& ps, V3 ro, V3 rd, BdVertex* vs, V3& L,
-                                                     uint32_t* err) {
+__device__ __forceinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& st, bool valid,
+                                                        const RenderLaunch& P, const PathSamplerDev& ps, V3 ro, V3 rd,
+                                                        BdVertex* vs, V3& L, uint32_t* err) {
   uint32_t n = 0;
   V3 beta = V3{1.0f, 1.0f, 1.0f};
-  bool count_emission = true, have_pending = false;
+  bool count_emission = true, have_pending = false, alive = valid;
   V3 pending_from = V3{0.0f, 0.0f, 0.0f};
   float pending_pdf = 0.0f;
   for (uint32_t depth = 0; depth < P.max_depth; ++depth) {
+    const unsigned live = __ballot_sync(0xffffffffu, alive);
+    if (!live) break;
     TraceResult h;
-    if (!closest_hit(S, st, ro, rd, h, err)) break;
+    if (alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    if (!alive) continue;
+    if (h.tri < 0) {
+      alive = false;
+      continue;
+    }
     const Vertex v = shade_hit<Stack>(S, h, rd);
     const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
     BdVertex& pv = vs[n];
@@ -292,13 +309,17 @@ __device__ __noinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& 
     if (m.kind == kDevEmissive) {
       const float w = count_emission ? 1.0f : camera_light_hit_mis(S, vs, n);
       L = L + beta * emissive_le(m) * w;
-      break;  // pure emitter: sample() is None
+      alive = false;  // pure emitter: sample() is None
+      continue;
     }
     float ud0, ud1;
     ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
     const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
     MatSample s;
-    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, false, s)) break;
+    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, false, s)) {
+      alive = false;
+      continue;
+    }
     pv.flags = s.delta ? kBdDelta : kBdConnectible;
     if (n >= 2) vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
     ro = offset_origin(v.p, v.ng, s.wi);
@@ -306,7 +327,10 @@ __device__ __noinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& 
     beta = beta * s.weight;
     if (depth + 1 >= 4) {
       const float q = clampf(max_element(beta), 0.05f, 1.0f);
-      if (ps.sample_1d(vertex_dim(depth, kOffRr)) > q) break;
+      if (ps.sample_1d(vertex_dim(depth, kOffRr)) > q) {
+        alive = false;
+        continue;
+      }
       beta = beta / q;
     }
     have_pending = true;
@@ -317,12 +341,13 @@ __device__ __noinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& 
   return n;
 }
 
-// bdpt.rs:264-385
-template <class Stack>
-__device__ __noinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& st, const RenderLaunch& P,
-                                                    const PathSamplerDev& ps, BdVertex* vs, uint32_t* err) {
-  if (P.max_depth == 0 || S.d.num_area_lights == 0 || S.d.area_light_weight_sum <= 0.0f) return 0;
-  // sample_area_light_triangle (bdpt.rs:540-553): first prefix >= u * sum
+// sample_area_light_triangle and the light endpoint (bdpt.rs:264-300, 540-553):
+// false when the light subpath is empty.
+__device__ __forceinline__ bool bdpt_light_endpoint(const DevRender& S, const RenderLaunch& P,
+                                                    const PathSamplerDev& ps, BdVertex* vs, V3& ro, V3& rd, V3& beta,
+                                                    V3& pending_from, float& pending_pdf) {
+  if (P.max_depth == 0 || S.d.num_area_lights == 0 || S.d.area_light_weight_sum <= 0.0f) return false;
+  // first prefix >= u * sum
   const float target = clampf(ps.sample_1d(vertex_dim(0, kOffCategory)), 0.0f, 1.0f) * S.d.area_light_weight_sum;
   uint32_t lo = 0, hi = S.d.num_area_lights;
   while (lo < hi) {
@@ -343,7 +368,7 @@ __device__ __noinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& s
   const float area = 0.5f * length(cross(T.p[1] - T.p[0], T.p[2] - T.p[0]));
   const float pdf_point = area > 0.0f ? 1.0f / area : 0.0f;
   const float pdf_area = pmf * pdf_point;
-  if (pdf_area <= 0.0f) return 0;
+  if (pdf_area <= 0.0f) return false;
   const V3 gn = normalize_or_zero(cross(T.p[1] - T.p[0], T.p[2] - T.p[0]));
   const Frame fr = frame_from_normal(gn);
   float ud0, ud1;
@@ -351,28 +376,46 @@ __device__ __noinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& s
   const V3 ld = opbr::sample_cosine_hemisphere(ud0, ud1);
   const V3 emit = normalize_or_zero(to_world(fr, ld));
   const float pdf_dir = fmaxf(ld.z, 0.0f) / kPiF;
-  if (length_sq(emit) == 0.0f || pdf_dir <= 0.0f) return 0;
+  if (length_sq(emit) == 0.0f || pdf_dir <= 0.0f) return false;
   Vertex lvx = make_vertex(T, al.inst, al.tri, b0, b1, b2, -emit);
   lvx.wo = emit;
   const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[al.inst].material)];
-  if (lm.kind != kDevEmissive) return 0;  // le() is None
+  if (lm.kind != kDevEmissive) return false;  // le() is None
   const float cos_emit = fmaxf(dot(lvx.ng, emit), 0.0f);
-  if (cos_emit <= 0.0f) return 0;
+  if (cos_emit <= 0.0f) return false;
   const V3 endpoint_beta = emissive_le(lm) / pdf_area;
-  uint32_t n = 0;
   vs[0].v = lvx;
   vs[0].beta = endpoint_beta;
   vs[0].pdf_fwd = pdf_area;
   vs[0].pdf_rev = 0.0f;
   vs[0].flags = kBdLight | kBdConnectible;
-  n = 1;
-  V3 ro = offset_origin(lvx.p, lvx.ng, emit), rd = emit;
-  V3 beta = endpoint_beta * (cos_emit / pdf_dir);
-  V3 pending_from = lvx.p;
-  float pending_pdf = pdf_dir;
+  ro = offset_origin(lvx.p, lvx.ng, emit);
+  rd = emit;
+  beta = endpoint_beta * (cos_emit / pdf_dir);
+  pending_from = lvx.p;
+  pending_pdf = pdf_dir;
+  return true;
+}
+
+// bdpt.rs:264-385
+template <class Stack>
+__device__ __forceinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& st, bool valid,
+                                                       const RenderLaunch& P, const PathSamplerDev& ps, BdVertex* vs,
+                                                       uint32_t* err) {
+  V3 ro, rd, beta, pending_from;
+  float pending_pdf = 0.0f;
+  bool alive = valid && bdpt_light_endpoint(S, P, ps, vs, ro, rd, beta, pending_from, pending_pdf);
+  uint32_t n = alive ? 1u : 0u;
   for (uint32_t depth = 1; depth < P.max_depth; ++depth) {
+    const unsigned live = __ballot_sync(0xffffffffu, alive);
+    if (!live) break;
     TraceResult h;
-    if (!closest_hit(S, st, ro, rd, h, err)) break;
+    if (alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    if (!alive) continue;
+    if (h.tri < 0) {
+      alive = false;
+      continue;
+    }
     const Vertex v = shade_hit<Stack>(S, h, rd);
     const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
     BdVertex& pv = vs[n];
@@ -382,12 +425,18 @@ __device__ __noinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& s
     pv.pdf_rev = 0.0f;
     pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
     ++n;
-    if (m.kind == kDevEmissive) break;
+    if (m.kind == kDevEmissive) {
+      alive = false;
+      continue;
+    }
     float ud0, ud1;
     ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
     const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
     MatSample s;
-    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, true, s)) break;
+    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, true, s)) {
+      alive = false;
+      continue;
+    }
     pv.flags = s.delta ? kBdDelta : kBdConnectible;
     vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
     ro = offset_origin(v.p, v.ng, s.wi);
@@ -399,24 +448,44 @@ __device__ __noinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& s
   return n;
 }
 
-// bdpt::trace_radiance for one sample (bdpt.rs:70-131)
+// bdpt::trace_radiance for one sample (bdpt.rs:70-131), warp-synchronous.  The
+// connections run over k = li * nc + ci in the reference's (light, camera)
+// order; their MIS weights are finite (in [0, 1]), so a zero connection adds
+// exactly zero and is skipped with its visibility ray and pdfs.
 template <class Stack>
-__device__ V3 trace_bdpt(const DevRender& S, Stack& st, const RenderLaunch& P, const PathSamplerDev& ps, V3 ro, V3 rd,
-                         uint32_t* err) {
+__device__ V3 trace_bdpt(const DevRender& S, Stack& st, bool valid, const RenderLaunch& P, const PathSamplerDev& ps,
+                         V3 ro, V3 rd, uint32_t* err) {
   BdVertex cam[kBdptMaxDepth], lig[kBdptMaxDepth];
   V3 L = V3{0.0f, 0.0f, 0.0f};
-  const uint32_t nc = bdpt_camera_subpath(S, st, P, ps, ro, rd, cam, L, err);
-  const uint32_t nl = bdpt_light_subpath(S, st, P, ps, lig, err);
-  for (uint32_t li = 0; li < nl; ++li)
-    for (uint32_t ci = 0; ci < nc; ++ci) {
-      if (!(lig[li].flags & kBdConnectible) || !(cam[ci].flags & kBdConnectible)) continue;
-      // the MIS weight is finite (in [0, 1]), so a zero connection adds exactly
-      // zero whatever it is: skip its four pdf evaluations
-      const V3 c = bdpt_connect(S, st, lig[li], cam[ci], err);
-      if (c.x == 0.0f && c.y == 0.0f && c.z == 0.0f) continue;
-      const float w = bdpt_mis(S, lig, li + 1, cam, ci + 1);
-      L = L + w * c;
+  const uint32_t nc = bdpt_camera_subpath(S, st, valid, P, ps, ro, rd, cam, L, err);
+  const uint32_t nl = bdpt_light_subpath(S, st, valid, P, ps, lig, err);
+  const uint32_t np = valid ? nl * nc : 0u;
+  const uint32_t max_np = __reduce_max_sync(0xffffffffu, np);
+  for (uint32_t k = 0; k < max_np; ++k) {
+    bool want = false;
+    BdConnection cn;
+    uint32_t li = 0, ci = 0;
+    if (k < np) {
+      li = k / nc;
+      ci = k - li * nc;
+      if ((lig[li].flags & kBdConnectible) && (cam[ci].flags & kBdConnectible))
+        want = bdpt_connect_prepare(S, lig[li], cam[ci], cn);
     }
+    const unsigned tm = __ballot_sync(0xffffffffu, want);
+    if (!tm) continue;
+    TraceResult h;
+    if (want)
+      trace_ray_ww<0>(S.geo, st, tm, cn.origin.x, cn.origin.y, cn.origin.z, cn.dir.x, cn.dir.y, cn.dir.z,
+                      __int_as_float(0x7f800000), h, err);
+    if (!want) continue;
+    // visible_between (bdpt.rs:577-602)
+    if (h.tri >= 0) {
+      const bool target = (uint32_t)h.inst == cam[ci].v.inst && (uint32_t)h.tri == cam[ci].v.tri;
+      if (!target && !(h.t >= cn.dist * (1.0f - kShadowTolerance))) continue;
+    }
+    const float w = bdpt_mis(S, lig, li + 1, cam, ci + 1);
+    L = L + w * cn.c;
+  }
   return L;
 }
 

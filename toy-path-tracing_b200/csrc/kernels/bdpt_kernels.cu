@@ -1,6 +1,6 @@
-// BDPT kernel: one thread per (pixel, sample), integrator/bdpt.rs.  Same grid
-// policy and per-sample output as the MIS megakernel; the per-pixel running
-// mean is the shared accumulate kernel.
+// BDPT kernel: one thread per (pixel, sample), integrator/bdpt.rs, the lanes of
+// a warp stepping through their subpaths and connections together (see
+// trace_bdpt).  The per-pixel running mean is the shared accumulate kernel.
 #include "../api/internal.h"
 #include "../device/bdpt.cuh"
 
@@ -15,9 +15,14 @@ __global__ void __launch_bounds__(kBdptBlock) render_bdpt_kernel(DevRender S, Re
   __shared__ uint32_t stack_sh[kBdptShStack * kBdptBlock];
   SplitStack<kBdptShStack> st;
   st.sh = stack_sh + threadIdx.x;
+  // warp-uniform loop: the lanes of a warp take consecutive samples together
+  // (trace_bdpt is warp-synchronous); lanes past the end carry no sample
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_paths; k += stride) {
-    const uint64_t path = first_path + k;
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < n_paths; base += stride) {
+    const uint64_t k = base + lane;
+    const bool valid = k < n_paths;
+    const uint64_t path = first_path + (valid ? k : 0);
     const uint32_t pixel = (uint32_t)(path / P.spp);
     const uint32_t sample = (uint32_t)(path % P.spp);
     const uint32_t px = pixel % P.width, py = pixel / P.width;
@@ -29,10 +34,12 @@ __global__ void __launch_bounds__(kBdptBlock) render_bdpt_kernel(DevRender S, Re
     const float fy = ((float)py + 0.5f) + 0.5f * tent(c1);
     const V3 d = camera_dir(P.cam, P.width, P.height, fx, fy);
     const V3 o = V3{P.cam.eye[0], P.cam.eye[1], P.cam.eye[2]};
-    const V3 L = trace_bdpt(S, st, P, ps, o, d, err);
-    samples[3 * k + 0] = L.x;
-    samples[3 * k + 1] = L.y;
-    samples[3 * k + 2] = L.z;
+    const V3 L = trace_bdpt(S, st, valid, P, ps, o, d, err);
+    if (valid) {
+      samples[3 * k + 0] = L.x;
+      samples[3 * k + 1] = L.y;
+      samples[3 * k + 2] = L.z;
+    }
   }
 }
 
