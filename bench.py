@@ -50,6 +50,9 @@ def parse_args():
     p.add_argument("--no-render", action="store_true", help="skip the render workload block")
     # profiling shapes of the render block (defaults: the plain-MIS configuration)
     p.add_argument("--render-only", action="store_true", help="run the render block alone")
+    p.add_argument("--only", choices=["render", "large", "batch", "adjoint"], default=None,
+                   help="run one block alone (profiling); prints a JSON line with that block")
+    p.add_argument("--large-res", type=int, nargs=2, default=(1920, 1080), help="large-scene resolution")
     p.add_argument("--render-res", type=int, default=256)
     p.add_argument("--render-spp", type=int, default=64)
     p.add_argument("--render-exec", choices=["both", "wavefront", "megakernel"], default="both")
@@ -58,6 +61,7 @@ def parse_args():
     p.add_argument("--no-batch", action="store_true", help="skip the batched-render block")
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-render block")
     p.add_argument("--large-spp", type=int, default=16, help="spp timed on the large scene")
+    p.add_argument("--adjoint-steps", type=int, default=200, help="Adam steps of the inverse-rendering run")
     p.add_argument("--batch-spp-scale", type=float, default=0.25, help="spp scale of the batched workload")
     return p.parse_args()
 
@@ -309,7 +313,8 @@ def large_block(ctx, args, cpu=True):
     sc = tpt_scenes.grid_scene()
     scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
     setup_s = time.perf_counter() - t0
-    W, H, spp = 1920, 1080, args.large_spp
+    W, H = args.large_res
+    spp = args.large_spp
     st = torch.cuda.current_stream().cuda_stream
     img = torch.empty(W * H * 3, device="cuda")
     out = {"config": {"triangles": sc["triangles"], "emissive_triangles": sc["emissive_triangles"],
@@ -438,7 +443,7 @@ def adjoint_block(ctx, args, cpu=True):
     losses = []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(200):
+    for _ in range(args.adjoint_steps):
         opt.zero_grad()
         im = RenderFunction.apply(params, scene, job, list(range(64)), tpt_scenes.patch_material, mask, 0.0,
                                   adj_job)
@@ -449,7 +454,7 @@ def adjoint_block(ctx, args, cpu=True):
             params.copy_(torch.maximum(torch.minimum(params, hi), lo))
         losses.append(float(loss.detach()))
     adam_s = time.perf_counter() - t0
-    out["inverse_rendering"] = {"steps": 200, "adjoint_spp": 2 * spp, "loss_first": losses[0], "loss_last": losses[-1],
+    out["inverse_rendering"] = {"steps": args.adjoint_steps, "adjoint_spp": 2 * spp, "loss_first": losses[0], "loss_last": losses[-1],
                                 "loss_min": min(losses), "seconds": adam_s,
                                 "param_mae_start": float(np.abs(start - sc["params"]).mean()),
                                 "param_mae_end": float(np.abs(params.detach().numpy() - sc["params"]).mean())}
@@ -491,9 +496,14 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     ctx = tpt.Context(local)
     if args.render_only:
+        args.only = "render"
+    if args.only:
         if rank == 0:
-            line = {"render": render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline, args=args)}
-            print(json.dumps(line), flush=True)
+            cpu = not args.no_cpu_baseline
+            run = {"render": lambda: render_block(ctx, args.steps, args.warmup, cpu=cpu, args=args),
+                   "large": lambda: large_block(ctx, args, cpu=cpu), "batch": lambda: batch_block(ctx, args),
+                   "adjoint": lambda: adjoint_block(ctx, args, cpu=cpu)}[args.only]
+            print(json.dumps({args.only: run()}), flush=True)
         ctx.close()
         return 0
     mesh, batches = make_workload(rank, args.rays_log2)
