@@ -81,6 +81,24 @@ def config_dict(args, world):
     }
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The largest x over all ranks (the job's time is its slowest rank's)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_rank: float, seconds: float) -> float:
+    """Units all ranks processed per second of the slowest rank (weak scaling:
+    every rank runs its own replica of the workload)."""
+    return world * units_per_rank / seconds
+
+
 def make_workload(rank: int, rays_log2: int):
     import tpt_scenes
 
@@ -557,12 +575,8 @@ def run_ours(args):
     clk = clocks.stop()
     elapsed_ms = t0.elapsed_time(t1)
     dom_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
-    if world > 1:
-        tmax = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(tmax.item())
-    total_rays = world * len(queries) * n * args.steps
-    value = total_rays / (elapsed_ms / 1e3)
+    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    value = whole_job_rate(world, len(queries) * n * args.steps, elapsed_ms / 1e3)
 
     # end to end through the host-pointer entry point, pinned host buffers
     h_rays = [torch.from_numpy(b).pin_memory() for b in batches]
@@ -589,11 +603,8 @@ def run_ours(args):
         e2e_step()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - w0
-    if world > 1:
-        tm = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        e2e_s = float(tm.item())
-    e2e_value = world * len(queries) * n * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(e2e_s, world)
+    e2e_value = whole_job_rate(world, len(queries) * n * e2e_steps, e2e_s)
 
     peak, peak_kind = measured_peak()
     achieved_gbs = algo_bytes / (dom_ms / 1e3) / 1e9
