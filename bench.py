@@ -341,7 +341,8 @@ def large_block(ctx, args, cpu=True):
            "unit": "Msamples/s", "upload_s": setup_s}
     for name, ex, integ, depth, s_spp in (("mis_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_MIS, 16, spp),
                                           ("mis_megakernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_MIS, 16, spp),
-                                          ("bdpt", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_BDPT, 10, 1)):
+                                          ("bdpt_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_BDPT, 10, 1),
+                                          ("bdpt_single_kernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_BDPT, 10, 1)):
         job = scene.job(sc["camera"], W, H, s_spp, depth, integrator=integ, execution=ex)
         ms = _time_ms(lambda: scene.render_device(job, img.data_ptr(), st))
         out[name] = {"value": W * H * s_spp / ms / 1e3, "ms_per_image": ms, "spp": s_spp}

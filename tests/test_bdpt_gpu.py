@@ -1,5 +1,9 @@
 """Device BDPT (integrator/bdpt.rs) against the oracle restatement.
 
+The wavefront execution (subpaths, connection queue, visibility rays through
+the persistent traversal kernel, MIS, in-order per-sample sums) and the
+one-kernel execution give the same samples bit for bit.
+
 Same bar as the MIS render tests: with the reference's per-pixel sample streams
 replayed, >= 99% of the per-sample radiances agree to 1e-5 relative and >= 99.5%
 to 1e-3 (libm last-bit differences compound through the MIS weights' products
@@ -21,12 +25,12 @@ def rel_rmse(a, b):
     return float(np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) / np.sqrt(np.mean(b.astype(np.float64) ** 2)))
 
 
-def bdpt_samples(dev, sc, w, h, spp, depth):
+def bdpt_samples(dev, sc, w, h, spp, depth, execution=tpt.EXEC_WAVEFRONT):
     import torch
 
     n = w * h * spp
     out = torch.empty(n * 3, dtype=torch.float32, device="cuda")
-    job = dev.job(sc["camera"], w, h, spp, depth, integrator=tpt.INTEGRATOR_BDPT)
+    job = dev.job(sc["camera"], w, h, spp, depth, integrator=tpt.INTEGRATOR_BDPT, execution=execution)
     dev.render_samples_device(job, 0, n, out.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     return out.cpu().numpy().reshape(n, 3)
@@ -89,3 +93,19 @@ def test_bdpt_depth_limit(ctx):
         dev.render(sc["camera"], 8, 8, 1, 17, integrator=tpt.INTEGRATOR_BDPT)
     img = dev.render(sc["camera"], 8, 8, 1, 16, integrator=tpt.INTEGRATOR_BDPT)
     assert np.all(np.isfinite(img))
+
+
+@pytest.mark.parametrize("kind", ["openpbr", "mixed"])
+def test_bdpt_wavefront_equals_single_kernel(ctx, kind):
+    sc = tpt_scenes.cornell_box(3, tpt_scenes.OPENPBR)
+    if kind == "mixed":
+        for k, m in enumerate(MIXED):
+            sc["materials"][3 + k] = m
+    dev, _ = scene_pair(ctx, sc)
+    a = bdpt_samples(dev, sc, 40, 24, 8, 10, tpt.EXEC_WAVEFRONT)
+    b = bdpt_samples(dev, sc, 40, 24, 8, 10, tpt.EXEC_MEGAKERNEL)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    ia = dev.render(sc["camera"], 32, 32, 4, 7, integrator=tpt.INTEGRATOR_BDPT, execution=tpt.EXEC_WAVEFRONT)
+    ib = dev.render(sc["camera"], 32, 32, 4, 7, integrator=tpt.INTEGRATOR_BDPT, execution=tpt.EXEC_MEGAKERNEL)
+    assert np.array_equal(ia.view(np.uint32), ib.view(np.uint32))
+    dev.close()

@@ -102,3 +102,24 @@ def test_scene_without_lights_is_black(ctx):
     dev = upload(ctx, sc)
     img = dev.render(sc["camera"], 16, 16, 4, 4)
     assert np.count_nonzero(img) == 0
+
+
+@pytest.mark.parametrize("kind", [tpt_scenes.LAMBERT, tpt_scenes.OPENPBR], ids=["lambert", "openpbr"])
+def test_converged_image_matches_fp64_oracle(ctx, kind):
+    """4096 spp: the device image (f32 running mean, main.rs:107-123) against
+    the oracle's samples of the same streams averaged in float64.  Bar: 2e-3
+    relative RMSE (measured differences come from the rare samples whose path
+    diverges through last-bit transcendental differences, plus f32 rounding of
+    the running mean)."""
+    sc = tpt_scenes.cornell_box(1, kind)
+    dev = upload(ctx, sc)
+    ref = orc.RenderScene(sc, dev.light_tree())
+    w = h = 24
+    spp, depth = 4096, 8
+    img = dev.render(sc["camera"], w, h, spp, depth).reshape(-1, 3).astype(np.float64)
+    smp = ref.samples(sc["camera"], w, h, spp, depth, 0, w * h * spp).astype(np.float64)
+    fp64 = smp.reshape(w * h, spp, 3).mean(1) * sc["camera"].get("exposure", 1.0)
+    err = rel_rmse(img, fp64)
+    print("converged rel RMSE vs fp64 oracle:", err)
+    assert err <= 2e-3
+    dev.close()

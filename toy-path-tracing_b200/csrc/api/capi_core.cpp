@@ -236,6 +236,7 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
   if (ctx->d_scratch) cudaFree(ctx->d_scratch);
   if (ctx->d_wf) cudaFree(ctx->d_wf);
   if (ctx->d_jobs) cudaFree(ctx->d_jobs);
+  if (ctx->d_bd) cudaFree(ctx->d_bd);
   for (auto& kv : ctx->da_tables) cudaFree(kv.second);
   if (ctx->d_cec_e) cudaFree(ctx->d_cec_e);
   if (ctx->d_dec_e) cudaFree(ctx->d_dec_e);

@@ -170,6 +170,68 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
   return cuda_check(ctx, e, "wavefront launch");
 }
 
+// BDPT wavefront arena for `max_vertices` vertices per subpath: as many samples
+// as keep the connection queue at 2^24 slots (each sample has at most
+// max_vertices^2 connections).
+tpt_status ensure_bdpt_wavefront(tpt_context* ctx, uint32_t max_vertices) {
+  const uint32_t mv = std::max<uint32_t>(1, max_vertices);
+  const uint64_t samples = std::max<uint64_t>(1024, (1ull << 24) / ((uint64_t)mv * mv));
+  const uint64_t pairs = samples * mv * mv;
+  if (ctx->d_bd && ctx->bd.max_vertices == mv) return TPT_OK;
+  const size_t bytes = samples * 2 * mv * (size_t)kBdVertexBytes + samples * (3 * 4 + 3 * 4) +
+                       pairs * (4 + 12 + 12 + 4) + pairs * (7 * 4 + 4 + 4 + 4 + 4) + 16 * 256;
+  if (ctx->d_bd) {
+    cudaDeviceSynchronize();
+    cudaFree(ctx->d_bd);
+    ctx->d_bd = nullptr;
+    ctx->d_bd_bytes = 0;
+    ctx->bd = BdWfBuffers{};
+  }
+  tpt_status st = cuda_check(ctx, cudaMalloc(&ctx->d_bd, bytes), "cudaMalloc(BDPT wavefront arena)");
+  if (st) return st;
+  ctx->d_bd_bytes = bytes;
+  char* p = (char*)ctx->d_bd;
+  auto take = [&](size_t b) {
+    char* r = p;
+    p += (b + 255) & ~(size_t)255;
+    return r;
+  };
+  BdWfBuffers& B = ctx->bd;
+  B.sample_capacity = (uint32_t)samples;
+  B.pair_capacity = (uint32_t)pairs;
+  B.max_vertices = mv;
+  B.verts = (BdVertex*)take(samples * 2 * mv * (size_t)kBdVertexBytes);
+  B.nc = (uint32_t*)take(samples * 4);
+  B.nl = (uint32_t*)take(samples * 4);
+  B.pair_base = (uint32_t*)take(samples * 4);
+  B.L0 = (float*)take(samples * 12);
+  B.pair_sample = (uint32_t*)take(pairs * 4);
+  B.c = (float*)take(pairs * 12);
+  B.contrib = (float*)take(pairs * 12);
+  B.dist = (float*)take(pairs * 4);
+  B.s_ray = (float*)take(pairs * 28);
+  B.s_pair = (uint32_t*)take(pairs * 4);
+  B.s_tri = (int32_t*)take(pairs * 4);
+  B.s_inst = (int32_t*)take(pairs * 4);
+  B.s_t = (float*)take(pairs * 4);
+  B.counts = (uint32_t*)take(256);
+  return TPT_OK;
+}
+
+tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
+                                 uint64_t n, float* samples, cudaStream_t s) {
+  tpt_status st = ensure_bdpt_wavefront(ctx, L.max_depth);
+  if (st) return st;
+  const BdWfBuffers& B = ctx->bd;
+  for (uint64_t b = 0; b < n; b += B.sample_capacity) {
+    const uint32_t m = (uint32_t)std::min<uint64_t>(B.sample_capacity, n - b);
+    cudaError_t e = launch_bdpt_wavefront(job->scene->geo, job->scene->render, L, B, first + b, m, samples + 3 * b,
+                                          next_counter(ctx), ctx->d_err, ctx->num_sms, s);
+    if ((st = cuda_check(ctx, e, "BDPT wavefront launch"))) return st;
+  }
+  return TPT_OK;
+}
+
 // Pixels per chunk: the per-sample buffer stays below 1 GiB and a chunk has at
 // most `capacity` paths (the wavefront arena's slot count; 0 = 2^22).
 uint32_t chunk_pixels(const RenderLaunch& L, uint32_t capacity) {
@@ -221,7 +283,9 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
   const uint32_t exec = job->execution == TPT_EXEC_AUTO ? ctx->tuned_execution : job->execution;
   for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
     const uint32_t n = std::min(cp, npix - p0);
-    if (exec == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
+    if (job->integrator == TPT_INTEGRATOR_BDPT && exec != TPT_EXEC_MEGAKERNEL) {
+      if ((st = render_bdpt_wavefront(ctx, job, L, (uint64_t)p0 * L.spp, (uint64_t)n * L.spp, samples, s))) return st;
+    } else if (exec == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
       cudaError_t e = launch_render(job->scene->geo, job->scene->render, L, samples, (uint64_t)p0 * L.spp,
                                     (uint64_t)n * L.spp, ctx->d_err, ctx->num_sms, s, next_counter(ctx));
       if ((st = cuda_check(ctx, e, "render kernel launch"))) return st;
@@ -246,6 +310,8 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   const uint32_t exec = job->execution == TPT_EXEC_AUTO ? ctx->tuned_execution : job->execution;
+  if (job->integrator == TPT_INTEGRATOR_BDPT && exec != TPT_EXEC_MEGAKERNEL)
+    return render_bdpt_wavefront(ctx, job, L, first, count, out_samples, s);
   if (exec == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT)
     return cuda_check(ctx,
                       launch_render(job->scene->geo, job->scene->render, L, out_samples, first, count, ctx->d_err,

@@ -41,6 +41,10 @@ struct tpt_context {
   void* d_wf = nullptr;
   size_t d_wf_bytes = 0;
   tpt::WfBuffers wf{};
+  // BDPT wavefront arena (grown on demand) and its layout
+  void* d_bd = nullptr;
+  size_t d_bd_bytes = 0;
+  tpt::BdWfBuffers bd{};
   // batched renders: device job table (grown on demand) and the wavefront
   // capacity (path slots per chunk; 0 = 2^22)
   tpt::DevJob* d_jobs = nullptr;
@@ -115,6 +119,14 @@ cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const
                           unsigned long long* counter);
 cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first_pixel, uint32_t n_pixels,
                               float exposure, float* image, cudaStream_t stream);
+// bdpt_wavefront.cu: n samples (paths first_path..) of a BDPT job through the
+// wavefront stages (n <= B.sample_capacity); per-sample radiance into samples.
+cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
+                                  const BdWfBuffers& B, uint64_t first_path, uint32_t n, float* samples,
+                                  unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s);
+// capi_render.cpp: BDPT paths [first, first + n) through the wavefront, in chunks.
+tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
+                                 uint64_t n, float* samples, cudaStream_t s);
 // bdpt_kernels.cu (launch_render dispatches to it for TPT_INTEGRATOR_BDPT)
 cudaError_t launch_render_bdpt(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P, float* samples,
                                uint64_t first_path, uint64_t n_paths, uint32_t* err, int num_sms, cudaStream_t stream);

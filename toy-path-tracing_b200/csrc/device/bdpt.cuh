@@ -140,6 +140,8 @@ struct BdVertex {
   uint32_t flags;
 };
 
+static_assert(sizeof(BdVertex) <= kBdVertexBytes, "BDPT vertex record");
+
 __device__ __forceinline__ float remap0(float x) { return x == 0.0f ? 1.0f : x; }
 
 // bdpt.rs:626-642
@@ -191,7 +193,7 @@ __device__ __forceinline__ float vertex_pdf_area(const DevRender& S, const BdVer
 }
 
 // bdpt.rs:717-746
-__device__ __noinline__ float camera_light_hit_mis(const DevRender& S, const BdVertex* cp, uint32_t n) {
+static __device__ __noinline__ float camera_light_hit_mis(const DevRender& S, const BdVertex* cp, uint32_t n) {
   if (n <= 1) return 1.0f;
   const uint32_t pt = n - 1, ptm = pt - 1;
   const float pt_rev = area_light_origin_pdf(S, cp[pt]);

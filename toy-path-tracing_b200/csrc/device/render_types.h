@@ -166,6 +166,29 @@ struct DevAdjoint {
   uint32_t mask;           // parameter groups to differentiate (bit g = group g)
 };
 
+// BDPT wavefront state (kernels/bdpt_wavefront.cu) for up to sample_capacity
+// samples of max_vertices vertices per subpath and pair_capacity connections.
+struct BdVertex;
+constexpr uint32_t kBdVertexBytes = 128;  // >= sizeof(BdVertex), for host-side sizing
+struct BdWfBuffers {
+  uint32_t sample_capacity, pair_capacity, max_vertices, pad;
+  BdVertex* verts;       // [sample][camera 0..max_vertices, light 0..max_vertices]
+  uint32_t* nc;          // camera subpath length per sample
+  uint32_t* nl;          // light subpath length per sample
+  uint32_t* pair_base;   // first connection slot of each sample
+  float* L0;             // camera-subpath emission per sample (3 planes interleaved)
+  uint32_t* pair_sample; // sample of each connection slot
+  float* c;              // connection contribution before MIS (x3)
+  float* contrib;        // MIS-weighted contribution, zero if none (x3)
+  float* dist;           // connection length
+  float* s_ray;          // visibility rays: 7 planes of pair_capacity
+  uint32_t* s_pair;      // connection slot of each visibility ray
+  int32_t* s_tri;
+  int32_t* s_inst;
+  float* s_t;
+  uint32_t* counts;      // [0] connections, [1] visibility rays
+};
+
 // Wavefront state: per path slot of a chunk (capacity slots), two ray queues,
 // the hit records of the current queue and the shadow queue.  Planes of a
 // structured array are `capacity` elements apart.

@@ -1,0 +1,201 @@
+// BDPT as a wavefront (integrator/bdpt.rs:70-131 split into stages), per chunk
+// of samples:
+//
+//   bd_subpaths  : per sample, the camera and the light subpath (warp-
+//                  synchronous, as the one-kernel BDPT) into HBM; camera-side
+//                  emission into L0; the sample's nl * nc connection slots
+//                  allocated contiguously in a pair queue (one atomic per warp)
+//   bd_connect   : per pair, bdpt_connect_prepare; non-zero contributions
+//                  append their visibility ray to the shadow queue
+//   traverse     : the persistent traversal kernel over the shadow queue
+//   bd_resolve   : per visible connection, the MIS weight (bdpt_mis) times the
+//                  contribution, into the pair's slot
+//   bd_finalize  : per sample, L0 plus the pair slots in the reference's
+//                  (light, camera) order
+//
+// Every connection does the arithmetic of the one-kernel BDPT in the same
+// order (the sums per sample too), so both executions give the same samples
+// bit for bit.  The connections, the bulk of the work, thus run as uniform
+// kernels over compacted queues instead of inside each sample's thread.
+#include "../api/internal.h"
+#include "../device/bdpt.cuh"
+
+namespace tpt {
+
+constexpr int kBdWfBlock = 128;
+constexpr int kBdShStack = 32;
+
+// Warp-exclusive prefix sum of `v` (all lanes call); returns the lane's offset
+// and the warp total in `total`.
+__device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, uint32_t& total) {
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  total = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+__global__ void __launch_bounds__(kBdWfBlock) bd_subpaths(DevRender S, RenderLaunch P, BdWfBuffers B,
+                                                          uint64_t first_path, uint32_t n, uint32_t* err) {
+  __shared__ uint32_t stack_sh[kBdShStack * kBdWfBlock];
+  SplitStack<kBdShStack> st;
+  st.sh = stack_sh + threadIdx.x;
+  const uint32_t MD = B.max_vertices;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x - lane); base < n; base += stride) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    const uint64_t path = first_path + (valid ? i : 0);
+    const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
+    const uint32_t px = pixel % P.width, py = pixel / P.width;
+    PathSamplerDev ps;
+    ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+    float c0, c1;
+    ps.sample_2d(kDimCamera, c0, c1);
+    const float fx = ((float)px + 0.5f) + 0.5f * tent(c0);
+    const float fy = ((float)py + 0.5f) + 0.5f * tent(c1);
+    const V3 d = camera_dir(P.cam, P.width, P.height, fx, fy);
+    const V3 o = V3{P.cam.eye[0], P.cam.eye[1], P.cam.eye[2]};
+    BdVertex* cam = B.verts + (size_t)(valid ? i : 0) * 2 * MD;
+    V3 L = V3{0.0f, 0.0f, 0.0f};
+    const uint32_t nc = bdpt_camera_subpath(S, st, valid, P, ps, o, d, cam, L, err);
+    const uint32_t nl = bdpt_light_subpath(S, st, valid, P, ps, cam + MD, err);
+    const uint32_t np = valid ? nl * nc : 0u;
+    uint32_t total;
+    const uint32_t off = warp_exclusive_scan(np, total);
+    uint32_t pbase = 0;
+    if (lane == 31 && total) pbase = atomicAdd(B.counts, total);
+    pbase = __shfl_sync(0xffffffffu, pbase, 31) + off;
+    if (valid) {
+      B.nc[i] = nc;
+      B.nl[i] = nl;
+      B.pair_base[i] = pbase;
+      B.L0[3 * (size_t)i] = L.x;
+      B.L0[3 * (size_t)i + 1] = L.y;
+      B.L0[3 * (size_t)i + 2] = L.z;
+      for (uint32_t k = 0; k < np; ++k) B.pair_sample[pbase + k] = i;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t warp_append1(uint32_t* counter, bool pred) {
+  const unsigned act = __activemask();
+  const unsigned m = __ballot_sync(act, pred);
+  const unsigned lane = threadIdx.x & 31u;
+  const int leader = __ffs(act) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader && m) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(act, base, leader);
+  return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(kBdWfBlock) bd_connect(DevRender S, BdWfBuffers B) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= B.counts[0]) return;
+  const uint32_t MD = B.max_vertices;
+  const uint32_t i = B.pair_sample[j];
+  const uint32_t k = j - B.pair_base[i];
+  const uint32_t nc = B.nc[i];
+  const uint32_t li = k / nc, ci = k - (k / nc) * nc;
+  const BdVertex* cam = B.verts + (size_t)i * 2 * MD;
+  const BdVertex& lv = cam[MD + li];
+  const BdVertex& cv = cam[ci];
+  BdConnection cn;
+  bool want = false;
+  if ((lv.flags & kBdConnectible) && (cv.flags & kBdConnectible)) want = bdpt_connect_prepare(S, lv, cv, cn);
+  B.contrib[3 * (size_t)j] = 0.0f;
+  B.contrib[3 * (size_t)j + 1] = 0.0f;
+  B.contrib[3 * (size_t)j + 2] = 0.0f;
+  const uint32_t q = warp_append1(&B.counts[1], want);
+  if (!want) return;
+  const uint32_t C = B.pair_capacity;
+  float* r = B.s_ray;
+  r[q] = cn.origin.x;
+  r[C + q] = cn.origin.y;
+  r[2 * C + q] = cn.origin.z;
+  r[3 * C + q] = cn.dir.x;
+  r[4 * C + q] = cn.dir.y;
+  r[5 * C + q] = cn.dir.z;
+  r[6 * C + q] = __int_as_float(0x7f800000);
+  B.s_pair[q] = j;
+  B.c[3 * (size_t)j] = cn.c.x;
+  B.c[3 * (size_t)j + 1] = cn.c.y;
+  B.c[3 * (size_t)j + 2] = cn.c.z;
+  B.dist[j] = cn.dist;
+}
+
+__global__ void __launch_bounds__(kBdWfBlock) bd_resolve(DevRender S, BdWfBuffers B) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= B.counts[1]) return;
+  const uint32_t MD = B.max_vertices;
+  const uint32_t j = B.s_pair[e];
+  const uint32_t i = B.pair_sample[j];
+  const uint32_t k = j - B.pair_base[i];
+  const uint32_t nc = B.nc[i];
+  const uint32_t li = k / nc, ci = k - (k / nc) * nc;
+  const BdVertex* cam = B.verts + (size_t)i * 2 * MD;
+  // visible_between (bdpt.rs:577-602)
+  const int32_t tri = B.s_tri[e];
+  if (tri >= 0) {
+    const bool target = (uint32_t)B.s_inst[e] == cam[ci].v.inst && (uint32_t)tri == cam[ci].v.tri;
+    if (!target && !(B.s_t[e] >= B.dist[j] * (1.0f - kShadowTolerance))) return;
+  }
+  const float w = bdpt_mis(S, cam + MD, li + 1, cam, ci + 1);
+  const V3 c = V3{B.c[3 * (size_t)j], B.c[3 * (size_t)j + 1], B.c[3 * (size_t)j + 2]};
+  const V3 wc = w * c;
+  B.contrib[3 * (size_t)j] = wc.x;
+  B.contrib[3 * (size_t)j + 1] = wc.y;
+  B.contrib[3 * (size_t)j + 2] = wc.z;
+}
+
+__global__ void __launch_bounds__(kBdWfBlock) bd_finalize(BdWfBuffers B, uint32_t n, float* __restrict__ samples) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  V3 L = V3{B.L0[3 * (size_t)i], B.L0[3 * (size_t)i + 1], B.L0[3 * (size_t)i + 2]};
+  const uint32_t np = B.nl[i] * B.nc[i];
+  const float* c = B.contrib + 3 * (size_t)B.pair_base[i];
+  for (uint32_t k = 0; k < np; ++k) {
+    const V3 wc = V3{c[3 * k], c[3 * k + 1], c[3 * k + 2]};
+    if (wc.x == 0.0f && wc.y == 0.0f && wc.z == 0.0f) continue;  // a zero connection adds exactly zero
+    L = L + wc;
+  }
+  samples[3 * (size_t)i] = L.x;
+  samples[3 * (size_t)i + 1] = L.y;
+  samples[3 * (size_t)i + 2] = L.z;
+}
+
+static inline unsigned grid_of(uint64_t n) { return (unsigned)((n + kBdWfBlock - 1) / kBdWfBlock); }
+
+cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
+                                  const BdWfBuffers& B, uint64_t first_path, uint32_t n, float* samples,
+                                  unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  DevRender S{geo, rd};
+  cudaError_t e = cudaMemsetAsync(B.counts, 0, 2 * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  static int bpsm = 0;
+  if (bpsm == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, bd_subpaths, kBdWfBlock, 0) != cudaSuccess || bpsm <= 0)
+      bpsm = 2;
+  }
+  const uint64_t blocks = std::min<uint64_t>(grid_of(n), (uint64_t)num_sms * bpsm * 8);
+  bd_subpaths<<<(unsigned)blocks, kBdWfBlock, 0, s>>>(S, P, B, first_path, n, err);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  bd_connect<<<grid_of(B.pair_capacity), kBdWfBlock, 0, s>>>(S, B);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  e = launch_traverse_strided(geo, B.s_ray, B.pair_capacity, B.pair_capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t,
+                              B.s_inst, nullptr, B.pair_capacity, counter, err, num_sms, s, nullptr, nullptr,
+                              B.counts + 1);
+  if (e != cudaSuccess) return e;
+  bd_resolve<<<grid_of(B.pair_capacity), kBdWfBlock, 0, s>>>(S, B);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  bd_finalize<<<grid_of(n), kBdWfBlock, 0, s>>>(B, n, samples);
+  return cudaGetLastError();
+}
+
+}  // namespace tpt
