@@ -118,3 +118,16 @@ def test_autotune_applies_a_setting_that_renders_the_same(ctx, mixed):
     finally:
         ctx.wavefront_capacity = 0
         ctx.set_graphs(True)
+
+
+def test_host_render_of_several_jobs_is_batched_and_equal(ctx, mixed):
+    """tpt_render with several wavefront jobs takes the batched path; images equal the single renders."""
+    import ctypes as C
+
+    ref = _render_each(ctx, mixed)
+    outs = [np.empty(j.width * j.height * 3, np.float32) for j in mixed]
+    arr = (tpt.RenderJob * len(mixed))(*mixed)
+    ptrs = (C.c_void_p * len(mixed))(*[o.ctypes.data for o in outs])
+    assert tpt.lib().tpt_render(ctx.h, arr, len(mixed), ptrs) == 0
+    for a, b in zip(outs, ref):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))

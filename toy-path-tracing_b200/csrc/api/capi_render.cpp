@@ -178,8 +178,10 @@ tpt_status ensure_bdpt_wavefront(tpt_context* ctx, uint32_t max_vertices) {
   const uint64_t samples = std::max<uint64_t>(1024, (1ull << 24) / ((uint64_t)mv * mv));
   const uint64_t pairs = samples * mv * mv;
   if (ctx->d_bd && ctx->bd.max_vertices == mv) return TPT_OK;
+  const uint64_t q = 2 * samples;  // subpath ray queue slots (camera + light per sample)
   const size_t bytes = samples * 2 * mv * (size_t)kBdVertexBytes + samples * (3 * 4 + 3 * 4) +
-                       pairs * (4 + 12 + 12 + 4) + pairs * (7 * 4 + 4 + 4 + 4 + 4) + 16 * 256;
+                       pairs * (4 + 12 + 12 + 4) + pairs * (7 * 4 + 4 + 4 + 4 + 4) +
+                       samples * 2 * (size_t)kBdStateBytes + q * (2 * 7 * 4 + 2 * 4 + 4 + 4 + 4 + 12) + 32 * 256;
   if (ctx->d_bd) {
     cudaDeviceSynchronize();
     cudaFree(ctx->d_bd);
@@ -214,6 +216,16 @@ tpt_status ensure_bdpt_wavefront(tpt_context* ctx, uint32_t max_vertices) {
   B.s_tri = (int32_t*)take(pairs * 4);
   B.s_inst = (int32_t*)take(pairs * 4);
   B.s_t = (float*)take(pairs * 4);
+  B.cam_state = (BdCamState*)take(samples * kBdStateBytes);
+  B.light_state = (BdLightState*)take(samples * kBdStateBytes);
+  for (int k = 0; k < 2; ++k) {
+    B.q_ray[k] = (float*)take(q * 28);
+    B.q_tag[k] = (uint32_t*)take(q * 4);
+  }
+  B.h_tri = (int32_t*)take(q * 4);
+  B.h_inst = (int32_t*)take(q * 4);
+  B.h_t = (float*)take(q * 4);
+  B.h_bary = (float*)take(q * 12);
   B.counts = (uint32_t*)take(256);
   return TPT_OK;
 }
@@ -329,6 +341,30 @@ tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, 
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (n_jobs < 0 || (n_jobs && (!jobs || !out_rgb))) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad job list");
   cudaSetDevice(ctx->device);
+  // several MIS wavefront jobs: one batched launch sequence
+  bool batch = n_jobs > 1;
+  for (int j = 0; j < n_jobs && batch; ++j) {
+    const uint32_t ex = jobs[j].execution == TPT_EXEC_AUTO ? ctx->tuned_execution : jobs[j].execution;
+    batch = jobs[j].integrator == TPT_INTEGRATOR_MIS && ex == TPT_EXEC_WAVEFRONT && out_rgb[j] && jobs[j].scene;
+  }
+  if (batch) {
+    std::vector<float*> d(n_jobs, nullptr);
+    std::vector<size_t> bytes(n_jobs);
+    tpt_status st = TPT_OK;
+    for (int j = 0; j < n_jobs && !st; ++j) {
+      bytes[j] = (size_t)jobs[j].width * jobs[j].height * 12;
+      st = cuda_check(ctx, cudaMallocAsync((void**)&d[j], std::max<size_t>(bytes[j], 16), ctx->stream),
+                      "cudaMallocAsync(image)");
+    }
+    if (!st) st = render_batch(ctx, jobs, n_jobs, d.data(), ctx->stream, ctx->batch_capacity);
+    for (int j = 0; j < n_jobs && !st; ++j)
+      st = cuda_check(ctx, cudaMemcpyAsync(out_rgb[j], d[j], bytes[j], cudaMemcpyDeviceToHost, ctx->stream),
+                      "D2H image");
+    for (float* p : d)
+      if (p) cudaFreeAsync(p, ctx->stream);
+    if (!st) st = check_device_errors(ctx, ctx->stream);
+    return st;
+  }
   for (int j = 0; j < n_jobs; ++j) {
     if (!out_rgb[j]) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output image");
     RenderLaunch L;

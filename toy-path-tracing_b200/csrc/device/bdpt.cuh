@@ -279,68 +279,90 @@ __device__ __forceinline__ bool bdpt_connect_prepare(const DevRender& S, const B
 // interior nodes together before testing leaves).  Each lane's own arithmetic
 // and order are those of bdpt.rs.
 
-// bdpt.rs:135-262 (no environment or non-area lights in scope)
+// State of a camera subpath between the iterations of bdpt.rs's camera loop.
+struct BdCamState {
+  V3 beta, pending_from;
+  float pending_pdf;
+  uint32_t n;
+  bool count_emission, have_pending, alive;
+};
+__device__ __forceinline__ void camera_state_init(BdCamState& c, bool valid) {
+  c.beta = V3{1.0f, 1.0f, 1.0f};
+  c.pending_from = V3{0.0f, 0.0f, 0.0f};
+  c.pending_pdf = 0.0f;
+  c.n = 0;
+  c.count_emission = true;
+  c.have_pending = false;
+  c.alive = valid;
+}
+
+// One iteration of the camera loop (bdpt.rs:135-262; no environment or
+// non-area lights in scope) after its ray (rd) was traced to h: the hit vertex
+// into vs[c.n], emission into L, and the next ray into (ro, rd) while c.alive.
+template <class Stack>
+__device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaunch& P, const PathSamplerDev& ps,
+                                            uint32_t depth, const TraceResult& h, V3& ro, V3& rd, BdVertex* vs,
+                                            BdCamState& c, V3& L) {
+  if (h.tri < 0) {
+    c.alive = false;
+    return;
+  }
+  const Vertex v = shade_hit<Stack>(S, h, rd);
+  const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
+  BdVertex& pv = vs[c.n];
+  pv.v = v;
+  pv.beta = c.beta;
+  pv.pdf_fwd = c.have_pending ? solid_angle_to_area(c.pending_pdf, c.pending_from, v.p, v.ng) : 0.0f;
+  pv.pdf_rev = 0.0f;
+  pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
+  const uint32_t n = ++c.n;
+  if (m.kind == kDevEmissive) {
+    const float w = c.count_emission ? 1.0f : camera_light_hit_mis(S, vs, n);
+    L = L + c.beta * emissive_le(m) * w;
+    c.alive = false;  // pure emitter: sample() is None
+    return;
+  }
+  float ud0, ud1;
+  ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
+  const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
+  MatSample s;
+  if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, false, s)) {
+    c.alive = false;
+    return;
+  }
+  pv.flags = s.delta ? kBdDelta : kBdConnectible;
+  if (n >= 2) vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
+  ro = offset_origin(v.p, v.ng, s.wi);
+  rd = s.wi;
+  c.beta = c.beta * s.weight;
+  if (depth + 1 >= 4) {
+    const float q = clampf(max_element(c.beta), 0.05f, 1.0f);
+    if (ps.sample_1d(vertex_dim(depth, kOffRr)) > q) {
+      c.alive = false;
+      return;
+    }
+    c.beta = c.beta / q;
+  }
+  c.have_pending = true;
+  c.pending_from = v.p;
+  c.pending_pdf = s.pdf;
+  c.count_emission = s.delta;
+}
+
 template <class Stack>
 __device__ __forceinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& st, bool valid,
                                                         const RenderLaunch& P, const PathSamplerDev& ps, V3 ro, V3 rd,
                                                         BdVertex* vs, V3& L, uint32_t* err) {
-  uint32_t n = 0;
-  V3 beta = V3{1.0f, 1.0f, 1.0f};
-  bool count_emission = true, have_pending = false, alive = valid;
-  V3 pending_from = V3{0.0f, 0.0f, 0.0f};
-  float pending_pdf = 0.0f;
+  BdCamState c;
+  camera_state_init(c, valid);
   for (uint32_t depth = 0; depth < P.max_depth; ++depth) {
-    const unsigned live = __ballot_sync(0xffffffffu, alive);
+    const unsigned live = __ballot_sync(0xffffffffu, c.alive);
     if (!live) break;
     TraceResult h;
-    if (alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
-    if (!alive) continue;
-    if (h.tri < 0) {
-      alive = false;
-      continue;
-    }
-    const Vertex v = shade_hit<Stack>(S, h, rd);
-    const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
-    BdVertex& pv = vs[n];
-    pv.v = v;
-    pv.beta = beta;
-    pv.pdf_fwd = have_pending ? solid_angle_to_area(pending_pdf, pending_from, v.p, v.ng) : 0.0f;
-    pv.pdf_rev = 0.0f;
-    pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
-    ++n;
-    if (m.kind == kDevEmissive) {
-      const float w = count_emission ? 1.0f : camera_light_hit_mis(S, vs, n);
-      L = L + beta * emissive_le(m) * w;
-      alive = false;  // pure emitter: sample() is None
-      continue;
-    }
-    float ud0, ud1;
-    ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
-    const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
-    MatSample s;
-    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, false, s)) {
-      alive = false;
-      continue;
-    }
-    pv.flags = s.delta ? kBdDelta : kBdConnectible;
-    if (n >= 2) vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
-    ro = offset_origin(v.p, v.ng, s.wi);
-    rd = s.wi;
-    beta = beta * s.weight;
-    if (depth + 1 >= 4) {
-      const float q = clampf(max_element(beta), 0.05f, 1.0f);
-      if (ps.sample_1d(vertex_dim(depth, kOffRr)) > q) {
-        alive = false;
-        continue;
-      }
-      beta = beta / q;
-    }
-    have_pending = true;
-    pending_from = v.p;
-    pending_pdf = s.pdf;
-    count_emission = s.delta;
+    if (c.alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    if (c.alive) camera_step<Stack>(S, P, ps, depth, h, ro, rd, vs, c, L);
   }
-  return n;
+  return c.n;
 }
 
 // sample_area_light_triangle and the light endpoint (bdpt.rs:264-300, 540-553):
@@ -399,55 +421,71 @@ __device__ __forceinline__ bool bdpt_light_endpoint(const DevRender& S, const Re
   return true;
 }
 
-// bdpt.rs:264-385
+// State of a light subpath between the iterations of bdpt.rs's light loop.
+struct BdLightState {
+  V3 beta, pending_from;
+  float pending_pdf;
+  uint32_t n;
+  bool alive;
+};
+
+static_assert(sizeof(BdCamState) <= kBdStateBytes && sizeof(BdLightState) <= kBdStateBytes, "BDPT loop states");
+
+// One iteration of the light loop (bdpt.rs:264-385) after its ray was traced to h.
+template <class Stack>
+__device__ __forceinline__ void light_step(const DevRender& S, const PathSamplerDev& ps, uint32_t depth,
+                                           const TraceResult& h, V3& ro, V3& rd, BdVertex* vs, BdLightState& l) {
+  if (h.tri < 0) {
+    l.alive = false;
+    return;
+  }
+  const Vertex v = shade_hit<Stack>(S, h, rd);
+  const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
+  BdVertex& pv = vs[l.n];
+  pv.v = v;
+  pv.beta = l.beta;
+  pv.pdf_fwd = solid_angle_to_area(l.pending_pdf, l.pending_from, v.p, v.ng);
+  pv.pdf_rev = 0.0f;
+  pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
+  const uint32_t n = ++l.n;
+  if (m.kind == kDevEmissive) {
+    l.alive = false;
+    return;
+  }
+  float ud0, ud1;
+  ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
+  const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
+  MatSample s;
+  if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, true, s)) {
+    l.alive = false;
+    return;
+  }
+  pv.flags = s.delta ? kBdDelta : kBdConnectible;
+  vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
+  ro = offset_origin(v.p, v.ng, s.wi);
+  rd = s.wi;
+  l.beta = l.beta * s.weight;
+  l.pending_from = v.p;
+  l.pending_pdf = s.pdf;
+}
+
 template <class Stack>
 __device__ __forceinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& st, bool valid,
                                                        const RenderLaunch& P, const PathSamplerDev& ps, BdVertex* vs,
                                                        uint32_t* err) {
-  V3 ro, rd, beta, pending_from;
-  float pending_pdf = 0.0f;
-  bool alive = valid && bdpt_light_endpoint(S, P, ps, vs, ro, rd, beta, pending_from, pending_pdf);
-  uint32_t n = alive ? 1u : 0u;
+  V3 ro, rd;
+  BdLightState l;
+  l.pending_pdf = 0.0f;
+  l.alive = valid && bdpt_light_endpoint(S, P, ps, vs, ro, rd, l.beta, l.pending_from, l.pending_pdf);
+  l.n = l.alive ? 1u : 0u;
   for (uint32_t depth = 1; depth < P.max_depth; ++depth) {
-    const unsigned live = __ballot_sync(0xffffffffu, alive);
+    const unsigned live = __ballot_sync(0xffffffffu, l.alive);
     if (!live) break;
     TraceResult h;
-    if (alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
-    if (!alive) continue;
-    if (h.tri < 0) {
-      alive = false;
-      continue;
-    }
-    const Vertex v = shade_hit<Stack>(S, h, rd);
-    const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
-    BdVertex& pv = vs[n];
-    pv.v = v;
-    pv.beta = beta;
-    pv.pdf_fwd = solid_angle_to_area(pending_pdf, pending_from, v.p, v.ng);
-    pv.pdf_rev = 0.0f;
-    pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
-    ++n;
-    if (m.kind == kDevEmissive) {
-      alive = false;
-      continue;
-    }
-    float ud0, ud1;
-    ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
-    const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
-    MatSample s;
-    if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, true, s)) {
-      alive = false;
-      continue;
-    }
-    pv.flags = s.delta ? kBdDelta : kBdConnectible;
-    vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
-    ro = offset_origin(v.p, v.ng, s.wi);
-    rd = s.wi;
-    beta = beta * s.weight;
-    pending_from = v.p;
-    pending_pdf = s.pdf;
+    if (l.alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    if (l.alive) light_step<Stack>(S, ps, depth, h, ro, rd, vs, l);
   }
-  return n;
+  return l.n;
 }
 
 // bdpt::trace_radiance for one sample (bdpt.rs:70-131), warp-synchronous.  The

@@ -1,5 +1,7 @@
 // Per-sample rendering on the device: camera ray, shading vertex, NEE through
-// the SG light tree, BSDF sampling and the MIS path loop.
+// the SG light tree and BSDF sampling, the pieces the MIS path loop of the
+// megakernel (render_kernels.cu) and of the wavefront stages
+// (wavefront_kernels.cu) are built from.
 //
 // Restates crates/renderer/src/{scene/camera.rs, scene/mod.rs:471-635,
 // light/{mod,area}.rs, material/{mod,normalized_lambert,emissive}.rs,
@@ -250,16 +252,6 @@ __device__ __forceinline__ V3 offset_origin(V3 p, V3 ng, V3 dir) {
   return p + 1.0e-4f * n;
 }
 
-// One out-of-line copy of the traversal for every caller of the megakernel:
-// inlining it at each call site multiplies the kernel's code size and makes the
-// kernel instruction-fetch bound.
-template <class Stack>
-__device__ __noinline__ bool closest_hit(const DevRender& S, Stack& st, V3 o, V3 d, TraceResult& r, uint32_t* err) {
-  TraceCounters c;
-  trace_ray<0, false>(S.geo, st, o.x, o.y, o.z, d.x, d.y, d.z, __int_as_float(0x7f800000), r, c, err);
-  return r.tri >= 0;
-}
-
 // direct_light_mis_contribution (integrator/mis.rs:145-210) for a diffuse
 // vertex, up to the visibility test: returns false when the contribution is
 // zero whatever the visibility; otherwise `contrib` (radiance * f * cos * mis /
@@ -337,56 +329,6 @@ __device__ __forceinline__ Vertex shade_hit(const DevRender& S, const TraceResul
   TriData T;
   fetch_triangle(S, (uint32_t)h.inst, (uint32_t)h.tri, T, true);
   return make_vertex(T, (uint32_t)h.inst, (uint32_t)h.tri, h.b0, h.b1, h.b2, incident);
-}
-
-// mis::trace_radiance (integrator/mis.rs:19-139)
-template <class Stack>
-__device__ V3 trace_mis(const DevRender& S, Stack& st, const RenderLaunch& P, const PathSamplerDev& ps, V3 ro, V3 rd,
-                        uint32_t* err) {
-  V3 L = V3{0, 0, 0};
-  V3 beta = V3{1, 1, 1};
-  TraceResult h;
-  if (!closest_hit(S, st, ro, rd, h, err)) return L;  // infinite_light_le: no environment light
-  Vertex v = shade_hit<Stack>(S, h, rd);
-  DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
-  if (m.kind == kDevEmissive) L = L + emissive_le(m);
-  for (uint32_t depth = 0; depth < P.max_depth; ++depth) {
-    if (m.kind == kDevEmissive) break;  // pure emitter: no NEE, and sample() is None
-    float us0, us1;
-    ps.sample_2d(vertex_dim(depth, kOffSurface), us0, us1);
-    const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
-    DirectPrep dp;
-    if (prepare_direct(S, m, v, u_tree, us0, us1, dp)) {
-      TraceResult sh;
-      if (!closest_hit(S, st, dp.so, dp.wi, sh, err) || ((uint32_t)sh.inst == dp.inst && (uint32_t)sh.tri == dp.tri))
-        L = L + beta * dp.contrib;
-    }
-    BsdfSampleOut s;
-    if (!material_sample(S, m, v, ps, depth, s)) break;
-    beta = beta * s.weight;
-    if (depth + 1 >= 4) {
-      const float q = clampf(max_element(beta), 0.05f, 1.0f);
-      if (ps.sample_1d(vertex_dim(depth, kOffRr)) > q) break;
-      beta = beta / q;
-    }
-    const V3 no = offset_origin(v.p, v.ng, s.wi);
-    TraceResult nh;
-    if (!closest_hit(S, st, no, s.wi, nh, err)) break;  // environment: none
-    const Vertex nv = shade_hit<Stack>(S, nh, s.wi);
-    const DevMaterialRec nm = S.d.mats[__ldg(&S.d.inst[nv.inst].material)];
-    if (nm.kind == kDevEmissive) {
-      const V3 le = emissive_le(nm);
-      if (s.delta) {
-        L = L + beta * le;
-      } else {
-        const float lp = light_pdf_for_hit(S, m, v, nv);
-        L = L + beta * le * balance_heuristic(s.pdf, lp);
-      }
-    }
-    v = nv;
-    m = nm;
-  }
-  return L;
 }
 
 }  // namespace tpt

@@ -169,9 +169,21 @@ struct DevAdjoint {
 // BDPT wavefront state (kernels/bdpt_wavefront.cu) for up to sample_capacity
 // samples of max_vertices vertices per subpath and pair_capacity connections.
 struct BdVertex;
+struct BdCamState;
+struct BdLightState;
 constexpr uint32_t kBdVertexBytes = 128;  // >= sizeof(BdVertex), for host-side sizing
+constexpr uint32_t kBdStateBytes = 64;    // >= sizeof(BdCamState), sizeof(BdLightState)
 struct BdWfBuffers {
   uint32_t sample_capacity, pair_capacity, max_vertices, pad;
+  // subpath stage: per-sample loop states and two ray queues of 2 x sample_capacity
+  BdCamState* cam_state;
+  BdLightState* light_state;
+  float* q_ray[2];       // 7 planes each
+  uint32_t* q_tag[2];    // sample index, bit 31: light subpath
+  int32_t* h_tri;
+  int32_t* h_inst;
+  float* h_t;
+  float* h_bary;         // 3 planes
   BdVertex* verts;       // [sample][camera 0..max_vertices, light 0..max_vertices]
   uint32_t* nc;          // camera subpath length per sample
   uint32_t* nl;          // light subpath length per sample
@@ -186,7 +198,7 @@ struct BdWfBuffers {
   int32_t* s_tri;
   int32_t* s_inst;
   float* s_t;
-  uint32_t* counts;      // [0] connections, [1] visibility rays
+  uint32_t* counts;      // [0] connections, [1] visibility rays, [2], [3] subpath ray queues
 };
 
 // Wavefront state: per path slot of a chunk (capacity slots), two ray queues,

@@ -1,10 +1,14 @@
 // BDPT as a wavefront (integrator/bdpt.rs:70-131 split into stages), per chunk
 // of samples:
 //
-//   bd_subpaths  : per sample, the camera and the light subpath (warp-
-//                  synchronous, as the one-kernel BDPT) into HBM; camera-side
-//                  emission into L0; the sample's nl * nc connection slots
-//                  allocated contiguously in a pair queue (one atomic per warp)
+//   bd_init      : per sample, the camera ray and the light endpoint
+//   bd_step x max_depth, each after a traversal of the subpath ray queue:
+//                  one iteration of the camera loop (depth = step) or of the
+//                  light loop (depth = step + 1) per queued ray, vertices into
+//                  HBM, camera-side emission into L0, next rays into the other
+//                  queue (the same step functions the one-kernel BDPT runs)
+//   bd_pairs     : per sample, its nl * nc connection slots allocated
+//                  contiguously in the pair queue (one atomic per warp)
 //   bd_connect   : per pair, bdpt_connect_prepare; non-zero contributions
 //                  append their visibility ray to the shadow queue
 //   traverse     : the persistent traversal kernel over the shadow queue
@@ -39,50 +43,6 @@ __device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t v, uint32_t& to
   return x - v;
 }
 
-__global__ void __launch_bounds__(kBdWfBlock) bd_subpaths(DevRender S, RenderLaunch P, BdWfBuffers B,
-                                                          uint64_t first_path, uint32_t n, uint32_t* err) {
-  __shared__ uint32_t stack_sh[kBdShStack * kBdWfBlock];
-  SplitStack<kBdShStack> st;
-  st.sh = stack_sh + threadIdx.x;
-  const uint32_t MD = B.max_vertices;
-  const unsigned lane = threadIdx.x & 31u;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x - lane); base < n; base += stride) {
-    const uint32_t i = base + lane;
-    const bool valid = i < n;
-    const uint64_t path = first_path + (valid ? i : 0);
-    const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
-    const uint32_t px = pixel % P.width, py = pixel / P.width;
-    PathSamplerDev ps;
-    ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
-    float c0, c1;
-    ps.sample_2d(kDimCamera, c0, c1);
-    const float fx = ((float)px + 0.5f) + 0.5f * tent(c0);
-    const float fy = ((float)py + 0.5f) + 0.5f * tent(c1);
-    const V3 d = camera_dir(P.cam, P.width, P.height, fx, fy);
-    const V3 o = V3{P.cam.eye[0], P.cam.eye[1], P.cam.eye[2]};
-    BdVertex* cam = B.verts + (size_t)(valid ? i : 0) * 2 * MD;
-    V3 L = V3{0.0f, 0.0f, 0.0f};
-    const uint32_t nc = bdpt_camera_subpath(S, st, valid, P, ps, o, d, cam, L, err);
-    const uint32_t nl = bdpt_light_subpath(S, st, valid, P, ps, cam + MD, err);
-    const uint32_t np = valid ? nl * nc : 0u;
-    uint32_t total;
-    const uint32_t off = warp_exclusive_scan(np, total);
-    uint32_t pbase = 0;
-    if (lane == 31 && total) pbase = atomicAdd(B.counts, total);
-    pbase = __shfl_sync(0xffffffffu, pbase, 31) + off;
-    if (valid) {
-      B.nc[i] = nc;
-      B.nl[i] = nl;
-      B.pair_base[i] = pbase;
-      B.L0[3 * (size_t)i] = L.x;
-      B.L0[3 * (size_t)i + 1] = L.y;
-      B.L0[3 * (size_t)i + 2] = L.z;
-      for (uint32_t k = 0; k < np; ++k) B.pair_sample[pbase + k] = i;
-    }
-  }
-}
-
 __device__ __forceinline__ uint32_t warp_append1(uint32_t* counter, bool pred) {
   const unsigned act = __activemask();
   const unsigned m = __ballot_sync(act, pred);
@@ -92,6 +52,130 @@ __device__ __forceinline__ uint32_t warp_append1(uint32_t* counter, bool pred) {
   if ((int)lane == leader && m) base = atomicAdd(counter, (uint32_t)__popc(m));
   base = __shfl_sync(act, base, leader);
   return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void push_ray(const BdWfBuffers& B, int q, uint32_t slot, V3 o, V3 d, uint32_t tag) {
+  const uint32_t Q = 2 * B.sample_capacity;
+  float* r = B.q_ray[q];
+  r[slot] = o.x;
+  r[Q + slot] = o.y;
+  r[2 * Q + slot] = o.z;
+  r[3 * Q + slot] = d.x;
+  r[4 * Q + slot] = d.y;
+  r[5 * Q + slot] = d.z;
+  r[6 * Q + slot] = __int_as_float(0x7f800000);
+  B.q_tag[q][slot] = tag;
+}
+
+__device__ __forceinline__ PathSamplerDev sampler_of(const RenderLaunch& P, uint64_t path, uint32_t& px,
+                                                     uint32_t& py) {
+  const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
+  px = pixel % P.width;
+  py = pixel / P.width;
+  PathSamplerDev ps;
+  ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+  return ps;
+}
+
+constexpr uint32_t kLightTag = 0x80000000u;
+
+// Per sample: the camera ray and the light endpoint (bdpt.rs:96-110, 264-300);
+// both first rays into queue 0.
+__global__ void __launch_bounds__(kBdWfBlock) bd_init(DevRender S, RenderLaunch P, BdWfBuffers B,
+                                                      uint64_t first_path, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t px, py;
+  const PathSamplerDev ps = sampler_of(P, first_path + i, px, py);
+  float c0, c1;
+  ps.sample_2d(kDimCamera, c0, c1);
+  const float fx = ((float)px + 0.5f) + 0.5f * tent(c0);
+  const float fy = ((float)py + 0.5f) + 0.5f * tent(c1);
+  const V3 d = camera_dir(P.cam, P.width, P.height, fx, fy);
+  const V3 o = V3{P.cam.eye[0], P.cam.eye[1], P.cam.eye[2]};
+  BdCamState c;
+  camera_state_init(c, P.max_depth > 0);
+  BdVertex* lig = B.verts + (size_t)i * 2 * B.max_vertices + B.max_vertices;
+  V3 lo, ld;
+  BdLightState l;
+  l.pending_pdf = 0.0f;
+  l.alive = bdpt_light_endpoint(S, P, ps, lig, lo, ld, l.beta, l.pending_from, l.pending_pdf);
+  l.n = l.alive ? 1u : 0u;
+  B.cam_state[i] = c;
+  B.light_state[i] = l;
+  B.L0[3 * (size_t)i] = 0.0f;
+  B.L0[3 * (size_t)i + 1] = 0.0f;
+  B.L0[3 * (size_t)i + 2] = 0.0f;
+  const bool cam_ray = c.alive;
+  const bool light_ray = l.alive && P.max_depth > 1;
+  const uint32_t qc = warp_append1(&B.counts[2], cam_ray);
+  if (cam_ray) push_ray(B, 0, qc, o, d, i);
+  const uint32_t ql = warp_append1(&B.counts[2], light_ray);
+  if (light_ray) push_ray(B, 0, ql, lo, ld, i | kLightTag);
+}
+
+// Step `step` of both loops: camera rays of depth `step`, light rays of depth
+// step + 1, traced into the hit arrays; the next rays into queue cur ^ 1.
+__global__ void __launch_bounds__(kBdWfBlock) bd_step(DevRender S, RenderLaunch P, BdWfBuffers B,
+                                                      uint64_t first_path, uint32_t step, int cur) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= B.counts[2 + cur]) return;
+  const uint32_t Q = 2 * B.sample_capacity;
+  const uint32_t tag = B.q_tag[cur][j];
+  const uint32_t i = tag & ~kLightTag;
+  const bool light = (tag & kLightTag) != 0;
+  uint32_t px, py;
+  const PathSamplerDev ps = sampler_of(P, first_path + i, px, py);
+  TraceResult h;
+  h.tri = B.h_tri[j];
+  h.inst = B.h_inst[j];
+  h.t = B.h_t[j];
+  h.b0 = B.h_bary[j];
+  h.b1 = B.h_bary[Q + j];
+  h.b2 = B.h_bary[2 * Q + j];
+  const float* r = B.q_ray[cur];
+  V3 ro = V3{r[j], r[Q + j], r[2 * Q + j]};
+  V3 rd = V3{r[3 * Q + j], r[4 * Q + j], r[5 * Q + j]};
+  BdVertex* cam = B.verts + (size_t)i * 2 * B.max_vertices;
+  bool next = false;
+  if (!light) {
+    BdCamState c = B.cam_state[i];
+    V3 L = V3{B.L0[3 * (size_t)i], B.L0[3 * (size_t)i + 1], B.L0[3 * (size_t)i + 2]};
+    camera_step<int>(S, P, ps, step, h, ro, rd, cam, c, L);
+    B.cam_state[i] = c;
+    B.L0[3 * (size_t)i] = L.x;
+    B.L0[3 * (size_t)i + 1] = L.y;
+    B.L0[3 * (size_t)i + 2] = L.z;
+    next = c.alive && step + 1 < P.max_depth;
+  } else {
+    BdLightState l = B.light_state[i];
+    light_step<int>(S, ps, step + 1, h, ro, rd, cam + B.max_vertices, l);
+    B.light_state[i] = l;
+    next = l.alive && step + 2 < P.max_depth;
+  }
+  const uint32_t q = warp_append1(&B.counts[2 + (cur ^ 1)], next);
+  if (next) push_ray(B, cur ^ 1, q, ro, rd, tag);
+}
+
+// Per sample: subpath lengths and the nl * nc connection slots, contiguous
+// per sample (one atomic per warp).
+__global__ void __launch_bounds__(kBdWfBlock) bd_pairs(BdWfBuffers B, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < n;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t nc = valid ? B.cam_state[i].n : 0u;
+  const uint32_t nl = valid ? B.light_state[i].n : 0u;
+  const uint32_t np = nl * nc;
+  uint32_t total;
+  const uint32_t off = warp_exclusive_scan(np, total);
+  uint32_t pbase = 0;
+  if (lane == 31 && total) pbase = atomicAdd(B.counts, total);
+  pbase = __shfl_sync(0xffffffffu, pbase, 31) + off;
+  if (!valid) return;
+  B.nc[i] = nc;
+  B.nl[i] = nl;
+  B.pair_base[i] = pbase;
+  for (uint32_t k = 0; k < np; ++k) B.pair_sample[pbase + k] = i;
 }
 
 __global__ void __launch_bounds__(kBdWfBlock) bd_connect(DevRender S, BdWfBuffers B) {
@@ -178,13 +262,20 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
   DevRender S{geo, rd};
   cudaError_t e = cudaMemsetAsync(B.counts, 0, 2 * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  static int bpsm = 0;
-  if (bpsm == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, bd_subpaths, kBdWfBlock, 0) != cudaSuccess || bpsm <= 0)
-      bpsm = 2;
+  const uint32_t Q = 2 * B.sample_capacity;
+  if ((e = cudaMemsetAsync(B.counts + 2, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  bd_init<<<grid_of(n), kBdWfBlock, 0, s>>>(S, P, B, first_path, n);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  for (uint32_t step = 0; step < P.max_depth; ++step) {
+    const int cur = (int)(step & 1u);
+    if ((e = cudaMemsetAsync(B.counts + 2 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+    e = launch_traverse_strided(geo, B.q_ray[cur], Q, Q, TPT_CLOSEST_HIT, B.h_tri, B.h_t, B.h_inst, B.h_bary, Q,
+                                counter, err, num_sms, s, nullptr, nullptr, B.counts + 2 + cur);
+    if (e != cudaSuccess) return e;
+    bd_step<<<grid_of(Q), kBdWfBlock, 0, s>>>(S, P, B, first_path, step, cur);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  const uint64_t blocks = std::min<uint64_t>(grid_of(n), (uint64_t)num_sms * bpsm * 8);
-  bd_subpaths<<<(unsigned)blocks, kBdWfBlock, 0, s>>>(S, P, B, first_path, n, err);
+  bd_pairs<<<grid_of(n), kBdWfBlock, 0, s>>>(B, n);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   bd_connect<<<grid_of(B.pair_capacity), kBdWfBlock, 0, s>>>(S, B);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
