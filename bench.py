@@ -365,6 +365,19 @@ def large_block(ctx, args, cpu=True):
         out["cpu_baseline"] = {"value": len(rows) * W / dt / 1e6, "cores": threads, "kind": "port",
                                "sample": f"MIS: {len(rows)} evenly spaced rows of {W} pixels x 1 spp, {dt:.1f} s"}
         out["wavefront_over_cpu"] = out["mis_wavefront"]["value"] / out["cpu_baseline"]["value"]
+        n_rows = 2
+        while True:  # BDPT, path length 10
+            rows = [int(r) for r in np.linspace(0, H - 1, n_rows)]
+            t0 = time.perf_counter()
+            for r in rows:
+                ref.render(sc["camera"], W, H, 1, 10, pixels=(r * W, (r + 1) * W), nthreads=threads, integrator=1)
+            dt = time.perf_counter() - t0
+            if dt > 3.0 or n_rows >= H:
+                break
+            n_rows = min(H, n_rows * max(2, int(5.0 / max(dt, 1e-3))))
+        out["cpu_baseline_bdpt"] = {"value": len(rows) * W / dt / 1e6, "cores": threads, "kind": "port",
+                                    "sample": f"BDPT: {len(rows)} evenly spaced rows of {W} pixels x 1 spp, {dt:.1f} s"}
+        out["bdpt_wavefront_over_cpu"] = out["bdpt_wavefront"]["value"] / out["cpu_baseline_bdpt"]["value"]
     scene.close()
     return out
 

@@ -33,6 +33,9 @@
 namespace tpt {
 
 constexpr int kWfBlock = 256;
+#ifndef TPT_SHADE_MINB
+#define TPT_SHADE_MINB 1  // blocks per SM the shade kernel's register budget is sized for
+#endif
 
 __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   const unsigned act = __activemask();
@@ -108,7 +111,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaun
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
 template <bool ADJ, bool BATCH>
-__global__ void __launch_bounds__(kWfBlock) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, int cur,
+__global__ void __launch_bounds__(kWfBlock, TPT_SHADE_MINB) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, int cur,
                                                      DevAdjoint A, const DevJob* __restrict__ jobs) {
   __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
