@@ -15,7 +15,7 @@
 * Material updates: a render after tpt_scene_set_openpbr equals a render of a
   freshly uploaded scene with the new parameters, bit for bit.
 * Inverse rendering: Adam on the 64 patch materials from a perturbed start
-  lowers the L2 image loss against a higher-spp target.
+  lowers the L2 image loss (measured at 256 spp) against a 1024-spp target.
 """
 import numpy as np
 import pytest
@@ -165,34 +165,48 @@ def test_adjoint_rejects_bdpt_and_bad_masks(patches):
 
 
 def test_inverse_rendering_lowers_loss(ctx):
+    """200 Adam steps (lr 0.003) on the 64 patch materials from a perturbed
+    start, 128x128 at 16 spp forward and adjoint: the image loss measured at
+    256 spp against the 1024-spp target must fall below 0.6 of its start
+    (measured on a B200: 38.7 -> 12.9).  Parameter error is printed, not
+    checked: base colour, metalness and roughness trade off against each other
+    in the image and several patches are barely visible."""
     import torch
 
     sc = tpt_scenes.cornell_patches()
-    W, spp, depth = 64, 16, 6
+    W, spp, depth = 128, 16, 6
+    st = _stream()
     target_scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"])
-    target = torch.from_numpy(render(target_scene, sc, W, 256, depth)).float().cuda().view(W, W, 3)
+    target = torch.from_numpy(render(target_scene, sc, W, 1024, depth)).float().cuda().view(W, W, 3)
     target_scene.close()
     start = tpt_scenes.patch_params(5, start=True)
     sc0 = tpt_scenes.with_patch_params(sc, start)
     scene = tpt.Scene(ctx, sc0["meshes"], sc0["instances"], materials=sc0["materials"])
+
+    def clean_loss(p):
+        set_params(scene, p)
+        img = torch.from_numpy(render(scene, sc, W, 256, depth)).float().cuda().view(W, W, 3)
+        return float(((img - target) ** 2).sum())
+
+    loss0 = clean_loss(start)
     RenderFunction = tpt.render_function()
     job = scene.job(sc["camera"], W, W, spp, depth)
     params = torch.tensor(start, requires_grad=True)
-    opt = torch.optim.Adam([params], lr=0.02)
+    opt = torch.optim.Adam([params], lr=0.003)
     lo = torch.tensor([0.02, 0.02, 0.02, 0.05, 0.0])
     hi = torch.tensor([0.98, 0.98, 0.98, 1.0, 1.0])
-    losses = []
-    for _ in range(40):
+    mask = tpt.GRAD_MASK_BASE_COLOR | tpt.GRAD_MASK_ROUGHNESS | tpt.GRAD_MASK_METALNESS
+    for _ in range(200):
         opt.zero_grad()
-        img = RenderFunction.apply(params, scene, job, list(range(64)), tpt_scenes.patch_material)
+        img = RenderFunction.apply(params, scene, job, list(range(64)), tpt_scenes.patch_material, mask)
         loss = ((img - target) ** 2).sum()
         loss.backward()
         opt.step()
         with torch.no_grad():
             params.copy_(torch.maximum(torch.minimum(params, hi), lo))
-        losses.append(float(loss.detach()))
-    err0 = np.abs(start - sc["params"]).mean()
-    err1 = np.abs(params.detach().numpy() - sc["params"]).mean()
-    print("loss", losses[0], "->", losses[-1], "parameter error", err0, "->", err1)
-    assert np.mean(losses[-5:]) < 0.5 * np.mean(losses[:5])
+    p = params.detach().numpy()
+    loss1 = clean_loss(p)
+    print("256-spp image loss", loss0, "->", loss1, "parameter error", np.abs(start - sc["params"]).mean(), "->",
+          np.abs(p - sc["params"]).mean())
+    assert loss1 < 0.6 * loss0
     scene.close()
