@@ -417,8 +417,9 @@ def batch_block(ctx, args):
     out["autotune"] = dict(tune, seconds=time.perf_counter() - t0)
     ms = _time_ms(lambda: ctx.render_batch_device(jw, ptrs, st))
     out["batched_wavefront"] = {"value": total / ms / 1e3, "ms": ms}
-    ctx.wavefront_capacity = 0
+    ctx.wavefront_capacity = 0  # the job-by-job comparisons run the default settings
     ctx.set_graphs(True)
+    ctx.set_shade_block(256)
     ms = _time_ms(lambda: [sc.render_device(j, p, st) for sc, j, p in zip(scenes, jw, ptrs)])
     out["per_job_wavefront"] = {"value": total / ms / 1e3, "ms": ms}
     ms = _time_ms(lambda: [sc.render_device(j, p, st) for sc, j, p in zip(scenes, jm, ptrs)])
@@ -634,7 +635,9 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sphere soup + ray batches)",
         "config": config_dict(args, world),
-        "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": len(queries) * n * 7 * 4,
+        "e2e": {"value": e2e_value, "unit": "rays/s",
+                # closest-hit queries copy 6 ray planes (their tmax plane is not read), any-hit 7
+                "h2d_bytes_per_step": sum(n * (6 if m == tpt.CLOSEST_HIT else 7) * 4 for _, m in queries),
                 "d2h_bytes_per_step": len(queries) * n * 8},
         "gpu_launches": len(queries) * args.steps,
         "roofline": {

@@ -246,7 +246,8 @@ typedef enum tpt_query_mode {
  * bary (3 planes of barycentrics) may be NULL.
  * Host-pointer variant: the batch is split into chunks pipelined over two
  * streams (copy in, query, copy out overlap); page-locked caller buffers are
- * copied directly, pageable ones through pinned staging. */
+ * copied directly, pageable ones through pinned staging.  For TPT_CLOSEST_HIT
+ * the tmax plane is not copied. */
 tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n, int mode,
                         int32_t* prim, float* t, int32_t* instance, float* bary);
 tpt_status tpt_traverse_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n, int mode,
@@ -308,10 +309,14 @@ uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx);
  * always launched directly (they join the caller's graph).  Results do not
  * depend on it. */
 tpt_status tpt_context_set_graphs(tpt_context* ctx, int enable);
+/* Threads per block of the wavefront shade stage: 128 or 256 (default). */
+tpt_status tpt_context_set_shade_block(tpt_context* ctx, uint32_t threads);
 
 /* Renders each job into out_rgb[j] (host, width*height*3 floats, row-major,
  * pixel = y*width + x): per pixel the running mean of `spp` samples in sample
- * order, times exposure — the raw linear buffer main.rs writes before output. */
+ * order, times exposure — the raw linear buffer main.rs writes before output.
+ * Several MIS wavefront jobs go through one batched launch sequence
+ * (tpt_render_batch_device); the images are the same either way. */
 tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb);
 /* One job into a device buffer, asynchronous on `stream`. */
 tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream);
@@ -322,21 +327,25 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
                                      float* out_samples, void* stream);
 
 /* Autotuner (no counterpart in the reference): times the candidate settings
- * on a pilot of `jobs` (each job's rows scaled down until the pilot holds at
- * most 2^24 paths) and applies the fastest to the context: the execution used
+ * on pilots of `jobs` (each job's rows scaled down: every candidate on at most
+ * 2^24 paths, the candidates within 5 % of the best again on at most 2^26) and
+ * applies the fastest to the context: the execution used
  * by jobs whose `execution` is TPT_EXEC_AUTO, and, when that is the wavefront,
  * its queue capacity (tpt_context_set_wavefront_capacity) and graph replay
  * (tpt_context_set_graphs).  Candidates: the megakernel, and the wavefront
  * (batched when n_jobs > 1) at capacities 2^18 .. 2^23, with and without graph
- * replay.  MIS jobs only.  Results do not depend on the settings. */
+ * replay, at the context's shade block size (tpt_context_set_shade_block: a
+ * scaled-down pilot does not predict it).  MIS jobs only.  Results do not
+ * depend on the settings. */
 typedef struct tpt_tune_result {
   uint32_t execution;          /* TPT_EXEC_WAVEFRONT or TPT_EXEC_MEGAKERNEL */
   uint32_t wavefront_capacity; /* path slots per chunk */
   uint32_t graphs;             /* 1: bounces replayed from captured graphs */
+  uint32_t shade_block;        /* threads per block of the wavefront shade stage (the context's) */
   float ms;                    /* pilot time of the chosen settings */
-  float ms_megakernel;         /* pilot time of the megakernel */
+  float ms_megakernel;         /* first-pilot time of the megakernel */
   float ms_wavefront_default;  /* pilot time of the wavefront at 2^22 slots with graphs */
-  uint64_t pilot_paths;
+  uint64_t pilot_paths;        /* paths of the last pilot (about) */
 } tpt_tune_result;
 tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, tpt_tune_result* out);
 

@@ -51,15 +51,18 @@ def _render_batch(ctx, jobs):
     return [o.cpu().numpy() for o in outs]
 
 
-@pytest.mark.parametrize("capacity", [0, 4096], ids=["default", "small_chunks"])
-def test_batch_equals_single_jobs(ctx, mixed, capacity):
+@pytest.mark.parametrize("capacity,block", [(0, 256), (4096, 256), (0, 128)],
+                         ids=["default", "small_chunks", "shade_block_128"])
+def test_batch_equals_single_jobs(ctx, mixed, capacity, block):
     ctx.wavefront_capacity = 0
     ref = _render_each(ctx, mixed)
     ctx.wavefront_capacity = capacity
+    ctx.set_shade_block(block)
     try:
         got = _render_batch(ctx, mixed)
     finally:
         ctx.wavefront_capacity = 0
+        ctx.set_shade_block(256)
     for a, b in zip(got, ref):
         assert np.all(np.isfinite(a)) and b.max() > 0
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
@@ -118,6 +121,7 @@ def test_autotune_applies_a_setting_that_renders_the_same(ctx, mixed):
     finally:
         ctx.wavefront_capacity = 0
         ctx.set_graphs(True)
+        ctx.set_shade_block(256)
 
 
 def test_host_render_of_several_jobs_is_batched_and_equal(ctx, mixed):

@@ -3,13 +3,19 @@
 // wavefront's queue capacity and whether bounces replay captured graphs, by
 // timing each candidate on a pilot of the workload on the device.
 //
-// No counterpart in the reference (one CPU code path).  The pilot keeps every
+// No counterpart in the reference (one CPU code path).  A pilot keeps every
 // job's scene, camera, spp and depth and scales its rows down (the same field
-// of view at a lower vertical resolution) until the pilot holds at most
-// 2^24 paths, or the whole workload when it is smaller.  Each candidate runs
-// once to warm up (graph capture, arena growth) and once timed with CUDA
-// events on the context's stream.  Results do not depend on any of the tuned
-// settings (the tests check this), only the time does.
+// of view at a lower vertical resolution).  Stage 1 times every candidate on a
+// pilot of at most 2^24 paths (the whole workload when it is smaller); stage 2
+// re-times the candidates within 5 % of the best, and the default, on a pilot
+// four times larger, whose chunks look more like the full workload's.  Each
+// timing is one warm-up (graph capture, arena growth) and the median of three
+// runs, CUDA events on the context's stream.  A candidate replaces the default
+// wavefront settings (2^22 slots, graphs) only when it is more than 3 %
+// faster.  The shade stage's block size is the context's (256 by default):
+// pilots preferred 128-thread blocks by 1-4 % where the full 64-job workload ran
+// 13 % slower with them, so it is not a pilot decision.  Results do not depend
+// on any of the tuned settings (the tests check this), only the time does.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -52,83 +58,130 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
       return set_error(ctx, TPT_ERR_INVALID_ARG, "the autotuner covers MIS jobs");
     total += (uint64_t)L.width * L.height * L.spp;
   }
-  // pilot: rows scaled by f
-  const double f = total > kPilotPaths ? (double)kPilotPaths / (double)total : 1.0;
-  std::vector<tpt_render_job> pilot(jobs, jobs + n_jobs);
-  std::vector<float*> imgs(n_jobs, nullptr);
-  uint64_t pilot_paths = 0;
-  tpt_status st = TPT_OK;
-  for (int j = 0; j < n_jobs && !st; ++j) {
-    pilot[j].height = std::max<uint32_t>(1, (uint32_t)std::ceil(jobs[j].height * f));
-    pilot_paths += (uint64_t)pilot[j].width * pilot[j].height * pilot[j].spp;
-    st = cuda_check(ctx, cudaMalloc((void**)&imgs[j], (size_t)pilot[j].width * pilot[j].height * 12),
-                    "cudaMalloc(pilot image)");
-  }
+  struct Pilot {
+    std::vector<tpt_render_job> jobs;
+    std::vector<float*> imgs;
+    uint64_t paths = 0;
+  };
+  // pilot of at most `limit` paths: every job's rows scaled by the same factor
+  auto make_pilot = [&](uint64_t limit, Pilot& p) -> tpt_status {
+    const double f = total > limit ? (double)limit / (double)total : 1.0;
+    p.jobs.assign(jobs, jobs + n_jobs);
+    p.imgs.assign(n_jobs, nullptr);
+    for (int j = 0; j < n_jobs; ++j) {
+      p.jobs[j].height = std::max<uint32_t>(1, (uint32_t)std::ceil(jobs[j].height * f));
+      p.paths += (uint64_t)p.jobs[j].width * p.jobs[j].height * p.jobs[j].spp;
+      tpt_status s2 = cuda_check(ctx, cudaMalloc((void**)&p.imgs[j], (size_t)p.jobs[j].width * p.jobs[j].height * 12),
+                                 "cudaMalloc(pilot image)");
+      if (s2) return s2;
+    }
+    return TPT_OK;
+  };
+  auto free_pilot = [](Pilot& p) {
+    for (float* x : p.imgs)
+      if (x) cudaFree(x);
+    p.imgs.clear();
+  };
+  struct Cand {
+    uint32_t exec, cap, graphs, block;
+    float ms;
+  };
   const uint32_t saved_cap = ctx->batch_capacity;
   const bool saved_graphs = ctx->use_graphs;
+  const uint32_t saved_block = ctx->shade_block;
   Timer T;
-  auto run = [&](uint32_t exec, uint32_t cap, bool graphs, float* ms) -> tpt_status {
-    ctx->batch_capacity = cap;
-    ctx->use_graphs = graphs;
-    for (int rep = 0; rep < 2; ++rep) {
-      if (rep == 1) cudaEventRecord(T.a, ctx->stream);
+  // one warm-up, then the median of three timed runs
+  auto run = [&](Pilot& p, const Cand& c, float* ms) -> tpt_status {
+    ctx->batch_capacity = c.cap;
+    ctx->use_graphs = c.graphs != 0;
+    ctx->shade_block = c.block;
+    float t[3] = {0.0f, 0.0f, 0.0f};
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(T.a, ctx->stream);
       tpt_status s2 = TPT_OK;
-      if (exec == TPT_EXEC_WAVEFRONT && n_jobs > 1) {
-        s2 = render_batch(ctx, pilot.data(), n_jobs, imgs.data(), ctx->stream, cap);
+      if (c.exec == TPT_EXEC_WAVEFRONT && n_jobs > 1) {
+        s2 = render_batch(ctx, p.jobs.data(), n_jobs, p.imgs.data(), ctx->stream, c.cap);
       } else {
         for (int j = 0; j < n_jobs && !s2; ++j) {
-          tpt_render_job pj = pilot[j];
-          pj.execution = exec;
-          s2 = tpt_render_device(ctx, &pj, imgs[j], nullptr);
+          tpt_render_job pj = p.jobs[j];
+          pj.execution = c.exec;
+          s2 = tpt_render_device(ctx, &pj, p.imgs[j], nullptr);
         }
       }
       if (s2) return s2;
+      cudaEventRecord(T.b, ctx->stream);
+      cudaError_t e = cudaEventSynchronize(T.b);
+      if (e == cudaSuccess && rep > 0) e = cudaEventElapsedTime(&t[rep - 1], T.a, T.b);
+      if (e != cudaSuccess) return cuda_check(ctx, e, "autotune timing");
     }
-    cudaEventRecord(T.b, ctx->stream);
-    cudaError_t e = cudaEventSynchronize(T.b);
-    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, T.a, T.b);
-    return cuda_check(ctx, e, "autotune timing");
+    std::sort(t, t + 3);
+    *ms = t[1];
+    return TPT_OK;
   };
-  tpt_tune_result best{};
-  best.ms = 1e30f;
-  float ms_default = 0.0f, ms_mk = 0.0f;
-  if (!st) st = run(TPT_EXEC_MEGAKERNEL, 0, false, &ms_mk);
+  // stage 1: every candidate on a pilot of at most 2^24 paths
+  Pilot p1;
+  tpt_status st = make_pilot(kPilotPaths, p1);
+  std::vector<Cand> cands;
+  cands.push_back(Cand{TPT_EXEC_MEGAKERNEL, 0, 0, 256, 0.0f});
   const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23};
   for (uint32_t cap : caps) {
-    if (st) break;
-    if (cap > 2 * std::max<uint64_t>(pilot_paths, 1u << 18)) break;  // larger queues than the pilot gain nothing
-    for (int g = 1; g >= 0 && !st; --g) {
-      float ms = 0.0f;
-      st = run(TPT_EXEC_WAVEFRONT, cap, g != 0, &ms);
-      if (st) break;
-      if (cap == (1u << 22) && g == 1) ms_default = ms;
-      if (ms < best.ms) {
-        best.ms = ms;
-        best.execution = TPT_EXEC_WAVEFRONT;
-        best.wavefront_capacity = cap;
-        best.graphs = (uint32_t)g;
-      }
-    }
+    if (cap > 2 * std::max<uint64_t>(p1.paths, 1u << 18) && cap != (1u << 22)) continue;  // queues beyond the work
+    for (uint32_t g : {1u, 0u}) cands.push_back(Cand{TPT_EXEC_WAVEFRONT, cap, g, saved_block, 0.0f});
   }
-  for (float* p : imgs)
-    if (p) cudaFree(p);
+  for (Cand& c : cands) {
+    if (st) break;
+    st = run(p1, c, &c.ms);
+  }
+  free_pilot(p1);
+  const float ms_mk = cands[0].ms;  // stage-1 time of the megakernel
+  // stage 2: the candidates within 5 % of the best (and the default) on a
+  // pilot four times larger, closer to the full workload's chunk composition
+  if (!st && total > kPilotPaths) {
+    float best1 = 1e30f;
+    for (const Cand& c : cands) best1 = std::min(best1, c.ms);
+    Pilot p2;
+    st = make_pilot(4 * kPilotPaths, p2);
+    for (Cand& c : cands) {
+      if (st) break;
+      const bool is_default = c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs;
+      if (c.ms <= 1.05f * best1 || is_default) st = run(p2, c, &c.ms);
+      else c.ms = 1e30f;
+    }
+    free_pilot(p2);
+  }
   ctx->batch_capacity = saved_cap;
   ctx->use_graphs = saved_graphs;
+  ctx->shade_block = saved_block;
   if (st) return st;
-  if (ms_mk < best.ms) {
-    best.ms = ms_mk;
-    best.execution = TPT_EXEC_MEGAKERNEL;
-    best.wavefront_capacity = saved_cap;
-    best.graphs = saved_graphs ? 1u : 0u;
+  tpt_tune_result best{};
+  best.ms = 1e30f;
+  float ms_default = 0.0f;
+  for (const Cand& c : cands) {
+    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs) ms_default = c.ms;
+    if (c.ms < best.ms) {
+      best.ms = c.ms;
+      best.execution = c.exec;
+      best.wavefront_capacity = c.exec == TPT_EXEC_WAVEFRONT ? c.cap : saved_cap;
+      best.graphs = c.exec == TPT_EXEC_WAVEFRONT ? c.graphs : (saved_graphs ? 1u : 0u);
+      best.shade_block = c.exec == TPT_EXEC_WAVEFRONT ? c.block : saved_block;
+    }
   }
+  // keep the default wavefront settings unless a wavefront candidate beats
+  // them by 3 %: the pilots are scaled-down workloads and carry noise
+  if (best.execution == TPT_EXEC_WAVEFRONT && ms_default > 0.0f && best.ms > 0.97f * ms_default) {
+    best.ms = ms_default;
+    best.wavefront_capacity = 1u << 22;
+    best.graphs = 1;
+  }
+  best.pilot_paths = std::min<uint64_t>(total, total > kPilotPaths ? 4 * kPilotPaths : total);
   best.ms_megakernel = ms_mk;
   best.ms_wavefront_default = ms_default;
-  best.pilot_paths = pilot_paths;
   // apply
   ctx->tuned_execution = best.execution;
   if (best.execution == TPT_EXEC_WAVEFRONT) {
     ctx->batch_capacity = best.wavefront_capacity;
     ctx->use_graphs = best.graphs != 0;
+    ctx->shade_block = best.shade_block;
   }
   *out = best;
   return TPT_OK;

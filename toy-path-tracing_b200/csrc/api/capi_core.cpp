@@ -533,6 +533,8 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
   int32_t* d_inst = instance ? (int32_t*)(d_t + n) : nullptr;
   float* d_bary = bary ? (instance ? (float*)(d_inst + n) : (d_t + n)) : nullptr;
 
+  // closest-hit queries start at t_max = +inf and never read the tmax plane: it is not copied
+  const int in_planes = mode == TPT_CLOSEST_HIT ? 6 : 7;
   const bool in_pinned = is_pinned(rays);
   const bool out_pinned = is_pinned(prim) && is_pinned(t) && (!instance || is_pinned(instance)) &&
                           (!bary || is_pinned(bary));
@@ -555,11 +557,11 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
       cudaEventSynchronize(ctx->ev_slot[k]);
     }
     if (in_pinned) {
-      for (int p = 0; p < 7; ++p)
+      for (int p = 0; p < in_planes; ++p)
         cudaMemcpyAsync(d_rays + p * n + b, rays + p * n + b, m * 4, cudaMemcpyHostToDevice, s);
     } else {
-      for (int p = 0; p < 7; ++p) std::memcpy(hslot + p * m, rays + p * n + b, m * 4);
-      for (int p = 0; p < 7; ++p)
+      for (int p = 0; p < in_planes; ++p) std::memcpy(hslot + p * m, rays + p * n + b, m * 4);
+      for (int p = 0; p < in_planes; ++p)
         cudaMemcpyAsync(d_rays + p * n + b, hslot + p * m, m * 4, cudaMemcpyHostToDevice, s);
     }
     // the kernel reads plane p of the chunk at d_rays + p*n + b: pass a view with stride n

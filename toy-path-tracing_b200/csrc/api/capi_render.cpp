@@ -270,6 +270,13 @@ tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots) 
   return TPT_OK;
 }
 
+tpt_status tpt_context_set_shade_block(tpt_context* ctx, uint32_t threads) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  if (threads != 128 && threads != 256) return set_error(ctx, TPT_ERR_INVALID_ARG, "shade block must be 128 or 256");
+  ctx->shade_block = threads;
+  return TPT_OK;
+}
+
 tpt_status tpt_context_set_graphs(tpt_context* ctx, int enable) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   ctx->use_graphs = enable != 0;

@@ -53,6 +53,7 @@ struct tpt_context {
   // per-bounce CUDA graphs of the wavefront (bounce_graphs.cpp)
   bool use_graphs = true;
   uint32_t tuned_execution = 0;  // what TPT_EXEC_AUTO means (tpt_autotune)
+  uint32_t shade_block = 256;    // threads per block of the wavefront shade stage (128 or 256)
   std::vector<tpt::BounceGraphSet*> graphs;
   uint64_t graph_clock = 0;
   cudaStream_t cap_stream = nullptr;
@@ -150,13 +151,15 @@ cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, 
                                const WfBuffers& B, uint64_t first_path, uint32_t n_paths, cudaStream_t s,
                                const float* primal = nullptr);
 // shade reads the chunk's first path from the queue counters (written by generate)
+// `block`: threads per block of the (forward) shade stage, 128 or 256 (tpt_autotune picks it)
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                            const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A = nullptr);
+                            const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A = nullptr,
+                            int block = 256);
 cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint = false);
 // Batched stages: slot i is global path first_path + i of the jobs' index space.
 cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const WfBuffers& B, uint64_t first_path,
                                      uint32_t n_paths, cudaStream_t s);
-cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s);
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s, int block = 256);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
 
 // bounce_graphs.cpp: one wavefront bounce (single job when jobs == nullptr,

@@ -110,10 +110,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaun
 }
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
-template <bool ADJ, bool BATCH>
-__global__ void __launch_bounds__(kWfBlock, TPT_SHADE_MINB) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, int cur,
+template <bool ADJ, bool BATCH, int BS>
+__global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, int cur,
                                                      DevAdjoint A, const DevJob* __restrict__ jobs) {
-  __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
+  __shared__ float grad_sh[ADJ ? BS * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[cur]) return;
   const uint64_t first_path = (uint64_t)B.counts[4] | ((uint64_t)B.counts[5] << 32);
@@ -290,13 +290,17 @@ cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, 
   return cudaGetLastError();
 }
 
+static inline unsigned grid_for_block(uint32_t n, int bs) { return (n + bs - 1) / bs; }
+
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
-                            const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A) {
+                            const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A, int block) {
   DevRender S{geo, rd};
   if (A)
-    wf_shade<true, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, *A, nullptr);
+    wf_shade<true, false, kWfBlock><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, *A, nullptr);
+  else if (block == 128)
+    wf_shade<false, false, 128><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(S, P, B, cur, DevAdjoint{}, nullptr);
   else
-    wf_shade<false, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, DevAdjoint{}, nullptr);
+    wf_shade<false, false, kWfBlock><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, DevAdjoint{}, nullptr);
   return cudaGetLastError();
 }
 
@@ -307,9 +311,13 @@ cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s) {
-  wf_shade<false, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(DevRender{}, RenderLaunch{}, B, cur,
-                                                                  DevAdjoint{}, jobs);
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s, int block) {
+  if (block == 128)
+    wf_shade<false, true, 128><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(DevRender{}, RenderLaunch{}, B, cur,
+                                                                             DevAdjoint{}, jobs);
+  else
+    wf_shade<false, true, kWfBlock><<<grid_for(B.capacity), kWfBlock, 0, s>>>(DevRender{}, RenderLaunch{}, B, cur,
+                                                                            DevAdjoint{}, jobs);
   return cudaGetLastError();
 }
 

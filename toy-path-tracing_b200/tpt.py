@@ -170,7 +170,7 @@ GRAD_ALL = 31
 
 class TuneResult(C.Structure):
     _fields_ = [("execution", C.c_uint32), ("wavefront_capacity", C.c_uint32), ("graphs", C.c_uint32),
-                ("ms", C.c_float), ("ms_megakernel", C.c_float), ("ms_wavefront_default", C.c_float),
+                ("shade_block", C.c_uint32), ("ms", C.c_float), ("ms_megakernel", C.c_float), ("ms_wavefront_default", C.c_float),
                 ("pilot_paths", C.c_uint64)]
 
 
@@ -230,6 +230,7 @@ EXPORTED_SYMBOLS = [
     "tpt_context_set_wavefront_capacity",
     "tpt_context_wavefront_capacity",
     "tpt_context_set_graphs",
+    "tpt_context_set_shade_block",
     "tpt_autotune",
     "tpt_adjoint_device",
     "tpt_adjoint",
@@ -271,6 +272,7 @@ def _declare(L):
         "tpt_context_set_wavefront_capacity": (i32, [vp, C.c_uint32]),
         "tpt_context_wavefront_capacity": (C.c_uint32, [vp]),
         "tpt_context_set_graphs": (i32, [vp, i32]),
+        "tpt_context_set_shade_block": (i32, [vp, C.c_uint32]),
         "tpt_autotune": (i32, [vp, vp, i32, C.POINTER(TuneResult)]),
         "tpt_adjoint_device": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp, vp]),
         "tpt_adjoint": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp]),
@@ -331,6 +333,10 @@ class Context:
         r = TuneResult()
         _check(lib().tpt_autotune(self.h, arr, len(jobs), C.byref(r)), self)
         return {k: getattr(r, k) for k, _ in TuneResult._fields_}
+
+    def set_shade_block(self, threads: int):
+        """`tpt_context_set_shade_block`: 128 or 256 threads per shade block."""
+        _check(lib().tpt_context_set_shade_block(self.h, int(threads)), self)
 
     def render_batch_device(self, jobs, out_ptrs, stream=None):
         """`tpt_render_batch_device`: jobs (RenderJob list) into device images."""
