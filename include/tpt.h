@@ -172,10 +172,44 @@ typedef struct tpt_material_desc {
   const struct tpt_openpbr_desc* openpbr;
 } tpt_material_desc;
 
+/* Lights other than emissive triangles (light/{point,spot,directional}.rs),
+ * with the reference's authoring conventions.  PointLight::new: `intensity` is
+ * the emitted power in W.  SpotLight::new: the same power with a cone mask,
+ * angles in radians (total_width clamped to [0, pi], falloff_start to
+ * [0, total_width]; smoothstep falloff between them), direction normalised on
+ * upload.  DirectionalLight::new: `direction` is the direction of travel
+ * (normalised on upload), `intensity` the perpendicular irradiance in W/m^2.
+ * Point and spot lights are leaves of the SG light tree; each directional
+ * light is its own category of the light sampler (light/mod.rs:1-21). */
+typedef struct tpt_point_light_desc {
+  float position[3];
+  float color[3];
+  float intensity;
+} tpt_point_light_desc;
+
+typedef struct tpt_spot_light_desc {
+  float position[3];
+  float direction[3];
+  float color[3];
+  float intensity;
+  float total_width;
+  float falloff_start;
+} tpt_spot_light_desc;
+
+typedef struct tpt_directional_light_desc {
+  float direction[3];
+  float color[3];
+  float intensity;
+} tpt_directional_light_desc;
+
 /* One node of the SG light tree (light_tree/mod.rs:65-86), 64 bytes:
  * interior nodes have leaf_instance == leaf_triangle == 0xFFFFFFFF; leaves name
- * the emissive triangle and carry its area.  Children/parent are node
- * indices (0xFFFFFFFF = none). */
+ * the emissive triangle and carry its area, or a point light
+ * (leaf_instance == TPT_LIGHT_LEAF_POINT, leaf_triangle = its index) or a spot
+ * light (TPT_LIGHT_LEAF_SPOT).  Children/parent are node indices
+ * (0xFFFFFFFF = none). */
+#define TPT_LIGHT_LEAF_POINT 0xFFFFFFFEu
+#define TPT_LIGHT_LEAF_SPOT 0xFFFFFFFDu
 typedef struct tpt_light_node {
   float flux;
   float mu[3];
@@ -206,8 +240,18 @@ typedef struct tpt_scene_desc {
   uint32_t num_materials;
   /* Pre-built light tree (`Scene::light_tree`); NULL nodes = build on upload
    * with the binned-SAOH builder (light_tree/builder.rs) over the emissive
-   * triangles, in the order Scene::add_instance registers them. */
+   * triangles, in the order Scene::add_instance registers them, then the
+   * point lights, then the spot lights. */
   tpt_light_tree_view light_tree;
+  /* Scene::point_lights / spot_lights / directional_lights (may be NULL when
+   * the count is 0).  BDPT jobs reject scenes with lights that are not
+   * emissive triangles (the device BDPT covers area lights only). */
+  const tpt_point_light_desc* point_lights;
+  uint32_t num_point_lights;
+  const tpt_spot_light_desc* spot_lights;
+  uint32_t num_spot_lights;
+  const tpt_directional_light_desc* directional_lights;
+  uint32_t num_directional_lights;
 } tpt_scene_desc;
 
 /* Copies the scene into device memory in the B200 layout (128-byte nodes,
@@ -449,7 +493,9 @@ typedef struct tpt_adjoint_desc {
  * the radiance the path collects after the vertex and df/dtheta a central
  * difference of the BSDF at the sampled direction between host-lowered
  * theta -/+ fd_step copies of the material (clipped to [0, 1], the IOR to
- * [1, 10]).  Accumulation is FP64 atomics, so the sums' order (and last bits)
+ * [1, 10]); an unoccluded light sample C at an OpenPBR vertex (directional
+ * lights) adds dLoss/dL * C * (df/dtheta) / f at the light direction.
+ * Accumulation is FP64 atomics, so the sums' order (and last bits)
  * vary between runs.  adesc may be NULL (all groups, step 1e-3). */
 tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const tpt_adjoint_desc* adesc,
                               const float* d_image, double* grad, void* stream);

@@ -87,7 +87,8 @@ def _declare(L):
         "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u32, u64, u64, vp, i32]),
         "orc_render_adjoint": (None, [vp, vp, u32, u32, u32, u32, vp, u32, C.c_float, vp, i32]),
         "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
-        "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, vp]),
+        "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, f32, vp]),
+        "orc_render_scene_set_lights": (None, [vp, vp, u32, vp, u32, vp, u32]),
         "orc_render_emitted": (None, [vp, i32, i32, vp, vp, i32, i32, vp, vp, vp, f32, i32, vp]),
         "orc_render_material_pdf": (f32, [vp, i32, i32, vp, vp, vp]),
         "orc_render_scene_set_openpbr": (C.c_char_p, [vp, u32, vp]),
@@ -230,8 +231,20 @@ def camera_ray(params, rx, ry, px, py, ux, uy, spp):
     return out
 
 
+def light_arrays(scene: dict):
+    """Point (n x 7), spot (n x 12) and directional (n x 7) light arrays of a
+    scene dict's "point_lights", "spot_lights", "directional_lights" lists."""
+    pts = np.array([[*l["position"], *l["color"], l["intensity"]] for l in scene.get("point_lights", [])],
+                   np.float32).reshape(-1, 7)
+    spots = np.array([[*l["position"], *l["direction"], *l["color"], l["intensity"], l["total_width"],
+                       l["falloff_start"]] for l in scene.get("spot_lights", [])], np.float32).reshape(-1, 12)
+    dirs = np.array([[*l["direction"], *l["color"], l["intensity"]] for l in scene.get("directional_lights", [])],
+                    np.float32).reshape(-1, 7)
+    return pts, spots, dirs
+
+
 class RenderScene:
-    """Oracle render scene: geometry + materials + a flattened light tree.
+    """Oracle render scene: geometry + materials + lights + a flattened light tree.
 
     scene: dict with meshes, instances, materials (tpt_scenes layout);
     light_tree: (nodes, root) in the tpt_light_node layout (the tree the
@@ -259,6 +272,9 @@ class RenderScene:
                 why = lib().orc_render_scene_set_openpbr(self.h, i, _p(pack_openpbr(m)))
                 if why:
                     raise ValueError(why.decode())
+        pts, spots, dirs = light_arrays(scene)
+        self.non_area_lights = len(pts) + len(spots) + len(dirs)
+        lib().orc_render_scene_set_lights(self.h, _p(pts), len(pts), _p(spots), len(spots), _p(dirs), len(dirs))
         nodes, root = light_tree
         nodes = np.ascontiguousarray(nodes)
         lib().orc_render_scene_set_light_tree(self.h, nodes.ctypes.data if len(nodes) else None, len(nodes), int(root))
@@ -275,9 +291,14 @@ class RenderScene:
         return np.array([*camera["eye"], *camera["look_at"], *camera["up"], camera["fov_y"],
                          camera.get("exposure", 1.0)], np.float32)
 
+    def _check_integrator(self, integrator):
+        if integrator == 1 and self.non_area_lights:
+            raise ValueError("the oracle's BDPT covers area lights only")
+
     def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0):
         """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3].
         integrator: 0 MIS (integrator/mis.rs), 1 BDPT (integrator/bdpt.rs)."""
+        self._check_integrator(integrator)
         p0, p1 = pixels if pixels is not None else (0, width * height)
         out = np.empty((p1 - p0, 3), np.float32)
         cam = self._cam(camera)
@@ -286,6 +307,7 @@ class RenderScene:
         return out
 
     def samples(self, camera, width, height, spp, max_depth, first, count, nthreads=None, integrator=0):
+        self._check_integrator(integrator)
         out = np.empty((count, 3), np.float32)
         cam = self._cam(camera)
         lib().orc_render_samples(self.h, _p(cam), width, height, spp, max_depth, integrator, first, count, _p(out),
@@ -305,12 +327,12 @@ class RenderScene:
         return out
 
     # -- unit-level queries (reference integrator unit tests) -------------------
-    def direct_light(self, inst, tri, bary, incident, u_tree, us):
+    def direct_light(self, inst, tri, bary, incident, u_tree, us, u_category=0.0):
         out = np.zeros(3, np.float32)
         b = np.asarray(bary, np.float32)
         d = np.asarray(incident, np.float32)
-        lib().orc_render_direct_light(self.h, inst, tri, _p(b), _p(d), float(u_tree), float(us[0]), float(us[1]),
-                                      _p(out))
+        lib().orc_render_direct_light(self.h, inst, tri, _p(b), _p(d), float(u_category), float(u_tree),
+                                      float(us[0]), float(us[1]), _p(out))
         return out
 
     def emitted(self, inst, tri, bary, incident, linst, ltri, lbary, lincident, throughput, bsdf_pdf, delta=False):

@@ -1,4 +1,5 @@
 // Oracle C entry points for rendering (test infrastructure only).
+#include <cmath>
 #include <cstring>
 
 #include "render.h"
@@ -25,6 +26,36 @@ void orc_render_scene_set_materials(void* h, const uint32_t* kinds, const float*
     s->materials[i].rho = Vec3(rho[3 * i], rho[3 * i + 1], rho[3 * i + 2]);
     s->materials[i].color = Vec3(color[3 * i], color[3 * i + 1], color[3 * i + 2]);
     s->materials[i].strength = strength[i];
+  }
+}
+
+// Point lights: n x 7 floats (position, color, intensity); spot lights: n x 12
+// (position, direction, color, intensity, total width, falloff start in
+// radians: SpotLight::new); directional: n x 7 (direction, color, intensity:
+// DirectionalLight::new).  Call before the light tree (which finalises).
+void orc_render_scene_set_lights(void* h, const float* points, uint32_t np, const float* spots, uint32_t ns,
+                                 const float* dirs, uint32_t nd) {
+  auto* s = (RenderScene*)h;
+  s->points.resize(np);
+  for (uint32_t i = 0; i < np; ++i) {
+    const float* a = points + 7 * i;
+    s->points[i] = PointLight{Vec3(a[0], a[1], a[2]), Vec3(a[3], a[4], a[5]), a[6]};
+  }
+  const float pi = 3.14159274101257324f;
+  s->spots.resize(ns);
+  for (uint32_t i = 0; i < ns; ++i) {
+    const float* a = spots + 12 * i;
+    float total_width = clampf(a[10], 0.0f, pi);
+    float falloff_start = clampf(a[11], 0.0f, total_width);
+    Vec3 d(a[3], a[4], a[5]);
+    s->spots[i] = SpotLight{Vec3(a[0], a[1], a[2]), d * (1.0f / length(d)), Vec3(a[6], a[7], a[8]), a[9],
+                            std::cos(total_width), std::cos(falloff_start)};
+  }
+  s->dirs.resize(nd);
+  for (uint32_t i = 0; i < nd; ++i) {
+    const float* a = dirs + 7 * i;
+    Vec3 d(a[0], a[1], a[2]);
+    s->dirs[i] = DirLight{d * (1.0f / length(d)), Vec3(a[3], a[4], a[5]), a[6]};
   }
 }
 

@@ -306,35 +306,121 @@ bool closest(const RenderScene& s, Vec3 o, Vec3 d, SceneHit* h) {
   return s.geo.closest_hit(r, h);
 }
 
-// integrator/mis.rs:145-210
-Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd) {
-  if (!s.has_tree) return Vec3(0, 0, 0);  // sample_category: no category
-  if (m.kind != kLambert) return Vec3(0, 0, 0);
-  Query q;
-  q.rho = luminance(m.rho);
-  if (q.rho <= 0.0f) return Vec3(0, 0, 0);
-  q.p = v.p;
-  q.n = v.ns;
-  float leaf_pmf;
-  uint32_t leaf = sample_tree(s, q, rnd.light.u_tree, &leaf_pmf);
-  if (leaf == kNoNode) return Vec3(0, 0, 0);
+// point::sample_li (light/point.rs:32-50)
+bool sample_li_point(const PointLight& l, Vec3 p_ref, LiSample* out) {
+  Vec3 to_light = l.position - p_ref;
+  float d2 = length_squared(to_light);
+  if (d2 <= 0.0f) return false;
+  float dist = std::sqrt(d2);
+  out->wi = to_light / dist;
+  out->radiance = l.color * (l.intensity / (4.0f * kPi * d2));
+  out->pdf = 1.0f;
+  out->distance = dist;
+  out->inst = out->tri = -1;
+  return true;
+}
+// math/mod.rs:180-183
+float smoothstep(float e0, float e1, float x) {
+  float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+// spot::sample_li (light/spot.rs:51-76)
+bool sample_li_spot(const SpotLight& l, Vec3 p_ref, LiSample* out) {
+  Vec3 to_light = l.position - p_ref;
+  float d2 = length_squared(to_light);
+  if (d2 <= 0.0f) return false;
+  float dist = std::sqrt(d2);
+  Vec3 wi = to_light / dist;
+  float falloff = smoothstep(l.cos_total_width, l.cos_falloff_start, dot(-wi, l.direction));
+  if (falloff <= 0.0f) return false;
+  out->wi = wi;
+  out->radiance = l.color * (l.intensity * falloff / (2.0f * kTau * d2));
+  out->pdf = 1.0f;
+  out->distance = dist;
+  out->inst = out->tri = -1;
+  return true;
+}
+
+// LightSampler::sample_category (light/mod.rs:197-212); -2 when empty
+int sample_category(const RenderScene& s, float u, float* pmf) {
+  if (s.cat_kind.empty()) return -2;
+  u = clampf(u, 0.0f, 1.0f);
+  size_t n = 0;
+  for (size_t k = 0; k < s.cat_cdf.size(); ++k)
+    if (s.cat_cdf[k] <= u) n = k + 1;
+  size_t idx = std::min(n == 0 ? (size_t)0 : n - 1, s.cat_kind.size() - 1);
+  *pmf = s.cat_pmf[idx];
+  return s.cat_kind[idx];
+}
+
+// integrator/mis.rs:145-210 with sample_light_mis_compensated_lazy
+// (light/mod.rs:296-340): the tree category needs a light-tree query (the
+// diffuse material is the only one in scope that builds one); directional
+// lights serve every scattering material.  Delta lights take no MIS weight.
+// wi_out (optional) receives the sampled light direction.
+Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
+                  Vec3* wi_out = nullptr) {
+  float cat_pmf = 0.0f;
+  int cat = sample_category(s, rnd.light.u_category, &cat_pmf);
+  if (cat == -2) return Vec3(0, 0, 0);  // no category
   LiSample li;
-  if (!sample_li_triangle(s, (int)s.tree[leaf].leaf_instance, (int)s.tree[leaf].leaf_triangle, v.p,
-                          rnd.light.u_surface, &li))
-    return Vec3(0, 0, 0);
-  float sel = s.tree_cat_pmf * leaf_pmf;
+  float sel;
+  bool delta = true;
+  if (cat == -1) {
+    if (m.kind != kLambert) return Vec3(0, 0, 0);
+    Query q;
+    q.rho = luminance(m.rho);
+    if (q.rho <= 0.0f) return Vec3(0, 0, 0);
+    q.p = v.p;
+    q.n = v.ns;
+    float leaf_pmf;
+    uint32_t leaf = sample_tree(s, q, rnd.light.u_tree, &leaf_pmf);
+    if (leaf == kNoNode) return Vec3(0, 0, 0);
+    const uint32_t li_inst = s.tree[leaf].leaf_instance, li_tri = s.tree[leaf].leaf_triangle;
+    if (li_inst == kLeafPoint) {
+      if (!sample_li_point(s.points[li_tri], v.p, &li)) return Vec3(0, 0, 0);
+    } else if (li_inst == kLeafSpot) {
+      if (!sample_li_spot(s.spots[li_tri], v.p, &li)) return Vec3(0, 0, 0);
+    } else {
+      if (!sample_li_triangle(s, (int)li_inst, (int)li_tri, v.p, rnd.light.u_surface, &li)) return Vec3(0, 0, 0);
+      delta = false;
+    }
+    sel = cat_pmf * leaf_pmf;
+  } else {
+    // directional::sample_li (light/directional.rs:33-42)
+    const DirLight& d = s.dirs[cat];
+    li.radiance = d.color * d.intensity;
+    li.wi = -d.direction;
+    li.pdf = 1.0f;
+    li.distance = INFINITY;
+    li.inst = li.tri = -1;
+    sel = cat_pmf;
+  }
   if (li.pdf <= 0.0f || sel <= 0.0f) return Vec3(0, 0, 0);
-  Vec3 f = lambert_eval(m, v, li.wi);
-  float bsdf_pdf = length_squared(f) == 0.0f ? 0.0f : lambert_pdf(v, li.wi);
+  Vec3 f;
+  float bsdf_pdf = 0.0f;
+  if (delta) {
+    f = m.kind == kLambert ? lambert_eval(m, v, li.wi) : material_eval(m, v, li.wi, kRadiance);
+  } else {
+    f = lambert_eval(m, v, li.wi);
+    bsdf_pdf = length_squared(f) == 0.0f ? 0.0f : lambert_pdf(v, li.wi);
+  }
   if (length_squared(f) == 0.0f) return Vec3(0, 0, 0);
   float cos_surface = std::fabs(dot(v.ng, li.wi));
   if (cos_surface <= 0.0f) return Vec3(0, 0, 0);
   // unoccluded_ray (integrator/mod.rs:239-265)
   SceneHit h;
-  if (closest(s, offset_origin(v.p, v.ng, li.wi), li.wi, &h) && !(h.instance == li.inst && h.triangle == li.tri))
-    return Vec3(0, 0, 0);
+  if (closest(s, offset_origin(v.p, v.ng, li.wi), li.wi, &h)) {
+    bool visible;
+    if (li.inst >= 0) visible = h.instance == li.inst && h.triangle == li.tri;
+    else if (std::isinf(li.distance)) visible = false;
+    else visible = h.t >= li.distance * (1.0f - 1.0e-3f);
+    if (!visible) return Vec3(0, 0, 0);
+  }
   float pdf_total = sel * li.pdf;
   if (pdf_total <= 0.0f) return Vec3(0, 0, 0);
+  if (wi_out) *wi_out = li.wi;
+  if (delta) return li.radiance * f * (cos_surface / pdf_total);
   float mis = balance(pdf_total, bsdf_pdf);
   return li.radiance * f * (cos_surface * mis / pdf_total);
 }
@@ -394,9 +480,11 @@ void RenderScene::finalize() {
   for (size_t i = 0; i < geo.instances.size(); ++i)
     if (materials[geo.instances[i].material_index].kind == kEmissive)
       leaf_of[i].assign(geo.meshes[geo.instances[i].mesh_index].triangle_count(), kNoNode);
-  for (uint32_t k = 0; k < tree.size(); ++k)
-    if (tree[k].leaf_instance != kNoNode && !leaf_of[tree[k].leaf_instance].empty())
-      leaf_of[tree[k].leaf_instance][tree[k].leaf_triangle] = k;
+  for (uint32_t k = 0; k < tree.size(); ++k) {
+    const uint32_t li = tree[k].leaf_instance;
+    if (li == kNoNode || li == kLeafPoint || li == kLeafSpot) continue;
+    if (!leaf_of[li].empty()) leaf_of[li][tree[k].leaf_triangle] = k;
+  }
   // Scene::register_area_light_triangles (scene/mod.rs:649-684), per instance in order
   area_lights.clear();
   area_light_weight_sum = 0.0f;
@@ -417,10 +505,37 @@ void RenderScene::finalize() {
       area_lights.push_back(AreaLight{(int32_t)i, t, area, weight, area_light_weight_sum});
     }
   }
+  // LightSampler::build_from_scene (light/mod.rs:134-188): Tree, then one
+  // category per directional light with luminance(color) * intensity > 0
   float w = tree.empty() ? 0.0f : fmax_num(tree[root].flux, 0.0f);
   has_tree = w > 0.0f;
-  float total = 0.0f + w;
-  tree_cat_pmf = has_tree ? w / total : 0.0f;
+  std::vector<float> weights;
+  cat_kind.clear();
+  if (w > 0.0f) {
+    cat_kind.push_back(-1);
+    weights.push_back(w);
+  }
+  for (size_t i = 0; i < dirs.size(); ++i) {
+    float dw = fmax_num(luminance(dirs[i].color) * dirs[i].intensity, 0.0f);
+    if (dw > 0.0f) {
+      cat_kind.push_back((int)i);
+      weights.push_back(dw);
+    }
+  }
+  cat_cdf.assign(1, 0.0f);
+  float total = 0.0f;
+  for (float x : weights) {
+    total += x;
+    cat_cdf.push_back(total);
+  }
+  if (total > 0.0f) {
+    float inv = 1.0f / total;
+    for (float& c : cat_cdf) c *= inv;
+  }
+  cat_pmf.assign(weights.size(), 0.0f);
+  for (size_t k = 0; k < weights.size(); ++k) cat_pmf[k] = total > 0.0f ? weights[k] / total : 0.0f;
+  if (!(total > 0.0f)) cat_kind.clear();
+  tree_cat_pmf = has_tree && total > 0.0f ? w / total : 0.0f;
 }
 
 void RenderScene::triangle_world(int inst, int tri, Vec3* p) const {
@@ -520,7 +635,12 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
     if (m->kind == kEmissive) break;
-    R = R - beta * direct_light(s, *m, v, rnd);
+    Vec3 wl(0, 0, 0);
+    const Vec3 c = beta * direct_light(s, *m, v, rnd, &wl);
+    R = R - c;
+    // a light sample at an OpenPBR vertex (directional lights): its
+    // contribution scales with f at the light direction
+    if (m->kind == kOpenPbr && length_squared(c) > 0.0f) sink.vertex(mi, v, wl, c);
     MatSample bs;
     bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
                                   : lambert_sample(*m, v, rnd.material.u_dir, &bs);
@@ -591,13 +711,14 @@ extern "C" {
 
 // direct_light_mis_contribution at the shading vertex of (inst, tri, bary) seen
 // along `incident` (integrator/mis.rs:145-210).
-void orc_render_direct_light(void* h, int inst, int tri, const float* bary3, const float* incident3, float u_tree,
-                             float us0, float us1, float* out3) {
+void orc_render_direct_light(void* h, int inst, int tri, const float* bary3, const float* incident3, float u_cat,
+                             float u_tree, float us0, float us1, float* out3) {
   using namespace orc;
   const RenderScene& s = *(const RenderScene*)h;
   Vertex v = s.shading_vertex(inst, tri, Vec3(bary3[0], bary3[1], bary3[2]),
                               Vec3(incident3[0], incident3[1], incident3[2]));
   VertexRandoms rnd{};
+  rnd.light.u_category = u_cat;
   rnd.light.u_tree = u_tree;
   rnd.light.u_surface = Vec2(us0, us1);
   Vec3 r = direct_light(s, s.mat_of(inst), v, rnd);

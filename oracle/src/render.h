@@ -70,9 +70,34 @@ struct AreaLight {
   float area, weight, prefix_weight;
 };
 
+// light/point.rs, light/spot.rs, light/directional.rs as their constructors
+// store them (SpotLight::new clamps the angles and keeps their cosines; spot and
+// directional directions are normalised).
+struct PointLight {
+  Vec3 position, color;
+  float intensity;
+};
+struct SpotLight {
+  Vec3 position, direction, color;
+  float intensity, cos_total_width, cos_falloff_start;
+};
+struct DirLight {
+  Vec3 direction, color;
+  float intensity;
+};
+static constexpr uint32_t kLeafPoint = 0xFFFFFFFEu;  // light-tree leaf of a point light
+static constexpr uint32_t kLeafSpot = 0xFFFFFFFDu;   // light-tree leaf of a spot light
+
 struct RenderScene {
   Geometry geo;
   std::vector<Material> materials;
+  std::vector<PointLight> points;
+  std::vector<SpotLight> spots;
+  std::vector<DirLight> dirs;
+  // LightSampler (light/mod.rs:117-188): categories (-1 = the tree, i >= 0 =
+  // directional light i), their CDF and pmfs
+  std::vector<int> cat_kind;
+  std::vector<float> cat_cdf, cat_pmf;
   std::vector<AreaLight> area_lights;  // Scene::area_light_triangles, instance order
   float area_light_weight_sum = 0.0f;
   std::vector<LightNode> tree;

@@ -152,10 +152,23 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   A.grad = grad;
   A.scale = L.cam.exposure / (float)L.spp;
   A.mask = mask;
+  A.s_grad = nullptr;
+  A.s_gkey = nullptr;
   const uint32_t npix = L.width * L.height;
   const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
-  if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
+  // light samples at OpenPBR vertices come from directional lights only (the
+  // light tree serves diffuse vertices): their gradient planes follow the
+  // samples in the scratch buffer, sized for the wavefront's capacity
+  const bool light_grads = scene->num_directional_lights > 0;
+  if ((st = ensure_wavefront(ctx, cp * L.spp))) return st;
+  const size_t sample_bytes = ((size_t)cp * L.spp * 12 + 255) & ~(size_t)255;
+  const size_t plane_bytes = light_grads ? (size_t)(kGradParams + 1) * ctx->wf.capacity * 4 : 0;
+  if ((st = ensure_scratch(ctx, sample_bytes + plane_bytes))) return st;
   float* samples = (float*)ctx->d_scratch;
+  if (light_grads) {
+    A.s_grad = (float*)((char*)ctx->d_scratch + sample_bytes);
+    A.s_gkey = (uint32_t*)(A.s_grad + (size_t)kGradParams * ctx->wf.capacity);
+  }
   for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
     const uint32_t n = std::min(cp, npix - p0);
     const uint64_t first = (uint64_t)p0 * L.spp;

@@ -29,6 +29,10 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
     return set_error(ctx, TPT_ERR_INVALID_ARG, "width, height and spp must be positive");
   if (job->integrator != TPT_INTEGRATOR_MIS && job->integrator != TPT_INTEGRATOR_BDPT)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown integrator");
+  if (job->integrator == TPT_INTEGRATOR_BDPT &&
+      job->scene->num_point_lights + job->scene->num_spot_lights + job->scene->num_directional_lights > 0)
+    return set_error(ctx, TPT_ERR_INVALID_ARG,
+                     "BDPT with point, spot or directional lights is not on the device path (area lights only)");
   if (job->integrator == TPT_INTEGRATOR_BDPT && job->max_depth > kBdptMaxDepthApi)
     return set_error(ctx, TPT_ERR_CAPACITY,
                      "BDPT max_depth " + std::to_string(job->max_depth) + " above the device limit of " +
@@ -87,10 +91,10 @@ tpt_status ensure_scratch(tpt_context* ctx, size_t bytes) {
 tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   if (ctx->wf.capacity >= capacity && ctx->d_wf) return TPT_OK;
   const size_t C = capacity;
-  // float planes: beta 3, L 3, prev 7, q_ray 2*7, h_t 1, h_bary 3, s_ray 7, s_contrib 3, s_t 1
+  // float planes: beta 3, L 3, prev 7, q_ray 2*7, h_t 1, h_bary 3, s_ray 7, s_contrib 3, s_t 1, s_dist 1
   // u32 planes: prev_mat, depth, q_slot 2, h_tri, h_inst, s_slot, s_target 2, s_tri, s_inst,
   // job, q_job 2, s_job
-  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4;
+  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4;
   const size_t bytes = planes * C * 4 + 256;
   if (ctx->d_wf) {
     cudaDeviceSynchronize();
@@ -130,6 +134,7 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   B.s_tri = (int32_t*)take(1);
   B.s_inst = (int32_t*)take(1);
   B.s_t = (float*)take(1);
+  B.s_dist = (float*)take(1);
   B.job = (uint32_t*)take(1);
   B.q_job[0] = (uint32_t*)take(1);
   B.q_job[1] = (uint32_t*)take(1);
@@ -164,7 +169,7 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
       e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
                                   nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
                                   nullptr, B.counts + 2);
-    if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s, A != nullptr);
+    if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s, A);
   }
   if (e == cudaSuccess && !A) e = launch_wf_finalize(B, n, samples, s);
   return cuda_check(ctx, e, "wavefront launch");

@@ -79,6 +79,7 @@ struct tpt_scene {
   tpt::DevRenderData render{};          // shading data for the render kernels
   tpt::LightTreeHost light_tree;        // host copy of the light tree
   std::vector<uint32_t> material_kinds; // tpt_material_kind per material
+  uint32_t num_point_lights = 0, num_spot_lights = 0, num_directional_lights = 0;
   // OpenPBR materials: host copy of each table entry's parameters and the
   // material -> table index map (0xFFFFFFFF: not OpenPBR)
   std::vector<tpt_openpbr_desc> opbr_desc;
@@ -155,7 +156,7 @@ cudaError_t launch_wf_generate(const DevGeometry& geo, const DevRenderData& rd, 
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                             const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A = nullptr,
                             int block = 256);
-cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint = false);
+cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, const DevAdjoint* A = nullptr);
 // Batched stages: slot i is global path first_path + i of the jobs' index space.
 cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const WfBuffers& B, uint64_t first_path,
                                      uint32_t n_paths, cudaStream_t s);

@@ -116,6 +116,56 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
     hmesh[m] = HostMesh{md.positions, md.normals, md.uvs, md.indices, (uint32_t)md.num_vertices, mi.num_tris};
   }
 
+  // point, spot and directional lights (PointLight::new, SpotLight::new, DirectionalLight::new)
+  if ((desc->num_point_lights && !desc->point_lights) || (desc->num_spot_lights && !desc->spot_lights) ||
+      (desc->num_directional_lights && !desc->directional_lights))
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL light array");
+  std::vector<HostPointLight> hpoints(desc->num_point_lights);
+  std::vector<DevPointLight> dpoints(desc->num_point_lights);
+  for (uint32_t i = 0; i < desc->num_point_lights; ++i) {
+    const tpt_point_light_desc& d = desc->point_lights[i];
+    HostPointLight h{};
+    DevPointLight dp{};
+    for (int k = 0; k < 3; ++k) {
+      h.position[k] = dp.position[k] = d.position[k];
+      h.color[k] = dp.color[k] = d.color[k];
+    }
+    h.intensity = dp.intensity = d.intensity;
+    hpoints[i] = h;
+    dpoints[i] = dp;
+  }
+  std::vector<HostSpotLight> hspots(desc->num_spot_lights);
+  std::vector<DevSpotLight> dspots(desc->num_spot_lights);
+  for (uint32_t i = 0; i < desc->num_spot_lights; ++i) {
+    const tpt_spot_light_desc& d = desc->spot_lights[i];
+    make_spot_light(d.position, d.direction, d.color, d.intensity, d.total_width, d.falloff_start, &hspots[i]);
+    DevSpotLight ds{};
+    std::memcpy(ds.position, hspots[i].position, 12);
+    std::memcpy(ds.direction, hspots[i].direction, 12);
+    std::memcpy(ds.color, hspots[i].color, 12);
+    ds.intensity = hspots[i].intensity;
+    ds.cos_total_width = hspots[i].cos_total_width;
+    ds.cos_falloff_start = hspots[i].cos_falloff_start;
+    dspots[i] = ds;
+  }
+  std::vector<DevDirLight> ddirs(desc->num_directional_lights);
+  for (uint32_t i = 0; i < desc->num_directional_lights; ++i) {
+    const tpt_directional_light_desc& d = desc->directional_lights[i];
+    const float len = std::sqrt(d.direction[0] * d.direction[0] + d.direction[1] * d.direction[1] +
+                                d.direction[2] * d.direction[2]);
+    const float r = 1.0f / len;  // glam normalize: v * (1 / length)
+    DevDirLight dd{};
+    for (int k = 0; k < 3; ++k) {
+      dd.direction[k] = d.direction[k] * r;
+      dd.color[k] = d.color[k];
+    }
+    dd.intensity = d.intensity;
+    ddirs[i] = dd;
+  }
+  s->num_point_lights = desc->num_point_lights;
+  s->num_spot_lights = desc->num_spot_lights;
+  s->num_directional_lights = desc->num_directional_lights;
+
   // light tree: the caller's, or built here (builder.rs)
   std::vector<HostInstance> hinst(desc->num_instances);
   for (uint32_t i = 0; i < desc->num_instances; ++i) {
@@ -131,7 +181,10 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
     for (uint64_t i = 0; i < nn; ++i) {
       const LightNodeHost& n = s->light_tree.nodes[i];
       const bool leaf = n.leaf_instance != kInvalidNode;
-      if (leaf) {
+      if (leaf && (n.leaf_instance == kLeafPoint || n.leaf_instance == kLeafSpot)) {
+        if (n.leaf_triangle >= (n.leaf_instance == kLeafPoint ? desc->num_point_lights : desc->num_spot_lights))
+          return set_error(ctx, TPT_ERR_INVALID_ARG, "light tree leaf names an unknown point or spot light");
+      } else if (leaf) {
         if (n.leaf_instance >= desc->num_instances ||
             n.leaf_triangle >= minfo[desc->instances[n.leaf_instance].mesh_index].num_tris)
           return set_error(ctx, TPT_ERR_INVALID_ARG, "light tree leaf names an unknown triangle");
@@ -142,7 +195,8 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
     }
   } else if (desc->num_materials) {
     HostSceneView view{hmesh.data(), desc->num_meshes, hinst.data(), desc->num_instances, hmats.data(),
-                       desc->num_materials};
+                       desc->num_materials, hpoints.data(), desc->num_point_lights, hspots.data(),
+                       desc->num_spot_lights};
     build_light_tree_host(view, &s->light_tree);
   }
 
@@ -168,7 +222,7 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   std::vector<uint32_t> emap(map_size, kInvalidNode);
   for (uint32_t k = 0; k < s->light_tree.nodes.size(); ++k) {
     const LightNodeHost& n = s->light_tree.nodes[k];
-    if (n.leaf_instance == kInvalidNode) continue;
+    if (n.leaf_instance == kInvalidNode || n.leaf_instance == kLeafPoint || n.leaf_instance == kLeafSpot) continue;
     const uint32_t base = sinst[n.leaf_instance].leaf_base;
     if (base != kInvalidNode) emap[base + n.leaf_triangle] = k;
   }
@@ -204,6 +258,9 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   if (!st) st = put(s, opbr, &R.openpbr);
   if (!st) st = put(s, dal, &R.area_lights);
   if (!st) st = put(s, al_of, &R.area_light_of);
+  if (!st) st = put(s, dpoints, &R.points);
+  if (!st) st = put(s, dspots, &R.spots);
+  if (!st) st = put(s, ddirs, &R.dirs);
   if (st) return st;
   R.num_area_lights = (uint32_t)dal.size();
   R.area_light_weight_sum = al_sum;
@@ -211,12 +268,43 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   R.dec_e = ctx->d_dec_e;
   R.ltree_root = s->light_tree.root;
   R.num_materials = desc->num_materials;
-  // LightSampler::build_from_scene (light/mod.rs:134-188) with only the Tree category
+  // LightSampler::build_from_scene (light/mod.rs:134-188): the Tree category,
+  // then one per directional light with luminance(color) * intensity > 0
+  // (there is no environment light here)
   const float tree_w = lnodes.empty() ? 0.0f : std::fmax(lnodes[R.ltree_root].flux, 0.0f);
   R.has_tree = tree_w > 0.0f ? 1u : 0u;
-  const float total = 0.0f + tree_w;
-  R.tree_cat_pmf = R.has_tree ? tree_w / total : 0.0f;
-  return TPT_OK;
+  std::vector<uint32_t> kinds;
+  std::vector<float> weights;
+  if (tree_w > 0.0f) {
+    kinds.push_back(kCatTree);
+    weights.push_back(tree_w);
+  }
+  for (uint32_t i = 0; i < desc->num_directional_lights; ++i) {
+    const DevDirLight& d = ddirs[i];
+    const float w = std::fmax((0.2126f * d.color[0] + 0.7152f * d.color[1] + 0.0722f * d.color[2]) * d.intensity,
+                              0.0f);
+    if (w > 0.0f) {
+      kinds.push_back(1u + i);
+      weights.push_back(w);
+    }
+  }
+  std::vector<float> cdf(1, 0.0f), pmf(weights.size());
+  float total = 0.0f;
+  for (float w : weights) {
+    total += w;
+    cdf.push_back(total);
+  }
+  if (total > 0.0f) {
+    const float inv = 1.0f / total;
+    for (float& c : cdf) c *= inv;
+  }
+  for (size_t k = 0; k < weights.size(); ++k) pmf[k] = total > 0.0f ? weights[k] / total : 0.0f;
+  R.tree_cat_pmf = R.has_tree && total > 0.0f ? tree_w / total : 0.0f;
+  R.num_cat = total > 0.0f ? (uint32_t)kinds.size() : 0u;
+  if (!st) st = put(s, cdf, &R.cat_cdf);
+  if (!st) st = put(s, pmf, &R.cat_pmf);
+  if (!st) st = put(s, kinds, &R.cat_kind);
+  return st;
 }
 
 }  // namespace tpt
@@ -260,11 +348,28 @@ tpt_status tpt_light_tree_build(const tpt_scene_desc* desc, tpt_light_tree** out
       return set_error(nullptr, TPT_ERR_INVALID_ARG, "instance " + std::to_string(i) + " references out of range");
     inst[i] = HostInstance{id.mesh_index, id.material_index, id.local_to_world, id.world_to_local, id.normal_to_world};
   }
+  if ((desc->num_point_lights && !desc->point_lights) || (desc->num_spot_lights && !desc->spot_lights))
+    return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL light array");
+  std::vector<HostPointLight> points(desc->num_point_lights);
+  for (uint32_t i = 0; i < desc->num_point_lights; ++i) {
+    const tpt_point_light_desc& d = desc->point_lights[i];
+    for (int k = 0; k < 3; ++k) {
+      points[i].position[k] = d.position[k];
+      points[i].color[k] = d.color[k];
+    }
+    points[i].intensity = d.intensity;
+  }
+  std::vector<HostSpotLight> spots(desc->num_spot_lights);
+  for (uint32_t i = 0; i < desc->num_spot_lights; ++i) {
+    const tpt_spot_light_desc& d = desc->spot_lights[i];
+    make_spot_light(d.position, d.direction, d.color, d.intensity, d.total_width, d.falloff_start, &spots[i]);
+  }
   auto* t = new tpt_light_tree();
-  HostSceneView v{meshes.data(), desc->num_meshes, inst.data(), desc->num_instances, hm.data(), desc->num_materials};
+  HostSceneView v{meshes.data(), desc->num_meshes, inst.data(), desc->num_instances, hm.data(), desc->num_materials,
+                  points.data(), desc->num_point_lights, spots.data(), desc->num_spot_lights};
   if (!build_light_tree_host(v, &t->t)) {
     delete t;
-    return set_error(nullptr, TPT_ERR_INVALID_ARG, "no emissive triangle: build_light_tree returns None");
+    return set_error(nullptr, TPT_ERR_INVALID_ARG, "no emitter with positive flux: build_light_tree returns None");
   }
   *out = t;
   return TPT_OK;

@@ -37,13 +37,16 @@ __device__ __forceinline__ V3 perturbed_f(const opbr::OpbrVertex& base, const De
   return f;
 }
 
-// Gradient contributions of one rough OpenPBR vertex: w = dLoss/dL (per
-// channel) * R, out[kGradParams] (zeros where the group is masked off).
-static __device__ __noinline__ void openpbr_vertex_grads(const DevRender& S, const DevAdjoint& A,
-                                                          uint32_t opbr_index, const Vertex& v, V3 wi, V3 w,
-                                                          float* out) {
+// Per-channel sensitivities of one rough OpenPBR vertex at the pair (wo, wi):
+// sens[3 * g + c] = (df_c / dtheta_g) / f_c for parameter group g (for the
+// base colour, channel c's own parameter), zero where the group is masked off
+// or f_c = 0.  A contribution C that scales with f_c adds C_c * sens[3g + c]
+// to the group's gradient.
+static __device__ __noinline__ void openpbr_vertex_sens(const DevRender& S, const DevAdjoint& A,
+                                                         uint32_t opbr_index, const Vertex& v, V3 wi,
+                                                         float* sens) {
 #pragma unroll
-  for (int k = 0; k < (int)kGradParams; ++k) out[k] = 0.0f;
+  for (int k = 0; k < 3 * (int)kGradGroups; ++k) sens[k] = 0.0f;
   const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
   const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
   opbr::OpbrVertex base;
@@ -52,8 +55,6 @@ static __device__ __noinline__ void openpbr_vertex_grads(const DevRender& S, con
   float pdf0;
   opbr::eval_pdf(base, base, wi_l, f0, pdf0, false);
   const float f0c[3] = {f0.x, f0.y, f0.z};
-  const float wc[3] = {w.x, w.y, w.z};
-  const int slot[kGradGroups] = {0, 3, 4, 5, 6};
   for (int g = 0; g < (int)kGradGroups; ++g) {
     if (!(A.mask & (1u << g))) continue;
     const DevOpenPbr* lo = A.pert + ((size_t)opbr_index * kGradGroups + g) * 2;
@@ -62,18 +63,24 @@ static __device__ __noinline__ void openpbr_vertex_grads(const DevRender& S, con
     const V3 fp = perturbed_f(base, lo + 1, reuse, wo_l, wi_l, v.front);
     const V3 fm = perturbed_f(base, lo, reuse, wo_l, wi_l, v.front);
     const float df[3] = {fp.x - fm.x, fp.y - fm.y, fp.z - fm.z};
-    if (g == 0) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        if (f0c[c] > 0.0f && span[c] > 0.0f) out[c] = wc[c] * (df[c] / span[c]) / f0c[c];
-    } else if (span[0] > 0.0f) {
-      float acc = 0.0f;
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-        if (f0c[c] > 0.0f) acc += wc[c] * (df[c] / span[0]) / f0c[c];
-      out[slot[g]] = acc;
+    for (int c = 0; c < 3; ++c) {
+      const float sp = g == 0 ? span[c] : span[0];
+      if (f0c[c] > 0.0f && sp > 0.0f) sens[3 * g + c] = (df[c] / sp) / f0c[c];
     }
   }
+}
+
+// Gradient slots of a contribution w (per channel, dLoss/dL already applied)
+// with sensitivities sens: out[kGradParams] = base colour r, g, b, then one
+// slot per further group.
+__device__ __forceinline__ void grads_from_sens(const float* sens, V3 w, float* out) {
+  const float wc[3] = {w.x, w.y, w.z};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c] = wc[c] * sens[c];
+#pragma unroll
+  for (int g = 1; g < (int)kGradGroups; ++g) out[g + 2] = wc[0] * sens[3 * g] + wc[1] * sens[3 * g + 1] +
+                                                         wc[2] * sens[3 * g + 2];
 }
 
 // Adds each lane's kGradParams values to grad[key * kGradParams + k] in FP64:

@@ -10,16 +10,9 @@
 namespace tpt {
 
 constexpr uint32_t kBdptMaxDepth = kBdptMaxDepthApi;
-constexpr float kShadowTolerance = 1.0e-3f;
 
-// ---- material interface with transport modes (material/mod.rs:33-79) --------
-__device__ __forceinline__ V3 modified_eval(const Vertex& v, V3 wi, V3 f, bool importance) {
-  if (length_sq(f) == 0.0f) return V3{0.0f, 0.0f, 0.0f};
-  const V3 dir = importance ? v.wo : wi;
-  const float cos_geom = fabsf(dot(dir, v.ng));
-  if (cos_geom <= kGeomCosEps) return V3{0.0f, 0.0f, 0.0f};
-  return f * (fabsf(dot(dir, v.ns)) / cos_geom);
-}
+// ---- material interface with transport modes (material/mod.rs:33-79): eval
+// (material_eval) is in render.cuh --------------------------------------------
 __device__ __forceinline__ V3 modified_weight(const Vertex& v, V3 wi, V3 w, bool delta, bool importance) {
   if (!importance || delta || length_sq(w) == 0.0f) return w;
   const float cos_wo_geom = fabsf(dot(v.wo, v.ng)), cos_wo_sh = fabsf(dot(v.wo, v.ns));
@@ -30,39 +23,6 @@ __device__ __forceinline__ V3 modified_weight(const Vertex& v, V3 wi, V3 w, bool
 __device__ __forceinline__ float lambert_bsdf_pdf(V3 wo, V3 wi) {
   if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
   return fmaxf(wi.z, 0.0f) / kPiF;
-}
-
-// Material::eval (NormalizedLambert, OpenPbr; zero for the pure emitter)
-static __device__ __noinline__ V3 material_eval(const DevRender& S, const DevMaterialRec& m, const Vertex& v, V3 wi,
-                                               bool importance) {
-  if (m.kind == kDevLambert) {
-    if (dot(v.wo, v.ng) <= 0.0f || dot(wi, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
-    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
-    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
-    V3 f = V3{0.0f, 0.0f, 0.0f};
-    if (!(wo_l.z <= 0.0f || wi_l.z <= 0.0f)) f = V3{m.rho[0], m.rho[1], m.rho[2]} / kPiF;
-    return modified_eval(v, wi, f, importance);
-  }
-  if (m.kind == kDevOpenPbr) {
-    if (dot(v.wo, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
-    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
-    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
-    if (wo_l.z <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
-    const DevOpenPbr* mp = S.d.openpbr + m.openpbr;
-    opbr::OpbrVertex s;
-    opbr::init_vertex(s, mp, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
-    V3 f;
-    float pdf;
-    if (importance) {
-      opbr::OpbrVertex lay;
-      opbr::init_vertex(lay, mp, S.d.cec_e, S.d.dec_e, wi_l, v.front, fabsf(wo_l.z));
-      opbr::eval_pdf(s, lay, wi_l, f, pdf);
-    } else {
-      opbr::eval_pdf(s, s, wi_l, f, pdf);
-    }
-    return modified_eval(v, wi, f, importance);
-  }
-  return V3{0.0f, 0.0f, 0.0f};
 }
 
 // Material::pdf

@@ -252,47 +252,190 @@ __device__ __forceinline__ V3 offset_origin(V3 p, V3 ng, V3 dir) {
   return p + 1.0e-4f * n;
 }
 
-// direct_light_mis_contribution (integrator/mis.rs:145-210) for a diffuse
-// vertex, up to the visibility test: returns false when the contribution is
-// zero whatever the visibility; otherwise `contrib` (radiance * f * cos * mis /
-// pdf) counts iff the shadow ray (so, li.wi) first hits triangle (inst, tri).
+// ---- material eval with transport modes (material/mod.rs:33-79) -------------
+__device__ __forceinline__ V3 modified_eval(const Vertex& v, V3 wi, V3 f, bool importance) {
+  if (length_sq(f) == 0.0f) return V3{0.0f, 0.0f, 0.0f};
+  const V3 dir = importance ? v.wo : wi;
+  const float cos_geom = fabsf(dot(dir, v.ng));
+  if (cos_geom <= kGeomCosEps) return V3{0.0f, 0.0f, 0.0f};
+  return f * (fabsf(dot(dir, v.ns)) / cos_geom);
+}
+
+// Material::eval (NormalizedLambert, OpenPbr; zero for the pure emitter)
+static __device__ __noinline__ V3 material_eval(const DevRender& S, const DevMaterialRec& m, const Vertex& v, V3 wi,
+                                               bool importance) {
+  if (m.kind == kDevLambert) {
+    if (dot(v.wo, v.ng) <= 0.0f || dot(wi, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
+    V3 f = V3{0.0f, 0.0f, 0.0f};
+    if (!(wo_l.z <= 0.0f || wi_l.z <= 0.0f)) f = V3{m.rho[0], m.rho[1], m.rho[2]} / kPiF;
+    return modified_eval(v, wi, f, importance);
+  }
+  if (m.kind == kDevOpenPbr) {
+    if (dot(v.wo, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
+    if (wo_l.z <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const DevOpenPbr* mp = S.d.openpbr + m.openpbr;
+    opbr::OpbrVertex s;
+    opbr::init_vertex(s, mp, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    V3 f;
+    float pdf;
+    if (importance) {
+      opbr::OpbrVertex lay;
+      opbr::init_vertex(lay, mp, S.d.cec_e, S.d.dec_e, wi_l, v.front, fabsf(wo_l.z));
+      opbr::eval_pdf(s, lay, wi_l, f, pdf);
+    } else {
+      opbr::eval_pdf(s, s, wi_l, f, pdf);
+    }
+    return modified_eval(v, wi, f, importance);
+  }
+  return V3{0.0f, 0.0f, 0.0f};
+}
+
+// ---- lights that are not emissive triangles (light/{point,spot,directional}.rs)
+constexpr float kShadowTolerance = 1.0e-3f;  // integrator/mod.rs:50
+
+// point::sample_li (light/point.rs:32-50): Li = color * P / (4 pi r^2)
+__device__ __forceinline__ bool sample_li_point(const DevPointLight& l, V3 p_ref, LightSample& out) {
+  const V3 to_light = V3{l.position[0], l.position[1], l.position[2]} - p_ref;
+  const float d2 = length_sq(to_light);
+  if (d2 <= 0.0f) return false;
+  const float dist = sqrtf(d2);
+  out.wi = to_light / dist;
+  out.radiance = V3{l.color[0], l.color[1], l.color[2]} * (l.intensity / (4.0f * kPiF * d2));
+  out.pdf = 1.0f;
+  out.distance = dist;
+  return true;
+}
+
+// spot::sample_li (light/spot.rs:51-76) with smoothstep (math/mod.rs:180-183)
+__device__ __forceinline__ bool sample_li_spot(const DevSpotLight& l, V3 p_ref, LightSample& out) {
+  const V3 to_light = V3{l.position[0], l.position[1], l.position[2]} - p_ref;
+  const float d2 = length_sq(to_light);
+  if (d2 <= 0.0f) return false;
+  const float dist = sqrtf(d2);
+  const V3 wi = to_light / dist;
+  const float cos_theta = dot(-wi, V3{l.direction[0], l.direction[1], l.direction[2]});
+  const float t = clampf((cos_theta - l.cos_total_width) / (l.cos_falloff_start - l.cos_total_width), 0.0f, 1.0f);
+  const float falloff = t * t * (3.0f - 2.0f * t);
+  if (falloff <= 0.0f) return false;
+  out.wi = wi;
+  out.radiance = V3{l.color[0], l.color[1], l.color[2]} * (l.intensity * falloff / (2.0f * kTauF * d2));
+  out.pdf = 1.0f;
+  out.distance = dist;
+  return true;
+}
+
+// LightSampler::sample_category (light/mod.rs:197-212): the entry whose CDF
+// interval holds u.
+__device__ __forceinline__ uint32_t sample_category(const DevRenderData& d, float u, float& pmf) {
+  u = clampf(u, 0.0f, 1.0f);
+  uint32_t n = 0;  // entries of cdf[0..num_cat] that are <= u
+  for (uint32_t k = 0; k <= d.num_cat; ++k)
+    if (__ldg(d.cat_cdf + k) <= u) n = k + 1;
+  const uint32_t idx = min(n == 0 ? 0u : n - 1, d.num_cat - 1);
+  pmf = __ldg(d.cat_pmf + idx);
+  return __ldg(d.cat_kind + idx);
+}
+
+// direct_light_mis_contribution (integrator/mis.rs:145-210) up to the
+// visibility test: returns false when the contribution is zero whatever the
+// visibility; otherwise `contrib` (radiance * f * cos [* mis] / pdf) counts iff
+// the shadow ray (so, wi) first hits triangle (inst, tri) for an area light,
+// hits nothing or nothing nearer than dist * (1 - 1e-3) for a point or spot
+// light (inst = 0xFFFFFFFF, finite dist), or hits nothing for a directional
+// light (inst = 0xFFFFFFFF, dist = inf) -- unoccluded_ray, integrator/mod.rs:
+// 239-265.  The light tree is only queried by the diffuse material (the only
+// material in scope with a light-tree query); directional lights serve every
+// scattering material.
+// Li of a delta light, kept out of line so the area-light path of the shade
+// kernels does not carry its registers: kind 0 point light, 1 spot light,
+// 2 directional light (index into the scene's arrays of that kind).
+static __device__ __noinline__ bool sample_li_delta(const DevRenderData& d, uint32_t kind, uint32_t index, V3 p_ref,
+                                                    LightSample& li) {
+  if (kind == 0) return sample_li_point(d.points[index], p_ref, li);
+  if (kind == 1) return sample_li_spot(d.spots[index], p_ref, li);
+  // directional::sample_li (light/directional.rs:33-42)
+  const DevDirLight& dl = d.dirs[index];
+  li.radiance = V3{dl.color[0] * dl.intensity, dl.color[1] * dl.intensity, dl.color[2] * dl.intensity};
+  li.wi = -V3{dl.direction[0], dl.direction[1], dl.direction[2]};
+  li.pdf = 1.0f;
+  li.distance = __int_as_float(0x7f800000);
+  return true;
+}
+
 struct DirectPrep {
   V3 contrib, so, wi;
   uint32_t inst, tri;
+  float dist;
 };
 
 __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
-                                               float u_tree, float us0, float us1, DirectPrep& out) {
-  if (!S.d.has_tree) return false;              // LightSampler::sample_category: no category
-  if (m.kind != kDevLambert) return false;      // only the diffuse material builds a light-tree query
-  TreeQuery q;
-  q.rho = luminance(V3{m.rho[0], m.rho[1], m.rho[2]});
-  if (q.rho <= 0.0f) return false;
-  q.p = v.p;
-  q.n = v.ns;
-  float leaf_pmf;
-  const uint32_t leaf = sample_light_tree(S.d.ltree, S.d.ltree_root, q, u_tree, leaf_pmf);
-  if (leaf == 0xFFFFFFFFu) return false;
+                                               float u_cat, float u_tree, float us0, float us1, DirectPrep& out) {
+  if (S.d.num_cat == 0) return false;  // LightSampler::sample_category: no category
+  float cat_pmf;
+  const uint32_t cat = sample_category(S.d, u_cat, cat_pmf);
   LightSample li;
-  if (!sample_li_triangle(S, __ldg(&S.d.ltree[leaf].leaf_instance), __ldg(&S.d.ltree[leaf].leaf_triangle), v.p, us0,
-                          us1, li))
-    return false;
-  const float sel_pmf = S.d.tree_cat_pmf * leaf_pmf;
-  if (li.pdf <= 0.0f || sel_pmf <= 0.0f) return false;
-  const V3 f = lambert_eval(m, v, li.wi);
+  bool delta = true;
+  float sel;
+  out.inst = 0xFFFFFFFFu;
+  out.tri = 0xFFFFFFFFu;
+  if (cat == kCatTree) {
+    if (m.kind != kDevLambert) return false;  // build_query: only the diffuse material builds one
+    TreeQuery q;
+    q.rho = luminance(V3{m.rho[0], m.rho[1], m.rho[2]});
+    if (q.rho <= 0.0f) return false;
+    q.p = v.p;
+    q.n = v.ns;
+    float leaf_pmf;
+    const uint32_t leaf = sample_light_tree(S.d.ltree, S.d.ltree_root, q, u_tree, leaf_pmf);
+    if (leaf == 0xFFFFFFFFu) return false;
+    const uint32_t li_inst = __ldg(&S.d.ltree[leaf].leaf_instance), li_tri = __ldg(&S.d.ltree[leaf].leaf_triangle);
+    if (li_inst == kLeafPointDev || li_inst == kLeafSpotDev) {
+      if (!sample_li_delta(S.d, li_inst == kLeafPointDev ? 0u : 1u, li_tri, v.p, li)) return false;
+    } else {
+      if (!sample_li_triangle(S, li_inst, li_tri, v.p, us0, us1, li)) return false;
+      delta = false;
+      out.inst = li.inst;
+      out.tri = li.tri;
+    }
+    sel = cat_pmf * leaf_pmf;
+  } else {
+    if (!sample_li_delta(S.d, 2u, cat - 1, v.p, li)) return false;
+    sel = cat_pmf;
+  }
+  if (li.pdf <= 0.0f || sel <= 0.0f) return false;
+  V3 f;
+  float bsdf_pdf = 0.0f;
+  if (delta) {
+    f = m.kind == kDevLambert ? lambert_eval(m, v, li.wi) : material_eval(S, m, v, li.wi, false);
+  } else {
+    f = lambert_eval(m, v, li.wi);
+    if (length_sq(f) == 0.0f) return false;
+    bsdf_pdf = lambert_pdf(v, li.wi);
+  }
   if (length_sq(f) == 0.0f) return false;
-  const float bsdf_pdf = lambert_pdf(v, li.wi);
   const float cos_surface = fabsf(dot(v.ng, li.wi));
   if (cos_surface <= 0.0f) return false;
-  const float pdf_total = sel_pmf * li.pdf;
+  const float pdf_total = sel * li.pdf;
   if (pdf_total <= 0.0f) return false;
-  const float mis = balance_heuristic(pdf_total, bsdf_pdf);
-  out.contrib = li.radiance * f * (cos_surface * mis / pdf_total);
+  out.contrib = delta ? li.radiance * f * (cos_surface / pdf_total)
+                      : li.radiance * f * (cos_surface * balance_heuristic(pdf_total, bsdf_pdf) / pdf_total);
   out.so = offset_origin(v.p, v.ng, li.wi);  // spawn_ray of unoccluded_ray (integrator/mod.rs:239-265)
   out.wi = li.wi;
-  out.inst = li.inst;
-  out.tri = li.tri;
+  out.dist = li.distance;
   return true;
+}
+
+// unoccluded_ray's decision from the shadow ray's closest hit (tri < 0: none)
+__device__ __forceinline__ bool shadow_visible(int32_t tri, int32_t inst, float t, uint32_t tgt_inst, uint32_t tgt_tri,
+                                               float dist) {
+  if (tri < 0) return true;
+  if (tgt_inst != 0xFFFFFFFFu) return (uint32_t)inst == tgt_inst && (uint32_t)tri == tgt_tri;
+  if (isinf(dist)) return false;
+  return t >= dist * (1.0f - kShadowTolerance);
 }
 
 // pdf_for_triangle_hit (light/mod.rs:416-437) for a BSDF-sampled emitter hit

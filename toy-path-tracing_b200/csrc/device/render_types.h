@@ -107,6 +107,23 @@ struct alignas(16) DevAreaLight {
 };
 static_assert(sizeof(DevAreaLight) == 32, "area light record");
 
+// PointLight / SpotLight / DirectionalLight (light/{point,spot,directional}.rs)
+// as the constructors store them (spot and directional directions normalised,
+// spot cone angles as cosines).
+struct DevPointLight {
+  float position[3], color[3], intensity, pad;
+};
+struct DevSpotLight {
+  float position[3], direction[3], color[3], intensity, cos_total_width, cos_falloff_start;
+};
+struct DevDirLight {
+  float direction[3], color[3], intensity, pad;
+};
+constexpr uint32_t kLeafPointDev = 0xFFFFFFFEu;  // light-tree leaf of a point light
+constexpr uint32_t kLeafSpotDev = 0xFFFFFFFDu;   // light-tree leaf of a spot light
+constexpr uint32_t kCatTree = 0u;                // light-sampler category: the light tree;
+                                                 // 1 + i: directional light i
+
 struct DevMeshInfo {
   uint32_t vtx_base, idx_base, num_tris, flags;  // flags bit 0: normals, bit 1: uvs
 };
@@ -132,6 +149,16 @@ struct DevRenderData {
   uint32_t has_tree;
   float tree_cat_pmf;  // LightSampler pmf of the Tree category
   uint32_t num_materials;
+  // lights that are not emissive triangles, and the light sampler's category
+  // CDF (LightSampler::build_from_scene, light/mod.rs:134-188)
+  const DevPointLight* points;
+  const DevSpotLight* spots;
+  const DevDirLight* dirs;
+  const float* cat_cdf;      // num_cat + 1 entries, normalised
+  const float* cat_pmf;      // num_cat
+  const uint32_t* cat_kind;  // kCatTree or 1 + directional index
+  uint32_t num_cat;
+  uint32_t pad2;
 };
 
 // Camera constants computed on the host (scene/camera.rs:21-39).
@@ -164,6 +191,12 @@ struct DevAdjoint {
   double* grad;            // [material][kGradParams]
   float scale;             // exposure / spp: d image / d sample radiance
   uint32_t mask;           // parameter groups to differentiate (bit g = group g)
+  // light samples at OpenPBR vertices (directional lights), per shadow-queue
+  // entry: the gradient change if the shadow ray is unoccluded (kGradParams
+  // planes of the wavefront capacity) and its material (0xFFFFFFFF: none).
+  // NULL when the scene has no such light samples.
+  float* s_grad;
+  uint32_t* s_gkey;
 };
 
 // BDPT wavefront state (kernels/bdpt_wavefront.cu) for up to sample_capacity
@@ -220,7 +253,8 @@ struct WfBuffers {
   uint32_t* s_slot;
   float* s_ray;       // 7 planes
   float* s_contrib;   // 3 planes
-  uint32_t* s_target; // 2 planes: instance, triangle
+  uint32_t* s_target; // 2 planes: instance, triangle (0xFFFFFFFF: a point, spot or directional light)
+  float* s_dist;      // distance to a point or spot light (inf: directional)
   int32_t* s_tri;
   int32_t* s_inst;
   float* s_t;

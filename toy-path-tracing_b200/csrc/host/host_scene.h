@@ -45,6 +45,15 @@ struct HostInstance {
   const float* normal_to_world;  // 9, column-major
 };
 
+// PointLight::new / SpotLight::new (light/point.rs, light/spot.rs) as stored:
+// spot direction normalised, cone angles as cosines.
+struct HostPointLight {
+  float position[3], color[3], intensity;
+};
+struct HostSpotLight {
+  float position[3], direction[3], color[3], intensity, cos_total_width, cos_falloff_start;
+};
+
 struct HostSceneView {
   const HostMesh* meshes;
   uint32_t num_meshes;
@@ -52,7 +61,14 @@ struct HostSceneView {
   uint32_t num_instances;
   const HostMaterial* materials;
   uint32_t num_materials;
+  const HostPointLight* points = nullptr;
+  uint32_t num_points = 0;
+  const HostSpotLight* spots = nullptr;
+  uint32_t num_spots = 0;
 };
+
+constexpr uint32_t kLeafPoint = 0xFFFFFFFEu;  // tree leaf of a point light (leaf_triangle = index)
+constexpr uint32_t kLeafSpot = 0xFFFFFFFDu;   // tree leaf of a spot light
 
 // Same bytes as `tpt_light_node` in include/tpt.h (64 bytes).
 struct LightNodeHost {
@@ -84,6 +100,9 @@ inline void transform_point_glam(const float* m, const float* p, float* out) {
 }
 
 bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out);
+// SpotLight::new (light/spot.rs:32-48) from the C ABI's description.
+void make_spot_light(const float* position, const float* direction, const float* color, float intensity,
+                     float total_width_rad, float falloff_start_rad, HostSpotLight* out);
 
 struct HostAreaLight {
   uint32_t inst, tri;

@@ -2,7 +2,7 @@
 //
 // Restates crates/renderer/src/light_tree/builder.rs:58-765 and the cluster
 // algebra of crates/renderer/src/math/sg.rs:203-214, 325-346 for emissive
-// triangles (the renderer's point and spot lights are out of scope here).
+// triangles, point lights and spot lights.
 // Node order is the reference's: an interior node is reserved before its left
 // then right subtree (pre-order).  `sort_unstable_by` on centroids
 // (builder.rs:486-490, 758-762) has no defined order for equal keys; here
@@ -41,6 +41,8 @@ inline V3 vmin(V3 a, V3 b) { return {std::fmin(a.x, b.x), std::fmin(a.y, b.y), s
 inline V3 vmax(V3 a, V3 b) { return {std::fmax(a.x, b.x), std::fmax(a.y, b.y), std::fmax(a.z, b.z)}; }
 inline V3 vabs(V3 a) { return {std::fabs(a.x), std::fabs(a.y), std::fabs(a.z)}; }
 inline float comp(V3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+// sg.rs:314-316
+inline float luminance(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
 struct Box {
   V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
@@ -281,6 +283,25 @@ class TreeBuilder {
 
 }  // namespace
 
+void make_spot_light(const float* position, const float* direction, const float* color, float intensity,
+                     float total_width_rad, float falloff_start_rad, HostSpotLight* out) {
+  const float pi = 3.14159274101257324f;  // f32::consts::PI
+  const float total_width = std::fmin(std::fmax(total_width_rad, 0.0f), pi);
+  const float falloff_start = std::fmin(std::fmax(falloff_start_rad, 0.0f), total_width);
+  const V3 d{direction[0], direction[1], direction[2]};
+  const V3 n = mulv(d, 1.0f / length(d));  // glam normalize
+  for (int k = 0; k < 3; ++k) {
+    out->position[k] = position[k];
+    out->color[k] = color[k];
+  }
+  out->direction[0] = n.x;
+  out->direction[1] = n.y;
+  out->direction[2] = n.z;
+  out->intensity = intensity;
+  out->cos_total_width = std::cos(total_width);
+  out->cos_falloff_start = std::cos(falloff_start);
+}
+
 // Scene::register_area_light_triangles (scene/mod.rs:649-683): the area-light
 // registry BDPT samples its light subpaths from.
 void register_area_lights(const HostSceneView& s, std::vector<HostAreaLight>* out, float* weight_sum) {
@@ -359,6 +380,52 @@ bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out) {
       L.order = (uint32_t)leaves.size();
       leaves.push_back(L);
     }
+  }
+  // point_leaf / spot_leaf (builder.rs:189-242), kept when their flux is > 0
+  for (uint32_t i = 0; i < s.num_points; ++i) {
+    const HostPointLight& pl = s.points[i];
+    const V3 c{pl.color[0], pl.color[1], pl.color[2]};
+    const float phi = std::fmax(luminance(c) * pl.intensity, 0.0f);
+    if (!(phi > 0.0f)) continue;
+    Leaf L;
+    L.inst = kLeafPoint;
+    L.tri = i;
+    L.flux = phi;
+    L.mu = V3{pl.position[0], pl.position[1], pl.position[2]};
+    L.sigma_s2 = 0.0f;
+    L.nu_bar = V3{0, 0, 0};
+    L.aabb.lo = L.mu;
+    L.aabb.hi = L.mu;
+    L.radius = 0.0f;
+    L.cone = Cone{V3{0, 0, 1}, kPi, 0.0f, true};  // undirected: theta_o = pi
+    L.centroid = L.mu;
+    L.area = 0.0f;
+    L.order = (uint32_t)leaves.size();
+    leaves.push_back(L);
+  }
+  for (uint32_t i = 0; i < s.num_spots; ++i) {
+    const HostSpotLight& sl = s.spots[i];
+    const V3 c{sl.color[0], sl.color[1], sl.color[2]};
+    const float phi = std::fmax(luminance(c) * sl.intensity, 0.0f);
+    if (!(phi > 0.0f)) continue;
+    const V3 dir{sl.direction[0], sl.direction[1], sl.direction[2]};
+    const float cos_total = std::fmin(std::fmax(sl.cos_total_width, -1.0f), 1.0f);
+    const float mean_len = std::fmin(std::fmax((1.0f + cos_total) * 0.5f, 0.0f), 1.0f);
+    Leaf L;
+    L.inst = kLeafSpot;
+    L.tri = i;
+    L.flux = phi;
+    L.mu = V3{sl.position[0], sl.position[1], sl.position[2]};
+    L.sigma_s2 = 0.0f;
+    L.nu_bar = mul(mean_len, dir);
+    L.aabb.lo = L.mu;
+    L.aabb.hi = L.mu;
+    L.radius = 0.0f;
+    L.cone = Cone{dir, 0.0f, std::acos(cos_total), true};
+    L.centroid = L.mu;
+    L.area = 0.0f;
+    L.order = (uint32_t)leaves.size();
+    leaves.push_back(L);
   }
   if (leaves.empty()) return false;
   out->nodes.reserve(2 * leaves.size());

@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(D
   bool bounce_pending = false;
   V3 L, beta, contrib;         // contrib: NEE radiance counted if the shadow ray is clear
   uint32_t tgt_inst = 0, tgt_tri = 0;
+  float tgt_dist = 0.0f;
   V3 prev_p, prev_ns;          // previous vertex (emission MIS after a BSDF sample)
   float prev_pdf = 0.0f;
   uint32_t prev_mat = 0;       // material index, bit 31: delta sample
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(D
     bool done = false;
     if (kind == kRayShadow) {
       // unoccluded_ray (integrator/mod.rs:239-265)
-      if (h.tri < 0 || ((uint32_t)h.inst == tgt_inst && (uint32_t)h.tri == tgt_tri)) L = L + contrib;
+      if (shadow_visible(h.tri, h.inst, h.t, tgt_inst, tgt_tri, tgt_dist)) L = L + contrib;
       if (bounce_pending) {
         ro = bo;
         rd = bd;
@@ -123,12 +124,14 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(D
         float us0, us1;
         ps.sample_2d(vertex_dim(depth, kOffSurface), us0, us1);
         const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
+        const float u_cat = S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(depth, kOffCategory)) : 0.0f;
         DirectPrep dp;
-        const bool nee = prepare_direct(S, m, v, u_tree, us0, us1, dp);
+        const bool nee = prepare_direct(S, m, v, u_cat, u_tree, us0, us1, dp);
         if (nee) {
           contrib = beta * dp.contrib;
           tgt_inst = dp.inst;
           tgt_tri = dp.tri;
+          tgt_dist = dp.dist;
         }
         bool alive = false;
         BsdfSampleOut s;

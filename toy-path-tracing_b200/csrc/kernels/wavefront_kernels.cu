@@ -26,6 +26,11 @@
 // generate starts R at the path's radiance from the forward pass, shade and
 // resolve subtract what each vertex collects, and shade adds, at every rough
 // OpenPBR vertex, dLoss/dL * R * (df/dtheta) / f to the per-material gradients.
+// A light sample C at an OpenPBR vertex (directional lights) is only known to
+// count once its shadow ray is resolved, while shade has already used R with C
+// still in it; shade therefore queues, with the shadow ray, the change
+// dLoss/dL * C * [(df/dtheta) / f at the light direction - the same at the
+// sampled direction], which resolve adds when the ray is unoccluded.
 #include "../api/internal.h"
 #include "../device/adjoint.cuh"
 #include "../device/render.cuh"
@@ -118,8 +123,8 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
   if (j >= B.counts[cur]) return;
   const uint64_t first_path = (uint64_t)B.counts[4] | ((uint64_t)B.counts[5] << 32);
   const float sgn = ADJ ? -1.0f : 1.0f;  // the adjoint takes collected radiance off R
-  uint32_t grad_key = 0xFFFFFFFFu;
-  float grad_v[ADJ ? kGradParams : 1];
+  uint32_t grad_key = 0xFFFFFFFFu, s_key = 0xFFFFFFFFu;
+  float grad_v[ADJ ? kGradParams : 1], s_grad[ADJ ? kGradParams : 1];
   const uint32_t C = B.capacity;
   const uint32_t slot = B.q_slot[cur][j];
   const uint32_t jb = BATCH ? B.job[slot] : 0u;
@@ -164,17 +169,27 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
     }
     if (d < P.max_depth && m.kind != kDevEmissive) {
       const uint64_t path = first_path + slot - (BATCH ? jobs[jb].path_base : 0ull);
+      V3 dl = V3{0.0f, 0.0f, 0.0f};
+      if (ADJ) {
+        const uint32_t pixel = (uint32_t)(path / P.spp);
+        dl = V3{A.d_image[3 * (uint64_t)pixel], A.d_image[3 * (uint64_t)pixel + 1],
+                A.d_image[3 * (uint64_t)pixel + 2]} * A.scale;
+      }
       const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
       PathSamplerDev ps;
       ps.init(pixel % P.width, pixel / P.width, sample, P.log2_spp, P.n_base4_digits);
       float us0, us1;
       ps.sample_2d(vertex_dim(d, kOffSurface), us0, us1);
       const float u_tree = ps.sample_1d(vertex_dim(d, kOffTree));
-      if (prepare_direct(S, m, v, u_tree, us0, us1, dp)) {
+      // one light-sampler category takes any u: skip drawing it
+      const float u_cat = S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(d, kOffCategory)) : 0.0f;
+      if (prepare_direct(S, m, v, u_cat, u_tree, us0, us1, dp)) {
         dp.contrib = beta * dp.contrib;
         push_shadow = true;
       }
       BsdfSampleOut s;
+      bool sampled_grads = false;
+      float sens_s[ADJ ? 3 * kGradGroups : 1];
       if (material_sample(S, m, v, ps, d, s)) {
         beta = beta * s.weight;
         bool alive = true;
@@ -186,12 +201,12 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
         if (alive) {
           push_next = true;
           if (ADJ && m.kind == kDevOpenPbr && !s.delta) {
-            // OpenPBR vertices do no NEE, so R (= L here) is what the path collects after this vertex
-            const uint32_t pixel = (uint32_t)(path / P.spp);
-            const V3 dl = V3{A.d_image[3 * (uint64_t)pixel], A.d_image[3 * (uint64_t)pixel + 1],
-                             A.d_image[3 * (uint64_t)pixel + 2]} * A.scale;
-            openpbr_vertex_grads(S, A, m.openpbr, v, s.wi, dl * L, grad_v);
+            // R (= L here) still holds this vertex's light sample, if any:
+            // resolve corrects for it once the shadow ray is known unoccluded
+            openpbr_vertex_sens(S, A, m.openpbr, v, s.wi, sens_s);
+            grads_from_sens(sens_s, dl * L, grad_v);
             grad_key = mi;
+            sampled_grads = true;
           }
           next_o = offset_origin(v.p, v.ng, s.wi);
           next_d = s.wi;
@@ -204,6 +219,21 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
           B.prev[6 * C + slot] = s.pdf;
           B.prev_mat[slot] = mi | (s.delta ? 0x80000000u : 0u);
           B.depth[slot] = d + 1;
+        }
+      }
+      if (ADJ && push_shadow && A.s_gkey) {
+        s_key = 0xFFFFFFFFu;
+        if (m.kind == kDevOpenPbr) {
+          float sens_l[3 * kGradGroups], t[kGradParams];
+          openpbr_vertex_sens(S, A, m.openpbr, v, dp.wi, sens_l);
+          const V3 w = dl * dp.contrib;
+          grads_from_sens(sens_l, w, s_grad);
+          if (sampled_grads) {
+            grads_from_sens(sens_s, w, t);
+#pragma unroll
+            for (int k = 0; k < (int)kGradParams; ++k) s_grad[k] -= t[k];
+          }
+          s_key = mi;
         }
       }
     }
@@ -242,28 +272,46 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
     if (BATCH) B.s_job[qs] = jb;
     B.s_target[qs] = dp.inst;
     B.s_target[C + qs] = dp.tri;
+    B.s_dist[qs] = dp.dist;
     B.s_contrib[qs] = dp.contrib.x;
     B.s_contrib[C + qs] = dp.contrib.y;
     B.s_contrib[2 * C + qs] = dp.contrib.z;
+    if (ADJ && A.s_gkey) {
+      A.s_gkey[qs] = s_key;
+      if (s_key != 0xFFFFFFFFu) {
+#pragma unroll
+        for (int k = 0; k < (int)kGradParams; ++k) A.s_grad[(size_t)k * C + qs] = s_grad[k];
+      }
+    }
   }
   if (ADJ) warp_accumulate_grads(A.grad, grad_key, grad_v, grad_sh + (threadIdx.x & ~31u) * kGradParams);
 }
 
-// unoccluded_ray (integrator/mod.rs:239-265): visible when nothing is hit or the
-// first hit is the sampled emitter triangle.
+// unoccluded_ray (integrator/mod.rs:239-265): visible when nothing is hit, the
+// first hit is the sampled emitter triangle, or (point and spot lights) the
+// first hit lies beyond the light.
 template <bool ADJ>
-__global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B) {
+__global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B, DevAdjoint A) {
+  __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[2]) return;
   const uint32_t C = B.capacity;
-  const int32_t tri = B.s_tri[j];
-  const bool visible = tri < 0 || ((uint32_t)B.s_inst[j] == B.s_target[j] && (uint32_t)tri == B.s_target[C + j]);
-  if (!visible) return;
-  const uint32_t slot = B.s_slot[j];
-  const float sgn = ADJ ? -1.0f : 1.0f;
-  B.L[slot] = B.L[slot] + sgn * B.s_contrib[j];
-  B.L[C + slot] = B.L[C + slot] + sgn * B.s_contrib[C + j];
-  B.L[2 * C + slot] = B.L[2 * C + slot] + sgn * B.s_contrib[2 * C + j];
+  const bool visible =
+      shadow_visible(B.s_tri[j], B.s_inst[j], B.s_t[j], B.s_target[j], B.s_target[C + j], B.s_dist[j]);
+  if (visible) {
+    const uint32_t slot = B.s_slot[j];
+    const float sgn = ADJ ? -1.0f : 1.0f;
+    B.L[slot] = B.L[slot] + sgn * B.s_contrib[j];
+    B.L[C + slot] = B.L[C + slot] + sgn * B.s_contrib[C + j];
+    B.L[2 * C + slot] = B.L[2 * C + slot] + sgn * B.s_contrib[2 * C + j];
+  }
+  if (ADJ && A.s_gkey) {
+    const uint32_t key = visible ? A.s_gkey[j] : 0xFFFFFFFFu;
+    float vals[kGradParams];
+#pragma unroll
+    for (int k = 0; k < (int)kGradParams; ++k) vals[k] = key != 0xFFFFFFFFu ? A.s_grad[(size_t)k * C + j] : 0.0f;
+    warp_accumulate_grads(A.grad, key, vals, grad_sh + (threadIdx.x & ~31u) * kGradParams);
+  }
 }
 
 __global__ void __launch_bounds__(kWfBlock) wf_finalize(WfBuffers B, uint32_t n_paths, float* samples) {
@@ -321,9 +369,9 @@ cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cu
   return cudaGetLastError();
 }
 
-cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, bool adjoint) {
-  if (adjoint) wf_resolve<true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(B);
-  else wf_resolve<false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(B);
+cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, const DevAdjoint* A) {
+  if (A) wf_resolve<true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(B, *A);
+  else wf_resolve<false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(B, DevAdjoint{});
   return cudaGetLastError();
 }
 

@@ -133,6 +133,22 @@ class LightTreeView(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("num_nodes", C.c_uint64), ("root", C.c_uint32)]
 
 
+class PointLightDesc(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("color", C.c_float * 3), ("intensity", C.c_float)]
+
+
+class SpotLightDesc(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("direction", C.c_float * 3), ("color", C.c_float * 3),
+                ("intensity", C.c_float), ("total_width", C.c_float), ("falloff_start", C.c_float)]
+
+
+class DirectionalLightDesc(C.Structure):
+    _fields_ = [("direction", C.c_float * 3), ("color", C.c_float * 3), ("intensity", C.c_float)]
+
+
+LIGHT_LEAF_POINT, LIGHT_LEAF_SPOT = 0xFFFFFFFE, 0xFFFFFFFD  # tree leaf codes (tpt.h)
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("meshes", C.POINTER(MeshDesc)),
@@ -143,7 +159,39 @@ class SceneDesc(C.Structure):
         ("materials", C.POINTER(MaterialDesc)),
         ("num_materials", C.c_uint32),
         ("light_tree", LightTreeView),
+        ("point_lights", C.POINTER(PointLightDesc)),
+        ("num_point_lights", C.c_uint32),
+        ("spot_lights", C.POINTER(SpotLightDesc)),
+        ("num_spot_lights", C.c_uint32),
+        ("directional_lights", C.POINTER(DirectionalLightDesc)),
+        ("num_directional_lights", C.c_uint32),
     ]
+
+
+def _f3(v):
+    return [float(np.float32(x)) for x in np.asarray(v, np.float32).reshape(3)]
+
+
+def light_descs(lights: dict):
+    """C light arrays from a scene dict's "point_lights", "spot_lights" and
+    "directional_lights" lists (dicts: position, direction, color, intensity,
+    total_width / falloff_start in radians)."""
+    pts = lights.get("point_lights", [])
+    spots = lights.get("spot_lights", [])
+    dirs = lights.get("directional_lights", [])
+    pa = (PointLightDesc * max(1, len(pts)))()
+    for i, l in enumerate(pts):
+        pa[i] = PointLightDesc(tuple(_f3(l["position"])), tuple(_f3(l["color"])), float(np.float32(l["intensity"])))
+    sa = (SpotLightDesc * max(1, len(spots)))()
+    for i, l in enumerate(spots):
+        sa[i] = SpotLightDesc(tuple(_f3(l["position"])), tuple(_f3(l["direction"])), tuple(_f3(l["color"])),
+                              float(np.float32(l["intensity"])), float(np.float32(l["total_width"])),
+                              float(np.float32(l["falloff_start"])))
+    da = (DirectionalLightDesc * max(1, len(dirs)))()
+    for i, l in enumerate(dirs):
+        da[i] = DirectionalLightDesc(tuple(_f3(l["direction"])), tuple(_f3(l["color"])),
+                                     float(np.float32(l["intensity"])))
+    return (pa, len(pts)), (sa, len(spots)), (da, len(dirs))
 
 
 class CameraDesc(C.Structure):
@@ -394,8 +442,9 @@ def _view(q):
     )
 
 
-def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None):
-    """Build a `tpt_scene_desc` (and the list of arrays it points into)."""
+def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None, lights=None):
+    """Build a `tpt_scene_desc` (and the list of arrays it points into).
+    lights: dict with optional "point_lights", "spot_lights", "directional_lights"."""
     keep = []
     md = (MeshDesc * max(1, len(meshes)))()
     for i, m in enumerate(meshes):
@@ -444,14 +493,16 @@ def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None):
         nodes, root = np.ascontiguousarray(light_tree[0], LIGHT_NODE_DTYPE), int(light_tree[1])
         keep.append(nodes)
         ltv = LightTreeView(nodes.ctypes.data, len(nodes), root)
-    keep += [md, idesc, mdesc]
-    desc = SceneDesc(md, len(meshes), idesc, len(instances), _view(tlas), mdesc, len(materials), ltv)
+    (pa, npts), (sa, nsp), (da, ndir) = light_descs(lights or {})
+    keep += [md, idesc, mdesc, pa, sa, da]
+    desc = SceneDesc(md, len(meshes), idesc, len(instances), _view(tlas), mdesc, len(materials), ltv,
+                     pa, npts, sa, nsp, da, ndir)
     return desc, keep
 
 
 def build_light_tree(scene: dict):
     """Host light-tree builder (`tpt_light_tree_build`): (nodes[LIGHT_NODE_DTYPE], root)."""
-    desc, keep = scene_desc(scene["meshes"], scene["instances"], materials=scene["materials"])
+    desc, keep = scene_desc(scene["meshes"], scene["instances"], materials=scene["materials"], lights=scene)
     h = C.c_void_p()
     _check(lib().tpt_light_tree_build(C.byref(desc), C.byref(h)))
     try:
@@ -470,11 +521,12 @@ class Scene:
     meshes: list of dicts with positions [V,3], indices [3T], optional normals,
     uvs and a pre-built qbvh (nodes, prims).  instances: list of dicts with
     mesh, material, local_to_world, world_to_local (4x4 column-major) and
-    normal_to_world (3x3)."""
+    normal_to_world (3x3).  lights: a dict (e.g. the scene dict) with optional
+    "point_lights", "spot_lights" and "directional_lights" lists."""
 
-    def __init__(self, ctx: Context, meshes, instances, tlas=None, materials=None, light_tree=None):
+    def __init__(self, ctx: Context, meshes, instances, tlas=None, materials=None, light_tree=None, lights=None):
         self.ctx = ctx
-        desc, keep = scene_desc(meshes, instances, tlas, materials, light_tree)
+        desc, keep = scene_desc(meshes, instances, tlas, materials, light_tree, lights)
         h = C.c_void_p()
         _check(lib().tpt_scene_upload(ctx.h, C.byref(desc), C.byref(h)), ctx)
         self.h = h

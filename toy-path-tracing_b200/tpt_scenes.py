@@ -201,6 +201,26 @@ def cornell_box(seed: int = 1, material: int = OPENPBR, light_strength: float = 
             "angles": (float(a1), float(a2)), "seed": seed}
 
 
+def cornell_lights(seed: int = 1, material: int = LAMBERT, area: bool = True):
+    """The Cornell box lit by a point light, a spot light and a directional
+    light entering through the open front (plus the ceiling quad when `area`).
+    Light conventions are the reference's constructors (light/*.rs): point and
+    spot `intensity` is the emitted power, spot angles are radians, the
+    directional `direction` is the direction of travel and its `intensity` the
+    perpendicular irradiance."""
+    sc = cornell_box(seed, material)
+    if not area:
+        sc["meshes"] = sc["meshes"][:-1]
+        sc["materials"] = sc["materials"][:-1]
+        sc["instances"] = sc["instances"][:-1]
+    sc["point_lights"] = [{"position": (0.7, 2.5, 0.4), "color": (1.0, 0.85, 0.6), "intensity": 30.0}]
+    sc["spot_lights"] = [{"position": (-0.6, 2.85, 0.6), "direction": (0.25, -1.0, -0.3),
+                          "color": (0.6, 0.8, 1.0), "intensity": 60.0,
+                          "total_width": float(np.radians(35.0)), "falloff_start": float(np.radians(20.0))}]
+    sc["directional_lights"] = [{"direction": (-0.35, -0.45, -1.0), "color": (1.0, 0.95, 0.9), "intensity": 1.5}]
+    return sc
+
+
 # ---------------------------------------------------------------------------
 # Differentiable-render scene: the Cornell box with its five walls split into
 # 3 x 4 patches each (60 patches, every patch a 4 x 4 grid of quads) and each
