@@ -29,6 +29,7 @@ struct BounceKey {
   uint32_t* err;
   int num_sms;
   int shade_block;
+  int batch_lights;
 };
 
 // The operations of one bounce (the shared body of the direct and the captured path).
@@ -42,7 +43,7 @@ cudaError_t bounce_ops(const BounceKey& k, int cur, bool last, unsigned long lon
                                 B.h_inst, B.h_bary, B.capacity, c0, k.err, k.num_sms, s, nullptr, nullptr,
                                 B.counts + cur, k.jobs, k.jobs ? B.q_job[cur] : nullptr);
   if (e == cudaSuccess)
-    e = k.jobs ? launch_wf_shade_batch(k.jobs, B, cur, s, k.shade_block)
+    e = k.jobs ? launch_wf_shade_batch(k.jobs, B, cur, s, k.shade_block, k.batch_lights != 0)
                : launch_wf_shade(k.S.geo, k.S.d, k.P, B, cur, s, nullptr, k.shade_block);
   if (e == cudaSuccess && !last)
     e = launch_traverse_strided(k.S.geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
@@ -75,7 +76,8 @@ void destroy_bounce_graphs(tpt_context* ctx) {
 }
 
 cudaError_t enqueue_bounce(tpt_context* ctx, cudaStream_t s, const DevGeometry& geo, const DevRenderData& rd,
-                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last) {
+                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last,
+                           bool batch_lights) {
   BounceKey key;
   std::memset(&key, 0, sizeof key);
   if (!jobs) {
@@ -88,6 +90,7 @@ cudaError_t enqueue_bounce(tpt_context* ctx, cudaStream_t s, const DevGeometry& 
   key.err = ctx->d_err;
   key.num_sms = ctx->num_sms;
   key.shade_block = (int)ctx->shade_block;
+  key.batch_lights = jobs && batch_lights ? 1 : 0;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   const bool capturing = cudaStreamIsCapturing(s, &cap) == cudaSuccess && cap != cudaStreamCaptureStatusNone;
   if (!ctx->use_graphs || capturing) return bounce_ops(key, cur, last, next_counter(ctx), next_counter(ctx), s);

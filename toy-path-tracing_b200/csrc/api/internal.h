@@ -160,13 +160,16 @@ cudaError_t launch_wf_resolve(const WfBuffers& B, cudaStream_t s, const DevAdjoi
 // Batched stages: slot i is global path first_path + i of the jobs' index space.
 cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const WfBuffers& B, uint64_t first_path,
                                      uint32_t n_paths, cudaStream_t s);
-cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s, int block = 256);
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s, int block,
+                                  bool lights);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
 
 // bounce_graphs.cpp: one wavefront bounce (single job when jobs == nullptr,
 // else batched) on `s`, replayed from a cached CUDA graph when possible.
+// batch_lights: some job of the batch `jobs` has point, spot or directional lights
 cudaError_t enqueue_bounce(tpt_context* ctx, cudaStream_t s, const DevGeometry& geo, const DevRenderData& rd,
-                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last);
+                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last,
+                           bool batch_lights = false);
 void destroy_bounce_graphs(tpt_context* ctx);
 
 // capi_batch.cpp: jobs (MIS) through one wavefront launch sequence; out_rgb are

@@ -301,6 +301,7 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   for (size_t k = 0; k < weights.size(); ++k) pmf[k] = total > 0.0f ? weights[k] / total : 0.0f;
   R.tree_cat_pmf = R.has_tree && total > 0.0f ? tree_w / total : 0.0f;
   R.num_cat = total > 0.0f ? (uint32_t)kinds.size() : 0u;
+  R.num_delta_lights = desc->num_point_lights + desc->num_spot_lights + desc->num_directional_lights;
   if (!st) st = put(s, cdf, &R.cat_cdf);
   if (!st) st = put(s, pmf, &R.cat_pmf);
   if (!st) st = put(s, kinds, &R.cat_kind);

@@ -372,11 +372,24 @@ struct DirectPrep {
   float dist;
 };
 
+//
+// LIGHTS = false is the specialisation for scenes whose lights are all
+// emissive triangles: the light sampler then has the Tree category alone (pmf
+// tree_cat_pmf = 1, or no category without a tree) and every tree leaf is a
+// triangle, so the category draw and the delta-light paths are compiled out.
+template <bool LIGHTS>
 __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
                                                float u_cat, float u_tree, float us0, float us1, DirectPrep& out) {
-  if (S.d.num_cat == 0) return false;  // LightSampler::sample_category: no category
   float cat_pmf;
-  const uint32_t cat = sample_category(S.d, u_cat, cat_pmf);
+  uint32_t cat;
+  if (LIGHTS) {
+    if (S.d.num_cat == 0) return false;  // LightSampler::sample_category: no category
+    cat = sample_category(S.d, u_cat, cat_pmf);
+  } else {
+    if (!S.d.has_tree) return false;
+    cat = kCatTree;
+    cat_pmf = S.d.tree_cat_pmf;
+  }
   LightSample li;
   bool delta = true;
   float sel;
@@ -393,7 +406,7 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
     const uint32_t leaf = sample_light_tree(S.d.ltree, S.d.ltree_root, q, u_tree, leaf_pmf);
     if (leaf == 0xFFFFFFFFu) return false;
     const uint32_t li_inst = __ldg(&S.d.ltree[leaf].leaf_instance), li_tri = __ldg(&S.d.ltree[leaf].leaf_triangle);
-    if (li_inst == kLeafPointDev || li_inst == kLeafSpotDev) {
+    if (LIGHTS && (li_inst == kLeafPointDev || li_inst == kLeafSpotDev)) {
       if (!sample_li_delta(S.d, li_inst == kLeafPointDev ? 0u : 1u, li_tri, v.p, li)) return false;
     } else {
       if (!sample_li_triangle(S, li_inst, li_tri, v.p, us0, us1, li)) return false;

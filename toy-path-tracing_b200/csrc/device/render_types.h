@@ -158,6 +158,7 @@ struct DevRenderData {
   const float* cat_pmf;      // num_cat
   const uint32_t* cat_kind;  // kCatTree or 1 + directional index
   uint32_t num_cat;
+  uint32_t num_delta_lights; // point + spot + directional lights
   uint32_t pad2;
 };
 

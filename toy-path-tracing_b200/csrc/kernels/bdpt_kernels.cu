@@ -9,7 +9,8 @@ namespace tpt {
 constexpr int kBdptBlock = 128;
 constexpr int kBdptShStack = 32;
 
-__global__ void __launch_bounds__(kBdptBlock) render_bdpt_kernel(DevRender S, RenderLaunch P,
+__global__ void __launch_bounds__(kBdptBlock) render_bdpt_kernel(const __grid_constant__ DevRender S,
+                                                            const __grid_constant__ RenderLaunch P,
                                                                  float* __restrict__ samples, uint64_t first_path,
                                                                  uint64_t n_paths, uint32_t* err) {
   __shared__ uint32_t stack_sh[kBdptShStack * kBdptBlock];

@@ -81,7 +81,8 @@ constexpr uint32_t kLightTag = 0x80000000u;
 
 // Per sample: the camera ray and the light endpoint (bdpt.rs:96-110, 264-300);
 // both first rays into queue 0.
-__global__ void __launch_bounds__(kBdWfBlock) bd_init(DevRender S, RenderLaunch P, BdWfBuffers B,
+__global__ void __launch_bounds__(kBdWfBlock) bd_init(const __grid_constant__ DevRender S,
+                                                  const __grid_constant__ RenderLaunch P, BdWfBuffers B,
                                                       uint64_t first_path, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -116,7 +117,8 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_init(DevRender S, RenderLaunch 
 
 // Step `step` of both loops: camera rays of depth `step`, light rays of depth
 // step + 1, traced into the hit arrays; the next rays into queue cur ^ 1.
-__global__ void __launch_bounds__(kBdWfBlock) bd_step(DevRender S, RenderLaunch P, BdWfBuffers B,
+__global__ void __launch_bounds__(kBdWfBlock) bd_step(const __grid_constant__ DevRender S,
+                                                  const __grid_constant__ RenderLaunch P, BdWfBuffers B,
                                                       uint64_t first_path, uint32_t step, int cur) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[2 + cur]) return;
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_pairs(BdWfBuffers B, uint32_t n
   for (uint32_t k = 0; k < np; ++k) B.pair_sample[pbase + k] = i;
 }
 
-__global__ void __launch_bounds__(kBdWfBlock) bd_connect(DevRender S, BdWfBuffers B) {
+__global__ void __launch_bounds__(kBdWfBlock) bd_connect(const __grid_constant__ DevRender S, BdWfBuffers B) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[0]) return;
   const uint32_t MD = B.max_vertices;
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_connect(DevRender S, BdWfBuffer
   B.dist[j] = cn.dist;
 }
 
-__global__ void __launch_bounds__(kBdWfBlock) bd_resolve(DevRender S, BdWfBuffers B) {
+__global__ void __launch_bounds__(kBdWfBlock) bd_resolve(const __grid_constant__ DevRender S, BdWfBuffers B) {
   const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= B.counts[1]) return;
   const uint32_t MD = B.max_vertices;

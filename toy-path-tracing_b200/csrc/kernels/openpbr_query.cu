@@ -9,7 +9,7 @@ namespace tpt {
 namespace {
 constexpr int kQueryBlock = 128;
 
-__global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(DevRenderData rd, uint32_t material, uint64_t n,
+__global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(const __grid_constant__ DevRenderData rd, uint32_t material, uint64_t n,
                                                                 const float* __restrict__ wo,
                                                                 const float* __restrict__ wi,
                                                                 const uint32_t* __restrict__ front, uint32_t mode,
@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(DevRenderData rd
   pdf[i] = p;
 }
 
-__global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(DevRenderData rd, uint32_t material, uint64_t n,
+__global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(const __grid_constant__ DevRenderData rd, uint32_t material, uint64_t n,
                                                                   const float* __restrict__ wo,
                                                                   const float* __restrict__ u,
                                                                   const uint32_t* __restrict__ front, uint32_t mode,

@@ -28,7 +28,10 @@ namespace {
 enum : uint32_t { kRayNone = 0, kRayBounce = 1, kRayShadow = 2 };
 }
 
-__global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(DevRender S, RenderLaunch P,
+// LIGHTS: the scene has point, spot or directional lights (prepare_direct's specialisation).
+template <bool LIGHTS>
+__global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(const __grid_constant__ DevRender S,
+                                                                  const __grid_constant__ RenderLaunch P,
                                                                   float* __restrict__ samples, uint64_t first_path,
                                                                   uint64_t n_paths,
                                                                   unsigned long long* __restrict__ counter,
@@ -124,14 +127,14 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(D
         float us0, us1;
         ps.sample_2d(vertex_dim(depth, kOffSurface), us0, us1);
         const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
-        const float u_cat = S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(depth, kOffCategory)) : 0.0f;
+        const float u_cat = LIGHTS && S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(depth, kOffCategory)) : 0.0f;
         DirectPrep dp;
-        const bool nee = prepare_direct(S, m, v, u_cat, u_tree, us0, us1, dp);
+        const bool nee = prepare_direct<LIGHTS>(S, m, v, u_cat, u_tree, us0, us1, dp);
         if (nee) {
           contrib = beta * dp.contrib;
           tgt_inst = dp.inst;
           tgt_tri = dp.tri;
-          tgt_dist = dp.dist;
+          if (LIGHTS) tgt_dist = dp.dist;
         }
         bool alive = false;
         BsdfSampleOut s;
@@ -204,19 +207,26 @@ cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const
   DevRender S;
   S.geo = geo;
   S.d = rd;
-  static int blocks_per_sm = 0;
-  if (blocks_per_sm == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, render_mis_kernel, kRenderBlock, 0) !=
-            cudaSuccess ||
-        blocks_per_sm <= 0)
-      blocks_per_sm = 2;
+  const bool lights = rd.num_delta_lights > 0;
+  static int blocks_per_sm[2] = {0, 0};
+  int& bps = blocks_per_sm[lights ? 1 : 0];
+  if (bps == 0) {
+    const cudaError_t q =
+        lights ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, render_mis_kernel<true>, kRenderBlock, 0)
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, render_mis_kernel<false>, kRenderBlock, 0);
+    if (q != cudaSuccess || bps <= 0) bps = 2;
   }
   uint64_t blocks = (n_paths + kRenderBlock - 1) / kRenderBlock;
-  const uint64_t cap = (uint64_t)num_sms * blocks_per_sm;  // persistent: one wave
+  const uint64_t cap = (uint64_t)num_sms * bps;  // persistent: one wave
   if (blocks > cap) blocks = cap;
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
-  render_mis_kernel<<<(unsigned)blocks, kRenderBlock, 0, s>>>(S, P, samples, first_path, n_paths, counter, err);
+  if (lights)
+    render_mis_kernel<true><<<(unsigned)blocks, kRenderBlock, 0, s>>>(S, P, samples, first_path, n_paths, counter,
+                                                                      err);
+  else
+    render_mis_kernel<false><<<(unsigned)blocks, kRenderBlock, 0, s>>>(S, P, samples, first_path, n_paths, counter,
+                                                                       err);
   return cudaGetLastError();
 }
 

@@ -38,9 +38,13 @@
 namespace tpt {
 
 constexpr int kWfBlock = 256;
-#ifndef TPT_SHADE_MINB
-#define TPT_SHADE_MINB 1  // blocks per SM the shade kernel's register budget is sized for
-#endif
+// Blocks per SM the shade kernel's register budget is sized for: 512 threads
+// per SM (128 registers, 16 warps) for rendering, which the forward variants
+// reach without spilling; the adjoint variant (~200 registers) is not capped.
+template <bool ADJ, int BS>
+constexpr int shade_min_blocks() {
+  return ADJ ? 1 : 512 / BS;
+}
 
 __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   const unsigned act = __activemask();
@@ -65,7 +69,8 @@ __device__ __forceinline__ uint32_t job_of_path(const DevJob* __restrict__ jobs,
 }
 
 template <bool ADJ, bool BATCH>
-__global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaunch P0, WfBuffers B,
+__global__ void __launch_bounds__(kWfBlock) wf_generate(const __grid_constant__ DevRender S0,
+                                                                 const __grid_constant__ RenderLaunch P0, WfBuffers B,
                                                         uint64_t first_path, uint32_t n_paths,
                                                         const float* __restrict__ primal,
                                                         const DevJob* __restrict__ jobs, uint32_t n_jobs) {
@@ -115,9 +120,14 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(DevRender S0, RenderLaun
 }
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
-template <bool ADJ, bool BATCH, int BS>
-__global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, RenderLaunch P0, WfBuffers B, int cur,
-                                                     DevAdjoint A, const DevJob* __restrict__ jobs) {
+// LIGHTS: the scene (any scene of a batch) has point, spot or directional
+// lights (prepare_direct's specialisation).
+template <bool ADJ, bool BATCH, int BS, bool LIGHTS>
+__global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(const __grid_constant__ DevRender S0,
+                                                               const __grid_constant__ RenderLaunch P0,
+                                                               WfBuffers B, int cur,
+                                                               const __grid_constant__ DevAdjoint A,
+                                                               const DevJob* __restrict__ jobs) {
   __shared__ float grad_sh[ADJ ? BS * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[cur]) return;
@@ -182,8 +192,8 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
       ps.sample_2d(vertex_dim(d, kOffSurface), us0, us1);
       const float u_tree = ps.sample_1d(vertex_dim(d, kOffTree));
       // one light-sampler category takes any u: skip drawing it
-      const float u_cat = S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(d, kOffCategory)) : 0.0f;
-      if (prepare_direct(S, m, v, u_cat, u_tree, us0, us1, dp)) {
+      const float u_cat = LIGHTS && S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(d, kOffCategory)) : 0.0f;
+      if (prepare_direct<LIGHTS>(S, m, v, u_cat, u_tree, us0, us1, dp)) {
         dp.contrib = beta * dp.contrib;
         push_shadow = true;
       }
@@ -272,7 +282,7 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
     if (BATCH) B.s_job[qs] = jb;
     B.s_target[qs] = dp.inst;
     B.s_target[C + qs] = dp.tri;
-    B.s_dist[qs] = dp.dist;
+    if (LIGHTS) B.s_dist[qs] = dp.dist;
     B.s_contrib[qs] = dp.contrib.x;
     B.s_contrib[C + qs] = dp.contrib.y;
     B.s_contrib[2 * C + qs] = dp.contrib.z;
@@ -291,13 +301,15 @@ __global__ void __launch_bounds__(BS, TPT_SHADE_MINB) wf_shade(DevRender S0, Ren
 // first hit is the sampled emitter triangle, or (point and spot lights) the
 // first hit lies beyond the light.
 template <bool ADJ>
-__global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B, DevAdjoint A) {
+__global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B, const __grid_constant__ DevAdjoint A) {
   __shared__ float grad_sh[ADJ ? kWfBlock * kGradParams : 1];
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[2]) return;
   const uint32_t C = B.capacity;
-  const bool visible =
-      shadow_visible(B.s_tri[j], B.s_inst[j], B.s_t[j], B.s_target[j], B.s_target[C + j], B.s_dist[j]);
+  const uint32_t tgt_inst = B.s_target[j];
+  // the distance plane is written for delta-light shadow rays only
+  const bool visible = shadow_visible(B.s_tri[j], B.s_inst[j], B.s_t[j], tgt_inst, B.s_target[C + j],
+                                      tgt_inst == 0xFFFFFFFFu ? B.s_dist[j] : 0.0f);
   if (visible) {
     const uint32_t slot = B.s_slot[j];
     const float sgn = ADJ ? -1.0f : 1.0f;
@@ -343,12 +355,18 @@ static inline unsigned grid_for_block(uint32_t n, int bs) { return (n + bs - 1) 
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                             const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A, int block) {
   DevRender S{geo, rd};
-  if (A)
-    wf_shade<true, false, kWfBlock><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, *A, nullptr);
+  const bool lights = rd.num_delta_lights > 0;
+  const DevAdjoint none{};
+  if (A)  // one instantiation for the adjoint, with the delta-light paths
+    wf_shade<true, false, kWfBlock, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, *A, nullptr);
+  else if (block == 128 && lights)
+    wf_shade<false, false, 128, true><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(S, P, B, cur, none, nullptr);
   else if (block == 128)
-    wf_shade<false, false, 128><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(S, P, B, cur, DevAdjoint{}, nullptr);
+    wf_shade<false, false, 128, false><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(S, P, B, cur, none, nullptr);
+  else if (lights)
+    wf_shade<false, false, kWfBlock, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, none, nullptr);
   else
-    wf_shade<false, false, kWfBlock><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, DevAdjoint{}, nullptr);
+    wf_shade<false, false, kWfBlock, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, none, nullptr);
   return cudaGetLastError();
 }
 
@@ -359,13 +377,19 @@ cudaError_t launch_wf_generate_batch(const DevJob* jobs, uint32_t n_jobs, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s, int block) {
-  if (block == 128)
-    wf_shade<false, true, 128><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(DevRender{}, RenderLaunch{}, B, cur,
-                                                                             DevAdjoint{}, jobs);
+cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cur, cudaStream_t s, int block,
+                                  bool lights) {
+  const DevRender S{};
+  const RenderLaunch P{};
+  const DevAdjoint none{};
+  if (block == 128 && lights)
+    wf_shade<false, true, 128, true><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(S, P, B, cur, none, jobs);
+  else if (block == 128)
+    wf_shade<false, true, 128, false><<<grid_for_block(B.capacity, 128), 128, 0, s>>>(S, P, B, cur, none, jobs);
+  else if (lights)
+    wf_shade<false, true, kWfBlock, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, none, jobs);
   else
-    wf_shade<false, true, kWfBlock><<<grid_for(B.capacity), kWfBlock, 0, s>>>(DevRender{}, RenderLaunch{}, B, cur,
-                                                                            DevAdjoint{}, jobs);
+    wf_shade<false, true, kWfBlock, false><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, none, jobs);
   return cudaGetLastError();
 }
 
