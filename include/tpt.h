@@ -202,6 +202,22 @@ typedef struct tpt_directional_light_desc {
   float intensity;
 } tpt_directional_light_desc;
 
+/* EnvironmentLight::from_pixels (light/environment.rs:46-82): an
+ * equirectangular map of width x height RGB radiance values, row-major, row 0
+ * at the +y pole; u = phi / 2pi with phi = atan2(x, z), v = theta / pi with
+ * theta measured from +y.  `scale` multiplies the radiance, `rotate_y` rotates
+ * the map about +y (radians).  Sampled through the reference's two mip-pyramid
+ * distributions (luminance x sin(theta), and its MIS-compensated variant for
+ * NEE); the map is one category of the light sampler, weighted by its total
+ * power. */
+typedef struct tpt_environment_desc {
+  uint32_t width;
+  uint32_t height;
+  const float* pixels; /* width * height * 3 */
+  float scale;
+  float rotate_y;
+} tpt_environment_desc;
+
 /* One node of the SG light tree (light_tree/mod.rs:65-86), 64 bytes:
  * interior nodes have leaf_instance == leaf_triangle == 0xFFFFFFFF; leaves name
  * the emissive triangle and carry its area, or a point light
@@ -245,13 +261,17 @@ typedef struct tpt_scene_desc {
   tpt_light_tree_view light_tree;
   /* Scene::point_lights / spot_lights / directional_lights (may be NULL when
    * the count is 0).  BDPT jobs reject scenes with lights that are not
-   * emissive triangles (the device BDPT covers area lights only). */
+   * emissive triangles, the environment included (the device BDPT covers
+   * area lights only). */
   const tpt_point_light_desc* point_lights;
   uint32_t num_point_lights;
   const tpt_spot_light_desc* spot_lights;
   uint32_t num_spot_lights;
   const tpt_directional_light_desc* directional_lights;
   uint32_t num_directional_lights;
+  /* Scene::set_environment_light; NULL = none (rays that escape carry no
+   * radiance). */
+  const tpt_environment_desc* environment;
 } tpt_scene_desc;
 
 /* Copies the scene into device memory in the B200 layout (128-byte nodes,

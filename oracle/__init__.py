@@ -89,6 +89,16 @@ def _declare(L):
         "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
         "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, f32, vp]),
         "orc_render_scene_set_lights": (None, [vp, vp, u32, vp, u32, vp, u32]),
+        "orc_render_scene_set_environment": (None, [vp, u32, u32, vp, f32, f32]),
+        "orc_env_create": (vp, [u32, u32, vp, f32, f32]),
+        "orc_env_free": (None, [vp]),
+        "orc_env_total_power": (f32, [vp]),
+        "orc_env_radiance": (None, [vp, vp, vp]),
+        "orc_env_pdf": (f32, [vp, vp, i32]),
+        "orc_env_sample": (i32, [vp, f32, f32, i32, vp]),
+        "orc_env_direction_to_uv": (None, [vp, vp]),
+        "orc_env_uv_to_direction": (None, [f32, f32, vp]),
+        "orc_env_pyramid": (u32, [vp, i32, vp, vp, vp]),
         "orc_render_emitted": (None, [vp, i32, i32, vp, vp, i32, i32, vp, vp, vp, f32, i32, vp]),
         "orc_render_material_pdf": (f32, [vp, i32, i32, vp, vp, vp]),
         "orc_render_scene_set_openpbr": (C.c_char_p, [vp, u32, vp]),
@@ -231,6 +241,67 @@ def camera_ray(params, rx, ry, px, py, ux, uy, spp):
     return out
 
 
+class Environment:
+    """EnvironmentLight (light/environment.rs) on the oracle: pixels [H, W, 3]."""
+
+    def __init__(self, pixels, scale=1.0, rotate_y=0.0):
+        px = np.ascontiguousarray(pixels, np.float32)
+        self.height, self.width = px.shape[:2]
+        self.h = lib().orc_env_create(self.width, self.height, _p(px), float(scale), float(rotate_y))
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().orc_env_free(self.h)
+        except Exception:
+            pass
+
+    def total_power(self):
+        return lib().orc_env_total_power(self.h)
+
+    def radiance(self, direction):
+        d = np.asarray(direction, np.float32)
+        out = np.zeros(3, np.float32)
+        lib().orc_env_radiance(self.h, _p(d), _p(out))
+        return out
+
+    def pdf(self, direction, compensated=False):
+        d = np.asarray(direction, np.float32)
+        return lib().orc_env_pdf(self.h, _p(d), int(compensated))
+
+    def sample(self, u, v, compensated=False):
+        """dict(direction, radiance, uv, pdf) or None."""
+        out = np.zeros(9, np.float32)
+        if not lib().orc_env_sample(self.h, float(u), float(v), int(compensated), _p(out)):
+            return None
+        return {"direction": out[:3].copy(), "radiance": out[3:6].copy(), "uv": out[6:8].copy(),
+                "pdf": float(out[8])}
+
+    def pyramid(self, compensated=False):
+        """(level dims [(w, h)] coarsest first, total weight, leaf weights [ph, pw])."""
+        n = lib().orc_env_pyramid(self.h, int(compensated), None, None, None)
+        dims = np.zeros(2 * n, np.uint32)
+        total = np.zeros(1, np.float32)
+        lib().orc_env_pyramid(self.h, int(compensated), _p(dims), _p(total), None)
+        pw, ph = int(dims[-2]), int(dims[-1])
+        leaf = np.zeros((ph, pw), np.float32)
+        lib().orc_env_pyramid(self.h, int(compensated), None, None, _p(leaf))
+        return [tuple(int(x) for x in dims[2 * k:2 * k + 2]) for k in range(n)], float(total[0]), leaf
+
+
+def env_direction_to_uv(direction):
+    d = np.asarray(direction, np.float32)
+    uv = np.zeros(2, np.float32)
+    lib().orc_env_direction_to_uv(_p(d), _p(uv))
+    return uv
+
+
+def env_uv_to_direction(u, v):
+    d = np.zeros(3, np.float32)
+    lib().orc_env_uv_to_direction(float(u), float(v), _p(d))
+    return d
+
+
 def light_arrays(scene: dict):
     """Point (n x 7), spot (n x 12) and directional (n x 7) light arrays of a
     scene dict's "point_lights", "spot_lights", "directional_lights" lists."""
@@ -273,8 +344,14 @@ class RenderScene:
                 if why:
                     raise ValueError(why.decode())
         pts, spots, dirs = light_arrays(scene)
-        self.non_area_lights = len(pts) + len(spots) + len(dirs)
+        env = scene.get("environment")
+        self.non_area_lights = len(pts) + len(spots) + len(dirs) + (env is not None)
         lib().orc_render_scene_set_lights(self.h, _p(pts), len(pts), _p(spots), len(spots), _p(dirs), len(dirs))
+        if env is not None:
+            px = np.ascontiguousarray(env["pixels"], np.float32)
+            h, w = px.shape[:2]
+            lib().orc_render_scene_set_environment(self.h, w, h, _p(px), float(env.get("scale", 1.0)),
+                                                   float(env.get("rotate_y", 0.0)))
         nodes, root = light_tree
         nodes = np.ascontiguousarray(nodes)
         lib().orc_render_scene_set_light_tree(self.h, nodes.ctypes.data if len(nodes) else None, len(nodes), int(root))
@@ -293,7 +370,7 @@ class RenderScene:
 
     def _check_integrator(self, integrator):
         if integrator == 1 and self.non_area_lights:
-            raise ValueError("the oracle's BDPT covers area lights only")
+            raise ValueError("the oracle's BDPT covers area lights only (no point, spot, directional or environment)")
 
     def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0):
         """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3].

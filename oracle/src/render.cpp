@@ -386,6 +386,18 @@ Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, cons
       delta = false;
     }
     sel = cat_pmf * leaf_pmf;
+  } else if (cat == -3) {
+    // environment::sample_li_mis_compensated (light/environment.rs:258-273)
+    EnvSample es;
+    if (!s.env.sample_mis_compensated(rnd.light.u_surface.x, rnd.light.u_surface.y, &es)) return Vec3(0, 0, 0);
+    if (es.pdf <= 0.0f) return Vec3(0, 0, 0);
+    li.radiance = es.radiance;
+    li.wi = es.direction;
+    li.pdf = es.pdf;
+    li.distance = INFINITY;
+    li.inst = li.tri = -1;
+    delta = false;
+    sel = cat_pmf;
   } else {
     // directional::sample_li (light/directional.rs:33-42)
     const DirLight& d = s.dirs[cat];
@@ -401,9 +413,12 @@ Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, cons
   float bsdf_pdf = 0.0f;
   if (delta) {
     f = m.kind == kLambert ? lambert_eval(m, v, li.wi) : material_eval(m, v, li.wi, kRadiance);
-  } else {
+  } else if (m.kind == kLambert) {
     f = lambert_eval(m, v, li.wi);
     bsdf_pdf = length_squared(f) == 0.0f ? 0.0f : lambert_pdf(v, li.wi);
+  } else {  // Material::eval_pdf (material/mod.rs:351-370): the environment at an OpenPBR vertex
+    f = material_eval(m, v, li.wi, kRadiance);
+    bsdf_pdf = length_squared(f) == 0.0f ? 0.0f : material_pdf(m, v, li.wi);
   }
   if (length_squared(f) == 0.0f) return Vec3(0, 0, 0);
   float cos_surface = std::fabs(dot(v.ng, li.wi));
@@ -505,8 +520,9 @@ void RenderScene::finalize() {
       area_lights.push_back(AreaLight{(int32_t)i, t, area, weight, area_light_weight_sum});
     }
   }
-  // LightSampler::build_from_scene (light/mod.rs:134-188): Tree, then one
-  // category per directional light with luminance(color) * intensity > 0
+  // LightSampler::build_from_scene (light/mod.rs:134-188): Tree, the
+  // Environment (by total power), then one category per directional light
+  // with luminance(color) * intensity > 0
   float w = tree.empty() ? 0.0f : fmax_num(tree[root].flux, 0.0f);
   has_tree = w > 0.0f;
   std::vector<float> weights;
@@ -514,6 +530,11 @@ void RenderScene::finalize() {
   if (w > 0.0f) {
     cat_kind.push_back(-1);
     weights.push_back(w);
+  }
+  const float env_w = has_env ? fmax_num(env.total_power(), 0.0f) : 0.0f;
+  if (env_w > 0.0f) {
+    cat_kind.push_back(-3);
+    weights.push_back(env_w);
   }
   for (size_t i = 0; i < dirs.size(); ++i) {
     float dw = fmax_num(luminance(dirs[i].color) * dirs[i].intensity, 0.0f);
@@ -536,6 +557,7 @@ void RenderScene::finalize() {
   for (size_t k = 0; k < weights.size(); ++k) cat_pmf[k] = total > 0.0f ? weights[k] / total : 0.0f;
   if (!(total > 0.0f)) cat_kind.clear();
   tree_cat_pmf = has_tree && total > 0.0f ? w / total : 0.0f;
+  env_cat_pmf = env_w > 0.0f && total > 0.0f ? env_w / total : 0.0f;
 }
 
 void RenderScene::triangle_world(int inst, int tri, Vec3* p) const {
@@ -586,11 +608,23 @@ Vertex RenderScene::shading_vertex(int inst, int tri, Vec3 b, Vec3 incident) con
   return v;
 }
 
+// emitted_radiance_from_bsdf_sample_infinite (integrator/mis.rs:238-258) with
+// pdf_for_environment_hit (light/mod.rs:439-450, MIS-compensated), without the
+// path throughput
+Vec3 env_escape(const RenderScene& s, Vec3 dir, bool delta, float bsdf_pdf) {
+  if (!s.has_env) return Vec3(0, 0, 0);  // infinite_light_le without an environment
+  const Vec3 le = s.env.radiance(dir);
+  if (le.x == 0.0f && le.y == 0.0f && le.z == 0.0f) return Vec3(0, 0, 0);
+  if (delta) return le;
+  const float light_pdf = s.env_cat_pmf <= 0.0f ? 0.0f : s.env_cat_pmf * s.env.pdf_mis_compensated(dir);
+  return le * balance(bsdf_pdf, light_pdf);
+}
+
 // integrator/mis.rs:19-139
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
   Vec3 L(0, 0, 0), beta(1, 1, 1);
   SceneHit h;
-  if (!closest(s, ray.origin, ray.direction, &h)) return L;
+  if (!closest(s, ray.origin, ray.direction, &h)) return s.has_env ? s.env.radiance(ray.direction) : L;
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
   const Material* m = &s.mat_of(h.instance);
   if (m->kind == kEmissive) L += emissive_le(*m);
@@ -609,7 +643,10 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
       beta /= q;
     }
     SceneHit nh;
-    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) break;
+    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) {
+      L += beta * env_escape(s, bs.wi, bs.delta, bs.pdf);
+      break;
+    }
     Vertex nv = s.shading_vertex(nh.instance, nh.triangle, nh.bary, bs.wi);
     const Material* nm = &s.mat_of(nh.instance);
     if (nm->kind == kEmissive) {
@@ -653,7 +690,7 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
     }
     if (m->kind == kOpenPbr && !bs.delta) sink.vertex(mi, v, bs.wi, R);
     SceneHit nh;
-    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) break;
+    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) break;  // R = the escape emission
     Vertex nv = s.shading_vertex(nh.instance, nh.triangle, nh.bary, bs.wi);
     const Material* nm = &s.mat_of(nh.instance);
     if (nm->kind == kEmissive) {

@@ -9,6 +9,7 @@
 // the flattened node array as input (the same one the device uses).
 #pragma once
 #include "camera.h"
+#include "environment.h"
 #include "geometry.h"
 #include "openpbr.h"
 #include "sampler.h"
@@ -94,8 +95,11 @@ struct RenderScene {
   std::vector<PointLight> points;
   std::vector<SpotLight> spots;
   std::vector<DirLight> dirs;
-  // LightSampler (light/mod.rs:117-188): categories (-1 = the tree, i >= 0 =
-  // directional light i), their CDF and pmfs
+  bool has_env = false;  // Scene::environment_light
+  Environment env;
+  float env_cat_pmf = 0.0f;  // LightSampler::category_pmf(Environment)
+  // LightSampler (light/mod.rs:117-188): categories (-1 = the tree, -3 = the
+  // environment, i >= 0 = directional light i), their CDF and pmfs
   std::vector<int> cat_kind;
   std::vector<float> cat_cdf, cat_pmf;
   std::vector<AreaLight> area_lights;  // Scene::area_light_triangles, instance order

@@ -8,8 +8,9 @@ exactly for any set of samples:
   BSDF is linear in base_color, so at max_depth 1 every sample that scatters
   once satisfies sum_c bc_c * dL/dbc_c = L_c (the central difference of a
   linear function is exact).  Summed over the image: sum_m bc[m] * grad[m] =
-  image(depth 1) - image(depth 0), per channel.  With a directional light the
-  light samples at the first vertex (f at the light direction) enter both sides.
+  image(depth 1) - image(depth 0), per channel.  With a directional light or
+  an environment map the light samples at the first vertex (f at the light
+  direction) and the escaping rays enter both sides.
 * Masking: groups left out of the mask get exactly zero; groups are computed
   independently of each other.
 * Linearity in dLoss/dimage, and zero gradients for a zero dLoss/dimage.
@@ -25,17 +26,20 @@ import tpt_scenes
 SUN = {"direction": (-0.35, -0.45, -1.0), "color": (1.0, 0.95, 0.9), "intensity": 1.5}
 
 
-def linear_scene(directional=False):
+def linear_scene(extra=None):
     sc = tpt_scenes.cornell_patches()
     for m in sc["materials"][:64]:
         m["specular_weight"] = 0.0
         m["base_metalness"] = 0.0
-    if directional:  # light samples at OpenPBR vertices: f at the light direction
+    if extra == "directional":  # light samples at OpenPBR vertices: f at the light direction
         sc["directional_lights"] = [SUN]
+    elif extra == "environment":  # the same, plus escaping rays
+        sc["environment"] = tpt_scenes.sky_environment(rotate_y=0.35)
     return sc
 
 
-@pytest.fixture(scope="module", params=[False, True], ids=["area", "area+directional"])
+@pytest.fixture(scope="module", params=[None, "directional", "environment"],
+                ids=["area", "area+directional", "area+environment"])
 def lin(request):
     sc = linear_scene(request.param)
     return sc, orc.RenderScene(sc, tpt.build_light_tree(sc))

@@ -156,10 +156,11 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   A.s_gkey = nullptr;
   const uint32_t npix = L.width * L.height;
   const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
-  // light samples at OpenPBR vertices come from directional lights only (the
-  // light tree serves diffuse vertices): their gradient planes follow the
-  // samples in the scratch buffer, sized for the wavefront's capacity
-  const bool light_grads = scene->num_directional_lights > 0;
+  // light samples at OpenPBR vertices come from directional lights and the
+  // environment only (the light tree serves diffuse vertices): their gradient
+  // planes follow the samples in the scratch buffer, sized for the
+  // wavefront's capacity
+  const bool light_grads = scene->num_directional_lights > 0 || scene->render.has_env;
   if ((st = ensure_wavefront(ctx, cp * L.spp))) return st;
   const size_t sample_bytes = ((size_t)cp * L.spp * 12 + 255) & ~(size_t)255;
   const size_t plane_bytes = light_grads ? (size_t)(kGradParams + 1) * ctx->wf.capacity * 4 : 0;

@@ -115,7 +115,7 @@ tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   float* samples = (float*)ctx->d_scratch;
   const DevGeometry no_geo{};
   bool lights = false;
-  for (int j = 0; j < n_jobs; ++j) lights = lights || jobs[j].scene->render.num_delta_lights > 0;
+  for (int j = 0; j < n_jobs; ++j) lights = lights || jobs[j].scene->render.num_extra_lights > 0;
   for (const Chunk& c : plan_chunks(L, path_base, capacity)) {
     cudaError_t e = launch_wf_generate_batch(ctx->d_jobs, (uint32_t)n_jobs, B, c.first_path, c.n_paths, s);
     for (uint32_t b = 0; e == cudaSuccess && b <= c.max_depth; ++b)

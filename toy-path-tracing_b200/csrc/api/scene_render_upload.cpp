@@ -6,6 +6,7 @@
 #include <cstring>
 #include <string>
 
+#include "../host/env_build.h"
 #include "../host/openpbr_lower.h"
 #include "internal.h"
 
@@ -268,9 +269,36 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   R.dec_e = ctx->d_dec_e;
   R.ltree_root = s->light_tree.root;
   R.num_materials = desc->num_materials;
+  // the environment (EnvironmentLight::from_pixels): map and distributions
+  R.has_env = 0;
+  R.env = DevEnvironment{};
+  EnvHost env;
+  const tpt_environment_desc* ed = desc->environment;
+  if (ed) {
+    if (!ed->pixels || ed->width == 0 || ed->height == 0)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "environment map must be non-empty");
+    build_environment(ed->width, ed->height, ed->pixels, ed->scale, ed->rotate_y, &env);
+    std::vector<float> px(ed->pixels, ed->pixels + (size_t)ed->width * ed->height * 3);
+    st = put(s, px, &R.env.pixels);
+    if (!st) st = put(s, env.dist.weights, &R.env.dist.weights);
+    if (!st) st = put(s, env.dist.levels, &R.env.dist.levels);
+    if (!st) st = put(s, env.mis.weights, &R.env.mis.weights);
+    if (!st) st = put(s, env.mis.levels, &R.env.mis.levels);
+    if (st) return st;
+    R.env.width = env.width;
+    R.env.height = env.height;
+    R.env.scale = env.scale;
+    std::memcpy(R.env.rot, env.rot, sizeof env.rot);
+    std::memcpy(R.env.inv_rot, env.inv_rot, sizeof env.inv_rot);
+    R.env.dist.num_levels = (uint32_t)(env.dist.levels.size() / 3);
+    R.env.dist.total_weight = env.dist.total_weight;
+    R.env.mis.num_levels = (uint32_t)(env.mis.levels.size() / 3);
+    R.env.mis.total_weight = env.mis.total_weight;
+    R.has_env = 1;
+  }
   // LightSampler::build_from_scene (light/mod.rs:134-188): the Tree category,
-  // then one per directional light with luminance(color) * intensity > 0
-  // (there is no environment light here)
+  // the Environment (weighted by its total power), then one per directional
+  // light with luminance(color) * intensity > 0
   const float tree_w = lnodes.empty() ? 0.0f : std::fmax(lnodes[R.ltree_root].flux, 0.0f);
   R.has_tree = tree_w > 0.0f ? 1u : 0u;
   std::vector<uint32_t> kinds;
@@ -278,6 +306,11 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   if (tree_w > 0.0f) {
     kinds.push_back(kCatTree);
     weights.push_back(tree_w);
+  }
+  const float env_w = R.has_env ? std::fmax(env.total_power, 0.0f) : 0.0f;
+  if (env_w > 0.0f) {
+    kinds.push_back(kCatEnv);
+    weights.push_back(env_w);
   }
   for (uint32_t i = 0; i < desc->num_directional_lights; ++i) {
     const DevDirLight& d = ddirs[i];
@@ -300,8 +333,10 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   }
   for (size_t k = 0; k < weights.size(); ++k) pmf[k] = total > 0.0f ? weights[k] / total : 0.0f;
   R.tree_cat_pmf = R.has_tree && total > 0.0f ? tree_w / total : 0.0f;
+  R.env.cat_pmf = env_w > 0.0f && total > 0.0f ? env_w / total : 0.0f;  // LightSampler::category_pmf
   R.num_cat = total > 0.0f ? (uint32_t)kinds.size() : 0u;
-  R.num_delta_lights = desc->num_point_lights + desc->num_spot_lights + desc->num_directional_lights;
+  R.num_extra_lights =
+      desc->num_point_lights + desc->num_spot_lights + desc->num_directional_lights + (R.has_env ? 1u : 0u);
   if (!st) st = put(s, cdf, &R.cat_cdf);
   if (!st) st = put(s, pmf, &R.cat_pmf);
   if (!st) st = put(s, kinds, &R.cat_kind);

@@ -10,6 +10,7 @@
 // differentials, which no material in scope reads.
 #pragma once
 #include "batch_types.h"
+#include "environment.cuh"
 #include "lights.cuh"
 #include "openpbr.cuh"
 #include "render_types.h"
@@ -366,6 +367,56 @@ static __device__ __noinline__ bool sample_li_delta(const DevRenderData& d, uint
   return true;
 }
 
+// Material::eval_pdf (material/mod.rs:351-370) in radiance mode: f with the
+// shading-normal correction, and the BSDF's pdf when f is not zero.
+static __device__ __noinline__ V3 material_eval_pdf(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
+                                                    V3 wi, float& pdf_out) {
+  pdf_out = 0.0f;
+  if (m.kind == kDevLambert) {
+    const V3 f = lambert_eval(m, v, wi);
+    if (length_sq(f) != 0.0f) pdf_out = lambert_pdf(v, wi);
+    return f;
+  }
+  if (m.kind == kDevOpenPbr) {
+    if (dot(v.wo, v.ng) <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+    const V3 wi_l = normalize_or_zero(to_local(v.frame, wi));
+    if (wo_l.z <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+    opbr::OpbrVertex s;
+    opbr::init_vertex(s, S.d.openpbr + m.openpbr, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    V3 f;
+    float pdf;
+    opbr::eval_pdf(s, s, wi_l, f, pdf);
+    f = modified_eval(v, wi, f, false);
+    if (length_sq(f) != 0.0f) pdf_out = pdf;
+    return f;
+  }
+  return V3{0.0f, 0.0f, 0.0f};
+}
+
+// environment::sample_li_mis_compensated (light/environment.rs:258-273)
+static __device__ __noinline__ bool sample_li_env(const DevRenderData& d, float us0, float us1, LightSample& li) {
+  float pdf;
+  if (!env_sample(d.env, d.env.mis, us0, us1, li.wi, li.radiance, pdf)) return false;
+  if (pdf <= 0.0f) return false;
+  li.pdf = pdf;
+  li.distance = __int_as_float(0x7f800000);
+  li.inst = li.tri = 0xFFFFFFFFu;
+  return true;
+}
+
+// emitted_radiance_from_bsdf_sample_infinite (integrator/mis.rs:238-258) for a
+// ray that left the scene after a BSDF sample of pdf `bsdf_pdf` (camera rays:
+// `camera` = true, the map's radiance as is -- mis.rs:33-35).
+static __device__ __noinline__ V3 env_escape(const DevRenderData& d, V3 dir, bool camera, bool delta, float bsdf_pdf) {
+  const V3 le = env_radiance(d.env, dir);
+  if (camera || (le.x == 0.0f && le.y == 0.0f && le.z == 0.0f) || delta) return le;
+  // pdf_for_environment_hit (light/mod.rs:439-450), MIS-compensated
+  const float cat = d.env.cat_pmf;
+  const float light_pdf = cat <= 0.0f ? 0.0f : cat * env_pdf(d.env, d.env.mis, dir);
+  return le * balance_heuristic(bsdf_pdf, light_pdf);
+}
+
 struct DirectPrep {
   V3 contrib, so, wi;
   uint32_t inst, tri;
@@ -415,6 +466,10 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
       out.tri = li.tri;
     }
     sel = cat_pmf * leaf_pmf;
+  } else if (cat == kCatEnv) {
+    if (!sample_li_env(S.d, us0, us1, li)) return false;
+    delta = false;
+    sel = cat_pmf;
   } else {
     if (!sample_li_delta(S.d, 2u, cat - 1, v.p, li)) return false;
     sel = cat_pmf;
@@ -424,10 +479,12 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
   float bsdf_pdf = 0.0f;
   if (delta) {
     f = m.kind == kDevLambert ? lambert_eval(m, v, li.wi) : material_eval(S, m, v, li.wi, false);
-  } else {
+  } else if (m.kind == kDevLambert) {
     f = lambert_eval(m, v, li.wi);
     if (length_sq(f) == 0.0f) return false;
     bsdf_pdf = lambert_pdf(v, li.wi);
+  } else {  // the environment at an OpenPBR vertex
+    f = material_eval_pdf(S, m, v, li.wi, bsdf_pdf);
   }
   if (length_sq(f) == 0.0f) return false;
   const float cos_surface = fabsf(dot(v.ng, li.wi));

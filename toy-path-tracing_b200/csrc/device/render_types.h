@@ -123,6 +123,29 @@ constexpr uint32_t kLeafPointDev = 0xFFFFFFFEu;  // light-tree leaf of a point l
 constexpr uint32_t kLeafSpotDev = 0xFFFFFFFDu;   // light-tree leaf of a spot light
 constexpr uint32_t kCatTree = 0u;                // light-sampler category: the light tree;
                                                  // 1 + i: directional light i
+constexpr uint32_t kCatEnv = 0xFFFFFFFFu;        // light-sampler category: the environment
+
+// One hierarchical distribution of EnvironmentLight (light/environment.rs:
+// 22-35): all mip levels of the padded (power-of-two) weight map, coarsest
+// (1 x 1) first; levels[3 l .. 3 l + 2] = width, height, offset of level l.
+struct DevEnvDist {
+  const float* weights;
+  const uint32_t* levels;
+  uint32_t num_levels;
+  float total_weight;
+};
+
+// EnvironmentLight: RGB map (row-major), scale, rotation about +y as
+// Mat3::from_rotation_y(+-rotate_y) columns, and its two distributions.
+struct DevEnvironment {
+  const float* pixels;
+  uint32_t width, height;
+  float scale;
+  float cat_pmf;         // LightSampler pmf of the Environment category (0: not a category)
+  float rot[9], inv_rot[9];  // column-major 3 x 3
+  DevEnvDist dist;       // luminance x sin(theta)
+  DevEnvDist mis;        // MIS-compensated: (luminance - mean) x sin(theta) where above epsilon
+};
 
 struct DevMeshInfo {
   uint32_t vtx_base, idx_base, num_tris, flags;  // flags bit 0: normals, bit 1: uvs
@@ -156,10 +179,11 @@ struct DevRenderData {
   const DevDirLight* dirs;
   const float* cat_cdf;      // num_cat + 1 entries, normalised
   const float* cat_pmf;      // num_cat
-  const uint32_t* cat_kind;  // kCatTree or 1 + directional index
+  const uint32_t* cat_kind;  // kCatTree, kCatEnv or 1 + directional index
   uint32_t num_cat;
-  uint32_t num_delta_lights; // point + spot + directional lights
-  uint32_t pad2;
+  uint32_t num_extra_lights; // point + spot + directional lights + the environment
+  uint32_t has_env;
+  DevEnvironment env;
 };
 
 // Camera constants computed on the host (scene/camera.rs:21-39).

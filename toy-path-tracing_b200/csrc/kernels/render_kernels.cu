@@ -102,7 +102,12 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
         done = true;
       }
     } else if (h.tri < 0) {
-      done = true;  // infinite_light_le: no environment light
+      // the ray left the scene: the environment's radiance (mis.rs:33-35, 127-135)
+      if (LIGHTS && S.d.has_env) {
+        const V3 le = env_escape(S.d, rd, depth == 0, (prev_mat >> 31) != 0, depth == 0 ? 0.0f : prev_pdf);
+        L = L + (depth == 0 ? le : beta * le);
+      }
+      done = true;
     } else {
       const Vertex v = shade_hit<int>(S, h, rd);
       const uint32_t mi = __ldg(&S.d.inst[v.inst].material);
@@ -207,7 +212,7 @@ cudaError_t launch_render(const DevGeometry& geo, const DevRenderData& rd, const
   DevRender S;
   S.geo = geo;
   S.d = rd;
-  const bool lights = rd.num_delta_lights > 0;
+  const bool lights = rd.num_extra_lights > 0;
   static int blocks_per_sm[2] = {0, 0};
   int& bps = blocks_per_sm[lights ? 1 : 0];
   if (bps == 0) {

@@ -248,6 +248,14 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
       }
     }
   }
+  if (LIGHTS && tri < 0 && S.d.has_env) {
+    // the ray left the scene: the environment's radiance (mis.rs:33-35, 127-135)
+    const float* qr = B.q_ray[cur];
+    const V3 rd = V3{qr[3 * C + j], qr[4 * C + j], qr[5 * C + j]};
+    const uint32_t pm = B.prev_mat[slot];
+    const V3 le = env_escape(S.d, rd, d == 0, (pm >> 31) != 0, d == 0 ? 0.0f : B.prev[6 * C + slot]);
+    L = L + sgn * (d == 0 ? le : beta * le);
+  }
   B.L[slot] = L.x;
   B.L[C + slot] = L.y;
   B.L[2 * C + slot] = L.z;
@@ -355,7 +363,7 @@ static inline unsigned grid_for_block(uint32_t n, int bs) { return (n + bs - 1) 
 cudaError_t launch_wf_shade(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                             const WfBuffers& B, int cur, cudaStream_t s, const DevAdjoint* A, int block) {
   DevRender S{geo, rd};
-  const bool lights = rd.num_delta_lights > 0;
+  const bool lights = rd.num_extra_lights > 0;
   const DevAdjoint none{};
   if (A)  // one instantiation for the adjoint, with the delta-light paths
     wf_shade<true, false, kWfBlock, true><<<grid_for(B.capacity), kWfBlock, 0, s>>>(S, P, B, cur, *A, nullptr);

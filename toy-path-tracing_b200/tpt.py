@@ -149,6 +149,11 @@ class DirectionalLightDesc(C.Structure):
 LIGHT_LEAF_POINT, LIGHT_LEAF_SPOT = 0xFFFFFFFE, 0xFFFFFFFD  # tree leaf codes (tpt.h)
 
 
+class EnvironmentDesc(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("pixels", C.c_void_p), ("scale", C.c_float),
+                ("rotate_y", C.c_float)]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("meshes", C.POINTER(MeshDesc)),
@@ -165,6 +170,7 @@ class SceneDesc(C.Structure):
         ("num_spot_lights", C.c_uint32),
         ("directional_lights", C.POINTER(DirectionalLightDesc)),
         ("num_directional_lights", C.c_uint32),
+        ("environment", C.POINTER(EnvironmentDesc)),
     ]
 
 
@@ -495,8 +501,16 @@ def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None, li
         ltv = LightTreeView(nodes.ctypes.data, len(nodes), root)
     (pa, npts), (sa, nsp), (da, ndir) = light_descs(lights or {})
     keep += [md, idesc, mdesc, pa, sa, da]
+    env = (lights or {}).get("environment")
+    env_ptr = None
+    if env is not None:
+        px = np.ascontiguousarray(env["pixels"], np.float32)
+        ed = EnvironmentDesc(px.shape[1], px.shape[0], px.ctypes.data, float(np.float32(env.get("scale", 1.0))),
+                             float(np.float32(env.get("rotate_y", 0.0))))
+        keep += [px, ed]
+        env_ptr = C.pointer(ed)
     desc = SceneDesc(md, len(meshes), idesc, len(instances), _view(tlas), mdesc, len(materials), ltv,
-                     pa, npts, sa, nsp, da, ndir)
+                     pa, npts, sa, nsp, da, ndir, env_ptr)
     return desc, keep
 
 
@@ -522,7 +536,8 @@ class Scene:
     uvs and a pre-built qbvh (nodes, prims).  instances: list of dicts with
     mesh, material, local_to_world, world_to_local (4x4 column-major) and
     normal_to_world (3x3).  lights: a dict (e.g. the scene dict) with optional
-    "point_lights", "spot_lights" and "directional_lights" lists."""
+    "point_lights", "spot_lights" and "directional_lights" lists and an
+    "environment" dict (pixels [H, W, 3], scale, rotate_y)."""
 
     def __init__(self, ctx: Context, meshes, instances, tlas=None, materials=None, light_tree=None, lights=None):
         self.ctx = ctx

@@ -221,6 +221,35 @@ def cornell_lights(seed: int = 1, material: int = LAMBERT, area: bool = True):
     return sc
 
 
+def sky_environment(width: int = 64, height: int = 32, sun=(3, 10), sun_radiance: float = 60.0,
+                    scale: float = 1.0, rotate_y: float = 0.0) -> dict:
+    """A procedural equirectangular sky (row 0 at +y): a blue gradient above
+    the horizon, a dark ground below, and a 2 x 2-texel sun."""
+    v = (np.arange(height, dtype=np.float32) + 0.5) / height
+    zenith = np.array([0.25, 0.45, 0.9], np.float32)
+    horizon = np.array([0.9, 0.85, 0.75], np.float32)
+    ground = np.array([0.06, 0.05, 0.04], np.float32)
+    t = np.clip(v / 0.5, 0.0, 1.0)[:, None]
+    rows = np.where((v < 0.5)[:, None], (1.0 - t) * zenith + t * horizon, ground)
+    px = np.repeat(rows[:, None, :], width, axis=1).astype(np.float32)
+    i, j = sun
+    px[j:j + 2, i:i + 2] = sun_radiance
+    return {"pixels": px, "scale": scale, "rotate_y": rotate_y}
+
+
+def cornell_environment(seed: int = 1, material: int = LAMBERT, area: bool = True, **sky):
+    """The Cornell box (open at the front) under the procedural sky, rotated so
+    that the sun shines in through the opening."""
+    sc = cornell_box(seed, material)
+    if not area:
+        sc["meshes"] = sc["meshes"][:-1]
+        sc["materials"] = sc["materials"][:-1]
+        sc["instances"] = sc["instances"][:-1]
+    sky.setdefault("rotate_y", 0.35)
+    sc["environment"] = sky_environment(**sky)
+    return sc
+
+
 # ---------------------------------------------------------------------------
 # Differentiable-render scene: the Cornell box with its five walls split into
 # 3 x 4 patches each (60 patches, every patch a 4 x 4 grid of quads) and each
