@@ -27,7 +27,6 @@
 namespace tpt {
 
 constexpr int kBdWfBlock = 128;
-constexpr int kBdShStack = 32;
 
 // Warp-exclusive prefix sum of `v` (all lanes call); returns the lane's offset
 // and the warp total in `total`.
