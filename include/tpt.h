@@ -260,9 +260,9 @@ typedef struct tpt_scene_desc {
    * point lights, then the spot lights. */
   tpt_light_tree_view light_tree;
   /* Scene::point_lights / spot_lights / directional_lights (may be NULL when
-   * the count is 0).  BDPT jobs reject scenes with lights that are not
-   * emissive triangles, the environment included (the device BDPT covers
-   * area lights only). */
+   * the count is 0).  In BDPT, as in the reference, light subpaths start on
+   * emissive triangles only; these lights (and the environment) reach BDPT
+   * through one light sample per camera vertex (bdpt.rs:207-221, 396-464). */
   const tpt_point_light_desc* point_lights;
   uint32_t num_point_lights;
   const tpt_spot_light_desc* spot_lights;

@@ -87,7 +87,8 @@ def _declare(L):
         "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u32, u64, u64, vp, i32]),
         "orc_render_adjoint": (None, [vp, vp, u32, u32, u32, u32, vp, u32, C.c_float, vp, i32]),
         "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
-        "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, f32, vp]),
+        "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, f32, vp, i32]),
+        "orc_render_env_escape": (None, [vp, vp, vp, f32, i32, vp]),
         "orc_render_scene_set_lights": (None, [vp, vp, u32, vp, u32, vp, u32]),
         "orc_render_scene_set_environment": (None, [vp, u32, u32, vp, f32, f32]),
         "orc_env_create": (vp, [u32, u32, vp, f32, f32]),
@@ -369,8 +370,8 @@ class RenderScene:
                          camera.get("exposure", 1.0)], np.float32)
 
     def _check_integrator(self, integrator):
-        if integrator == 1 and self.non_area_lights:
-            raise ValueError("the oracle's BDPT covers area lights only (no point, spot, directional or environment)")
+        if integrator not in (0, 1):
+            raise ValueError("integrator: 0 MIS, 1 BDPT")
 
     def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0):
         """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3].
@@ -404,12 +405,21 @@ class RenderScene:
         return out
 
     # -- unit-level queries (reference integrator unit tests) -------------------
-    def direct_light(self, inst, tri, bary, incident, u_tree, us, u_category=0.0):
+    def direct_light(self, inst, tri, bary, incident, u_tree, us, u_category=0.0, non_area_only=False):
+        """MIS NEE (mis.rs:145-210); non_area_only: BDPT's non-area NEE (bdpt.rs:396-464)."""
         out = np.zeros(3, np.float32)
         b = np.asarray(bary, np.float32)
         d = np.asarray(incident, np.float32)
         lib().orc_render_direct_light(self.h, inst, tri, _p(b), _p(d), float(u_category), float(u_tree),
-                                      float(us[0]), float(us[1]), _p(out))
+                                      float(us[0]), float(us[1]), _p(out), int(non_area_only))
+        return out
+
+    def env_escape(self, direction, throughput, bsdf_pdf, delta=False):
+        """Environment radiance for an escaping BSDF sample, MIS-weighted (mis.rs:238-258)."""
+        out = np.zeros(3, np.float32)
+        d = np.asarray(direction, np.float32)
+        t = np.asarray(throughput, np.float32)
+        lib().orc_render_env_escape(self.h, _p(d), _p(t), float(bsdf_pdf), int(delta), _p(out))
         return out
 
     def emitted(self, inst, tri, bary, incident, linst, ltri, lbary, lincident, throughput, bsdf_pdf, delta=False):

@@ -159,10 +159,15 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
   bool have_pending = false;
   Vec3 pending_from;
   float pending_pdf = 0.0f;
+  const bool non_area = scene_has_non_area_lights(s);
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sp.path_vertex_randoms(depth);
     SceneHit h;
-    if (!closest(s, ro, rd, &h)) break;  // infinite light: none
+    if (!closest(s, ro, rd, &h)) {
+      // emitted_radiance_from_infinite_hit (bdpt.rs:466-486)
+      L += beta * env_escape(s, rd, count_emission, pending_pdf);
+      break;
+    }
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
     const Material& m = s.mat_of(h.instance);
     PathVertex pv;
@@ -179,6 +184,8 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
       float w = count_emission ? 1.0f : camera_light_hit_mis_weight(s, vs);
       L += beta * le * w;
     }
+    // direct_non_area_light_contribution (bdpt.rs:207-221, 396-464)
+    if (non_area && !is_pure_emitter(m)) L += beta * direct_light(s, m, v, rnd, nullptr, true);
     MatSampleOut smp;
     if (!material_sample(m, v, rnd.material, kRadiance, &smp)) break;
     vs[vi].delta = smp.delta;

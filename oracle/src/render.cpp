@@ -358,8 +358,8 @@ int sample_category(const RenderScene& s, float u, float* pmf) {
 // diffuse material is the only one in scope that builds one); directional
 // lights serve every scattering material.  Delta lights take no MIS weight.
 // wi_out (optional) receives the sampled light direction.
-Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
-                  Vec3* wi_out = nullptr) {
+Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
+                       Vec3* wi_out, bool non_area_only) {
   float cat_pmf = 0.0f;
   int cat = sample_category(s, rnd.light.u_category, &cat_pmf);
   if (cat == -2) return Vec3(0, 0, 0);  // no category
@@ -382,6 +382,8 @@ Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, cons
     } else if (li_inst == kLeafSpot) {
       if (!sample_li_spot(s.spots[li_tri], v.p, &li)) return Vec3(0, 0, 0);
     } else {
+      // bdpt.rs:424-426: BDPT's camera vertices take no area-light samples here
+      if (non_area_only) return Vec3(0, 0, 0);
       if (!sample_li_triangle(s, (int)li_inst, (int)li_tri, v.p, rnd.light.u_surface, &li)) return Vec3(0, 0, 0);
       delta = false;
     }
@@ -466,6 +468,11 @@ float light_pdf_for_hit(const RenderScene& s, const Material& shading, const Ver
 }
 
 }  // namespace
+
+Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd, Vec3* wi_out,
+                  bool non_area_only) {
+  return direct_light_impl(s, m, v, rnd, wi_out, non_area_only);
+}
 
 // orthonormal_basis.rs:11-56
 Frame Frame::from_normal(Vec3 normal) {
@@ -608,9 +615,10 @@ Vertex RenderScene::shading_vertex(int inst, int tri, Vec3 b, Vec3 incident) con
   return v;
 }
 
-// emitted_radiance_from_bsdf_sample_infinite (integrator/mis.rs:238-258) with
-// pdf_for_environment_hit (light/mod.rs:439-450, MIS-compensated), without the
-// path throughput
+// emitted_radiance_from_bsdf_sample_infinite (integrator/mis.rs:238-258; in
+// BDPT emitted_radiance_from_infinite_hit, bdpt.rs:466-486, with `delta` = count
+// the full emission) with pdf_for_environment_hit (light/mod.rs:439-450,
+// MIS-compensated), without the path throughput
 Vec3 env_escape(const RenderScene& s, Vec3 dir, bool delta, float bsdf_pdf) {
   if (!s.has_env) return Vec3(0, 0, 0);  // infinite_light_le without an environment
   const Vec3 le = s.env.radiance(dir);
@@ -747,9 +755,10 @@ void render_samples(const RenderScene& s, const RenderJob& job, uint64_t first, 
 extern "C" {
 
 // direct_light_mis_contribution at the shading vertex of (inst, tri, bary) seen
-// along `incident` (integrator/mis.rs:145-210).
+// along `incident` (integrator/mis.rs:145-210); non_area_only != 0: BDPT's
+// direct_non_area_light_contribution (integrator/bdpt.rs:396-464).
 void orc_render_direct_light(void* h, int inst, int tri, const float* bary3, const float* incident3, float u_cat,
-                             float u_tree, float us0, float us1, float* out3) {
+                             float u_tree, float us0, float us1, float* out3, int non_area_only) {
   using namespace orc;
   const RenderScene& s = *(const RenderScene*)h;
   Vertex v = s.shading_vertex(inst, tri, Vec3(bary3[0], bary3[1], bary3[2]),
@@ -758,7 +767,18 @@ void orc_render_direct_light(void* h, int inst, int tri, const float* bary3, con
   rnd.light.u_category = u_cat;
   rnd.light.u_tree = u_tree;
   rnd.light.u_surface = Vec2(us0, us1);
-  Vec3 r = direct_light(s, s.mat_of(inst), v, rnd);
+  Vec3 r = direct_light(s, s.mat_of(inst), v, rnd, nullptr, non_area_only != 0);
+  out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
+}
+
+// The environment's contribution to a ray that left the scene after a BSDF
+// sample (integrator/mis.rs:238-258, bdpt.rs:466-486), times `throughput3`.
+void orc_render_env_escape(void* h, const float* dir3, const float* throughput3, float bsdf_pdf, int delta,
+                           float* out3) {
+  using namespace orc;
+  const RenderScene& s = *(const RenderScene*)h;
+  const Vec3 r = Vec3(throughput3[0], throughput3[1], throughput3[2]) *
+                 env_escape(s, Vec3(dir3[0], dir3[1], dir3[2]), delta != 0, bsdf_pdf);
   out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
 }
 

@@ -137,6 +137,20 @@ bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& 
 bool material_le(const Material& m, Vec3* le);  // Emissive only (two-sided)
 inline bool is_pure_emitter(const Material& m) { return m.kind == kEmissive; }
 
+// direct_light_mis_contribution (integrator/mis.rs:145-210); non_area_only:
+// direct_non_area_light_contribution (integrator/bdpt.rs:396-464), zero when
+// the sampled light is an area light.  wi_out (optional): the light direction.
+Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
+                  Vec3* wi_out = nullptr, bool non_area_only = false);
+// The environment's radiance along `dir` for a ray that left the scene after a
+// BSDF sample of pdf `bsdf_pdf` (`delta`: count it in full), MIS-weighted
+// against the environment's NEE pdf; zero without an environment.
+Vec3 env_escape(const RenderScene& s, Vec3 dir, bool delta, float bsdf_pdf);
+// Scene::environment_light, point, spot or directional lights (bdpt.rs:131-136)
+inline bool scene_has_non_area_lights(const RenderScene& s) {
+  return s.has_env || !s.points.empty() || !s.dirs.empty() || !s.spots.empty();
+}
+
 // mis::trace_radiance for one sample
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
 // bdpt::trace_radiance for one sample (integrator/bdpt.rs:70-131)

@@ -29,10 +29,6 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
     return set_error(ctx, TPT_ERR_INVALID_ARG, "width, height and spp must be positive");
   if (job->integrator != TPT_INTEGRATOR_MIS && job->integrator != TPT_INTEGRATOR_BDPT)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown integrator");
-  if (job->integrator == TPT_INTEGRATOR_BDPT && job->scene->render.num_extra_lights > 0)
-    return set_error(ctx, TPT_ERR_INVALID_ARG,
-                     "BDPT with point, spot, directional or environment lights is not on the device path "
-                     "(area lights only)");
   if (job->integrator == TPT_INTEGRATOR_BDPT && job->max_depth > kBdptMaxDepthApi)
     return set_error(ctx, TPT_ERR_CAPACITY,
                      "BDPT max_depth " + std::to_string(job->max_depth) + " above the device limit of " +

@@ -1,7 +1,10 @@
-// Bidirectional path tracing on the device, integrator/bdpt.rs:70-791, for
-// area lights (the light type in scope): camera subpath, light subpath from an
-// emissive triangle picked by power, and every connection between their
-// connectible vertices with a visibility ray and the reference's MIS weight.
+// Bidirectional path tracing on the device, integrator/bdpt.rs:70-791: camera
+// subpath, light subpath from an emissive triangle picked by power, and every
+// connection between their connectible vertices with a visibility ray and the
+// reference's MIS weight.  Point, spot, directional and environment lights take
+// no part in the light subpaths: as in the reference, each camera vertex of a
+// scene that has them takes one light sample that skips area lights, and a
+// camera ray that leaves the scene reads the environment.
 // Both subpaths live in the thread's local memory (interleaved across the warp
 // by the hardware, so vertex k of every lane is one coalesced line).
 #pragma once
@@ -256,14 +259,21 @@ __device__ __forceinline__ void camera_state_init(BdCamState& c, bool valid) {
   c.alive = valid;
 }
 
-// One iteration of the camera loop (bdpt.rs:135-262; no environment or
-// non-area lights in scope) after its ray (rd) was traced to h: the hit vertex
-// into vs[c.n], emission into L, and the next ray into (ro, rd) while c.alive.
+// One iteration of the camera loop (bdpt.rs:135-262) after its ray (rd) was
+// traced to h: the hit vertex into vs[c.n], emission (or, for a ray that left
+// the scene, the environment) into L, and the next ray into (ro, rd) while
+// c.alive.  In a scene with lights that are not emissive triangles, `nee` says
+// whether the vertex took such a light sample (bdpt.rs:207-221): its
+// contribution, times the path throughput, counts into L once the shadow ray
+// of `dp` is found unoccluded, before the next iteration adds anything.
 template <class Stack>
 __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaunch& P, const PathSamplerDev& ps,
                                             uint32_t depth, const TraceResult& h, V3& ro, V3& rd, BdVertex* vs,
-                                            BdCamState& c, V3& L) {
+                                            BdCamState& c, V3& L, bool& nee, DirectPrep& dp) {
+  nee = false;
   if (h.tri < 0) {
+    // emitted_radiance_from_infinite_hit (bdpt.rs:466-486)
+    if (S.d.has_env) L = L + c.beta * env_escape(S.d, rd, c.count_emission, false, c.pending_pdf);
     c.alive = false;
     return;
   }
@@ -281,6 +291,14 @@ __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaun
     L = L + c.beta * emissive_le(m) * w;
     c.alive = false;  // pure emitter: sample() is None
     return;
+  }
+  if (S.d.num_extra_lights > 0) {  // direct_non_area_light_contribution
+    float us0, us1;
+    ps.sample_2d(vertex_dim(depth, kOffSurface), us0, us1);
+    const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
+    const float u_cat = S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(depth, kOffCategory)) : 0.0f;
+    nee = prepare_direct<true, true>(S, m, v, u_cat, u_tree, us0, us1, dp);
+    if (nee) dp.contrib = c.beta * dp.contrib;
   }
   float ud0, ud1;
   ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
@@ -320,7 +338,17 @@ __device__ __forceinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stac
     if (!live) break;
     TraceResult h;
     if (c.alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
-    if (c.alive) camera_step<Stack>(S, P, ps, depth, h, ro, rd, vs, c, L);
+    bool nee = false;
+    DirectPrep dp;
+    if (c.alive) camera_step<Stack>(S, P, ps, depth, h, ro, rd, vs, c, L, nee, dp);
+    const unsigned sm = __ballot_sync(0xffffffffu, nee);
+    if (sm) {  // the light samples' shadow rays (unoccluded, integrator/mod.rs:239-265)
+      TraceResult hs;
+      if (nee)
+        trace_ray_ww<0>(S.geo, st, sm, dp.so.x, dp.so.y, dp.so.z, dp.wi.x, dp.wi.y, dp.wi.z,
+                        __int_as_float(0x7f800000), hs, err);
+      if (nee && shadow_visible(hs.tri, hs.inst, hs.t, dp.inst, dp.tri, dp.dist)) L = L + dp.contrib;
+    }
   }
   return c.n;
 }

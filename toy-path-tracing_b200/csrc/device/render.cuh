@@ -428,7 +428,9 @@ struct DirectPrep {
 // emissive triangles: the light sampler then has the Tree category alone (pmf
 // tree_cat_pmf = 1, or no category without a tree) and every tree leaf is a
 // triangle, so the category draw and the delta-light paths are compiled out.
-template <bool LIGHTS>
+// NON_AREA: BDPT's direct_non_area_light_contribution (integrator/bdpt.rs:
+// 396-464), which returns zero when the sampled light is an area light.
+template <bool LIGHTS, bool NON_AREA = false>
 __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
                                                float u_cat, float u_tree, float us0, float us1, DirectPrep& out) {
   float cat_pmf;
@@ -460,6 +462,7 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
     if (LIGHTS && (li_inst == kLeafPointDev || li_inst == kLeafSpotDev)) {
       if (!sample_li_delta(S.d, li_inst == kLeafPointDev ? 0u : 1u, li_tri, v.p, li)) return false;
     } else {
+      if (NON_AREA) return false;
       if (!sample_li_triangle(S, li_inst, li_tri, v.p, us0, us1, li)) return false;
       delta = false;
       out.inst = li.inst;

@@ -6,7 +6,11 @@
 //                  one iteration of the camera loop (depth = step) or of the
 //                  light loop (depth = step + 1) per queued ray, vertices into
 //                  HBM, camera-side emission into L0, next rays into the other
-//                  queue (the same step functions the one-kernel BDPT runs)
+//                  queue (the same step functions the one-kernel BDPT runs);
+//                  in scenes with point, spot, directional or environment
+//                  lights, the camera vertices' light samples queue a shadow
+//                  ray, traversed after the step, and bd_nee_resolve adds the
+//                  unoccluded ones to L0 before the next step
 //   bd_pairs     : per sample, its nl * nc connection slots allocated
 //                  contiguously in the pair queue (one atomic per warp)
 //   bd_connect   : per pair, bdpt_connect_prepare; non-zero contributions
@@ -139,10 +143,12 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_step(const __grid_constant__ De
   V3 rd = V3{r[3 * Q + j], r[4 * Q + j], r[5 * Q + j]};
   BdVertex* cam = B.verts + (size_t)i * 2 * B.max_vertices;
   bool next = false;
+  bool nee = false;
+  DirectPrep dp;
   if (!light) {
     BdCamState c = B.cam_state[i];
     V3 L = V3{B.L0[3 * (size_t)i], B.L0[3 * (size_t)i + 1], B.L0[3 * (size_t)i + 2]};
-    camera_step<int>(S, P, ps, step, h, ro, rd, cam, c, L);
+    camera_step<int>(S, P, ps, step, h, ro, rd, cam, c, L, nee, dp);
     B.cam_state[i] = c;
     B.L0[3 * (size_t)i] = L.x;
     B.L0[3 * (size_t)i + 1] = L.y;
@@ -156,6 +162,37 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_step(const __grid_constant__ De
   }
   const uint32_t q = warp_append1(&B.counts[2 + (cur ^ 1)], next);
   if (next) push_ray(B, cur ^ 1, q, ro, rd, tag);
+  // a camera vertex's light sample: its shadow ray into the visibility queue
+  // (free until the connection stage), contribution and light distance beside it
+  const uint32_t qs = warp_append1(&B.counts[1], nee);
+  if (!nee) return;
+  const uint32_t C = B.pair_capacity;
+  float* sr = B.s_ray;
+  sr[qs] = dp.so.x;
+  sr[C + qs] = dp.so.y;
+  sr[2 * C + qs] = dp.so.z;
+  sr[3 * C + qs] = dp.wi.x;
+  sr[4 * C + qs] = dp.wi.y;
+  sr[5 * C + qs] = dp.wi.z;
+  sr[6 * C + qs] = __int_as_float(0x7f800000);
+  B.s_pair[qs] = i;
+  B.c[3 * (size_t)qs] = dp.contrib.x;
+  B.c[3 * (size_t)qs + 1] = dp.contrib.y;
+  B.c[3 * (size_t)qs + 2] = dp.contrib.z;
+  B.dist[qs] = dp.dist;
+}
+
+// The camera vertices' light samples of one step whose shadow rays are
+// unoccluded (unoccluded_ray, integrator/mod.rs:239-265; point, spot,
+// directional and environment lights have no target triangle) into L0.
+__global__ void __launch_bounds__(kBdWfBlock) bd_nee_resolve(BdWfBuffers B) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= B.counts[1]) return;
+  if (!shadow_visible(B.s_tri[e], B.s_inst[e], B.s_t[e], 0xFFFFFFFFu, 0xFFFFFFFFu, B.dist[e])) return;
+  const uint32_t i = B.s_pair[e];
+  B.L0[3 * (size_t)i] = B.L0[3 * (size_t)i] + B.c[3 * (size_t)e];
+  B.L0[3 * (size_t)i + 1] = B.L0[3 * (size_t)i + 1] + B.c[3 * (size_t)e + 1];
+  B.L0[3 * (size_t)i + 2] = B.L0[3 * (size_t)i + 2] + B.c[3 * (size_t)e + 2];
 }
 
 // Per sample: subpath lengths and the nl * nc connection slots, contiguous
@@ -267,6 +304,7 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
   if ((e = cudaMemsetAsync(B.counts + 2, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
   bd_init<<<grid_of(n), kBdWfBlock, 0, s>>>(S, P, B, first_path, n);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const bool lights = rd.num_extra_lights > 0;
   for (uint32_t step = 0; step < P.max_depth; ++step) {
     const int cur = (int)(step & 1u);
     if ((e = cudaMemsetAsync(B.counts + 2 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
@@ -275,6 +313,15 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
     if (e != cudaSuccess) return e;
     bd_step<<<grid_of(Q), kBdWfBlock, 0, s>>>(S, P, B, first_path, step, cur);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (lights) {  // at most one light sample per sample and step: n <= sample_capacity <= pair_capacity
+      e = launch_traverse_strided(geo, B.s_ray, B.pair_capacity, B.pair_capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t,
+                                  B.s_inst, nullptr, B.pair_capacity, counter, err, num_sms, s, nullptr, nullptr,
+                                  B.counts + 1);
+      if (e != cudaSuccess) return e;
+      bd_nee_resolve<<<grid_of(B.sample_capacity), kBdWfBlock, 0, s>>>(B);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(B.counts + 1, 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+    }
   }
   bd_pairs<<<grid_of(n), kBdWfBlock, 0, s>>>(B, n);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
