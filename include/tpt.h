@@ -326,13 +326,19 @@ tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, c
 /* Rendering (`IntegratorKind::trace_radiance` per sample, main.rs:99-126 loop) */
 
 typedef enum tpt_integrator {
-  TPT_INTEGRATOR_MIS = 0, /* integrator/mis.rs: BSDF sampling + light-tree NEE, balance heuristic */
+  TPT_INTEGRATOR_MIS = 0, /* integrator/mis.rs: BSDF sampling + light sampling, balance heuristic */
   /* integrator/bdpt.rs: camera and light subpaths, every connection between
    * them, balance-heuristic MIS over the strategies (area lights picked by
-   * power).  Runs as one thread per sample whatever `execution` says; the
-   * device keeps both subpaths on chip, so max_depth is limited to 16
+   * power; other lights through one light sample per camera vertex).  The
+   * wavefront (subpath steps, connection queue) unless `execution` is
+   * TPT_EXEC_MEGAKERNEL (one thread per sample); max_depth is limited to 16
    * (TPT_ERR_CAPACITY above). */
-  TPT_INTEGRATOR_BDPT = 1
+  TPT_INTEGRATOR_BDPT = 1,
+  /* integrator/nee.rs: light sampling without MIS (emitters and the
+   * environment count only from the camera and after delta samples). */
+  TPT_INTEGRATOR_NEE = 2,
+  /* integrator/pt.rs: BSDF sampling only; every emitter hit and escape counts. */
+  TPT_INTEGRATOR_PT = 3
 } tpt_integrator;
 
 /* PinholeCamera::new(eye, look_at, up, fov_y, exposure) (scene/camera.rs:21-39). */

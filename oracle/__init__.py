@@ -370,12 +370,13 @@ class RenderScene:
                          camera.get("exposure", 1.0)], np.float32)
 
     def _check_integrator(self, integrator):
-        if integrator not in (0, 1):
-            raise ValueError("integrator: 0 MIS, 1 BDPT")
+        if integrator not in (0, 1, 2, 3):
+            raise ValueError("integrator: 0 MIS, 1 BDPT, 2 NEE, 3 PT")
 
     def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0):
         """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3].
-        integrator: 0 MIS (integrator/mis.rs), 1 BDPT (integrator/bdpt.rs)."""
+        integrator: 0 MIS (integrator/mis.rs), 1 BDPT (integrator/bdpt.rs), 2 NEE
+        (integrator/nee.rs), 3 PT (integrator/pt.rs)."""
         self._check_integrator(integrator)
         p0, p1 = pixels if pixels is not None else (0, width * height)
         out = np.empty((p1 - p0, 3), np.float32)
@@ -405,13 +406,15 @@ class RenderScene:
         return out
 
     # -- unit-level queries (reference integrator unit tests) -------------------
-    def direct_light(self, inst, tri, bary, incident, u_tree, us, u_category=0.0, non_area_only=False):
-        """MIS NEE (mis.rs:145-210); non_area_only: BDPT's non-area NEE (bdpt.rs:396-464)."""
+    def direct_light(self, inst, tri, bary, incident, u_tree, us, u_category=0.0, non_area_only=False, nee=False):
+        """MIS light sampling (mis.rs:145-210); non_area_only: BDPT's non-area
+        light sampling (bdpt.rs:396-464); nee: the NEE integrator's (nee.rs:104-150)."""
         out = np.zeros(3, np.float32)
         b = np.asarray(bary, np.float32)
         d = np.asarray(incident, np.float32)
+        mode = 2 if nee else (1 if non_area_only else 0)
         lib().orc_render_direct_light(self.h, inst, tri, _p(b), _p(d), float(u_category), float(u_tree),
-                                      float(us[0]), float(us[1]), _p(out), int(non_area_only))
+                                      float(us[0]), float(us[1]), _p(out), mode)
         return out
 
     def env_escape(self, direction, throughput, bsdf_pdf, delta=False):

@@ -185,7 +185,7 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
       L += beta * le * w;
     }
     // direct_non_area_light_contribution (bdpt.rs:207-221, 396-464)
-    if (non_area && !is_pure_emitter(m)) L += beta * direct_light(s, m, v, rnd, nullptr, true);
+    if (non_area && !is_pure_emitter(m)) L += beta * direct_light(s, m, v, rnd, nullptr, kDirectBdptNonArea);
     MatSampleOut smp;
     if (!material_sample(m, v, rnd.material, kRadiance, &smp)) break;
     vs[vi].delta = smp.delta;

@@ -359,7 +359,8 @@ int sample_category(const RenderScene& s, float u, float* pmf) {
 // lights serve every scattering material.  Delta lights take no MIS weight.
 // wi_out (optional) receives the sampled light direction.
 Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
-                       Vec3* wi_out, bool non_area_only) {
+                       Vec3* wi_out, int mode) {
+  const bool non_area_only = mode == kDirectBdptNonArea, nee = mode == kDirectNee;
   float cat_pmf = 0.0f;
   int cat = sample_category(s, rnd.light.u_category, &cat_pmf);
   if (cat == -2) return Vec3(0, 0, 0);  // no category
@@ -389,9 +390,12 @@ Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v,
     }
     sel = cat_pmf * leaf_pmf;
   } else if (cat == -3) {
-    // environment::sample_li_mis_compensated (light/environment.rs:258-273)
+    // environment::sample_li_mis_compensated (light/environment.rs:258-273);
+    // the NEE integrator's sample_light draws from the plain distribution
     EnvSample es;
-    if (!s.env.sample_mis_compensated(rnd.light.u_surface.x, rnd.light.u_surface.y, &es)) return Vec3(0, 0, 0);
+    const bool ok = nee ? s.env.sample(rnd.light.u_surface.x, rnd.light.u_surface.y, &es)
+                        : s.env.sample_mis_compensated(rnd.light.u_surface.x, rnd.light.u_surface.y, &es);
+    if (!ok) return Vec3(0, 0, 0);
     if (es.pdf <= 0.0f) return Vec3(0, 0, 0);
     li.radiance = es.radiance;
     li.wi = es.direction;
@@ -413,7 +417,7 @@ Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v,
   if (li.pdf <= 0.0f || sel <= 0.0f) return Vec3(0, 0, 0);
   Vec3 f;
   float bsdf_pdf = 0.0f;
-  if (delta) {
+  if (delta || nee) {  // nee.rs:140: Material::eval, no MIS weight
     f = m.kind == kLambert ? lambert_eval(m, v, li.wi) : material_eval(m, v, li.wi, kRadiance);
   } else if (m.kind == kLambert) {
     f = lambert_eval(m, v, li.wi);
@@ -437,7 +441,7 @@ Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v,
   float pdf_total = sel * li.pdf;
   if (pdf_total <= 0.0f) return Vec3(0, 0, 0);
   if (wi_out) *wi_out = li.wi;
-  if (delta) return li.radiance * f * (cos_surface / pdf_total);
+  if (delta || nee) return li.radiance * f * (cos_surface / pdf_total);
   float mis = balance(pdf_total, bsdf_pdf);
   return li.radiance * f * (cos_surface * mis / pdf_total);
 }
@@ -470,8 +474,8 @@ float light_pdf_for_hit(const RenderScene& s, const Material& shading, const Ver
 }  // namespace
 
 Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd, Vec3* wi_out,
-                  bool non_area_only) {
-  return direct_light_impl(s, m, v, rnd, wi_out, non_area_only);
+                  int mode) {
+  return direct_light_impl(s, m, v, rnd, wi_out, mode);
 }
 
 // orthonormal_basis.rs:11-56
@@ -628,6 +632,74 @@ Vec3 env_escape(const RenderScene& s, Vec3 dir, bool delta, float bsdf_pdf) {
   return le * balance(bsdf_pdf, light_pdf);
 }
 
+// integrator/pt.rs:15-76: BSDF sampling only; every emitter hit and every
+// escape counts in full
+Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
+  Vec3 L(0, 0, 0), beta(1, 1, 1);
+  Vec3 ro = ray.origin, rd = ray.direction;
+  for (uint32_t depth = 0; depth < max_depth; ++depth) {
+    VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    SceneHit h;
+    if (!closest(s, ro, rd, &h)) {
+      if (s.has_env) L += beta * s.env.radiance(rd);  // infinite_light_le
+      break;
+    }
+    Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
+    const Material& m = s.mat_of(h.instance);
+    if (m.kind == kEmissive) L += beta * emissive_le(m);
+    MatSample bs;
+    bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+              : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
+                                   : false;  // the pure emitter samples nothing
+    if (!ok) break;
+    beta *= bs.weight;
+    if (depth + 1 >= 4) {
+      float q = clampf(max_element(beta), 0.05f, 1.0f);
+      if (rnd.u_rr > q) break;
+      beta /= q;
+    }
+    ro = offset_origin(v.p, v.ng, bs.wi);
+    rd = bs.wi;
+  }
+  return L;
+}
+
+// integrator/nee.rs:15-93: light sampling without MIS (sample_light, the
+// plain environment distribution), emission and escapes counted only from
+// the camera and after delta samples
+Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
+  Vec3 L(0, 0, 0), beta(1, 1, 1);
+  Vec3 ro = ray.origin, rd = ray.direction;
+  bool count_emission = true;
+  for (uint32_t depth = 0; depth < max_depth; ++depth) {
+    VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    SceneHit h;
+    if (!closest(s, ro, rd, &h)) {
+      if (count_emission && s.has_env) L += beta * s.env.radiance(rd);
+      break;
+    }
+    Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
+    const Material& m = s.mat_of(h.instance);
+    if (count_emission && m.kind == kEmissive) L += beta * emissive_le(m);
+    if (m.kind != kEmissive) L += beta * direct_light_impl(s, m, v, rnd, nullptr, kDirectNee);
+    MatSample bs;
+    bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+              : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
+                                   : false;
+    if (!ok) break;
+    beta *= bs.weight;
+    if (depth + 1 >= 4) {
+      float q = clampf(max_element(beta), 0.05f, 1.0f);
+      if (rnd.u_rr > q) break;
+      beta /= q;
+    }
+    ro = offset_origin(v.p, v.ng, bs.wi);
+    rd = bs.wi;
+    count_emission = bs.delta;
+  }
+  return L;
+}
+
 // integrator/mis.rs:19-139
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
   Vec3 L(0, 0, 0), beta(1, 1, 1);
@@ -718,7 +790,12 @@ Vec3 one_sample(const RenderScene& s, const RenderJob& job, uint32_t pixel, uint
   PathSampler ps(px, py, sample, job.spp, job.width, job.height);
   Vec2 us = ps.camera_sample();
   Ray r = job.cam.generate_ray_differential(job.width, job.height, px, py, us, job.spp);
-  return job.integrator == 1 ? trace_bdpt(s, r, ps, job.max_depth) : trace_mis(s, r, ps, job.max_depth);
+  switch (job.integrator) {
+    case 1: return trace_bdpt(s, r, ps, job.max_depth);
+    case 2: return trace_nee(s, r, ps, job.max_depth);
+    case 3: return trace_pt(s, r, ps, job.max_depth);
+    default: return trace_mis(s, r, ps, job.max_depth);
+  }
 }
 }  // namespace
 
@@ -755,10 +832,11 @@ void render_samples(const RenderScene& s, const RenderJob& job, uint64_t first, 
 extern "C" {
 
 // direct_light_mis_contribution at the shading vertex of (inst, tri, bary) seen
-// along `incident` (integrator/mis.rs:145-210); non_area_only != 0: BDPT's
-// direct_non_area_light_contribution (integrator/bdpt.rs:396-464).
+// along `incident` (integrator/mis.rs:145-210); mode 1: BDPT's
+// direct_non_area_light_contribution (integrator/bdpt.rs:396-464); mode 2: the
+// NEE integrator's direct_light_nee_contribution (integrator/nee.rs:104-150).
 void orc_render_direct_light(void* h, int inst, int tri, const float* bary3, const float* incident3, float u_cat,
-                             float u_tree, float us0, float us1, float* out3, int non_area_only) {
+                             float u_tree, float us0, float us1, float* out3, int mode) {
   using namespace orc;
   const RenderScene& s = *(const RenderScene*)h;
   Vertex v = s.shading_vertex(inst, tri, Vec3(bary3[0], bary3[1], bary3[2]),
@@ -767,7 +845,7 @@ void orc_render_direct_light(void* h, int inst, int tri, const float* bary3, con
   rnd.light.u_category = u_cat;
   rnd.light.u_tree = u_tree;
   rnd.light.u_surface = Vec2(us0, us1);
-  Vec3 r = direct_light(s, s.mat_of(inst), v, rnd, nullptr, non_area_only != 0);
+  Vec3 r = direct_light(s, s.mat_of(inst), v, rnd, nullptr, mode);
   out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
 }
 

@@ -120,7 +120,7 @@ struct RenderScene {
 struct RenderJob {
   Camera cam;
   uint32_t width, height, spp, max_depth;
-  uint32_t integrator = 0;  // 0 MIS, 1 BDPT
+  uint32_t integrator = 0;  // 0 MIS, 1 BDPT, 2 NEE, 3 PT
 };
 
 // Material interface (material/mod.rs:251-502) for the kinds in scope, with
@@ -137,11 +137,15 @@ bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& 
 bool material_le(const Material& m, Vec3* le);  // Emissive only (two-sided)
 inline bool is_pure_emitter(const Material& m) { return m.kind == kEmissive; }
 
-// direct_light_mis_contribution (integrator/mis.rs:145-210); non_area_only:
+// Light sampling at a scattering vertex.  kDirectMis:
+// direct_light_mis_contribution (integrator/mis.rs:145-210); kDirectBdptNonArea:
 // direct_non_area_light_contribution (integrator/bdpt.rs:396-464), zero when
-// the sampled light is an area light.  wi_out (optional): the light direction.
+// the sampled light is an area light; kDirectNee: direct_light_nee_contribution
+// (integrator/nee.rs:104-150), no MIS weight and the plain environment
+// distribution.  wi_out (optional): the light direction.
+enum DirectMode : int { kDirectMis = 0, kDirectBdptNonArea = 1, kDirectNee = 2 };
 Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
-                  Vec3* wi_out = nullptr, bool non_area_only = false);
+                  Vec3* wi_out = nullptr, int mode = kDirectMis);
 // The environment's radiance along `dir` for a ray that left the scene after a
 // BSDF sample of pdf `bsdf_pdf` (`delta`: count it in full), MIS-weighted
 // against the environment's NEE pdf; zero without an environment.
@@ -151,6 +155,9 @@ inline bool scene_has_non_area_lights(const RenderScene& s) {
   return s.has_env || !s.points.empty() || !s.dirs.empty() || !s.spots.empty();
 }
 
+// pt::trace_radiance and nee::trace_radiance for one sample
+Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
+Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
 // mis::trace_radiance for one sample
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth);
 // bdpt::trace_radiance for one sample (integrator/bdpt.rs:70-131)

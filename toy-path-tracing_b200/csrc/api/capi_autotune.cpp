@@ -54,8 +54,8 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     RenderLaunch L;
     tpt_status st = render_launch_params(ctx, &jobs[j], &L);
     if (st) return st;
-    if (jobs[j].integrator != TPT_INTEGRATOR_MIS)
-      return set_error(ctx, TPT_ERR_INVALID_ARG, "the autotuner covers MIS jobs");
+    if (jobs[j].integrator == TPT_INTEGRATOR_BDPT)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "the autotuner covers MIS, NEE and PT jobs");
     total += (uint64_t)L.width * L.height * L.spp;
   }
   struct Pilot {

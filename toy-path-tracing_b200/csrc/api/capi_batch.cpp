@@ -85,8 +85,8 @@ tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   for (int j = 0; j < n_jobs; ++j) {
     tpt_status st = render_launch_params(ctx, &jobs[j], &L[j]);
     if (st) return st;
-    if (jobs[j].integrator != TPT_INTEGRATOR_MIS)
-      return set_error(ctx, TPT_ERR_INVALID_ARG, "batched rendering covers the MIS integrator");
+    if (jobs[j].integrator == TPT_INTEGRATOR_BDPT)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "batched rendering covers the MIS, NEE and PT integrators");
     if (!out_rgb[j]) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output image for job " + std::to_string(j));
     std::memset(&dj[j], 0, sizeof(DevJob));
     dj[j].render = DevRender{jobs[j].scene->geo, jobs[j].scene->render};

@@ -27,7 +27,8 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
   if (!job || !job->scene) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL job or scene");
   if (job->width == 0 || job->height == 0 || job->spp == 0)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "width, height and spp must be positive");
-  if (job->integrator != TPT_INTEGRATOR_MIS && job->integrator != TPT_INTEGRATOR_BDPT)
+  if (job->integrator != TPT_INTEGRATOR_MIS && job->integrator != TPT_INTEGRATOR_BDPT &&
+      job->integrator != TPT_INTEGRATOR_NEE && job->integrator != TPT_INTEGRATOR_PT)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown integrator");
   if (job->integrator == TPT_INTEGRATOR_BDPT && job->max_depth > kBdptMaxDepthApi)
     return set_error(ctx, TPT_ERR_CAPACITY,
@@ -353,7 +354,7 @@ tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, 
   bool batch = n_jobs > 1;
   for (int j = 0; j < n_jobs && batch; ++j) {
     const uint32_t ex = jobs[j].execution == TPT_EXEC_AUTO ? ctx->tuned_execution : jobs[j].execution;
-    batch = jobs[j].integrator == TPT_INTEGRATOR_MIS && ex == TPT_EXEC_WAVEFRONT && out_rgb[j] && jobs[j].scene;
+    batch = jobs[j].integrator != TPT_INTEGRATOR_BDPT && ex == TPT_EXEC_WAVEFRONT && out_rgb[j] && jobs[j].scene;
   }
   if (batch) {
     std::vector<float*> d(n_jobs, nullptr);

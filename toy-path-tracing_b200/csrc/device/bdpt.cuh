@@ -297,7 +297,7 @@ __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaun
     ps.sample_2d(vertex_dim(depth, kOffSurface), us0, us1);
     const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
     const float u_cat = S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(depth, kOffCategory)) : 0.0f;
-    nee = prepare_direct<true, true>(S, m, v, u_cat, u_tree, us0, us1, dp);
+    nee = prepare_direct<true, kDirectBdptNonArea>(S, m, v, u_cat, u_tree, us0, us1, dp);
     if (nee) dp.contrib = c.beta * dp.contrib;
   }
   float ud0, ud1;

@@ -394,10 +394,12 @@ static __device__ __noinline__ V3 material_eval_pdf(const DevRender& S, const De
   return V3{0.0f, 0.0f, 0.0f};
 }
 
-// environment::sample_li_mis_compensated (light/environment.rs:258-273)
-static __device__ __noinline__ bool sample_li_env(const DevRenderData& d, float us0, float us1, LightSample& li) {
+// environment::sample_li_mis_compensated (light/environment.rs:258-273), or
+// with `plain` environment::sample_li (:241-256, the NEE integrator's)
+static __device__ __noinline__ bool sample_li_env(const DevRenderData& d, float us0, float us1, bool plain,
+                                                  LightSample& li) {
   float pdf;
-  if (!env_sample(d.env, d.env.mis, us0, us1, li.wi, li.radiance, pdf)) return false;
+  if (!env_sample(d.env, plain ? d.env.dist : d.env.mis, us0, us1, li.wi, li.radiance, pdf)) return false;
   if (pdf <= 0.0f) return false;
   li.pdf = pdf;
   li.distance = __int_as_float(0x7f800000);
@@ -428,11 +430,16 @@ struct DirectPrep {
 // emissive triangles: the light sampler then has the Tree category alone (pmf
 // tree_cat_pmf = 1, or no category without a tree) and every tree leaf is a
 // triangle, so the category draw and the delta-light paths are compiled out.
-// NON_AREA: BDPT's direct_non_area_light_contribution (integrator/bdpt.rs:
-// 396-464), which returns zero when the sampled light is an area light.
-template <bool LIGHTS, bool NON_AREA = false>
+// MODE kDirectMis: direct_light_mis_contribution, or with `nee` the NEE
+// integrator's direct_light_nee_contribution (integrator/nee.rs:104-150):
+// sample_light with the plain environment distribution, Material::eval and no
+// MIS weight; kDirectBdptNonArea: BDPT's direct_non_area_light_contribution
+// (integrator/bdpt.rs:396-464), zero when the sampled light is an area light.
+enum DirectMode : int { kDirectMis = 0, kDirectBdptNonArea = 1 };
+template <bool LIGHTS, int MODE = kDirectMis>
 __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
-                                               float u_cat, float u_tree, float us0, float us1, DirectPrep& out) {
+                                               float u_cat, float u_tree, float us0, float us1, DirectPrep& out,
+                                               bool nee = false) {
   float cat_pmf;
   uint32_t cat;
   if (LIGHTS) {
@@ -462,7 +469,7 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
     if (LIGHTS && (li_inst == kLeafPointDev || li_inst == kLeafSpotDev)) {
       if (!sample_li_delta(S.d, li_inst == kLeafPointDev ? 0u : 1u, li_tri, v.p, li)) return false;
     } else {
-      if (NON_AREA) return false;
+      if (MODE == kDirectBdptNonArea) return false;
       if (!sample_li_triangle(S, li_inst, li_tri, v.p, us0, us1, li)) return false;
       delta = false;
       out.inst = li.inst;
@@ -470,7 +477,7 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
     }
     sel = cat_pmf * leaf_pmf;
   } else if (cat == kCatEnv) {
-    if (!sample_li_env(S.d, us0, us1, li)) return false;
+    if (!sample_li_env(S.d, us0, us1, nee, li)) return false;
     delta = false;
     sel = cat_pmf;
   } else {
@@ -480,7 +487,7 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
   if (li.pdf <= 0.0f || sel <= 0.0f) return false;
   V3 f;
   float bsdf_pdf = 0.0f;
-  if (delta) {
+  if (delta || nee) {
     f = m.kind == kDevLambert ? lambert_eval(m, v, li.wi) : material_eval(S, m, v, li.wi, false);
   } else if (m.kind == kDevLambert) {
     f = lambert_eval(m, v, li.wi);
@@ -494,8 +501,9 @@ __device__ __forceinline__ bool prepare_direct(const DevRender& S, const DevMate
   if (cos_surface <= 0.0f) return false;
   const float pdf_total = sel * li.pdf;
   if (pdf_total <= 0.0f) return false;
-  out.contrib = delta ? li.radiance * f * (cos_surface / pdf_total)
-                      : li.radiance * f * (cos_surface * balance_heuristic(pdf_total, bsdf_pdf) / pdf_total);
+  out.contrib = delta || nee
+                    ? li.radiance * f * (cos_surface / pdf_total)
+                    : li.radiance * f * (cos_surface * balance_heuristic(pdf_total, bsdf_pdf) / pdf_total);
   out.so = offset_origin(v.p, v.ng, li.wi);  // spawn_ray of unoccluded_ray (integrator/mod.rs:239-265)
   out.wi = li.wi;
   out.dist = li.distance;

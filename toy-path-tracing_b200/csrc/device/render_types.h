@@ -197,9 +197,10 @@ struct RenderLaunch {
   DevCamera cam;
   uint32_t width, height, spp, max_depth;
   uint32_t log2_spp, n_base4_digits;
-  uint32_t integrator;  // 0 = MIS
+  uint32_t integrator;  // tpt_integrator: 0 MIS, 1 BDPT, 2 NEE, 3 PT
   uint32_t pad;
 };
+constexpr uint32_t kIntegMis = 0, kIntegBdpt = 1, kIntegNee = 2, kIntegPt = 3;
 
 // Path-replay adjoint (no counterpart in the reference): inputs of the adjoint
 // instantiation of the wavefront stages.  Gradients are per scene material,

@@ -103,8 +103,10 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
       }
     } else if (h.tri < 0) {
       // the ray left the scene: the environment's radiance (mis.rs:33-35, 127-135)
-      if (LIGHTS && S.d.has_env) {
-        const V3 le = env_escape(S.d, rd, depth == 0, (prev_mat >> 31) != 0, depth == 0 ? 0.0f : prev_pdf);
+      // (PT in full, NEE from the camera and after delta samples only)
+      const bool full = depth == 0 || (prev_mat >> 31) != 0 || P.integrator == kIntegPt;
+      if (LIGHTS && S.d.has_env && (full || P.integrator == kIntegMis)) {
+        const V3 le = env_escape(S.d, rd, full, false, full ? 0.0f : prev_pdf);
         L = L + (depth == 0 ? le : beta * le);
       }
       done = true;
@@ -116,9 +118,9 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
         const V3 le = emissive_le(m);
         if (depth == 0) {
           L = L + le;
-        } else if (prev_mat >> 31) {
+        } else if ((prev_mat >> 31) || P.integrator == kIntegPt) {
           L = L + beta * le;
-        } else {
+        } else if (P.integrator == kIntegMis) {
           Vertex pv;
           pv.p = prev_p;
           pv.ns = prev_ns;
@@ -134,7 +136,8 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
         const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
         const float u_cat = LIGHTS && S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(depth, kOffCategory)) : 0.0f;
         DirectPrep dp;
-        const bool nee = prepare_direct<LIGHTS>(S, m, v, u_cat, u_tree, us0, us1, dp);
+        const bool nee = P.integrator != kIntegPt &&  // PT: BSDF sampling only
+                         prepare_direct<LIGHTS>(S, m, v, u_cat, u_tree, us0, us1, dp, P.integrator == kIntegNee);
         if (nee) {
           contrib = beta * dp.contrib;
           tgt_inst = dp.inst;

@@ -159,16 +159,18 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
     const Vertex v = shade_hit<int>(S, h, rd);
     const uint32_t mi = __ldg(&S.d.inst[v.inst].material);
     const DevMaterialRec m = S.d.mats[mi];
-    // emission of this vertex (mis.rs:45-47 for the camera vertex, 101-117 after a bounce)
+    // emission of this vertex (mis.rs:45-47 for the camera vertex, 101-117
+    // after a bounce; PT counts every hit in full, NEE only from the camera
+    // and after delta samples)
     if (m.kind == kDevEmissive) {
       const V3 le = emissive_le(m);
       if (d == 0) {
         L = L + sgn * le;
       } else {
         const uint32_t pm = B.prev_mat[slot];
-        if (pm >> 31) {
+        if ((pm >> 31) || P.integrator == kIntegPt) {
           L = L + sgn * (beta * le);
-        } else {
+        } else if (P.integrator == kIntegMis) {
           Vertex pv;
           pv.p = V3{B.prev[slot], B.prev[C + slot], B.prev[2 * C + slot]};
           pv.ns = V3{B.prev[3 * C + slot], B.prev[4 * C + slot], B.prev[5 * C + slot]};
@@ -193,7 +195,9 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
       const float u_tree = ps.sample_1d(vertex_dim(d, kOffTree));
       // one light-sampler category takes any u: skip drawing it
       const float u_cat = LIGHTS && S.d.num_cat > 1 ? ps.sample_1d(vertex_dim(d, kOffCategory)) : 0.0f;
-      if (prepare_direct<LIGHTS>(S, m, v, u_cat, u_tree, us0, us1, dp)) {
+      // (PT: BSDF sampling only)
+      if (P.integrator != kIntegPt &&
+          prepare_direct<LIGHTS>(S, m, v, u_cat, u_tree, us0, us1, dp, P.integrator == kIntegNee)) {
         dp.contrib = beta * dp.contrib;
         push_shadow = true;
       }
@@ -249,12 +253,17 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
     }
   }
   if (LIGHTS && tri < 0 && S.d.has_env) {
-    // the ray left the scene: the environment's radiance (mis.rs:33-35, 127-135)
-    const float* qr = B.q_ray[cur];
-    const V3 rd = V3{qr[3 * C + j], qr[4 * C + j], qr[5 * C + j]};
-    const uint32_t pm = B.prev_mat[slot];
-    const V3 le = env_escape(S.d, rd, d == 0, (pm >> 31) != 0, d == 0 ? 0.0f : B.prev[6 * C + slot]);
-    L = L + sgn * (d == 0 ? le : beta * le);
+    // the ray left the scene: the environment's radiance (mis.rs:33-35,
+    // 127-135; PT in full, pt.rs:36-39; NEE from the camera and after delta
+    // samples only, nee.rs:37-42)
+    const uint32_t pm = d == 0 ? 0u : B.prev_mat[slot];
+    const bool full = d == 0 || (pm >> 31) != 0 || P.integrator == kIntegPt;
+    if (full || P.integrator == kIntegMis) {
+      const float* qr = B.q_ray[cur];
+      const V3 rd = V3{qr[3 * C + j], qr[4 * C + j], qr[5 * C + j]};
+      const V3 le = env_escape(S.d, rd, full, false, full ? 0.0f : B.prev[6 * C + slot]);
+      L = L + sgn * (d == 0 ? le : beta * le);
+    }
   }
   B.L[slot] = L.x;
   B.L[C + slot] = L.y;

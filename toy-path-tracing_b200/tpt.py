@@ -234,7 +234,7 @@ EXEC_WAVEFRONT = 0
 EXEC_MEGAKERNEL = 1
 
 LAMBERT, EMISSIVE, OPENPBR = 0, 1, 2  # tpt_material_kind
-INTEGRATOR_MIS, INTEGRATOR_BDPT = 0, 1  # tpt_integrator
+INTEGRATOR_MIS, INTEGRATOR_BDPT, INTEGRATOR_NEE, INTEGRATOR_PT = 0, 1, 2, 3  # tpt_integrator
 
 
 def lib():
