@@ -50,7 +50,7 @@ def parse_args():
     p.add_argument("--no-render", action="store_true", help="skip the render workload block")
     # profiling shapes of the render block (defaults: the plain-MIS configuration)
     p.add_argument("--render-only", action="store_true", help="run the render block alone")
-    p.add_argument("--only", choices=["render", "large", "batch", "adjoint"], default=None,
+    p.add_argument("--only", choices=["render", "lights", "large", "batch", "adjoint"], default=None,
                    help="run one block alone (profiling); prints a JSON line with that block")
     p.add_argument("--large-res", type=int, nargs=2, default=(1920, 1080), help="large-scene resolution")
     p.add_argument("--render-res", type=int, default=256)
@@ -317,6 +317,41 @@ def _time_ms(fn, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
+def lights_block(ctx, args):
+    """The Cornell box (256x256, 64 spp, depth 8) lit by point, spot and
+    directional lights plus its ceiling quad (Lambert), and under a procedural
+    sky with a sun (OpenPBR): Msamples/s of the MIS wavefront and megakernel,
+    the NEE and PT integrators (wavefront) and BDPT (wavefront, 16 spp)."""
+    import torch
+
+    import tpt
+    import tpt_scenes
+
+    W = H = RENDER_CFG["width"]
+    spp, depth = RENDER_CFG["spp"], RENDER_CFG["max_depth"]
+    st = torch.cuda.current_stream().cuda_stream
+    img = torch.empty(W * H * 3, device="cuda")
+    out = {"config": {"width": W, "height": H, "spp": spp, "max_depth": depth, "bdpt_spp": 16}, "unit": "Msamples/s"}
+    scenes = (("lights_lambert", tpt_scenes.cornell_lights(1)),
+              ("sky_openpbr", tpt_scenes.cornell_environment(1, tpt_scenes.OPENPBR)))
+    runs = (("mis_wavefront", tpt.INTEGRATOR_MIS, tpt.EXEC_WAVEFRONT, spp),
+            ("mis_megakernel", tpt.INTEGRATOR_MIS, tpt.EXEC_MEGAKERNEL, spp),
+            ("nee_wavefront", tpt.INTEGRATOR_NEE, tpt.EXEC_WAVEFRONT, spp),
+            ("pt_wavefront", tpt.INTEGRATOR_PT, tpt.EXEC_WAVEFRONT, spp),
+            ("bdpt_wavefront", tpt.INTEGRATOR_BDPT, tpt.EXEC_WAVEFRONT, 16))
+    for key, sc in scenes:
+        scene = tpt.Scene(ctx, sc["meshes"], sc["instances"], materials=sc["materials"], lights=sc)
+        res = {}
+        for name, integ, ex, s_spp in runs:
+            job = scene.job(sc["camera"], W, H, s_spp, depth, integrator=integ, execution=ex)
+            reps = 1 if ex == tpt.EXEC_MEGAKERNEL else 3
+            ms = _time_ms(lambda: scene.render_device(job, img.data_ptr(), st), reps)
+            res[name] = W * H * s_spp / ms / 1e3
+        out[key] = res
+        scene.close()
+    return out
+
+
 def large_block(ctx, args, cpu=True):
     """The plain large render: ~2.1M triangles (1024 instanced spheres, boxes and
     tori + ground), 256 OpenPBR materials, 10,000 emissive triangles, 1920x1080,
@@ -541,6 +576,7 @@ def run_ours(args):
         if rank == 0:
             cpu = not args.no_cpu_baseline
             run = {"render": lambda: render_block(ctx, args.steps, args.warmup, cpu=cpu, args=args),
+                   "lights": lambda: lights_block(ctx, args),
                    "large": lambda: large_block(ctx, args, cpu=cpu), "batch": lambda: batch_block(ctx, args),
                    "adjoint": lambda: adjoint_block(ctx, args, cpu=cpu)}[args.only]
             print(json.dumps({args.only: run()}), flush=True)
@@ -655,6 +691,8 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}
     if rank == 0 and not args.no_render:
         line["render"] = render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline, args=args)
+    if rank == 0 and not args.no_render:
+        line["render_lights"] = lights_block(ctx, args)
     if rank == 0 and not args.no_large:
         line["render_large"] = large_block(ctx, args, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_batch:
