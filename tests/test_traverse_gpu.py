@@ -226,3 +226,39 @@ def test_full_size_traversal_against_oracle_sample(ctx):
         ref = g.query(np.ascontiguousarray(rays[:, sample]), 0)
         assert np.array_equal(prim[sample], ref["prim"])
         assert np.array_equal(t[sample].view(np.uint32), ref["t"].view(np.uint32))
+
+
+@pytest.mark.parametrize("n", [1000, 70000, 3_000_000])
+def test_host_entry_point_pinned_and_pageable(soup, n):
+    """`tpt_traverse` with pinned host buffers (copy-engine pipeline, ramped
+    chunk sizes) and with pageable ones (staging slots) gives the device
+    query's results bit for bit, for batch sizes below, across and well above
+    the chunk schedule's steps."""
+    import ctypes as C
+
+    import torch
+
+    g, s = soup
+    rays = tpt_scenes.incoherent_rays(n, seed=21, cube=30.0)
+    rays[6] = np.float32(25.0)  # a finite tmax, read by any-hit queries
+    lib = tpt.lib()
+    ctx = s.ctx
+    d = torch.from_numpy(rays).cuda()
+    for mode in (tpt.CLOSEST_HIT, tpt.ANY_HIT):
+        dprim = torch.empty(n, dtype=torch.int32, device="cuda")
+        dt = torch.empty(n, dtype=torch.float32, device="cuda")
+        s.traverse_device(d.data_ptr(), n, mode, dprim.data_ptr(), dt.data_ptr(),
+                          stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        want_p, want_t = dprim.cpu().numpy(), dt.cpu().numpy()
+        for pinned in (True, False):
+            hr = torch.from_numpy(rays)
+            hp = torch.empty(n, dtype=torch.int32)
+            ht = torch.empty(n, dtype=torch.float32)
+            if pinned:
+                hr, hp, ht = hr.pin_memory(), hp.pin_memory(), ht.pin_memory()
+            st = lib.tpt_traverse(ctx.h, s.h, C.c_void_p(hr.data_ptr()), n, mode, C.c_void_p(hp.data_ptr()),
+                                  C.c_void_p(ht.data_ptr()), None, None)
+            assert st == 0, lib.tpt_last_error(ctx.h)
+            assert np.array_equal(hp.numpy(), want_p), (mode, pinned)
+            assert np.array_equal(ht.numpy().view(np.uint32), want_t.view(np.uint32)), (mode, pinned)

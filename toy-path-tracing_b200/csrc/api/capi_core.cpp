@@ -100,6 +100,45 @@ tpt_status ensure_pipeline(tpt_context* ctx) {
   return cuda_check(ctx, cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming), "event");
 }
 
+// Chunk sizes of a pinned-buffer traversal: a ramp up from chunk / 8 (the
+// first kernel starts after a short copy), `chunk` in the middle, and halving
+// pieces at the end (the last copy-out follows a short kernel).
+std::vector<uint64_t> chunk_schedule(uint64_t n, uint64_t chunk) {
+  std::vector<uint64_t> out;
+  const uint64_t min_chunk = 1u << 16;
+  uint64_t left = n, s = std::max<uint64_t>(min_chunk, chunk / 8);
+  while (left > 0 && s < chunk) {
+    const uint64_t m = std::min(s, left);
+    out.push_back(m);
+    left -= m;
+    s *= 2;
+  }
+  while (left > 0) {
+    uint64_t m;
+    if (left > 2 * chunk) m = chunk;
+    else if (left > 2 * min_chunk) m = std::max<uint64_t>(min_chunk, (left + 1) / 2);
+    else m = left;
+    out.push_back(m);
+    left -= m;
+  }
+  return out;
+}
+
+tpt_status ensure_copy_pipeline(tpt_context* ctx, size_t n_chunks) {
+  tpt_status st = TPT_OK;
+  if (!ctx->copy_in) st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking), "stream");
+  if (!st && !ctx->copy_out)
+    st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking), "stream");
+  while (!st && ctx->ev_in.size() < n_chunks) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    st = cuda_check(ctx, cudaEventCreateWithFlags(&a, cudaEventDisableTiming), "event");
+    if (!st) st = cuda_check(ctx, cudaEventCreateWithFlags(&b, cudaEventDisableTiming), "event");
+    if (a) ctx->ev_in.push_back(a);
+    if (b) ctx->ev_done.push_back(b);
+  }
+  return st;
+}
+
 bool is_pinned(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -244,6 +283,10 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
     if (ctx->pipe[k]) cudaStreamDestroy(ctx->pipe[k]);
     if (ctx->ev_slot[k]) cudaEventDestroy(ctx->ev_slot[k]);
   }
+  if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+  if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+  for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->ev_done) cudaEventDestroy(e);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -538,8 +581,48 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
   const bool in_pinned = is_pinned(rays);
   const bool out_pinned = is_pinned(prim) && is_pinned(t) && (!instance || is_pinned(instance)) &&
                           (!bary || is_pinned(bary));
-  // Chunks of about 2M rays, at least 4 when the batch allows, pipelined on two streams.
+  // Chunks of about 2M rays, at least 4 when the batch allows.
   uint64_t chunk = std::max<uint64_t>(1 << 16, std::min<uint64_t>(1 << 21, (n + 3) / 4));
+  struct Out { void* host; const void* dev; size_t planes; };
+  const Out outs[4] = {{prim, d_prim, 1}, {t, d_t, 1}, {instance, d_inst, 1}, {bary, d_bary, 3}};
+  if (in_pinned && out_pinned) {
+    // Pinned buffers: copies in on one stream, kernels alternating on two
+    // streams, copies out on a third, ordered by per-chunk events, so the
+    // host-to-device copies run back to back while earlier chunks traverse
+    // and later ones drain.
+    const std::vector<uint64_t> sizes = chunk_schedule(n, chunk);
+    if ((st = ensure_copy_pipeline(ctx, sizes.size()))) return st;
+    cudaEventRecord(ctx->ev_start, ctx->stream);
+    cudaStreamWaitEvent(ctx->copy_in, ctx->ev_start, 0);
+    for (int k = 0; k < 2; ++k) cudaStreamWaitEvent(ctx->pipe[k], ctx->ev_start, 0);
+    uint64_t b = 0;
+    for (size_t c = 0; c < sizes.size(); ++c) {
+      const uint64_t m = sizes[c];
+      for (int p = 0; p < in_planes; ++p)
+        cudaMemcpyAsync(d_rays + p * n + b, rays + p * n + b, m * 4, cudaMemcpyHostToDevice, ctx->copy_in);
+      cudaEventRecord(ctx->ev_in[c], ctx->copy_in);
+      cudaStream_t s = ctx->pipe[c & 1];
+      cudaStreamWaitEvent(s, ctx->ev_in[c], 0);
+      cudaError_t e = launch_traverse_strided(scene->geo, d_rays + b, n, m, mode, d_prim + b, d_t + b,
+                                              d_inst ? d_inst + b : nullptr, d_bary ? d_bary + b : nullptr, n,
+                                              next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr, nullptr);
+      if ((st = cuda_check(ctx, e, "traverse kernel launch"))) return st;
+      cudaEventRecord(ctx->ev_done[c], s);
+      cudaStreamWaitEvent(ctx->copy_out, ctx->ev_done[c], 0);
+      for (const Out& o : outs) {
+        if (!o.host) continue;
+        for (size_t p = 0; p < o.planes; ++p)
+          cudaMemcpyAsync((char*)o.host + (p * n + b) * 4, (const char*)o.dev + (p * n + b) * 4, m * 4,
+                          cudaMemcpyDeviceToHost, ctx->copy_out);
+      }
+      b += m;
+    }
+    cudaEventRecord(ctx->ev_slot[0], ctx->copy_out);
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_slot[0], 0);
+    if ((st = cuda_check(ctx, cudaGetLastError(), "traverse pipeline"))) return st;
+    return check_device_errors(ctx, ctx->stream);
+  }
+  // Pageable buffers: pinned staging slots, pipelined on two streams.
   const uint64_t n_chunks = (n + chunk - 1) / chunk;
   if (!in_pinned || !out_pinned) {
     const size_t per_slot = (7 + (size_t)n_out) * chunk * 4;
@@ -569,11 +652,9 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
                                             d_inst ? d_inst + b : nullptr, d_bary ? d_bary + b : nullptr, n,
                                             next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr, nullptr);
     if ((st = cuda_check(ctx, e, "traverse kernel launch"))) return st;
-    struct Out { void* host; const void* dev; size_t planes; };
-    Out outs[4] = {{prim, d_prim, 1}, {t, d_t, 1}, {instance, d_inst, 1}, {bary, d_bary, 3}};
     float* hout = hslot + 7 * m;
     size_t ho = 0;
-    for (auto& o : outs) {
+    for (const Out& o : outs) {
       if (!o.host) continue;
       for (size_t p = 0; p < o.planes; ++p) {
         const char* src = (const char*)o.dev + (p * n + b) * 4;
@@ -589,7 +670,7 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
       // drain the slot before it is reused (two chunks later)
       cudaStreamSynchronize(s);
       size_t h2 = 0;
-      for (auto& o : outs) {
+      for (const Out& o : outs) {
         if (!o.host) continue;
         for (size_t p = 0; p < o.planes; ++p, ++h2)
           std::memcpy((char*)o.host + (p * n + b) * 4, hout + h2 * m, m * 4);

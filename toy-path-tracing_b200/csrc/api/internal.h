@@ -32,6 +32,10 @@ struct tpt_context {
   cudaStream_t pipe[2] = {nullptr, nullptr};  // copy/compute pipeline of tpt_traverse
   cudaEvent_t ev_slot[2] = {nullptr, nullptr};
   cudaEvent_t ev_start = nullptr;
+  // pinned-buffer pipeline of tpt_traverse: one stream per copy direction
+  // (each feeds its own copy engine) and per-chunk events
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> ev_in, ev_done;
   unsigned long long* d_counters = nullptr;  // work-distribution counters, one per in-flight launch
   uint32_t counter_next = 0;
   // device scratch for per-sample radiance of render calls (grown on demand)
