@@ -86,6 +86,19 @@ typedef struct tpt_qbvh_view {
  * bounds: n x 6 floats (min xyz, max xyz).  threads <= 0 uses all cores.
  * Fails with TPT_ERR_INVALID_ARG for n == 0 (the reference returns None). */
 tpt_status tpt_qbvh_build(const float* bounds, uint64_t n, int threads, tpt_qbvh** out);
+/* The same build on the GPU (no counterpart in the reference): `d_bounds` is a
+ * device array of n x 6 floats (stream: NULL = the context's).  The result is
+ * the host builder's tree, node for node and in the same primitive order (a box
+ * face at zero may hold +0.0 where the host builder keeps -0.0: both builders
+ * keep the first zero they meet, and the GPU reduces in no fixed order).
+ * Large ranges split level by level with all ranges of a level processed
+ * element-parallel (the reference's swap partition reproduced from prefix
+ * counts); ranges below 512 primitives are built by one thread each. */
+tpt_status tpt_qbvh_build_device(tpt_context* ctx, const float* d_bounds, uint64_t n, void* stream, tpt_qbvh** out);
+/* Whether tpt_scene_upload builds the QBVHs the description leaves empty on
+ * the GPU (meshes and instance sets of at least 4096 primitives); default 0.
+ * A GPU build that fails falls back to the host builder. */
+tpt_status tpt_context_set_gpu_build(tpt_context* ctx, int enable);
 tpt_status tpt_qbvh_view_of(const tpt_qbvh* q, tpt_qbvh_view* view);
 tpt_status tpt_qbvh_free(tpt_qbvh* q);
 

@@ -139,6 +139,28 @@ tpt_status ensure_copy_pipeline(tpt_context* ctx, size_t n_chunks) {
   return st;
 }
 
+bool is_pinned(const void* p);
+
+}  // namespace
+
+void tpt::build_qbvh_for(tpt_context* ctx, const float* bounds6, uint32_t n, int threads, QbvhHost* out) {
+  constexpr uint32_t kGpuBuildMin = 4096;  // below this the host builds faster than a launch sequence
+  if (ctx && ctx->gpu_build && n >= kGpuBuildMin) {
+    float* d = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d, (size_t)6 * n * 4, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d, bounds6, (size_t)6 * n * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = build_qbvh_gpu(d, n, out, ctx->stream);
+    if (d) cudaFreeAsync(d, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) return;
+    cudaGetLastError();
+  }
+  build_qbvh_host(bounds6, n, threads, out);
+}
+
+namespace {
+
 bool is_pinned(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -305,6 +327,31 @@ tpt_status tpt_qbvh_build(const float* bounds, uint64_t n, int threads, tpt_qbvh
   return TPT_OK;
 }
 
+tpt_status tpt_qbvh_build_device(tpt_context* ctx, const float* d_bounds, uint64_t n, void* stream, tpt_qbvh** out) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  if (!out || (!d_bounds && n)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  if (n == 0) return set_error(ctx, TPT_ERR_INVALID_ARG, "no primitives (build_qbvh returns None)");
+  if (n >= (1ull << 24)) return set_error(ctx, TPT_ERR_CAPACITY, "more than 2^24 primitives in one QBVH");
+  cudaSetDevice(ctx->device);
+  auto* q = new tpt_qbvh();
+  const cudaError_t e = build_qbvh_gpu(d_bounds, (uint32_t)n, &q->q, stream ? (cudaStream_t)stream : ctx->stream);
+  if (e != cudaSuccess) {
+    delete q;
+    if (e == cudaErrorLaunchOutOfResources)
+      return set_error(ctx, TPT_ERR_CAPACITY, "GPU QBVH build exceeded its work-list capacity");
+    return cuda_check(ctx, e, "GPU QBVH build");
+  }
+  *out = q;
+  return TPT_OK;
+}
+
+tpt_status tpt_context_set_gpu_build(tpt_context* ctx, int enable) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  ctx->gpu_build = enable != 0;
+  return TPT_OK;
+}
+
 tpt_status tpt_qbvh_view_of(const tpt_qbvh* q, tpt_qbvh_view* v) {
   if (!q || !v) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL argument");
   v->nodes = reinterpret_cast<const tpt_qbvh_node*>(q->q.nodes.data());
@@ -380,7 +427,7 @@ tpt_status tpt_scene_upload(tpt_context* ctx, const tpt_scene_desc* desc, tpt_sc
         b[4] = std::fmax(std::fmax(v[0].y, v[1].y), v[2].y);
         b[5] = std::fmax(std::fmax(v[0].z, v[1].z), v[2].z);
       }
-      build_qbvh_host(tb.data(), (uint32_t)ntri, threads, &built);
+      build_qbvh_for(ctx, tb.data(), (uint32_t)ntri, threads, &built);
       qn = built.nodes.data();
       qnn = built.nodes.size();
       qp = built.prim_indices.data();
@@ -464,7 +511,7 @@ tpt_status tpt_scene_upload(tpt_context* ctx, const tpt_scene_desc* desc, tpt_sc
       qpn = desc->tlas.num_primitives;
       if (qnn && !qn) return set_error(ctx, TPT_ERR_INVALID_ARG, "TLAS nodes is NULL");
     } else {
-      build_qbvh_host(inst_bounds.data(), desc->num_instances, threads, &built);
+      build_qbvh_for(ctx, inst_bounds.data(), desc->num_instances, threads, &built);
       qn = built.nodes.data();
       qnn = built.nodes.size();
       qp = built.prim_indices.data();

@@ -58,6 +58,7 @@ struct tpt_context {
   bool use_graphs = true;
   uint32_t tuned_execution = 0;  // what TPT_EXEC_AUTO means (tpt_autotune)
   uint32_t shade_block = 256;    // threads per block of the wavefront shade stage (128 or 256)
+  bool gpu_build = false;        // scene upload builds missing QBVHs on the GPU (tpt_context_set_gpu_build)
   std::vector<tpt::BounceGraphSet*> graphs;
   uint64_t graph_clock = 0;
   cudaStream_t cap_stream = nullptr;
@@ -114,6 +115,15 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t stream,
                                     uint32_t* node_tests, uint32_t* tri_tests, const uint32_t* n_dev = nullptr,
                                     const DevJob* jobs = nullptr, const uint32_t* ray_job = nullptr);
+
+// qbvh_build_gpu.cu: the QBVH of n primitive boxes (device, n x 6 floats) built
+// on the device, equal to build_qbvh_host's (a box face at zero may be +0.0
+// where the host keeps -0.0).  Errors: allocation, or capacity (never expected;
+// callers fall back to the host builder).
+cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cudaStream_t s);
+// The QBVH of host boxes: on the GPU when the context asks for it and the set is
+// large enough to gain, else (or if the GPU build fails) on the host.
+void build_qbvh_for(tpt_context* ctx, const float* bounds6, uint32_t n, int threads, QbvhHost* out);
 
 // A work counter slot for the next launch (ring of kCounterSlots per context).
 unsigned long long* next_counter(tpt_context* ctx);

@@ -257,6 +257,8 @@ EXPORTED_SYMBOLS = [
     "tpt_last_error",
     "tpt_version",
     "tpt_qbvh_build",
+    "tpt_qbvh_build_device",
+    "tpt_context_set_gpu_build",
     "tpt_qbvh_view_of",
     "tpt_qbvh_free",
     "tpt_scene_upload",
@@ -299,6 +301,8 @@ def _declare(L):
         "tpt_last_error": (cp, [vp]),
         "tpt_version": (cp, []),
         "tpt_qbvh_build": (i32, [vp, u64, i32, C.POINTER(vp)]),
+        "tpt_qbvh_build_device": (i32, [vp, vp, u64, vp, C.POINTER(vp)]),
+        "tpt_context_set_gpu_build": (i32, [vp, i32]),
         "tpt_qbvh_view_of": (i32, [vp, C.POINTER(QbvhView)]),
         "tpt_qbvh_free": (i32, [vp]),
         "tpt_scene_upload": (i32, [vp, C.POINTER(SceneDesc), C.POINTER(vp)]),
@@ -377,6 +381,10 @@ class Context:
     def wavefront_capacity(self, slots: int):
         _check(lib().tpt_context_set_wavefront_capacity(self.h, int(slots)), self)
 
+    def set_gpu_build(self, enable: bool):
+        """`tpt_context_set_gpu_build`: scene uploads build missing QBVHs on the GPU."""
+        _check(lib().tpt_context_set_gpu_build(self.h, int(bool(enable))), self)
+
     def set_graphs(self, enable: bool):
         """`tpt_context_set_graphs`: replay wavefront bounces from CUDA graphs."""
         _check(lib().tpt_context_set_graphs(self.h, int(bool(enable))), self)
@@ -426,6 +434,25 @@ def build_qbvh(bounds: np.ndarray, threads: int = 0):
     b = np.ascontiguousarray(bounds, np.float32).reshape(-1, 6)
     h = C.c_void_p()
     _check(lib().tpt_qbvh_build(_p(b), b.shape[0], threads, C.byref(h)))
+    try:
+        v = QbvhView()
+        _check(lib().tpt_qbvh_view_of(h, C.byref(v)))
+        nodes = np.zeros(v.num_nodes, NODE_DTYPE)
+        prims = np.zeros(v.num_primitives, np.uint32)
+        if v.num_nodes:
+            C.memmove(nodes.ctypes.data, v.nodes, nodes.nbytes)
+        C.memmove(prims.ctypes.data, v.primitive_indices, prims.nbytes)
+    finally:
+        lib().tpt_qbvh_free(h)
+    return nodes, prims
+
+
+def build_qbvh_device(ctx: "Context", bounds_ptr: int, n: int, stream=None):
+    """GPU builder (`tpt_qbvh_build_device`) from a device array of n x 6
+    floats: returns (nodes[NODE_DTYPE], primitive_indices[u32]), the host
+    builder's tree."""
+    h = C.c_void_p()
+    _check(lib().tpt_qbvh_build_device(ctx.h, C.c_void_p(bounds_ptr), n, _stream(stream), C.byref(h)), ctx)
     try:
         v = QbvhView()
         _check(lib().tpt_qbvh_view_of(h, C.byref(v)))
