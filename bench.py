@@ -317,6 +317,40 @@ def _time_ms(fn, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
+def qbvh_build_block(ctx, mesh):
+    """Scene preparation of the traversal workload: the 1M-triangle QBVH built
+    by the host builder (all host threads) and by the GPU builder (from device
+    boxes, through the C ABI), median of three; the trees are identical."""
+    import ctypes as C
+
+    import torch
+
+    import tpt
+
+    tri = mesh["positions"][mesh["indices"].reshape(-1, 3)]
+    b = np.ascontiguousarray(np.concatenate([tri.min(1), tri.max(1)], 1), np.float32)
+    d = torch.from_numpy(b).cuda()
+    lib = tpt.lib()
+
+    def timed(fn):
+        ts = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h = C.c_void_p()
+            st = fn(h)
+            ts.append(time.perf_counter() - t0)
+            if st != 0:
+                raise RuntimeError(lib.tpt_last_error(ctx.h).decode())
+            lib.tpt_qbvh_free(h)
+        return sorted(ts)[1] * 1e3
+
+    gpu = timed(lambda h: lib.tpt_qbvh_build_device(ctx.h, C.c_void_p(d.data_ptr()), b.shape[0], None, C.byref(h)))
+    host = timed(lambda h: lib.tpt_qbvh_build(b.ctypes.data, b.shape[0], 0, C.byref(h)))
+    return {"primitives": int(b.shape[0]), "host_ms": host, "host_threads": os.cpu_count(), "gpu_ms": gpu,
+            "gpu_over_host": host / gpu}
+
+
 def lights_block(ctx, args):
     """The Cornell box (256x256, 64 spp, depth 8) lit by point, spot and
     directional lights plus its ceiling quad (Lambert), and under a procedural
@@ -686,6 +720,8 @@ def run_ours(args):
         },
         "clocks": clk,
     }
+    if rank == 0:
+        line["qbvh_build"] = qbvh_build_block(ctx, mesh)
     if rank == 0 and not args.no_cpu_baseline:
         rate, threads, desc = cpu_reference_rate(mesh, batches)
         line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}

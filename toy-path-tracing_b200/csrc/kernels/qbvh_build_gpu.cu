@@ -45,7 +45,7 @@ namespace {
 
 constexpr int kBinsG = 16;
 constexpr uint32_t kLeafTargetG = 4, kLeafMaxG = 16;
-constexpr uint32_t kSeqMax = 512;  // ranges below this size are built whole by one thread
+constexpr uint32_t kSeqMax = 64;  // ranges below this size are built whole by one thread
 constexpr uint32_t kNoneG = 0xFFFFFFFFu;
 constexpr int kBlk = 256;
 constexpr int kSeqStack = 96;
@@ -772,15 +772,17 @@ cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cu
   const uint32_t seq_cap = n / 4 + 64;
   const uint32_t node_cap = 2 * n + 16;
   std::vector<void*> allocs;
+  // stream-ordered allocations: after the first build they come from the
+  // device's memory pool without synchronising
   auto take = [&](size_t bytes) -> void* {
     void* p = nullptr;
-    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+    if (cudaMallocAsync(&p, std::max<size_t>(bytes, 16), s) != cudaSuccess) return nullptr;
     allocs.push_back(p);
     return p;
   };
   auto release = [&]() {
+    for (void* p : allocs) cudaFreeAsync(p, s);
     cudaStreamSynchronize(s);
-    for (void* p : allocs) cudaFree(p);
   };
   BuildBuffers B{};
   B.n = n;
@@ -874,12 +876,14 @@ cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cu
       for (uint32_t k = 0; e == cudaSuccess && k < hc.medians; ++k) {
         const Task& tk = ht[idx[k]];
         GNode g;
-        e = cudaMemcpy(&g, B.nodes + tk.node, sizeof g, cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(&g, B.nodes + tk.node, sizeof g, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
         const float ex = g.hi[0] - g.lo[0], ey = g.hi[1] - g.lo[1], ez = g.hi[2] - g.lo[2];
         const int axis = (ex >= ey && ex >= ez) ? 0 : (ey >= ez ? 1 : 2);
         std::vector<uint32_t> ord(tk.count);
-        e = cudaMemcpy(ord.data(), B.order + tk.begin, (size_t)tk.count * 4, cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(ord.data(), B.order + tk.begin, (size_t)tk.count * 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
         const float* cn = h_cen.data() + (size_t)axis * n;
         std::sort(ord.begin(), ord.end(), [cn](uint32_t x, uint32_t y) {
@@ -887,17 +891,17 @@ cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cu
           if (cn[y] < cn[x]) return false;
           return x < y;
         });
-        e = cudaMemcpy(B.order + tk.begin, ord.data(), (size_t)tk.count * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(B.order + tk.begin, ord.data(), (size_t)tk.count * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
       }
       if (e != cudaSuccess) break;
     }
     k_emit<<<grid1(m), kBlk, 0, s>>>(T, m, B, Ls);
     k_seg<<<grid1(n), kBlk, 0, s>>>(B, T);
-    e = cudaMemcpyAsync(&hc, B.cnt, sizeof hc, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) break;
     uint32_t ov = 0;
-    e = cudaMemcpy(&ov, overflow, 4, cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(&hc, B.cnt, sizeof hc, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ov, overflow, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess && ov) e = cudaErrorLaunchOutOfResources;
     if (e != cudaSuccess) break;
     m = hc.next_tasks;
@@ -934,6 +938,7 @@ cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cu
     out->prim_indices.clear();
     return e;
   }
+  out->nodes.reserve(g.size() / 2 + 1);
   flatten(g, 0, out->nodes);
   return cudaSuccess;
 }
