@@ -403,6 +403,12 @@ tpt_status tpt_context_set_shade_block(tpt_context* ctx, uint32_t threads);
 tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb);
 /* One job into a device buffer, asynchronous on `stream`. */
 tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream);
+/* Pixels [first_pixel, first_pixel + num_pixels) of `job`'s image (pixel =
+ * y * width + x) into out_rgb (device, num_pixels * 3 floats), each the same
+ * bits as in tpt_render_device's image: the unit a multi-GPU caller gives each
+ * rank (row bands), gathering the bands into one image. */
+tpt_status tpt_render_pixels_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first_pixel,
+                                    uint64_t num_pixels, float* out_rgb, void* stream);
 /* The per-sample radiance of paths [first, first+count) in (pixel, sample)
  * order, path = pixel * spp + sample, into a device buffer of count*3 floats
  * (parity testing and sample-level consumers). */
@@ -520,11 +526,17 @@ enum {
 typedef struct tpt_adjoint_desc {
   uint32_t param_mask; /* groups to differentiate; 0 = TPT_GRAD_ALL */
   float fd_step;       /* parameter step of the BSDF central differences; 0 = 1e-3 */
+  /* Pixels [first_pixel, first_pixel + num_pixels) whose paths are replayed
+   * (num_pixels 0 = the whole image); d_image then holds those pixels only
+   * (num_pixels * 3 floats).  The gradients of disjoint pixel ranges sum to
+   * the whole image's (a multi-GPU caller all-reduces them). */
+  uint32_t first_pixel, num_pixels;
 } tpt_adjoint_desc;
 
 /* dLoss/d(material parameters) of the image tpt_render_device produces for
  * `job` (MIS integrator; `execution` is not read), given d_image = dLoss/dimage
- * (device, width*height*3 floats).  grad (device, num_materials x
+ * (device, width*height*3 floats, or the pixel range's when adesc names one).
+ * grad (device, num_materials x
  * TPT_GRAD_PARAMS doubles) is overwritten; non-OpenPBR materials get zeros.
  * Path replay with detached sampling: per chunk of paths the forward wavefront
  * is run again for the paths' radiance, then replayed from the same streams,
@@ -533,7 +545,7 @@ typedef struct tpt_adjoint_desc {
  * difference of the BSDF at the sampled direction between host-lowered
  * theta -/+ fd_step copies of the material (clipped to [0, 1], the IOR to
  * [1, 10]); an unoccluded light sample C at an OpenPBR vertex (directional
- * lights) adds dLoss/dL * C * (df/dtheta) / f at the light direction.
+ * lights, environment) adds dLoss/dL * C * (df/dtheta) / f at the light direction.
  * Accumulation is FP64 atomics, so the sums' order (and last bits)
  * vary between runs.  adesc may be NULL (all groups, step 1e-3). */
 tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const tpt_adjoint_desc* adesc,

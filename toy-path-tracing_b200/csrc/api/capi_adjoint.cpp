@@ -155,6 +155,14 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   A.s_grad = nullptr;
   A.s_gkey = nullptr;
   const uint32_t npix = L.width * L.height;
+  uint32_t pix_begin = 0, pix_end = npix;
+  if (adesc && adesc->num_pixels) {
+    if (adesc->first_pixel > npix || adesc->num_pixels > npix - adesc->first_pixel)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "adjoint pixel range out of bounds");
+    pix_begin = adesc->first_pixel;
+    pix_end = adesc->first_pixel + adesc->num_pixels;
+  }
+  A.pixel_base = pix_begin;
   const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
   // light samples at OpenPBR vertices come from directional lights and the
   // environment only (the light tree serves diffuse vertices): their gradient
@@ -170,8 +178,8 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
     A.s_grad = (float*)((char*)ctx->d_scratch + sample_bytes);
     A.s_gkey = (uint32_t*)(A.s_grad + (size_t)kGradParams * ctx->wf.capacity);
   }
-  for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
-    const uint32_t n = std::min(cp, npix - p0);
+  for (uint32_t p0 = pix_begin; p0 < pix_end; p0 += cp) {
+    const uint32_t n = std::min(cp, pix_end - p0);
     const uint64_t first = (uint64_t)p0 * L.spp;
     if ((st = render_wavefront(ctx, job, L, first, n * L.spp, samples, s))) return st;
     if ((st = render_wavefront(ctx, job, L, first, n * L.spp, samples, s, &A))) return st;
@@ -184,7 +192,8 @@ tpt_status tpt_adjoint(tpt_context* ctx, const tpt_render_job* job, const tpt_ad
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (!job || !job->scene || !d_image || !grad) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL argument");
   cudaSetDevice(ctx->device);
-  const size_t ibytes = (size_t)job->width * job->height * 12;
+  const size_t ibytes =
+      (size_t)(adesc && adesc->num_pixels ? adesc->num_pixels : (uint64_t)job->width * job->height) * 12;
   const size_t gbytes = (size_t)job->scene->render.num_materials * kGradParams * sizeof(double);
   float* di = nullptr;
   double* dg = nullptr;

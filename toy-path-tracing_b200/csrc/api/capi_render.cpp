@@ -291,19 +291,29 @@ uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx) {
 
 tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  if (!job) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL job");
+  return tpt_render_pixels_device(ctx, job, 0, (uint64_t)job->width * job->height, out_rgb, stream);
+}
+
+tpt_status tpt_render_pixels_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first_pixel,
+                                    uint64_t num_pixels, float* out_rgb, void* stream) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (!out_rgb) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
   RenderLaunch L;
   tpt_status st = make_launch(ctx, job, &L);
   if (st) return st;
+  const uint64_t total = (uint64_t)L.width * L.height;
+  if (first_pixel > total || num_pixels > total - first_pixel)
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "pixel range out of bounds");
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  const uint32_t npix = L.width * L.height;
+  const uint32_t pix_begin = (uint32_t)first_pixel, pix_end = (uint32_t)(first_pixel + num_pixels);
   const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
   if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
   float* samples = (float*)ctx->d_scratch;
   const uint32_t exec = job->execution == TPT_EXEC_AUTO ? ctx->tuned_execution : job->execution;
-  for (uint32_t p0 = 0; p0 < npix; p0 += cp) {
-    const uint32_t n = std::min(cp, npix - p0);
+  for (uint32_t p0 = pix_begin; p0 < pix_end; p0 += cp) {
+    const uint32_t n = std::min(cp, pix_end - p0);
     if (job->integrator == TPT_INTEGRATOR_BDPT && exec != TPT_EXEC_MEGAKERNEL) {
       if ((st = render_bdpt_wavefront(ctx, job, L, (uint64_t)p0 * L.spp, (uint64_t)n * L.spp, samples, s))) return st;
     } else if (exec == TPT_EXEC_MEGAKERNEL || job->integrator == TPT_INTEGRATOR_BDPT) {
@@ -313,7 +323,7 @@ tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float*
     } else {
       if ((st = render_wavefront(ctx, job, L, (uint64_t)p0 * L.spp, n * L.spp, samples, s))) return st;
     }
-    cudaError_t e = launch_accumulate(samples, L.spp, p0, n, L.cam.exposure, out_rgb, s);
+    cudaError_t e = launch_accumulate(samples, L.spp, p0 - pix_begin, n, L.cam.exposure, out_rgb, s);
     if ((st = cuda_check(ctx, e, "accumulate kernel launch"))) return st;
   }
   return TPT_OK;

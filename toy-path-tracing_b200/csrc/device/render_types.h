@@ -213,10 +213,11 @@ constexpr uint32_t kGradGroups = 5;
 struct DevAdjoint {
   const DevOpenPbr* pert;  // [OpenPBR table index][group][lo, hi]
   const float* span;       // [OpenPBR table index][group][3]: hi - lo per channel
-  const float* d_image;    // dLoss/dimage: width * height * 3
+  const float* d_image;    // dLoss/dimage of pixels [pixel_base, ...): 3 floats each
   double* grad;            // [material][kGradParams]
   float scale;             // exposure / spp: d image / d sample radiance
   uint32_t mask;           // parameter groups to differentiate (bit g = group g)
+  uint32_t pixel_base;     // first pixel of the replayed range
   // light samples at OpenPBR vertices (directional lights), per shadow-queue
   // entry: the gradient change if the shadow ray is unoccluded (kGradParams
   // planes of the wavefront capacity) and its material (0xFFFFFFFF: none).

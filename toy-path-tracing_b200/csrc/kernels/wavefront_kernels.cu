@@ -183,9 +183,8 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
       const uint64_t path = first_path + slot - (BATCH ? jobs[jb].path_base : 0ull);
       V3 dl = V3{0.0f, 0.0f, 0.0f};
       if (ADJ) {
-        const uint32_t pixel = (uint32_t)(path / P.spp);
-        dl = V3{A.d_image[3 * (uint64_t)pixel], A.d_image[3 * (uint64_t)pixel + 1],
-                A.d_image[3 * (uint64_t)pixel + 2]} * A.scale;
+        const uint64_t di = 3ull * ((uint32_t)(path / P.spp) - A.pixel_base);
+        dl = V3{A.d_image[di], A.d_image[di + 1], A.d_image[di + 2]} * A.scale;
       }
       const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
       PathSamplerDev ps;

@@ -212,7 +212,8 @@ class RenderJob(C.Structure):
 
 
 class AdjointDesc(C.Structure):
-    _fields_ = [("param_mask", C.c_uint32), ("fd_step", C.c_float)]
+    _fields_ = [("param_mask", C.c_uint32), ("fd_step", C.c_float), ("first_pixel", C.c_uint32),
+                ("num_pixels", C.c_uint32)]
 
 
 # gradient layout per material (tpt.h TPT_GRAD_*) and parameter-group bits
@@ -271,6 +272,7 @@ EXPORTED_SYMBOLS = [
     "tpt_render",
     "tpt_render_device",
     "tpt_render_samples_device",
+    "tpt_render_pixels_device",
     "tpt_light_tree_build",
     "tpt_light_tree_view_of",
     "tpt_light_tree_free",
@@ -315,6 +317,7 @@ def _declare(L):
         "tpt_render": (i32, [vp, C.POINTER(RenderJob), i32, C.POINTER(C.c_void_p)]),
         "tpt_render_device": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
         "tpt_render_samples_device": (i32, [vp, C.POINTER(RenderJob), u64, u64, vp, vp]),
+        "tpt_render_pixels_device": (i32, [vp, C.POINTER(RenderJob), u64, u64, vp, vp]),
         "tpt_light_tree_build": (i32, [C.POINTER(SceneDesc), C.POINTER(vp)]),
         "tpt_light_tree_view_of": (i32, [vp, C.POINTER(LightTreeView)]),
         "tpt_light_tree_free": (i32, [vp]),
@@ -605,6 +608,12 @@ class Scene:
     def render_device(self, job, out_ptr: int, stream=None):
         _check(lib().tpt_render_device(self.ctx.h, C.byref(job), C.c_void_p(out_ptr), _stream(stream)), self.ctx)
 
+    def render_pixels_device(self, job, first_pixel: int, num_pixels: int, out_ptr: int, stream=None):
+        """`tpt_render_pixels_device`: pixels [first_pixel, first_pixel + num_pixels)
+        of the job's image (float32 [num_pixels * 3] at out_ptr)."""
+        _check(lib().tpt_render_pixels_device(self.ctx.h, C.byref(job), first_pixel, num_pixels,
+                                              C.c_void_p(out_ptr), _stream(stream)), self.ctx)
+
     def render_samples_device(self, job, first: int, count: int, out_ptr: int, stream=None):
         _check(lib().tpt_render_samples_device(self.ctx.h, C.byref(job), first, count, C.c_void_p(out_ptr),
                                                _stream(stream)), self.ctx)
@@ -634,20 +643,22 @@ class Scene:
         _check(lib().tpt_scene_set_openpbr(self.ctx.h, self.h, len(ids), _p(ids), descs, _stream(stream)), self.ctx)
 
     def adjoint_device(self, job, d_image_ptr: int, grad_ptr: int, mask: int = 0, fd_step: float = 0.0,
-                       stream=None):
+                       stream=None, first_pixel: int = 0, num_pixels: int = 0):
         """`tpt_adjoint_device`: dLoss/d(material parameters) (float64 [n_materials, 7]
         at grad_ptr, n_materials = self.n_materials) from dLoss/dimage (float32
-        [h*w*3] at d_image_ptr)."""
-        ad = AdjointDesc(mask, fd_step)
+        [h*w*3] at d_image_ptr, or [num_pixels*3] for the paths of pixels
+        [first_pixel, first_pixel + num_pixels) when num_pixels > 0)."""
+        ad = AdjointDesc(mask, fd_step, first_pixel, num_pixels)
         _check(lib().tpt_adjoint_device(self.ctx.h, C.byref(job), C.byref(ad), C.c_void_p(d_image_ptr),
                                         C.c_void_p(grad_ptr), _stream(stream)), self.ctx)
 
-    def adjoint(self, job, d_image: np.ndarray, mask: int = 0, fd_step: float = 0.0):
+    def adjoint(self, job, d_image: np.ndarray, mask: int = 0, fd_step: float = 0.0, first_pixel: int = 0,
+                num_pixels: int = 0):
         """`tpt_adjoint` with host arrays; returns float64 [n_materials, 7]."""
         d = np.ascontiguousarray(d_image, np.float32).reshape(-1)
-        assert d.size == job.width * job.height * 3
+        assert d.size == (num_pixels or job.width * job.height) * 3
         out = np.zeros((self.n_materials, GRAD_PARAMS), np.float64)
-        ad = AdjointDesc(mask, fd_step)
+        ad = AdjointDesc(mask, fd_step, first_pixel, num_pixels)
         _check(lib().tpt_adjoint(self.ctx.h, C.byref(job), C.byref(ad), _p(d), _p(out)), self.ctx)
         return out
 
