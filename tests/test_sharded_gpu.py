@@ -10,6 +10,8 @@
   relative (FP64 atomics: the sums' order differs); the host-buffer entry
   point gives the same band gradient.
 * Ranges past the image end are rejected.
+* The cost-weighted partition from the device-timed pilot renders the same
+  image.
 """
 import numpy as np
 import pytest
@@ -114,3 +116,28 @@ def test_pixel_range_bounds(lit):
         scene.adjoint_device(job, out.data_ptr(), g.data_ptr(), stream=_stream(), first_pixel=W * H, num_pixels=1)
     scene.render_pixels_device(job, W * H, 0, out.data_ptr(), _stream())  # empty range: nothing to do
     torch.cuda.synchronize()
+
+
+def test_pilot_cost_partition(lit):
+    """estimate_row_cost (1-sample pilot, device-timed slabs) gives a finite,
+    positive per-row cost; the 3-rank cost-weighted bands it yields, rendered
+    one by one, equal the whole image bit for bit."""
+    import torch
+
+    sc, scene = lit
+    job = scene.job(sc["camera"], W, H, 16, 5)
+    cost = tpt_dist.estimate_row_cost(scene, job, slabs=8)
+    assert cost.shape == (H,) and np.all(np.isfinite(cost)) and np.all(cost > 0)
+    bands = tpt_dist.balanced_bands(cost, 3)
+    full = torch.empty(W * H * 3, device="cuda")
+    scene.render_device(job, full.data_ptr(), _stream())
+    parts = []
+    for r0, rows in bands:
+        band = torch.empty(rows * W * 3, device="cuda")
+        if rows:
+            scene.render_pixels_device(job, r0 * W, rows * W, band.data_ptr(), _stream())
+        parts.append(band)
+    torch.cuda.synchronize()
+    assert torch.equal(torch.cat(parts), full)
+    one = tpt_dist.render_sharded(scene, job, bands=[(0, H)])
+    assert torch.equal(one.view(-1), full)

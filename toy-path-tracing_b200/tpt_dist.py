@@ -3,9 +3,10 @@ split into row bands.
 
 The reference renders one image per process on the CPU (renderer/src/
 renderer.rs: rayon over the pixels); here a job can span several GPUs, each
-rank rendering the rows of its band through `tpt_render_pixels_device` and the
-bands gathered into one image (NCCL all-gather over NVLink; gloo on CPU in the
-tests).  Pixel streams depend only on (pixel, sample), so the gathered image
+rank rendering the rows of its band through `tpt_render_pixels_device` (equal
+rows, or a cost-weighted static partition from a 1-sample pilot:
+estimate_row_cost + balanced_bands) and the bands gathered into one image
+(NCCL all-gather over NVLink; gloo on CPU in the tests).  Pixel streams depend only on (pixel, sample), so the gathered image
 is bit-identical to a one-GPU render of the whole job.
 
 The adjoint shards the same way: each rank replays the paths of its band
@@ -33,31 +34,120 @@ def pixel_band(rank: int, world: int, width: int, height: int) -> tuple[int, int
     return r0 * width, (r1 - r0) * width
 
 
+def balanced_bands(row_cost, world: int) -> list[tuple[int, int]]:
+    """Cost-weighted static partition: (first_row, rows) per rank, contiguous
+    and in order, so that every band's summed row cost is close to
+    total / world: the boundary after band r is the row boundary whose cost
+    prefix is nearest to (r+1)/world of the total.  Bands may be empty when a
+    few rows carry most of the cost."""
+    import numpy as np
+
+    c = np.asarray(row_cost, np.float64)
+    if c.ndim != 1 or c.size == 0 or not np.all(np.isfinite(c)) or np.any(c < 0):
+        raise ValueError("row costs: a non-empty vector of finite, non-negative numbers")
+    if world < 1:
+        raise ValueError("world >= 1")
+    height = c.size
+    prefix = np.concatenate([[0.0], np.cumsum(c)])
+    total = prefix[-1]
+    if total <= 0:
+        return [(r * height // world, (r + 1) * height // world - r * height // world) for r in range(world)]
+    ends = []
+    for r in range(1, world):
+        target = total * r / world
+        k = int(np.searchsorted(prefix, target, side="left"))
+        # the boundary row nearer the target: the band either ends before or after row k-1
+        if k > 0 and abs(prefix[k - 1] - target) <= abs(prefix[k] - target):
+            k -= 1
+        ends.append(min(max(k, ends[-1] if ends else 0), height))
+    bounds = [0] + ends + [height]
+    return [(bounds[r], bounds[r + 1] - bounds[r]) for r in range(world)]
+
+
+def estimate_row_cost(scene: "tpt.Scene", job, slabs: int = 0, group=None) -> "np.ndarray":
+    """Per-row cost of `job` for balanced_bands, from a 1-sample pilot: the
+    rows are cut into `slabs` equal slabs (default 4 per rank), rank s % world
+    renders and times slab s on the device (CUDA events around
+    tpt_render_pixels_device), the times are summed over the ranks, and each
+    row gets its slab's time per row.  Every rank returns the same vector."""
+    import numpy as np
+
+    rank, world = _world(group)
+    slabs = slabs or 4 * world
+    slabs = max(1, min(slabs, job.height))
+    pilot = tpt.RenderJob.from_buffer_copy(job)
+    pilot.spp = 1
+    width, height = job.width, job.height
+    times = torch.zeros(slabs, dtype=torch.float64)
+    out = torch.empty(-(-height // slabs) * width * 3, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream()
+    for k in range(rank, slabs, world):
+        r0, r1 = k * height // slabs, (k + 1) * height // slabs
+        if r1 == r0:
+            continue
+        scene.render_pixels_device(pilot, r0 * width, (r1 - r0) * width, out.data_ptr(), s.cuda_stream)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        scene.render_pixels_device(pilot, r0 * width, (r1 - r0) * width, out.data_ptr(), s.cuda_stream)
+        e1.record(s)
+        e1.synchronize()
+        times[k] = e0.elapsed_time(e1)
+    if world > 1:
+        t = times.to("cuda" if dist.get_backend(group) == "nccl" else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        times = t.cpu()
+    cost = np.empty(height, np.float64)
+    for k in range(slabs):
+        r0, r1 = k * height // slabs, (k + 1) * height // slabs
+        if r1 > r0:
+            cost[r0:r1] = float(times[k]) / (r1 - r0)
+    return cost
+
+
 def _world(group):
     if dist.is_available() and dist.is_initialized():
         return dist.get_rank(group), dist.get_world_size(group)
     return 0, 1
 
 
-def gather_bands(band: torch.Tensor, width: int, height: int, group=None) -> torch.Tensor:
-    """All-gathers every rank's band (float32 [num_pixels*3], from `pixel_band`)
-    into the image float32 [height, width, 3] on every rank.  The bands are
-    padded to the tallest band's size for the collective."""
+def _band_pixels(rank, world, width, height, bands):
+    """(first_pixel, num_pixels) of `rank`: the equal-row band, or bands[rank]
+    = (first_row, rows) of a balanced_bands partition."""
+    if bands is None:
+        return pixel_band(rank, world, width, height)
+    if len(bands) != world:
+        raise ValueError("one band per rank")
+    pos = 0
+    for r0, rows in bands:
+        if r0 != pos or rows < 0:
+            raise ValueError("bands must tile the rows in order")
+        pos += rows
+    if pos != height:
+        raise ValueError("bands must cover every row")
+    r0, rows = bands[rank]
+    return r0 * width, rows * width
+
+
+def gather_bands(band: torch.Tensor, width: int, height: int, group=None, bands=None) -> torch.Tensor:
+    """All-gathers every rank's band (float32 [num_pixels*3]; the equal-row
+    `pixel_band`, or `bands` from balanced_bands) into the image float32
+    [height, width, 3] on every rank.  The bands are padded to the tallest
+    band's size for the collective."""
     rank, world = _world(group)
-    first, n = pixel_band(rank, world, width, height)
+    first, n = _band_pixels(rank, world, width, height, bands)
     if band.numel() != n * 3:
-        raise ValueError("band size does not match pixel_band")
+        raise ValueError("band size does not match the partition")
     if world == 1:
         return band.view(height, width, 3)
-    rows_max = -(-height // world)
-    padded = torch.zeros(rows_max * width * 3, dtype=torch.float32, device=band.device)
+    sizes = [_band_pixels(r, world, width, height, bands) for r in range(world)]
+    n_max = max(k for _, k in sizes)
+    padded = torch.zeros(max(1, n_max) * 3, dtype=torch.float32, device=band.device)
     padded[: n * 3] = band
     out = torch.empty(world * padded.numel(), dtype=torch.float32, device=band.device)
     dist.all_gather_into_tensor(out, padded, group=group)
     out = out.view(world, -1)
     image = torch.empty(height * width * 3, dtype=torch.float32, device=band.device)
-    for r in range(world):
-        f, k = pixel_band(r, world, width, height)
+    for r, (f, k) in enumerate(sizes):
         image[f * 3:(f + k) * 3] = out[r, : k * 3]
     return image.view(height, width, 3)
 
@@ -72,25 +162,26 @@ def sum_gradients(grad: torch.Tensor, group=None) -> torch.Tensor:
     return grad
 
 
-def render_sharded(scene: "tpt.Scene", job, group=None, stream=None) -> torch.Tensor:
+def render_sharded(scene: "tpt.Scene", job, group=None, stream=None, bands=None) -> torch.Tensor:
     """The job's image float32 [height, width, 3] on this rank's GPU: this rank
-    renders its band, then the bands are all-gathered."""
+    renders its band (equal rows, or `bands` from balanced_bands, the same
+    list on every rank), then the bands are all-gathered."""
     rank, world = _world(group)
-    first, n = pixel_band(rank, world, job.width, job.height)
+    first, n = _band_pixels(rank, world, job.width, job.height, bands)
     band = torch.empty(n * 3, dtype=torch.float32, device="cuda")
     s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
     if n:
         scene.render_pixels_device(job, first, n, band.data_ptr(), s)
-    return gather_bands(band, job.width, job.height, group)
+    return gather_bands(band, job.width, job.height, group, bands)
 
 
 def adjoint_sharded(scene: "tpt.Scene", job, d_image: torch.Tensor, mask: int = 0, fd_step: float = 0.0,
-                    group=None, stream=None) -> torch.Tensor:
+                    group=None, stream=None, bands=None) -> torch.Tensor:
     """dLoss/d(material parameters), float64 [n_materials, 7], summed over the
     ranks.  d_image: dLoss/dimage float32 [height, width, 3] (whole image; each
     rank reads its band) on this rank's GPU."""
     rank, world = _world(group)
-    first, n = pixel_band(rank, world, job.width, job.height)
+    first, n = _band_pixels(rank, world, job.width, job.height, bands)
     d = d_image.contiguous().view(-1)
     if d.numel() != job.width * job.height * 3:
         raise ValueError("d_image must cover the whole image")
