@@ -352,6 +352,10 @@ struct tpt_light_tree {
 extern "C" {
 
 tpt_status tpt_light_tree_build(const tpt_scene_desc* desc, tpt_light_tree** out) {
+  return tpt_light_tree_build_threads(desc, 0, out);
+}
+
+tpt_status tpt_light_tree_build_threads(const tpt_scene_desc* desc, int threads, tpt_light_tree** out) {
   using namespace tpt;
   if (!desc || !out) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL argument");
   *out = nullptr;
@@ -403,7 +407,7 @@ tpt_status tpt_light_tree_build(const tpt_scene_desc* desc, tpt_light_tree** out
   auto* t = new tpt_light_tree();
   HostSceneView v{meshes.data(), desc->num_meshes, inst.data(), desc->num_instances, hm.data(), desc->num_materials,
                   points.data(), desc->num_point_lights, spots.data(), desc->num_spot_lights};
-  if (!build_light_tree_host(v, &t->t)) {
+  if (!build_light_tree_host(v, &t->t, threads)) {
     delete t;
     return set_error(nullptr, TPT_ERR_INVALID_ARG, "no emitter with positive flux: build_light_tree returns None");
   }

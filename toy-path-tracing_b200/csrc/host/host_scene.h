@@ -99,7 +99,8 @@ inline void transform_point_glam(const float* m, const float* p, float* out) {
   out[0] = r[0]; out[1] = r[1]; out[2] = r[2];
 }
 
-bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out);
+// threads <= 0: all hardware threads; the tree does not depend on it.
+bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out, int threads = 0);
 // SpotLight::new (light/spot.rs:32-48) from the C ABI's description.
 void make_spot_light(const float* position, const float* direction, const float* color, float intensity,
                      float total_width_rad, float falloff_start_rad, HostSpotLight* out);

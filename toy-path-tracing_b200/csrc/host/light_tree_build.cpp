@@ -4,12 +4,19 @@
 // algebra of crates/renderer/src/math/sg.rs:203-214, 325-346 for emissive
 // triangles, point lights and spot lights.
 // Node order is the reference's: an interior node is reserved before its left
-// then right subtree (pre-order).  `sort_unstable_by` on centroids
+// then right subtree (pre-order).  The tree is full (every interior node has
+// two children), so a subtree over k emitters holds 2k - 1 nodes and the
+// right child of node i with a left part of k emitters is node i + 2k: the
+// two subtrees write disjoint node and emitter ranges, and large ones are
+// built on separate threads with the same result as one thread.
+// `sort_unstable_by` on centroids
 // (builder.rs:486-490, 758-762) has no defined order for equal keys; here
 // equal centroids keep their emitter registration order.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "host_scene.h"
@@ -160,12 +167,21 @@ struct Cluster {
   }
 };
 
+// Subtrees of at least this many emitters may go to another thread.
+constexpr size_t kParallelMin = 1024;
+
 class TreeBuilder {
  public:
-  explicit TreeBuilder(std::vector<LightNodeHost>* out) : nodes_(*out) {}
+  // `out` is sized to 2n - 1 nodes by the caller; `threads` caps the threads
+  // working at once (the caller's included).
+  TreeBuilder(std::vector<LightNodeHost>* out, int threads) : nodes_(*out), spare_(std::max(0, threads - 1)) {}
 
-  uint32_t build(Leaf* L, size_t n, uint32_t parent) {
-    if (n <= 1) return push_leaf(L[0], parent);
+  // Builds the subtree over L[0, n) at node `idx`.
+  void build(Leaf* L, size_t n, uint32_t parent, uint32_t idx) {
+    if (n <= 1) {
+      put_leaf(L[0], parent, idx);
+      return;
+    }
     Cluster total;
     for (size_t i = 0; i < n; ++i) total.merge_leaf(L[i]);
     total.finish_radius();
@@ -180,11 +196,9 @@ class TreeBuilder {
       split = n / 2;
     }
     split = std::min(std::max<size_t>(split, 1), n - 1);
-    uint32_t idx = (uint32_t)nodes_.size();
-    nodes_.push_back(LightNodeHost{});
-    uint32_t l = build(L, split, idx);
-    uint32_t r = build(L + split, n - split, idx);
+    const uint32_t l = idx + 1, r = idx + 2 * (uint32_t)split;
     LightNodeHost& nd = nodes_[idx];
+    nd = LightNodeHost{};
     nd.left = l;
     nd.right = r;
     nd.parent = parent;
@@ -192,7 +206,15 @@ class TreeBuilder {
     nd.leaf_instance = kInvalidNode;
     nd.leaf_triangle = kInvalidNode;
     nd.area = 0.0f;
-    return idx;
+    if (split >= kParallelMin && n - split >= kParallelMin && take_thread()) {
+      std::thread t([=] { build(L, split, idx, l); });
+      build(L + split, n - split, idx, r);
+      t.join();
+      spare_.fetch_add(1);
+    } else {
+      build(L, split, idx, l);
+      build(L + split, n - split, idx, r);
+    }
   }
 
  private:
@@ -206,8 +228,14 @@ class TreeBuilder {
     nd.radius = radius;
   }
 
-  uint32_t push_leaf(const Leaf& l, uint32_t parent) {
-    uint32_t idx = (uint32_t)nodes_.size();
+  bool take_thread() {
+    int k = spare_.load();
+    while (k > 0)
+      if (spare_.compare_exchange_weak(k, k - 1)) return true;
+    return false;
+  }
+
+  void put_leaf(const Leaf& l, uint32_t parent, uint32_t idx) {
     LightNodeHost nd{};
     fill_cluster(nd, l.flux, l.mu, l.sigma_s2, l.nu_bar, l.radius);
     nd.left = nd.right = kInvalidNode;
@@ -215,8 +243,7 @@ class TreeBuilder {
     nd.leaf_instance = l.inst;
     nd.leaf_triangle = l.tri;
     nd.area = l.area;
-    nodes_.push_back(nd);
-    return idx;
+    nodes_[idx] = nd;
   }
 
   static void sort_axis(Leaf* L, size_t n, int axis) {
@@ -279,6 +306,7 @@ class TreeBuilder {
   }
 
   std::vector<LightNodeHost>& nodes_;
+  std::atomic<int> spare_;
 };
 
 }  // namespace
@@ -334,7 +362,7 @@ void register_area_lights(const HostSceneView& s, std::vector<HostAreaLight>* ou
 
 // Scene::register_area_light_triangles (scene/mod.rs:649-683) + build_light_tree
 // (builder.rs:58-99): emitters in instance/triangle order, leaves with flux > 0.
-bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out) {
+bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out, int threads) {
   out->nodes.clear();
   out->root = kInvalidNode;
   std::vector<Leaf> leaves;
@@ -428,9 +456,14 @@ bool build_light_tree_host(const HostSceneView& s, LightTreeHost* out) {
     leaves.push_back(L);
   }
   if (leaves.empty()) return false;
-  out->nodes.reserve(2 * leaves.size());
-  TreeBuilder b(&out->nodes);
-  out->root = b.build(leaves.data(), leaves.size(), kInvalidNode);
+  if (threads <= 0) {
+    const unsigned hc = std::thread::hardware_concurrency();
+    threads = hc ? (int)hc : 1;
+  }
+  out->nodes.assign(2 * leaves.size() - 1, LightNodeHost{});
+  TreeBuilder b(&out->nodes, threads);
+  b.build(leaves.data(), leaves.size(), kInvalidNode, 0);
+  out->root = 0;
   // fixup_parents (builder.rs:628-644)
   out->nodes[out->root].parent = kInvalidNode;
   for (uint32_t i = 0; i < out->nodes.size(); ++i) {

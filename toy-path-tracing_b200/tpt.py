@@ -274,6 +274,7 @@ EXPORTED_SYMBOLS = [
     "tpt_render_samples_device",
     "tpt_render_pixels_device",
     "tpt_light_tree_build",
+    "tpt_light_tree_build_threads",
     "tpt_light_tree_view_of",
     "tpt_light_tree_free",
     "tpt_render_device_noalloc",
@@ -319,6 +320,7 @@ def _declare(L):
         "tpt_render_samples_device": (i32, [vp, C.POINTER(RenderJob), u64, u64, vp, vp]),
         "tpt_render_pixels_device": (i32, [vp, C.POINTER(RenderJob), u64, u64, vp, vp]),
         "tpt_light_tree_build": (i32, [C.POINTER(SceneDesc), C.POINTER(vp)]),
+        "tpt_light_tree_build_threads": (i32, [C.POINTER(SceneDesc), C.c_int, C.POINTER(vp)]),
         "tpt_light_tree_view_of": (i32, [vp, C.POINTER(LightTreeView)]),
         "tpt_light_tree_free": (i32, [vp]),
         "tpt_render_device_noalloc": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
@@ -544,11 +546,12 @@ def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None, li
     return desc, keep
 
 
-def build_light_tree(scene: dict):
-    """Host light-tree builder (`tpt_light_tree_build`): (nodes[LIGHT_NODE_DTYPE], root)."""
+def build_light_tree(scene: dict, threads: int = 0):
+    """Host light-tree builder (`tpt_light_tree_build_threads`; threads <= 0: all
+    hardware threads): (nodes[LIGHT_NODE_DTYPE], root)."""
     desc, keep = scene_desc(scene["meshes"], scene["instances"], materials=scene["materials"], lights=scene)
     h = C.c_void_p()
-    _check(lib().tpt_light_tree_build(C.byref(desc), C.byref(h)))
+    _check(lib().tpt_light_tree_build_threads(C.byref(desc), threads, C.byref(h)))
     try:
         v = LightTreeView()
         _check(lib().tpt_light_tree_view_of(h, C.byref(v)))
