@@ -175,3 +175,22 @@ def test_three_gloo_ranks_weighted_bands():
         bands, image = res[r]
         assert [k for _, k in bands] == [1, 2, 4]
         assert np.array_equal(image, full)
+
+
+def test_partition_jobs_balances_batches():
+    rng = np.random.default_rng(12)
+    for world in (1, 2, 3, 8):
+        for n_jobs in (0, 1, 5, 64):
+            costs = rng.choice([16, 64, 256], n_jobs) * rng.choice([128 * 128, 640 * 480, 1024 * 768], n_jobs)
+            parts = tpt_dist.partition_jobs(costs, world)
+            assert len(parts) == world
+            assert sorted(j for p in parts for j in p) == list(range(n_jobs))
+            assert all(p == sorted(p) for p in parts)
+            if n_jobs:
+                load = [sum(costs[j] for j in p) for p in parts]
+                # the LPT bound: no rank exceeds the mean by more than its largest job
+                assert max(load) <= costs.sum() / world + costs.max()
+            assert tpt_dist.partition_jobs(costs, world) == parts  # deterministic
+    assert tpt_dist.partition_jobs([5, 4, 3, 3, 3], 2) == [[0, 3], [1, 2, 4]]
+    with pytest.raises(ValueError):
+        tpt_dist.partition_jobs([1.0, float("nan")], 2)

@@ -12,6 +12,8 @@
 * Ranges past the image end are rejected.
 * The cost-weighted partition from the device-timed pilot renders the same
   image.
+* A batch split by job (render_batch_sharded) renders each job as its
+  single-job render.
 """
 import numpy as np
 import pytest
@@ -141,3 +143,19 @@ def test_pilot_cost_partition(lit):
     assert torch.equal(torch.cat(parts), full)
     one = tpt_dist.render_sharded(scene, job, bands=[(0, H)])
     assert torch.equal(one.view(-1), full)
+
+
+def test_batch_sharded_one_rank(ctx, lit):
+    """render_batch_sharded with one rank renders every job of the batch, each
+    image equal to its single-job render bit for bit."""
+    import torch
+
+    sc, scene = lit
+    jobs = [scene.job(sc["camera"], w, h, spp, 5) for w, h, spp in ((32, 24, 16), (17, 9, 64), (40, 29, 4))]
+    images = tpt_dist.render_batch_sharded(ctx, jobs)
+    assert sorted(images) == [0, 1, 2]
+    for j, job in enumerate(jobs):
+        ref = torch.empty(job.width * job.height * 3, device="cuda")
+        scene.render_device(job, ref.data_ptr(), _stream())
+        torch.cuda.synchronize()
+        assert torch.equal(images[j].view(-1), ref)

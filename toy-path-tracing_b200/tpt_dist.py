@@ -14,6 +14,10 @@ The adjoint shards the same way: each rank replays the paths of its band
 the FP64 gradients are summed with one all-reduce, which equals the one-GPU
 gradient up to the order of the FP64 sums.
 
+A batch of jobs splits by job instead (render_batch_sharded): a
+longest-processing-time-first partition on the jobs' costs, each rank
+rendering its jobs in one batched launch sequence.
+
 torch.distributed is the plumbing only; every pixel is rendered by the
 library's kernels.
 """
@@ -192,3 +196,43 @@ def adjoint_sharded(scene: "tpt.Scene", job, d_image: torch.Tensor, mask: int = 
         scene.adjoint_device(job, band.data_ptr(), grad.data_ptr(), mask, fd_step, s, first_pixel=first,
                              num_pixels=n)
     return sum_gradients(grad, group).view(scene.n_materials, tpt.GRAD_PARAMS)
+
+
+def partition_jobs(job_costs, world: int) -> list[list[int]]:
+    """Cost-weighted static partition of a batch of jobs over the ranks:
+    longest-processing-time-first (jobs by decreasing cost, ties by index, each
+    to the rank with the least cost so far, ties to the lower rank), so the
+    slowest rank's cost is at most 4/3 of the best possible.  Returns each
+    rank's job indices in increasing order; the same list on every rank."""
+    costs = [float(c) for c in job_costs]
+    if any(not (c >= 0.0) or c == float("inf") for c in costs):
+        raise ValueError("job costs: finite, non-negative numbers")
+    if world < 1:
+        raise ValueError("world >= 1")
+    load = [0.0] * world
+    owned = [[] for _ in range(world)]
+    for j in sorted(range(len(costs)), key=lambda j: (-costs[j], j)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        load[r] += costs[j]
+        owned[r].append(j)
+    return [sorted(o) for o in owned]
+
+
+def job_cost(job) -> float:
+    """Default job cost for partition_jobs: its samples (width x height x spp)."""
+    return float(job.width) * float(job.height) * float(job.spp)
+
+
+def render_batch_sharded(ctx: "tpt.Context", jobs, group=None, stream=None, costs=None):
+    """Splits a batch of jobs over the ranks (partition_jobs on `costs`, default
+    job_cost) and renders this rank's jobs in one `tpt_render_batch_device`
+    call.  Returns {job index: float32 [height, width, 3] device image} for the
+    jobs this rank owns; no image crosses ranks (a serving caller answers each
+    job from the rank that rendered it)."""
+    rank, world = _world(group)
+    owned = partition_jobs(costs if costs is not None else [job_cost(j) for j in jobs], world)[rank]
+    images = {j: torch.empty(jobs[j].height, jobs[j].width, 3, dtype=torch.float32, device="cuda") for j in owned}
+    if owned:
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        ctx.render_batch_device([jobs[j] for j in owned], [images[j].data_ptr() for j in owned], s)
+    return images
