@@ -307,7 +307,7 @@ tpt_status tpt_light_tree_build(const tpt_scene_desc* desc, tpt_light_tree** out
 /* The same with at most `threads` host threads (<= 0: all hardware threads;
  * no counterpart in the reference, which builds on one): subtrees of 1,024 or
  * more emitters are built in parallel, and the tree is the same for every
- * thread count.  tpt_scene_create builds with all hardware threads. */
+ * thread count.  tpt_scene_upload builds with all hardware threads. */
 tpt_status tpt_light_tree_build_threads(const tpt_scene_desc* desc, int threads, tpt_light_tree** out);
 tpt_status tpt_light_tree_view_of(const tpt_light_tree* tree, tpt_light_tree_view* view);
 tpt_status tpt_light_tree_free(tpt_light_tree* tree);
