@@ -143,6 +143,9 @@ def test_pilot_cost_partition(lit):
     assert torch.equal(torch.cat(parts), full)
     one = tpt_dist.render_sharded(scene, job, bands=[(0, H)])
     assert torch.equal(one.view(-1), full)
+    side = torch.cuda.Stream()  # a caller's stream: ordered against torch's current one
+    two = tpt_dist.render_sharded(scene, job, stream=side.cuda_stream)
+    assert torch.equal(two.view(-1), full)
 
 
 def test_batch_sharded_one_rank(ctx, lit):

@@ -108,6 +108,18 @@ def estimate_row_cost(scene: "tpt.Scene", job, slabs: int = 0, group=None) -> "n
     return cost
 
 
+def _stream_for(stream):
+    """The raw stream the library launches on and a function that makes torch's
+    current stream (where the collectives run) wait for it.  A caller's own
+    stream first waits for the current one, whose tensors it reads."""
+    cur = torch.cuda.current_stream()
+    if stream is None:
+        return cur.cuda_stream, lambda: None
+    ext = torch.cuda.ExternalStream(stream)
+    ext.wait_stream(cur)
+    return stream, lambda: cur.wait_stream(ext)
+
+
 def _world(group):
     if dist.is_available() and dist.is_initialized():
         return dist.get_rank(group), dist.get_world_size(group)
@@ -173,9 +185,10 @@ def render_sharded(scene: "tpt.Scene", job, group=None, stream=None, bands=None)
     rank, world = _world(group)
     first, n = _band_pixels(rank, world, job.width, job.height, bands)
     band = torch.empty(n * 3, dtype=torch.float32, device="cuda")
-    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    s, join = _stream_for(stream)
     if n:
         scene.render_pixels_device(job, first, n, band.data_ptr(), s)
+    join()
     return gather_bands(band, job.width, job.height, group, bands)
 
 
@@ -191,10 +204,11 @@ def adjoint_sharded(scene: "tpt.Scene", job, d_image: torch.Tensor, mask: int = 
         raise ValueError("d_image must cover the whole image")
     band = d[first * 3:(first + n) * 3].contiguous()
     grad = torch.zeros(scene.n_materials * tpt.GRAD_PARAMS, dtype=torch.float64, device="cuda")
-    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    s, join = _stream_for(stream)
     if n:
         scene.adjoint_device(job, band.data_ptr(), grad.data_ptr(), mask, fd_step, s, first_pixel=first,
                              num_pixels=n)
+    join()
     return sum_gradients(grad, group).view(scene.n_materials, tpt.GRAD_PARAMS)
 
 
@@ -232,7 +246,8 @@ def render_batch_sharded(ctx: "tpt.Context", jobs, group=None, stream=None, cost
     rank, world = _world(group)
     owned = partition_jobs(costs if costs is not None else [job_cost(j) for j in jobs], world)[rank]
     images = {j: torch.empty(jobs[j].height, jobs[j].width, 3, dtype=torch.float32, device="cuda") for j in owned}
+    s, join = _stream_for(stream)
     if owned:
-        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         ctx.render_batch_device([jobs[j] for j in owned], [images[j].data_ptr() for j in owned], s)
+    join()
     return images
