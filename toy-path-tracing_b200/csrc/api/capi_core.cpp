@@ -143,6 +143,23 @@ bool is_pinned(const void* p);
 
 }  // namespace
 
+cudaMemPool_t tpt::build_pool(tpt_context* ctx) {
+  if (ctx->build_pool) return ctx->build_pool;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  uint64_t keep = 1ull << 30;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  ctx->build_pool = pool;
+  return pool;
+}
+
 void tpt::build_qbvh_for(tpt_context* ctx, const float* bounds6, uint32_t n, int threads, QbvhHost* out) {
   constexpr uint32_t kGpuBuildMin = 4096;  // below this the host builds faster than a launch sequence
   if (ctx && ctx->gpu_build && n >= kGpuBuildMin) {
@@ -150,7 +167,7 @@ void tpt::build_qbvh_for(tpt_context* ctx, const float* bounds6, uint32_t n, int
     cudaError_t e = cudaMallocAsync((void**)&d, (size_t)6 * n * 4, ctx->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d, bounds6, (size_t)6 * n * 4, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = build_qbvh_gpu(d, n, out, ctx->stream);
+    if (e == cudaSuccess) e = build_qbvh_gpu(d, n, out, ctx->stream, build_pool(ctx));
     if (d) cudaFreeAsync(d, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) return;
@@ -305,6 +322,7 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
     if (ctx->pipe[k]) cudaStreamDestroy(ctx->pipe[k]);
     if (ctx->ev_slot[k]) cudaEventDestroy(ctx->ev_slot[k]);
   }
+  if (ctx->build_pool) cudaMemPoolDestroy(ctx->build_pool);
   if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
   if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
   for (cudaEvent_t e : ctx->ev_in) cudaEventDestroy(e);
@@ -335,7 +353,8 @@ tpt_status tpt_qbvh_build_device(tpt_context* ctx, const float* d_bounds, uint64
   if (n >= (1ull << 24)) return set_error(ctx, TPT_ERR_CAPACITY, "more than 2^24 primitives in one QBVH");
   cudaSetDevice(ctx->device);
   auto* q = new tpt_qbvh();
-  const cudaError_t e = build_qbvh_gpu(d_bounds, (uint32_t)n, &q->q, stream ? (cudaStream_t)stream : ctx->stream);
+  const cudaError_t e =
+      build_qbvh_gpu(d_bounds, (uint32_t)n, &q->q, stream ? (cudaStream_t)stream : ctx->stream, build_pool(ctx));
   if (e != cudaSuccess) {
     delete q;
     if (e == cudaErrorLaunchOutOfResources)

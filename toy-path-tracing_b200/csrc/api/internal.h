@@ -59,6 +59,9 @@ struct tpt_context {
   uint32_t tuned_execution = 0;  // what TPT_EXEC_AUTO means (tpt_autotune)
   uint32_t shade_block = 256;    // threads per block of the wavefront shade stage (128 or 256)
   bool gpu_build = false;        // scene upload builds missing QBVHs on the GPU (tpt_context_set_gpu_build)
+  // stream-ordered pool of the GPU QBVH build: keeps up to 1 GiB mapped between
+  // builds (the default pool unmaps every freed block at the next synchronisation)
+  cudaMemPool_t build_pool = nullptr;
   std::vector<tpt::BounceGraphSet*> graphs;
   uint64_t graph_clock = 0;
   cudaStream_t cap_stream = nullptr;
@@ -120,7 +123,12 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
 // on the device, equal to build_qbvh_host's (a box face at zero may be +0.0
 // where the host keeps -0.0).  Errors: allocation, or capacity (never expected;
 // callers fall back to the host builder).
-cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cudaStream_t s);
+// Scratch comes from `pool` (NULL: the device's default pool).
+cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cudaStream_t s,
+                           cudaMemPool_t pool = nullptr);
+// The context's build pool, created on first use (NULL if that fails: the
+// default pool then serves the build).
+cudaMemPool_t build_pool(tpt_context* ctx);
 // The QBVH of host boxes: on the GPU when the context asks for it and the set is
 // large enough to gain, else (or if the GPU build fails) on the host.
 void build_qbvh_for(tpt_context* ctx, const float* bounds6, uint32_t n, int threads, QbvhHost* out);

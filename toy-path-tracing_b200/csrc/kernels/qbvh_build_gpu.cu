@@ -764,7 +764,7 @@ uint32_t flatten(const std::vector<GNode>& g, uint32_t id, std::vector<QbvhNodeH
 // max xyz) on the device; the result (nodes and primitive order) in `out`.
 // Returns cudaErrorMemoryAllocation / cudaErrorInvalidValue on failure;
 // capacity overflows (never expected) return cudaErrorLaunchOutOfResources.
-cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cudaStream_t s) {
+cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cudaStream_t s, cudaMemPool_t pool) {
   out->nodes.clear();
   out->prim_indices.clear();
   if (n == 0) return cudaErrorInvalidValue;
@@ -772,11 +772,12 @@ cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cu
   const uint32_t seq_cap = n / 4 + 64;
   const uint32_t node_cap = 2 * n + 16;
   std::vector<void*> allocs;
-  // stream-ordered allocations: after the first build they come from the
-  // device's memory pool without synchronising
+  // stream-ordered allocations: with a pool that keeps its memory mapped,
+  // later builds take them without mapping or synchronising
   auto take = [&](size_t bytes) -> void* {
     void* p = nullptr;
-    if (cudaMallocAsync(&p, std::max<size_t>(bytes, 16), s) != cudaSuccess) return nullptr;
+    const size_t b = std::max<size_t>(bytes, 16);
+    if ((pool ? cudaMallocFromPoolAsync(&p, b, pool, s) : cudaMallocAsync(&p, b, s)) != cudaSuccess) return nullptr;
     allocs.push_back(p);
     return p;
   };
