@@ -164,10 +164,13 @@ void tpt::build_qbvh_for(tpt_context* ctx, const float* bounds6, uint32_t n, int
   constexpr uint32_t kGpuBuildMin = 4096;  // below this the host builds faster than a launch sequence
   if (ctx && ctx->gpu_build && n >= kGpuBuildMin) {
     float* d = nullptr;
-    cudaError_t e = cudaMallocAsync((void**)&d, (size_t)6 * n * 4, ctx->stream);
+    cudaMemPool_t pool = build_pool(ctx);
+    const size_t bytes = (size_t)6 * n * 4;
+    cudaError_t e = pool ? cudaMallocFromPoolAsync((void**)&d, bytes, pool, ctx->stream)
+                         : cudaMallocAsync((void**)&d, bytes, ctx->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d, bounds6, (size_t)6 * n * 4, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = build_qbvh_gpu(d, n, out, ctx->stream, build_pool(ctx));
+    if (e == cudaSuccess) e = build_qbvh_gpu(d, n, out, ctx->stream, pool);
     if (d) cudaFreeAsync(d, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) return;
