@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "../api/internal.h"
@@ -725,12 +726,55 @@ __global__ void __launch_bounds__(128) k_seq(const Task* __restrict__ tasks, uin
 
 inline unsigned grid1(uint64_t n, int blk = kBlk) { return (unsigned)((n + blk - 1) / blk); }
 
-// pre-order flattening (qbvh.rs:491-516)
-uint32_t flatten(const std::vector<GNode>& g, uint32_t id, std::vector<QbvhNodeHost>& out) {
+// pre-order flattening (qbvh.rs:491-516).  The interior nodes below a GNode
+// are counted first, so each child subtree knows where its pre-order range
+// starts, and the top two levels hand their subtrees to separate threads
+// (the output is the same as one depth-first pass).
+inline uint32_t kids_of(const GNode& nd, uint32_t* kids) {
+  uint32_t nk = 0;
+  for (int side = 0; side < 2; ++side)
+    for (uint32_t k = 0; k < nd.nkid[side]; ++k) kids[nk++] = nd.kid[side][k];
+  return nk;
+}
+
+uint32_t count_interior(const std::vector<GNode>& g, uint32_t id, std::vector<uint32_t>& cnt, int par_depth) {
+  uint32_t kids[4];
+  const uint32_t nk = kids_of(g[id], kids);
+  uint32_t c = nk ? 1 : 0;
+  if (par_depth > 0 && nk > 1) {
+    std::vector<std::thread> th;
+    for (uint32_t i = 1; i < nk; ++i)
+      th.emplace_back([&, i] { count_interior(g, kids[i], cnt, par_depth - 1); });
+    count_interior(g, kids[0], cnt, par_depth - 1);
+    for (auto& t : th) t.join();
+    for (uint32_t i = 0; i < nk; ++i) c += cnt[kids[i]];
+  } else {
+    for (uint32_t i = 0; i < nk; ++i) c += count_interior(g, kids[i], cnt, 0);
+  }
+  cnt[id] = c;
+  return c;
+}
+
+// Writes the subtree of GNode `id` with its root at out[idx]; returns the
+// child reference (node index, or the leaf's flagged primitive range).
+uint32_t flatten(const std::vector<GNode>& g, uint32_t id, const std::vector<uint32_t>& cnt, QbvhNodeHost* out,
+                 uint32_t idx, int par_depth) {
   const GNode& nd = g[id];
-  if (nd.nkid[0] + nd.nkid[1] == 0) return kLeafFlag | (nd.count << 24) | nd.begin;
-  const uint32_t idx = (uint32_t)out.size();
-  out.emplace_back();
+  uint32_t kids[4];
+  const uint32_t nk = kids_of(nd, kids);
+  if (nk == 0) return kLeafFlag | (nd.count << 24) | nd.begin;
+  uint32_t at[4], refs[4];
+  at[0] = idx + 1;
+  for (uint32_t i = 1; i < nk; ++i) at[i] = at[i - 1] + cnt[kids[i - 1]];
+  if (par_depth > 0 && nk > 1) {
+    std::vector<std::thread> th;
+    for (uint32_t i = 1; i < nk; ++i)
+      th.emplace_back([&, i] { refs[i] = flatten(g, kids[i], cnt, out, at[i], par_depth - 1); });
+    refs[0] = flatten(g, kids[0], cnt, out, at[0], par_depth - 1);
+    for (auto& t : th) t.join();
+  } else {
+    for (uint32_t i = 0; i < nk; ++i) refs[i] = flatten(g, kids[i], cnt, out, at[i], 0);
+  }
   QbvhNodeHost nn;
   for (int s = 0; s < 4; ++s) {
     for (int k = 0; k < 3; ++k) {
@@ -741,17 +785,13 @@ uint32_t flatten(const std::vector<GNode>& g, uint32_t id, std::vector<QbvhNodeH
   }
   nn.valid_mask = 0;
   nn.reserved[0] = nn.reserved[1] = nn.reserved[2] = 0;
-  uint32_t kids[4], nk = 0;
-  for (int side = 0; side < 2; ++side)
-    for (uint32_t k = 0; k < nd.nkid[side]; ++k) kids[nk++] = nd.kid[side][k];
   for (uint32_t i = 0; i < nk; ++i) {
-    const uint32_t ref = flatten(g, kids[i], out);
     const GNode& c = g[kids[i]];
     for (int k = 0; k < 3; ++k) {
       nn.b[k][i] = c.lo[k];
       nn.b[3 + k][i] = c.hi[k];
     }
-    nn.children[i] = ref;
+    nn.children[i] = refs[i];
     nn.valid_mask |= 1u << i;
   }
   out[idx] = nn;
@@ -939,8 +979,11 @@ cudaError_t build_qbvh_gpu(const float* d_bounds6, uint32_t n, QbvhHost* out, cu
     out->prim_indices.clear();
     return e;
   }
-  out->nodes.reserve(g.size() / 2 + 1);
-  flatten(g, 0, out->nodes);
+  // two threaded levels (up to 16 subtrees) once the tree is large enough to gain
+  const int par_depth = g.size() >= (1u << 16) ? 2 : 0;
+  std::vector<uint32_t> cnt(g.size());
+  out->nodes.resize(count_interior(g, 0, cnt, par_depth));
+  flatten(g, 0, cnt, out->nodes.data(), 0, par_depth);
   return cudaSuccess;
 }
 
