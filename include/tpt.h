@@ -14,7 +14,12 @@
  *    during the call.  Device allocations belong to a tpt_context / tpt_scene
  *    handle and are freed by the matching *_destroy / *_release call.
  *  - `*_device` variants take device pointers and a cudaStream_t (as void*,
- *    NULL = the context's stream); they are asynchronous on that stream.
+ *    NULL = the context's stream); they are asynchronous on that stream.  Their
+ *    return value covers argument checks and launches only: the device-side
+ *    checks of the work they queue (traversal stack depth, queue capacity,
+ *    bounded waits, index checks) set a per-context error word that
+ *    tpt_context_check reads once that work has run.  Host-buffer variants read
+ *    it themselves before returning.
  *  - Calls on one context must be serialised by the caller; contexts are
  *    independent.  There is no CPU fallback: without a usable CUDA device
  *    tpt_context_create fails with TPT_ERR_CUDA.
@@ -52,6 +57,16 @@ typedef struct tpt_qbvh tpt_qbvh;
 /* Binds a context to CUDA device `device` and creates its stream. */
 tpt_status tpt_context_create(int device, tpt_context** out);
 tpt_status tpt_context_destroy(tpt_context* ctx);
+/* Waits for `stream` (NULL = the context's stream) and reads, then clears, the
+ * device-side error word that kernels queued by `*_device` calls set when one
+ * of their checks fires (the reference's `ClosestHitError` and debug_assert!s,
+ * scene/mod.rs:100-113, qbvh.rs:666): TPT_ERR_DEVICE_CHECK (traversal stack
+ * deeper than 128 entries, an index check), TPT_ERR_CAPACITY (a device queue
+ * overflowed) or TPT_ERR_TIMEOUT (a bounded wait gave up); the message names
+ * the entry points whose work was queued since the word was last read.  Call
+ * it after a `*_device` call's work (or a captured graph's replay) has been
+ * ordered on `stream`; it cannot be called inside a stream capture. */
+tpt_status tpt_context_check(tpt_context* ctx, void* stream);
 /* Message of the last failed call on `ctx` (or of the last failed context-less
  * call when ctx is NULL).  Valid until the next call on the same context. */
 const char* tpt_last_error(const tpt_context* ctx);
@@ -420,6 +435,19 @@ tpt_status tpt_render_pixels_device(tpt_context* ctx, const tpt_render_job* job,
 tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job, uint64_t first, uint64_t count,
                                      float* out_samples, void* stream);
 
+/* The device's per-pixel sample streams (`PathSampler`, sampler/path_sampler.rs:
+ * 81-141, over the Z-Sobol IndexSampler of sampler/zsobol.rs:206-285 and the
+ * PCG hash of sampler/pcg.rs:1-13), exposed for testing them value for value.
+ * For an image of width x height pixels at spp samples per pixel and n queries
+ * (device, n x 4 uint32, 16-byte aligned: px, py, sample_index, depth):
+ * out (device, n x 16 floats) = camera_sample (2), then
+ * path_vertex_randoms(depth): u_category, u_tree, u_light_aux, u_surface (2),
+ * u_lobe, u_layer, u_dir (2), u_extra0, u_extra1, u_extra2, u_extra3, u_rr;
+ * seeds (device, n x 2) = initial_aux_rng_seed, the vertex's aux_rng_seed.
+ * These are the values every render kernel draws for that (pixel, sample). */
+tpt_status tpt_sampler_values_device(tpt_context* ctx, uint32_t width, uint32_t height, uint32_t spp, uint64_t n,
+                                     const uint32_t* queries, float* out, uint32_t* seeds, void* stream);
+
 /* Autotuner (no counterpart in the reference): times the candidate settings
  * on pilots of `jobs` (each job's rows scaled down: every candidate on at most
  * 2^24 paths, the candidates within 5 % of the best again on at most 2^26) and
@@ -461,8 +489,11 @@ tpt_status tpt_render_batch_device(tpt_context* ctx, const tpt_render_job* jobs,
  * width * height * spp = 2^20 paths per call (12 MiB, held on every device that
  * loads the library until exit); larger jobs fail with TPT_ERR_CAPACITY.
  * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Calls share the array: two calls
- * whose work overlaps on the GPU race.  Output equals tpt_render_device's. */
+ * first call before any stream capture.  Calls share the array and the
+ * kernel's work counter (a fixed word beside the array, not one of the
+ * context's counters): two calls whose work overlaps on the GPU race.  Output
+ * equals tpt_render_device's bit for bit.  Device-side checks surface through
+ * tpt_context_check, as for every `*_device` call. */
 tpt_status tpt_render_device_noalloc(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream);
 
 /* ---- OpenPBR tables and BSDF queries -------------------------------------

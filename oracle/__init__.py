@@ -68,6 +68,9 @@ def _declare(L):
         "orc_geometry_query": (None, [vp, vp, u64, i32, vp, vp, vp, vp, vp, i32]),
         "orc_sampler_vertex_randoms": (None, [u32, u32, u32, u32, u32, u32, u32, vp, vp]),
         "orc_sampler_camera": (None, [u32, u32, u32, u32, u32, u32, vp, vp]),
+        "orc_sampler_values": (None, [u32, u32, u32, u64, vp, vp, vp, C.c_int]),
+        "orc_brute_force_f64": (None, [vp, vp, u64, vp, u64, vp, vp, vp, C.c_int]),
+        "orc_triangle_f64": (None, [vp, vp, vp, vp, u64, vp, vp, C.c_int]),
         "orc_zsobol_sample_index": (u64, [u32, u32, u32, u32, u32, u32, u32]),
         "orc_shuffled_scrambled_sobol": (None, [u32, u32, i32, vp]),
         "orc_uint_to_float": (f32, [u32]),
@@ -226,6 +229,44 @@ def vertex_randoms(px, py, sample, spp, rx, ry, depth):
     seed = np.zeros(1, np.uint32)
     lib().orc_sampler_vertex_randoms(px, py, sample, spp, rx, ry, depth, _p(out), _p(seed))
     return out, int(seed[0])
+
+
+def brute_force_f64(positions, indices, rays, nthreads=None):
+    """FP64 brute force (every ray against every triangle, Moller-Trumbore in
+    double): nearest triangle (-1 = miss), its t, and the nearest other t."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    r = np.ascontiguousarray(rays, np.float32)
+    n = r.shape[1]
+    prim = np.empty(n, np.int32)
+    t1, t2 = np.empty(n, np.float64), np.empty(n, np.float64)
+    lib().orc_brute_force_f64(_p(pos), _p(idx), idx.size // 3, _p(r), n, _p(prim), _p(t1), _p(t2),
+                              nthreads or os.cpu_count() or 1)
+    return prim, t1, t2
+
+
+def triangle_f64(positions, indices, tri, rays, nthreads=None):
+    """FP64 t (+inf on a miss) and smallest barycentric of triangle tri[i] for ray i."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    r = np.ascontiguousarray(rays, np.float32)
+    tr = np.ascontiguousarray(tri, np.int32)
+    n = r.shape[1]
+    t, mb = np.empty(n, np.float64), np.empty(n, np.float64)
+    lib().orc_triangle_f64(_p(pos), _p(idx), _p(tr), _p(r), n, _p(t), _p(mb), nthreads or os.cpu_count() or 1)
+    return t, mb
+
+
+def sampler_values(width, height, spp, queries, nthreads=None):
+    """Per query row (px, py, sample, depth): 16 floats (camera sample, then the
+    vertex randoms in dimension order) and 2 seeds (initial aux seed, vertex aux
+    seed), the layout of tpt_sampler_values_device."""
+    q = np.ascontiguousarray(queries, np.uint32).reshape(-1, 4)
+    out = np.zeros((q.shape[0], 16), np.float32)
+    seeds = np.zeros((q.shape[0], 2), np.uint32)
+    lib().orc_sampler_values(width, height, spp, q.shape[0], _p(q), _p(out), _p(seeds),
+                             nthreads or os.cpu_count() or 1)
+    return out, seeds
 
 
 def camera_sample(px, py, sample, spp, rx, ry):

@@ -219,6 +219,26 @@ void orc_sampler_camera(uint32_t px, uint32_t py, uint32_t sample, uint32_t spp,
   out2[0] = c.x; out2[1] = c.y;
   *aux_seed = s.initial_aux_rng_seed();
 }
+// Per query (px, py, sample, depth) of a width x height image at spp: the
+// camera sample and path_vertex_randoms(depth) (path_sampler.rs:97-118, the 11
+// values in dimension order, u_extra2/3 included) as 16 floats, and the
+// initial and vertex aux seeds; the layout tpt_sampler_values_device writes.
+void orc_sampler_values(uint32_t width, uint32_t height, uint32_t spp, uint64_t n, const uint32_t* q, float* out,
+                        uint32_t* seeds, int nthreads) {
+  parallel_for(n, nthreads, [&](uint64_t i) {
+    const uint32_t* qi = q + 4 * i;
+    PathSampler s(qi[0], qi[1], qi[2], spp, width, height);
+    const Vec2 c = s.camera_sample();
+    const VertexRandoms r = s.path_vertex_randoms(qi[3]);
+    const float v[16] = {c.x, c.y, r.light.u_category, r.light.u_tree, r.light.u_light_aux, r.light.u_surface.x,
+                         r.light.u_surface.y, r.material.u_lobe, r.material.u_layer, r.material.u_dir.x,
+                         r.material.u_dir.y, r.material.u_extra0, r.material.u_extra1, r.material.u_extra2,
+                         r.material.u_extra3, r.u_rr};
+    std::memcpy(out + 16 * i, v, sizeof v);
+    seeds[2 * i] = s.initial_aux_rng_seed();
+    seeds[2 * i + 1] = r.aux_rng_seed;
+  });
+}
 uint64_t orc_zsobol_sample_index(uint32_t spp, uint32_t rx, uint32_t ry, uint32_t px, uint32_t py, uint32_t sample,
                                  uint32_t dim) {
   IndexSampler s(spp, rx, ry);

@@ -230,3 +230,28 @@ def test_camera_center_and_normalised_and_differentials():
     assert np.all(r[6:9] == r[0:3]) and np.all(r[9:12] == r[0:3])
     assert np.any(r[12:15] != r[3:6]) and np.any(r[15:18] != r[3:6])
     assert r[19] > 0
+
+
+def test_oracle_traversal_matches_fp64_brute_force():
+    """The oracle's QBVH traversal (qbvh.rs:611-675 + math/ray.rs:107-209 in f32)
+    finds the nearest triangle of an FP64 brute force over every triangle, as
+    the reference's traverse_closest_matches_brute_force_on_grid
+    (qbvh.rs:902-969) checks: the same triangle, or a tie within 1e-6 t."""
+    import tpt_scenes
+
+    mesh = tpt_scenes.sphere_soup(seed=5, n_spheres=64, cube=8.0)
+    rays = tpt_scenes.incoherent_rays(4096, seed=9, cube=8.0)
+    g = orc.Geometry()
+    g.add_mesh(mesh["positions"], mesh["indices"])
+    g.add_instance(0, 0, np.eye(4, dtype=np.float32), np.eye(4, dtype=np.float32), np.eye(3, dtype=np.float32))
+    g.build()
+    ref = g.query(rays, 0)
+    bp, bt, _ = orc.brute_force_f64(mesh["positions"], mesh["indices"], rays)
+    assert (bp >= 0).sum() > 1000
+    assert np.array_equal(ref["prim"] >= 0, bp >= 0)
+    t64, _ = orc.triangle_f64(mesh["positions"], mesh["indices"], ref["prim"], rays)
+    same = ref["prim"] == bp
+    with np.errstate(invalid="ignore"):  # inf - inf on rays both miss (they are `same`)
+        assert np.all(same | (np.abs(t64 - bt) <= 1e-6 * bt))
+    hit = bp >= 0
+    assert np.all(np.abs(ref["t"][hit] - bt[hit]) <= 1e-5 * bt[hit] + 2.0 ** -20 * 8.0)

@@ -111,3 +111,22 @@ def test_vertex_randoms_in_unit_interval_and_deterministic():
     assert np.all((a >= 0) & (a < 1))
     c, _ = orc.vertex_randoms(3, 5, 8, 64, 256, 256, 2)
     assert not np.array_equal(a, c)
+
+
+def test_sampler_values_layout_matches_the_per_call_queries():
+    """orc_sampler_values (the layout the device query is compared in) gives the
+    same values as camera_sample / vertex_randoms, which the tests above pin to
+    the reference's known answers."""
+    rng = np.random.default_rng(5)
+    for w, h, spp in ((256, 256, 64), (1920, 1080, 48), (5, 3, 1)):
+        q = np.stack([rng.integers(0, w, 200), rng.integers(0, h, 200), rng.integers(0, spp, 200),
+                      rng.integers(0, 17, 200)], 1).astype(np.uint32)
+        vals, seeds = orc.sampler_values(w, h, spp, q)
+        for i in range(0, 200, 7):
+            px, py, s, d = (int(x) for x in q[i])
+            cam, seed0 = orc.camera_sample(px, py, s, spp, w, h)
+            vr, seed_v = orc.vertex_randoms(px, py, s, spp, w, h, d)
+            assert np.array_equal(vals[i, :2], cam) and seeds[i, 0] == seed0
+            # vertex_randoms: 11 values without u_extra2/3, then u_rr
+            assert np.array_equal(vals[i, 2:13], vr[:11]) and vals[i, 15] == vr[11]
+            assert seeds[i, 1] == seed_v

@@ -99,7 +99,7 @@ tpt_status tpt_scene_set_openpbr(tpt_context* ctx, tpt_scene* scene, uint32_t co
                                  const tpt_openpbr_desc* descs, void* stream) {
   if (!ctx || !scene) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL context or scene");
   if (count && (!material_ids || !descs)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL material list");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   std::vector<DevOpenPbr> recs(count);
   for (uint32_t k = 0; k < count; ++k) {
@@ -138,7 +138,8 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   if (mask & ~(uint32_t)TPT_GRAD_ALL) return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown gradient group bits");
   const float step = adesc && adesc->fd_step > 0.0f ? adesc->fd_step : kDefaultFdStep;
   if (!(step < 0.5f)) return set_error(ctx, TPT_ERR_INVALID_ARG, "fd_step must be in (0, 0.5)");
-  cudaSetDevice(ctx->device);
+  if ((st = set_device(ctx))) return st;
+  note_device_call(ctx, "tpt_adjoint_device");
   tpt_scene* scene = const_cast<tpt_scene*>(job->scene);
   if ((st = ensure_adjoint_tables(ctx, scene, mask, step))) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
@@ -191,7 +192,7 @@ tpt_status tpt_adjoint(tpt_context* ctx, const tpt_render_job* job, const tpt_ad
                        const float* d_image, double* grad) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (!job || !job->scene || !d_image || !grad) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL argument");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   const size_t ibytes =
       (size_t)(adesc && adesc->num_pixels ? adesc->num_pixels : (uint64_t)job->width * job->height) * 12;
   const size_t gbytes = (size_t)job->scene->render.num_materials * kGradParams * sizeof(double);

@@ -48,7 +48,7 @@ extern "C" {
 tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, tpt_tune_result* out) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (n_jobs <= 0 || !jobs || !out) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad job list");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   uint64_t total = 0;
   for (int j = 0; j < n_jobs; ++j) {
     RenderLaunch L;

@@ -140,8 +140,9 @@ tpt_status tpt_render_batch_device(tpt_context* ctx, const tpt_render_job* jobs,
                                    void* stream) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (n_jobs < 0 || (n_jobs && (!jobs || !out_rgb))) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad job list");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  note_device_call(ctx, "tpt_render_batch_device");
   return render_batch(ctx, jobs, n_jobs, out_rgb, s, ctx->batch_capacity);
 }
 

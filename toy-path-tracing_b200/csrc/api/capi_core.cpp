@@ -32,19 +32,33 @@ tpt_status cuda_check(tpt_context* ctx, cudaError_t e, const char* what) {
   return set_error(ctx, TPT_ERR_CUDA, m);
 }
 
+void note_device_call(tpt_context* ctx, const char* name) {
+  auto& v = ctx->unchecked_calls;
+  for (const std::string& n : v)
+    if (n == name) return;
+  if (v.size() < 16) v.emplace_back(name);
+}
+
+tpt_status set_device(tpt_context* ctx) { return cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice"); }
+
 tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream) {
   uint32_t h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, ctx->d_err, 4, cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_check(ctx, e, "reading device error word");
+  std::string who;
+  for (const std::string& n : ctx->unchecked_calls) who += (who.empty() ? "" : ", ") + n;
+  ctx->unchecked_calls.clear();
   if (h == 0) return TPT_OK;
   cudaMemsetAsync(ctx->d_err, 0, 4, stream);
   cudaStreamSynchronize(stream);
-  if (h & kDevErrTimeout) return set_error(ctx, TPT_ERR_TIMEOUT, "device-side bounded wait expired");
-  if (h & kDevErrCapacity) return set_error(ctx, TPT_ERR_CAPACITY, "device queue capacity exceeded");
+  const std::string from = who.empty() ? std::string() : " (in work queued by " + who + ")";
+  if (h & kDevErrTimeout) return set_error(ctx, TPT_ERR_TIMEOUT, "device-side bounded wait expired" + from);
+  if (h & kDevErrCapacity) return set_error(ctx, TPT_ERR_CAPACITY, "device queue capacity exceeded" + from);
   if (h & kDevErrStackOverflow)
-    return set_error(ctx, TPT_ERR_DEVICE_CHECK, "traversal stack depth 128 exceeded (reference limit, qbvh.rs:609)");
-  return set_error(ctx, TPT_ERR_DEVICE_CHECK, "device index check failed (flags " + std::to_string(h) + ")");
+    return set_error(ctx, TPT_ERR_DEVICE_CHECK,
+                     "traversal stack depth 128 exceeded (reference limit, qbvh.rs:609)" + from);
+  return set_error(ctx, TPT_ERR_DEVICE_CHECK, "device index check failed (flags " + std::to_string(h) + ")" + from);
 }
 
 unsigned long long* next_counter(tpt_context* ctx) {
@@ -336,6 +350,13 @@ tpt_status tpt_context_destroy(tpt_context* ctx) {
   return TPT_OK;
 }
 
+tpt_status tpt_context_check(tpt_context* ctx, void* stream) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  tpt_status st = set_device(ctx);
+  if (st) return st;
+  return check_device_errors(ctx, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
 // ---- host QBVH builder -----------------------------------------------------
 tpt_status tpt_qbvh_build(const float* bounds, uint64_t n, int threads, tpt_qbvh** out) {
   if (!out || (!bounds && n)) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL argument");
@@ -354,7 +375,7 @@ tpt_status tpt_qbvh_build_device(tpt_context* ctx, const float* d_bounds, uint64
   *out = nullptr;
   if (n == 0) return set_error(ctx, TPT_ERR_INVALID_ARG, "no primitives (build_qbvh returns None)");
   if (n >= (1ull << 24)) return set_error(ctx, TPT_ERR_CAPACITY, "more than 2^24 primitives in one QBVH");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   auto* q = new tpt_qbvh();
   const cudaError_t e =
       build_qbvh_gpu(d_bounds, (uint32_t)n, &q->q, stream ? (cudaStream_t)stream : ctx->stream, build_pool(ctx));
@@ -394,7 +415,7 @@ tpt_status tpt_scene_upload(tpt_context* ctx, const tpt_scene_desc* desc, tpt_sc
   *out = nullptr;
   if (desc->num_meshes && !desc->meshes) return set_error(ctx, TPT_ERR_INVALID_ARG, "meshes is NULL");
   if (desc->num_instances && !desc->instances) return set_error(ctx, TPT_ERR_INVALID_ARG, "instances is NULL");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   const int threads = host_threads(0);
 
   std::vector<DevNode> nodes;
@@ -602,7 +623,10 @@ tpt_status tpt_traverse_device(tpt_context* ctx, const tpt_scene* scene, const f
   if (!ctx || !scene) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL context or scene");
   if (n && (!rays || !prim || !t)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL ray or output buffer");
   if (mode != TPT_CLOSEST_HIT && mode != TPT_ANY_HIT) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad mode");
+  tpt_status st = set_device(ctx);
+  if (st) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  note_device_call(ctx, "tpt_traverse_device");
   return cuda_check(ctx,
                     launch_traverse_strided(scene->geo, rays, n, n, mode, prim, t, instance, bary, n,
                                             next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr, nullptr),
@@ -616,8 +640,11 @@ tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, c
   if (n && (!rays || !prim || !t || !node_tests || !tri_tests))
     return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
   if (mode != TPT_CLOSEST_HIT && mode != TPT_ANY_HIT) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad mode");
+  tpt_status st = set_device(ctx);
+  if (st) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  tpt_status st = cuda_check(ctx,
+  note_device_call(ctx, "tpt_traverse_stats_device");
+  st = cuda_check(ctx,
                              launch_traverse_strided(scene->geo, rays, n, n, mode, prim, t, nullptr, nullptr, n,
                                                      next_counter(ctx), ctx->d_err, ctx->num_sms, s, node_tests,
                                                      tri_tests),
@@ -632,8 +659,8 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
   if (n == 0) return TPT_OK;
   if (!rays || !prim || !t) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL ray or output buffer");
   if (mode != TPT_CLOSEST_HIT && mode != TPT_ANY_HIT) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad mode");
-  cudaSetDevice(ctx->device);
-  tpt_status st = ensure_pipeline(ctx);
+  tpt_status st = set_device(ctx);
+  if (!st) st = ensure_pipeline(ctx);
   if (st) return st;
   // Device buffers for the whole batch: rays (7 planes) then outputs.
   const int n_out = 2 + (instance ? 1 : 0) + (bary ? 3 : 0);

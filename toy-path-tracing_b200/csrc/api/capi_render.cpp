@@ -305,8 +305,9 @@ tpt_status tpt_render_pixels_device(tpt_context* ctx, const tpt_render_job* job,
   const uint64_t total = (uint64_t)L.width * L.height;
   if (first_pixel > total || num_pixels > total - first_pixel)
     return set_error(ctx, TPT_ERR_INVALID_ARG, "pixel range out of bounds");
-  cudaSetDevice(ctx->device);
+  if ((st = set_device(ctx))) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  note_device_call(ctx, first_pixel == 0 && num_pixels == total ? "tpt_render_device" : "tpt_render_pixels_device");
   const uint32_t pix_begin = (uint32_t)first_pixel, pix_end = (uint32_t)(first_pixel + num_pixels);
   const uint32_t cp = chunk_pixels(L, ctx->batch_capacity);
   if ((st = ensure_scratch(ctx, (size_t)cp * L.spp * 12))) return st;
@@ -338,8 +339,9 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
   const uint64_t total = (uint64_t)L.width * L.height * L.spp;
   if (first > total || count > total - first) return set_error(ctx, TPT_ERR_INVALID_ARG, "path range out of bounds");
   if (count && !out_samples) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL output");
-  cudaSetDevice(ctx->device);
+  if ((st = set_device(ctx))) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  note_device_call(ctx, "tpt_render_samples_device");
   const uint32_t exec = job->execution == TPT_EXEC_AUTO ? ctx->tuned_execution : job->execution;
   if (job->integrator == TPT_INTEGRATOR_BDPT && exec != TPT_EXEC_MEGAKERNEL)
     return render_bdpt_wavefront(ctx, job, L, first, count, out_samples, s);
@@ -359,7 +361,7 @@ tpt_status tpt_render_samples_device(tpt_context* ctx, const tpt_render_job* job
 tpt_status tpt_render(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, float* const* out_rgb) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (n_jobs < 0 || (n_jobs && (!jobs || !out_rgb))) return set_error(ctx, TPT_ERR_INVALID_ARG, "bad job list");
-  cudaSetDevice(ctx->device);
+  if (tpt_status st = set_device(ctx)) return st;
   // several MIS wavefront jobs: one batched launch sequence
   bool batch = n_jobs > 1;
   for (int j = 0; j < n_jobs && batch; ++j) {

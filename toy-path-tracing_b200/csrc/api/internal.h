@@ -24,6 +24,9 @@ struct tpt_context {
   uint32_t* d_err = nullptr;  // device error word
   int num_sms = 0;
   std::string last_error;
+  // *_device entry points that queued work since the device error word was
+  // last read (tpt_context_check, or a host-buffer call that synchronises)
+  std::vector<std::string> unchecked_calls;
   // pinned staging for the host-pointer entry points
   void* h_stage = nullptr;
   size_t h_stage_bytes = 0;
@@ -107,8 +110,13 @@ constexpr uint32_t kGraphCounterSlots = 32;  // the last slots: two per cached b
 
 tpt_status set_error(tpt_context* ctx, tpt_status st, const std::string& msg);
 tpt_status cuda_check(tpt_context* ctx, cudaError_t e, const char* what);
-// Reads and clears the device error word (synchronising `stream`).
+// Reads and clears the device error word (synchronising `stream`); an error
+// names the *_device calls whose work ran since the last read.
 tpt_status check_device_errors(tpt_context* ctx, cudaStream_t stream);
+// Records that entry point `name` queued device work whose checks are read later.
+void note_device_call(tpt_context* ctx, const char* name);
+// cudaSetDevice(ctx->device) with its status checked.
+tpt_status set_device(tpt_context* ctx);
 
 // kernels (traverse_kernels.cu).  Ray plane p of ray i at rays[p * rs + i];
 // barycentric output plane p at bary[p * bs + i].  `counter` is a device word

@@ -16,6 +16,7 @@
 #include <atomic>
 #include <cmath>
 #include <numeric>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -206,8 +207,17 @@ class TreeBuilder {
     nd.leaf_instance = kInvalidNode;
     nd.leaf_triangle = kInvalidNode;
     nd.area = 0.0f;
+    std::thread t;
+    bool threaded = false;
     if (split >= kParallelMin && n - split >= kParallelMin && take_thread()) {
-      std::thread t([=] { build(L, split, idx, l); });
+      try {
+        t = std::thread([=] { build(L, split, idx, l); });
+        threaded = true;
+      } catch (const std::exception&) {
+        spare_.fetch_add(1);  // no thread could be started: build both halves here
+      }
+    }
+    if (threaded) {
       build(L + split, n - split, idx, r);
       t.join();
       spare_.fetch_add(1);

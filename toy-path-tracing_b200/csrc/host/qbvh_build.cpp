@@ -101,7 +101,13 @@ class Builder {
   }
   void worker_loop_until_done() {
     std::vector<std::thread> pool;
-    for (int i = 1; i < threads_; ++i) pool.emplace_back([this] { work(); });
+    for (int i = 1; i < threads_; ++i) {
+      try {
+        pool.emplace_back([this] { work(); });
+      } catch (const std::exception&) {
+        break;  // fewer workers (thread limit): the tasks are the same, the tree too
+      }
+    }
     work();
     for (auto& t : pool) t.join();
   }

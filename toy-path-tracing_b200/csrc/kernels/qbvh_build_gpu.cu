@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -742,10 +743,20 @@ uint32_t count_interior(const std::vector<GNode>& g, uint32_t id, std::vector<ui
   const uint32_t nk = kids_of(g[id], kids);
   uint32_t c = nk ? 1 : 0;
   if (par_depth > 0 && nk > 1) {
+    // a child whose thread cannot be started (thread limit, memory) is counted
+    // on this thread instead: the counts do not depend on who computes them
     std::vector<std::thread> th;
-    for (uint32_t i = 1; i < nk; ++i)
-      th.emplace_back([&, i] { count_interior(g, kids[i], cnt, par_depth - 1); });
+    bool serial[4] = {false, false, false, false};
+    for (uint32_t i = 1; i < nk; ++i) {
+      try {
+        th.emplace_back([&, i] { count_interior(g, kids[i], cnt, par_depth - 1); });
+      } catch (const std::exception&) {
+        serial[i] = true;
+      }
+    }
     count_interior(g, kids[0], cnt, par_depth - 1);
+    for (uint32_t i = 1; i < nk; ++i)
+      if (serial[i]) count_interior(g, kids[i], cnt, 0);
     for (auto& t : th) t.join();
     for (uint32_t i = 0; i < nk; ++i) c += cnt[kids[i]];
   } else {
@@ -767,10 +778,20 @@ uint32_t flatten(const std::vector<GNode>& g, uint32_t id, const std::vector<uin
   at[0] = idx + 1;
   for (uint32_t i = 1; i < nk; ++i) at[i] = at[i - 1] + cnt[kids[i - 1]];
   if (par_depth > 0 && nk > 1) {
+    // as in count_interior: a subtree whose thread cannot start is flattened
+    // here; every subtree owns its pre-order range, so the tree is the same
     std::vector<std::thread> th;
-    for (uint32_t i = 1; i < nk; ++i)
-      th.emplace_back([&, i] { refs[i] = flatten(g, kids[i], cnt, out, at[i], par_depth - 1); });
+    bool serial[4] = {false, false, false, false};
+    for (uint32_t i = 1; i < nk; ++i) {
+      try {
+        th.emplace_back([&, i] { refs[i] = flatten(g, kids[i], cnt, out, at[i], par_depth - 1); });
+      } catch (const std::exception&) {
+        serial[i] = true;
+      }
+    }
     refs[0] = flatten(g, kids[0], cnt, out, at[0], par_depth - 1);
+    for (uint32_t i = 1; i < nk; ++i)
+      if (serial[i]) refs[i] = flatten(g, kids[i], cnt, out, at[i], 0);
     for (auto& t : th) t.join();
   } else {
     for (uint32_t i = 0; i < nk; ++i) refs[i] = flatten(g, kids[i], cnt, out, at[i], 0);

@@ -255,6 +255,7 @@ def lib():
 EXPORTED_SYMBOLS = [
     "tpt_context_create",
     "tpt_context_destroy",
+    "tpt_context_check",
     "tpt_last_error",
     "tpt_version",
     "tpt_qbvh_build",
@@ -278,6 +279,7 @@ EXPORTED_SYMBOLS = [
     "tpt_light_tree_view_of",
     "tpt_light_tree_free",
     "tpt_render_device_noalloc",
+    "tpt_sampler_values_device",
     "tpt_openpbr_defaults",
     "tpt_lut_dielectric_albedo",
     "tpt_lut_conductor_ec",
@@ -301,6 +303,7 @@ def _declare(L):
     sig = {
         "tpt_context_create": (i32, [i32, C.POINTER(vp)]),
         "tpt_context_destroy": (i32, [vp]),
+        "tpt_context_check": (i32, [vp, vp]),
         "tpt_last_error": (cp, [vp]),
         "tpt_version": (cp, []),
         "tpt_qbvh_build": (i32, [vp, u64, i32, C.POINTER(vp)]),
@@ -324,6 +327,7 @@ def _declare(L):
         "tpt_light_tree_view_of": (i32, [vp, C.POINTER(LightTreeView)]),
         "tpt_light_tree_free": (i32, [vp]),
         "tpt_render_device_noalloc": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
+        "tpt_sampler_values_device": (i32, [vp, C.c_uint32, C.c_uint32, C.c_uint32, u64, vp, vp, vp, vp]),
         "tpt_openpbr_defaults": (None, [C.POINTER(OpenPbrDesc)]),
         "tpt_lut_dielectric_albedo": (i32, [vp, C.c_float, vp]),
         "tpt_lut_conductor_ec": (i32, [vp, vp, vp]),
@@ -378,6 +382,11 @@ class Context:
             lib().tpt_context_destroy(self.h)
             self.h = None
 
+    def check(self, stream=None):
+        """`tpt_context_check`: waits for `stream` and raises TptError when a
+        device-side check of work queued by `*_device` calls fired."""
+        _check(lib().tpt_context_check(self.h, _stream(stream)), self)
+
     @property
     def wavefront_capacity(self) -> int:
         return int(lib().tpt_context_wavefront_capacity(self.h))
@@ -400,6 +409,21 @@ class Context:
         r = TuneResult()
         _check(lib().tpt_autotune(self.h, arr, len(jobs), C.byref(r)), self)
         return {k: getattr(r, k) for k, _ in TuneResult._fields_}
+
+    def sampler_values(self, width: int, height: int, spp: int, queries: np.ndarray):
+        """`tpt_sampler_values_device`: the device's sample values for query rows
+        (px, py, sample, depth) -> (n x 16 floats, n x 2 seeds) on the host."""
+        import torch
+
+        q = torch.from_numpy(np.ascontiguousarray(queries, np.uint32).reshape(-1, 4).view(np.int32)).cuda()
+        n = q.shape[0]
+        out = torch.empty((n, 16), dtype=torch.float32, device="cuda")
+        seeds = torch.empty((n, 2), dtype=torch.int32, device="cuda")
+        _check(lib().tpt_sampler_values_device(self.h, width, height, spp, n, C.c_void_p(q.data_ptr()),
+                                               C.c_void_p(out.data_ptr()), C.c_void_p(seeds.data_ptr()), None),
+               self)
+        self.check()
+        return out.cpu().numpy(), seeds.cpu().numpy().view(np.uint32)
 
     def set_shade_block(self, threads: int):
         """`tpt_context_set_shade_block`: 128 or 256 threads per shade block."""

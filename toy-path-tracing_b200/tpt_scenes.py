@@ -475,11 +475,13 @@ BATCH_RESOLUTIONS = [(128, 128), (256, 192), (512, 384), (640, 480), (1024, 768)
 BATCH_SPP = [16, 64, 256]
 
 
-def batch_jobs(seed: int = 4, n_jobs: int = 64, spp_scale: float = 1.0):
+def batch_jobs(seed: int = 4, n_jobs: int = 64, spp_scale: float = 1.0, only=None):
     """The batched-render workload: n_jobs seeded grid_scene variants with
     10k-500k triangles (log-uniform), 4-1024 emissive triangles, 8-64
     materials, a resolution from BATCH_RESOLUTIONS, spp from BATCH_SPP (times
-    spp_scale, at least 1) and max depth 8-16.  Returns (scene dicts, job specs)."""
+    spp_scale, at least 1) and max depth 8-16.  Returns (scene dicts, job specs).
+    only: job indices to build (the others' random draws are still made, so job
+    k is the same scene and spec either way); each spec then carries "job": k."""
     rng = np.random.default_rng(seed)
     scenes, specs = [], []
     for k in range(n_jobs):
@@ -487,10 +489,13 @@ def batch_jobs(seed: int = 4, n_jobs: int = 64, spp_scale: float = 1.0):
         n_side = int(rng.integers(4, 17))
         per = max(24, int(tris / (n_side * n_side)))
         emis = int(np.exp(rng.uniform(np.log(4), np.log(1024))))
-        sc = grid_scene(seed=1000 + k, n_side=n_side, tris_per_object=per, n_materials=int(rng.integers(8, 65)),
-                        n_emissive_tris=emis)
+        n_mat = int(rng.integers(8, 65))
         w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
         spp = max(1, int(round(BATCH_SPP[int(rng.integers(0, len(BATCH_SPP)))] * spp_scale)))
-        scenes.append(sc)
-        specs.append({"width": w, "height": h, "spp": spp, "max_depth": int(rng.integers(8, 17))})
+        depth = int(rng.integers(8, 17))
+        if only is not None and k not in only:
+            continue
+        scenes.append(grid_scene(seed=1000 + k, n_side=n_side, tris_per_object=per, n_materials=n_mat,
+                                 n_emissive_tris=emis))
+        specs.append({"width": w, "height": h, "spp": spp, "max_depth": depth, "job": k})
     return scenes, specs
