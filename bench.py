@@ -60,9 +60,11 @@ def parse_args():
     p.add_argument("--no-large", action="store_true", help="skip the large-scene render block")
     p.add_argument("--no-batch", action="store_true", help="skip the batched-render block")
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-render block")
-    p.add_argument("--large-spp", type=int, default=16, help="spp timed on the large scene")
+    p.add_argument("--large-spp", type=int, default=256, help="MIS spp timed on the large scene (configured: 256)")
+    p.add_argument("--large-bdpt-spp", type=int, default=16,
+                   help="BDPT spp timed on the large scene (configured: 256; 16 keeps the block to seconds)")
     p.add_argument("--adjoint-steps", type=int, default=200, help="Adam steps of the inverse-rendering run")
-    p.add_argument("--batch-spp-scale", type=float, default=0.25, help="spp scale of the batched workload")
+    p.add_argument("--batch-spp-scale", type=float, default=1.0, help="spp scale of the batched workload")
     return p.parse_args()
 
 
@@ -139,25 +141,60 @@ def cpu_reference_rate(mesh, batches, target_s=8.0, max_log2=24):
         k += 1 if dt > target_s / 4 else 2
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def run_reference(args):
+    """The reference arm: the oracle's traverser (the CPU restatement of
+    qbvh.rs / Scene::closest_hit) on all host cores.  Each step is one bounded
+    sample of the workload -- 2^20 rays of each batch, closest hit and any hit
+    (4 x 2^20 queries) -- and ms_per_step is that sample's own wall time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    import oracle as orc
+
     mesh, batches = make_workload(0, args.rays_log2)
-    rates = []
-    desc = None
-    threads = 1
-    for _ in range(args.warmup + args.steps):
-        r, threads, desc = cpu_reference_rate(mesh, batches, target_s=2.0, max_log2=20)
-        rates.append(r)
-    rate = float(np.median(rates[args.warmup:]))
-    per_step_s = (4 << args.rays_log2) / rate
+    g = orc.Geometry()
+    g.add_mesh(mesh["positions"], mesh["indices"])
+    g.add_instance(0, 0, np.eye(4, dtype=np.float32), np.eye(4, dtype=np.float32), np.eye(3, dtype=np.float32))
+    g.build()
+    threads = os.cpu_count() or 1
+    m = min(1 << 20, batches[0].shape[1])
+    rng = np.random.default_rng(0)
+    samples = [np.ascontiguousarray(b[:, np.sort(rng.choice(b.shape[1], m, replace=False))]) for b in batches]
+
+    def one_step(nthreads):
+        t0 = time.perf_counter()
+        for sample in samples:
+            for mode in (0, 1):
+                g.query(sample, mode, nthreads=nthreads)
+        return time.perf_counter() - t0
+
+    times = [one_step(threads) for _ in range(args.warmup + args.steps)][args.warmup:]
+    step_s = float(np.median(times))
+    queries = 4 * m
+    rate = queries / step_s
+    # the reference's own default thread count: logical cores - 2 (main.rs:134-138)
+    ref_threads = max(1, threads - 2)
+    rate_default = queries / one_step(ref_threads)
+    desc = (f"each step: {m} rays from each of the 2 batches x (closest, any) = {queries} queries "
+            f"({queries / (4 << args.rays_log2):.4f} of a full step), median {step_s:.2f} s")
     line = {
         "metric": METRIC, "value": rate, "unit": "rays/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": per_step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sphere soup + ray batches)",
         "config": config_dict(args, 1), "impl": "reference",
-        "cpu_baseline": {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc},
+        "cpu_baseline": {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc,
+                         "cpu_model": cpu_model(),
+                         "reference_default_threads": ref_threads, "value_at_reference_default": rate_default},
         "e2e": {"value": rate, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -209,13 +246,69 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+def profiled(key):
+    """A per-launch figure of the dominant kernel from the committed ncu summary
+    (dram / L2 / L1 bytes of a full 2^24-ray launch, L1 throughput %)."""
     p = os.path.join(ROOT, "profiles", "traverse_closest_incoherent_1M.txt")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_full_launch:\s*([0-9.eE+]+)", open(p).read())
+    m = re.search(key + r":\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
+
+
+def profiled_traffic():
+    """dram bytes per launch of the dominant kernel from the committed ncu summary."""
+    return profiled("dram_bytes_per_full_launch")
+
+
+# render algorithmic bytes: the traversal account above for every ray traced
+# (path and shadow/visibility rays), plus per hit of a path ray its vertex data
+# and per shading event its material record
+ALGO_BYTES_HIT_VERTEX = 96
+ALGO_BYTES_SHADING_EVENT = 160
+
+
+def render_counts(ctx, scene, job):
+    """Rays, node tests, triangle tests and hits of one wavefront render of
+    `job` (tpt_context_set_render_stats; untimed).  The megakernel traces the
+    same rays (its samples equal the wavefront's bit for bit)."""
+    import torch
+
+    import tpt
+
+    cnt = torch.zeros(8, dtype=torch.int64, device="cuda")
+    img = torch.empty(job.width * job.height * 3, device="cuda")
+    j = tpt.RenderJob.from_buffer_copy(job)
+    j.execution = tpt.EXEC_WAVEFRONT
+    ctx.set_render_stats(cnt.data_ptr())
+    try:
+        scene.render_device(j, img.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+    finally:
+        ctx.set_render_stats(None)
+    c = [int(x) for x in cnt.cpu().numpy()]
+    return {"path_rays": c[0], "path_node_tests": c[1], "path_tri_tests": c[2], "path_hits": c[3],
+            "shadow_rays": c[4], "shadow_node_tests": c[5], "shadow_tri_tests": c[6], "shadow_hits": c[7]}
+
+
+def render_roofline(counts, ms, bdpt=False, repeat=1):
+    """Algorithmic bytes of a render (traversal bytes of every ray + 96 B per
+    path-ray hit + 160 B per shading event; for BDPT each visibility ray also
+    evaluates two BSDFs) over its CUDA-event time, against the measured HBM
+    copy bandwidth.  `repeat`: the rays are traced that many times (the
+    adjoint traces its paths twice)."""
+    c = counts
+    rays = c["path_rays"] + c["shadow_rays"]
+    trav = (ALGO_BYTES_RAY * rays + ALGO_BYTES_NODE * (c["path_node_tests"] + c["shadow_node_tests"])
+            + ALGO_BYTES_TRI * (c["path_tri_tests"] + c["shadow_tri_tests"]))
+    events = c["path_hits"] + (2 * c["shadow_rays"] if bdpt else 0)
+    total = repeat * (trav + ALGO_BYTES_HIT_VERTEX * c["path_hits"] + ALGO_BYTES_SHADING_EVENT * events)
+    peak, kind = measured_peak()
+    gbs = total / (ms / 1e3) / 1e9
+    return {"bound": "latency (L1/L2-resident scene data; DRAM and tensor pipes idle)", "achieved": gbs,
+            "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_kind": kind, "traffic": None,
+            "algorithmic_bytes_per_image": total, "rays_per_image": repeat * rays,
+            "rays_per_s": repeat * rays / (ms / 1e3), "counts": c}
 
 
 RENDER_CFG = {"width": 256, "height": 256, "spp": 64, "max_depth": 8, "triangles": 36}
@@ -260,6 +353,7 @@ def render_scene_block(ctx, kind, steps, warmup, cpu=True, cfg=RENDER_CFG, execs
     stream = torch.cuda.current_stream()
     img = torch.empty(W * H * 3, device="cuda")
     out = {}
+    counts = render_counts(ctx, scene, scene.job(sc["camera"], W, H, spp, depth))
     for name, ex in (("wavefront", tpt.EXEC_WAVEFRONT), ("megakernel", tpt.EXEC_MEGAKERNEL)):
         if execs not in ("both", name):
             continue
@@ -276,6 +370,7 @@ def render_scene_block(ctx, kind, steps, warmup, cpu=True, cfg=RENDER_CFG, execs
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / n
         out[name] = {"value": W * H * spp / ms / 1e3, "ms_per_image": ms}
+        out[name]["roofline"] = render_roofline(counts, ms)
     if execs == "both":
         out["wavefront_over_megakernel"] = out["wavefront"]["value"] / out["megakernel"]["value"]
     if cpu and "wavefront" in out:
@@ -380,7 +475,9 @@ def lights_block(ctx, args):
             job = scene.job(sc["camera"], W, H, s_spp, depth, integrator=integ, execution=ex)
             reps = 1 if ex == tpt.EXEC_MEGAKERNEL else 3
             ms = _time_ms(lambda: scene.render_device(job, img.data_ptr(), st), reps)
-            res[name] = W * H * s_spp / ms / 1e3
+            rl = render_roofline(render_counts(ctx, scene, job), ms, bdpt=integ == tpt.INTEGRATOR_BDPT)
+            res[name] = {"value": W * H * s_spp / ms / 1e3, "ms_per_image": ms, "rays_per_s": rl["rays_per_s"],
+                         "roofline_frac": rl["frac"], "achieved_gbs": rl["achieved"]}
         out[key] = res
         scene.close()
     return out
@@ -389,8 +486,11 @@ def lights_block(ctx, args):
 def large_block(ctx, args, cpu=True):
     """The plain large render: ~2.1M triangles (1024 instanced spheres, boxes and
     tori + ground), 256 OpenPBR materials, 10,000 emissive triangles, 1920x1080,
-    depth 16 (MIS) and path length 10 (BDPT).  Msamples/s is timed at
-    --large-spp samples per pixel (the per-sample cost does not depend on spp)."""
+    depth 16 (MIS) and path length 10 (BDPT).  MIS is timed at the configured
+    256 spp (--large-spp); BDPT at --large-bdpt-spp (16: 256 would hold the GPU
+    for tens of seconds per image) and its one-kernel variant at 1 spp, both
+    labelled `reduced_spp` (per-sample cost does not depend on spp).  Each run is
+    warmed up by the same render at 1 spp."""
     import torch
 
     import tpt
@@ -405,16 +505,35 @@ def large_block(ctx, args, cpu=True):
     st = torch.cuda.current_stream().cuda_stream
     img = torch.empty(W * H * 3, device="cuda")
     out = {"config": {"triangles": sc["triangles"], "emissive_triangles": sc["emissive_triangles"],
-                      "materials": 256, "width": W, "height": H, "spp_timed": spp, "spp_configured": 256,
+                      "materials": 256, "width": W, "height": H, "spp_configured": 256,
                       "mis_max_depth": 16, "bdpt_max_path_length": 10},
            "unit": "Msamples/s", "upload_s": setup_s}
-    for name, ex, integ, depth, s_spp in (("mis_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_MIS, 16, spp),
-                                          ("mis_megakernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_MIS, 16, spp),
-                                          ("bdpt_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_BDPT, 10, 1),
-                                          ("bdpt_single_kernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_BDPT, 10, 1)):
+    counted = {}
+    runs = (("mis_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_MIS, 16, spp),
+            ("mis_megakernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_MIS, 16, spp),
+            ("bdpt_wavefront", tpt.EXEC_WAVEFRONT, tpt.INTEGRATOR_BDPT, 10, args.large_bdpt_spp),
+            ("bdpt_single_kernel", tpt.EXEC_MEGAKERNEL, tpt.INTEGRATOR_BDPT, 10, 1))
+    for name, ex, integ, depth, s_spp in runs:
         job = scene.job(sc["camera"], W, H, s_spp, depth, integrator=integ, execution=ex)
-        ms = _time_ms(lambda: scene.render_device(job, img.data_ptr(), st))
-        out[name] = {"value": W * H * s_spp / ms / 1e3, "ms_per_image": ms, "spp": s_spp}
+        warm = scene.job(sc["camera"], W, H, 1, depth, integrator=integ, execution=ex)
+        scene.render_device(warm, img.data_ptr(), st)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        scene.render_device(job, img.data_ptr(), st)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"value": W * H * s_spp / ms / 1e3, "ms_per_image": ms, "spp": s_spp,
+                     "reduced_spp": s_spp != 256}
+        # the rays of a render scale with its samples: count at 1 spp (BDPT) or 16 spp and scale
+        c_spp = min(s_spp, 16 if integ == tpt.INTEGRATOR_MIS else 1)
+        key = (integ, c_spp, depth)
+        if key not in counted:
+            counted[key] = render_counts(ctx, scene, scene.job(sc["camera"], W, H, c_spp, depth, integrator=integ))
+        scaled = {k: v * s_spp // c_spp for k, v in counted[key].items()}
+        out[name]["roofline"] = render_roofline(scaled, ms, bdpt=integ == tpt.INTEGRATOR_BDPT)
+        out[name]["roofline"]["counts_note"] = f"counted on a {c_spp}-spp render, scaled by {s_spp // c_spp}"
     out["wavefront_over_megakernel"] = out["mis_wavefront"]["value"] / out["mis_megakernel"]["value"]
     if cpu:
         import oracle as orc
@@ -494,6 +613,16 @@ def batch_block(ctx, args):
     ms = _time_ms(lambda: [sc.render_device(j, p, st) for sc, j, p in zip(scenes, jm, ptrs)])
     out["per_job_megakernel"] = {"value": total / ms / 1e3, "ms": ms}
     out["batched_over_megakernel"] = out["batched_wavefront"]["value"] / out["per_job_megakernel"]["value"]
+    # algorithmic bytes: every job counted at 1/16 of its spp (at least 1) and scaled
+    total_counts = None
+    for sc, s, p in zip(scenes, scs, specs):
+        c_spp = max(1, p["spp"] // 16)
+        c = render_counts(ctx, sc, sc.job(s["camera"], p["width"], p["height"], c_spp, p["max_depth"]))
+        c = {k: v * p["spp"] // c_spp for k, v in c.items()}
+        total_counts = c if total_counts is None else {k: total_counts[k] + c[k] for k in c}
+    for key in ("batched_wavefront", "per_job_wavefront", "per_job_megakernel"):
+        out[key]["roofline"] = render_roofline(total_counts, out[key]["ms"])
+    out["batched_wavefront"]["roofline"]["counts_note"] = "each job counted at max(1, spp/16) spp and scaled"
     for sc in scenes:
         sc.close()
     return out
@@ -527,6 +656,10 @@ def adjoint_block(ctx, args, cpu=True):
                       "max_depth": depth, "fd_step": 1e-3},
            "unit": "grads/s", "forward_ms": fwd, "adjoint_ms": bwd, "adjoint_over_forward": bwd / fwd,
            "value": n_params / (bwd / 1e3), "samples_per_s_adjoint": W * W * spp / (bwd / 1e3)}
+    counts = render_counts(ctx, scene, job)
+    out["forward_roofline"] = render_roofline(counts, fwd)
+    # the adjoint runs the forward wavefront again, then replays the same paths
+    out["roofline"] = render_roofline(counts, bwd, repeat=2)
     # inverse rendering: Adam on the 320 parameters from a perturbed start; the
     # success measure is the image loss at 256 spp (the 16-spp training loss is
     # dominated by its own noise)
@@ -711,12 +844,20 @@ def run_ours(args):
                 "d2h_bytes_per_step": len(queries) * n * 8},
         "gpu_launches": len(queries) * args.steps,
         "roofline": {
-            "bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
+            # the counters name L1/texture throughput and load latency as the limit: DRAM carries ~2 % of
+            # the algorithmic bytes (the BVH and triangles stay L2-resident); frac is still stated against
+            # the measured HBM copy bandwidth, the only measured memory peak
+            "bound": "l1tex", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s", "frac": achieved_gbs / peak,
             "traffic": profiled_traffic(), "peak_kind": peak_kind,
             "kernel": "traverse_kernel<closest,incoherent>", "launch_ms": dom_ms,
             "algorithmic_bytes_per_launch": algo_bytes, "node_tests": nodes, "tri_tests": tris,
+            "l2_bytes_per_launch": profiled("lts_bytes_per_full_launch"),
+            "l1_bytes_per_launch": profiled("l1tex_bytes_per_full_launch"),
+            "l1tex_throughput_pct": profiled("l1tex_throughput_pct"),
+            "l2_achieved_gbs": (profiled("lts_bytes_per_full_launch") or 0) / (dom_ms / 1e3) / 1e9 or None,
+            "l1_achieved_gbs": (profiled("l1tex_bytes_per_full_launch") or 0) / (dom_ms / 1e3) / 1e9 or None,
             "note": "algorithmic bytes count every 4-wide node and triangle fetch; the BVH is L2-resident, "
-                    "so this rate is mostly L2 bandwidth",
+                    "so they are served by L1/L2, whose bytes per launch come from the committed ncu summary",
         },
         "clocks": clk,
     }
@@ -724,7 +865,8 @@ def run_ours(args):
         line["qbvh_build"] = qbvh_build_block(ctx, mesh)
     if rank == 0 and not args.no_cpu_baseline:
         rate, threads, desc = cpu_reference_rate(mesh, batches)
-        line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc}
+        line["cpu_baseline"] = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port", "sample": desc,
+                                "cpu_model": cpu_model()}
     if rank == 0 and not args.no_render:
         line["render"] = render_block(ctx, args.steps, args.warmup, cpu=not args.no_cpu_baseline, args=args)
     if rank == 0 and not args.no_render:

@@ -412,6 +412,16 @@ uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx);
  * always launched directly (they join the caller's graph).  Results do not
  * depend on it. */
 tpt_status tpt_context_set_graphs(tpt_context* ctx, int enable);
+/* Measurement aid (no counterpart in the reference): while `d_counters` (device,
+ * 8 uint64, zeroed by the caller) is set, single-job wavefront renders
+ * (MIS, NEE, PT, BDPT and the adjoint replay) launch their stages directly
+ * instead of replaying graphs, and their traversals add, per launch,
+ * d_counters[0..3] = rays, 4-wide node tests, triangle tests and hits of the
+ * path (camera, bounce, subpath) rays, and d_counters[4..7] the same for the
+ * shadow and visibility rays.  These give the algorithmic bytes of a render.
+ * Megakernel and batched renders are not counted.  NULL turns it off.  Results
+ * do not depend on it. */
+tpt_status tpt_context_set_render_stats(tpt_context* ctx, uint64_t* d_counters);
 /* Threads per block of the wavefront shade stage: 128 or 256 (default). */
 tpt_status tpt_context_set_shade_block(tpt_context* ctx, uint32_t threads);
 

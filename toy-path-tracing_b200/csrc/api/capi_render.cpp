@@ -151,21 +151,24 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
   const DevGeometry& geo = job->scene->geo;
   const DevRenderData& rd = job->scene->render;
   cudaError_t e = launch_wf_generate(geo, rd, L, B, first, n, s, A ? samples : nullptr);
-  for (uint32_t b = 0; !A && e == cudaSuccess && b <= L.max_depth; ++b)
+  // direct launches for the adjoint replay and while render statistics are on
+  const bool direct = A || ctx->render_stats;
+  unsigned long long* tot = ctx->render_stats;
+  for (uint32_t b = 0; !direct && e == cudaSuccess && b <= L.max_depth; ++b)
     e = enqueue_bounce(ctx, s, geo, rd, L, B, nullptr, (int)(b & 1u), b == L.max_depth);
-  for (uint32_t b = 0; A && e == cudaSuccess && b <= L.max_depth; ++b) {
+  for (uint32_t b = 0; direct && e == cudaSuccess && b <= L.max_depth; ++b) {
     const int cur = (int)(b & 1u);
     e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
     if (e == cudaSuccess)
       e = launch_traverse_strided(geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
                                   B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
-                                  nullptr, nullptr, B.counts + cur);
+                                  nullptr, nullptr, B.counts + cur, nullptr, nullptr, tot);
     if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, cur, s, A);
     if (e == cudaSuccess && b < L.max_depth)
       e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
                                   nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
-                                  nullptr, B.counts + 2);
+                                  nullptr, B.counts + 2, nullptr, nullptr, tot ? tot + 4 : nullptr);
     if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s, A);
   }
   if (e == cudaSuccess && !A) e = launch_wf_finalize(B, n, samples, s);
@@ -240,7 +243,7 @@ tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, co
   for (uint64_t b = 0; b < n; b += B.sample_capacity) {
     const uint32_t m = (uint32_t)std::min<uint64_t>(B.sample_capacity, n - b);
     cudaError_t e = launch_bdpt_wavefront(job->scene->geo, job->scene->render, L, B, first + b, m, samples + 3 * b,
-                                          next_counter(ctx), ctx->d_err, ctx->num_sms, s);
+                                          next_counter(ctx), ctx->d_err, ctx->num_sms, s, ctx->render_stats);
     if ((st = cuda_check(ctx, e, "BDPT wavefront launch"))) return st;
   }
   return TPT_OK;
@@ -276,6 +279,12 @@ tpt_status tpt_context_set_shade_block(tpt_context* ctx, uint32_t threads) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
   if (threads != 128 && threads != 256) return set_error(ctx, TPT_ERR_INVALID_ARG, "shade block must be 128 or 256");
   ctx->shade_block = threads;
+  return TPT_OK;
+}
+
+tpt_status tpt_context_set_render_stats(tpt_context* ctx, uint64_t* d_counters) {
+  if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
+  ctx->render_stats = reinterpret_cast<unsigned long long*>(d_counters);
   return TPT_OK;
 }
 

@@ -61,6 +61,9 @@ struct tpt_context {
   bool use_graphs = true;
   uint32_t tuned_execution = 0;  // what TPT_EXEC_AUTO means (tpt_autotune)
   uint32_t shade_block = 256;    // threads per block of the wavefront shade stage (128 or 256)
+  // tpt_context_set_render_stats: device counters the wavefront traversals add
+  // to (queue rays at [0..3], shadow/visibility rays at [4..7]); NULL = off
+  unsigned long long* render_stats = nullptr;
   bool gpu_build = false;        // scene upload builds missing QBVHs on the GPU (tpt_context_set_gpu_build)
   // stream-ordered pool of the GPU QBVH build: keeps up to 1 GiB mapped between
   // builds (the default pool unmaps every freed block at the next synchronisation)
@@ -125,7 +128,8 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t stream,
                                     uint32_t* node_tests, uint32_t* tri_tests, const uint32_t* n_dev = nullptr,
-                                    const DevJob* jobs = nullptr, const uint32_t* ray_job = nullptr);
+                                    const DevJob* jobs = nullptr, const uint32_t* ray_job = nullptr,
+                                    unsigned long long* totals = nullptr);
 
 // qbvh_build_gpu.cu: the QBVH of n primitive boxes (device, n x 6 floats) built
 // on the device, equal to build_qbvh_host's (a box face at zero may be +0.0
@@ -155,7 +159,8 @@ cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first
 // wavefront stages (n <= B.sample_capacity); per-sample radiance into samples.
 cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                                   const BdWfBuffers& B, uint64_t first_path, uint32_t n, float* samples,
-                                  unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s);
+                                  unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
+                                  unsigned long long* totals = nullptr);
 // capi_render.cpp: BDPT paths [first, first + n) through the wavefront, in chunks.
 tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
                                  uint64_t n, float* samples, cudaStream_t s);

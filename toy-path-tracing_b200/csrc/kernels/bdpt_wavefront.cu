@@ -295,7 +295,8 @@ static inline unsigned grid_of(uint64_t n) { return (unsigned)((n + kBdWfBlock -
 
 cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                                   const BdWfBuffers& B, uint64_t first_path, uint32_t n, float* samples,
-                                  unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s) {
+                                  unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
+                                  unsigned long long* totals) {
   if (n == 0) return cudaSuccess;
   DevRender S{geo, rd};
   cudaError_t e = cudaMemsetAsync(B.counts, 0, 2 * sizeof(uint32_t), s);
@@ -309,14 +310,15 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
     const int cur = (int)(step & 1u);
     if ((e = cudaMemsetAsync(B.counts + 2 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
     e = launch_traverse_strided(geo, B.q_ray[cur], Q, Q, TPT_CLOSEST_HIT, B.h_tri, B.h_t, B.h_inst, B.h_bary, Q,
-                                counter, err, num_sms, s, nullptr, nullptr, B.counts + 2 + cur);
+                                counter, err, num_sms, s, nullptr, nullptr, B.counts + 2 + cur, nullptr, nullptr,
+                                totals);
     if (e != cudaSuccess) return e;
     bd_step<<<grid_of(Q), kBdWfBlock, 0, s>>>(S, P, B, first_path, step, cur);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (lights) {  // at most one light sample per sample and step: n <= sample_capacity <= pair_capacity
       e = launch_traverse_strided(geo, B.s_ray, B.pair_capacity, B.pair_capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t,
                                   B.s_inst, nullptr, B.pair_capacity, counter, err, num_sms, s, nullptr, nullptr,
-                                  B.counts + 1);
+                                  B.counts + 1, nullptr, nullptr, totals ? totals + 4 : nullptr);
       if (e != cudaSuccess) return e;
       bd_nee_resolve<<<grid_of(B.sample_capacity), kBdWfBlock, 0, s>>>(B);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -329,7 +331,7 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   e = launch_traverse_strided(geo, B.s_ray, B.pair_capacity, B.pair_capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t,
                               B.s_inst, nullptr, B.pair_capacity, counter, err, num_sms, s, nullptr, nullptr,
-                              B.counts + 1);
+                              B.counts + 1, nullptr, nullptr, totals ? totals + 4 : nullptr);
   if (e != cudaSuccess) return e;
   bd_resolve<<<grid_of(B.pair_capacity), kBdWfBlock, 0, s>>>(S, B);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -9,6 +9,10 @@
 // time without changing any ray's own visit order.
 // Traversal stacks: 32 entries per thread in shared memory, spilling to local
 // memory beyond that (total depth 128, as the reference).
+// Counting (STATS): per-ray node and triangle test counts into node_tests /
+// tri_tests when given, and, when `totals` is given, the launch's sums added
+// to totals[0..3] = rays, 4-wide node tests, triangle tests, hits (one atomic
+// per warp at the end) -- the algorithmic-bytes account of renders.
 // The batched instantiation (BATCH) serves rays of many scenes in one launch:
 // ray i belongs to job ray_job[i], and a lane loads that job's geometry record
 // when it takes the ray.
@@ -32,7 +36,8 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
                     int32_t* __restrict__ prim, float* __restrict__ tout, int32_t* __restrict__ inst,
                     float* __restrict__ bary, uint32_t* __restrict__ node_tests, uint32_t* __restrict__ tri_tests,
                     unsigned long long* __restrict__ counter, const uint32_t* __restrict__ n_dev, uint32_t* err,
-                    const DevJob* __restrict__ jobs, const uint32_t* __restrict__ ray_job) {
+                    const DevJob* __restrict__ jobs, const uint32_t* __restrict__ ray_job,
+                    unsigned long long* __restrict__ totals) {
   if (n_dev) n = *n_dev;  // queue length produced on the device (wavefront stages)
   DevGeometry lane_geo;  // BATCH: the scene of this lane's ray
   const DevGeometry& G = BATCH ? lane_geo : geo;
@@ -45,6 +50,8 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
   TraceCounters c;
   int64_t ray = -1;  // -1: needs a ray, -2: no rays left, >= 0: active ray index
   int stalled = 0;   // consecutive iterations in which no lane of the warp advanced
+  uint32_t sum_rays = 0, sum_hits = 0;  // STATS with totals: this lane's finished rays
+  unsigned long long sum_nodes = 0, sum_tris = 0;
   for (;;) {
     bool moved = false;
     // refill finished lanes: one warp-aggregated atomic, converged ray setup
@@ -102,8 +109,14 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
         __stcs(bary + 2 * bs + i, s.res.b2);
       }
       if (STATS) {
-        node_tests[i] = c.nodes;
-        tri_tests[i] = c.tris;
+        if (node_tests) {
+          node_tests[i] = c.nodes;
+          tri_tests[i] = c.tris;
+        }
+        sum_rays += 1;
+        sum_hits += s.res.tri >= 0 ? 1 : 0;
+        sum_nodes += c.nodes;
+        sum_tris += c.tris;
       }
       ray = -1;
     }
@@ -116,13 +129,29 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
       break;
     }
   }
+  if (STATS && totals) {  // the loop ends converged (every exit is warp-uniform)
+    unsigned long long r = sum_rays, h = sum_hits, nn = sum_nodes, tt = sum_tris;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      r += __shfl_down_sync(0xffffffffu, r, o);
+      h += __shfl_down_sync(0xffffffffu, h, o);
+      nn += __shfl_down_sync(0xffffffffu, nn, o);
+      tt += __shfl_down_sync(0xffffffffu, tt, o);
+    }
+    if (lane == 0 && r) {
+      atomicAdd(totals, r);
+      atomicAdd(totals + 1, nn);
+      atomicAdd(totals + 2, tt);
+      atomicAdd(totals + 3, h);
+    }
+  }
 }
 
 template <int MODE, bool STATS, bool BARY, bool BATCH>
 static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, uint64_t bs,
                             int32_t* prim, float* t, int32_t* inst, float* bary, uint32_t* nt, uint32_t* tt,
                             unsigned long long* counter, const uint32_t* n_dev, uint32_t* err, int num_sms,
-                            cudaStream_t s, const DevJob* jobs, const uint32_t* ray_job) {
+                            cudaStream_t s, const DevJob* jobs, const uint32_t* ray_job, unsigned long long* totals) {
   if (n == 0) return cudaSuccess;
   static int blocks_per_sm = 0;
   if (blocks_per_sm == 0) {
@@ -136,7 +165,7 @@ static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t 
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   traverse_kernel<MODE, STATS, BARY, BATCH><<<(unsigned)blocks, kBlock, 0, s>>>(
-      geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, jobs, ray_job);
+      geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, jobs, ray_job, totals);
   return cudaGetLastError();
 }
 
@@ -144,17 +173,19 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
                                     uint32_t* nt, uint32_t* tt, const uint32_t* n_dev, const DevJob* jobs,
-                                    const uint32_t* ray_job) {
-  const bool stats = nt != nullptr;
+                                    const uint32_t* ray_job, unsigned long long* totals) {
+  const bool stats = nt != nullptr || totals != nullptr;
   const bool b = bary != nullptr;
 #define TPT_L(M, S, B, J) \
-  launch_t<M, S, B, J>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, num_sms, s, jobs, ray_job)
+  launch_t<M, S, B, J>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, num_sms, s, jobs, \
+                       ray_job, totals)
   if (jobs) {  // batched wavefront: closest hit, with or without barycentrics
     if (mode != 0 || stats) return cudaErrorInvalidValue;
     if (b) return TPT_L(0, false, true, true);
     return TPT_L(0, false, false, true);
   }
   if (mode == 0) {
+    if (stats && b) return TPT_L(0, true, true, false);
     if (stats) return TPT_L(0, true, false, false);
     if (b) return TPT_L(0, false, true, false);
     return TPT_L(0, false, false, false);

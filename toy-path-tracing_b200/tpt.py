@@ -291,6 +291,7 @@ EXPORTED_SYMBOLS = [
     "tpt_context_set_wavefront_capacity",
     "tpt_context_wavefront_capacity",
     "tpt_context_set_graphs",
+    "tpt_context_set_render_stats",
     "tpt_context_set_shade_block",
     "tpt_autotune",
     "tpt_adjoint_device",
@@ -339,6 +340,7 @@ def _declare(L):
         "tpt_context_set_wavefront_capacity": (i32, [vp, C.c_uint32]),
         "tpt_context_wavefront_capacity": (C.c_uint32, [vp]),
         "tpt_context_set_graphs": (i32, [vp, i32]),
+        "tpt_context_set_render_stats": (i32, [vp, vp]),
         "tpt_context_set_shade_block": (i32, [vp, C.c_uint32]),
         "tpt_autotune": (i32, [vp, vp, i32, C.POINTER(TuneResult)]),
         "tpt_adjoint_device": (i32, [vp, C.POINTER(RenderJob), C.POINTER(AdjointDesc), vp, vp, vp]),
@@ -402,6 +404,13 @@ class Context:
     def set_graphs(self, enable: bool):
         """`tpt_context_set_graphs`: replay wavefront bounces from CUDA graphs."""
         _check(lib().tpt_context_set_graphs(self.h, int(bool(enable))), self)
+
+    def set_render_stats(self, counters_ptr):
+        """`tpt_context_set_render_stats`: device pointer of 8 uint64 counters
+        (rays, node tests, triangle tests, hits of path rays, then of shadow
+        rays) that wavefront renders add to; None turns counting off."""
+        _check(lib().tpt_context_set_render_stats(self.h, None if counters_ptr is None
+                                                  else C.c_void_p(counters_ptr)), self)
 
     def autotune(self, jobs) -> dict:
         """`tpt_autotune`: times candidate settings on a pilot of `jobs` and applies the fastest."""
