@@ -506,7 +506,8 @@ OPENPBR_PARAM_FIELDS = [
     ("specular_alpha_y", 1), ("specular_eta", 1), ("transmission_eta", 1), ("metalness", 1), ("coat", 1),
     ("coat_color", 3), ("coat_darkening", 3), ("coat_alpha_x", 1), ("coat_alpha_y", 1), ("coat_eta", 1),
     ("fuzz", 1), ("fuzz_color", 3), ("fuzz_roughness", 1), ("transmission", 1), ("transmission_color", 3),
-    ("diffuse_roughness", 1), ("subsurface", 1), ("subsurface_color", 3), ("front_face", 1),
+    ("transmission_alpha_x", 1), ("transmission_alpha_y", 1),
+    ("diffuse_roughness", 1), ("subsurface", 1), ("subsurface_color", 3), ("thin_walled", 1), ("front_face", 1),
 ]
 
 
@@ -519,6 +520,12 @@ def pack_openpbr(m: dict) -> np.ndarray:
 
 
 def pack_openpbr_params(p: dict) -> np.ndarray:
+    """Flat OpenPbrBsdfParams; the transmission alphas default to the specular
+    ones (as make_bsdf sets them) and thin_walled to False."""
+    p = dict(p)
+    p.setdefault("transmission_alpha_x", p["specular_alpha_x"])
+    p.setdefault("transmission_alpha_y", p["specular_alpha_y"])
+    p.setdefault("thin_walled", 0.0)
     out = []
     for name, k in OPENPBR_PARAM_FIELDS:
         v = p[name]

@@ -40,9 +40,12 @@ OpenPbrParams params_from_flat(const float* f) {
   p.fuzz_roughness = f[i++];
   p.transmission = f[i++];
   p.transmission_color = v3();
+  p.transmission_alpha_x = f[i++];
+  p.transmission_alpha_y = f[i++];
   p.diffuse_roughness = f[i++];
   p.subsurface = f[i++];
   p.subsurface_color = v3();
+  p.thin_walled = f[i++] != 0.0f;
   p.front_face = f[i++] != 0.0f;
   return p;
 }

@@ -93,7 +93,13 @@ bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& 
     BsdfSample bs;
     if (!make_bsdf(m, v, wo_l).sample(wo_l, r.u_lobe, r.u_dir, mode, &bs)) return false;
     Vec3 wi = v.frame.to_world(bs.wi);
-    if (dot(wi, v.ng) <= kGeomCosEps) return false;  // reflection lobes only
+    // material/open_pbr.rs:523-531: transmission must leave below the geometric
+    // surface (delta transmission is kept either way), reflection above it
+    if (bs.flags & kTransmission) {
+      if (dot(wi, v.ng) >= -kGeomCosEps && !(bs.flags & kDelta)) return false;
+    } else if (dot(wi, v.ng) <= kGeomCosEps) {
+      return false;
+    }
     s->delta = (bs.flags & kDelta) != 0;
     s->weight = modified_weight(v, wi, bs.weight, s->delta, mode);
     s->wi = wi;

@@ -293,6 +293,21 @@ struct Impl {
   float coat_proxy() const { return clampf(std::sqrt(fmax_num(p.coat_alpha_x, p.coat_alpha_y)), 0.0f, 1.0f); }
   float spec_proxy() const { return clampf(std::sqrt(fmax_num(p.specular_alpha_x, p.specular_alpha_y)), 0.0f, 1.0f); }
   float conductor_req() const { return std::pow(p.specular_alpha_x * p.specular_alpha_y, 0.25f); }
+  bool btdf_smooth() const {
+    return p.transmission <= 0.0f || fmax_num(p.transmission_alpha_x, p.transmission_alpha_y) < kSmoothAlpha;
+  }
+  // TransportMode::transmission_scale (bsdf/mod.rs:102-107)
+  static float trans_scale(TransportMode mode, float eta_rel) {
+    return mode == kRadiance ? 1.0f / (eta_rel * eta_rel) : 1.0f;
+  }
+  // thin_wall_transmission_alpha_xy (open_pbr.rs:553-564)
+  void thin_wall_alpha(float* ax, float* ay) const {
+    float eta = fmax_num(p.transmission_eta, 1.0f);
+    float scale = std::sqrt(fmax_num(3.7f * (eta - 1.0f) * powi(eta - 0.5f, 2) / powi(eta, 3), 0.0f));
+    float s2 = scale * scale;
+    *ax = clampf(p.transmission_alpha_x * s2, kMinAlpha, 1.0f);
+    *ay = clampf(p.transmission_alpha_y * s2, kMinAlpha, 1.0f);
+  }
 
   MsParams ms_params(float ax, float ay, float eta) const {
     MsParams m;
@@ -321,6 +336,11 @@ struct Impl {
     float ms = fmax_num(1.0f - m.e_avg_o, 0.0f) * ms_factor(m);
     return {ss, ms, fmax_num(ss + ms, 1.0e-8f)};
   }
+  TwoLobe transmission_lobe_weights(const MsParams& m) const {  // open_pbr.rs:638-646
+    float ss = clampf(m.e_avg_o, 0.0f, 1.0f);
+    float ms = fmax_num(1.0f - m.e_avg_o, 0.0f) * clampf(1.0f - m.ratio_r, 0.0f, 1.0f);
+    return {ss, ms, fmax_num(ss + ms, 1.0e-8f)};
+  }
   TwoLobe conductor_lobe_weights() const {
     float e_avg = clampf(L.conductor->lookup_e_avg(conductor_req()), 0.0f, 1.0f);
     float ms = fmax_num(1.0f - e_avg, 0.0f);
@@ -340,6 +360,7 @@ struct Impl {
   float spec_albedo(Vec3 wo) const {
     if (wo.z <= 0.0f) return 0.0f;
     float ss = L.spec->lookup(wo, spec_proxy(), 0.0f);
+    if (p.thin_walled) return ss;
     return albedo_with_ms(wo, p.specular_alpha_x, p.specular_alpha_y, p.specular_eta, ss);
   }
   float fuzz_albedo(Vec3 wo) const {
@@ -376,9 +397,10 @@ struct Impl {
     Vec3 leakage = vmax(one - spec_amp * e_spec, Vec3(0, 0, 0));
     Vec3 below_spec = below_metal * leakage;
     float trans = p.transmission;
-    Vec3 spec_btdf_w = below_spec * trans * p.transmission_color;
+    Vec3 tint = p.thin_walled ? Vec3(1, 1, 1) : p.transmission_color;
+    Vec3 spec_btdf_w = below_spec * trans * tint;
     Vec3 below_trans = below_spec * (1.0f - trans);
-    float thin_factor = 0.0f;
+    float thin_factor = p.thin_walled ? 1.0f : 0.0f;
     Vec3 diff_brdf_w = below_trans * ((1.0f - p.subsurface) * p.base) * p.base_color;
     Vec3 diff_btdf_w = below_trans * (p.subsurface * thin_factor) * p.subsurface_color;
     return {coat_amp * below_fuzz_s, metal, spec_brdf_w, spec_btdf_w, fuzz_w, diff_brdf_w, diff_btdf_w};
@@ -491,6 +513,11 @@ struct Impl {
     float d = ggx_d(wm, p.specular_alpha_x, p.specular_alpha_y);
     float g = ggx_g2(wo, wi, p.specular_alpha_x, p.specular_alpha_y);
     if (d <= 0.0f || g <= 0.0f) return Vec3(0, 0, 0);
+    if (p.thin_walled) {
+      Vec3 R, T;
+      thin_wall_coeffs(std::fabs(wo.z), &R, &T);
+      return R * (d * g / (4.0f * wo.z * wi.z));
+    }
     Vec3 f = spec_fresnel(std::fabs(dot(wo, wm)));
     Vec3 ss = f * (d * g / (4.0f * wo.z * wi.z));
     Vec3 ms = Vec3::splat(eval_refl_ms(wo, wi, p.specular_alpha_x, p.specular_alpha_y, p.specular_eta));
@@ -512,9 +539,140 @@ struct Impl {
   }
   float pdf_spec_brdf(Vec3 wo, Vec3 wi) const {
     if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
+    if (p.thin_walled) return pdf_spec_ss(wo, wi);
     MsParams m = ms_params(p.specular_alpha_x, p.specular_alpha_y, p.specular_eta);
     TwoLobe w = reflection_lobe_weights(m);
     return (w.ss * pdf_spec_ss(wo, wi) + w.ms * cosine_pdf(wi.z)) / w.total;
+  }
+
+  // thin_wall_coefficients (open_pbr.rs:931-959) without thin film: the slab's
+  // reflectance and transmittance with the absorption of its interior
+  void thin_wall_coeffs(float cos_theta_o, Vec3* R, Vec3* T) const {
+    const Vec3 one(1, 1, 1);
+    float eta = fmax_num(p.transmission_eta, 1.0e-4f);
+    float eta_prime = fmax_num(p.specular_eta, 1.0e-4f);
+    float cos_o = clampf(cos_theta_o, 0.0f, 1.0f);
+    float sin2_o = fmax_num(1.0f - cos_o * cos_o, 0.0f);
+    float sin2_i = clampf(sin2_o / (eta * eta), 0.0f, 1.0f);
+    float cos_i = fmax_num(std::sqrt(1.0f - sin2_i), 1.0e-4f);
+    Vec3 f_o = vclamp01(spec_fresnel(cos_o));
+    // thin_wall_internal_fresnel (open_pbr.rs:961-979)
+    Vec3 f_i = vclamp01(Vec3::splat(
+        weighted_fresnel_ratio(cos_i, 1.0f / fmax_num(eta, 1.0e-4f), 1.0f / fmax_num(eta_prime, 1.0e-4f))));
+    Vec3 a = vpowf(vclamp01(p.transmission_color), 1.0f / cos_i);
+    Vec3 a2 = a * a;
+    Vec3 f_i2_a2 = a2 * f_i * f_i;
+    Vec3 denom = vmax(one - f_i2_a2, Vec3::splat(1.0e-6f));
+    Vec3 omfo = vmax(one - f_o, Vec3(0, 0, 0));
+    Vec3 omfi = vmax(one - f_i, Vec3(0, 0, 0));
+    Vec3 refl = f_o + omfo * omfi * f_i * a2 / denom;
+    Vec3 trans = omfo * omfi * a * (one + f_i2_a2 / denom);
+    *R = vclamp01(refl);
+    *T = vclamp01(trans);
+  }
+  // eval_dielectric_transmission_ms (open_pbr.rs:672-696)
+  float eval_trans_ms(Vec3 wo, Vec3 wi, float ax, float ay, float eta, TransportMode mode) const {
+    if (wo.z <= 0.0f || wi.z >= 0.0f) return 0.0f;
+    MsParams m = ms_params(ax, ay, eta);
+    float cos_o = wo.z, cos_i = std::fabs(wi.z);
+    float e_o = L.dielectric->lookup_e(cos_o, m.roughness_eq, m.eta_o);
+    float e_i = L.dielectric->lookup_e(cos_i, m.roughness_eq, m.eta_rel);
+    float scale = trans_scale(mode, m.eta_rel);
+    return (1.0f - m.ratio_r) * (1.0f - e_o) * (1.0f - e_i) * scale / (kPi * m.one_minus_e_avg_t);
+  }
+  float eta_rel_t() const { return p.front_face ? 1.0f / p.transmission_eta : p.transmission_eta; }
+  // eval_spec_btdf_scalar_with_eta (open_pbr.rs:1074-1117): false for None
+  bool btdf_scalar(Vec3 wo, Vec3 wi, float eta_rel, TransportMode mode, float* scalar, float* cos_wo_wm) const {
+    Vec3 wmu = eta_rel * wo + wi;
+    if (length_squared(wmu) < 1.0e-12f) return false;
+    Vec3 wm = normalize(wmu);
+    if (wm.z < 0.0f) wm = -wm;
+    float co = dot(wo, wm);
+    if (co <= 0.0f) return false;
+    float ci = dot(wi, wm);
+    float den = ci + eta_rel * co;
+    if (std::fabs(den) < 1.0e-6f) return false;
+    float d = ggx_d(wm, p.transmission_alpha_x, p.transmission_alpha_y);
+    float g = ggx_g2(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y);
+    if (d <= 0.0f || g <= 0.0f) return false;
+    float scale = trans_scale(mode, eta_rel);
+    float s = d * g * std::fabs(ci * co);
+    float denom = den * den * std::fabs(wo.z) * std::fabs(wi.z);
+    if (denom <= 0.0f) return false;
+    *scalar = s * scale / denom;
+    *cos_wo_wm = co;
+    return true;
+  }
+  // eval_thin_wall_spec_btdf (open_pbr.rs:1053-1072)
+  Vec3 eval_thin_btdf(Vec3 wo, Vec3 wi) const {
+    if (wo.z <= 0.0f || wi.z >= 0.0f) return Vec3(0, 0, 0);
+    Vec3 R, T;
+    thin_wall_coeffs(std::fabs(wo.z), &R, &T);
+    if (btdf_smooth()) return Vec3(0, 0, 0);
+    Vec3 wim(wi.x, wi.y, -wi.z);
+    Vec3 wm;
+    if (!reflection_half_vector(wo, wim, &wm)) return Vec3(0, 0, 0);
+    float ax, ay;
+    thin_wall_alpha(&ax, &ay);
+    float d = ggx_d(wm, ax, ay);
+    float g = ggx_g2(wo, wim, ax, ay);
+    if (d <= 0.0f || g <= 0.0f) return Vec3(0, 0, 0);
+    return T * (d * g / (4.0f * wo.z * std::fabs(wi.z)));
+  }
+  // eval_spec_btdf (open_pbr.rs:1024-1051), no dispersion
+  Vec3 eval_spec_btdf(Vec3 wo, Vec3 wi, TransportMode mode) const {
+    if (p.thin_walled) return eval_thin_btdf(wo, wi);
+    if (wo.z <= 0.0f || wi.z >= 0.0f) return Vec3(0, 0, 0);
+    float scalar, co;
+    if (!btdf_scalar(wo, wi, eta_rel_t(), mode, &scalar, &co)) return Vec3(0, 0, 0);
+    Vec3 f = Vec3::splat(base_dielectric_fresnel(co, p.transmission_eta, p.specular_eta));
+    Vec3 ss = vmax(Vec3(1, 1, 1) - f, Vec3(0, 0, 0)) * scalar;
+    Vec3 ms = Vec3::splat(eval_trans_ms(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y, p.specular_eta, mode));
+    return ss + ms;
+  }
+  // pdf_specular_btdf_ss_with_eta (open_pbr.rs:1193-1222)
+  float pdf_btdf_ss(Vec3 wo, Vec3 wi, float eta_rel) const {
+    Vec3 wmu = eta_rel * wo + wi;
+    if (length_squared(wmu) < 1.0e-12f) return 0.0f;
+    Vec3 wm = normalize(wmu);
+    if (wm.z < 0.0f) wm = -wm;
+    float co = dot(wo, wm);
+    if (co <= 0.0f) return 0.0f;
+    float ci = dot(wi, wm);
+    float den = ci + eta_rel * co;
+    if (std::fabs(den) < 1.0e-6f) return 0.0f;
+    float pdf_wm = pdf_wm_vndf(wo, wm, p.transmission_alpha_x, p.transmission_alpha_y);
+    if (pdf_wm <= 0.0f) return 0.0f;
+    return pdf_wm * std::fabs(ci) / (den * den);
+  }
+  // pdf_specular_btdf and _with_eta (open_pbr.rs:1154-1191), no dispersion
+  float pdf_spec_btdf(Vec3 wo, Vec3 wi) const {
+    if (p.thin_walled) {
+      if (btdf_smooth() || wo.z <= 0.0f || wi.z >= 0.0f) return 0.0f;
+      Vec3 wim(wi.x, wi.y, -wi.z);
+      Vec3 wm;
+      if (!reflection_half_vector(wo, wim, &wm)) return 0.0f;
+      float ax, ay;
+      thin_wall_alpha(&ax, &ay);
+      float pdf_wm = pdf_wm_bounded_vndf(wo, wm, ax, ay);
+      float denom = 4.0f * std::fabs(dot(wo, wm));
+      return denom > 0.0f ? pdf_wm / denom : 0.0f;
+    }
+    if (wo.z <= 0.0f || wi.z >= 0.0f) return 0.0f;
+    MsParams m = ms_params(p.transmission_alpha_x, p.transmission_alpha_y, p.transmission_eta);
+    TwoLobe w = transmission_lobe_weights(m);
+    float pdf_ss = pdf_btdf_ss(wo, wi, eta_rel_t());
+    float pdf_ms = cosine_pdf(-wi.z);
+    return (w.ss * pdf_ss + w.ms * pdf_ms) / w.total;
+  }
+  // eval_diff_btdf / pdf_diff_btdf (open_pbr.rs:1445-1465): thin-walled only
+  Vec3 eval_diff_btdf(Vec3 wo, Vec3 wi) const {
+    if (!p.thin_walled || wo.z <= 0.0f || wi.z >= 0.0f) return Vec3(0, 0, 0);
+    return Eon(p.diffuse_roughness).eval(wo, Vec3(wi.x, wi.y, -wi.z));
+  }
+  float pdf_diff_btdf(Vec3 wo, Vec3 wi) const {
+    if (!p.thin_walled || wo.z <= 0.0f || wi.z >= 0.0f) return 0.0f;
+    return Eon(p.diffuse_roughness).pdf(wo, Vec3(wi.x, wi.y, -wi.z));
   }
 
   // open_pbr.rs:224-296
@@ -526,8 +684,10 @@ struct Impl {
     if (w.coat_amp > 0.0f && !coat_smooth()) total += w.coat_amp * eval_coat(wo, wi);
     if (length_squared(w.metal) > 0.0f && !metal_smooth()) total += w.metal * eval_metal(wo, wi);
     if (length_squared(w.spec_brdf) > 0.0f && !spec_smooth()) total += w.spec_brdf * eval_spec_brdf(wo, wi);
+    if (length_squared(w.spec_btdf) > 0.0f && !btdf_smooth()) total += w.spec_btdf * eval_spec_btdf(wo, wi, mode);
     if (length_squared(w.fuzz) > 0.0f) total += w.fuzz * Fuzz(p.fuzz_roughness).eval(wo, wi);
     if (length_squared(w.diff_brdf) > 0.0f) total += w.diff_brdf * Eon(p.diffuse_roughness).eval(wo, wi);
+    if (length_squared(w.diff_btdf) > 0.0f) total += w.diff_btdf * eval_diff_btdf(wo, wi);
     return total;
   }
   float pdf(Vec3 wo, Vec3 wi) const {
@@ -538,13 +698,15 @@ struct Impl {
     if (q.coat > 0.0f && !coat_smooth()) pdf += (q.coat / q.total) * pdf_coat(wo, wi);
     if (q.metal > 0.0f && !metal_smooth()) pdf += (q.metal / q.total) * pdf_metal(wo, wi);
     if (q.spec_brdf > 0.0f && !spec_smooth()) pdf += (q.spec_brdf / q.total) * pdf_spec_brdf(wo, wi);
+    if (q.spec_btdf > 0.0f && !btdf_smooth()) pdf += (q.spec_btdf / q.total) * pdf_spec_btdf(wo, wi);
     if (q.fuzz > 0.0f) pdf += (q.fuzz / q.total) * Fuzz(p.fuzz_roughness).pdf(wo, wi);
     if (q.diff_brdf > 0.0f) pdf += (q.diff_brdf / q.total) * Eon(p.diffuse_roughness).pdf(wo, wi);
+    if (q.diff_btdf > 0.0f) pdf += (q.diff_btdf / q.total) * pdf_diff_btdf(wo, wi);
     return pdf;
   }
 
   // finalize_rough_sample_with_wavelength (open_pbr.rs:1997-2027)
-  bool finalize(Vec3 wo, Vec3 wi, uint32_t flags, TransportMode mode, BsdfSample* out) const {
+  bool finalize(Vec3 wo, Vec3 wi, uint32_t flags, TransportMode mode, BsdfSample* out, float eta = 1.0f) const {
     float pdf_v = pdf(wo, wi);
     if (pdf_v <= 0.0f) return false;
     Vec3 f = eval(wo, wi, mode);
@@ -556,7 +718,7 @@ struct Impl {
     out->pdf = pdf_v;
     out->pdf_rev = pdf(wi, wo);
     out->flags = flags;
-    out->eta = 1.0f;
+    out->eta = eta;
     return true;
   }
   bool delta_out(Vec3 wi, Vec3 weight, float p_lobe, BsdfSample* out) const {
@@ -605,11 +767,120 @@ struct Impl {
   bool sample_spec(Vec3 wo, Vec2 us, float p_lobe, TransportMode mode, BsdfSample* out) const {
     if (spec_smooth()) {
       Vec3 wi(-wo.x, -wo.y, wo.z);
-      Vec3 f = spec_fresnel(std::fabs(wi.z));
+      Vec3 f;
+      if (p.thin_walled) {
+        Vec3 T;
+        thin_wall_coeffs(std::fabs(wo.z), &f, &T);
+      } else {
+        f = spec_fresnel(std::fabs(wi.z));
+      }
       return delta_out(wi, (layer_weights(wo, &wi).spec_brdf * f) / p_lobe, p_lobe, out);
+    }
+    if (p.thin_walled) {
+      Vec3 wm;
+      if (!sample_wm_bounded_vndf(wo, p.specular_alpha_x, p.specular_alpha_y, us, &wm)) return false;
+      Vec3 wi = reflect_local(wo, wm);
+      if (wi.z <= 0.0f) return false;
+      return finalize(wo, wi, kGlossy | kReflection, mode, out);
     }
     MsParams m = ms_params(p.specular_alpha_x, p.specular_alpha_y, p.specular_eta);
     return sample_two_lobe(wo, us, reflection_lobe_weights(m), p.specular_alpha_x, p.specular_alpha_y, mode, out);
+  }
+  // math/mod.rs:83-100
+  static bool refract_z(Vec3 wo, float eta, Vec3* out) {
+    if (wo.z <= 0.0f) return false;
+    float sin2_o = fmax_num(1.0f - wo.z * wo.z, 0.0f);
+    float sin2_t = eta * eta * sin2_o;
+    if (sin2_t >= 1.0f) return false;
+    float cos_t = std::sqrt(fmax_num(1.0f - sin2_t, 0.0f));
+    Vec3 wi = normalize_or_zero(Vec3(-eta * wo.x, -eta * wo.y, -cos_t));
+    if (length_squared(wi) == 0.0f) return false;
+    *out = wi;
+    return true;
+  }
+  // refract_about (open_pbr.rs:2043-2058)
+  static bool refract_about(Vec3 wo, Vec3 wm, float eta, Vec3* out) {
+    float cos_o = dot(wo, wm);
+    if (cos_o <= 0.0f) return false;
+    float sin2_t = eta * eta * fmax_num(1.0f - cos_o * cos_o, 0.0f);
+    if (sin2_t >= 1.0f) return false;
+    float cos_t = std::sqrt(fmax_num(1.0f - sin2_t, 0.0f));
+    Vec3 wi = normalize_or_zero(-eta * wo + (eta * cos_o - cos_t) * wm);
+    if (length_squared(wi) == 0.0f) return false;
+    *out = wi;
+    return true;
+  }
+  // sample_spec_btdf (open_pbr.rs:1670-1836) without dispersion
+  bool sample_spec_btdf(Vec3 wo, Vec2 us, float p_lobe, TransportMode mode, BsdfSample* out) const {
+    if (p.thin_walled) {
+      Vec3 R, T;
+      thin_wall_coeffs(std::fabs(wo.z), &R, &T);
+      if (btdf_smooth()) {
+        Vec3 wi = -wo;
+        Vec3 bw = layer_weights(wo, &wi).spec_btdf;
+        out->weight = (bw * T) / p_lobe;
+        out->wi = wi;
+        out->pdf = p_lobe;
+        out->pdf_rev = 0.0f;
+        out->flags = kDelta | kTransmission;
+        out->eta = 1.0f;
+        return true;
+      }
+      float ax, ay;
+      thin_wall_alpha(&ax, &ay);
+      Vec3 wm;
+      if (!sample_wm_bounded_vndf(wo, ax, ay, us, &wm)) return false;
+      Vec3 wr = reflect_local(wo, wm);
+      if (wr.z <= 0.0f) return false;
+      Vec3 wi(wr.x, wr.y, -wr.z);
+      Vec3 bw = layer_weights(wo, &wi).spec_btdf;
+      float pdf_total = p_lobe * pdf_spec_btdf(wo, wi);
+      if (pdf_total <= 0.0f) return false;
+      Vec3 f = eval_thin_btdf(wo, wi);
+      out->weight = bw * f * std::fabs(wi.z) / pdf_total;
+      out->wi = wi;
+      out->pdf = pdf_total;
+      out->pdf_rev = pdf(wi, wo);
+      out->flags = kGlossy | kTransmission;
+      out->eta = 1.0f;
+      return true;
+    }
+    const float eta_used = p.transmission_eta, eta_fresnel = p.specular_eta;
+    const float eta_rel = p.front_face ? 1.0f / eta_used : eta_used;
+    if (btdf_smooth()) {
+      Vec3 wi;
+      if (!refract_z(wo, eta_rel, &wi)) return false;
+      float f = base_dielectric_fresnel(std::fabs(wo.z), eta_used, eta_fresnel);
+      float scale = trans_scale(mode, eta_rel);
+      Vec3 bw = layer_weights(wo, &wi).spec_btdf;
+      out->weight = (bw * Vec3(1, 1, 1) * (1.0f - f) * scale) / p_lobe;
+      out->wi = wi;
+      out->pdf = p_lobe;
+      out->pdf_rev = 0.0f;
+      out->flags = kDelta | kTransmission;
+      out->eta = eta_rel;
+      return true;
+    }
+    MsParams m = ms_params(p.transmission_alpha_x, p.transmission_alpha_y, eta_fresnel);
+    TwoLobe w = transmission_lobe_weights(m);
+    float ss_p = w.ss / w.total;
+    if (us.x >= ss_p) {
+      float u = ss_p < 1.0f ? (us.x - ss_p) / (1.0f - ss_p) : 0.0f;
+      Vec3 up = sample_cosine_hemisphere(Vec2(u, us.y));
+      return finalize(wo, Vec3(up.x, up.y, -up.z), kGlossy | kTransmission, mode, out, eta_rel);
+    }
+    float u = ss_p > 0.0f ? us.x / ss_p : 0.0f;
+    Vec3 wm;
+    if (!sample_wm_vndf(wo, p.transmission_alpha_x, p.transmission_alpha_y, Vec2(u, us.y), &wm)) return false;
+    float co = dot(wo, wm);
+    if (co <= 0.0f) return false;
+    Vec3 wi;
+    if (!refract_about(wo, wm, eta_rel, &wi)) return false;
+    if (wi.z >= 0.0f) return false;
+    float ci = dot(wi, wm);
+    float den = ci + eta_rel * co;
+    if (std::fabs(den) < 1.0e-6f) return false;
+    return finalize(wo, wi, kGlossy | kTransmission, mode, out, eta_rel);
   }
   // open_pbr.rs:298-332 and pick_lobe (open_pbr.rs:2043-2070)
   bool sample(Vec3 wo, float u_lobe, Vec2 us, TransportMode mode, BsdfSample* out) const {
@@ -642,7 +913,13 @@ struct Impl {
         if (!Eon(p.diffuse_roughness).sample(wo, us, &wi)) return false;
         return finalize(wo, wi, kDiffuse | kReflection, mode, out);
       }
-      default: return false;  // transmission lobes (not covered; their weights are zero)
+      case kSpecBtdf: return sample_spec_btdf(wo, us, p_lobe, mode, out);
+      default: {  // kDiffBtdf: sample_diff_btdf (open_pbr.rs:1942-1957), thin-walled only
+        if (!p.thin_walled) return false;
+        Vec3 wi;
+        if (!Eon(p.diffuse_roughness).sample(wo, us, &wi)) return false;
+        return finalize(wo, Vec3(wi.x, wi.y, -wi.z), kDiffuse | kTransmission, mode, out);
+      }
     }
   }
 };
@@ -707,11 +984,9 @@ float openpbr_specular_eta(const OpenPbrDesc& m) {
 }
 
 const char* openpbr_unsupported(const OpenPbrDesc& m) {
-  if (m.transmission_weight > 0.0f) return "transmission_weight > 0 (specular transmission)";
   if (m.thin_film_weight > 0.0f) return "thin_film_weight > 0";
   if (m.emission_luminance > 0.0f) return "emission_luminance > 0";
   if (m.geometry_opacity < 1.0f) return "geometry_opacity < 1";
-  if (m.geometry_thin_walled) return "geometry_thin_walled";
   return "";
 }
 
@@ -784,6 +1059,9 @@ OpenPbrParams make_openpbr_params(const OpenPbrDesc& m, bool front_face, Vec3 wo
   p.fuzz_roughness = fuzz_r;
   p.transmission = clampf(m.transmission_weight, 0.0f, 1.0f);
   p.transmission_color = vclamp01(Vec3(m.transmission_color[0], m.transmission_color[1], m.transmission_color[2]));
+  p.transmission_alpha_x = p.specular_alpha_x;
+  p.transmission_alpha_y = p.specular_alpha_y;
+  p.thin_walled = m.geometry_thin_walled != 0;
   p.diffuse_roughness = clampf(m.base_diffuse_roughness, 0.0f, 1.0f);
   p.subsurface = 0.0f;
   p.subsurface_color = vclamp01(Vec3(m.subsurface_color[0], m.subsurface_color[1], m.subsurface_color[2]));

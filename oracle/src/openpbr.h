@@ -5,10 +5,14 @@
 // tables), bsdf/directional_albedo.rs, material/open_pbr.rs}.
 //
 // Covered: base (EON diffuse), metal (F82-tint + multiple scattering), specular
-// reflection (GGX + multiple scattering), coat, fuzz (LTC), with optional
-// anisotropy and smooth (delta) lobes.  Not covered: specular transmission,
-// thin-walled surfaces, thin film, dispersion, emission, opacity and textures;
-// the material lowering rejects parameters that would need them.
+// reflection (GGX + multiple scattering), specular transmission (GGX BTDF +
+// multiple scattering, rough and smooth), thin-walled surfaces (the two-interface
+// slab of thin_wall_coefficients, the thin-wall BTDF and the diffuse BTDF),
+// coat, fuzz (LTC), with optional anisotropy and smooth (delta) lobes.  Not
+// covered: thin film, dispersion (transmission_dispersion_scale is not part of
+// the untextured parameter set here, so dispersion is always off), emission,
+// opacity and textures; the material lowering rejects parameters that would
+// need them.
 #pragma once
 #include "common.h"
 
@@ -117,9 +121,11 @@ struct OpenPbrParams {
   float fuzz_roughness;
   float transmission;
   Vec3 transmission_color;
+  float transmission_alpha_x, transmission_alpha_y;
   float diffuse_roughness;
   float subsurface;
   Vec3 subsurface_color;
+  bool thin_walled;
   bool front_face;
 };
 

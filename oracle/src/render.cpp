@@ -250,7 +250,13 @@ bool openpbr_sample(const Material& m, const Vertex& v, float u_lobe, Vec2 u_dir
   BsdfSample bs;
   if (!b.sample(wo_l, u_lobe, u_dir, kRadiance, &bs)) return false;
   Vec3 wi = v.frame.to_world(bs.wi);
-  if (dot(wi, v.ng) <= kGeomCosEps) return false;  // reflection only
+  // material/open_pbr.rs:523-531: transmission below the geometric surface
+  // (delta transmission kept either way), reflection above it
+  if (bs.flags & kTransmission) {
+    if (dot(wi, v.ng) >= -kGeomCosEps && !(bs.flags & kDelta)) return false;
+  } else if (dot(wi, v.ng) <= kGeomCosEps) {
+    return false;
+  }
   s->weight = bs.weight;
   s->wi = wi;
   s->pdf = bs.pdf;

@@ -212,6 +212,12 @@ MATERIALS = [
     {"base_color": [0.2, 0.7, 0.3], "specular_roughness": 0.3, "coat_weight": 0.7, "coat_roughness": 0.2},
     {"base_color": [0.6, 0.6, 0.6], "specular_roughness": 0.5, "fuzz_weight": 0.6, "fuzz_roughness": 0.5,
      "coat_weight": 0.3, "coat_roughness": 0.1, "specular_roughness_anisotropy": 0.5, "base_metalness": 0.3},
+    # rough glass, frosted glass with a tint, and a thin-walled sheet
+    {"base_color": [0.8, 0.8, 0.8], "specular_roughness": 0.3, "transmission_weight": 1.0},
+    {"base_color": [0.5, 0.7, 0.2], "specular_roughness": 0.6, "transmission_weight": 0.7,
+     "transmission_color": [0.9, 0.6, 0.3], "coat_weight": 0.4, "coat_roughness": 0.2},
+    {"base_color": [0.4, 0.5, 0.6], "specular_roughness": 0.4, "transmission_weight": 0.8,
+     "geometry_thin_walled": 1, "transmission_color": [0.7, 0.8, 0.9]},
 ]
 
 
@@ -240,7 +246,78 @@ def test_material_sample_consistent_with_eval_and_pdf(mi):
 
 
 def test_unsupported_parameters_are_rejected():
-    for bad in ({"transmission_weight": 0.5}, {"thin_film_weight": 1.0}, {"emission_luminance": 2.0},
-                {"geometry_opacity": 0.5}, {"geometry_thin_walled": 1}):
+    for bad in ({"thin_film_weight": 1.0}, {"emission_luminance": 2.0}, {"geometry_opacity": 0.5}):
         with pytest.raises(ValueError):
             orc.OpenPbrMaterial(bad)
+    orc.OpenPbrMaterial({"transmission_weight": 0.5})
+    orc.OpenPbrMaterial({"geometry_thin_walled": 1})
+
+
+# ---- transmission (bsdf/open_pbr.rs:2561-2643) ----------------------------------
+def test_thin_walled_specular_btdf_yields_pass_through():
+    """open_pbr.rs:2561-2584: a smooth thin-walled sheet transmits straight
+    through (wi = -wo)."""
+    p = default_params()
+    p.update(thin_walled=1, transmission=1.0, transmission_alpha_x=0.0, transmission_alpha_y=0.0, specular=0.0,
+             base=0.0)
+    b = orc.OpenPbrParamsBsdf(p, luts="const")
+    wo = unit([0.2, -0.3, 0.9327379])
+    rng = np.random.default_rng(0)
+    got = False
+    for _ in range(32):
+        u = rng.random(3)
+        s = b.sample(wo, u[0], (u[1], u[2]))
+        if s is not None and s["flags"] & 2:
+            np.testing.assert_allclose(s["wi"], -wo, atol=1e-5)
+            got = True
+            break
+    assert got
+
+
+def refract(wo, eta):  # math/mod.rs:83-100
+    sin2_t = eta * eta * max(1.0 - wo[2] * wo[2], 0.0)
+    cos_t = np.sqrt(max(1.0 - sin2_t, 0.0))
+    return unit([-eta * wo[0], -eta * wo[1], -cos_t])
+
+
+def test_smooth_transmission_eta_controls_refraction_direction():
+    """open_pbr.rs:2619-2642: the smooth BTDF refracts with the transmission
+    eta (1.5), not the specular one (1.0)."""
+    p = default_params()
+    p.update(base=0.0, specular=0.0, transmission=1.0, transmission_alpha_x=0.0, transmission_alpha_y=0.0,
+             specular_eta=1.0, transmission_eta=1.5)
+    b = orc.OpenPbrParamsBsdf(p, luts="const")
+    wo = unit([0.35, 0.0, 0.93675])
+    s = b.sample(wo, 0.999, (0.0, 0.0))  # the last non-empty lobe: the BTDF
+    assert s is not None and s["flags"] & 2 and s["flags"] & 16
+    np.testing.assert_allclose(s["wi"], refract(wo, 1.0 / 1.5), atol=1e-5)
+
+
+def test_rough_transmission_pdf_and_weight_consistent():
+    """Rough BTDF samples (both faces): weight = f |cos| / pdf and pdf = the
+    pdf query, the identities finalize_rough_sample (open_pbr.rs:1997-2027)
+    builds them from; the pdf over the lower hemisphere integrates below 1."""
+    for front in (1, 0):
+        p = default_params()
+        p.update(base=0.0, transmission=1.0, specular_alpha_x=0.2, specular_alpha_y=0.2, transmission_alpha_x=0.2,
+                 transmission_alpha_y=0.2, front_face=front)
+        b = orc.OpenPbrParamsBsdf(p, luts="real")
+        rng = np.random.default_rng(front)
+        n_t = 0
+        for _ in range(300):
+            wo = unit(rng.normal(size=3) * [1, 1, 0.3] + [0, 0, 1.0])
+            u = rng.random(3)
+            s = b.sample(wo, u[0], (u[1], u[2]))
+            if s is None or not (s["flags"] & 2):
+                continue
+            n_t += 1
+            assert s["wi"][2] < 0
+            f = b.eval(wo, s["wi"])
+            pdf = b.pdf(wo, s["wi"])
+            assert abs(pdf - s["pdf"]) <= 1e-5 * max(pdf, 1.0)
+            np.testing.assert_allclose(s["weight"], f * (abs(s["wi"][2]) / pdf), rtol=1e-4, atol=1e-7)
+        assert n_t > 50
+        wis, dA = orc.hemisphere_grid(256, 256)
+        wis = wis * [1, 1, -1]
+        _, pdf = b.eval_pdf_batch(WO, wis)
+        assert 0.3 < float(pdf.astype(np.float64).sum() * dA) <= 1.0 + 1e-2

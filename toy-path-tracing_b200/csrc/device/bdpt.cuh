@@ -82,7 +82,7 @@ static __device__ __noinline__ bool material_sample_rev(const DevRender& S, cons
     opbr::Sample bs;
     if (!opbr::sample(ov, u_lobe, u0, u1, bs, importance, true)) return false;
     const V3 wi = to_world(v.frame, bs.wi);
-    if (dot(wi, v.ng) <= kGeomCosEps) return false;
+    if (!opbr_sample_side_ok(v, wi, bs.flags)) return false;
     s.delta = (bs.flags & opbr::kFlagDelta) != 0;
     s.weight = modified_weight(v, wi, bs.weight, s.delta, importance);
     s.wi = wi;

@@ -26,7 +26,8 @@ constexpr float kRcpPi = 1.0f / kPiF;
 constexpr float kC1Fon = 0.5f - 2.0f / (3.0f * kPiF);
 constexpr float kC2Fon = 2.0f / 3.0f - 28.0f / (15.0f * kPiF);
 constexpr float kEonEps = 1.0e-7f;
-constexpr uint32_t kFlagReflection = 1u, kFlagDiffuse = 4u, kFlagGlossy = 8u, kFlagDelta = 16u;
+constexpr uint32_t kFlagReflection = 1u, kFlagTransmission = 2u, kFlagDiffuse = 4u, kFlagGlossy = 8u,
+                   kFlagDelta = 16u;
 
 __device__ __forceinline__ float lum(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 __device__ __forceinline__ V3 splat(float s) { return V3{s, s, s}; }
@@ -122,6 +123,65 @@ __device__ __forceinline__ float pdf_wm_bounded_vndf(V3 wo, V3 wm, float ax, flo
   const float denom = k * wo.z + t;
   if (denom <= 0.0f) return 0.0f;
   return 2.0f * ggx_d(wm, ax, ay) * fmaxf(dot(wo, wm), 0.0f) / denom;
+}
+__device__ __forceinline__ float ggx_g1(V3 w, float ax, float ay) {
+  const float l = ggx_lambda(w, ax, ay);
+  if (!isfinite(l)) return 0.0f;
+  return 1.0f / (1.0f + l);
+}
+// smith_ggx.rs:62-75
+__device__ __forceinline__ float pdf_wm_vndf(V3 wo, V3 wm, float ax, float ay) {
+  if (!(wo.z > 0.0f) || wm.z <= 0.0f) return 0.0f;
+  const float d = ggx_d(wm, ax, ay);
+  const float g1 = ggx_g1(wo, ax, ay);
+  const float c = fmaxf(dot(wo, wm), 0.0f);
+  if (d <= 0.0f || g1 <= 0.0f || c <= 0.0f) return 0.0f;
+  return d * g1 * c / wo.z;
+}
+// sample_wm_vndf, Heitz 2018 (smith_ggx.rs:77-123)
+__device__ __forceinline__ bool sample_wm_vndf(V3 wo, float ax, float ay, float u0, float u1, V3& out) {
+  if (wo.z <= 0.0f) return false;
+  ax = fmaxf(ax, kMinAlpha);
+  ay = fmaxf(ay, kMinAlpha);
+  const V3 wo_std = normalize_or_zero(V3{ax * wo.x, ay * wo.y, wo.z});
+  if (length_sq(wo_std) == 0.0f) return false;
+  const float lensq = wo_std.x * wo_std.x + wo_std.y * wo_std.y;
+  const V3 t1 = lensq > 0.0f ? V3{-wo_std.y, wo_std.x, 0.0f} / sqrtf(lensq) : V3{1.0f, 0.0f, 0.0f};
+  const V3 t2 = cross(wo_std, t1);
+  const float r = sqrtf(clampf(u0, 0.0f, 1.0f));
+  const float phi = kTauF * u1;
+  const float p1 = r * cosf(phi);
+  float p2 = r * sinf(phi);
+  const float s = 0.5f * (1.0f + wo_std.z);
+  p2 = (1.0f - s) * sqrtf(fmaxf(1.0f - p1 * p1, 0.0f)) + s * p2;
+  const V3 nh = p1 * t1 + p2 * t2 + sqrtf(fmaxf(1.0f - p1 * p1 - p2 * p2, 0.0f)) * wo_std;
+  const V3 wm = normalize_or_zero(V3{ax * nh.x, ay * nh.y, fmaxf(nh.z, 0.0f)});
+  if (length_sq(wm) == 0.0f || wm.z <= 0.0f) return false;
+  out = wm;
+  return true;
+}
+// math/mod.rs:83-100 (refraction about +z) and refract_about (open_pbr.rs:2043-2058)
+__device__ __forceinline__ bool refract_z(V3 wo, float eta, V3& out) {
+  if (wo.z <= 0.0f) return false;
+  const float sin2_o = fmaxf(1.0f - wo.z * wo.z, 0.0f);
+  const float sin2_t = eta * eta * sin2_o;
+  if (sin2_t >= 1.0f) return false;
+  const float cos_t = sqrtf(fmaxf(1.0f - sin2_t, 0.0f));
+  const V3 wi = normalize_or_zero(V3{-eta * wo.x, -eta * wo.y, -cos_t});
+  if (length_sq(wi) == 0.0f) return false;
+  out = wi;
+  return true;
+}
+__device__ __forceinline__ bool refract_about(V3 wo, V3 wm, float eta, V3& out) {
+  const float cos_o = dot(wo, wm);
+  if (cos_o <= 0.0f) return false;
+  const float sin2_t = eta * eta * fmaxf(1.0f - cos_o * cos_o, 0.0f);
+  if (sin2_t >= 1.0f) return false;
+  const float cos_t = sqrtf(fmaxf(1.0f - sin2_t, 0.0f));
+  const V3 wi = normalize_or_zero(-eta * wo + (eta * cos_o - cos_t) * wm);
+  if (length_sq(wi) == 0.0f) return false;
+  out = wi;
+  return true;
 }
 // math/mod.rs:26-40
 __device__ __forceinline__ V3 sample_cosine_hemisphere(float u0, float u1) {
@@ -388,12 +448,14 @@ struct OpbrVertex {
   float dec_eo[2];     // dielectric E(wo) of the specular and coat lobes
   float cec_eo;        // conductor E(wo)
   V3 darkening;
-  float q_coat, q_metal, q_spec, q_fuzz, q_diff, q_total;
+  V3 tw_r, tw_t;  // thin_wall_coefficients(|wo.z|) of thin-walled materials
+  float q_coat, q_metal, q_spec, q_btdf, q_fuzz, q_diff, q_total;
 };
 
-// LayerWeights below the coat for a given coat tint (open_pbr.rs:334-406)
+// LayerWeights below the coat for a given coat tint (open_pbr.rs:334-406);
+// the diffuse BTDF's weight is zero (subsurface is forced to 0 on add)
 struct Below {
-  V3 metal, spec, diff;
+  V3 metal, spec, btdf, diff;
 };
 __device__ __forceinline__ Below weights_below(const OpbrVertex& s, V3 tint) {
   const DevOpenPbr& m = *s.m;
@@ -410,8 +472,44 @@ __device__ __forceinline__ Below weights_below(const OpbrVertex& s, V3 tint) {
   const V3 sc = ld3(m.specular_color);
   b.spec = below_metal * sc;
   const V3 below_spec = below_metal * vmaxv(one - sc * s.e_spec, V3{0.0f, 0.0f, 0.0f});
-  b.diff = below_spec * ((1.0f - 0.0f) * m.base) * ld3(m.base_color);
+  const V3 trans_tint = (m.flags & kOpbrThinWalled) ? one : ld3(m.trans_color);
+  b.btdf = below_spec * m.transmission * trans_tint;
+  const V3 below_trans = below_spec * (1.0f - m.transmission);
+  b.diff = below_trans * ((1.0f - 0.0f) * m.base) * ld3(m.base_color);
   return b;
+}
+
+__device__ __forceinline__ float spec_fresnel(const DevOpenPbr& m, uint32_t face, float c) {
+  const DevFresnelFace& f = m.fres[face];
+  const float unc = weighted_fresnel_ratio(c, f.unc_ti, f.unc_tp);
+  if (m.coat_clamped <= 0.0f) return unc;
+  const float coated = weighted_fresnel_ratio(c, f.coat_ti, f.coat_tp);
+  return unc + (coated - unc) * m.coat_clamped;
+}
+
+// thin_wall_coefficients (open_pbr.rs:931-959, thin_wall_internal_fresnel
+// 961-979) without thin film: reflectance and transmittance of the slab.
+__device__ __forceinline__ void thin_wall_coeffs(const DevOpenPbr& m, uint32_t face, float cos_theta_o, V3& r_out,
+                                                 V3& t_out) {
+  const V3 one = V3{1.0f, 1.0f, 1.0f}, zero = V3{0.0f, 0.0f, 0.0f};
+  const float eta = fmaxf(m.trans_eta, 1.0e-4f);
+  const float eta_prime = fmaxf(m.trans_eta, 1.0e-4f);  // specular_eta = transmission_eta
+  const float cos_o = clampf(cos_theta_o, 0.0f, 1.0f);
+  const float sin2_o = fmaxf(1.0f - cos_o * cos_o, 0.0f);
+  const float sin2_i = clampf(sin2_o / (eta * eta), 0.0f, 1.0f);
+  const float cos_i = fmaxf(sqrtf(1.0f - sin2_i), 1.0e-4f);
+  const V3 f_o = clamp01(splat(spec_fresnel(m, face, cos_o)));
+  const V3 f_i = clamp01(splat(weighted_fresnel_ratio(cos_i, 1.0f / fmaxf(eta, 1.0e-4f), 1.0f / fmaxf(eta_prime, 1.0e-4f))));
+  const float e = 1.0f / cos_i;
+  const V3 tc = clamp01(ld3(m.trans_color));
+  const V3 a = V3{powf(tc.x, e), powf(tc.y, e), powf(tc.z, e)};
+  const V3 a2 = a * a;
+  const V3 f_i2_a2 = a2 * f_i * f_i;
+  const V3 denom = vmaxv(one - f_i2_a2, splat(1.0e-6f));
+  const V3 omfo = vmaxv(one - f_o, zero);
+  const V3 omfi = vmaxv(one - f_i, zero);
+  r_out = clamp01(f_o + vdiv(omfo * omfi * f_i * a2, denom));
+  t_out = clamp01(omfo * omfi * a * (one + vdiv(f_i2_a2, denom)));
 }
 
 __device__ __forceinline__ float albedo_with_ms(const OpbrVertex& s, int lobe, bool alpha_rough, float ss) {
@@ -460,15 +558,18 @@ static __device__ __noinline__ void init_vertex(OpbrVertex& s, const DevOpenPbr*
   s.e_spec = 0.0f;
   if (wo.z > 0.0f) {
     const float ss = da_lookup(m.spec_da, m.spec_da_eta, (m.flags & kOpbrSpecDaSmooth) != 0, m.spec_da_r, wo);
-    s.e_spec = albedo_with_ms(s, 0, spec_alpha_rough, ss);
+    // thin-walled: the single-scattering albedo alone (open_pbr.rs:485-487)
+    s.e_spec = (m.flags & kOpbrThinWalled) ? ss : albedo_with_ms(s, 0, spec_alpha_rough, ss);
   }
+  if (m.flags & kOpbrThinWalled) thin_wall_coeffs(m, s.face, fabsf(wo.z), s.tw_r, s.tw_t);
   const Below b = weights_below(s, ld3(m.coat_color));
   s.q_coat = m.coat > 0.0f ? m.coat * s.below_fuzz_s : 0.0f;
   s.q_metal = lum(b.metal * (splat(0.5f) + 0.5f * ld3(m.base_color)));
   s.q_spec = lum(b.spec);
+  s.q_btdf = (m.flags & kOpbrTrans) ? fmaxf(lum(b.btdf), 0.0f) : 0.0f;
   s.q_fuzz = fmaxf(lum(m.fuzz * ld3(m.fuzz_color)), 0.0f);
   s.q_diff = fmaxf(lum(b.diff), 0.0f);
-  s.q_total = s.q_coat + s.q_metal + s.q_spec + s.q_fuzz + s.q_diff;
+  s.q_total = s.q_coat + s.q_metal + s.q_spec + s.q_btdf + s.q_fuzz + s.q_diff;
 }
 
 __device__ __forceinline__ V3 metal_fresnel(const DevOpenPbr& m, float c) {
@@ -478,13 +579,6 @@ __device__ __forceinline__ V3 metal_fresnel(const DevOpenPbr& m, float c) {
   const float cc = clampf(c, 0.0f, 1.0f);
   const float corr = cc * powi6(1.0f - cc) / m.f82_denom;
   return clamp01(m.specular * (fs - corr * ld3(m.f82_delta)));
-}
-__device__ __forceinline__ float spec_fresnel(const DevOpenPbr& m, uint32_t face, float c) {
-  const DevFresnelFace& f = m.fres[face];
-  const float unc = weighted_fresnel_ratio(c, f.unc_ti, f.unc_tp);
-  if (m.coat_clamped <= 0.0f) return unc;
-  const float coated = weighted_fresnel_ratio(c, f.coat_ti, f.coat_tp);
-  return unc + (coated - unc) * m.coat_clamped;
 }
 __device__ __forceinline__ float refl_ms(const OpbrVertex& s, int lobe, float wi_z) {
   const DevMsFace& f = s.m->ms[lobe][s.face];
@@ -501,12 +595,75 @@ __device__ __forceinline__ V3 coat_tint(const DevOpenPbr& m, V3 wo, V3 wi) {
             powf(fmaxf(m.coat_color[2], 0.0f), e)};
 }
 
+// The specular BTDF and its pdf for wi below the surface (eval_spec_btdf,
+// eval_thin_wall_spec_btdf, pdf_specular_btdf, open_pbr.rs:1024-1222, without
+// dispersion); `importance` selects the transport mode's eta^2 scaling.
+__device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool importance, float& f, float& pdf,
+                                              V3& f_thin) {
+  const DevOpenPbr& m = *s.m;
+  const V3 wo = s.wo;
+  f = 0.0f;
+  pdf = 0.0f;
+  f_thin = V3{0.0f, 0.0f, 0.0f};
+  if (!(m.flags & kOpbrTransRough)) return;  // spec_btdf_is_smooth: neither term
+  if (m.flags & kOpbrThinWalled) {
+    const V3 wim = V3{wi.x, wi.y, -wi.z};
+    V3 wm;
+    if (!half_vector(wo, wim, wm)) return;
+    const float d = ggx_d(wm, m.tw_ax, m.tw_ay);
+    const float g = ggx_g2(wo, wim, m.tw_ax, m.tw_ay);
+    if (!(d <= 0.0f || g <= 0.0f)) f_thin = s.tw_t * (d * g / (4.0f * wo.z * fabsf(wi.z)));
+    const float pdf_wm = pdf_wm_bounded_vndf(wo, wm, m.tw_ax, m.tw_ay);
+    const float denom = 4.0f * fabsf(dot(wo, wm));
+    pdf = denom > 0.0f ? pdf_wm / denom : 0.0f;
+    return;
+  }
+  const float eta_rel = m.teta_rel[s.face];
+  const DevMsFace& fm = m.ms[0][s.face];
+  // the single-scattering half, shared by eval and pdf (their validity tests agree)
+  float pdf_ss = 0.0f;
+  const V3 wmu = eta_rel * wo + wi;
+  if (!(length_sq(wmu) < 1.0e-12f)) {
+    V3 wm = normalize(wmu);
+    if (wm.z < 0.0f) wm = -wm;
+    const float co = dot(wo, wm);
+    const float ci = dot(wi, wm);
+    const float den = ci + eta_rel * co;
+    if (!(co <= 0.0f) && !(fabsf(den) < 1.0e-6f)) {
+      const float d = ggx_d(wm, m.spec_ax, m.spec_ay);
+      const float g = ggx_g2(wo, wi, m.spec_ax, m.spec_ay);
+      if (!(d <= 0.0f || g <= 0.0f)) {
+        const float scale = importance ? 1.0f : 1.0f / (eta_rel * eta_rel);
+        const float sc = d * g * fabsf(ci * co);
+        const float denom = den * den * fabsf(wo.z) * fabsf(wi.z);
+        if (!(denom <= 0.0f)) {
+          const float scalar = sc * scale / denom;
+          const float fr = spec_fresnel(m, s.face, co);
+          // eval_dielectric_transmission_ms (open_pbr.rs:672-696)
+          const float e_o = s.dec_eo[0];
+          DevMsFace ft = fm;
+          ft.eta_axis = fm.eta_rel_axis;
+          const float e_i = dec_lookup_e(s.dec_e, ft, fabsf(wi.z));
+          const float ms_scale = importance ? 1.0f : 1.0f / (fm.eta_rel * fm.eta_rel);
+          const float ms = (1.0f - fm.ratio_r) * (1.0f - e_o) * (1.0f - e_i) * ms_scale /
+                           (kPiF * fm.one_minus_e_avg_t);
+          f = fmaxf(1.0f - fr, 0.0f) * scalar + ms;
+        }
+      }
+      const float pdf_wm = pdf_wm_vndf(wo, wm, m.spec_ax, m.spec_ay);
+      pdf_ss = pdf_wm <= 0.0f ? 0.0f : pdf_wm * fabsf(ci) / (den * den);
+    }
+  }
+  pdf = (fm.trans_ss * pdf_ss + fm.trans_ms * cosine_pdf(-wi.z)) / fm.trans_total;
+}
+
 // OpenPbrBsdf::eval and ::pdf for one direction pair.  `lay` is the state of
 // the direction the layer weights are taken at: the vertex itself in radiance
 // transport, wi in importance transport (open_pbr.rs:228-233).  want_pdf =
-// false leaves pdf_out at 0 (callers that need f only).
+// false leaves pdf_out at 0 (callers that need f only).  `importance` is the
+// transport mode (the BTDF's eta^2 scaling depends on it).
 static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVertex& lay, V3 wi, V3& f_out,
-                                             float& pdf_out, bool want_pdf = true) {
+                                             float& pdf_out, bool want_pdf = true, bool importance = false) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
   V3 total = V3{0.0f, 0.0f, 0.0f};
@@ -514,7 +671,22 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVert
   f_out = total;
   pdf_out = 0.0f;
   if (!(wo.z > 0.0f)) return;  // is_upper_hemisphere(wo)
-  if (wi.z <= 0.0f) return;     // every covered lobe is zero below the surface
+  if (wi.z < 0.0f) {
+    // below the surface only the specular BTDF is non-zero (the reflection
+    // lobes, fuzz and EON test wi.z > 0; the diffuse BTDF has zero weight);
+    // the coat tint of a direction below the coat is one
+    if (!(m.flags & kOpbrTrans)) return;
+    const Below b = weights_below(lay, V3{1.0f, 1.0f, 1.0f});
+    float fb, pb;
+    V3 f_thin;
+    btdf_eval_pdf(s, wi, importance, fb, pb, f_thin);
+    if (length_sq(b.btdf) > 0.0f && (m.flags & kOpbrTransRough))
+      f_out = (m.flags & kOpbrThinWalled) ? b.btdf * f_thin : b.btdf * splat(fb);
+    if (want_pdf && s.q_total > 0.0f && s.q_btdf > 0.0f && (m.flags & kOpbrTransRough))
+      pdf_out = (s.q_btdf / s.q_total) * pb;
+    return;
+  }
+  if (wi.z <= 0.0f) return;  // grazing (or NaN): every lobe is zero
   V3 wm;
   const bool has_wm = half_vector(wo, wi, wm);
   // layer weights with this wi (the coat tint depends on it)
@@ -555,9 +727,13 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVert
   }
   // dielectric specular reflection (eval_spec_brdf)
   if (length_sq(b.spec) > 0.0f && (m.flags & kOpbrSpecRough) && has_wm && !(d_s <= 0.0f || g_s <= 0.0f)) {
-    const float fr = spec_fresnel(m, s.face, fabsf(dot(wo, wm)));
-    const V3 ss = splat(fr) * (d_s * g_s / inv4);
-    total = total + b.spec * (ss + splat(refl_ms(s, 0, wi.z)));
+    if (m.flags & kOpbrThinWalled) {
+      total = total + b.spec * (s.tw_r * (d_s * g_s / inv4));
+    } else {
+      const float fr = spec_fresnel(m, s.face, fabsf(dot(wo, wm)));
+      const V3 ss = splat(fr) * (d_s * g_s / inv4);
+      total = total + b.spec * (ss + splat(refl_ms(s, 0, wi.z)));
+    }
   }
   float fz_f = 0.0f, fz_pdf = 0.0f;
   if (m.fuzz > 0.0f) fuzz_eval_pdf(m.fuzz_roughness, wo, wi, fz_f, fz_pdf);
@@ -588,7 +764,9 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVert
     pdf += (s.q_metal / s.q_total) * ((m.cond_ss * pdf_ss_s + m.cond_ms * pdf_cos) / m.cond_total);
   if (s.q_spec > 0.0f && (m.flags & kOpbrSpecRough)) {
     const DevMsFace& f = m.ms[0][s.face];
-    pdf += (s.q_spec / s.q_total) * ((f.lobe_ss * pdf_ss_s + f.lobe_ms * pdf_cos) / f.lobe_total);
+    pdf += (s.q_spec / s.q_total) * ((m.flags & kOpbrThinWalled) ? pdf_ss_s
+                                                                   : (f.lobe_ss * pdf_ss_s + f.lobe_ms * pdf_cos) /
+                                                                         f.lobe_total);
   }
   if (s.q_fuzz > 0.0f) pdf += (s.q_fuzz / s.q_total) * fz_pdf;
   if (s.q_diff > 0.0f) pdf += (s.q_diff / s.q_total) * eon_pdf(m.eon_r, m.eon_r_pow01, wo, wi);
@@ -610,7 +788,7 @@ __device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t fl
   float pdf;
   OpbrVertex at_wi;  // the same BSDF seen from wi
   if (importance || want_rev) init_vertex(at_wi, s.m, s.cec_e, s.dec_e, wi, s.face == 0u, s.dk_cos);
-  eval_pdf(s, importance ? at_wi : s, wi, f, pdf);
+  eval_pdf(s, importance ? at_wi : s, wi, f, pdf, true, importance);
   if (pdf <= 0.0f) return false;
   if (length_sq(f) == 0.0f) return false;
   const float c = fabsf(wi.z);
@@ -627,13 +805,83 @@ __device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t fl
   return true;
 }
 
+// sample_spec_btdf (open_pbr.rs:1670-1836) without dispersion: thin-walled
+// (smooth pass-through or the mirrored thin-wall GGX lobe), smooth refraction,
+// or the rough BTDF (VNDF single scattering / cosine multiple scattering).
+static __device__ __noinline__ bool sample_btdf(const OpbrVertex& s, float p_lobe, float u0, float u1, Sample& out,
+                                                bool importance, bool want_rev) {
+  const DevOpenPbr& m = *s.m;
+  const V3 wo = s.wo;
+  const V3 one = V3{1.0f, 1.0f, 1.0f};
+  const bool rough = (m.flags & kOpbrTransRough) != 0;
+  out.pdf_rev = 0.0f;
+  if (m.flags & kOpbrThinWalled) {
+    if (!rough) {
+      const V3 wi = -wo;
+      out.weight = (weights_below(s, one).btdf * s.tw_t) / p_lobe;
+      out.wi = wi;
+      out.pdf = p_lobe;
+      out.flags = kFlagDelta | kFlagTransmission;
+      return true;
+    }
+    V3 wm;
+    if (!sample_wm_bounded_vndf(wo, m.tw_ax, m.tw_ay, u0, u1, wm)) return false;
+    const V3 wr = reflect_local(wo, wm);
+    if (wr.z <= 0.0f) return false;
+    const V3 wi = V3{wr.x, wr.y, -wr.z};
+    const V3 bw = weights_below(s, one).btdf;
+    float fb, pb;
+    V3 f_thin;
+    btdf_eval_pdf(s, wi, importance, fb, pb, f_thin);
+    const float pdf_total = p_lobe * pb;
+    if (pdf_total <= 0.0f) return false;
+    out.weight = bw * f_thin * fabsf(wi.z) / pdf_total;
+    out.wi = wi;
+    out.pdf = pdf_total;
+    out.flags = kFlagGlossy | kFlagTransmission;
+    return true;  // pdf_rev = pdf(wi, wo) = 0: wi is below the surface
+  }
+  const float eta_rel = m.teta_rel[s.face];
+  if (!rough) {
+    V3 wi;
+    if (!refract_z(wo, eta_rel, wi)) return false;
+    const float fr = spec_fresnel(m, s.face, fabsf(wo.z));
+    const float scale = importance ? 1.0f : 1.0f / (eta_rel * eta_rel);
+    out.weight = (weights_below(s, one).btdf * one * (1.0f - fr) * scale) / p_lobe;
+    out.wi = wi;
+    out.pdf = p_lobe;
+    out.flags = kFlagDelta | kFlagTransmission;
+    return true;
+  }
+  const DevMsFace& fm = m.ms[0][s.face];
+  const float ss_p = fm.trans_ss / fm.trans_total;
+  V3 wi;
+  if (u0 >= ss_p) {
+    const float uu = ss_p < 1.0f ? (u0 - ss_p) / (1.0f - ss_p) : 0.0f;
+    const V3 up = sample_cosine_hemisphere(uu, u1);
+    wi = V3{up.x, up.y, -up.z};
+  } else {
+    const float uu = ss_p > 0.0f ? u0 / ss_p : 0.0f;
+    V3 wm;
+    if (!sample_wm_vndf(wo, m.spec_ax, m.spec_ay, uu, u1, wm)) return false;
+    const float co = dot(wo, wm);
+    if (co <= 0.0f) return false;
+    if (!refract_about(wo, wm, eta_rel, wi)) return false;
+    if (wi.z >= 0.0f) return false;
+    const float ci = dot(wi, wm);
+    const float den = ci + eta_rel * co;
+    if (fabsf(den) < 1.0e-6f) return false;
+  }
+  return finalize(s, wi, kFlagGlossy | kFlagTransmission, importance, want_rev, out);
+}
+
 // OpenPbrBsdf::sample (open_pbr.rs:298-332) in the shading frame.
 static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, float u0, float u1, Sample& out,
                                            bool importance = false, bool want_rev = false) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
   if (!(wo.z > 0.0f) || s.q_total <= 0.0f) return false;
-  // pick_lobe over (coat, metal, spec_brdf, spec_btdf = 0, fuzz, diff_brdf, diff_btdf = 0)
+  // pick_lobe over (coat, metal, spec_brdf, spec_btdf, fuzz, diff_brdf, diff_btdf = 0)
   float u = u_lobe * s.q_total;
   int lobe;
   float pl;
@@ -646,9 +894,10 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
   } else if ((u -= s.q_metal) < s.q_spec) {
     lobe = 2;
     pl = s.q_spec;
-  } else if ((u -= s.q_spec) < 0.0f) {
-    return false;  // specular transmission (weight zero)
-  } else if ((u -= 0.0f) < s.q_fuzz) {
+  } else if ((u -= s.q_spec) < s.q_btdf) {
+    lobe = 5;
+    pl = s.q_btdf;
+  } else if ((u -= s.q_btdf) < s.q_fuzz) {
     lobe = 3;
     pl = s.q_fuzz;
   } else if ((u -= s.q_fuzz) < s.q_diff) {
@@ -659,6 +908,7 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
   }
   const float p_lobe = pl / s.q_total;
   if (p_lobe <= 0.0f) return false;
+  if (lobe == 5) return sample_btdf(s, p_lobe, u0, u1, out, importance, want_rev);
   if (lobe == 3 || lobe == 4) {
     V3 wi;
     const bool ok = lobe == 3 ? fuzz_sample_dir(m.fuzz_roughness, wo, u0, u1, wi)
@@ -679,13 +929,22 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
       out.weight = splat(m.coat * s.below_fuzz_s * fr / p_lobe);
     } else {
       const Below b = weights_below(s, tint);
-      out.weight = lobe == 1 ? (b.metal * metal_fresnel(m, fabsf(wi.z))) / p_lobe
-                             : (b.spec * splat(spec_fresnel(m, s.face, fabsf(wi.z)))) / p_lobe;
+      // a thin-walled sheet reflects its slab reflectance (open_pbr.rs:1596-1602)
+      const V3 fs = (m.flags & kOpbrThinWalled) ? s.tw_r : splat(spec_fresnel(m, s.face, fabsf(wi.z)));
+      out.weight = lobe == 1 ? (b.metal * metal_fresnel(m, fabsf(wi.z))) / p_lobe : (b.spec * fs) / p_lobe;
     }
     out.wi = wi;
     out.pdf = p_lobe;
     out.flags = kFlagDelta | kFlagReflection;
     return true;
+  }
+  // rough thin-walled specular: GGX single scattering only (open_pbr.rs:1615-1628)
+  if (lobe == 2 && (m.flags & kOpbrThinWalled)) {
+    V3 wm;
+    if (!sample_wm_bounded_vndf(wo, m.spec_ax, m.spec_ay, u0, u1, wm)) return false;
+    const V3 wi = reflect_local(wo, wm);
+    if (wi.z <= 0.0f) return false;
+    return finalize(s, wi, kFlagGlossy | kFlagReflection, importance, want_rev, out);
   }
   // rough: GGX single scattering or cosine multiple scattering
   float ss, tot, ax, ay;

@@ -171,6 +171,14 @@ __device__ __forceinline__ bool lambert_sample(const DevMaterialRec& m, const Ve
   return dot(s.wi, v.ng) > kGeomCosEps;
 }
 
+// material/open_pbr.rs:523-531: a transmitted direction must leave below the
+// geometric surface (a delta transmission is kept either way), a reflected one
+// above it.
+__device__ __forceinline__ bool opbr_sample_side_ok(const Vertex& v, V3 wi, uint32_t flags) {
+  if (flags & opbr::kFlagTransmission) return !(dot(wi, v.ng) >= -kGeomCosEps && !(flags & opbr::kFlagDelta));
+  return dot(wi, v.ng) > kGeomCosEps;
+}
+
 // OpenPbrMaterial::sample (material/open_pbr.rs:489-563) in radiance transport
 // (modified_bsdf_sample_weight leaves the weight unchanged there).
 static __device__ __noinline__ bool openpbr_sample(const DevRenderData& d, uint32_t opbr_index, const Vertex& v,
@@ -183,7 +191,7 @@ static __device__ __noinline__ bool openpbr_sample(const DevRenderData& d, uint3
   opbr::Sample bs;
   if (!opbr::sample(ov, u_lobe, u0, u1, bs)) return false;
   const V3 wi = to_world(v.frame, bs.wi);
-  if (dot(wi, v.ng) <= kGeomCosEps) return false;  // reflection lobes only
+  if (!opbr_sample_side_ok(v, wi, bs.flags)) return false;
   s.wi = wi;
   s.weight = bs.weight;
   s.pdf = bs.pdf;
@@ -286,7 +294,7 @@ static __device__ __noinline__ V3 material_eval(const DevRender& S, const DevMat
     if (importance) {
       opbr::OpbrVertex lay;
       opbr::init_vertex(lay, mp, S.d.cec_e, S.d.dec_e, wi_l, v.front, fabsf(wo_l.z));
-      opbr::eval_pdf(s, lay, wi_l, f, pdf);
+      opbr::eval_pdf(s, lay, wi_l, f, pdf, true, true);
     } else {
       opbr::eval_pdf(s, s, wi_l, f, pdf);
     }

@@ -47,6 +47,11 @@ struct DevMsFace {  // dielectric multiple scattering of one lobe seen from one 
   float eta_o, one_minus_e_avg_o, ms_factor;
   float lobe_ss, lobe_ms, lobe_total;  // dielectric_reflection_lobe_weights
   DevLerpAxis r_axis, eta_axis;         // energy-compensation table axes at (roughness_eq, eta_o)
+  // the transmission half of dielectric_ms_params (open_pbr.rs:612-636) and
+  // dielectric_transmission_lobe_weights (638-646)
+  float eta_rel, one_minus_e_avg_t, ratio_r;
+  float trans_ss, trans_ms, trans_total;
+  DevLerpAxis eta_rel_axis;  // table axis at eta_rel
 };
 struct DevFresnelFace {  // base_dielectric_fresnel's weighted_fresnel_ratio arguments
   float unc_ti, unc_tp, coat_ti, coat_tp;
@@ -58,6 +63,9 @@ enum : uint32_t {
   kOpbrDarkening = 8u,    // coat darkening active
   kOpbrSpecDaSmooth = 16u,
   kOpbrCoatDaSmooth = 32u,
+  kOpbrTrans = 64u,         // transmission > 0
+  kOpbrTransRough = 128u,   // transmission > 0 and not smooth (spec_btdf_is_smooth false)
+  kOpbrThinWalled = 256u,   // geometry_thin_walled
 };
 struct alignas(16) DevOpenPbr {
   float base_color[3], base;
@@ -85,7 +93,12 @@ struct alignas(16) DevOpenPbr {
   // coat darkening (material/open_pbr.rs:823-858) without the view term
   float dk_kr, dk_rb, dk_wd, dk_eta;
   float dk_e_base[3];
-  uint32_t pad[3];
+  // specular transmission: weight, clamped transmission colour, the thin-wall
+  // GGX alphas (thin_wall_transmission_alpha_xy), the transmission eta and
+  // the relative eta per face (transmission_eta_rel: 1/eta front, eta back)
+  float transmission;
+  float trans_color[3], tw_ax;
+  float tw_ay, trans_eta, teta_rel[2];
 };
 
 struct alignas(16) DevShadeInstance {

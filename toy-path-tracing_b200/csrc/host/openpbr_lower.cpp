@@ -129,7 +129,20 @@ DevMsFace ms_face(float ax, float ay, float eta, bool front, const float* dec_e_
   float factor = clampf(f_avg * f_avg * e_avg_o / std::fmax(denom, kMsEps), 0.0f, 1.0f);
   float ss = clampf(f_avg * e_avg_o, 0.0f, 1.0f);
   float ms = std::fmax(1.0f - e_avg_o, 0.0f) * factor;
-  (void)eta_rel;  // the transmission terms that read it are not covered
+  // transmission terms (open_pbr.rs:621-636, 638-646)
+  float e_avg_t = dec_lookup_e_avg(dec_e_avg, req, eta_rel);
+  float om_t = std::fmax(1.0f - e_avg_t, kMsEps);
+  float f_avg_o = f_avg_dielectric(eta_o), f_avg_t = f_avg_dielectric(eta_rel);
+  float a = (1.0f - f_avg_o) / om_o;
+  float b = (1.0f - f_avg_t) * eta_o * eta_o / om_t;
+  float x = a + b > kMsEps ? b / (a + b) : 0.5f;
+  f.eta_rel = eta_rel;
+  f.one_minus_e_avg_t = om_t;
+  f.ratio_r = clampf(1.0f - x * (1.0f - f_avg_o), 0.0f, 1.0f);
+  f.trans_ss = clampf(e_avg_o, 0.0f, 1.0f);
+  f.trans_ms = std::fmax(1.0f - e_avg_o, 0.0f) * clampf(1.0f - f.ratio_r, 0.0f, 1.0f);
+  f.trans_total = std::fmax(f.trans_ss + f.trans_ms, 1.0e-8f);
+  f.eta_rel_axis = axis_lerp(dec_eta_to_axis(eta_rel), 32);
   f.eta_o = eta_o;
   f.one_minus_e_avg_o = om_o;
   f.ms_factor = factor;
@@ -191,11 +204,9 @@ float radical_inverse_base3(uint32_t n) {
 }  // namespace
 
 std::string openpbr_unsupported(const tpt_openpbr_desc& m) {
-  if (m.transmission_weight > 0.0f) return "transmission_weight > 0 (specular transmission is not on the device path)";
   if (m.thin_film_weight > 0.0f) return "thin_film_weight > 0 (thin film is not on the device path)";
   if (m.emission_luminance > 0.0f) return "emission_luminance > 0 (OpenPBR emission is not on the device path)";
   if (m.geometry_opacity < 1.0f) return "geometry_opacity < 1 (alpha testing is not on the device path)";
-  if (m.geometry_thin_walled) return "geometry_thin_walled (thin-walled surfaces are not on the device path)";
   return "";
 }
 
@@ -321,6 +332,26 @@ void lower_openpbr(const tpt_openpbr_desc& m, const float* spec_da, const float*
     d.fres[1] = DevFresnelFace{1.0f / eta_ph, 1.0f / eta_pr, 1.0f / std::fmax(a, 1.0e-4f), 1.0f / std::fmax(bb, 1.0e-4f)};
   }
   d.coat_clamped = clampf(coat_w, 0.0f, 1.0f);
+
+  // specular transmission (make_bsdf: transmission alphas = specular alphas,
+  // transmission_eta = specular_eta; open_pbr.rs:553-564 thin-wall alphas)
+  const float trans = clampf(m.transmission_weight, 0.0f, 1.0f);
+  d.transmission = trans;
+  put(d.trans_color, clamp01(f3(m.transmission_color)));
+  d.trans_eta = spec_eta;
+  d.teta_rel[0] = 1.0f / spec_eta;
+  d.teta_rel[1] = spec_eta;
+  {
+    const float eta = std::fmax(spec_eta, 1.0f);
+    // powi(eta, 3) expands as eta * (eta * eta), as the oracle's powi does
+    const float scale = std::sqrt(std::fmax(3.7f * (eta - 1.0f) * sq(eta - 0.5f) / (eta * (eta * eta)), 0.0f));
+    const float s2 = scale * scale;
+    d.tw_ax = clampf(sax * s2, kMinAlpha, 1.0f);
+    d.tw_ay = clampf(say * s2, kMinAlpha, 1.0f);
+  }
+  if (trans > 0.0f) flags |= kOpbrTrans;
+  if (!(trans <= 0.0f || spec_alpha_smooth)) flags |= kOpbrTransRough;
+  if (m.geometry_thin_walled) flags |= kOpbrThinWalled;
 
   // coat darkening without the view term (material/open_pbr.rs:823-858)
   const float delta = clampf(m.coat_darkening, 0.0f, 1.0f);

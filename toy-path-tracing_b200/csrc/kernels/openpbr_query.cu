@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(const __grid_con
   if (mode == 1) {  // importance transport: layer weights at wi
     opbr::OpbrVertex lay;
     opbr::init_vertex(lay, m, rd.cec_e, rd.dec_e, w, front[i] != 0, fabsf(o.z));
-    opbr::eval_pdf(s, lay, w, fv, p);
+    opbr::eval_pdf(s, lay, w, fv, p, true, true);
   } else {
     opbr::eval_pdf(s, s, w, fv, p);
   }

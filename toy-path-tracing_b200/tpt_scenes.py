@@ -201,6 +201,22 @@ def cornell_box(seed: int = 1, material: int = OPENPBR, light_strength: float = 
             "angles": (float(a1), float(a2)), "seed": seed}
 
 
+def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPENPBR):
+    """The Cornell box with transmissive boxes: the tall box rough (specular
+    roughness 0.25) and the short box smooth, both fully transmissive OpenPBR
+    (the short one tinted); thin_walled makes both thin-walled sheets.  The
+    walls keep their diffuse materials (OpenPBR, or NormalizedLambert)."""
+    sc = cornell_box(seed, material)
+    thin = 1 if thin_walled else 0
+    sc["materials"][5] = {"kind": OPENPBR, "base_color": np.array([0.8, 0.8, 0.8], np.float32),
+                          "specular_roughness": 0.25, "transmission_weight": 1.0, "geometry_thin_walled": thin}
+    sc["materials"][6] = {"kind": OPENPBR, "base_color": np.array([0.6, 0.7, 0.5], np.float32),
+                          "specular_roughness": 0.0, "transmission_weight": 1.0,
+                          "transmission_color": np.array([0.9, 0.75, 0.6], np.float32),
+                          "geometry_thin_walled": thin}
+    return sc
+
+
 def cornell_lights(seed: int = 1, material: int = LAMBERT, area: bool = True):
     """The Cornell box lit by a point light, a spot light and a directional
     light entering through the open front (plus the ceiling quad when `area`).
