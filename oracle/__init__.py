@@ -70,6 +70,7 @@ def _declare(L):
         "orc_sampler_camera": (None, [u32, u32, u32, u32, u32, u32, vp, vp]),
         "orc_sampler_values": (None, [u32, u32, u32, u64, vp, vp, vp, C.c_int]),
         "orc_brute_force_f64": (None, [vp, vp, u64, vp, u64, vp, vp, vp, C.c_int]),
+        "orc_thin_film": (None, [f32, f32, f32, vp, vp, f32, vp]),
         "orc_triangle_f64": (None, [vp, vp, vp, vp, u64, vp, vp, C.c_int]),
         "orc_zsobol_sample_index": (u64, [u32, u32, u32, u32, u32, u32, u32]),
         "orc_shuffled_scrambled_sobol": (None, [u32, u32, i32, vp]),
@@ -255,6 +256,22 @@ def triangle_f64(positions, indices, tri, rays, nthreads=None):
     t, mb = np.empty(n, np.float64), np.empty(n, np.float64)
     lib().orc_triangle_f64(_p(pos), _p(idx), _p(tr), _p(r), n, _p(t), _p(mb), nthreads or os.cpu_count() or 1)
     return t, mb
+
+
+def thin_film_dielectric(cos_i, eta_outside, eta_film, eta_base, thickness_nm):
+    """eval_thin_film_dielectric (bsdf/thin_film.rs:11-25)."""
+    out = np.zeros(3, np.float32)
+    lib().orc_thin_film(float(cos_i), float(eta_outside), float(eta_film), _p(_v3([eta_base] * 3)),
+                        _p(_v3([0, 0, 0])), float(thickness_nm), _p(out))
+    return out
+
+
+def thin_film_conductor(cos_i, eta_outside, eta_film, n, k, thickness_nm):
+    """eval_thin_film_conductor (bsdf/thin_film.rs:27-45)."""
+    out = np.zeros(3, np.float32)
+    lib().orc_thin_film(float(cos_i), float(eta_outside), float(eta_film), _p(_v3(n)), _p(_v3(k)),
+                        float(thickness_nm), _p(out))
+    return out
 
 
 def sampler_values(width, height, spp, queries, nthreads=None):
@@ -507,7 +524,9 @@ OPENPBR_PARAM_FIELDS = [
     ("coat_color", 3), ("coat_darkening", 3), ("coat_alpha_x", 1), ("coat_alpha_y", 1), ("coat_eta", 1),
     ("fuzz", 1), ("fuzz_color", 3), ("fuzz_roughness", 1), ("transmission", 1), ("transmission_color", 3),
     ("transmission_alpha_x", 1), ("transmission_alpha_y", 1),
-    ("diffuse_roughness", 1), ("subsurface", 1), ("subsurface_color", 3), ("thin_walled", 1), ("front_face", 1),
+    ("diffuse_roughness", 1), ("subsurface", 1), ("subsurface_color", 3), ("thin_walled", 1),
+    ("thin_film_weight", 1), ("thin_film_thickness", 1), ("thin_film_ior", 1), ("metal_n", 3), ("metal_k", 3),
+    ("front_face", 1),
 ]
 
 
@@ -526,6 +545,11 @@ def pack_openpbr_params(p: dict) -> np.ndarray:
     p.setdefault("transmission_alpha_x", p["specular_alpha_x"])
     p.setdefault("transmission_alpha_y", p["specular_alpha_y"])
     p.setdefault("thin_walled", 0.0)
+    p.setdefault("thin_film_weight", 0.0)
+    p.setdefault("thin_film_thickness", 0.0)
+    p.setdefault("thin_film_ior", 1.5)
+    p.setdefault("metal_n", 0.0)
+    p.setdefault("metal_k", 0.0)
     out = []
     for name, k in OPENPBR_PARAM_FIELDS:
         v = p[name]

@@ -46,6 +46,11 @@ OpenPbrParams params_from_flat(const float* f) {
   p.subsurface = f[i++];
   p.subsurface_color = v3();
   p.thin_walled = f[i++] != 0.0f;
+  p.thin_film_weight = f[i++];
+  p.thin_film_thickness = f[i++];
+  p.thin_film_ior = f[i++];
+  p.metal_n = v3();
+  p.metal_k = v3();
   p.front_face = f[i++] != 0.0f;
   return p;
 }

@@ -452,7 +452,22 @@ struct Impl {
     if (denom <= 0.0f) return w.ms * pdf_ms / w.total;
     return (w.ss * (pdf_wm / denom) + w.ms * pdf_ms) / w.total;
   }
-  Vec3 metal_fresnel(float c) const {  // metal_f82_tint_fresnel (no thin film)
+  bool film() const { return p.thin_film_weight > 0.0f && p.thin_film_thickness > 0.0f; }
+  // metal_fresnel (open_pbr.rs:761-790): F82 tint, blended with the filmed
+  // conductor reflectance (over the coat's eta where there is a coat)
+  Vec3 metal_fresnel(float c) const {
+    Vec3 no_film = metal_f82(c);
+    float w = clampf(p.thin_film_weight, 0.0f, 1.0f);
+    if (!(w > 0.0f && p.thin_film_thickness > 0.0f)) return no_film;
+    Vec3 unc = thin_film_conductor(c, 1.0f, p.thin_film_ior, p.metal_n, p.metal_k, p.thin_film_thickness);
+    Vec3 f = unc;
+    if (p.coat > 0.0f) {
+      Vec3 coated = thin_film_conductor(c, p.coat_eta, p.thin_film_ior, p.metal_n, p.metal_k, p.thin_film_thickness);
+      f = lerp3(unc, coated, clampf(p.coat, 0.0f, 1.0f));
+    }
+    return lerp3(no_film, f, w);
+  }
+  Vec3 metal_f82(float c) const {  // metal_f82_tint_fresnel (open_pbr.rs:792-802)
     Vec3 f0 = vmax(p.base * p.base_color, Vec3(0, 0, 0));
     Vec3 fs = schlick3(f0, c);
     Vec3 fs82 = schlick3_82(f0);
@@ -461,7 +476,18 @@ struct Impl {
     float corr = cc * powi(1.0f - cc, 6) / fmax_num(cos82_denom(), 1.0e-8f);
     return vclamp01(p.specular * (fs - corr * (fs82 - ft82)));
   }
+  // metal_fresnel_avg (open_pbr.rs:818-830): the closed form without film,
+  // else a 16-point cosine-weighted average of the filmed Fresnel
   Vec3 metal_fresnel_avg() const {
+    if (!film()) return metal_f82_avg();
+    Vec3 sum(0, 0, 0);
+    for (int i = 0; i < 16; ++i) {
+      float mu = ((float)i + 0.5f) / 16.0f;
+      sum += metal_fresnel(mu) * (2.0f * mu);
+    }
+    return sum / 16.0f;
+  }
+  Vec3 metal_f82_avg() const {
     Vec3 f0 = vmax(p.base * p.base_color, Vec3(0, 0, 0));
     Vec3 fs82 = schlick3_82(f0);
     Vec3 ft82 = vclamp01(p.specular_color) * fs82;
@@ -505,7 +531,28 @@ struct Impl {
                        : weighted_fresnel_ratio(c, 1.0f / fmax_num(a, 1.0e-4f), 1.0f / fmax_num(b, 1.0e-4f));
     return lerp(unc, coated, coat);
   }
-  Vec3 spec_fresnel(float c) const { return Vec3::splat(base_dielectric_fresnel(c, p.transmission_eta, p.specular_eta)); }
+  // spec_brdf_fresnel (open_pbr.rs:869-898) and spec_btdf_fresnel_with_eta
+  // (1120-1152, film only off thin-walled surfaces): the dielectric Fresnel,
+  // blended with the filmed reflectance (over the coat's eta where coated)
+  Vec3 filmed_dielectric(Vec3 no_film, float c, float eta_base) const {
+    float w = clampf(p.thin_film_weight, 0.0f, 1.0f);
+    if (!(w > 0.0f && p.thin_film_thickness > 0.0f)) return no_film;
+    Vec3 unc = thin_film_dielectric(c, 1.0f, p.thin_film_ior, eta_base, p.thin_film_thickness);
+    Vec3 f = unc;
+    if (p.coat > 0.0f) {
+      Vec3 coated = thin_film_dielectric(c, p.coat_eta, p.thin_film_ior, eta_base, p.thin_film_thickness);
+      f = lerp3(unc, coated, clampf(p.coat, 0.0f, 1.0f));
+    }
+    return lerp3(no_film, f, w);
+  }
+  Vec3 spec_fresnel(float c) const {
+    return filmed_dielectric(Vec3::splat(base_dielectric_fresnel(c, p.transmission_eta, p.specular_eta)), c,
+                             p.specular_eta);
+  }
+  Vec3 btdf_fresnel(float c) const {
+    Vec3 no_film = Vec3::splat(base_dielectric_fresnel(c, p.transmission_eta, p.specular_eta));
+    return p.thin_walled ? no_film : filmed_dielectric(no_film, c, p.specular_eta);
+  }
   Vec3 eval_spec_brdf(Vec3 wo, Vec3 wi) const {
     if (wo.z <= 0.0f || wi.z <= 0.0f) return Vec3(0, 0, 0);
     Vec3 wm;
@@ -557,8 +604,13 @@ struct Impl {
     float cos_i = fmax_num(std::sqrt(1.0f - sin2_i), 1.0e-4f);
     Vec3 f_o = vclamp01(spec_fresnel(cos_o));
     // thin_wall_internal_fresnel (open_pbr.rs:961-979)
-    Vec3 f_i = vclamp01(Vec3::splat(
-        weighted_fresnel_ratio(cos_i, 1.0f / fmax_num(eta, 1.0e-4f), 1.0f / fmax_num(eta_prime, 1.0e-4f))));
+    Vec3 f_i = Vec3::splat(
+        weighted_fresnel_ratio(cos_i, 1.0f / fmax_num(eta, 1.0e-4f), 1.0f / fmax_num(eta_prime, 1.0e-4f)));
+    float w = clampf(p.thin_film_weight, 0.0f, 1.0f);
+    if (w > 0.0f && p.thin_film_thickness > 0.0f)
+      f_i = lerp3(f_i, thin_film_dielectric(cos_i, fmax_num(eta, 1.0e-4f), p.thin_film_ior, 1.0f, p.thin_film_thickness),
+                  w);
+    f_i = vclamp01(f_i);
     Vec3 a = vpowf(vclamp01(p.transmission_color), 1.0f / cos_i);
     Vec3 a2 = a * a;
     Vec3 f_i2_a2 = a2 * f_i * f_i;
@@ -625,7 +677,7 @@ struct Impl {
     if (wo.z <= 0.0f || wi.z >= 0.0f) return Vec3(0, 0, 0);
     float scalar, co;
     if (!btdf_scalar(wo, wi, eta_rel_t(), mode, &scalar, &co)) return Vec3(0, 0, 0);
-    Vec3 f = Vec3::splat(base_dielectric_fresnel(co, p.transmission_eta, p.specular_eta));
+    Vec3 f = btdf_fresnel(co);
     Vec3 ss = vmax(Vec3(1, 1, 1) - f, Vec3(0, 0, 0)) * scalar;
     Vec3 ms = Vec3::splat(eval_trans_ms(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y, p.specular_eta, mode));
     return ss + ms;
@@ -984,7 +1036,6 @@ float openpbr_specular_eta(const OpenPbrDesc& m) {
 }
 
 const char* openpbr_unsupported(const OpenPbrDesc& m) {
-  if (m.thin_film_weight > 0.0f) return "thin_film_weight > 0";
   if (m.emission_luminance > 0.0f) return "emission_luminance > 0";
   if (m.geometry_opacity < 1.0f) return "geometry_opacity < 1";
   return "";
@@ -1062,6 +1113,11 @@ OpenPbrParams make_openpbr_params(const OpenPbrDesc& m, bool front_face, Vec3 wo
   p.transmission_alpha_x = p.specular_alpha_x;
   p.transmission_alpha_y = p.specular_alpha_y;
   p.thin_walled = m.geometry_thin_walled != 0;
+  // thin film (make_bsdf, thin_film_thickness_nm_at: micrometres to nm)
+  p.thin_film_weight = clampf(m.thin_film_weight, 0.0f, 1.0f);
+  p.thin_film_thickness = m.thin_film_weight <= 0.0f ? 0.0f : fmax_num(m.thin_film_thickness, 0.0f) * 1000.0f;
+  p.thin_film_ior = fmax_num(m.thin_film_ior, 1.0e-4f);
+  artist_friendly_complex_ior(vclamp01(base_color), vclamp01(spec_color), &p.metal_n, &p.metal_k);
   p.diffuse_roughness = clampf(m.base_diffuse_roughness, 0.0f, 1.0f);
   p.subsurface = 0.0f;
   p.subsurface_color = vclamp01(Vec3(m.subsurface_color[0], m.subsurface_color[1], m.subsurface_color[2]));

@@ -9,10 +9,11 @@
 // multiple scattering, rough and smooth), thin-walled surfaces (the two-interface
 // slab of thin_wall_coefficients, the thin-wall BTDF and the diffuse BTDF),
 // coat, fuzz (LTC), with optional anisotropy and smooth (delta) lobes.  Not
-// covered: thin film, dispersion (transmission_dispersion_scale is not part of
-// the untextured parameter set here, so dispersion is always off), emission,
+// covered: dispersion (transmission_dispersion_scale is not part of the
+// untextured parameter set here, so dispersion is always off), emission,
 // opacity and textures; the material lowering rejects parameters that would
-// need them.
+// need them.  Thin film (bsdf/thin_film.rs) modulates the specular, metal and
+// transmission Fresnel terms.
 #pragma once
 #include "common.h"
 
@@ -126,8 +127,15 @@ struct OpenPbrParams {
   float subsurface;
   Vec3 subsurface_color;
   bool thin_walled;
+  float thin_film_weight, thin_film_thickness, thin_film_ior;  // thickness in nm
+  Vec3 metal_n, metal_k;                                       // artist_friendly_complex_ior
   bool front_face;
 };
+
+// bsdf/thin_film.rs:11-45 and bsdf/conductor_complex.rs:132-147
+Vec3 thin_film_dielectric(float cos_i, float eta_outside, float eta_film, float eta_base, float thickness_nm);
+Vec3 thin_film_conductor(float cos_i, float eta_outside, float eta_film, Vec3 n, Vec3 k, float thickness_nm);
+void artist_friendly_complex_ior(Vec3 face, Vec3 edge, Vec3* n, Vec3* k);
 
 struct OpenPbrLuts {
   const DielectricAlbedoLut* spec;

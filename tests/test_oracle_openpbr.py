@@ -246,11 +246,55 @@ def test_material_sample_consistent_with_eval_and_pdf(mi):
 
 
 def test_unsupported_parameters_are_rejected():
-    for bad in ({"thin_film_weight": 1.0}, {"emission_luminance": 2.0}, {"geometry_opacity": 0.5}):
+    for bad in ({"emission_luminance": 2.0}, {"geometry_opacity": 0.5}):
         with pytest.raises(ValueError):
             orc.OpenPbrMaterial(bad)
     orc.OpenPbrMaterial({"transmission_weight": 0.5})
     orc.OpenPbrMaterial({"geometry_thin_walled": 1})
+    orc.OpenPbrMaterial({"thin_film_weight": 1.0})
+
+
+# ---- thin film (bsdf/thin_film.rs:264-297) ----------------------------------------
+def test_thin_film_zero_thickness_returns_finite_rgb():
+    f = orc.thin_film_dielectric(0.7, 1.0, 1.5, 1.5, 0.0)
+    assert np.all(np.isfinite(f)) and np.all(f >= 0)
+
+
+def test_thin_film_dielectric_changes_response_with_thickness():
+    f0 = orc.thin_film_dielectric(0.85, 1.0, 2.4, 1.5, 0.0)
+    f250 = orc.thin_film_dielectric(0.85, 1.0, 2.4, 1.5, 250.0)
+    f500 = orc.thin_film_dielectric(0.85, 1.0, 2.4, 1.5, 500.0)
+    assert np.abs(f0 - f250).max() > 1e-3 or np.abs(f250 - f500).max() > 1e-3
+
+
+def test_thin_film_conductor_returns_finite_rgb():
+    f = orc.thin_film_conductor(0.7, 1.0, 2.0, [0.18, 0.42, 1.37], [3.42, 2.35, 1.77], 300.0)
+    assert np.all(np.isfinite(f)) and np.all((f >= 0) & (f <= 1))
+
+
+def test_thin_film_materials_sample_consistently():
+    """Filmed dielectric, metal, coated and thin-walled materials: sample
+    weight = f |cos| / pdf and pdf = the pdf query (finalize_rough_sample)."""
+    for m in ({"specular_roughness": 0.3, "thin_film_weight": 1.0, "thin_film_thickness": 0.4},
+              {"base_metalness": 1.0, "specular_roughness": 0.35, "thin_film_weight": 0.7, "thin_film_ior": 1.8},
+              {"specular_roughness": 0.4, "coat_weight": 0.6, "coat_roughness": 0.2, "thin_film_weight": 1.0},
+              {"specular_roughness": 0.3, "transmission_weight": 0.8, "geometry_thin_walled": 1,
+               "thin_film_weight": 0.8, "thin_film_thickness": 0.3}):
+        mat = orc.OpenPbrMaterial(m)
+        rng = np.random.default_rng(7)
+        n_ok = 0
+        for _ in range(150):
+            wo = unit(rng.normal(size=3) * [1, 1, 0.3] + [0, 0, 1.0])
+            u = rng.random(3).astype(np.float32)
+            s = mat.sample(wo, u[0], (u[1], u[2]))
+            if s is None or s["flags"] & 16:
+                continue
+            n_ok += 1
+            f = mat.eval(wo, s["wi"])
+            pdf = mat.pdf(wo, s["wi"])
+            assert abs(pdf - s["pdf"]) <= 1e-5 * max(pdf, 1.0)
+            np.testing.assert_allclose(s["weight"], f * (abs(s["wi"][2]) / pdf), rtol=1e-4, atol=1e-7)
+        assert n_ok > 80
 
 
 # ---- transmission (bsdf/open_pbr.rs:2561-2643) ----------------------------------

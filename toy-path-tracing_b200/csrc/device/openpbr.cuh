@@ -13,6 +13,7 @@
 // library is compiled with -fmad=false).
 #pragma once
 #include "render_types.h"
+#include "thin_film.h"
 #include "vmath.cuh"
 
 namespace tpt {
@@ -487,6 +488,23 @@ __device__ __forceinline__ float spec_fresnel(const DevOpenPbr& m, uint32_t face
   return unc + (coated - unc) * m.coat_clamped;
 }
 
+__device__ __forceinline__ V3 from_film(film::F3 a) { return V3{a.x, a.y, a.z}; }
+// A dielectric Fresnel blended with the thin film's reflectance over a base
+// of eta `eta_base` (over the coat's eta where coated): spec_brdf_fresnel
+// (open_pbr.rs:869-898) and spec_btdf_fresnel_with_eta (1120-1152).
+__device__ __forceinline__ V3 filmed_dielectric(const DevOpenPbr& m, V3 no_film, float c, float eta_base) {
+  film::F3 f = film::film_dielectric(c, 1.0f, m.film_ior, eta_base, m.film_thick);
+  if (m.coat > 0.0f)
+    f = film::lerp3(f, film::film_dielectric(c, m.coat_eta, m.film_ior, eta_base, m.film_thick),
+                    clampf(m.coat, 0.0f, 1.0f));
+  return no_film + (from_film(f) - no_film) * m.film_w;
+}
+// spec_brdf_fresnel: per channel once a film is present
+__device__ __forceinline__ V3 spec_fresnel3(const DevOpenPbr& m, uint32_t face, float c) {
+  const V3 no_film = splat(spec_fresnel(m, face, c));
+  return (m.flags & kOpbrFilm) ? filmed_dielectric(m, no_film, c, m.trans_eta) : no_film;
+}
+
 // thin_wall_coefficients (open_pbr.rs:931-959, thin_wall_internal_fresnel
 // 961-979) without thin film: reflectance and transmittance of the slab.
 __device__ __forceinline__ void thin_wall_coeffs(const DevOpenPbr& m, uint32_t face, float cos_theta_o, V3& r_out,
@@ -498,8 +516,12 @@ __device__ __forceinline__ void thin_wall_coeffs(const DevOpenPbr& m, uint32_t f
   const float sin2_o = fmaxf(1.0f - cos_o * cos_o, 0.0f);
   const float sin2_i = clampf(sin2_o / (eta * eta), 0.0f, 1.0f);
   const float cos_i = fmaxf(sqrtf(1.0f - sin2_i), 1.0e-4f);
-  const V3 f_o = clamp01(splat(spec_fresnel(m, face, cos_o)));
-  const V3 f_i = clamp01(splat(weighted_fresnel_ratio(cos_i, 1.0f / fmaxf(eta, 1.0e-4f), 1.0f / fmaxf(eta_prime, 1.0e-4f))));
+  const V3 f_o = clamp01(spec_fresnel3(m, face, cos_o));
+  V3 f_i = splat(weighted_fresnel_ratio(cos_i, 1.0f / fmaxf(eta, 1.0e-4f), 1.0f / fmaxf(eta_prime, 1.0e-4f)));
+  if (m.flags & kOpbrFilm)
+    f_i = f_i + (from_film(film::film_dielectric(cos_i, fmaxf(eta, 1.0e-4f), m.film_ior, 1.0f, m.film_thick)) - f_i) *
+                    m.film_w;
+  f_i = clamp01(f_i);
   const float e = 1.0f / cos_i;
   const V3 tc = clamp01(ld3(m.trans_color));
   const V3 a = V3{powf(tc.x, e), powf(tc.y, e), powf(tc.z, e)};
@@ -572,13 +594,22 @@ static __device__ __noinline__ void init_vertex(OpbrVertex& s, const DevOpenPbr*
   s.q_total = s.q_coat + s.q_metal + s.q_spec + s.q_btdf + s.q_fuzz + s.q_diff;
 }
 
+// metal_fresnel (open_pbr.rs:761-802): F82 tint, blended with the filmed
+// conductor's reflectance when the material has a thin film
 __device__ __forceinline__ V3 metal_fresnel(const DevOpenPbr& m, float c) {
   const V3 f0 = ld3(m.f0);
   const float om = 1.0f - clampf(c, 0.0f, 1.0f);
   const V3 fs = f0 + (V3{1.0f, 1.0f, 1.0f} - f0) * powi5(om);
   const float cc = clampf(c, 0.0f, 1.0f);
   const float corr = cc * powi6(1.0f - cc) / m.f82_denom;
-  return clamp01(m.specular * (fs - corr * ld3(m.f82_delta)));
+  const V3 no_film = clamp01(m.specular * (fs - corr * ld3(m.f82_delta)));
+  if (!(m.flags & kOpbrFilm)) return no_film;
+  const film::F3 n = film::F3{m.metal_n[0], m.metal_n[1], m.metal_n[2]};
+  const film::F3 k = film::F3{m.metal_k[0], m.metal_k[1], m.metal_k[2]};
+  film::F3 f = film::film_conductor(c, 1.0f, m.film_ior, n, k, m.film_thick);
+  if (m.coat > 0.0f)
+    f = film::lerp3(f, film::film_conductor(c, m.coat_eta, m.film_ior, n, k, m.film_thick), clampf(m.coat, 0.0f, 1.0f));
+  return no_film + (from_film(f) - no_film) * m.film_w;
 }
 __device__ __forceinline__ float refl_ms(const OpbrVertex& s, int lobe, float wi_z) {
   const DevMsFace& f = s.m->ms[lobe][s.face];
@@ -598,11 +629,11 @@ __device__ __forceinline__ V3 coat_tint(const DevOpenPbr& m, V3 wo, V3 wi) {
 // The specular BTDF and its pdf for wi below the surface (eval_spec_btdf,
 // eval_thin_wall_spec_btdf, pdf_specular_btdf, open_pbr.rs:1024-1222, without
 // dispersion); `importance` selects the transport mode's eta^2 scaling.
-__device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool importance, float& f, float& pdf,
+__device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool importance, V3& f, float& pdf,
                                               V3& f_thin) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
-  f = 0.0f;
+  f = V3{0.0f, 0.0f, 0.0f};
   pdf = 0.0f;
   f_thin = V3{0.0f, 0.0f, 0.0f};
   if (!(m.flags & kOpbrTransRough)) return;  // spec_btdf_is_smooth: neither term
@@ -638,7 +669,8 @@ __device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool i
         const float denom = den * den * fabsf(wo.z) * fabsf(wi.z);
         if (!(denom <= 0.0f)) {
           const float scalar = sc * scale / denom;
-          const float fr = spec_fresnel(m, s.face, co);
+          const V3 no_film = splat(spec_fresnel(m, s.face, co));
+          const V3 fr = (m.flags & kOpbrFilm) ? filmed_dielectric(m, no_film, co, m.trans_eta) : no_film;
           // eval_dielectric_transmission_ms (open_pbr.rs:672-696)
           const float e_o = s.dec_eo[0];
           DevMsFace ft = fm;
@@ -647,7 +679,7 @@ __device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool i
           const float ms_scale = importance ? 1.0f : 1.0f / (fm.eta_rel * fm.eta_rel);
           const float ms = (1.0f - fm.ratio_r) * (1.0f - e_o) * (1.0f - e_i) * ms_scale /
                            (kPiF * fm.one_minus_e_avg_t);
-          f = fmaxf(1.0f - fr, 0.0f) * scalar + ms;
+          f = vmaxv(V3{1.0f, 1.0f, 1.0f} - fr, V3{0.0f, 0.0f, 0.0f}) * scalar + splat(ms);
         }
       }
       const float pdf_wm = pdf_wm_vndf(wo, wm, m.spec_ax, m.spec_ay);
@@ -677,11 +709,11 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVert
     // the coat tint of a direction below the coat is one
     if (!(m.flags & kOpbrTrans)) return;
     const Below b = weights_below(lay, V3{1.0f, 1.0f, 1.0f});
-    float fb, pb;
-    V3 f_thin;
+    V3 fb, f_thin;
+    float pb;
     btdf_eval_pdf(s, wi, importance, fb, pb, f_thin);
     if (length_sq(b.btdf) > 0.0f && (m.flags & kOpbrTransRough))
-      f_out = (m.flags & kOpbrThinWalled) ? b.btdf * f_thin : b.btdf * splat(fb);
+      f_out = (m.flags & kOpbrThinWalled) ? b.btdf * f_thin : b.btdf * fb;
     if (want_pdf && s.q_total > 0.0f && s.q_btdf > 0.0f && (m.flags & kOpbrTransRough))
       pdf_out = (s.q_btdf / s.q_total) * pb;
     return;
@@ -730,8 +762,7 @@ static __device__ __noinline__ void eval_pdf(const OpbrVertex& s, const OpbrVert
     if (m.flags & kOpbrThinWalled) {
       total = total + b.spec * (s.tw_r * (d_s * g_s / inv4));
     } else {
-      const float fr = spec_fresnel(m, s.face, fabsf(dot(wo, wm)));
-      const V3 ss = splat(fr) * (d_s * g_s / inv4);
+      const V3 ss = spec_fresnel3(m, s.face, fabsf(dot(wo, wm))) * (d_s * g_s / inv4);
       total = total + b.spec * (ss + splat(refl_ms(s, 0, wi.z)));
     }
   }
@@ -830,8 +861,8 @@ static __device__ __noinline__ bool sample_btdf(const OpbrVertex& s, float p_lob
     if (wr.z <= 0.0f) return false;
     const V3 wi = V3{wr.x, wr.y, -wr.z};
     const V3 bw = weights_below(s, one).btdf;
-    float fb, pb;
-    V3 f_thin;
+    V3 fb, f_thin;
+    float pb;
     btdf_eval_pdf(s, wi, importance, fb, pb, f_thin);
     const float pdf_total = p_lobe * pb;
     if (pdf_total <= 0.0f) return false;
@@ -930,7 +961,7 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
     } else {
       const Below b = weights_below(s, tint);
       // a thin-walled sheet reflects its slab reflectance (open_pbr.rs:1596-1602)
-      const V3 fs = (m.flags & kOpbrThinWalled) ? s.tw_r : splat(spec_fresnel(m, s.face, fabsf(wi.z)));
+      const V3 fs = (m.flags & kOpbrThinWalled) ? s.tw_r : spec_fresnel3(m, s.face, fabsf(wi.z));
       out.weight = lobe == 1 ? (b.metal * metal_fresnel(m, fabsf(wi.z))) / p_lobe : (b.spec * fs) / p_lobe;
     }
     out.wi = wi;

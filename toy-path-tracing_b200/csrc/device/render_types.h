@@ -66,6 +66,7 @@ enum : uint32_t {
   kOpbrTrans = 64u,         // transmission > 0
   kOpbrTransRough = 128u,   // transmission > 0 and not smooth (spec_btdf_is_smooth false)
   kOpbrThinWalled = 256u,   // geometry_thin_walled
+  kOpbrFilm = 512u,         // thin film: weight > 0 and thickness > 0
 };
 struct alignas(16) DevOpenPbr {
   float base_color[3], base;
@@ -99,6 +100,11 @@ struct alignas(16) DevOpenPbr {
   float transmission;
   float trans_color[3], tw_ax;
   float tw_ay, trans_eta, teta_rel[2];
+  // thin film (bsdf/thin_film.rs): weight, thickness in nm, film IOR, and the
+  // metal base's complex IOR (artist_friendly_complex_ior)
+  float film_w, film_thick, film_ior, pad_f;
+  float metal_n[3], metal_k[3];
+  uint32_t pad2[2];
 };
 
 struct alignas(16) DevShadeInstance {

@@ -4,6 +4,8 @@
 // -ffp-contract=off so every f32 operation rounds as in the reference.
 #include "openpbr_lower.h"
 
+#include "../device/thin_film.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -204,7 +206,6 @@ float radical_inverse_base3(uint32_t n) {
 }  // namespace
 
 std::string openpbr_unsupported(const tpt_openpbr_desc& m) {
-  if (m.thin_film_weight > 0.0f) return "thin_film_weight > 0 (thin film is not on the device path)";
   if (m.emission_luminance > 0.0f) return "emission_luminance > 0 (OpenPBR emission is not on the device path)";
   if (m.geometry_opacity < 1.0f) return "geometry_opacity < 1 (alpha testing is not on the device path)";
   return "";
@@ -304,7 +305,40 @@ void lower_openpbr(const tpt_openpbr_desc& m, const float* spec_da, const float*
   const float e_avg_ms = cec_lookup_e_avg(cec_e_avg, cond_req);  // eval_metal_ms reads it unclamped
   d.cond_one_minus_e_avg = std::fmax(1.0f - e_avg_ms, kMsEps);
   const F3 b = (fs82 - ft82) / f82_denom;
-  const F3 f_avg = clamp01(specular * (f0 + (splat(1.0f) - f0) / 21.0f - b / 126.0f));
+  F3 f_avg = clamp01(specular * (f0 + (splat(1.0f) - f0) / 21.0f - b / 126.0f));
+  // thin film (make_bsdf: thickness in nm; artist_friendly_complex_ior of the
+  // clamped base and specular colours for the filmed metal)
+  const float film_w = clampf(m.thin_film_weight, 0.0f, 1.0f);
+  const float film_thick = m.thin_film_weight <= 0.0f ? 0.0f : std::fmax(m.thin_film_thickness, 0.0f) * 1000.0f;
+  const float film_ior = std::fmax(m.thin_film_ior, 1.0e-4f);
+  film::F3 mn, mk;
+  film::complex_ior(film::F3{clamp01(base_color).x, clamp01(base_color).y, clamp01(base_color).z},
+                    film::F3{spec_color.x, spec_color.y, spec_color.z}, &mn, &mk);
+  const bool has_film = film_w > 0.0f && film_thick > 0.0f;
+  if (has_film) {
+    // metal_fresnel_avg (open_pbr.rs:818-830): a 16-point average of the
+    // filmed metal Fresnel (metal_fresnel, 761-790)
+    auto filmed_metal = [&](float c) {
+      const float om = 1.0f - clampf(c, 0.0f, 1.0f);
+      const float om2 = om * om;
+      const F3 fs = f0 + (splat(1.0f) - f0) * (om * (om2 * om2));
+      const float cc = clampf(c, 0.0f, 1.0f);
+      const float omc = 1.0f - cc, omc2 = omc * omc;
+      const float corr = cc * (omc2 * (omc2 * omc2)) / f82_denom;
+      const F3 no_film = clamp01(specular * (fs - corr * (fs82 - ft82)));
+      film::F3 fl = film::film_conductor(c, 1.0f, film_ior, mn, mk, film_thick);
+      if (coat_w > 0.0f)
+        fl = film::lerp3(fl, film::film_conductor(c, coat_eta, film_ior, mn, mk, film_thick), clampf(coat_w, 0.0f, 1.0f));
+      const F3 f = F3{fl.x, fl.y, fl.z};
+      return no_film + (f - no_film) * film_w;
+    };
+    F3 sum = splat(0.0f);
+    for (int i = 0; i < 16; ++i) {
+      const float mu = ((float)i + 0.5f) / 16.0f;
+      sum = sum + filmed_metal(mu) * (2.0f * mu);
+    }
+    f_avg = sum / 16.0f;
+  }
   {  // compute_conductor_f_ms (open_pbr.rs:2193-2203)
     float om = std::fmax(1.0f - e_avg_ms, 0.0f);
     F3 denom = splat(1.0f) - f_avg * om;
@@ -352,6 +386,12 @@ void lower_openpbr(const tpt_openpbr_desc& m, const float* spec_da, const float*
   if (trans > 0.0f) flags |= kOpbrTrans;
   if (!(trans <= 0.0f || spec_alpha_smooth)) flags |= kOpbrTransRough;
   if (m.geometry_thin_walled) flags |= kOpbrThinWalled;
+  if (has_film) flags |= kOpbrFilm;
+  d.film_w = film_w;
+  d.film_thick = film_thick;
+  d.film_ior = film_ior;
+  d.metal_n[0] = mn.x; d.metal_n[1] = mn.y; d.metal_n[2] = mn.z;
+  d.metal_k[0] = mk.x; d.metal_k[1] = mk.y; d.metal_k[2] = mk.z;
 
   // coat darkening without the view term (material/open_pbr.rs:823-858)
   const float delta = clampf(m.coat_darkening, 0.0f, 1.0f);
