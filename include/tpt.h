@@ -460,24 +460,28 @@ tpt_status tpt_sampler_values_device(tpt_context* ctx, uint32_t width, uint32_t 
 
 /* Autotuner (no counterpart in the reference): times the candidate settings
  * on pilots of `jobs` (each job's rows scaled down: every candidate on at most
- * 2^24 paths, the candidates within 5 % of the best again on at most 2^26) and
- * applies the fastest to the context: the execution used
- * by jobs whose `execution` is TPT_EXEC_AUTO, and, when that is the wavefront,
- * its queue capacity (tpt_context_set_wavefront_capacity) and graph replay
- * (tpt_context_set_graphs).  Candidates: the megakernel, and the wavefront
- * (batched when n_jobs > 1) at capacities 2^18 .. 2^23, with and without graph
- * replay, at the context's shade block size (tpt_context_set_shade_block: a
- * scaled-down pilot does not predict it).  MIS jobs only.  Results do not
+ * 2^24 paths; the candidates within 5 % of the best, the default and the
+ * megakernel again on at most 2^26) and applies the fastest to the context:
+ * the execution used by jobs whose `execution` is TPT_EXEC_AUTO, and, when that
+ * is the wavefront, its queue capacity (tpt_context_set_wavefront_capacity),
+ * graph replay (tpt_context_set_graphs) and shade block size
+ * (tpt_context_set_shade_block).  Candidates: the megakernel, and the
+ * wavefront (batched when n_jobs > 1) at capacities 2^18 .. 2^23, with and
+ * without graph replay, at the context's shade block size; on the last pilot
+ * the best wavefront candidate also at the other block size.  Every time
+ * reported is from that last pilot.  MIS, NEE and PT jobs.  Results do not
  * depend on the settings. */
 typedef struct tpt_tune_result {
   uint32_t execution;          /* TPT_EXEC_WAVEFRONT or TPT_EXEC_MEGAKERNEL */
   uint32_t wavefront_capacity; /* path slots per chunk */
   uint32_t graphs;             /* 1: bounces replayed from captured graphs */
-  uint32_t shade_block;        /* threads per block of the wavefront shade stage (the context's) */
-  float ms;                    /* pilot time of the chosen settings */
-  float ms_megakernel;         /* first-pilot time of the megakernel */
-  float ms_wavefront_default;  /* pilot time of the wavefront at 2^22 slots with graphs */
+  uint32_t shade_block;        /* threads per block of the wavefront shade stage */
+  float ms;                    /* last-pilot time of the chosen settings */
+  float ms_megakernel;         /* last-pilot time of the megakernel */
+  float ms_wavefront_default;  /* last-pilot time of the wavefront at 2^22 slots, graphs, the context's block */
   uint64_t pilot_paths;        /* paths of the last pilot (about) */
+  uint32_t stage;              /* which pilot the times come from: 1 (at most 2^24 paths) or 2 (at most 2^26) */
+  uint32_t candidates;         /* settings timed */
 } tpt_tune_result;
 tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, tpt_tune_result* out);
 

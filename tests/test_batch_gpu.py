@@ -113,6 +113,8 @@ def test_autotune_applies_a_setting_that_renders_the_same(ctx, mixed):
         assert r["execution"] in (tpt.EXEC_WAVEFRONT, tpt.EXEC_MEGAKERNEL)
         assert r["ms"] > 0 and r["ms"] <= r["ms_megakernel"] * 1.0001
         assert r["pilot_paths"] == sum(j.width * j.height * j.spp for j in mixed)  # small: the whole workload
+        # every reported time is from the one (here: first) pilot, the other shade block included
+        assert r["stage"] == 1 and r["candidates"] >= 3 and r["shade_block"] in (128, 256)
         auto = [tpt.RenderJob(j.scene, j.camera, j.width, j.height, j.spp, j.max_depth, j.integrator, tpt.EXEC_AUTO)
                 for j in mixed]
         got = _render_each(ctx, auto)

@@ -7,15 +7,16 @@
 // job's scene, camera, spp and depth and scales its rows down (the same field
 // of view at a lower vertical resolution).  Stage 1 times every candidate on a
 // pilot of at most 2^24 paths (the whole workload when it is smaller); stage 2
-// re-times the candidates within 5 % of the best, and the default, on a pilot
-// four times larger, whose chunks look more like the full workload's.  Each
-// timing is one warm-up (graph capture, arena growth) and the median of three
-// runs, CUDA events on the context's stream.  A candidate replaces the default
-// wavefront settings (2^22 slots, graphs) only when it is more than 3 %
-// faster.  The shade stage's block size is the context's (256 by default):
-// pilots preferred 128-thread blocks by 1-4 % where the full 64-job workload ran
-// 13 % slower with them, so it is not a pilot decision.  Results do not depend
-// on any of the tuned settings (the tests check this), only the time does.
+// re-times the candidates within 5 % of the best, the default and the
+// megakernel on a pilot four times larger, whose chunks look more like the
+// full workload's.  On the last pilot the best wavefront candidate is also
+// timed with the other shade-stage block size (128 or 256 threads).  Every time
+// the result reports comes from that last pilot, so they compare directly.
+// Each timing is one warm-up (graph capture, arena growth) and the median of
+// three runs, CUDA events on the context's stream.  A candidate replaces the
+// default wavefront settings (2^22 slots, graphs, the context's block size)
+// only when it is more than 3 % faster.  Results do not depend on any of the
+// tuned settings (the tests check this), only the time does.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -132,23 +133,40 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     if (st) break;
     st = run(p1, c, &c.ms);
   }
-  free_pilot(p1);
-  const float ms_mk = cands[0].ms;  // stage-1 time of the megakernel
-  // stage 2: the candidates within 5 % of the best (and the default) on a
-  // pilot four times larger, closer to the full workload's chunk composition
+  uint32_t stage = 1;
+  Pilot* last = &p1;
+  Pilot p2;
+  // stage 2: the candidates within 5 % of the best, the default and the
+  // megakernel on a pilot four times larger, closer to the full workload's
+  // chunk composition
   if (!st && total > kPilotPaths) {
     float best1 = 1e30f;
     for (const Cand& c : cands) best1 = std::min(best1, c.ms);
-    Pilot p2;
     st = make_pilot(4 * kPilotPaths, p2);
     for (Cand& c : cands) {
       if (st) break;
       const bool is_default = c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs;
-      if (c.ms <= 1.05f * best1 || is_default) st = run(p2, c, &c.ms);
+      if (c.ms <= 1.05f * best1 || is_default || c.exec == TPT_EXEC_MEGAKERNEL) st = run(p2, c, &c.ms);
       else c.ms = 1e30f;
     }
-    free_pilot(p2);
+    stage = 2;
+    last = &p2;
   }
+  // the other shade block size for the best wavefront candidate, on the last pilot
+  if (!st) {
+    const Cand* bw = nullptr;
+    for (const Cand& c : cands)
+      if (c.exec == TPT_EXEC_WAVEFRONT && (!bw || c.ms < bw->ms)) bw = &c;
+    if (bw) {
+      Cand alt = *bw;
+      alt.block = bw->block == 256 ? 128 : 256;
+      st = run(*last, alt, &alt.ms);
+      cands.push_back(alt);
+    }
+  }
+  free_pilot(p1);
+  free_pilot(p2);
+  const float ms_mk = cands[0].ms;  // the megakernel on the last pilot
   ctx->batch_capacity = saved_cap;
   ctx->use_graphs = saved_graphs;
   ctx->shade_block = saved_block;
@@ -157,7 +175,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   best.ms = 1e30f;
   float ms_default = 0.0f;
   for (const Cand& c : cands) {
-    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs) ms_default = c.ms;
+    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs && c.block == saved_block) ms_default = c.ms;
     if (c.ms < best.ms) {
       best.ms = c.ms;
       best.execution = c.exec;
@@ -172,10 +190,13 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     best.ms = ms_default;
     best.wavefront_capacity = 1u << 22;
     best.graphs = 1;
+    best.shade_block = saved_block;
   }
   best.pilot_paths = std::min<uint64_t>(total, total > kPilotPaths ? 4 * kPilotPaths : total);
   best.ms_megakernel = ms_mk;
   best.ms_wavefront_default = ms_default;
+  best.stage = stage;
+  best.candidates = (uint32_t)cands.size();
   // apply
   ctx->tuned_execution = best.execution;
   if (best.execution == TPT_EXEC_WAVEFRONT) {

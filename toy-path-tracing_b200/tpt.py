@@ -226,7 +226,7 @@ GRAD_ALL = 31
 class TuneResult(C.Structure):
     _fields_ = [("execution", C.c_uint32), ("wavefront_capacity", C.c_uint32), ("graphs", C.c_uint32),
                 ("shade_block", C.c_uint32), ("ms", C.c_float), ("ms_megakernel", C.c_float), ("ms_wavefront_default", C.c_float),
-                ("pilot_paths", C.c_uint64)]
+                ("pilot_paths", C.c_uint64), ("stage", C.c_uint32), ("candidates", C.c_uint32)]
 
 
 INTEGRATOR_MIS = 0
