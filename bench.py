@@ -695,11 +695,24 @@ def adjoint_block(ctx, args, cpu=True):
         losses.append(float(loss.detach()))
     adam_s = time.perf_counter() - t0
     p_end = params.detach().numpy()
+    # the patches the camera sees directly (>= 1 % of the pixels each)
+    hit = scene.closest_hit(tpt_scenes.pixel_center_rays(sc["camera"], W, W), want_instance=True)
+    counts = np.bincount(hit["inst"][hit["prim"] >= 0], minlength=len(sc["instances"]))[:64]
+    vis = np.nonzero(counts >= 0.01 * W * W)[0]
+    true = sc["params"]
     out["inverse_rendering"] = {"steps": args.adjoint_steps, "lr": 0.003, "loss_first": losses[0],
                                 "loss_last": losses[-1], "seconds": adam_s,
+                                "backward": "decorrelated: the adjoint replays the job at spp + 1",
                                 "image_loss_256spp_start": clean_start, "image_loss_256spp_end": clean_loss(p_end),
-                                "param_mae_start": float(np.abs(start - sc["params"]).mean()),
-                                "param_mae_end": float(np.abs(p_end - sc["params"]).mean())}
+                                "param_mae_start": float(np.abs(start - true).mean()),
+                                "param_mae_end": float(np.abs(p_end - true).mean()),
+                                "visible_patches": int(len(vis)),
+                                "base_color_mae_visible_start": float(np.abs(start[vis, :3] - true[vis, :3]).mean()),
+                                "base_color_mae_visible_end": float(np.abs(p_end[vis, :3] - true[vis, :3]).mean()),
+                                "roughness_mae_visible_start": float(np.abs(start[vis, 3] - true[vis, 3]).mean()),
+                                "roughness_mae_visible_end": float(np.abs(p_end[vis, 3] - true[vis, 3]).mean()),
+                                "metalness_mae_visible_start": float(np.abs(start[vis, 4] - true[vis, 4]).mean()),
+                                "metalness_mae_visible_end": float(np.abs(p_end[vis, 4] - true[vis, 4]).mean())}
     if cpu:
         import oracle as orc
 

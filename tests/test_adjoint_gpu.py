@@ -164,13 +164,24 @@ def test_adjoint_rejects_bdpt_and_bad_masks(patches):
         scene.adjoint_device(job, d.data_ptr(), g.data_ptr(), mask=64)
 
 
+def visible_patches(scene, sc, W, min_frac=0.01):
+    """Materials (one per patch instance) seen directly by at least min_frac of
+    the pixels: the parameters the image constrains."""
+    out = scene.closest_hit(tpt_scenes.pixel_center_rays(sc["camera"], W, W), want_instance=True)
+    inst = out["inst"][out["prim"] >= 0]
+    counts = np.bincount(inst, minlength=len(sc["instances"]))[:tpt_scenes.N_PATCH_MATERIALS]
+    return np.nonzero(counts >= min_frac * W * W)[0]
+
+
 def test_inverse_rendering_lowers_loss(ctx):
     """200 Adam steps (lr 0.003) on the 64 patch materials from a perturbed
-    start, 128x128 at 16 spp forward and adjoint: the image loss measured at
-    256 spp against the 1024-spp target must fall below 0.6 of its start
-    (measured on a B200: 38.7 -> 12.9).  Parameter error is printed, not
-    checked: base colour, metalness and roughness trade off against each other
-    in the image and several patches are barely visible."""
+    start, 128x128 at 16 spp forward and adjoint (the backward pass replays the
+    job at 17 spp, so its paths are independent of the forward image's): the
+    image loss measured at 256 spp against the 1024-spp target must fall below
+    0.6 of its start, and the base-colour error of the patches the camera sees
+    (at least 1 % of the pixels each) must fall.  Roughness and metalness are
+    printed, not checked: they trade off against each other and against base
+    colour in the image."""
     import torch
 
     sc = tpt_scenes.cornell_patches()
@@ -206,7 +217,15 @@ def test_inverse_rendering_lowers_loss(ctx):
             params.copy_(torch.maximum(torch.minimum(params, hi), lo))
     p = params.detach().numpy()
     loss1 = clean_loss(p)
-    print("256-spp image loss", loss0, "->", loss1, "parameter error", np.abs(start - sc["params"]).mean(), "->",
-          np.abs(p - sc["params"]).mean())
+    vis = visible_patches(scene, sc, W)
+    bc0 = np.abs(start[vis, :3] - sc["params"][vis, :3]).mean()
+    bc1 = np.abs(p[vis, :3] - sc["params"][vis, :3]).mean()
+    print("256-spp image loss", loss0, "->", loss1, "; all parameters' error", np.abs(start - sc["params"]).mean(),
+          "->", np.abs(p - sc["params"]).mean(), f"; base colour of the {len(vis)} visible patches", bc0, "->", bc1,
+          "; roughness", np.abs(start[vis, 3] - sc["params"][vis, 3]).mean(), "->",
+          np.abs(p[vis, 3] - sc["params"][vis, 3]).mean(), "; metalness",
+          np.abs(start[vis, 4] - sc["params"][vis, 4]).mean(), "->", np.abs(p[vis, 4] - sc["params"][vis, 4]).mean())
+    assert len(vis) >= 20
     assert loss1 < 0.6 * loss0
+    assert bc1 < bc0
     scene.close()

@@ -769,9 +769,11 @@ def render_function():
     the listed materials (the TPT_GRAD_* order: base_color rgb, roughness,
     metalness, specular_ior, coat_weight), so params rows must follow that
     order up to k.  adjoint_job
-    (optional): the job the backward pass replays, e.g. the same image at another
-    spp, so that its paths are independent of the forward image's (an L2 loss
-    gradient from correlated samples is biased)."""
+    (optional): the job the backward pass replays.  By default it is the
+    forward job at spp + 1 samples per pixel: its sample indices, and so its
+    paths, differ from the forward image's, so the gradient of an L2 loss is
+    not correlated with that image's noise (a same-sample backward is biased).
+    Pass the forward job itself to replay its very paths."""
     import torch
 
     class RenderFunction(torch.autograd.Function):
@@ -783,7 +785,10 @@ def render_function():
             img = torch.empty(job.height * job.width * 3, dtype=torch.float32, device="cuda")
             scene.render_device(job, img.data_ptr(), stream)
             fctx.scene, fctx.ids, fctx.mask, fctx.step = scene, material_ids, mask, fd_step
-            fctx.job = adjoint_job if adjoint_job is not None else job
+            if adjoint_job is None:
+                adjoint_job = RenderJob.from_buffer_copy(job)
+                adjoint_job.spp = job.spp + 1
+            fctx.job = adjoint_job
             fctx.k = params.shape[1]
             fctx.device, fctx.dtype = params.device, params.dtype
             return img.view(job.height, job.width, 3)

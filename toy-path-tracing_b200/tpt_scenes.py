@@ -380,6 +380,28 @@ def cornell_patches(seed: int = 5, params=None, light_strength: float = 15.0):
             "angles": (float(a1), float(a2)), "seed": seed, "params": np.asarray(params, np.float32)}
 
 
+def pixel_center_rays(camera: dict, width: int, height: int) -> np.ndarray:
+    """Pinhole rays through the pixel centres (7 x width*height planes, pixel =
+    y * width + x, row 0 at the top), for coverage queries."""
+    eye = np.asarray(camera["eye"], np.float64)
+    fwd = np.asarray(camera["look_at"], np.float64) - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, np.asarray(camera["up"], np.float64))
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    t = np.tan(0.5 * camera["fov_y"])
+    aspect = width / height
+    x = (2.0 * (np.arange(width) + 0.5) / width - 1.0) * t * aspect
+    y = (1.0 - 2.0 * (np.arange(height) + 0.5) / height) * t
+    d = fwd[None, None, :] + x[None, :, None] * right + y[:, None, None] * up
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    rays = np.zeros((7, width * height), np.float32)
+    rays[0:3] = eye[:, None]
+    rays[3:6] = d.reshape(-1, 3).T
+    rays[6] = np.inf
+    return rays
+
+
 def with_patch_params(scene: dict, params) -> dict:
     """The same scene with its 64 patch materials set to `params` [64, 5]."""
     out = dict(scene)
