@@ -154,10 +154,16 @@ typedef enum tpt_material_kind {
  * 393-487) plus directional-albedo and energy-compensation tables built on the
  * GPU (bsdf/directional_albedo.rs).  The device path covers the base (EON
  * diffuse), metal, specular reflection, coat and fuzz lobes with anisotropy and
- * smooth (delta) lobes.  Upload rejects with TPT_ERR_INVALID_ARG a material
- * with transmission_weight > 0, thin_film_weight > 0, emission_luminance > 0,
- * geometry_opacity < 1 or geometry_thin_walled != 0.  subsurface_weight is
- * ignored, as the reference forces it to 0 (validate_and_warn). */
+ * smooth (delta) lobes, specular transmission (rough and smooth GGX BTDF with
+ * its multiple-scattering term), thin-walled slabs, thin-film interference on
+ * the Fresnel terms, and emission (OpenPbrMaterial::le, open_pbr.rs:351-391:
+ * emission_color * emission_luminance from the front face, both faces when
+ * thin-walled, tinted by the coat and fuzz above it; such a surface is a light
+ * of the light tree and of BDPT's area-light table).  Upload rejects with
+ * TPT_ERR_INVALID_ARG a material with geometry_opacity < 1 (alpha testing).
+ * subsurface_weight is ignored, as the reference forces it to 0
+ * (validate_and_warn); dispersion is off (the untextured parameter set has no
+ * dispersion scale). */
 typedef struct tpt_openpbr_desc {
   float base_weight;
   float base_color[3];
@@ -548,7 +554,8 @@ tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint
  * on the host and copied on `stream` (NULL = the context's stream), ordered
  * after the work already queued there; renders on other streams that read the
  * scene must have finished.  Fails with TPT_ERR_INVALID_ARG for a material that
- * is not OpenPBR or for parameters upload would reject. */
+ * is not OpenPBR, for parameters upload would reject, and for a change of
+ * emission_luminance or emission_color (the light tree was built from them). */
 tpt_status tpt_scene_set_openpbr(tpt_context* ctx, tpt_scene* scene, uint32_t count, const uint32_t* material_ids,
                                  const tpt_openpbr_desc* descs, void* stream);
 
@@ -597,7 +604,10 @@ typedef struct tpt_adjoint_desc {
  * [1, 10]); an unoccluded light sample C at an OpenPBR vertex (directional
  * lights, environment) adds dLoss/dL * C * (df/dtheta) / f at the light direction.
  * Accumulation is FP64 atomics, so the sums' order (and last bits)
- * vary between runs.  adesc may be NULL (all groups, step 1e-3). */
+ * vary between runs.  adesc may be NULL (all groups, step 1e-3).  Emission is
+ * replayed but not differentiated: with the coat group in the mask, a scene
+ * holding an OpenPBR emitter under a coat (whose exit tint depends on
+ * coat_weight) fails with TPT_ERR_INVALID_ARG. */
 tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const tpt_adjoint_desc* adesc,
                               const float* d_image, double* grad, void* stream);
 /* Host-buffer variant (synchronous). */

@@ -121,6 +121,7 @@ def _declare(L):
         "orc_openpbr_eval": (None, [vp, i32, vp, vp, i32, vp]),
         "orc_openpbr_pdf": (f32, [vp, i32, vp, vp]),
         "orc_openpbr_sample": (i32, [vp, i32, vp, f32, f32, f32, i32, vp]),
+        "orc_openpbr_le": (i32, [vp, i32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -666,6 +667,12 @@ class OpenPbrMaterial:
 
     def pdf(self, wo, wi, front=True):
         return lib().orc_openpbr_pdf(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)))
+
+    def le(self, wo, front=True):
+        """Emitted radiance toward the local direction wo, or None."""
+        out = np.zeros(3, np.float32)
+        ok = lib().orc_openpbr_le(_p(self.rec), int(front), _p(_v3(wo)), _p(out))
+        return out if ok else None
 
     def sample(self, wo, u_lobe, u_dir, front=True, mode=0):
         out = np.zeros(9, np.float32)

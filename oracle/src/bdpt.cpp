@@ -180,7 +180,7 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
     vs.push_back(pv);
     const size_t vi = vs.size() - 1;
     Vec3 le;
-    if (material_le(m, &le)) {
+    if (material_le(m, v, &le)) {
       float w = count_emission ? 1.0f : camera_light_hit_mis_weight(s, vs);
       L += beta * le * w;
     }
@@ -242,7 +242,7 @@ void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_dep
   Vertex lv = s.shading_vertex(al.inst, al.tri, bary, -emit);
   lv.wo = emit;
   Vec3 le;
-  if (!material_le(s.mat_of(al.inst), &le)) return;
+  if (!material_le(s.mat_of(al.inst), lv, &le)) return;
   float cos_emit = fmax_num(dot(lv.ng, emit), 0.0f);
   if (cos_emit <= 0.0f) return;
   Vec3 endpoint_beta = le / pdf_area;

@@ -209,6 +209,25 @@ int orc_openpbr_sample(const void* desc, int front, const float* wo, float u_lob
   return do_sample(bsdf_from_desc((const OpenPbrDesc*)desc, front, wo), wo, u_lobe, u0, u1, mode, out9);
 }
 
+// OpenPbrMaterial::le (material/open_pbr.rs:351-375) at a vertex whose shading
+// frame is the identity, for a local wo; 0: no emission (le() is None).
+int orc_openpbr_le(const void* desc, int front, const float* wo, float* out3) {
+  Material m;
+  m.kind = kOpenPbr;
+  m.openpbr = *(const OpenPbrDesc*)desc;
+  Vertex v{};
+  v.frame.t = Vec3(1, 0, 0);
+  v.frame.b = Vec3(0, 1, 0);
+  v.frame.n = Vec3(0, 0, 1);
+  v.ng = v.ns = v.frame.n;
+  v.wo = Vec3(wo[0], wo[1], wo[2]);
+  v.front_face = front != 0;
+  Vec3 le;
+  if (!material_le(m, v, &le)) return 0;
+  put3(out3, le);
+  return 1;
+}
+
 // Scene material: OpenPBR parameters of material `index` (kind must be 2).
 const char* orc_render_scene_set_openpbr(void* h, uint32_t index, const void* desc) {
   auto* s = (RenderScene*)h;

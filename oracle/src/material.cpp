@@ -110,9 +110,61 @@ bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& 
   return false;  // Emissive: pure emitter
 }
 
-bool material_le(const Material& m, Vec3* le) {
-  if (m.kind != kEmissive) return false;
-  *le = m.color * m.strength;
+bool may_emit(const Material& m) {
+  if (m.kind == kEmissive) return true;
+  return m.kind == kOpenPbr && m.openpbr.emission_luminance > 0.0f;
+}
+
+float max_emission(const Material& m) {
+  if (m.kind == kEmissive) {
+    Vec3 e = m.color * m.strength;
+    return fmax_num(fmax_num(fmax_num(e.x, e.y), e.z), 0.0f);
+  }
+  if (m.kind == kOpenPbr && m.openpbr.emission_luminance > 0.0f) {  // material/open_pbr.rs:381-391
+    const float* c = m.openpbr.emission_color;
+    return fmax_num(fmax_num(c[0], fmax_num(c[1], c[2])) * m.openpbr.emission_luminance * 1.0f, 0.0f);
+  }
+  return 0.0f;
+}
+
+namespace {
+// OpenPbrMaterial::emission_exit_tint (material/open_pbr.rs:608-638): the
+// emission leaves through the coat (its colour over the refracted path) and
+// under the fuzz (what the fuzz does not reflect)
+Vec3 openpbr_exit_tint(const OpenPbrDesc& d, const Vertex& v) {
+  Vec3 wo_l = normalize_or_zero(v.frame.to_local(v.wo));
+  float cos_o = clampf(std::fabs(wo_l.z), 0.0f, 1.0f);
+  if (cos_o <= 0.0f) return Vec3(0, 0, 0);
+  Vec3 tint(1, 1, 1);
+  float cw = clampf(d.coat_weight, 0.0f, 1.0f);
+  if (cw > 0.0f) {
+    float eta = fmax_num(d.coat_ior, 1.0e-4f);
+    float mu_t = fmax_num(std::sqrt(fmax_num(1.0f - (1.0f - cos_o * cos_o) / (eta * eta), 0.0f)), 1.0e-4f);
+    Vec3 cc = vmin(vmax(Vec3(d.coat_color[0], d.coat_color[1], d.coat_color[2]), Vec3(0, 0, 0)), Vec3(1, 1, 1));
+    float e = 1.0f / mu_t;
+    Vec3 trans(std::pow(cc.x, e), std::pow(cc.y, e), std::pow(cc.z, e));
+    tint *= Vec3(1, 1, 1) + (trans - Vec3(1, 1, 1)) * cw;
+  }
+  float fw = clampf(d.fuzz_weight * 1.0f, 0.0f, 1.0f);
+  if (fw > 0.0f) {
+    float e_fuzz = openpbr_fuzz_albedo(cos_o, clampf(d.fuzz_roughness * 1.0f, 0.0f, 1.0f));
+    tint *= Vec3::splat(1.0f + (fmax_num(1.0f - e_fuzz, 0.0f) - 1.0f) * fw);
+  }
+  return tint;
+}
+}  // namespace
+
+bool material_le(const Material& m, const Vertex& v, Vec3* le) {
+  if (m.kind == kEmissive) {
+    *le = m.color * m.strength;
+    return true;
+  }
+  if (m.kind != kOpenPbr) return false;
+  const OpenPbrDesc& d = m.openpbr;
+  if (d.emission_luminance <= 0.0f) return false;
+  if (!d.geometry_thin_walled && !v.front_face) return false;
+  Vec3 c(d.emission_color[0], d.emission_color[1], d.emission_color[2]);
+  *le = c * Vec3(1, 1, 1) * fmax_num(d.emission_luminance, 0.0f) * openpbr_exit_tint(d, v);
   return true;
 }
 

@@ -1031,12 +1031,13 @@ bool OpenPbrBsdf::sample(Vec3 wo, float u_lobe, Vec2 u_dir, TransportMode mode, 
   return Impl{p, L}.sample(wo, u_lobe, u_dir, mode, out);
 }
 
+float openpbr_fuzz_albedo(float ndot_v, float roughness) { return zeltner_dir_albedo(ndot_v, roughness); }
+
 float openpbr_specular_eta(const OpenPbrDesc& m) {
   return modulated_eta(fmax_num(m.specular_ior, 1.0e-4f), fmax_num(m.specular_weight, 0.0f));
 }
 
 const char* openpbr_unsupported(const OpenPbrDesc& m) {
-  if (m.emission_luminance > 0.0f) return "emission_luminance > 0";
   if (m.geometry_opacity < 1.0f) return "geometry_opacity < 1";
   return "";
 }

@@ -157,6 +157,9 @@ Vec3 eon_eval(Vec3 rho, float roughness, Vec3 wo, Vec3 wi);
 float eon_pdf(float roughness, Vec3 wo, Vec3 wi);
 bool eon_sample(Vec3 rho, float roughness, Vec3 wo, Vec2 us, BsdfSample* s);
 
+// zeltner_dir_albedo (material/open_pbr.rs:888-897): the fuzz lobe's albedo
+float openpbr_fuzz_albedo(float ndot_v, float roughness);
+
 // OpenPbrMaterial::make_bsdf (material/open_pbr.rs:393-487) for an untextured
 // material seen from `wo_local` on the front (or back) face.
 OpenPbrParams make_openpbr_params(const OpenPbrDesc& m, bool front_face, Vec3 wo_local);

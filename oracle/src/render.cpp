@@ -238,7 +238,6 @@ bool lambert_sample(const Material& m, const Vertex& v, Vec2 u, MatSample* s) {
   s->delta = false;
   return dot(s->wi, v.ng) > kGeomCosEps;
 }
-Vec3 emissive_le(const Material& m) { return m.color * m.strength; }
 
 // OpenPbrMaterial::sample (material/open_pbr.rs:489-563), radiance transport
 // (modified_bsdf_sample_weight leaves the weight unchanged).
@@ -292,11 +291,13 @@ bool sample_li_triangle(const RenderScene& s, int inst, int tri, Vec3 p_ref, Vec
   float dist = std::sqrt(d2);
   Vec3 wi = to_light / dist;
   const Material& lm = s.mat_of(inst);
-  if (lm.kind != kEmissive) return false;
+  if (!may_emit(lm)) return false;
   Vertex lv = s.shading_vertex(inst, tri, b, wi);
+  Vec3 le;
+  if (!material_le(lm, lv, &le)) return false;
   float cos_light = fmax_num(dot(lv.ng, -wi), 0.0f);
   if (cos_light <= 0.0f) return false;
-  out->radiance = emissive_le(lm);
+  out->radiance = le;
   out->wi = wi;
   out->pdf = pdf_area * d2 / cos_light;
   out->distance = dist;
@@ -510,7 +511,7 @@ Frame Frame::from_normal_and_tangent(Vec3 normal, Vec3 hint) {
 void RenderScene::finalize() {
   leaf_of.assign(geo.instances.size(), {});
   for (size_t i = 0; i < geo.instances.size(); ++i)
-    if (materials[geo.instances[i].material_index].kind == kEmissive)
+    if (may_emit(materials[geo.instances[i].material_index]))
       leaf_of[i].assign(geo.meshes[geo.instances[i].mesh_index].triangle_count(), kNoNode);
   for (uint32_t k = 0; k < tree.size(); ++k) {
     const uint32_t li = tree[k].leaf_instance;
@@ -522,16 +523,15 @@ void RenderScene::finalize() {
   area_light_weight_sum = 0.0f;
   for (size_t i = 0; i < geo.instances.size(); ++i) {
     const Material& m = materials[geo.instances[i].material_index];
-    if (m.kind != kEmissive) continue;  // may_emit
-    Vec3 e = m.color * m.strength;
-    float max_emission = fmax_num(fmax_num(fmax_num(e.x, e.y), e.z), 0.0f);
-    if (max_emission <= 0.0f) continue;
+    if (!may_emit(m)) continue;
+    const float max_em = max_emission(m);
+    if (max_em <= 0.0f) continue;
     int ntri = (int)geo.meshes[geo.instances[i].mesh_index].triangle_count();
     for (int t = 0; t < ntri; ++t) {
       Vec3 p[3];
       triangle_world((int)i, t, p);
       float area = 0.5f * length(cross(p[1] - p[0], p[2] - p[0]));
-      float weight = area * max_emission;
+      float weight = area * max_em;
       if (weight <= 0.0f) continue;
       area_light_weight_sum += weight;
       area_lights.push_back(AreaLight{(int32_t)i, t, area, weight, area_light_weight_sum});
@@ -652,7 +652,8 @@ Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, 
     }
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
     const Material& m = s.mat_of(h.instance);
-    if (m.kind == kEmissive) L += beta * emissive_le(m);
+    Vec3 le;
+    if (material_le(m, v, &le)) L += beta * le;
     MatSample bs;
     bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
               : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
@@ -686,8 +687,9 @@ Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
     }
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
     const Material& m = s.mat_of(h.instance);
-    if (count_emission && m.kind == kEmissive) L += beta * emissive_le(m);
-    if (m.kind != kEmissive) L += beta * direct_light_impl(s, m, v, rnd, nullptr, kDirectNee);
+    Vec3 le;
+    if (count_emission && material_le(m, v, &le)) L += beta * le;
+    if (!is_pure_emitter(m)) L += beta * direct_light_impl(s, m, v, rnd, nullptr, kDirectNee);
     MatSample bs;
     bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
               : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
@@ -713,10 +715,11 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
   if (!closest(s, ray.origin, ray.direction, &h)) return s.has_env ? s.env.radiance(ray.direction) : L;
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
   const Material* m = &s.mat_of(h.instance);
-  if (m->kind == kEmissive) L += emissive_le(*m);
+  Vec3 le0;
+  if (material_le(*m, v, &le0)) L += le0;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
-    if (m->kind == kEmissive) break;
+    if (is_pure_emitter(*m)) break;
     L += beta * direct_light(s, *m, v, rnd);
     MatSample bs;
     bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
@@ -735,8 +738,8 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
     }
     Vertex nv = s.shading_vertex(nh.instance, nh.triangle, nh.bary, bs.wi);
     const Material* nm = &s.mat_of(nh.instance);
-    if (nm->kind == kEmissive) {
-      Vec3 le = emissive_le(*nm);
+    Vec3 le;
+    if (material_le(*nm, nv, &le)) {
       if (bs.delta) L += beta * le;
       else L += beta * le * balance(bs.pdf, light_pdf_for_hit(s, *m, v, nv));
     }
@@ -754,10 +757,11 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
   const Material* m = &s.mat_of(h.instance);
   uint32_t mi = s.geo.instances[h.instance].material_index;
-  if (m->kind == kEmissive) R = R - emissive_le(*m);
+  Vec3 le0;
+  if (material_le(*m, v, &le0)) R = R - le0;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
-    if (m->kind == kEmissive) break;
+    if (is_pure_emitter(*m)) break;
     Vec3 wl(0, 0, 0);
     const Vec3 c = beta * direct_light(s, *m, v, rnd, &wl);
     R = R - c;
@@ -779,8 +783,8 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
     if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) break;  // R = the escape emission
     Vertex nv = s.shading_vertex(nh.instance, nh.triangle, nh.bary, bs.wi);
     const Material* nm = &s.mat_of(nh.instance);
-    if (nm->kind == kEmissive) {
-      Vec3 le = emissive_le(*nm);
+    Vec3 le;
+    if (material_le(*nm, nv, &le)) {
       if (bs.delta) R = R - beta * le;
       else R = R - beta * le * balance(bs.pdf, light_pdf_for_hit(s, *m, v, nv));
     }
@@ -878,9 +882,9 @@ void orc_render_emitted(void* h, int inst, int tri, const float* bary3, const fl
                                Vec3(lincident3[0], lincident3[1], lincident3[2]));
   const Material& lm = s.mat_of(linst);
   Vec3 r(0, 0, 0);
-  if (lm.kind == kEmissive) {
+  Vec3 le;
+  if (material_le(lm, lv, &le)) {
     Vec3 beta(throughput3[0], throughput3[1], throughput3[2]);
-    Vec3 le = emissive_le(lm);
     r = delta ? beta * le : beta * le * balance(bsdf_pdf, light_pdf_for_hit(s, s.mat_of(inst), v, lv));
   }
   out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;

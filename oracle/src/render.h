@@ -134,7 +134,13 @@ Vec3 material_eval(const Material& m, const Vertex& v, Vec3 wi, TransportMode mo
 float material_pdf(const Material& m, const Vertex& v, Vec3 wi);
 bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& r, TransportMode mode,
                      MatSampleOut* s);
-bool material_le(const Material& m, Vec3* le);  // Emissive only (two-sided)
+// Material::le at vertex v: EmissiveMaterial two-sided (emissive.rs:68-81),
+// OpenPbrMaterial front face only unless thin-walled, times its exit tint
+// (material/open_pbr.rs:351-375, 608-638); false for None.
+bool material_le(const Material& m, const Vertex& v, Vec3* le);
+// Material::may_emit / max_emission (material/mod.rs:395-420)
+bool may_emit(const Material& m);
+float max_emission(const Material& m);
 inline bool is_pure_emitter(const Material& m) { return m.kind == kEmissive; }
 
 // Light sampling at a scattering vertex.  kDirectMis:

@@ -108,6 +108,12 @@ tpt_status tpt_scene_set_openpbr(tpt_context* ctx, tpt_scene* scene, uint32_t co
       return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(m) + " is not an OpenPBR material");
     const std::string why = openpbr_unsupported(descs[k]);
     if (!why.empty()) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(m) + ": " + why);
+    // the light tree and the material record were built from the uploaded emission
+    const tpt_openpbr_desc& old = scene->opbr_desc[scene->opbr_of_material[m]];
+    if (descs[k].emission_luminance != old.emission_luminance ||
+        std::memcmp(descs[k].emission_color, old.emission_color, sizeof old.emission_color) != 0)
+      return set_error(ctx, TPT_ERR_INVALID_ARG,
+                       "material " + std::to_string(m) + ": emission differs from the uploaded scene's");
     tpt_status st = lower_openpbr_material(ctx, descs[k], &recs[k]);
     if (st) return st;
   }
@@ -138,9 +144,17 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   if (mask & ~(uint32_t)TPT_GRAD_ALL) return set_error(ctx, TPT_ERR_INVALID_ARG, "unknown gradient group bits");
   const float step = adesc && adesc->fd_step > 0.0f ? adesc->fd_step : kDefaultFdStep;
   if (!(step < 0.5f)) return set_error(ctx, TPT_ERR_INVALID_ARG, "fd_step must be in (0, 0.5)");
+  tpt_scene* scene = const_cast<tpt_scene*>(job->scene);
+  if (mask & TPT_GRAD_MASK_COAT) {
+    // emission leaving through a coat depends on coat_weight, and the replay
+    // differentiates the BSDF only
+    for (const tpt_openpbr_desc& d : scene->opbr_desc)
+      if (d.emission_luminance > 0.0f && d.coat_weight > 0.0f)
+        return set_error(ctx, TPT_ERR_INVALID_ARG,
+                         "coat gradients of a scene with a coated OpenPBR emitter are not differentiated");
+  }
   if ((st = set_device(ctx))) return st;
   note_device_call(ctx, "tpt_adjoint_device");
-  tpt_scene* scene = const_cast<tpt_scene*>(job->scene);
   if ((st = ensure_adjoint_tables(ctx, scene, mask, step))) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   const size_t gbytes = (size_t)scene->render.num_materials * kGradParams * sizeof(double);

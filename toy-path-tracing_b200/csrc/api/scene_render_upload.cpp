@@ -12,6 +12,23 @@
 
 namespace tpt {
 
+// The host-side view of a material: its kind, Lambert albedo and what it
+// emits (the emissive material's colour and strength; an OpenPBR material's
+// emission_color and emission_luminance).
+HostMaterial host_material(const tpt_material_desc& m) {
+  HostMaterial h{};
+  h.kind = m.kind;
+  std::memcpy(h.rho, m.rho, 12);
+  if (m.kind == TPT_MATERIAL_OPENPBR && m.openpbr) {
+    std::memcpy(h.color, m.openpbr->emission_color, 12);
+    h.strength = m.openpbr->emission_luminance;
+  } else {
+    std::memcpy(h.color, m.color, 12);
+    h.strength = m.strength;
+  }
+  return h;
+}
+
 tpt_status scene_alloc(tpt_scene* s, size_t bytes, void** out) {
   bytes = std::max<size_t>(bytes, 128);
   void* p = nullptr;
@@ -77,18 +94,15 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
       s->opbr_desc.push_back(*m.openpbr);
     }
     s->opbr_of_material.push_back(m.kind == TPT_MATERIAL_OPENPBR ? opbr_index : kInvalidNode);
-    HostMaterial h{};
-    h.kind = m.kind;
-    std::memcpy(h.rho, m.rho, 12);
-    std::memcpy(h.color, m.color, 12);
-    h.strength = m.strength;
+    HostMaterial h = host_material(m);
     hmats[i] = h;
     DevMaterialRec d{};
     d.kind = m.kind;
     std::memcpy(d.rho, m.rho, 12);
-    std::memcpy(d.color, m.color, 12);
-    d.strength = m.strength;
+    std::memcpy(d.color, h.color, 12);
+    d.strength = h.strength;
     d.openpbr = opbr_index;
+    d.emits = m.kind == TPT_MATERIAL_OPENPBR && h.may_emit() ? 1u : 0u;
     dmats[i] = d;
   }
   for (uint32_t i = 0; i < desc->num_instances; ++i)
@@ -364,12 +378,9 @@ tpt_status tpt_light_tree_build_threads(const tpt_scene_desc* desc, int threads,
     return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL array in scene description");
   std::vector<HostMaterial> hm(desc->num_materials);
   for (uint32_t i = 0; i < desc->num_materials; ++i) {
-    const tpt_material_desc& m = desc->materials[i];
-    hm[i] = HostMaterial{};
-    hm[i].kind = m.kind;
-    std::memcpy(hm[i].rho, m.rho, 12);
-    std::memcpy(hm[i].color, m.color, 12);
-    hm[i].strength = m.strength;
+    if (desc->materials[i].kind == TPT_MATERIAL_OPENPBR && !desc->materials[i].openpbr)
+      return set_error(nullptr, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": openpbr is NULL");
+    hm[i] = host_material(desc->materials[i]);
   }
   std::vector<HostMesh> meshes(desc->num_meshes);
   for (uint32_t i = 0; i < desc->num_meshes; ++i) {

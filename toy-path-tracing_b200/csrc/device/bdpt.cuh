@@ -286,9 +286,12 @@ __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaun
   pv.pdf_rev = 0.0f;
   pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
   const uint32_t n = ++c.n;
-  if (m.kind == kDevEmissive) {
+  V3 le;
+  if (may_emit(m) && material_le(S, m, v, le)) {
     const float w = c.count_emission ? 1.0f : camera_light_hit_mis(S, vs, n);
-    L = L + c.beta * emissive_le(m) * w;
+    L = L + c.beta * le * w;
+  }
+  if (m.kind == kDevEmissive) {
     c.alive = false;  // pure emitter: sample() is None
     return;
   }
@@ -392,10 +395,11 @@ __device__ __forceinline__ bool bdpt_light_endpoint(const DevRender& S, const Re
   Vertex lvx = make_vertex(T, al.inst, al.tri, b0, b1, b2, -emit);
   lvx.wo = emit;
   const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[al.inst].material)];
-  if (lm.kind != kDevEmissive) return false;  // le() is None
+  V3 le;
+  if (!may_emit(lm) || !material_le(S, lm, lvx, le)) return false;  // le() is None
   const float cos_emit = fmaxf(dot(lvx.ng, emit), 0.0f);
   if (cos_emit <= 0.0f) return false;
-  const V3 endpoint_beta = emissive_le(lm) / pdf_area;
+  const V3 endpoint_beta = le / pdf_area;
   vs[0].v = lvx;
   vs[0].beta = endpoint_beta;
   vs[0].pdf_fwd = pdf_area;

@@ -220,8 +220,50 @@ struct LightSample {
   uint32_t inst, tri;
 };
 
-__device__ __forceinline__ V3 emissive_le(const DevMaterialRec& m) {
-  return V3{m.color[0] * m.strength, m.color[1] * m.strength, m.color[2] * m.strength};
+// Material::may_emit: the emissive material, and OpenPBR with emission_luminance > 0
+// (emissive.rs, material/open_pbr.rs:377-379)
+__device__ __forceinline__ bool may_emit(const DevMaterialRec& m) { return m.kind == kDevEmissive || m.emits != 0u; }
+
+// OpenPBR emission leaving through the coat and fuzz layers
+// (emission_exit_tint, material/open_pbr.rs:608-638, untextured): the coat's
+// absorption along the refracted exit path, lerped by the coat weight, times
+// the energy the fuzz lobe leaves, lerped by the fuzz weight.
+__device__ __forceinline__ V3 openpbr_exit_tint(const DevOpenPbr& d, const Vertex& v) {
+  const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
+  const float cos_o = clampf(fabsf(wo_l.z), 0.0f, 1.0f);
+  if (cos_o <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
+  V3 tint = V3{1.0f, 1.0f, 1.0f};
+  if (d.coat > 0.0f) {  // coat weight, clamped to [0, 1]; coat_color clamped to [0, 1]
+    const float eta = d.coat_eta;
+    const float mu_t = fmaxf(sqrtf(fmaxf(1.0f - (1.0f - cos_o * cos_o) / (eta * eta), 0.0f)), 1.0e-4f);
+    const float e = 1.0f / mu_t;
+    const V3 trans = V3{powf(d.coat_color[0], e), powf(d.coat_color[1], e), powf(d.coat_color[2], e)};
+    tint = tint * (V3{1.0f, 1.0f, 1.0f} + (trans - V3{1.0f, 1.0f, 1.0f}) * d.coat);
+  }
+  if (d.fuzz > 0.0f) {
+    const float e_fuzz = opbr::zeltner_albedo(cos_o, d.fuzz_roughness);
+    const float t = 1.0f + (fmaxf(1.0f - e_fuzz, 0.0f) - 1.0f) * d.fuzz;
+    tint = tint * V3{t, t, t};
+  }
+  return tint;
+}
+
+// Material::le (emissive.rs:68-85, material/open_pbr.rs:351-375, untextured):
+// the emissive material radiates colour * strength from both faces; an OpenPBR
+// emitter radiates emission_color * emission_luminance from its front face
+// (both faces when thin-walled), tinted by the layers above it.  False: no
+// emission at this vertex.
+__device__ __forceinline__ bool material_le(const DevRender& S, const DevMaterialRec& m, const Vertex& v, V3& le) {
+  if (m.kind == kDevEmissive) {
+    le = V3{m.color[0] * m.strength, m.color[1] * m.strength, m.color[2] * m.strength};
+    return true;
+  }
+  if (!m.emits) return false;
+  const DevOpenPbr& d = S.d.openpbr[m.openpbr];
+  if (!(d.flags & kOpbrThinWalled) && !v.front) return false;
+  const float lum = fmaxf(m.strength, 0.0f);
+  le = V3{m.color[0], m.color[1], m.color[2]} * lum * openpbr_exit_tint(d, v);
+  return true;
 }
 
 __device__ __forceinline__ bool sample_li_triangle(const DevRender& S, uint32_t inst, uint32_t tri, V3 p_ref, float us0,
@@ -241,12 +283,20 @@ __device__ __forceinline__ bool sample_li_triangle(const DevRender& S, uint32_t 
   const float dist = sqrtf(d2);
   const V3 wi = to_light / dist;
   const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[inst].material)];
-  if (lm.kind != kDevEmissive) return false;  // may_emit
-  const V3 gn = normalize_or_zero(cross(T.p[1] - T.p[0], T.p[2] - T.p[0]));
-  const V3 ng = face_forward(gn, -wi);
+  if (!may_emit(lm)) return false;
+  V3 ng;
+  if (lm.kind == kDevEmissive) {
+    out.radiance = V3{lm.color[0] * lm.strength, lm.color[1] * lm.strength, lm.color[2] * lm.strength};
+    ng = face_forward(normalize_or_zero(cross(T.p[1] - T.p[0], T.p[2] - T.p[0])), -wi);
+  } else {
+    // the light's shading vertex, seen from p_ref, decides the face and the exit tint
+    fetch_triangle(S, inst, tri, T, true);
+    const Vertex lv = make_vertex(T, inst, tri, b.x, b.y, b.z, wi);
+    if (!material_le(S, lm, lv, out.radiance)) return false;
+    ng = lv.ng;
+  }
   const float cos_light = fmaxf(dot(ng, -wi), 0.0f);
   if (cos_light <= 0.0f) return false;
-  out.radiance = emissive_le(lm);
   out.wi = wi;
   out.pdf = pdf_area * d2 / cos_light;
   out.distance = dist;

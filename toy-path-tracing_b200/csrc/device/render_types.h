@@ -26,10 +26,11 @@ constexpr uint32_t kBdptMaxDepthApi = 16;
 struct alignas(16) DevMaterialRec {
   uint32_t kind;
   float rho[3];
-  float color[3];
-  float strength;
+  float color[3];    // Emissive colour; OpenPBR emission_color
+  float strength;    // Emissive strength; OpenPBR emission_luminance
   uint32_t openpbr;  // index into the OpenPBR parameter table
-  uint32_t pad[7];
+  uint32_t emits;    // OpenPBR with emission_luminance > 0 (may_emit): le() at its hits
+  uint32_t pad[6];
 };
 static_assert(sizeof(DevMaterialRec) == 64, "material record");
 

@@ -17,15 +17,24 @@ enum MaterialKind : uint32_t {
 struct HostMaterial {
   uint32_t kind;
   float rho[3];       // Lambert
-  float color[3];     // Emissive colour
-  float strength;     // Emissive strength
-  bool may_emit() const { return kind == kMatEmissive; }
-  // EmissiveMaterial::max_emission (emissive.rs:87-94): max channel of colour * strength, >= 0
+  float color[3];     // Emissive colour; OpenPBR emission_color
+  float strength;     // Emissive strength; OpenPBR emission_luminance
+  // Material::may_emit (material/mod.rs): the emissive material, and an
+  // OpenPBR material with emission_luminance > 0 (material/open_pbr.rs:377-379)
+  bool may_emit() const { return kind == kMatEmissive || (kind == kMatOpenPbr && strength > 0.0f); }
   float max_emission() const {
-    if (kind != kMatEmissive) return 0.0f;
-    float a = color[0] * strength, b = color[1] * strength, c = color[2] * strength;
-    float m = std::fmax(a, std::fmax(b, c));
-    return std::fmax(m, 0.0f);
+    if (kind == kMatEmissive) {
+      // EmissiveMaterial::max_emission (emissive.rs:87-94): max channel of colour * strength, >= 0
+      float a = color[0] * strength, b = color[1] * strength, c = color[2] * strength;
+      float m = std::fmax(a, std::fmax(b, c));
+      return std::fmax(m, 0.0f);
+    }
+    if (kind == kMatOpenPbr && strength > 0.0f) {
+      // OpenPbrMaterial::max_emission (material/open_pbr.rs:381-391), untextured
+      const float m = std::fmax(color[0], std::fmax(color[1], color[2]));
+      return std::fmax(m * strength * 1.0f, 0.0f);
+    }
+    return 0.0f;
   }
 };
 

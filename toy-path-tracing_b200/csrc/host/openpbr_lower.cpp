@@ -206,7 +206,6 @@ float radical_inverse_base3(uint32_t n) {
 }  // namespace
 
 std::string openpbr_unsupported(const tpt_openpbr_desc& m) {
-  if (m.emission_luminance > 0.0f) return "emission_luminance > 0 (OpenPBR emission is not on the device path)";
   if (m.geometry_opacity < 1.0f) return "geometry_opacity < 1 (alpha testing is not on the device path)";
   return "";
 }

@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
       const Vertex v = shade_hit<int>(S, h, rd);
       const uint32_t mi = __ldg(&S.d.inst[v.inst].material);
       const DevMaterialRec m = S.d.mats[mi];
-      if (m.kind == kDevEmissive) {
-        const V3 le = emissive_le(m);
+      V3 le;
+      if (may_emit(m) && material_le(S, m, v, le)) {
         if (depth == 0) {
           L = L + le;
         } else if ((prev_mat >> 31) || P.integrator == kIntegPt) {

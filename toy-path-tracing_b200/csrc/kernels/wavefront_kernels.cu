@@ -162,8 +162,8 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
     // emission of this vertex (mis.rs:45-47 for the camera vertex, 101-117
     // after a bounce; PT counts every hit in full, NEE only from the camera
     // and after delta samples)
-    if (m.kind == kDevEmissive) {
-      const V3 le = emissive_le(m);
+    V3 le;
+    if (may_emit(m) && material_le(S, m, v, le)) {
       if (d == 0) {
         L = L + sgn * le;
       } else {

@@ -217,6 +217,25 @@ def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPEN
     return sc
 
 
+def cornell_openpbr_emitter(seed: int = 1, coat: float = 0.0, fuzz: float = 0.0, thin_walled: bool = False):
+    """The Cornell box lit by OpenPBR emitters (material/open_pbr.rs:351-391):
+    the ceiling quad is an OpenPBR surface with emission_luminance 15 and the
+    short box glows with luminance 1.5 through its faces.  `coat` and `fuzz`
+    put a tinted coat and a fuzz layer over both emitters (their emission leaves
+    through the layers); `thin_walled` makes both emit from either face."""
+    sc = cornell_box(seed, OPENPBR)
+    thin = 1 if thin_walled else 0
+    layers = {"coat_weight": coat, "coat_color": np.array([0.6, 0.75, 0.9], np.float32), "coat_roughness": 0.2,
+              "fuzz_weight": fuzz, "fuzz_roughness": 0.6, "geometry_thin_walled": thin}
+    sc["materials"][7] = {"kind": OPENPBR, "base_color": np.array([0.7, 0.7, 0.7], np.float32),
+                          "specular_roughness": 0.5, "emission_luminance": 15.0,
+                          "emission_color": np.array([1.0, 0.9, 0.75], np.float32), **layers}
+    sc["materials"][6] = {"kind": OPENPBR, "base_color": np.array([0.5, 0.6, 0.4], np.float32),
+                          "specular_roughness": 0.4, "emission_luminance": 1.5,
+                          "emission_color": np.array([0.3, 0.8, 1.0], np.float32), **layers}
+    return sc
+
+
 def cornell_lights(seed: int = 1, material: int = LAMBERT, area: bool = True):
     """The Cornell box lit by a point light, a spot light and a directional
     light entering through the open front (plus the ceiling quad when `area`).
