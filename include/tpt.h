@@ -162,8 +162,11 @@ typedef enum tpt_material_kind {
  * of the light tree and of BDPT's area-light table).  Upload rejects with
  * TPT_ERR_INVALID_ARG a material with geometry_opacity < 1 (alpha testing).
  * subsurface_weight is ignored, as the reference forces it to 0
- * (validate_and_warn); dispersion is off (the untextured parameter set has no
- * dispersion scale). */
+ * (validate_and_warn).  Dispersion (transmission_dispersion_scale > 0,
+ * bsdf/dispersion.rs) makes the transmission IOR a Cauchy function of
+ * wavelength: an unlocked path evaluates the rough BTDF integrated over the
+ * camera's spectral basis, and a sampled dispersive refraction locks the path
+ * to one wavelength (the path state every integrator carries). */
 typedef struct tpt_openpbr_desc {
   float base_weight;
   float base_color[3];
@@ -194,6 +197,8 @@ typedef struct tpt_openpbr_desc {
   float emission_color[3];
   float geometry_opacity;
   uint32_t geometry_thin_walled;
+  float transmission_dispersion_scale;       /* 0 = no dispersion */
+  float transmission_dispersion_abbe_number; /* Abbe number at scale 1 (abbe / scale is used) */
 } tpt_openpbr_desc;
 
 void tpt_openpbr_defaults(tpt_openpbr_desc* desc);
@@ -542,6 +547,18 @@ tpt_status tpt_bsdf_eval_device(tpt_context* ctx, const tpt_scene* scene, uint32
 tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
                                   const float* wo, const float* u, const uint32_t* front_face, uint32_t mode,
                                   float* out, void* stream);
+/* The same queries with the path state a shading vertex carries
+ * (ShadingVertex::path_throughput and wavelength_lock, which dispersive
+ * transmission reads): state n x 4 = throughput r, g, b and the lock in nm
+ * (NaN = none).  Sampling takes u n x 7 = (u_lobe, u_dir.x, u_dir.y,
+ * u_extra0..3 of MaterialSampleRandoms) and writes n x 10: the 9 values above
+ * and the wavelength lock the sample sets (NaN = none). */
+tpt_status tpt_bsdf_eval_path_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
+                                     const float* wo, const float* wi, const uint32_t* front_face, const float* state,
+                                     uint32_t mode, float* f, float* pdf, void* stream);
+tpt_status tpt_bsdf_sample_path_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
+                                       const float* wo, const float* u, const uint32_t* front_face, const float* state,
+                                       uint32_t mode, float* out, void* stream);
 
 /* ---- Material updates and the path-replay adjoint -------------------------
  * Neither has a counterpart in the reference: its materials are fixed once

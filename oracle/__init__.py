@@ -122,6 +122,15 @@ def _declare(L):
         "orc_openpbr_pdf": (f32, [vp, i32, vp, vp]),
         "orc_openpbr_sample": (i32, [vp, i32, vp, f32, f32, f32, i32, vp]),
         "orc_openpbr_le": (i32, [vp, i32, vp, vp]),
+        "orc_openpbr_eval_ex": (None, [vp, i32, vp, vp, vp, i32, vp]),
+        "orc_openpbr_pdf_ex": (f32, [vp, i32, vp, vp, vp]),
+        "orc_openpbr_sample_ex": (i32, [vp, i32, vp, f32, f32, f32, vp, vp, i32, vp]),
+        "orc_openpbr_params_sample_ex": (i32, [vp, i32, f32, f32, vp, f32, f32, f32, vp, i32, vp]),
+        "orc_cauchy_ior": (f32, [f32, f32, f32]),
+        "orc_sample_dispersion_wavelength": (f32, [f32, vp, vp]),
+        "orc_sample_camera_channel_wavelength": (f32, [i32, f32]),
+        "orc_camera_wavelength_sampling_pdf": (f32, [f32, vp]),
+        "orc_camera_rgb_basis_at": (None, [f32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -511,11 +520,12 @@ OPENPBR_FIELDS = [
     ("coat_roughness_anisotropy", 1, 0.0), ("coat_ior", 1, 1.6), ("coat_darkening", 1, 1.0),
     ("thin_film_weight", 1, 0.0), ("thin_film_thickness", 1, 0.5), ("thin_film_ior", 1, 1.4),
     ("emission_luminance", 1, 0.0), ("emission_color", 3, 1.0), ("geometry_opacity", 1, 1.0),
-    ("geometry_thin_walled", 1, 0),
+    ("geometry_thin_walled", 1, 0), ("transmission_dispersion_scale", 1, 0.0),
+    ("transmission_dispersion_abbe_number", 1, 20.0),
 ]
 OPENPBR_DTYPE = np.dtype([(n, "<u4" if n == "geometry_thin_walled" else "<f4", (k,) if k > 1 else ())
                           for n, k, _ in OPENPBR_FIELDS])
-assert OPENPBR_DTYPE.itemsize == 43 * 4
+assert OPENPBR_DTYPE.itemsize == 45 * 4
 
 # OpenPbrBsdfParams as the flat float array of orc_openpbr_params_* (order of
 # the oracle's OpenPbrParams; front_face last, as 0/1).
@@ -527,7 +537,8 @@ OPENPBR_PARAM_FIELDS = [
     ("transmission_alpha_x", 1), ("transmission_alpha_y", 1),
     ("diffuse_roughness", 1), ("subsurface", 1), ("subsurface_color", 3), ("thin_walled", 1),
     ("thin_film_weight", 1), ("thin_film_thickness", 1), ("thin_film_ior", 1), ("metal_n", 3), ("metal_k", 3),
-    ("front_face", 1),
+    ("front_face", 1), ("transmission_dispersion_abbe", 1), ("path_throughput", 3), ("has_lock", 1),
+    ("wavelength_lock", 1),
 ]
 
 
@@ -551,6 +562,11 @@ def pack_openpbr_params(p: dict) -> np.ndarray:
     p.setdefault("thin_film_ior", 1.5)
     p.setdefault("metal_n", 0.0)
     p.setdefault("metal_k", 0.0)
+    p.setdefault("transmission_dispersion_abbe", 0.0)
+    p.setdefault("path_throughput", 1.0)
+    lock = p.get("wavelength_lock")
+    p["has_lock"] = 0.0 if lock is None else 1.0
+    p["wavelength_lock"] = 0.0 if lock is None else float(lock)
     out = []
     for name, k in OPENPBR_PARAM_FIELDS:
         v = p[name]
@@ -583,8 +599,17 @@ def _v3(a):
 def _unpack_sample(ok, out):
     if not ok:
         return None
-    return {"weight": out[0:3].copy(), "wi": out[3:6].copy(), "pdf": float(out[6]), "pdf_rev": float(out[7]),
-            "flags": int(out[8:9].view(np.uint32)[0])}
+    r = {"weight": out[0:3].copy(), "wi": out[3:6].copy(), "pdf": float(out[6]), "pdf_rev": float(out[7]),
+         "flags": int(out[8:9].view(np.uint32)[0])}
+    if len(out) > 9:
+        r["wavelength_lock"] = None if np.isnan(out[9]) else float(out[9])
+    return r
+
+
+def _state(throughput, lock):
+    """Path state of a shading vertex: throughput (3) and lock (NaN = None)."""
+    t = np.broadcast_to(np.asarray(throughput, np.float32), (3,))
+    return np.ascontiguousarray(np.append(t, np.float32(np.nan if lock is None else lock)), np.float32)
 
 
 class OpenPbrParamsBsdf:
@@ -614,10 +639,17 @@ class OpenPbrParamsBsdf:
                                             len(wis), mode, _p(f), _p(pdf))
         return f, pdf
 
-    def sample(self, wo, u_lobe, u_dir, mode=0):
-        out = np.zeros(9, np.float32)
-        ok = lib().orc_openpbr_params_sample(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)), float(u_lobe),
-                                             float(u_dir[0]), float(u_dir[1]), mode, _p(out))
+    def sample(self, wo, u_lobe, u_dir, mode=0, u_extra=None):
+        if u_extra is None:
+            out = np.zeros(9, np.float32)
+            ok = lib().orc_openpbr_params_sample(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)),
+                                                 float(u_lobe), float(u_dir[0]), float(u_dir[1]), mode, _p(out))
+            return _unpack_sample(ok, out)
+        out = np.zeros(10, np.float32)
+        ue = np.ascontiguousarray(u_extra, np.float32).reshape(4)
+        ok = lib().orc_openpbr_params_sample_ex(_p(self.flat), self.mode, self.se, self.ce, _p(_v3(wo)),
+                                                float(u_lobe), float(u_dir[0]), float(u_dir[1]), _p(ue), mode,
+                                                _p(out))
         return _unpack_sample(ok, out)
 
 
@@ -660,13 +692,15 @@ class OpenPbrMaterial:
         if why:
             raise ValueError(why.decode())
 
-    def eval(self, wo, wi, front=True, mode=0):
+    def eval(self, wo, wi, front=True, mode=0, throughput=1.0, lock=None):
         out = np.zeros(3, np.float32)
-        lib().orc_openpbr_eval(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)), mode, _p(out))
+        st = _state(throughput, lock)
+        lib().orc_openpbr_eval_ex(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)), _p(st), mode, _p(out))
         return out
 
-    def pdf(self, wo, wi, front=True):
-        return lib().orc_openpbr_pdf(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)))
+    def pdf(self, wo, wi, front=True, throughput=1.0, lock=None):
+        st = _state(throughput, lock)
+        return lib().orc_openpbr_pdf_ex(_p(self.rec), int(front), _p(_v3(wo)), _p(_v3(wi)), _p(st))
 
     def le(self, wo, front=True):
         """Emitted radiance toward the local direction wo, or None."""
@@ -674,8 +708,38 @@ class OpenPbrMaterial:
         ok = lib().orc_openpbr_le(_p(self.rec), int(front), _p(_v3(wo)), _p(out))
         return out if ok else None
 
-    def sample(self, wo, u_lobe, u_dir, front=True, mode=0):
-        out = np.zeros(9, np.float32)
-        ok = lib().orc_openpbr_sample(_p(self.rec), int(front), _p(_v3(wo)), float(u_lobe), float(u_dir[0]),
-                                      float(u_dir[1]), mode, _p(out))
+    def sample(self, wo, u_lobe, u_dir, front=True, mode=0, u_extra=(0.0, 0.0, 0.0, 0.0), throughput=1.0,
+               lock=None):
+        """One sample; the result carries the wavelength lock it sets (None: none)."""
+        out = np.zeros(10, np.float32)
+        ue = np.ascontiguousarray(u_extra, np.float32).reshape(4)
+        st = _state(throughput, lock)
+        ok = lib().orc_openpbr_sample_ex(_p(self.rec), int(front), _p(_v3(wo)), float(u_lobe), float(u_dir[0]),
+                                         float(u_dir[1]), _p(ue), _p(st), mode, _p(out))
         return _unpack_sample(ok, out)
+
+
+# bsdf/dispersion.rs
+def cauchy_ior(lambda_nm, n_d, abbe):
+    return lib().orc_cauchy_ior(float(lambda_nm), float(n_d), float(abbe))
+
+
+def sample_dispersion_wavelength(u, throughput=(1.0, 1.0, 1.0)):
+    """(lambda, camera basis / pdf) of sample_dispersion_wavelength_weighted."""
+    basis = np.zeros(3, np.float32)
+    lam = lib().orc_sample_dispersion_wavelength(float(u), _p(_v3(throughput)), _p(basis))
+    return lam, basis
+
+
+def sample_camera_channel_wavelength(channel, u):
+    return lib().orc_sample_camera_channel_wavelength(int(channel), float(u))
+
+
+def camera_wavelength_sampling_pdf(lambda_nm, throughput=(1.0, 1.0, 1.0)):
+    return lib().orc_camera_wavelength_sampling_pdf(float(lambda_nm), _p(_v3(throughput)))
+
+
+def camera_rgb_basis_at(lambda_nm):
+    out = np.zeros(3, np.float32)
+    lib().orc_camera_rgb_basis_at(float(lambda_nm), _p(out))
+    return out

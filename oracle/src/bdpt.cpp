@@ -157,6 +157,8 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
   Vec3 ro = ray0.origin, rd = ray0.direction;
   bool count_emission = true;
   bool have_pending = false;
+  bool has_lock = false;
+  float lock = 0.0f;
   Vec3 pending_from;
   float pending_pdf = 0.0f;
   const bool non_area = scene_has_non_area_lights(s);
@@ -169,6 +171,10 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
       break;
     }
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
+    // the path state the vertex keeps for its connections (bdpt.rs:177-178, 344-345)
+    v.path_throughput = beta;
+    v.has_lock = has_lock;
+    v.wavelength_lock = lock;
     const Material& m = s.mat_of(h.instance);
     PathVertex pv;
     pv.light = false;
@@ -194,6 +200,10 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
     ro = offset_origin(v.p, v.ng, smp.wi);
     rd = smp.wi;
     beta *= smp.weight;
+    if (smp.has_lock) {
+      has_lock = true;
+      lock = smp.wavelength_lock;
+    }
     if (depth + 1 >= 4) {
       float q = clampf(max_element(beta), 0.05f, 1.0f);
       if (rnd.u_rr > q) break;
@@ -258,11 +268,17 @@ void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_dep
   Vec3 pending_from = lv.p;
   float pending_pdf = pdf_dir;
   bool have_pending = true;
+  bool has_lock = false;
+  float lock = 0.0f;
   for (uint32_t depth = 1; depth < max_depth; ++depth) {
     VertexRandoms rnd = sp.path_vertex_randoms(depth);
     SceneHit h;
     if (!closest(s, ro, rd, &h)) break;
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
+    // the path state the vertex keeps for its connections (bdpt.rs:177-178, 344-345)
+    v.path_throughput = beta;
+    v.has_lock = has_lock;
+    v.wavelength_lock = lock;
     const Material& m = s.mat_of(h.instance);
     PathVertex pv;
     pv.light = false;
@@ -280,6 +296,10 @@ void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_dep
     ro = offset_origin(v.p, v.ng, smp.wi);
     rd = smp.wi;
     beta *= smp.weight;
+    if (smp.has_lock) {
+      has_lock = true;
+      lock = smp.wavelength_lock;
+    }
     pending_from = v.p;
     pending_pdf = smp.pdf;
     have_pending = true;

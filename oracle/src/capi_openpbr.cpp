@@ -3,6 +3,7 @@
 #include <cstring>
 #include <thread>
 
+#include "dispersion.h"
 #include "render.h"
 
 using namespace orc;
@@ -52,7 +53,19 @@ OpenPbrParams params_from_flat(const float* f) {
   p.metal_n = v3();
   p.metal_k = v3();
   p.front_face = f[i++] != 0.0f;
+  p.transmission_dispersion_abbe = f[i++];
+  p.path_throughput = v3();
+  p.has_lock = f[i++] != 0.0f;
+  p.wavelength_lock = f[i++];
   return p;
+}
+
+// path state (throughput r, g, b, wavelength lock; NaN = no lock) onto params
+void apply_state(OpenPbrBsdf& b, const float* state) {
+  if (!state) return;
+  b.p.path_throughput = Vec3(state[0], state[1], state[2]);
+  b.p.has_lock = !std::isnan(state[3]);
+  b.p.wavelength_lock = b.p.has_lock ? state[3] : 0.0f;
 }
 
 // The constant tables of the reference's OpenPBR unit tests
@@ -97,15 +110,19 @@ OpenPbrBsdf bsdf_from_desc(const OpenPbrDesc* m, int front, const float* wo) {
 
 void put3(float* o, Vec3 v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
 
-int do_sample(const OpenPbrBsdf& b, const float* wo, float u_lobe, float u0, float u1, int mode, float* out9) {
+// out: weight (3), wi (3), pdf, pdf_rev, flags (bits), then with u_extra the
+// sampled wavelength lock (NaN = none) as a tenth value
+int do_sample(const OpenPbrBsdf& b, const float* wo, float u_lobe, float u0, float u1, int mode, float* out,
+              const float* u_extra = nullptr) {
   BsdfSample s;
-  if (!b.sample(Vec3(wo[0], wo[1], wo[2]), u_lobe, Vec2(u0, u1), (TransportMode)mode, &s)) return 0;
-  put3(out9, s.weight);
-  put3(out9 + 3, s.wi);
-  out9[6] = s.pdf;
-  out9[7] = s.pdf_rev;
+  if (!b.sample(Vec3(wo[0], wo[1], wo[2]), u_lobe, Vec2(u0, u1), (TransportMode)mode, &s, u_extra)) return 0;
+  put3(out, s.weight);
+  put3(out + 3, s.wi);
+  out[6] = s.pdf;
+  out[7] = s.pdf_rev;
   uint32_t fl = s.flags;
-  std::memcpy(out9 + 8, &fl, 4);
+  std::memcpy(out + 8, &fl, 4);
+  if (u_extra) out[9] = s.has_lock ? s.wavelength_lock : std::nanf("");
   return 1;
 }
 }  // namespace
@@ -227,6 +244,43 @@ int orc_openpbr_le(const void* desc, int front, const float* wo, float* out3) {
   put3(out3, le);
   return 1;
 }
+
+// The same queries with the path state a shading vertex carries (throughput,
+// wavelength lock) and the dispersion randoms u_extra0..3.
+void orc_openpbr_eval_ex(const void* desc, int front, const float* wo, const float* wi, const float* state, int mode,
+                         float* out3) {
+  OpenPbrBsdf b = bsdf_from_desc((const OpenPbrDesc*)desc, front, wo);
+  apply_state(b, state);
+  put3(out3, b.eval(Vec3(wo[0], wo[1], wo[2]), Vec3(wi[0], wi[1], wi[2]), (TransportMode)mode));
+}
+float orc_openpbr_pdf_ex(const void* desc, int front, const float* wo, const float* wi, const float* state) {
+  OpenPbrBsdf b = bsdf_from_desc((const OpenPbrDesc*)desc, front, wo);
+  apply_state(b, state);
+  return b.pdf(Vec3(wo[0], wo[1], wo[2]), Vec3(wi[0], wi[1], wi[2]));
+}
+int orc_openpbr_sample_ex(const void* desc, int front, const float* wo, float u_lobe, float u0, float u1,
+                          const float* u_extra, const float* state, int mode, float* out10) {
+  OpenPbrBsdf b = bsdf_from_desc((const OpenPbrDesc*)desc, front, wo);
+  apply_state(b, state);
+  return do_sample(b, wo, u_lobe, u0, u1, mode, out10, u_extra);
+}
+int orc_openpbr_params_sample_ex(const float* params, int lut_mode, float spec_eta, float coat_eta, const float* wo,
+                                 float u_lobe, float u0, float u1, const float* u_extra, int mode, float* out10) {
+  return do_sample(bsdf_from(params, lut_mode, spec_eta, coat_eta), wo, u_lobe, u0, u1, mode, out10, u_extra);
+}
+// bsdf/dispersion.rs entry points (their unit tests restated in tests/)
+float orc_cauchy_ior(float lambda_nm, float n_d, float abbe) { return cauchy_ior(lambda_nm, n_d, abbe); }
+float orc_sample_dispersion_wavelength(float u, const float* throughput, float* basis3) {
+  Vec3 b;
+  const float l = sample_dispersion_wavelength_weighted(u, Vec3(throughput[0], throughput[1], throughput[2]), &b);
+  put3(basis3, b);
+  return l;
+}
+float orc_sample_camera_channel_wavelength(int channel, float u) { return sample_camera_channel_wavelength(channel, u); }
+float orc_camera_wavelength_sampling_pdf(float lambda_nm, const float* throughput) {
+  return camera_wavelength_sampling_pdf(lambda_nm, Vec3(throughput[0], throughput[1], throughput[2]));
+}
+void orc_camera_rgb_basis_at(float lambda_nm, float* out3) { put3(out3, camera_rgb_basis_at(lambda_nm)); }
 
 // Scene material: OpenPBR parameters of material `index` (kind must be 2).
 const char* orc_render_scene_set_openpbr(void* h, uint32_t index, const void* desc) {

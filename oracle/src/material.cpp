@@ -32,7 +32,11 @@ float lambert_bsdf_pdf(Vec3 wo, Vec3 wi) {  // bsdf/normalized_lambert.rs:27-33
   return fmax_num(wi.z, 0.0f) / kPi;
 }
 OpenPbrBsdf make_bsdf(const Material& m, const Vertex& v, Vec3 wo_l) {
-  return OpenPbrBsdf{make_openpbr_params(m.openpbr, v.front_face, wo_l), m.luts};
+  OpenPbrBsdf b{make_openpbr_params(m.openpbr, v.front_face, wo_l), m.luts};
+  b.p.path_throughput = v.path_throughput;
+  b.p.has_lock = v.has_lock;
+  b.p.wavelength_lock = v.wavelength_lock;
+  return b;
 }
 }  // namespace
 
@@ -91,7 +95,8 @@ bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& 
     Vec3 wo_l = normalize_or_zero(v.frame.to_local(v.wo));
     if (wo_l.z <= 0.0f) return false;
     BsdfSample bs;
-    if (!make_bsdf(m, v, wo_l).sample(wo_l, r.u_lobe, r.u_dir, mode, &bs)) return false;
+    const float u_extra[4] = {r.u_extra0, r.u_extra1, r.u_extra2, r.u_extra3};
+    if (!make_bsdf(m, v, wo_l).sample(wo_l, r.u_lobe, r.u_dir, mode, &bs, u_extra)) return false;
     Vec3 wi = v.frame.to_world(bs.wi);
     // material/open_pbr.rs:523-531: transmission must leave below the geometric
     // surface (delta transmission is kept either way), reflection above it
@@ -105,6 +110,8 @@ bool material_sample(const Material& m, const Vertex& v, const MaterialRandoms& 
     s->wi = wi;
     s->pdf = bs.pdf;
     s->pdf_rev = bs.pdf_rev;
+    s->has_lock = bs.has_lock;
+    s->wavelength_lock = bs.wavelength_lock;
     return true;
   }
   return false;  // Emissive: pure emitter

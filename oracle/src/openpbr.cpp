@@ -1,6 +1,7 @@
 // Oracle: OpenPBR BSDF and its lobes (bsdf/open_pbr.rs, bsdf/eon.rs) and the
 // untextured material lowering (material/open_pbr.rs).
 #include "openpbr.h"
+#include "dispersion.h"
 
 #include <cstring>
 
@@ -549,9 +550,9 @@ struct Impl {
     return filmed_dielectric(Vec3::splat(base_dielectric_fresnel(c, p.transmission_eta, p.specular_eta)), c,
                              p.specular_eta);
   }
-  Vec3 btdf_fresnel(float c) const {
-    Vec3 no_film = Vec3::splat(base_dielectric_fresnel(c, p.transmission_eta, p.specular_eta));
-    return p.thin_walled ? no_film : filmed_dielectric(no_film, c, p.specular_eta);
+  Vec3 btdf_fresnel(float c, float eta_ph, float eta_pr) const {
+    Vec3 no_film = Vec3::splat(base_dielectric_fresnel(c, eta_ph, eta_pr));
+    return p.thin_walled ? no_film : filmed_dielectric(no_film, c, eta_pr);
   }
   Vec3 eval_spec_brdf(Vec3 wo, Vec3 wi) const {
     if (wo.z <= 0.0f || wi.z <= 0.0f) return Vec3(0, 0, 0);
@@ -632,7 +633,45 @@ struct Impl {
     float scale = trans_scale(mode, m.eta_rel);
     return (1.0f - m.ratio_r) * (1.0f - e_o) * (1.0f - e_i) * scale / (kPi * m.one_minus_e_avg_t);
   }
-  float eta_rel_t() const { return p.front_face ? 1.0f / p.transmission_eta : p.transmission_eta; }
+  // dispersion (open_pbr.rs:1223-1253): the etas at the path's locked
+  // wavelength, and whether an unlocked path integrates over the camera basis
+  bool dispersive() const { return p.transmission_dispersion_abbe > 0.0f; }
+  float eta_used() const {
+    return p.has_lock && dispersive() ? cauchy_ior(p.wavelength_lock, p.transmission_eta, p.transmission_dispersion_abbe)
+                                      : p.transmission_eta;
+  }
+  float fresnel_eta_used() const {
+    return p.has_lock && dispersive() ? cauchy_ior(p.wavelength_lock, p.specular_eta, p.transmission_dispersion_abbe)
+                                      : p.specular_eta;
+  }
+  float eta_rel_t() const {
+    const float eta = eta_used();
+    return p.front_face ? 1.0f / eta : eta;
+  }
+  bool camera_dispersion() const { return dispersive() && p.front_face && !btdf_smooth(); }
+  struct Channel {
+    float lambda;
+    int color;
+    float probability;
+  };
+  // sampled_dispersion_channels / pick_dispersion_channel (open_pbr.rs:1314-1354)
+  void dispersion_channels(const float* u_rgb, Channel* ch) const {
+    const Vec3 t = vmax(p.path_throughput, Vec3(0, 0, 0));
+    const Vec3 w = max_element(t) > 0.0f ? t : Vec3(1, 1, 1);
+    const float sum = fmax_num(w.x + w.y + w.z, 1.0e-8f);
+    ch[0] = Channel{sample_camera_channel_wavelength(0, u_rgb[0]), 0, w.x / sum};
+    ch[1] = Channel{sample_camera_channel_wavelength(1, u_rgb[1]), 1, w.y / sum};
+    ch[2] = Channel{sample_camera_channel_wavelength(2, u_rgb[2]), 2, w.z / sum};
+  }
+  static Channel pick_channel(const Channel* ch, float u) {
+    u = clampf(u, 0.0f, 1.0f);
+    for (int k = 0; k < 3; ++k) {
+      if (u <= ch[k].probability) return ch[k];
+      u -= ch[k].probability;
+    }
+    return ch[2];
+  }
+  static Vec3 unit(int c) { return Vec3(c == 0 ? 1.0f : 0.0f, c == 1 ? 1.0f : 0.0f, c == 2 ? 1.0f : 0.0f); }
   // eval_spec_btdf_scalar_with_eta (open_pbr.rs:1074-1117): false for None
   bool btdf_scalar(Vec3 wo, Vec3 wi, float eta_rel, TransportMode mode, float* scalar, float* cos_wo_wm) const {
     Vec3 wmu = eta_rel * wo + wi;
@@ -676,11 +715,49 @@ struct Impl {
     if (p.thin_walled) return eval_thin_btdf(wo, wi);
     if (wo.z <= 0.0f || wi.z >= 0.0f) return Vec3(0, 0, 0);
     float scalar, co;
+    if (camera_dispersion() && !p.has_lock) return eval_btdf_camera(wo, wi, mode);
     if (!btdf_scalar(wo, wi, eta_rel_t(), mode, &scalar, &co)) return Vec3(0, 0, 0);
-    Vec3 f = btdf_fresnel(co);
+    const float eta_fr = fresnel_eta_used();
+    Vec3 f = btdf_fresnel(co, eta_used(), eta_fr);
     Vec3 ss = vmax(Vec3(1, 1, 1) - f, Vec3(0, 0, 0)) * scalar;
-    Vec3 ms = Vec3::splat(eval_trans_ms(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y, p.specular_eta, mode));
+    Vec3 ms = Vec3::splat(eval_trans_ms(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y, eta_fr, mode));
     return ss + ms;
+  }
+  // eval_spec_btdf_camera_integrated (open_pbr.rs:1255-1289): the BTDF summed
+  // over the 32 camera intervals at their midpoint wavelengths
+  Vec3 eval_btdf_camera(Vec3 wo, Vec3 wi, TransportMode mode) const {
+    Vec3 value(0, 0, 0);
+    for (int i = 0; i < kSpectralIntervals; ++i) {
+      const float lambda = camera_spectral_interval_midpoint_nm(i);
+      const float eta = cauchy_ior(lambda, p.transmission_eta, p.transmission_dispersion_abbe);
+      const float eta_fr = cauchy_ior(lambda, p.specular_eta, p.transmission_dispersion_abbe);
+      const float eta_rel = p.front_face ? 1.0f / eta : eta;
+      Vec3 ss(0, 0, 0);
+      float scalar, co;
+      if (btdf_scalar(wo, wi, eta_rel, mode, &scalar, &co))
+        ss = vmax(Vec3(1, 1, 1) - btdf_fresnel(co, eta, eta_fr), Vec3(0, 0, 0)) * scalar;
+      const Vec3 ms =
+          Vec3::splat(eval_trans_ms(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y, eta_fr, mode));
+      value += camera_rgb_basis_at(lambda) * (ss + ms) * kLambdaStepNm;
+    }
+    return value;
+  }
+  // eval_spec_btdf_sampled_channels (open_pbr.rs:1356-1397)
+  Vec3 eval_btdf_channels(Vec3 wo, Vec3 wi, const Channel* ch, TransportMode mode) const {
+    Vec3 value(0, 0, 0);
+    for (int k = 0; k < 3; ++k) {
+      if (ch[k].probability <= 0.0f) continue;
+      const float eta = cauchy_ior(ch[k].lambda, p.transmission_eta, p.transmission_dispersion_abbe);
+      const float eta_fr = cauchy_ior(ch[k].lambda, p.specular_eta, p.transmission_dispersion_abbe);
+      const float eta_rel = p.front_face ? 1.0f / eta : eta;
+      const Vec3 color = unit(ch[k].color);
+      float ss = 0.0f, scalar, co;
+      if (btdf_scalar(wo, wi, eta_rel, mode, &scalar, &co))
+        ss = fmax_num(1.0f - dot(btdf_fresnel(co, eta, eta_fr), color), 0.0f) * scalar;
+      const float ms = eval_trans_ms(wo, wi, p.transmission_alpha_x, p.transmission_alpha_y, eta_fr, mode);
+      value += color * (ss + ms);
+    }
+    return value;
   }
   // pdf_specular_btdf_ss_with_eta (open_pbr.rs:1193-1222)
   float pdf_btdf_ss(Vec3 wo, Vec3 wi, float eta_rel) const {
@@ -711,11 +788,41 @@ struct Impl {
       return denom > 0.0f ? pdf_wm / denom : 0.0f;
     }
     if (wo.z <= 0.0f || wi.z >= 0.0f) return 0.0f;
-    MsParams m = ms_params(p.transmission_alpha_x, p.transmission_alpha_y, p.transmission_eta);
+    if (camera_dispersion() && !p.has_lock) return pdf_btdf_camera(wo, wi);
+    return pdf_btdf_with_eta(wo, wi, eta_rel_t(), eta_used());
+  }
+  float pdf_btdf_with_eta(Vec3 wo, Vec3 wi, float eta_rel, float eta) const {
+    if (wo.z <= 0.0f || wi.z >= 0.0f) return 0.0f;
+    MsParams m = ms_params(p.transmission_alpha_x, p.transmission_alpha_y, eta);
     TwoLobe w = transmission_lobe_weights(m);
-    float pdf_ss = pdf_btdf_ss(wo, wi, eta_rel_t());
+    float pdf_ss = pdf_btdf_ss(wo, wi, eta_rel);
     float pdf_ms = cosine_pdf(-wi.z);
     return (w.ss * pdf_ss + w.ms * pdf_ms) / w.total;
+  }
+  // pdf_specular_btdf_camera_mixture (open_pbr.rs:1291-1312)
+  float pdf_btdf_camera(Vec3 wo, Vec3 wi) const {
+    float pdf = 0.0f;
+    for (int i = 0; i < kSpectralIntervals; ++i) {
+      const float lambda = camera_spectral_interval_midpoint_nm(i);
+      const float eta = cauchy_ior(lambda, p.transmission_eta, p.transmission_dispersion_abbe);
+      const float eta_fr = cauchy_ior(lambda, p.specular_eta, p.transmission_dispersion_abbe);
+      const float eta_rel = p.front_face ? 1.0f / eta : eta;
+      const float p_lambda = camera_wavelength_sampling_pdf(lambda, p.path_throughput);
+      pdf += p_lambda * pdf_btdf_with_eta(wo, wi, eta_rel, eta_fr) * kLambdaStepNm;
+    }
+    return pdf;
+  }
+  // pdf_specular_btdf_sampled_channel_mixture (open_pbr.rs:1399-1427)
+  float pdf_btdf_channels(Vec3 wo, Vec3 wi, const Channel* ch) const {
+    float pdf = 0.0f;
+    for (int k = 0; k < 3; ++k) {
+      if (ch[k].probability <= 0.0f) continue;
+      const float eta = cauchy_ior(ch[k].lambda, p.transmission_eta, p.transmission_dispersion_abbe);
+      const float eta_fr = cauchy_ior(ch[k].lambda, p.specular_eta, p.transmission_dispersion_abbe);
+      const float eta_rel = p.front_face ? 1.0f / eta : eta;
+      pdf += ch[k].probability * pdf_btdf_with_eta(wo, wi, eta_rel, eta_fr);
+    }
+    return pdf;
   }
   // eval_diff_btdf / pdf_diff_btdf (open_pbr.rs:1445-1465): thin-walled only
   Vec3 eval_diff_btdf(Vec3 wo, Vec3 wi) const {
@@ -862,8 +969,53 @@ struct Impl {
     *out = wi;
     return true;
   }
-  // sample_spec_btdf (open_pbr.rs:1670-1836) without dispersion
-  bool sample_spec_btdf(Vec3 wo, Vec2 us, float p_lobe, TransportMode mode, BsdfSample* out) const {
+  // sample_spec_btdf_camera_channels (open_pbr.rs:1838-1928): one of three
+  // per-channel wavelengths picked by throughput, the direction sampled at its
+  // eta, weighted by the three-channel BTDF over the channel-mixture pdf
+  bool sample_btdf_channels(Vec3 wo, Vec2 us, float p_lobe, float u_pick, const float* u_rgb, TransportMode mode,
+                            BsdfSample* out) const {
+    Channel ch[3];
+    dispersion_channels(u_rgb, ch);
+    const Channel c = pick_channel(ch, u_pick);
+    if (c.probability <= 0.0f) return false;
+    const float eta_u = cauchy_ior(c.lambda, p.transmission_eta, p.transmission_dispersion_abbe);
+    const float eta_fr = cauchy_ior(c.lambda, p.specular_eta, p.transmission_dispersion_abbe);
+    const float eta_rel = p.front_face ? 1.0f / eta_u : eta_u;
+    MsParams m = ms_params(p.transmission_alpha_x, p.transmission_alpha_y, eta_fr);
+    TwoLobe w = transmission_lobe_weights(m);
+    float ss_p = w.ss / w.total;
+    Vec3 wi;
+    if (us.x >= ss_p) {
+      float u = ss_p < 1.0f ? (us.x - ss_p) / (1.0f - ss_p) : 0.0f;
+      Vec3 up = sample_cosine_hemisphere(Vec2(u, us.y));
+      wi = Vec3(up.x, up.y, -up.z);
+    } else {
+      float u = ss_p > 0.0f ? us.x / ss_p : 0.0f;
+      Vec3 wm;
+      if (!sample_wm_vndf(wo, p.transmission_alpha_x, p.transmission_alpha_y, Vec2(u, us.y), &wm)) return false;
+      if (dot(wo, wm) <= 0.0f) return false;
+      if (!refract_about(wo, wm, eta_rel, &wi)) return false;
+      if (wi.z >= 0.0f) return false;
+    }
+    if (wi.z >= 0.0f) return false;
+    Vec3 bw = layer_weights(wo, &wi).spec_btdf;
+    float pdf_total = p_lobe * pdf_btdf_channels(wo, wi, ch);
+    if (pdf_total <= 0.0f) return false;
+    Vec3 f = eval_btdf_channels(wo, wi, ch, mode);
+    out->weight = bw * f * (std::fabs(wi.z) / pdf_total);
+    out->wi = wi;
+    out->pdf = pdf_total;
+    out->pdf_rev = pdf(wi, wo);
+    out->flags = kGlossy | kTransmission;
+    out->eta = eta_rel;
+    out->has_lock = true;
+    out->wavelength_lock = c.lambda;
+    return true;
+  }
+  // sample_spec_btdf (open_pbr.rs:1670-1836): u_aux draws the wavelength of a
+  // smooth dispersive refraction, u_rgb the per-channel wavelengths of a rough one
+  bool sample_spec_btdf(Vec3 wo, Vec2 us, float p_lobe, float u_aux, const float* u_rgb, TransportMode mode,
+                        BsdfSample* out) const {
     if (p.thin_walled) {
       Vec3 R, T;
       thin_wall_coeffs(std::fabs(wo.z), &R, &T);
@@ -897,15 +1049,33 @@ struct Impl {
       out->eta = 1.0f;
       return true;
     }
-    const float eta_used = p.transmission_eta, eta_fresnel = p.specular_eta;
+    if (camera_dispersion() && !p.has_lock) return sample_btdf_channels(wo, us, p_lobe, u_aux, u_rgb, mode, out);
+    float eta_used = p.transmission_eta;
+    Vec3 dispersion_basis(1, 1, 1);
+    bool fresh = false;
+    float fresh_lambda = 0.0f;
+    if (dispersive()) {
+      if (p.has_lock) {
+        eta_used = cauchy_ior(p.wavelength_lock, p.transmission_eta, p.transmission_dispersion_abbe);
+      } else if (p.front_face) {
+        fresh_lambda = sample_dispersion_wavelength_weighted(u_aux, p.path_throughput, &dispersion_basis);
+        eta_used = cauchy_ior(fresh_lambda, p.transmission_eta, p.transmission_dispersion_abbe);
+        fresh = true;
+      }
+    }
+    float eta_fresnel = p.specular_eta;
+    if ((fresh || p.has_lock) && dispersive())
+      eta_fresnel = cauchy_ior(fresh ? fresh_lambda : p.wavelength_lock, p.specular_eta, p.transmission_dispersion_abbe);
     const float eta_rel = p.front_face ? 1.0f / eta_used : eta_used;
+    out->has_lock = fresh;
+    out->wavelength_lock = fresh_lambda;
     if (btdf_smooth()) {
       Vec3 wi;
       if (!refract_z(wo, eta_rel, &wi)) return false;
       float f = base_dielectric_fresnel(std::fabs(wo.z), eta_used, eta_fresnel);
       float scale = trans_scale(mode, eta_rel);
       Vec3 bw = layer_weights(wo, &wi).spec_btdf;
-      out->weight = (bw * Vec3(1, 1, 1) * (1.0f - f) * scale) / p_lobe;
+      out->weight = (bw * dispersion_basis * (1.0f - f) * scale) / p_lobe;
       out->wi = wi;
       out->pdf = p_lobe;
       out->pdf_rev = 0.0f;
@@ -935,7 +1105,7 @@ struct Impl {
     return finalize(wo, wi, kGlossy | kTransmission, mode, out, eta_rel);
   }
   // open_pbr.rs:298-332 and pick_lobe (open_pbr.rs:2043-2070)
-  bool sample(Vec3 wo, float u_lobe, Vec2 us, TransportMode mode, BsdfSample* out) const {
+  bool sample(Vec3 wo, float u_lobe, Vec2 us, TransportMode mode, BsdfSample* out, const float* u_extra) const {
     if (!(wo.z > 0.0f)) return false;
     LobeProbs q = lobe_probabilities(wo);
     if (q.total <= 0.0f) return false;
@@ -965,7 +1135,7 @@ struct Impl {
         if (!Eon(p.diffuse_roughness).sample(wo, us, &wi)) return false;
         return finalize(wo, wi, kDiffuse | kReflection, mode, out);
       }
-      case kSpecBtdf: return sample_spec_btdf(wo, us, p_lobe, mode, out);
+      case kSpecBtdf: return sample_spec_btdf(wo, us, p_lobe, u_extra[0], u_extra + 1, mode, out);
       default: {  // kDiffBtdf: sample_diff_btdf (open_pbr.rs:1942-1957), thin-walled only
         if (!p.thin_walled) return false;
         Vec3 wi;
@@ -1027,8 +1197,10 @@ float dielectric_fresnel_avg(float eta) {  // material/open_pbr.rs:881-887
 
 Vec3 OpenPbrBsdf::eval(Vec3 wo, Vec3 wi, TransportMode mode) const { return Impl{p, L}.eval(wo, wi, mode); }
 float OpenPbrBsdf::pdf(Vec3 wo, Vec3 wi) const { return Impl{p, L}.pdf(wo, wi); }
-bool OpenPbrBsdf::sample(Vec3 wo, float u_lobe, Vec2 u_dir, TransportMode mode, BsdfSample* out) const {
-  return Impl{p, L}.sample(wo, u_lobe, u_dir, mode, out);
+bool OpenPbrBsdf::sample(Vec3 wo, float u_lobe, Vec2 u_dir, TransportMode mode, BsdfSample* out,
+                         const float* u_extra) const {
+  static const float kZeros[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  return Impl{p, L}.sample(wo, u_lobe, u_dir, mode, out, u_extra ? u_extra : kZeros);
 }
 
 float openpbr_fuzz_albedo(float ndot_v, float roughness) { return zeltner_dir_albedo(ndot_v, roughness); }
@@ -1123,6 +1295,9 @@ OpenPbrParams make_openpbr_params(const OpenPbrDesc& m, bool front_face, Vec3 wo
   p.subsurface = 0.0f;
   p.subsurface_color = vclamp01(Vec3(m.subsurface_color[0], m.subsurface_color[1], m.subsurface_color[2]));
   p.front_face = front_face;
+  // transmission_dispersion_abbe (material/open_pbr.rs:783-790)
+  const float scale = fmax_num(m.transmission_dispersion_scale, 0.0f);
+  p.transmission_dispersion_abbe = scale <= 0.0f ? 0.0f : fmax_num(m.transmission_dispersion_abbe_number, 1.0e-6f) / scale;
   return p;
 }
 

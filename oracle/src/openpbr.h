@@ -9,11 +9,12 @@
 // multiple scattering, rough and smooth), thin-walled surfaces (the two-interface
 // slab of thin_wall_coefficients, the thin-wall BTDF and the diffuse BTDF),
 // coat, fuzz (LTC), with optional anisotropy and smooth (delta) lobes.  Not
-// covered: dispersion (transmission_dispersion_scale is not part of the
-// untextured parameter set here, so dispersion is always off), emission,
-// opacity and textures; the material lowering rejects parameters that would
-// need them.  Thin film (bsdf/thin_film.rs) modulates the specular, metal and
-// transmission Fresnel terms.
+// covered: opacity and textures; the material lowering rejects parameters
+// that would need them.  Thin film (bsdf/thin_film.rs) modulates the specular,
+// metal and transmission Fresnel terms; dispersion (bsdf/dispersion.rs) makes
+// the transmission IOR a Cauchy function of wavelength: camera-integrated
+// evaluation while the path is unlocked, a wavelength lock once a dispersive
+// refraction is sampled.
 #pragma once
 #include "common.h"
 
@@ -51,8 +52,10 @@ struct OpenPbrDesc {
   float emission_color[3];
   float geometry_opacity;
   uint32_t geometry_thin_walled;
+  float transmission_dispersion_scale;
+  float transmission_dispersion_abbe_number;
 };
-static_assert(sizeof(OpenPbrDesc) == 43 * 4, "OpenPbrDesc layout");
+static_assert(sizeof(OpenPbrDesc) == 45 * 4, "OpenPbrDesc layout");
 
 // ---- lookup tables (bsdf/directional_albedo.rs) ------------------------------
 constexpr int kDaCos = 64, kDaPhi = 16, kDaRough = 64, kDaAniso = 16;
@@ -104,6 +107,8 @@ struct BsdfSample {
   Vec3 weight, wi;
   float pdf = 0, pdf_rev = 0, eta = 1;
   uint32_t flags = 0;
+  bool has_lock = false;  // BsdfSample::wavelength_lock is Some(wavelength_lock)
+  float wavelength_lock = 0;
 };
 
 // OpenPbrBsdfParams (bsdf/open_pbr.rs:33-70) restricted to the covered lobes.
@@ -130,6 +135,12 @@ struct OpenPbrParams {
   float thin_film_weight, thin_film_thickness, thin_film_ior;  // thickness in nm
   Vec3 metal_n, metal_k;                                       // artist_friendly_complex_ior
   bool front_face;
+  // dispersion (bsdf/open_pbr.rs:58, 69-70): the Abbe number (0 = off), the
+  // path throughput arriving at the vertex, and the path's wavelength lock
+  float transmission_dispersion_abbe = 0;
+  Vec3 path_throughput = Vec3(1, 1, 1);
+  bool has_lock = false;
+  float wavelength_lock = 0;
 };
 
 // bsdf/thin_film.rs:11-45 and bsdf/conductor_complex.rs:132-147
@@ -149,7 +160,9 @@ struct OpenPbrBsdf {
   OpenPbrLuts L;
   Vec3 eval(Vec3 wo, Vec3 wi, TransportMode mode) const;
   float pdf(Vec3 wo, Vec3 wi) const;
-  bool sample(Vec3 wo, float u_lobe, Vec2 u_dir, TransportMode mode, BsdfSample* out) const;
+  // u_extra: MaterialSampleRandoms::u_extra0..3 (the dispersion randoms); NULL = zeros
+  bool sample(Vec3 wo, float u_lobe, Vec2 u_dir, TransportMode mode, BsdfSample* out,
+              const float* u_extra = nullptr) const;
 };
 
 // EonBsdf (bsdf/eon.rs) with an arbitrary albedo.

@@ -221,6 +221,8 @@ struct MatSample {
   Vec3 weight, wi;
   float pdf;
   bool delta;
+  bool has_lock = false;  // MaterialSample::wavelength_lock
+  float wavelength_lock = 0;
 };
 bool lambert_sample(const Material& m, const Vertex& v, Vec2 u, MatSample* s) {
   Vec3 wo_l = normalize_or_zero(v.frame.to_local(v.wo));
@@ -241,13 +243,17 @@ bool lambert_sample(const Material& m, const Vertex& v, Vec2 u, MatSample* s) {
 
 // OpenPbrMaterial::sample (material/open_pbr.rs:489-563), radiance transport
 // (modified_bsdf_sample_weight leaves the weight unchanged).
-bool openpbr_sample(const Material& m, const Vertex& v, float u_lobe, Vec2 u_dir, MatSample* s) {
+bool openpbr_sample(const Material& m, const Vertex& v, const MaterialRandoms& r, MatSample* s) {
   if (dot(v.wo, v.ng) <= 0.0f) return false;
   Vec3 wo_l = normalize_or_zero(v.frame.to_local(v.wo));
   if (wo_l.z <= 0.0f) return false;
   OpenPbrBsdf b{make_openpbr_params(m.openpbr, v.front_face, wo_l), m.luts};
+  b.p.path_throughput = v.path_throughput;
+  b.p.has_lock = v.has_lock;
+  b.p.wavelength_lock = v.wavelength_lock;
   BsdfSample bs;
-  if (!b.sample(wo_l, u_lobe, u_dir, kRadiance, &bs)) return false;
+  const float u_extra[4] = {r.u_extra0, r.u_extra1, r.u_extra2, r.u_extra3};
+  if (!b.sample(wo_l, r.u_lobe, r.u_dir, kRadiance, &bs, u_extra)) return false;
   Vec3 wi = v.frame.to_world(bs.wi);
   // material/open_pbr.rs:523-531: transmission below the geometric surface
   // (delta transmission kept either way), reflection above it
@@ -260,8 +266,27 @@ bool openpbr_sample(const Material& m, const Vertex& v, float u_lobe, Vec2 u_dir
   s->wi = wi;
   s->pdf = bs.pdf;
   s->delta = (bs.flags & kDelta) != 0;
+  s->has_lock = bs.has_lock;
+  s->wavelength_lock = bs.wavelength_lock;
   return true;
 }
+
+// the path state a vertex sees (mis.rs:54-55, nee.rs:45-46, pt.rs:41-42)
+struct PathLock {
+  bool has = false;
+  float lambda = 0;
+  void stamp(Vertex& v, Vec3 beta) const {
+    v.path_throughput = beta;
+    v.has_lock = has;
+    v.wavelength_lock = lambda;
+  }
+  void take(const MatSample& bs) {
+    if (bs.has_lock) {
+      has = true;
+      lambda = bs.wavelength_lock;
+    }
+  }
+};
 
 Vec3 offset_origin(Vec3 p, Vec3 ng, Vec3 d) {
   Vec3 n = dot(d, ng) >= 0.0f ? ng : -ng;
@@ -642,6 +667,7 @@ Vec3 env_escape(const RenderScene& s, Vec3 dir, bool delta, float bsdf_pdf) {
 // escape counts in full
 Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
   Vec3 L(0, 0, 0), beta(1, 1, 1);
+  PathLock lock;
   Vec3 ro = ray.origin, rd = ray.direction;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
@@ -652,14 +678,16 @@ Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, 
     }
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
     const Material& m = s.mat_of(h.instance);
+    lock.stamp(v, beta);
     Vec3 le;
     if (material_le(m, v, &le)) L += beta * le;
     MatSample bs;
-    bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+    bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material, &bs)
               : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
                                    : false;  // the pure emitter samples nothing
     if (!ok) break;
     beta *= bs.weight;
+    lock.take(bs);
     if (depth + 1 >= 4) {
       float q = clampf(max_element(beta), 0.05f, 1.0f);
       if (rnd.u_rr > q) break;
@@ -676,6 +704,7 @@ Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, 
 // the camera and after delta samples
 Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
   Vec3 L(0, 0, 0), beta(1, 1, 1);
+  PathLock lock;
   Vec3 ro = ray.origin, rd = ray.direction;
   bool count_emission = true;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
@@ -687,15 +716,17 @@ Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
     }
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
     const Material& m = s.mat_of(h.instance);
+    lock.stamp(v, beta);
     Vec3 le;
     if (count_emission && material_le(m, v, &le)) L += beta * le;
     if (!is_pure_emitter(m)) L += beta * direct_light_impl(s, m, v, rnd, nullptr, kDirectNee);
     MatSample bs;
-    bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+    bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material, &bs)
               : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
                                    : false;
     if (!ok) break;
     beta *= bs.weight;
+    lock.take(bs);
     if (depth + 1 >= 4) {
       float q = clampf(max_element(beta), 0.05f, 1.0f);
       if (rnd.u_rr > q) break;
@@ -711,6 +742,7 @@ Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
 // integrator/mis.rs:19-139
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
   Vec3 L(0, 0, 0), beta(1, 1, 1);
+  PathLock lock;
   SceneHit h;
   if (!closest(s, ray.origin, ray.direction, &h)) return s.has_env ? s.env.radiance(ray.direction) : L;
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
@@ -719,13 +751,15 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
   if (material_le(*m, v, &le0)) L += le0;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    lock.stamp(v, beta);
     if (is_pure_emitter(*m)) break;
     L += beta * direct_light(s, *m, v, rnd);
     MatSample bs;
-    bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+    bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material, &bs)
                                   : lambert_sample(*m, v, rnd.material.u_dir, &bs);
     if (!ok) break;
     beta *= bs.weight;
+    lock.take(bs);
     if (depth + 1 >= 4) {
       float q = clampf(max_element(beta), 0.05f, 1.0f);
       if (rnd.u_rr > q) break;
@@ -752,6 +786,7 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
 void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth, Vec3 L,
                 AdjointVertexSink& sink) {
   Vec3 R = L, beta(1, 1, 1);
+  PathLock lock;
   SceneHit h;
   if (!closest(s, ray.origin, ray.direction, &h)) return;
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
@@ -761,6 +796,7 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
   if (material_le(*m, v, &le0)) R = R - le0;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    lock.stamp(v, beta);
     if (is_pure_emitter(*m)) break;
     Vec3 wl(0, 0, 0);
     const Vec3 c = beta * direct_light(s, *m, v, rnd, &wl);
@@ -769,10 +805,11 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
     // contribution scales with f at the light direction
     if (m->kind == kOpenPbr && length_squared(c) > 0.0f) sink.vertex(mi, v, wl, c);
     MatSample bs;
-    bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material.u_lobe, rnd.material.u_dir, &bs)
+    bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material, &bs)
                                   : lambert_sample(*m, v, rnd.material.u_dir, &bs);
     if (!ok) break;
     beta *= bs.weight;
+    lock.take(bs);
     if (depth + 1 >= 4) {
       float q = clampf(max_element(beta), 0.05f, 1.0f);
       if (rnd.u_rr > q) break;

@@ -62,6 +62,11 @@ struct Vertex {
   Frame frame;
   int32_t inst, tri;
   bool front_face;
+  // ShadingVertex::path_throughput / wavelength_lock: set by the integrators
+  // before the vertex is shaded (read by dispersive transmission only)
+  Vec3 path_throughput = Vec3(1, 1, 1);
+  bool has_lock = false;
+  float wavelength_lock = 0;
 };
 
 // scene/mod.rs:48-54: an emissive triangle with its selection weight
@@ -129,6 +134,8 @@ struct MatSampleOut {
   Vec3 weight, wi;
   float pdf = 0, pdf_rev = 0;
   bool delta = false;
+  bool has_lock = false;  // MaterialSample::wavelength_lock
+  float wavelength_lock = 0;
 };
 Vec3 material_eval(const Material& m, const Vertex& v, Vec3 wi, TransportMode mode);
 float material_pdf(const Material& m, const Vertex& v, Vec3 wi);

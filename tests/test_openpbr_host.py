@@ -28,6 +28,8 @@ def test_descriptor_bytes_agree_with_oracle_packing():
 
 def test_field_offsets_follow_the_header():
     names = [n for n, _, _ in tpt.OPENPBR_FIELDS]
-    assert names[0] == "base_weight" and names[-1] == "geometry_thin_walled"
+    assert names[0] == "base_weight" and names[-1] == "transmission_dispersion_abbe_number"
     assert tpt.OpenPbrDesc.base_color.offset == 4
     assert tpt.OpenPbrDesc.geometry_thin_walled.offset == 42 * 4
+    assert tpt.OpenPbrDesc.transmission_dispersion_scale.offset == 43 * 4
+    assert tpt.OpenPbrDesc.transmission_dispersion_abbe_number.offset == 44 * 4

@@ -145,6 +145,9 @@ tpt_status tpt_adjoint_device(tpt_context* ctx, const tpt_render_job* job, const
   const float step = adesc && adesc->fd_step > 0.0f ? adesc->fd_step : kDefaultFdStep;
   if (!(step < 0.5f)) return set_error(ctx, TPT_ERR_INVALID_ARG, "fd_step must be in (0, 0.5)");
   tpt_scene* scene = const_cast<tpt_scene*>(job->scene);
+  for (const tpt_openpbr_desc& d : scene->opbr_desc)
+    if (d.transmission_dispersion_scale > 0.0f && d.transmission_weight > 0.0f)
+      return set_error(ctx, TPT_ERR_INVALID_ARG, "dispersive OpenPBR transmission is not differentiated");
   if (mask & TPT_GRAD_MASK_COAT) {
     // emission leaving through a coat depends on coat_weight, and the replay
     // differentiates the BSDF only

@@ -37,7 +37,9 @@ tpt_status ensure_ec_tables(tpt_context* ctx) {
     return st;
   float *cec = nullptr, *dec = nullptr;
   if ((st = cuda_check(ctx, cudaMalloc(&cec, kCecLen * 4), "cudaMalloc(conductor table)"))) return st;
-  if ((st = cuda_check(ctx, cudaMalloc(&dec, kDecLen * 4), "cudaMalloc(dielectric table)"))) {
+  // the dielectric table with its E_avg behind it (the device's dispersive
+  // BTDF looks up E_avg at arbitrary etas)
+  if ((st = cuda_check(ctx, cudaMalloc(&dec, (kDecLen + kDecAvgLen) * 4), "cudaMalloc(dielectric table)"))) {
     cudaFree(cec);
     return st;
   }
@@ -58,6 +60,12 @@ tpt_status ensure_ec_tables(tpt_context* ctx) {
   ctx->h_dec_e_avg.assign(kDecAvgLen, 0.0f);
   conductor_e_avg(ctx->h_cec_e.data(), ctx->h_cec_e_avg.data());
   dielectric_e_avg(ctx->h_dec_e.data(), ctx->h_dec_e_avg.data());
+  e = cudaMemcpy(dec + kDecLen, ctx->h_dec_e_avg.data(), kDecAvgLen * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(cec);
+    cudaFree(dec);
+    return cuda_check(ctx, e, "dielectric E_avg upload");
+  }
   ctx->d_cec_e = cec;
   ctx->d_dec_e = dec;
   return TPT_OK;
@@ -139,7 +147,7 @@ tpt_status tpt_bsdf_eval_device(tpt_context* ctx, const tpt_scene* scene, uint32
   if (n && (!wo || !wi || !front_face || !f || !pdf)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
   if (mode > 1) return set_error(ctx, TPT_ERR_INVALID_ARG, "mode must be 0 (radiance) or 1 (importance)");
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  return cuda_check(ctx, launch_bsdf_eval(scene->render, material, n, wo, wi, front_face, mode, f, pdf, s),
+  return cuda_check(ctx, launch_bsdf_eval(scene->render, material, n, wo, wi, front_face, mode, nullptr, f, pdf, s),
                     "bsdf eval launch");
 }
 
@@ -151,7 +159,32 @@ tpt_status tpt_bsdf_sample_device(tpt_context* ctx, const tpt_scene* scene, uint
   if (n && (!wo || !u || !front_face || !out)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
   if (mode > 1) return set_error(ctx, TPT_ERR_INVALID_ARG, "mode must be 0 (radiance) or 1 (importance)");
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  return cuda_check(ctx, launch_bsdf_sample(scene->render, material, n, wo, u, front_face, mode, out, s),
+  return cuda_check(ctx, launch_bsdf_sample(scene->render, material, n, wo, u, front_face, mode, nullptr, out, s),
+                    "bsdf sample launch");
+}
+
+tpt_status tpt_bsdf_eval_path_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
+                                     const float* wo, const float* wi, const uint32_t* front_face, const float* state,
+                                     uint32_t mode, float* f, float* pdf, void* stream) {
+  tpt_status st = check_query(ctx, scene, material);
+  if (st) return st;
+  if (n && (!wo || !wi || !front_face || !state || !f || !pdf))
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
+  if (mode > 1) return set_error(ctx, TPT_ERR_INVALID_ARG, "mode must be 0 (radiance) or 1 (importance)");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return cuda_check(ctx, launch_bsdf_eval(scene->render, material, n, wo, wi, front_face, mode, state, f, pdf, s),
+                    "bsdf eval launch");
+}
+
+tpt_status tpt_bsdf_sample_path_device(tpt_context* ctx, const tpt_scene* scene, uint32_t material, uint64_t n,
+                                       const float* wo, const float* u, const uint32_t* front_face, const float* state,
+                                       uint32_t mode, float* out, void* stream) {
+  tpt_status st = check_query(ctx, scene, material);
+  if (st) return st;
+  if (n && (!wo || !u || !front_face || !state || !out)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL buffer");
+  if (mode > 1) return set_error(ctx, TPT_ERR_INVALID_ARG, "mode must be 0 (radiance) or 1 (importance)");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return cuda_check(ctx, launch_bsdf_sample(scene->render, material, n, wo, u, front_face, mode, state, out, s),
                     "bsdf sample launch");
 }
 

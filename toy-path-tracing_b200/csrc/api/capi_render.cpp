@@ -90,8 +90,8 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   const size_t C = capacity;
   // float planes: beta 3, L 3, prev 7, q_ray 2*7, h_t 1, h_bary 3, s_ray 7, s_contrib 3, s_t 1, s_dist 1
   // u32 planes: prev_mat, depth, q_slot 2, h_tri, h_inst, s_slot, s_target 2, s_tri, s_inst,
-  // job, q_job 2, s_job
-  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4;
+  // job, q_job 2, s_job; lock 1
+  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4 + 1;
   const size_t bytes = planes * C * 4 + 256;
   if (ctx->d_wf) {
     cudaDeviceSynchronize();
@@ -116,6 +116,7 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   B.prev = (float*)take(7);
   B.prev_mat = (uint32_t*)take(1);
   B.depth = (uint32_t*)take(1);
+  B.lock = (float*)take(1);
   B.q_slot[0] = (uint32_t*)take(1);
   B.q_slot[1] = (uint32_t*)take(1);
   B.q_ray[0] = (float*)take(7);

@@ -222,11 +222,15 @@ cudaError_t launch_lut_dielectric_albedo(float eta, const float* dirs, const flo
                                          cudaStream_t s);
 cudaError_t launch_lut_conductor_e(const float* u, const float* cs, float* e, cudaStream_t s);
 cudaError_t launch_lut_dielectric_e(const float* uc, const float* ux, const float* cs, float* e, cudaStream_t s);
-// openpbr_query.cu: batched BSDF queries of one material.
+// openpbr_query.cu: batched BSDF queries of one material; `state` (n x 4:
+// path throughput, wavelength lock or NaN) may be NULL (the defaults), and
+// with it u has 7 values per sample (with u_extra0..3) and out 10 (with the lock).
 cudaError_t launch_bsdf_eval(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo, const float* wi,
-                             const uint32_t* front, uint32_t mode, float* f, float* pdf, cudaStream_t s);
+                             const uint32_t* front, uint32_t mode, const float* state, float* f, float* pdf,
+                             cudaStream_t s);
 cudaError_t launch_bsdf_sample(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo,
-                               const float* u, const uint32_t* front, uint32_t mode, float* out, cudaStream_t s);
+                               const float* u, const uint32_t* front, uint32_t mode, const float* state, float* out,
+                               cudaStream_t s);
 
 // scene_render_upload.cpp: materials, shading arrays, light tree, emitter map.
 tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc);

@@ -41,6 +41,8 @@ static __device__ __noinline__ float material_pdf(const DevRender& S, const DevM
     if (wo_l.z <= 0.0f) return 0.0f;
     opbr::OpbrVertex s;
     opbr::init_vertex(s, S.d.openpbr + m.openpbr, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    s.thr = v.thr;
+    s.lock = v.lock;
     V3 f;
     float pdf;
     opbr::eval_pdf(s, s, wi_l, f, pdf);
@@ -53,12 +55,14 @@ struct MatSample {
   V3 weight, wi;
   float pdf, pdf_rev;
   bool delta;
+  float lock;  // wavelength lock set by the sample (< 0: none)
 };
 
 // Material::sample with pdf_rev
 static __device__ __noinline__ bool material_sample_rev(const DevRender& S, const DevMaterialRec& m, const Vertex& v,
-                                                       float u_lobe, float u0, float u1, bool importance,
-                                                       MatSample& s) {
+                                                       float u_lobe, float u0, float u1, const float* ux,
+                                                       bool importance, MatSample& s) {
+  s.lock = -1.0f;
   if (m.kind == kDevLambert) {
     const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
     if (wo_l.z <= 0.0f) return false;
@@ -79,8 +83,11 @@ static __device__ __noinline__ bool material_sample_rev(const DevRender& S, cons
     if (wo_l.z <= 0.0f) return false;
     opbr::OpbrVertex ov;
     opbr::init_vertex(ov, S.d.openpbr + m.openpbr, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    ov.thr = v.thr;
+    ov.lock = v.lock;
     opbr::Sample bs;
-    if (!opbr::sample(ov, u_lobe, u0, u1, bs, importance, true)) return false;
+    if (!opbr::sample(ov, u_lobe, u0, u1, bs, importance, true, ux)) return false;
+    s.lock = bs.lock;
     const V3 wi = to_world(v.frame, bs.wi);
     if (!opbr_sample_side_ok(v, wi, bs.flags)) return false;
     s.delta = (bs.flags & opbr::kFlagDelta) != 0;
@@ -96,9 +103,10 @@ static __device__ __noinline__ bool material_sample_rev(const DevRender& S, cons
 // ---- path vertices ---------------------------------------------------------
 constexpr uint32_t kBdLight = 1u, kBdDelta = 2u, kBdConnectible = 4u;
 
+// beta: v.thr (ShadingVertex::path_throughput is the throughput arriving at
+// the vertex; the light endpoint's is its emitted radiance over its pdf)
 struct BdVertex {
   Vertex v;
-  V3 beta;
   float pdf_fwd, pdf_rev;
   uint32_t flags;
 };
@@ -228,7 +236,7 @@ __device__ __forceinline__ bool bdpt_connect_prepare(const DevRender& S, const B
   if (length_sq(f_light) == 0.0f) return false;
   const float g = fabsf(dot(lv.v.ng, w_lc)) * fabsf(dot(cv.v.ng, w_cl)) / dist2;
   if (g <= 0.0f) return false;
-  out.c = lv.beta * f_light * g * f_cam * cv.beta;
+  out.c = lv.v.thr * f_light * g * f_cam * cv.v.thr;
   out.origin = offset_origin(lv.v.p, lv.v.ng, w_lc);
   out.dir = w_lc;
   out.dist = dist;
@@ -246,11 +254,13 @@ __device__ __forceinline__ bool bdpt_connect_prepare(const DevRender& S, const B
 struct BdCamState {
   V3 beta, pending_from;
   float pending_pdf;
+  float lock;  // the path's wavelength lock (< 0: none)
   uint32_t n;
   bool count_emission, have_pending, alive;
 };
 __device__ __forceinline__ void camera_state_init(BdCamState& c, bool valid) {
   c.beta = V3{1.0f, 1.0f, 1.0f};
+  c.lock = -1.0f;
   c.pending_from = V3{0.0f, 0.0f, 0.0f};
   c.pending_pdf = 0.0f;
   c.n = 0;
@@ -277,11 +287,12 @@ __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaun
     c.alive = false;
     return;
   }
-  const Vertex v = shade_hit<Stack>(S, h, rd);
+  Vertex v = shade_hit<Stack>(S, h, rd);
+  v.thr = c.beta;  // the path state the vertex keeps (bdpt.rs:177-178)
+  v.lock = c.lock;
   const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
   BdVertex& pv = vs[c.n];
   pv.v = v;
-  pv.beta = c.beta;
   pv.pdf_fwd = c.have_pending ? solid_angle_to_area(c.pending_pdf, c.pending_from, v.p, v.ng) : 0.0f;
   pv.pdf_rev = 0.0f;
   pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
@@ -306,11 +317,14 @@ __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaun
   float ud0, ud1;
   ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
   const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
+  float ux[4];
+  extra_randoms(S.d, m, ps, depth, ux);
   MatSample s;
-  if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, false, s)) {
+  if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, ux, false, s)) {
     c.alive = false;
     return;
   }
+  if (s.lock >= 0.0f) c.lock = s.lock;
   pv.flags = s.delta ? kBdDelta : kBdConnectible;
   if (n >= 2) vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
   ro = offset_origin(v.p, v.ng, s.wi);
@@ -401,7 +415,7 @@ __device__ __forceinline__ bool bdpt_light_endpoint(const DevRender& S, const Re
   if (cos_emit <= 0.0f) return false;
   const V3 endpoint_beta = le / pdf_area;
   vs[0].v = lvx;
-  vs[0].beta = endpoint_beta;
+  vs[0].v.thr = endpoint_beta;
   vs[0].pdf_fwd = pdf_area;
   vs[0].pdf_rev = 0.0f;
   vs[0].flags = kBdLight | kBdConnectible;
@@ -417,6 +431,7 @@ __device__ __forceinline__ bool bdpt_light_endpoint(const DevRender& S, const Re
 struct BdLightState {
   V3 beta, pending_from;
   float pending_pdf;
+  float lock;  // the path's wavelength lock (< 0: none)
   uint32_t n;
   bool alive;
 };
@@ -431,11 +446,12 @@ __device__ __forceinline__ void light_step(const DevRender& S, const PathSampler
     l.alive = false;
     return;
   }
-  const Vertex v = shade_hit<Stack>(S, h, rd);
+  Vertex v = shade_hit<Stack>(S, h, rd);
+  v.thr = l.beta;  // bdpt.rs:344-345
+  v.lock = l.lock;
   const DevMaterialRec m = S.d.mats[__ldg(&S.d.inst[v.inst].material)];
   BdVertex& pv = vs[l.n];
   pv.v = v;
-  pv.beta = l.beta;
   pv.pdf_fwd = solid_angle_to_area(l.pending_pdf, l.pending_from, v.p, v.ng);
   pv.pdf_rev = 0.0f;
   pv.flags = m.kind != kDevEmissive ? kBdConnectible : 0u;
@@ -447,11 +463,14 @@ __device__ __forceinline__ void light_step(const DevRender& S, const PathSampler
   float ud0, ud1;
   ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
   const float u_lobe = m.kind == kDevOpenPbr ? ps.sample_1d(vertex_dim(depth, kOffLobe)) : 0.0f;
+  float ux[4];
+  extra_randoms(S.d, m, ps, depth, ux);
   MatSample s;
-  if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, true, s)) {
+  if (!material_sample_rev(S, m, v, u_lobe, ud0, ud1, ux, true, s)) {
     l.alive = false;
     return;
   }
+  if (s.lock >= 0.0f) l.lock = s.lock;
   pv.flags = s.delta ? kBdDelta : kBdConnectible;
   vs[n - 2].pdf_rev = solid_angle_to_area(s.pdf_rev, v.p, vs[n - 2].v.p, vs[n - 2].v.ng);
   ro = offset_origin(v.p, v.ng, s.wi);
@@ -468,6 +487,7 @@ __device__ __forceinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack
   V3 ro, rd;
   BdLightState l;
   l.pending_pdf = 0.0f;
+  l.lock = -1.0f;
   l.alive = valid && bdpt_light_endpoint(S, P, ps, vs, ro, rd, l.beta, l.pending_from, l.pending_pdf);
   l.n = l.alive ? 1u : 0u;
   for (uint32_t depth = 1; depth < P.max_depth; ++depth) {

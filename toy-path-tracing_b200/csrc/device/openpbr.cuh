@@ -13,6 +13,7 @@
 // library is compiled with -fmad=false).
 #pragma once
 #include "render_types.h"
+#include "dispersion.cuh"
 #include "thin_film.h"
 #include "vmath.cuh"
 
@@ -451,6 +452,10 @@ struct OpbrVertex {
   V3 darkening;
   V3 tw_r, tw_t;  // thin_wall_coefficients(|wo.z|) of thin-walled materials
   float q_coat, q_metal, q_spec, q_btdf, q_fuzz, q_diff, q_total;
+  // the path state of the shading vertex (ShadingVertex::path_throughput and
+  // wavelength_lock, lock < 0: none); read by dispersive transmission only
+  V3 thr;
+  float lock;
 };
 
 // LayerWeights below the coat for a given coat tint (open_pbr.rs:334-406);
@@ -554,6 +559,8 @@ static __device__ __noinline__ void init_vertex(OpbrVertex& s, const DevOpenPbr*
   s.wo = wo;
   s.face = front_face ? 0u : 1u;
   s.dk_cos = dk_cos;
+  s.thr = V3{1.0f, 1.0f, 1.0f};
+  s.lock = -1.0f;
   // coat_darkening_factor's view term (material/open_pbr.rs:836-857)
   s.darkening = V3{1.0f, 1.0f, 1.0f};
   if (m.flags & kOpbrDarkening) {
@@ -626,9 +633,166 @@ __device__ __forceinline__ V3 coat_tint(const DevOpenPbr& m, V3 wo, V3 wi) {
             powf(fmaxf(m.coat_color[2], 0.0f), e)};
 }
 
+// ---- dispersion (open_pbr.rs:1223-1427, 1670-1928) --------------------------
+// The transmission eta is a Cauchy function of wavelength.  make_bsdf sets
+// transmission_eta = specular_eta, so the refraction eta and the Fresnel /
+// multiple-scattering eta of one wavelength are the same number here, and the
+// host-lowered constants of the non-dispersive path are replaced by their
+// values at that eta: the Fresnel arguments, dielectric_ms_params'
+// transmission half (over the energy-compensation tables; roughness_eq does
+// not depend on eta, so its table axis is the lowered one).
+__device__ __forceinline__ float f_avg_dielectric(float eta) {  // open_pbr.rs:2183-2191
+  if (eta >= 1.0f) return clampf((eta - 1.0f) / (4.08567f + 1.00071f * eta), 0.0f, 1.0f);
+  const float e = fmaxf(eta, kMsEps);
+  const float v = 0.997118f + 0.1014f * e - 0.965241f * e * e - 0.130607f * e * e * e;
+  return clampf(v, 0.0f, 1.0f);
+}
+__device__ __forceinline__ float dec_eta_to_axis(float eta) {  // directional_albedo.rs:845-853
+  const float kMinInv = 1.0f / 3.0f, kMax = 3.0f;
+  eta = clampf(eta, kMinInv, kMax);
+  if (eta >= 1.0f) return 0.5f + 0.5f * ((eta - 1.0f) / (kMax - 1.0f));
+  const float inv = 1.0f / eta;
+  return 0.5f - 0.5f * ((inv - 1.0f) / (kMax - 1.0f));
+}
+// DielectricGgxEnergyCompensationLut::lookup_e_avg / lookup_e at given axes
+__device__ __forceinline__ float dec_e_avg_at(const float* __restrict__ e_avg, DevLerpAxis r, DevLerpAxis h) {
+  const uint32_t ri[2] = {r.lo, r.hi}, hi[2] = {h.lo, h.hi};
+  const float rw[2] = {1.0f - r.t, r.t}, hw[2] = {1.0f - h.t, h.t};
+  float value = 0.0f;
+#pragma unroll
+  for (int x = 0; x < 2; ++x)
+#pragma unroll
+    for (int y = 0; y < 2; ++y) value += hw[x] * rw[y] * __ldg(e_avg + hi[x] * 32u + ri[y]);
+  return clampf(value, 0.0f, 1.0f);
+}
+__device__ __forceinline__ float dec_e_at(const float* __restrict__ e, DevLerpAxis h, DevLerpAxis r, float cos_theta) {
+  DevMsFace f;
+  f.eta_axis = h;
+  f.r_axis = r;
+  return dec_lookup_e(e, f, cos_theta);
+}
+// dielectric_ms_params (open_pbr.rs:583-636) with the transmission lobe weights (638-646)
+struct TransMs {
+  float eta_rel, one_minus_e_avg_t, ratio_r, ss, ms, total;
+  DevLerpAxis eta_axis, eta_rel_axis;
+};
+__device__ __forceinline__ TransMs trans_ms_at(const OpbrVertex& s, float eta) {
+  TransMs t;
+  const float eta_o = s.face == 0u ? fmaxf(eta, 1.0e-4f) : 1.0f / fmaxf(eta, 1.0e-4f);
+  t.eta_rel = 1.0f / eta_o;
+  const DevLerpAxis r = s.m->ms[0][s.face].r_axis;
+  const float* e_avg = s.dec_e + kDecTableLen;
+  t.eta_axis = axis_lerp(dec_eta_to_axis(eta_o), 32);
+  t.eta_rel_axis = axis_lerp(dec_eta_to_axis(t.eta_rel), 32);
+  const float e_avg_o = dec_e_avg_at(e_avg, r, t.eta_axis);
+  const float e_avg_t = dec_e_avg_at(e_avg, r, t.eta_rel_axis);
+  const float om_o = fmaxf(1.0f - e_avg_o, kMsEps);
+  t.one_minus_e_avg_t = fmaxf(1.0f - e_avg_t, kMsEps);
+  const float f_avg_o = f_avg_dielectric(eta_o), f_avg_t = f_avg_dielectric(t.eta_rel);
+  const float a = (1.0f - f_avg_o) / om_o;
+  const float b = (1.0f - f_avg_t) * eta_o * eta_o / t.one_minus_e_avg_t;
+  const float x = a + b > kMsEps ? b / (a + b) : 0.5f;
+  t.ratio_r = clampf(1.0f - x * (1.0f - f_avg_o), 0.0f, 1.0f);
+  t.ss = clampf(e_avg_o, 0.0f, 1.0f);
+  t.ms = fmaxf(1.0f - e_avg_o, 0.0f) * clampf(1.0f - t.ratio_r, 0.0f, 1.0f);
+  t.total = fmaxf(t.ss + t.ms, 1.0e-8f);
+  return t;
+}
+// base_dielectric_fresnel (open_pbr.rs:902-929) at physical / prime etas
+__device__ __forceinline__ float dielectric_fresnel_eta(const DevOpenPbr& m, uint32_t face, float c, float eta_ph,
+                                                        float eta_pr) {
+  const bool front = face == 0u;
+  const float unc = front ? weighted_fresnel_ratio(c, eta_ph, eta_pr)
+                          : weighted_fresnel_ratio(c, 1.0f / eta_ph, 1.0f / eta_pr);
+  if (m.coat_clamped <= 0.0f) return unc;
+  const float eta_bc = eta_ph / fmaxf(m.coat_eta, 1.0e-4f);
+  const float eta_bcp = eta_pr / fmaxf(m.coat_eta, 1.0e-4f);
+  float a = eta_bc, b = eta_bcp;
+  if (m.coat_eta > eta_ph) {
+    a = 1.0f / fmaxf(eta_bc, 1.0e-4f);
+    b = 1.0f / fmaxf(eta_bcp, 1.0e-4f);
+  }
+  const float coated = front ? weighted_fresnel_ratio(c, a, b)
+                             : weighted_fresnel_ratio(c, 1.0f / fmaxf(a, 1.0e-4f), 1.0f / fmaxf(b, 1.0e-4f));
+  return unc + (coated - unc) * m.coat_clamped;
+}
+// The rough BTDF at one wavelength's eta (eval_spec_btdf_scalar_with_eta,
+// spec_btdf_fresnel_with_eta, eval_dielectric_transmission_ms,
+// pdf_specular_btdf_with_eta; open_pbr.rs:672-696, 1074-1222): the single-
+// scattering value (ss_ok false when it is None), the multiple-scattering
+// value and the pdf.
+struct BtdfEta {
+  bool ss_ok;
+  V3 ss;
+  float ms, pdf;
+};
+__device__ __forceinline__ BtdfEta btdf_at_eta(const OpbrVertex& s, V3 wi, bool importance, float eta) {
+  const DevOpenPbr& m = *s.m;
+  const V3 wo = s.wo;
+  BtdfEta r;
+  r.ss_ok = false;
+  r.ss = V3{0.0f, 0.0f, 0.0f};
+  const float eta_rel = s.face == 0u ? 1.0f / eta : eta;
+  const TransMs t = trans_ms_at(s, eta);
+  float pdf_ss = 0.0f;
+  const V3 wmu = eta_rel * wo + wi;
+  if (!(length_sq(wmu) < 1.0e-12f)) {
+    V3 wm = normalize(wmu);
+    if (wm.z < 0.0f) wm = -wm;
+    const float co = dot(wo, wm);
+    const float ci = dot(wi, wm);
+    const float den = ci + eta_rel * co;
+    if (!(co <= 0.0f) && !(fabsf(den) < 1.0e-6f)) {
+      const float d = ggx_d(wm, m.spec_ax, m.spec_ay);
+      const float g = ggx_g2(wo, wi, m.spec_ax, m.spec_ay);
+      if (!(d <= 0.0f || g <= 0.0f)) {
+        const float scale = importance ? 1.0f : 1.0f / (eta_rel * eta_rel);
+        const float sc = d * g * fabsf(ci * co);
+        const float denom = den * den * fabsf(wo.z) * fabsf(wi.z);
+        if (!(denom <= 0.0f)) {
+          const float scalar = sc * scale / denom;
+          const V3 no_film = splat(dielectric_fresnel_eta(m, s.face, co, eta, eta));
+          const V3 fr = (m.flags & kOpbrFilm) ? filmed_dielectric(m, no_film, co, eta) : no_film;
+          r.ss = vmaxv(V3{1.0f, 1.0f, 1.0f} - fr, V3{0.0f, 0.0f, 0.0f}) * scalar;
+          r.ss_ok = true;
+        }
+      }
+      const float pdf_wm = pdf_wm_vndf(wo, wm, m.spec_ax, m.spec_ay);
+      pdf_ss = pdf_wm <= 0.0f ? 0.0f : pdf_wm * fabsf(ci) / (den * den);
+    }
+  }
+  const float e_o = dec_e_at(s.dec_e, t.eta_axis, m.ms[0][s.face].r_axis, wo.z);
+  const float e_i = dec_e_at(s.dec_e, t.eta_rel_axis, m.ms[0][s.face].r_axis, fabsf(wi.z));
+  const float ms_scale = importance ? 1.0f : 1.0f / (t.eta_rel * t.eta_rel);
+  r.ms = (1.0f - t.ratio_r) * (1.0f - e_o) * (1.0f - e_i) * ms_scale / (kPiF * t.one_minus_e_avg_t);
+  r.pdf = (t.ss * pdf_ss + t.ms * cosine_pdf(-wi.z)) / t.total;
+  return r;
+}
+// A dispersive rough BTDF seen from the front of an unlocked path integrates
+// over the camera basis (camera_dispersion_active, open_pbr.rs:1250-1312)
+__device__ __forceinline__ bool camera_dispersion(const OpbrVertex& s) {
+  return (s.m->flags & kOpbrDisp) && s.face == 0u && (s.m->flags & kOpbrTransRough) && s.lock < 0.0f;
+}
+// eval_spec_btdf_camera_integrated and pdf_specular_btdf_camera_mixture
+static __device__ __noinline__ void btdf_camera(const OpbrVertex& s, V3 wi, bool importance, V3& f, float& pdf) {
+  const V3 scale = disp::norm_scale();
+  float w[disp::kIntervals];
+  const float total = disp::interval_weights(s.thr, scale, w);
+  f = V3{0.0f, 0.0f, 0.0f};
+  pdf = 0.0f;
+  for (int i = 0; i < disp::kIntervals; ++i) {
+    const float lambda = disp::interval_midpoint(i);
+    const float eta = disp::cauchy_ior(lambda, s.m->trans_eta, s.m->disp_abbe);
+    const BtdfEta b = btdf_at_eta(s, wi, importance, eta);
+    f = f + disp::basis_at(lambda, scale) * (b.ss + splat(b.ms)) * disp::kLambdaStep;
+    const float p_lambda = w[i] / (total * disp::kLambdaStep);
+    pdf += p_lambda * b.pdf * disp::kLambdaStep;
+  }
+}
+
 // The specular BTDF and its pdf for wi below the surface (eval_spec_btdf,
-// eval_thin_wall_spec_btdf, pdf_specular_btdf, open_pbr.rs:1024-1222, without
-// dispersion); `importance` selects the transport mode's eta^2 scaling.
+// eval_thin_wall_spec_btdf, pdf_specular_btdf, open_pbr.rs:1024-1222);
+// `importance` selects the transport mode's eta^2 scaling.
 __device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool importance, V3& f, float& pdf,
                                               V3& f_thin) {
   const DevOpenPbr& m = *s.m;
@@ -648,6 +812,18 @@ __device__ __forceinline__ void btdf_eval_pdf(const OpbrVertex& s, V3 wi, bool i
     const float denom = 4.0f * fabsf(dot(wo, wm));
     pdf = denom > 0.0f ? pdf_wm / denom : 0.0f;
     return;
+  }
+  if (m.flags & kOpbrDisp) {
+    if (camera_dispersion(s)) {
+      btdf_camera(s, wi, importance, f, pdf);
+      return;
+    }
+    if (s.lock >= 0.0f) {  // the path's locked wavelength
+      const BtdfEta b = btdf_at_eta(s, wi, importance, disp::cauchy_ior(s.lock, m.trans_eta, m.disp_abbe));
+      if (b.ss_ok) f = b.ss + splat(b.ms);
+      pdf = b.pdf;
+      return;
+    }
   }
   const float eta_rel = m.teta_rel[s.face];
   const DevMsFace& fm = m.ms[0][s.face];
@@ -809,6 +985,7 @@ struct Sample {
   float pdf;
   float pdf_rev;  // pdf(wi -> wo), computed when requested (0 for delta samples)
   uint32_t flags;
+  float lock;     // the wavelength this sample locks the path to (< 0: none)
 };
 
 // finalize_rough_sample_with_wavelength (open_pbr.rs:1997-2027).  `importance`
@@ -818,7 +995,11 @@ __device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t fl
   V3 f;
   float pdf;
   OpbrVertex at_wi;  // the same BSDF seen from wi
-  if (importance || want_rev) init_vertex(at_wi, s.m, s.cec_e, s.dec_e, wi, s.face == 0u, s.dk_cos);
+  if (importance || want_rev) {
+    init_vertex(at_wi, s.m, s.cec_e, s.dec_e, wi, s.face == 0u, s.dk_cos);
+    at_wi.thr = s.thr;
+    at_wi.lock = s.lock;
+  }
   eval_pdf(s, importance ? at_wi : s, wi, f, pdf, true, importance);
   if (pdf <= 0.0f) return false;
   if (length_sq(f) == 0.0f) return false;
@@ -836,11 +1017,81 @@ __device__ __forceinline__ bool finalize(const OpbrVertex& s, V3 wi, uint32_t fl
   return true;
 }
 
-// sample_spec_btdf (open_pbr.rs:1670-1836) without dispersion: thin-walled
-// (smooth pass-through or the mirrored thin-wall GGX lobe), smooth refraction,
-// or the rough BTDF (VNDF single scattering / cosine multiple scattering).
+// sample_spec_btdf_camera_channels (open_pbr.rs:1838-1928): three per-channel
+// wavelengths (u_rgb = ux[1..3]), one picked by the clamped throughput (ux[0]),
+// the direction sampled at its eta, weighted by the three-channel BTDF over
+// the channel-mixture pdf; the path locks to the picked wavelength.
+static __device__ __noinline__ bool sample_btdf_channels(const OpbrVertex& s, float p_lobe, float u0, float u1,
+                                                         const float* ux, Sample& out, bool importance) {
+  const DevOpenPbr& m = *s.m;
+  const V3 wo = s.wo;
+  const V3 t = vmaxv(s.thr, V3{0.0f, 0.0f, 0.0f});
+  const V3 w = max_element(t) > 0.0f ? t : V3{1.0f, 1.0f, 1.0f};
+  const float sum = fmaxf(w.x + w.y + w.z, 1.0e-8f);
+  const float prob[3] = {w.x / sum, w.y / sum, w.z / sum};
+  float lam[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) lam[c] = disp::sample_channel_wavelength(c, ux[1 + c]);
+  // pick_dispersion_channel
+  float u = clampf(ux[0], 0.0f, 1.0f);
+  int pick = 2;
+  for (int c = 0; c < 3; ++c) {
+    if (u <= prob[c]) {
+      pick = c;
+      break;
+    }
+    u -= prob[c];
+  }
+  if (prob[pick] <= 0.0f) return false;
+  const float eta_u = disp::cauchy_ior(lam[pick], m.trans_eta, m.disp_abbe);
+  const float eta_rel = s.face == 0u ? 1.0f / eta_u : eta_u;
+  const TransMs tm = trans_ms_at(s, eta_u);
+  const float ss_p = tm.ss / tm.total;
+  V3 wi;
+  if (u0 >= ss_p) {
+    const float uu = ss_p < 1.0f ? (u0 - ss_p) / (1.0f - ss_p) : 0.0f;
+    const V3 up = sample_cosine_hemisphere(uu, u1);
+    wi = V3{up.x, up.y, -up.z};
+  } else {
+    const float uu = ss_p > 0.0f ? u0 / ss_p : 0.0f;
+    V3 wm;
+    if (!sample_wm_vndf(wo, m.spec_ax, m.spec_ay, uu, u1, wm)) return false;
+    if (dot(wo, wm) <= 0.0f) return false;
+    if (!refract_about(wo, wm, eta_rel, wi)) return false;
+    if (wi.z >= 0.0f) return false;
+  }
+  if (wi.z >= 0.0f) return false;
+  const V3 bw = weights_below(s, V3{1.0f, 1.0f, 1.0f}).btdf;
+  float pdf_mix = 0.0f;
+  V3 f = V3{0.0f, 0.0f, 0.0f};
+  for (int c = 0; c < 3; ++c) {
+    if (prob[c] <= 0.0f) continue;
+    const BtdfEta b = btdf_at_eta(s, wi, importance, disp::cauchy_ior(lam[c], m.trans_eta, m.disp_abbe));
+    pdf_mix += prob[c] * b.pdf;
+    // eval_spec_btdf_sampled_channels: channel c's component of (1 - F) * scalar, plus ms
+    const float ss = c == 0 ? b.ss.x : (c == 1 ? b.ss.y : b.ss.z);
+    const float v = ss + b.ms;
+    f = f + V3{c == 0 ? v : 0.0f, c == 1 ? v : 0.0f, c == 2 ? v : 0.0f};
+  }
+  const float pdf_total = p_lobe * pdf_mix;
+  if (pdf_total <= 0.0f) return false;
+  out.weight = bw * f * (fabsf(wi.z) / pdf_total);
+  out.wi = wi;
+  out.pdf = pdf_total;
+  out.pdf_rev = 0.0f;  // pdf(wi, wo) with wi below the surface
+  out.flags = kFlagGlossy | kFlagTransmission;
+  out.lock = lam[pick];
+  return true;
+}
+
+// sample_spec_btdf (open_pbr.rs:1670-1836): thin-walled (smooth pass-through
+// or the mirrored thin-wall GGX lobe), smooth refraction, or the rough BTDF
+// (VNDF single scattering / cosine multiple scattering); a dispersive one at
+// the path's locked wavelength, at a wavelength drawn with ux[0] (smooth, front
+// face: the path locks to it), or over sampled camera channels (rough, front
+// face, unlocked).
 static __device__ __noinline__ bool sample_btdf(const OpbrVertex& s, float p_lobe, float u0, float u1, Sample& out,
-                                                bool importance, bool want_rev) {
+                                                bool importance, bool want_rev, const float* ux) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
   const V3 one = V3{1.0f, 1.0f, 1.0f};
@@ -871,6 +1122,52 @@ static __device__ __noinline__ bool sample_btdf(const OpbrVertex& s, float p_lob
     out.pdf = pdf_total;
     out.flags = kFlagGlossy | kFlagTransmission;
     return true;  // pdf_rev = pdf(wi, wo) = 0: wi is below the surface
+  }
+  if (m.flags & kOpbrDisp) {
+    if (camera_dispersion(s)) return sample_btdf_channels(s, p_lobe, u0, u1, ux, out, importance);
+    if (s.lock >= 0.0f || s.face == 0u) {
+      V3 basis = one;
+      float eta_u;
+      if (s.lock >= 0.0f) {
+        eta_u = disp::cauchy_ior(s.lock, m.trans_eta, m.disp_abbe);
+      } else {  // smooth, front face, unlocked: a fresh wavelength
+        out.lock = disp::sample_wavelength_weighted(ux[0], s.thr, basis);
+        eta_u = disp::cauchy_ior(out.lock, m.trans_eta, m.disp_abbe);
+      }
+      const float eta_rel = s.face == 0u ? 1.0f / eta_u : eta_u;
+      if (!rough) {
+        V3 wi;
+        if (!refract_z(wo, eta_rel, wi)) return false;
+        const float fr = dielectric_fresnel_eta(m, s.face, fabsf(wo.z), eta_u, eta_u);
+        const float scale = importance ? 1.0f : 1.0f / (eta_rel * eta_rel);
+        out.weight = (weights_below(s, one).btdf * basis * (1.0f - fr) * scale) / p_lobe;
+        out.wi = wi;
+        out.pdf = p_lobe;
+        out.flags = kFlagDelta | kFlagTransmission;
+        return true;
+      }
+      // rough and locked: the locked eta's lobe weights, evaluated at the lock
+      const TransMs tm = trans_ms_at(s, eta_u);
+      const float ss_p = tm.ss / tm.total;
+      V3 wi;
+      if (u0 >= ss_p) {
+        const float uu = ss_p < 1.0f ? (u0 - ss_p) / (1.0f - ss_p) : 0.0f;
+        const V3 up = sample_cosine_hemisphere(uu, u1);
+        wi = V3{up.x, up.y, -up.z};
+      } else {
+        const float uu = ss_p > 0.0f ? u0 / ss_p : 0.0f;
+        V3 wm;
+        if (!sample_wm_vndf(wo, m.spec_ax, m.spec_ay, uu, u1, wm)) return false;
+        const float co = dot(wo, wm);
+        if (co <= 0.0f) return false;
+        if (!refract_about(wo, wm, eta_rel, wi)) return false;
+        if (wi.z >= 0.0f) return false;
+        const float ci = dot(wi, wm);
+        const float den = ci + eta_rel * co;
+        if (fabsf(den) < 1.0e-6f) return false;
+      }
+      return finalize(s, wi, kFlagGlossy | kFlagTransmission, importance, want_rev, out);
+    }
   }
   const float eta_rel = m.teta_rel[s.face];
   if (!rough) {
@@ -908,9 +1205,11 @@ static __device__ __noinline__ bool sample_btdf(const OpbrVertex& s, float p_lob
 
 // OpenPbrBsdf::sample (open_pbr.rs:298-332) in the shading frame.
 static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, float u0, float u1, Sample& out,
-                                           bool importance = false, bool want_rev = false) {
+                                           bool importance = false, bool want_rev = false,
+                                           const float* ux = nullptr) {
   const DevOpenPbr& m = *s.m;
   const V3 wo = s.wo;
+  out.lock = -1.0f;
   if (!(wo.z > 0.0f) || s.q_total <= 0.0f) return false;
   // pick_lobe over (coat, metal, spec_brdf, spec_btdf, fuzz, diff_brdf, diff_btdf = 0)
   float u = u_lobe * s.q_total;
@@ -939,7 +1238,10 @@ static __device__ __noinline__ bool sample(const OpbrVertex& s, float u_lobe, fl
   }
   const float p_lobe = pl / s.q_total;
   if (p_lobe <= 0.0f) return false;
-  if (lobe == 5) return sample_btdf(s, p_lobe, u0, u1, out, importance, want_rev);
+  if (lobe == 5) {
+    const float zeros[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    return sample_btdf(s, p_lobe, u0, u1, out, importance, want_rev, ux ? ux : zeros);
+  }
   if (lobe == 3 || lobe == 4) {
     V3 wi;
     const bool ok = lobe == 3 ? fuzz_sample_dir(m.fuzz_roughness, wo, u0, u1, wi)

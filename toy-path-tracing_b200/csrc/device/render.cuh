@@ -50,6 +50,11 @@ struct Vertex {
   Frame frame;
   uint32_t inst, tri;
   bool front;  // geometric normal faces the incoming ray (ShadingVertex::front_face)
+  // ShadingVertex::wavelength_lock (< 0: none) and path_throughput: the path
+  // state the integrators stamp on the vertex before shading it (read by
+  // dispersive transmission only)
+  float lock;
+  V3 thr;
 };
 
 struct TriData {
@@ -118,6 +123,8 @@ __device__ __forceinline__ Vertex make_vertex(const TriData& T, uint32_t inst, u
   if (!surface_dpdu(T, dpdu)) dpdu = frame_from_normal(v.ns).t;
   v.frame = frame_from_normal_tangent(v.ns, dpdu);
   v.wo = normalize_or_zero(minus_in);
+  v.lock = -1.0f;
+  v.thr = V3{1.0f, 1.0f, 1.0f};
   return v;
 }
 
@@ -129,6 +136,7 @@ struct BsdfSampleOut {
   V3 weight, wi;
   float pdf;
   bool delta;
+  float lock;  // the wavelength the sample locks the path to (< 0: none)
 };
 
 __device__ __forceinline__ V3 lambert_eval(const DevMaterialRec& m, const Vertex& v, V3 wi) {
@@ -168,6 +176,7 @@ __device__ __forceinline__ bool lambert_sample(const DevMaterialRec& m, const Ve
   s.weight = V3{m.rho[0], m.rho[1], m.rho[2]};
   s.pdf = pdf;
   s.delta = false;
+  s.lock = -1.0f;
   return dot(s.wi, v.ng) > kGeomCosEps;
 }
 
@@ -182,21 +191,36 @@ __device__ __forceinline__ bool opbr_sample_side_ok(const Vertex& v, V3 wi, uint
 // OpenPbrMaterial::sample (material/open_pbr.rs:489-563) in radiance transport
 // (modified_bsdf_sample_weight leaves the weight unchanged there).
 static __device__ __noinline__ bool openpbr_sample(const DevRenderData& d, uint32_t opbr_index, const Vertex& v,
-                                            float u_lobe, float u0, float u1, BsdfSampleOut& s) {
+                                            float u_lobe, float u0, float u1, const float* ux, BsdfSampleOut& s) {
   if (dot(v.wo, v.ng) <= 0.0f) return false;
   const V3 wo_l = normalize_or_zero(to_local(v.frame, v.wo));
   if (wo_l.z <= 0.0f) return false;
   opbr::OpbrVertex ov;
   opbr::init_vertex(ov, d.openpbr + opbr_index, d.cec_e, d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+  ov.thr = v.thr;
+  ov.lock = v.lock;
   opbr::Sample bs;
-  if (!opbr::sample(ov, u_lobe, u0, u1, bs)) return false;
+  if (!opbr::sample(ov, u_lobe, u0, u1, bs, false, false, ux)) return false;
   const V3 wi = to_world(v.frame, bs.wi);
   if (!opbr_sample_side_ok(v, wi, bs.flags)) return false;
   s.wi = wi;
   s.weight = bs.weight;
   s.pdf = bs.pdf;
   s.delta = (bs.flags & opbr::kFlagDelta) != 0;
+  s.lock = bs.lock;
   return true;
+}
+
+// MaterialSampleRandoms::u_extra0..3 (offsets 9-12), drawn only for a
+// dispersive material (the only reader); zeros otherwise.
+__device__ __forceinline__ void extra_randoms(const DevRenderData& d, const DevMaterialRec& m,
+                                              const PathSamplerDev& ps, uint32_t depth, float* ux) {
+  ux[0] = ux[1] = ux[2] = ux[3] = 0.0f;
+  if (m.kind != kDevOpenPbr || !(d.openpbr[m.openpbr].flags & kOpbrDisp)) return;
+  ux[0] = ps.sample_1d(vertex_dim(depth, kOffExtra0));
+  ux[1] = ps.sample_1d(vertex_dim(depth, kOffExtra1));
+  ux[2] = ps.sample_1d(vertex_dim(depth, kOffExtra2));
+  ux[3] = ps.sample_1d(vertex_dim(depth, kOffExtra3));
 }
 
 // Material::sample for the BSDF materials in scope, with the vertex's
@@ -207,7 +231,9 @@ __device__ __forceinline__ bool material_sample(const DevRender& S, const DevMat
   ps.sample_2d(vertex_dim(depth, kOffDir), ud0, ud1);
   if (m.kind == kDevOpenPbr) {
     const float u_lobe = ps.sample_1d(vertex_dim(depth, kOffLobe));
-    return openpbr_sample(S.d, m.openpbr, v, u_lobe, ud0, ud1, s);
+    float ux[4];
+    extra_randoms(S.d, m, ps, depth, ux);
+    return openpbr_sample(S.d, m.openpbr, v, u_lobe, ud0, ud1, ux, s);
   }
   return lambert_sample(m, v, ud0, ud1, s);
 }
@@ -339,11 +365,15 @@ static __device__ __noinline__ V3 material_eval(const DevRender& S, const DevMat
     const DevOpenPbr* mp = S.d.openpbr + m.openpbr;
     opbr::OpbrVertex s;
     opbr::init_vertex(s, mp, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    s.thr = v.thr;
+    s.lock = v.lock;
     V3 f;
     float pdf;
     if (importance) {
       opbr::OpbrVertex lay;
       opbr::init_vertex(lay, mp, S.d.cec_e, S.d.dec_e, wi_l, v.front, fabsf(wo_l.z));
+      lay.thr = v.thr;
+      lay.lock = v.lock;
       opbr::eval_pdf(s, lay, wi_l, f, pdf, true, true);
     } else {
       opbr::eval_pdf(s, s, wi_l, f, pdf);
@@ -442,6 +472,8 @@ static __device__ __noinline__ V3 material_eval_pdf(const DevRender& S, const De
     if (wo_l.z <= 0.0f) return V3{0.0f, 0.0f, 0.0f};
     opbr::OpbrVertex s;
     opbr::init_vertex(s, S.d.openpbr + m.openpbr, S.d.cec_e, S.d.dec_e, wo_l, v.front, fabsf(wo_l.z));
+    s.thr = v.thr;
+    s.lock = v.lock;
     V3 f;
     float pdf;
     opbr::eval_pdf(s, s, wi_l, f, pdf);

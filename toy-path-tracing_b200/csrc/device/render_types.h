@@ -68,7 +68,11 @@ enum : uint32_t {
   kOpbrTransRough = 128u,   // transmission > 0 and not smooth (spec_btdf_is_smooth false)
   kOpbrThinWalled = 256u,   // geometry_thin_walled
   kOpbrFilm = 512u,         // thin film: weight > 0 and thickness > 0
+  kOpbrDisp = 1024u,        // dispersive transmission (transmission_dispersion_abbe > 0)
 };
+// The dielectric energy-compensation table E (32 eta x 32 roughness x 32
+// sqrt cos); its E_avg (32 eta x 32 roughness) follows it in the same buffer.
+constexpr uint32_t kDecTableLen = 32u * 32u * 32u;
 struct alignas(16) DevOpenPbr {
   float base_color[3], base;
   float specular, specular_color[3];
@@ -103,7 +107,8 @@ struct alignas(16) DevOpenPbr {
   float tw_ay, trans_eta, teta_rel[2];
   // thin film (bsdf/thin_film.rs): weight, thickness in nm, film IOR, and the
   // metal base's complex IOR (artist_friendly_complex_ior)
-  float film_w, film_thick, film_ior, pad_f;
+  float film_w, film_thick, film_ior;
+  float disp_abbe;  // transmission_dispersion_abbe (0: no dispersion)
   float metal_n[3], metal_k[3];
   uint32_t pad2[2];
 };
@@ -291,6 +296,7 @@ struct WfBuffers {
   float* prev;        // 7 planes: previous vertex p (3), ns (3), BSDF pdf
   uint32_t* prev_mat; // previous vertex material index, bit 31 = delta sample
   uint32_t* depth;    // vertices processed
+  float* lock;        // the path's wavelength lock (< 0: none)
   uint32_t* q_slot[2];
   float* q_ray[2];    // 7 planes each: o, d, tmax
   int32_t* h_tri;

@@ -386,6 +386,10 @@ void lower_openpbr(const tpt_openpbr_desc& m, const float* spec_da, const float*
   if (!(trans <= 0.0f || spec_alpha_smooth)) flags |= kOpbrTransRough;
   if (m.geometry_thin_walled) flags |= kOpbrThinWalled;
   if (has_film) flags |= kOpbrFilm;
+  // transmission_dispersion_abbe (material/open_pbr.rs:783-790)
+  const float disp_scale = std::fmax(m.transmission_dispersion_scale, 0.0f);
+  d.disp_abbe = disp_scale <= 0.0f ? 0.0f : std::fmax(m.transmission_dispersion_abbe_number, 1.0e-6f) / disp_scale;
+  if (d.disp_abbe > 0.0f) flags |= kOpbrDisp;
   d.film_w = film_w;
   d.film_thick = film_thick;
   d.film_ior = film_ior;
@@ -504,4 +508,5 @@ extern "C" void tpt_openpbr_defaults(tpt_openpbr_desc* d) {
   d->thin_film_ior = 1.4f;
   d->emission_color[0] = d->emission_color[1] = d->emission_color[2] = 1.0f;
   d->geometry_opacity = 1.0f;
+  d->transmission_dispersion_abbe_number = 20.0f;
 }

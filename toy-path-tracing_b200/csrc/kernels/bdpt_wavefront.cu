@@ -103,6 +103,7 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_init(const __grid_constant__ De
   V3 lo, ld;
   BdLightState l;
   l.pending_pdf = 0.0f;
+  l.lock = -1.0f;
   l.alive = bdpt_light_endpoint(S, P, ps, lig, lo, ld, l.beta, l.pending_from, l.pending_pdf);
   l.n = l.alive ? 1u : 0u;
   B.cam_state[i] = c;

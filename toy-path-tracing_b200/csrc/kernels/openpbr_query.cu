@@ -13,6 +13,7 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(const __grid_con
                                                                 const float* __restrict__ wo,
                                                                 const float* __restrict__ wi,
                                                                 const uint32_t* __restrict__ front, uint32_t mode,
+                                                                const float* __restrict__ state,
                                                                 float* __restrict__ f, float* __restrict__ pdf) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -21,11 +22,17 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_eval_kernel(const __grid_con
   const V3 o = V3{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]};
   const V3 w = V3{wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]};
   opbr::init_vertex(s, m, rd.cec_e, rd.dec_e, o, front[i] != 0, fabsf(o.z));
+  if (state) {  // path throughput and wavelength lock (NaN: none)
+    s.thr = V3{state[4 * i], state[4 * i + 1], state[4 * i + 2]};
+    s.lock = isnan(state[4 * i + 3]) ? -1.0f : state[4 * i + 3];
+  }
   V3 fv;
   float p;
   if (mode == 1) {  // importance transport: layer weights at wi
     opbr::OpbrVertex lay;
     opbr::init_vertex(lay, m, rd.cec_e, rd.dec_e, w, front[i] != 0, fabsf(o.z));
+    lay.thr = s.thr;
+    lay.lock = s.lock;
     opbr::eval_pdf(s, lay, w, fv, p, true, true);
   } else {
     opbr::eval_pdf(s, s, w, fv, p);
@@ -40,6 +47,7 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(const __grid_c
                                                                   const float* __restrict__ wo,
                                                                   const float* __restrict__ u,
                                                                   const uint32_t* __restrict__ front, uint32_t mode,
+                                                                  const float* __restrict__ state,
                                                                   float* __restrict__ out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -47,12 +55,22 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(const __grid_c
   opbr::OpbrVertex s;
   const V3 w = V3{wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]};
   opbr::init_vertex(s, m, rd.cec_e, rd.dec_e, w, front[i] != 0, fabsf(w.z));
+  // with a path state: u holds 7 values (u_lobe, u_dir, u_extra0..3) and the
+  // record 10 (the sampled wavelength lock last, NaN: none)
+  const int nu = state ? 7 : 3, no = state ? 10 : 9;
+  float ux[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (state) {
+    s.thr = V3{state[4 * i], state[4 * i + 1], state[4 * i + 2]};
+    s.lock = isnan(state[4 * i + 3]) ? -1.0f : state[4 * i + 3];
+    for (int k = 0; k < 4; ++k) ux[k] = u[nu * i + 3 + k];
+  }
   opbr::Sample smp;
-  float* o = out + 9 * i;
-  if (!opbr::sample(s, u[3 * i], u[3 * i + 1], u[3 * i + 2], smp, mode == 1, true)) {
-    for (int k = 0; k < 9; ++k) o[k] = 0.0f;
+  float* o = out + no * i;
+  if (!opbr::sample(s, u[nu * i], u[nu * i + 1], u[nu * i + 2], smp, mode == 1, true, ux)) {
+    for (int k = 0; k < no; ++k) o[k] = 0.0f;
     return;
   }
+  if (state) o[9] = smp.lock >= 0.0f ? smp.lock : __int_as_float(0x7fc00000);
   o[0] = smp.weight.x;
   o[1] = smp.weight.y;
   o[2] = smp.weight.z;
@@ -66,18 +84,20 @@ __global__ void __launch_bounds__(kQueryBlock) bsdf_sample_kernel(const __grid_c
 }  // namespace
 
 cudaError_t launch_bsdf_eval(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo, const float* wi,
-                             const uint32_t* front, uint32_t mode, float* f, float* pdf, cudaStream_t s) {
+                             const uint32_t* front, uint32_t mode, const float* state, float* f, float* pdf,
+                             cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   bsdf_eval_kernel<<<(unsigned)((n + kQueryBlock - 1) / kQueryBlock), kQueryBlock, 0, s>>>(rd, material, n, wo, wi,
-                                                                                          front, mode, f, pdf);
+                                                                                          front, mode, state, f, pdf);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bsdf_sample(const DevRenderData& rd, uint32_t material, uint64_t n, const float* wo,
-                               const float* u, const uint32_t* front, uint32_t mode, float* out, cudaStream_t s) {
+                               const float* u, const uint32_t* front, uint32_t mode, const float* state, float* out,
+                               cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   bsdf_sample_kernel<<<(unsigned)((n + kQueryBlock - 1) / kQueryBlock), kQueryBlock, 0, s>>>(rd, material, n, wo, u,
-                                                                                            front, mode, out);
+                                                                                            front, mode, state, out);
   return cudaGetLastError();
 }
 

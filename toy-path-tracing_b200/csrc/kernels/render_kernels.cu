@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
   V3 prev_p, prev_ns;          // previous vertex (emission MIS after a BSDF sample)
   float prev_pdf = 0.0f;
   uint32_t prev_mat = 0;       // material index, bit 31: delta sample
+  float lock = -1.0f;          // the path's wavelength lock (< 0: none)
   PathSamplerDev ps;
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, k == -1);
@@ -78,6 +79,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
           depth = 0;
           L = V3{0.0f, 0.0f, 0.0f};
           beta = V3{1.0f, 1.0f, 1.0f};
+          lock = -1.0f;
           bounce_pending = false;
         } else {
           k = -2;
@@ -111,7 +113,9 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
       }
       done = true;
     } else {
-      const Vertex v = shade_hit<int>(S, h, rd);
+      Vertex v = shade_hit<int>(S, h, rd);
+      v.thr = beta;  // the path state of the vertex (mis.rs:54-55)
+      v.lock = lock;
       const uint32_t mi = __ldg(&S.d.inst[v.inst].material);
       const DevMaterialRec m = S.d.mats[mi];
       V3 le;
@@ -148,6 +152,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
         BsdfSampleOut s;
         if (material_sample(S, m, v, ps, depth, s)) {
           beta = beta * s.weight;
+          if (s.lock >= 0.0f) lock = s.lock;
           alive = true;
           if (depth + 1 >= 4) {
             const float q = clampf(max_element(beta), 0.05f, 1.0f);

@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(const __grid_constant__ 
     B.L[k * C + i] = ADJ ? primal[3 * (uint64_t)i + k] : 0.0f;
   }
   B.depth[i] = 0;
+  B.lock[i] = -1.0f;
 }
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
@@ -156,7 +157,9 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
     h.b2 = B.h_bary[2 * C + j];
     const float* qr = B.q_ray[cur];
     const V3 rd = V3{qr[3 * C + j], qr[4 * C + j], qr[5 * C + j]};
-    const Vertex v = shade_hit<int>(S, h, rd);
+    Vertex v = shade_hit<int>(S, h, rd);
+    v.thr = beta;  // the path state of the vertex (mis.rs:54-55)
+    v.lock = B.lock[slot];
     const uint32_t mi = __ldg(&S.d.inst[v.inst].material);
     const DevMaterialRec m = S.d.mats[mi];
     // emission of this vertex (mis.rs:45-47 for the camera vertex, 101-117
@@ -205,6 +208,7 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
       float sens_s[ADJ ? 3 * kGradGroups : 1];
       if (material_sample(S, m, v, ps, d, s)) {
         beta = beta * s.weight;
+        if (s.lock >= 0.0f) B.lock[slot] = s.lock;
         bool alive = true;
         if (d + 1 >= 4) {
           const float q = clampf(max_element(beta), 0.05f, 1.0f);

@@ -85,7 +85,8 @@ OPENPBR_FIELDS = [
     ("coat_roughness_anisotropy", 1, 0.0), ("coat_ior", 1, 1.6), ("coat_darkening", 1, 1.0),
     ("thin_film_weight", 1, 0.0), ("thin_film_thickness", 1, 0.5), ("thin_film_ior", 1, 1.4),
     ("emission_luminance", 1, 0.0), ("emission_color", 3, 1.0), ("geometry_opacity", 1, 1.0),
-    ("geometry_thin_walled", 1, 0),
+    ("geometry_thin_walled", 1, 0), ("transmission_dispersion_scale", 1, 0.0),
+    ("transmission_dispersion_abbe_number", 1, 20.0),
 ]
 
 
@@ -94,7 +95,7 @@ class OpenPbrDesc(C.Structure):
                 for n, k, _ in OPENPBR_FIELDS]
 
 
-assert C.sizeof(OpenPbrDesc) == 43 * 4
+assert C.sizeof(OpenPbrDesc) == 45 * 4
 
 
 def openpbr_desc(m: dict) -> OpenPbrDesc:
@@ -286,6 +287,8 @@ EXPORTED_SYMBOLS = [
     "tpt_lut_dielectric_ec",
     "tpt_bsdf_eval_device",
     "tpt_bsdf_sample_device",
+    "tpt_bsdf_eval_path_device",
+    "tpt_bsdf_sample_path_device",
     "tpt_scene_set_openpbr",
     "tpt_render_batch_device",
     "tpt_context_set_wavefront_capacity",
@@ -335,6 +338,8 @@ def _declare(L):
         "tpt_lut_dielectric_ec": (i32, [vp, vp, vp]),
         "tpt_bsdf_eval_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp, vp]),
         "tpt_bsdf_sample_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, C.c_uint32, vp, vp]),
+        "tpt_bsdf_eval_path_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, vp, C.c_uint32, vp, vp, vp]),
+        "tpt_bsdf_sample_path_device": (i32, [vp, vp, C.c_uint32, u64, vp, vp, vp, vp, C.c_uint32, vp, vp]),
         "tpt_scene_set_openpbr": (i32, [vp, vp, C.c_uint32, vp, vp, vp]),
         "tpt_render_batch_device": (i32, [vp, vp, i32, vp, vp]),
         "tpt_context_set_wavefront_capacity": (i32, [vp, C.c_uint32]),
@@ -668,6 +673,23 @@ class Scene:
         _check(lib().tpt_bsdf_sample_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr), C.c_void_p(u_ptr),
                                             C.c_void_p(front_ptr), mode, C.c_void_p(out_ptr), _stream(stream)),
                self.ctx)
+
+    def bsdf_eval_path_device(self, material: int, n: int, wo_ptr: int, wi_ptr: int, front_ptr: int, state_ptr: int,
+                              f_ptr: int, pdf_ptr: int, stream=None, mode: int = 0):
+        """`tpt_bsdf_eval_path_device`: eval + pdf with a path state per pair
+        (n x 4: throughput r, g, b and the wavelength lock, NaN = none)."""
+        _check(lib().tpt_bsdf_eval_path_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr),
+                                               C.c_void_p(wi_ptr), C.c_void_p(front_ptr), C.c_void_p(state_ptr),
+                                               mode, C.c_void_p(f_ptr), C.c_void_p(pdf_ptr), _stream(stream)),
+               self.ctx)
+
+    def bsdf_sample_path_device(self, material: int, n: int, wo_ptr: int, u_ptr: int, front_ptr: int,
+                                state_ptr: int, out_ptr: int, stream=None, mode: int = 0):
+        """`tpt_bsdf_sample_path_device`: samples with a path state; u n x 7
+        (u_lobe, u_dir, u_extra0..3), out n x 10 (the sampled lock last, NaN = none)."""
+        _check(lib().tpt_bsdf_sample_path_device(self.ctx.h, self.h, material, n, C.c_void_p(wo_ptr),
+                                                 C.c_void_p(u_ptr), C.c_void_p(front_ptr), C.c_void_p(state_ptr),
+                                                 mode, C.c_void_p(out_ptr), _stream(stream)), self.ctx)
 
     # -- material updates and the adjoint (no counterpart in the reference) ----
     def set_openpbr(self, material_ids, materials, stream=None):

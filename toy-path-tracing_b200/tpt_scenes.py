@@ -201,11 +201,13 @@ def cornell_box(seed: int = 1, material: int = OPENPBR, light_strength: float = 
             "angles": (float(a1), float(a2)), "seed": seed}
 
 
-def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPENPBR):
+def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPENPBR, dispersion: float = 0.0):
     """The Cornell box with transmissive boxes: the tall box rough (specular
     roughness 0.25) and the short box smooth, both fully transmissive OpenPBR
-    (the short one tinted); thin_walled makes both thin-walled sheets.  The
-    walls keep their diffuse materials (OpenPBR, or NormalizedLambert)."""
+    (the short one tinted); thin_walled makes both thin-walled sheets;
+    dispersion > 0 gives both glasses that transmission_dispersion_scale
+    (Abbe number 20 at scale 1).  The walls keep their diffuse materials
+    (OpenPBR, or NormalizedLambert)."""
     sc = cornell_box(seed, material)
     thin = 1 if thin_walled else 0
     sc["materials"][5] = {"kind": OPENPBR, "base_color": np.array([0.8, 0.8, 0.8], np.float32),
@@ -214,6 +216,9 @@ def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPEN
                           "specular_roughness": 0.0, "transmission_weight": 1.0,
                           "transmission_color": np.array([0.9, 0.75, 0.6], np.float32),
                           "geometry_thin_walled": thin}
+    if dispersion > 0.0:
+        for k in (5, 6):
+            sc["materials"][k]["transmission_dispersion_scale"] = float(dispersion)
     return sc
 
 
