@@ -160,8 +160,8 @@ typedef enum tpt_material_kind {
  * emission_color * emission_luminance from the front face, both faces when
  * thin-walled, tinted by the coat and fuzz above it; such a surface is a light
  * of the light tree and of BDPT's area-light table).  Upload rejects with
- * TPT_ERR_INVALID_ARG a material with geometry_opacity < 1 (alpha testing).
- * subsurface_weight is ignored, as the reference forces it to 0
+ * TPT_ERR_INVALID_ARG no untextured parameter: geometry_opacity < 1 is the
+ * alpha test of tpt_material_desc.opacity.  subsurface_weight is ignored, as the reference forces it to 0
  * (validate_and_warn).  Dispersion (transmission_dispersion_scale > 0,
  * bsdf/dispersion.rs) makes the transmission IOR a Cauchy function of
  * wavelength: an unlocked path evaluates the rough BTDF integrated over the
@@ -209,6 +209,14 @@ typedef struct tpt_material_desc {
   float color[3];   /* Emissive colour */
   float strength;   /* Emissive strength */
   const struct tpt_openpbr_desc* openpbr;
+  /* NormalizedLambert / Emissive opacity (their `opacity` field): used when
+   * has_opacity != 0, else the material is opaque (1), so that a zeroed
+   * record is opaque.  OpenPBR materials take geometry_opacity instead.  An
+   * opacity below 1 gives the material an alpha test: Scene::closest_hit keeps
+   * a hit on it iff an AuxRng draw is below the (clamped) opacity
+   * (scene/mod.rs:360-377, 686-723). */
+  uint32_t has_opacity;
+  float opacity;
 } tpt_material_desc;
 
 /* Lights other than emissive triangles (light/{point,spot,directional}.rs),
@@ -360,6 +368,16 @@ tpt_status tpt_traverse(tpt_context* ctx, const tpt_scene* scene, const float* r
                         int32_t* prim, float* t, int32_t* instance, float* bary);
 tpt_status tpt_traverse_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n, int mode,
                                int32_t* prim, float* t, int32_t* instance, float* bary, void* stream);
+/* Scene::closest_hit with the alpha tests of its materials (scene/mod.rs:
+ * 340-395, 686-723): aux (device, n uint32) holds each ray's AuxRng state
+ * (aux_rng.rs: the state after from_seed); a candidate hit on an instance whose
+ * material has opacity < 1 draws next_f32 from it and is kept iff the draw is
+ * below the opacity.  aux is advanced in place by the draws, as the
+ * reference's &mut AuxRng.  Without alpha-tested materials this is the
+ * closest-hit query.  tpt_traverse / tpt_traverse_device ignore opacity. */
+tpt_status tpt_traverse_alpha_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n,
+                                     uint32_t* aux, int32_t* prim, float* t, int32_t* instance, float* bary,
+                                     void* stream);
 /* Same query, also writing per-ray counts of 4-wide node tests and triangle
  * tests (device pointers, n each); used for the algorithmic-bytes account. */
 tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n,

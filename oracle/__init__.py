@@ -121,6 +121,8 @@ def _declare(L):
         "orc_openpbr_eval": (None, [vp, i32, vp, vp, i32, vp]),
         "orc_openpbr_pdf": (f32, [vp, i32, vp, vp]),
         "orc_openpbr_sample": (i32, [vp, i32, vp, f32, f32, f32, i32, vp]),
+        "orc_render_scene_set_opacity": (None, [vp, vp, u32]),
+        "orc_render_scene_closest_alpha": (None, [vp, vp, u64, vp, vp, vp, vp]),
         "orc_openpbr_le": (i32, [vp, i32, vp, vp]),
         "orc_openpbr_eval_ex": (None, [vp, i32, vp, vp, vp, i32, vp]),
         "orc_openpbr_pdf_ex": (f32, [vp, i32, vp, vp, vp]),
@@ -407,6 +409,8 @@ class RenderScene:
         col = np.array([np.asarray(m.get("color", (0, 0, 0)), np.float32) for m in mats], np.float32)
         st = np.array([m.get("strength", 0.0) for m in mats], np.float32)
         lib().orc_render_scene_set_materials(self.h, _p(kinds), _p(rho), _p(col), _p(st), len(mats))
+        op = np.array([m.get("opacity", 1.0) for m in mats], np.float32)
+        lib().orc_render_scene_set_opacity(self.h, _p(op), len(mats))
         for i, m in enumerate(mats):
             if m["kind"] == 2:
                 why = lib().orc_render_scene_set_openpbr(self.h, i, _p(pack_openpbr(m)))
@@ -431,6 +435,19 @@ class RenderScene:
                 lib().orc_render_scene_free(self.h)
         except Exception:
             pass
+
+    def closest_alpha(self, rays, aux):
+        """Scene::closest_hit with the alpha filter: rays (n, 6) origin +
+        direction, aux (n,) uint32 AuxRng states (advanced copy returned).
+        Returns (instance, triangle, t, aux)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        n = len(rays)
+        a = np.ascontiguousarray(aux, np.uint32).copy()
+        inst = np.empty(n, np.int32)
+        tri = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        lib().orc_render_scene_closest_alpha(self.h, _p(rays), n, _p(a), _p(inst), _p(tri), _p(t))
+        return inst, tri, t, a
 
     @staticmethod
     def _cam(camera):

@@ -2,6 +2,8 @@
 // lights (the only light type in scope: no environment, point, spot or
 // directional lights, so the camera subpath's non-area-light NEE and the
 // infinite-light terms are zero).
+#include <cstdio>
+#include <cstdlib>
 #include "render.h"
 
 namespace orc {
@@ -17,11 +19,11 @@ struct PathVertex {
   bool delta = false, connectible = false;
 };
 
-bool closest(const RenderScene& s, Vec3 o, Vec3 d, SceneHit* h) {
+bool closest(const RenderScene& s, Vec3 o, Vec3 d, SceneHit* h, AuxRng* aux) {
   Ray r;
   r.origin = o;
   r.direction = d;
-  return s.geo.closest_hit(r, h);
+  return s.geo.closest_hit(r, h, nullptr, aux);
 }
 Vec3 offset_origin(Vec3 p, Vec3 ng, Vec3 d) {  // integrator/mod.rs:77-85
   Vec3 n = dot(d, ng) >= 0.0f ? ng : -ng;
@@ -120,20 +122,21 @@ float bdpt_mis_weight(const RenderScene& s, const PathVertex* lp, size_t ns, con
 }
 
 // bdpt.rs:555-575, 577-602
-bool visible_between(const RenderScene& s, Vec3 o, Vec3 ng, Vec3 dir, float dist, int tinst, int ttri) {
+bool visible_between(const RenderScene& s, Vec3 o, Vec3 ng, Vec3 dir, float dist, int tinst, int ttri,
+                     AuxRng* aux) {
   SceneHit h;
-  if (!closest(s, offset_origin(o, ng, dir), dir, &h)) return true;
+  if (!closest(s, offset_origin(o, ng, dir), dir, &h, aux)) return true;
   if (h.instance == tinst && h.triangle == ttri) return true;
   return h.t >= dist * (1.0f - kShadowTolerance);
 }
-Vec3 connect(const RenderScene& s, const PathVertex& lv, const PathVertex& cv) {
+Vec3 connect(const RenderScene& s, const PathVertex& lv, const PathVertex& cv, AuxRng* aux) {
   Vec3 delta = cv.vtx.p - lv.vtx.p;
   float dist2 = length_squared(delta);
   if (dist2 <= 0.0f) return Vec3(0, 0, 0);
   float dist = std::sqrt(dist2);
   Vec3 w_lc = delta / dist;
   Vec3 w_cl = -w_lc;
-  if (!visible_between(s, lv.vtx.p, lv.vtx.ng, w_lc, dist, cv.vtx.inst, cv.vtx.tri)) return Vec3(0, 0, 0);
+  if (!visible_between(s, lv.vtx.p, lv.vtx.ng, w_lc, dist, cv.vtx.inst, cv.vtx.tri, aux)) return Vec3(0, 0, 0);
   Vec3 f_cam = material_eval(s.mat_of(cv.vtx.inst), cv.vtx, w_cl, kRadiance);
   if (length_squared(f_cam) == 0.0f) return Vec3(0, 0, 0);
   Vec3 f_light;
@@ -151,7 +154,7 @@ Vec3 connect(const RenderScene& s, const PathVertex& lv, const PathVertex& cv) {
 
 // bdpt.rs:135-262
 Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp, uint32_t max_depth,
-                    std::vector<PathVertex>& vs) {
+                    std::vector<PathVertex>& vs, AuxRng* aux) {
   vs.clear();
   Vec3 L(0, 0, 0), beta(1, 1, 1);
   Vec3 ro = ray0.origin, rd = ray0.direction;
@@ -164,8 +167,9 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
   const bool non_area = scene_has_non_area_lights(s);
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sp.path_vertex_randoms(depth);
+    *aux = AuxRng(rnd.aux_rng_seed);  // bdpt.rs:160: the arriving ray, then the vertex's light sample
     SceneHit h;
-    if (!closest(s, ro, rd, &h)) {
+    if (!closest(s, ro, rd, &h, aux)) {
       // emitted_radiance_from_infinite_hit (bdpt.rs:466-486)
       L += beta * env_escape(s, rd, count_emission, pending_pdf);
       break;
@@ -191,7 +195,8 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
       L += beta * le * w;
     }
     // direct_non_area_light_contribution (bdpt.rs:207-221, 396-464)
-    if (non_area && !is_pure_emitter(m)) L += beta * direct_light(s, m, v, rnd, nullptr, kDirectBdptNonArea);
+    if (non_area && !is_pure_emitter(m))
+      L += beta * direct_light(s, m, v, rnd, nullptr, kDirectBdptNonArea, aux);
     MatSampleOut smp;
     if (!material_sample(m, v, rnd.material, kRadiance, &smp)) break;
     vs[vi].delta = smp.delta;
@@ -218,7 +223,8 @@ Vec3 camera_subpath(const RenderScene& s, const Ray& ray0, const PathSampler& sp
 }
 
 // bdpt.rs:264-385
-void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_depth, std::vector<PathVertex>& vs) {
+void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_depth, std::vector<PathVertex>& vs,
+                   AuxRng* aux) {
   vs.clear();
   if (max_depth == 0) return;
   VertexRandoms rnd0 = sp.path_vertex_randoms(0);
@@ -272,8 +278,9 @@ void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_dep
   float lock = 0.0f;
   for (uint32_t depth = 1; depth < max_depth; ++depth) {
     VertexRandoms rnd = sp.path_vertex_randoms(depth);
+    *aux = AuxRng(rnd.aux_rng_seed);  // bdpt.rs:335
     SceneHit h;
-    if (!closest(s, ro, rd, &h)) break;
+    if (!closest(s, ro, rd, &h, aux)) break;
     Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, rd);
     // the path state the vertex keeps for its connections (bdpt.rs:177-178, 344-345)
     v.path_throughput = beta;
@@ -307,15 +314,40 @@ void light_subpath(const RenderScene& s, const PathSampler& sp, uint32_t max_dep
 }
 }  // namespace
 
+// ORC_BDPT_TRACE=1: print each connection strategy's MIS weight and
+// unweighted contribution, and the camera subpath's radiance, to stderr
+// (debugging aid of the checker; off by default).
+bool trace_on() {
+  static const bool on = std::getenv("ORC_BDPT_TRACE") != nullptr;
+  return on;
+}
+
 Vec3 trace_bdpt(const RenderScene& s, const Ray& ray, const PathSampler& sp, uint32_t max_depth) {
   thread_local std::vector<PathVertex> cam, lig;
-  Vec3 L = camera_subpath(s, ray, sp, max_depth, cam);
-  light_subpath(s, sp, max_depth, lig);
+  // one AuxRng through both subpaths (each depth reseeds it) and then every
+  // connection's visibility test in loop order (bdpt.rs:81-121)
+  AuxRng aux(sp.initial_aux_rng_seed());
+  Vec3 L = camera_subpath(s, ray, sp, max_depth, cam, &aux);
+  light_subpath(s, sp, max_depth, lig, &aux);
+  if (trace_on()) {
+    std::fprintf(stderr, "bdpt camera L=(%.9g %.9g %.9g) |cam|=%zu |light|=%zu\n", L.x, L.y, L.z, cam.size(), lig.size());
+    for (size_t i = 0; i < cam.size(); ++i)
+      std::fprintf(stderr, "  cam %zu inst %d tri %d conn %d delta %d beta (%.6g %.6g %.6g) fwd %.6g rev %.6g\n", i,
+                   cam[i].vtx.inst, cam[i].vtx.tri, (int)cam[i].connectible, (int)cam[i].delta, cam[i].beta.x,
+                   cam[i].beta.y, cam[i].beta.z, cam[i].pdf_fwd_area, cam[i].pdf_rev_area);
+    for (size_t i = 0; i < lig.size(); ++i)
+      std::fprintf(stderr, "  lig %zu inst %d tri %d conn %d delta %d beta (%.6g %.6g %.6g) fwd %.6g rev %.6g\n", i,
+                   lig[i].vtx.inst, lig[i].vtx.tri, (int)lig[i].connectible, (int)lig[i].delta, lig[i].beta.x,
+                   lig[i].beta.y, lig[i].beta.z, lig[i].pdf_fwd_area, lig[i].pdf_rev_area);
+  }
   for (size_t li = 0; li < lig.size(); ++li)
     for (size_t ci = 0; ci < cam.size(); ++ci) {
       if (!lig[li].connectible || !cam[ci].connectible) continue;
       float w = bdpt_mis_weight(s, lig.data(), li + 1, cam.data(), ci + 1);
-      L += w * connect(s, lig[li], cam[ci]);
+      const Vec3 c = connect(s, lig[li], cam[ci], &aux);
+      if (trace_on())
+        std::fprintf(stderr, "bdpt s=%zu t=%zu w=%.9g c=(%.9g %.9g %.9g)\n", li + 1, ci + 1, w, c.x, c.y, c.z);
+      L += w * c;
     }
   return L;
 }

@@ -29,6 +29,35 @@ void orc_render_scene_set_materials(void* h, const uint32_t* kinds, const float*
   }
 }
 
+// NormalizedLambert / Emissive opacity per material (1 = opaque; OpenPBR
+// materials take geometry_opacity from their parameters).  Call before the
+// light tree (which finalises).
+void orc_render_scene_set_opacity(void* h, const float* opacity, uint32_t n) {
+  auto* s = (RenderScene*)h;
+  for (uint32_t i = 0; i < n && i < s->materials.size(); ++i) s->materials[i].opacity = opacity[i];
+}
+
+// Scene::closest_hit with an AuxRng per ray (scene/mod.rs:340-395, 686-723):
+// rays n x 6 (origin, direction); aux: the AuxRng states, advanced in place by
+// the alpha tests' draws; out: instance, triangle (-1: miss), t per ray.
+void orc_render_scene_closest_alpha(void* h, const float* rays, uint64_t n, uint32_t* aux, int32_t* inst,
+                                    int32_t* tri, float* t) {
+  const auto* s = (const RenderScene*)h;
+  for (uint64_t i = 0; i < n; ++i) {
+    Ray r;
+    r.origin = Vec3(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+    r.direction = Vec3(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+    AuxRng a(0);
+    a.state = aux[i];
+    SceneHit hit;
+    const bool found = s->geo.closest_hit(r, &hit, nullptr, &a);
+    aux[i] = a.state;
+    inst[i] = found ? hit.instance : -1;
+    tri[i] = found ? hit.triangle : -1;
+    t[i] = found ? hit.t : kInf;
+  }
+}
+
 // Point lights: n x 7 floats (position, color, intensity); spot lights: n x 12
 // (position, direction, color, intensity, total width, falloff start in
 // radians: SpotLight::new); directional: n x 7 (direction, color, intensity:

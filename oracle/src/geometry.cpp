@@ -1,5 +1,6 @@
 // Oracle: triangle test, QBVH builder and scene queries.
 #include "geometry.h"
+#include "sampler.h"
 
 namespace orc {
 
@@ -302,7 +303,7 @@ Bounds transform_bounds(const Bounds& b, const Mat4& m) {
 }
 
 // scene/mod.rs:340-395 and 686-723
-bool Geometry::closest_hit(const Ray& ray, SceneHit* hit, TraversalStats* st) const {
+bool Geometry::closest_hit(const Ray& ray, SceneHit* hit, TraversalStats* st, AuxRng* aux) const {
   *hit = SceneHit();
   if (instances.empty()) return false;
   bool found = false;
@@ -318,6 +319,8 @@ bool Geometry::closest_hit(const Ray& ray, SceneHit* hit, TraversalStats* st) co
           lr.direction = inst.world_to_local.transform_vector3(ray.direction);
           const Mesh& mesh = meshes[inst.mesh_index];
           if (st) st->instances++;
+          // Material::has_alpha_test of the instance's material
+          const float alpha = aux && !this->alpha.empty() ? this->alpha[ii] : 1.0f;
           bool mesh_found = false;
           TriHit best{};
           uint32_t best_tri = 0;
@@ -332,6 +335,8 @@ bool Geometry::closest_hit(const Ray& ray, SceneHit* hit, TraversalStats* st) co
                   if (st) st->triangles++;
                   TriHit h;
                   if (intersect_triangle(lr, tm, v[0], v[1], v[2], &h)) {
+                    // any_hit: alpha >= 1 || u < alpha (alpha = the clamped opacity)
+                    if (alpha < 1.0f && !(aux->next_f32() < alpha)) continue;
                     tm = h.t;
                     best = h;
                     best_tri = tri;

@@ -119,12 +119,20 @@ struct SceneHit {
   Vec3 bary;
 };
 
+struct AuxRng;
+
 struct Geometry {
   std::vector<Mesh> meshes;
   std::vector<Instance> instances;
   Qbvh tlas;
-  // scene/mod.rs:340-395 (no alpha-tested materials in scope: the filter accepts every hit)
-  bool closest_hit(const Ray& ray, SceneHit* hit, TraversalStats* st = nullptr) const;
+  // Per instance: the opacity of its material's alpha test (Material::
+  // has_alpha_test / any_hit, untextured), 1 where the material has none.
+  // Empty: no instance has one.
+  std::vector<float> alpha;
+  // scene/mod.rs:340-395 with closest_mesh_hit_with_filter (686-723): with an
+  // AuxRng, a candidate hit on an alpha-tested instance draws u from it and
+  // is kept iff u < opacity; without one every hit is kept.
+  bool closest_hit(const Ray& ray, SceneHit* hit, TraversalStats* st = nullptr, AuxRng* aux = nullptr) const;
   // First accepted hit in the same visit order; used for occlusion-only queries.
   bool any_hit(const Ray& ray, float t_max, SceneHit* hit, TraversalStats* st = nullptr) const;
 };

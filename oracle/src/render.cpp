@@ -1,4 +1,6 @@
 // Oracle: per-sample rendering.  See render.h for the reference files restated.
+#include <cstdio>
+#include <cstdlib>
 #include "render.h"
 
 #include <atomic>
@@ -331,11 +333,11 @@ bool sample_li_triangle(const RenderScene& s, int inst, int tri, Vec3 p_ref, Vec
   return true;
 }
 
-bool closest(const RenderScene& s, Vec3 o, Vec3 d, SceneHit* h) {
+bool closest(const RenderScene& s, Vec3 o, Vec3 d, SceneHit* h, AuxRng* aux) {
   Ray r;
   r.origin = o;
   r.direction = d;
-  return s.geo.closest_hit(r, h);
+  return s.geo.closest_hit(r, h, nullptr, aux);
 }
 
 // point::sample_li (light/point.rs:32-50)
@@ -391,7 +393,7 @@ int sample_category(const RenderScene& s, float u, float* pmf) {
 // lights serve every scattering material.  Delta lights take no MIS weight.
 // wi_out (optional) receives the sampled light direction.
 Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
-                       Vec3* wi_out, int mode) {
+                       Vec3* wi_out, int mode, AuxRng* aux) {
   const bool non_area_only = mode == kDirectBdptNonArea, nee = mode == kDirectNee;
   float cat_pmf = 0.0f;
   int cat = sample_category(s, rnd.light.u_category, &cat_pmf);
@@ -463,7 +465,7 @@ Vec3 direct_light_impl(const RenderScene& s, const Material& m, const Vertex& v,
   if (cos_surface <= 0.0f) return Vec3(0, 0, 0);
   // unoccluded_ray (integrator/mod.rs:239-265)
   SceneHit h;
-  if (closest(s, offset_origin(v.p, v.ng, li.wi), li.wi, &h)) {
+  if (closest(s, offset_origin(v.p, v.ng, li.wi), li.wi, &h, aux)) {
     bool visible;
     if (li.inst >= 0) visible = h.instance == li.inst && h.triangle == li.tri;
     else if (std::isinf(li.distance)) visible = false;
@@ -506,8 +508,8 @@ float light_pdf_for_hit(const RenderScene& s, const Material& shading, const Ver
 }  // namespace
 
 Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd, Vec3* wi_out,
-                  int mode) {
-  return direct_light_impl(s, m, v, rnd, wi_out, mode);
+                  int mode, AuxRng* aux) {
+  return direct_light_impl(s, m, v, rnd, wi_out, mode, aux);
 }
 
 // orthonormal_basis.rs:11-56
@@ -533,7 +535,20 @@ Frame Frame::from_normal_and_tangent(Vec3 normal, Vec3 hint) {
   return f;
 }
 
+// Material::has_alpha_test and the clamped opacity any_hit compares u with
+// (normalized_lambert.rs:85-107, emissive.rs:96-118, material/open_pbr.rs:
+// 321-343), untextured: 1 for a material without an alpha test.
+float material_alpha(const Material& m) {
+  const float o = m.kind == kOpenPbr ? m.openpbr.geometry_opacity : m.opacity;
+  return o < 1.0f ? clampf(o, 0.0f, 1.0f) : 1.0f;
+}
+
 void RenderScene::finalize() {
+  geo.alpha.clear();
+  for (size_t i = 0; i < geo.instances.size(); ++i)
+    if (material_alpha(materials[geo.instances[i].material_index]) < 1.0f) geo.alpha.resize(geo.instances.size(), 1.0f);
+  if (!geo.alpha.empty())
+    for (size_t i = 0; i < geo.instances.size(); ++i) geo.alpha[i] = material_alpha(materials[geo.instances[i].material_index]);
   leaf_of.assign(geo.instances.size(), {});
   for (size_t i = 0; i < geo.instances.size(); ++i)
     if (may_emit(materials[geo.instances[i].material_index]))
@@ -671,8 +686,9 @@ Vec3 trace_pt(const RenderScene& s, const Ray& ray, const PathSampler& sampler, 
   Vec3 ro = ray.origin, rd = ray.direction;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    AuxRng aux(rnd.aux_rng_seed);  // pt.rs:29-33: the ray arriving at this depth draws from it
     SceneHit h;
-    if (!closest(s, ro, rd, &h)) {
+    if (!closest(s, ro, rd, &h, &aux)) {
       if (s.has_env) L += beta * s.env.radiance(rd);  // infinite_light_le
       break;
     }
@@ -709,8 +725,9 @@ Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
   bool count_emission = true;
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
+    AuxRng aux(rnd.aux_rng_seed);  // nee.rs:31-34: the arriving ray, then the light sample
     SceneHit h;
-    if (!closest(s, ro, rd, &h)) {
+    if (!closest(s, ro, rd, &h, &aux)) {
       if (count_emission && s.has_env) L += beta * s.env.radiance(rd);
       break;
     }
@@ -719,7 +736,7 @@ Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
     lock.stamp(v, beta);
     Vec3 le;
     if (count_emission && material_le(m, v, &le)) L += beta * le;
-    if (!is_pure_emitter(m)) L += beta * direct_light_impl(s, m, v, rnd, nullptr, kDirectNee);
+    if (!is_pure_emitter(m)) L += beta * direct_light_impl(s, m, v, rnd, nullptr, kDirectNee, &aux);
     MatSample bs;
     bool ok = m.kind == kOpenPbr ? openpbr_sample(m, v, rnd.material, &bs)
               : m.kind == kLambert ? lambert_sample(m, v, rnd.material.u_dir, &bs)
@@ -743,8 +760,9 @@ Vec3 trace_nee(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
 Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler, uint32_t max_depth) {
   Vec3 L(0, 0, 0), beta(1, 1, 1);
   PathLock lock;
+  AuxRng aux0(sampler.initial_aux_rng_seed());  // mis.rs:28-31
   SceneHit h;
-  if (!closest(s, ray.origin, ray.direction, &h)) return s.has_env ? s.env.radiance(ray.direction) : L;
+  if (!closest(s, ray.origin, ray.direction, &h, &aux0)) return s.has_env ? s.env.radiance(ray.direction) : L;
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
   const Material* m = &s.mat_of(h.instance);
   Vec3 le0;
@@ -752,8 +770,10 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
     lock.stamp(v, beta);
+    // mis.rs:52: the light sample's shadow ray, then the bounce ray, draw from it
+    AuxRng aux(rnd.aux_rng_seed);
     if (is_pure_emitter(*m)) break;
-    L += beta * direct_light(s, *m, v, rnd);
+    L += beta * direct_light(s, *m, v, rnd, nullptr, kDirectMis, &aux);
     MatSample bs;
     bool ok = m->kind == kOpenPbr ? openpbr_sample(*m, v, rnd.material, &bs)
                                   : lambert_sample(*m, v, rnd.material.u_dir, &bs);
@@ -766,7 +786,7 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
       beta /= q;
     }
     SceneHit nh;
-    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) {
+    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh, &aux)) {
       L += beta * env_escape(s, bs.wi, bs.delta, bs.pdf);
       break;
     }
@@ -777,6 +797,10 @@ Vec3 trace_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler,
       if (bs.delta) L += beta * le;
       else L += beta * le * balance(bs.pdf, light_pdf_for_hit(s, *m, v, nv));
     }
+    if (std::getenv("ORC_MIS_TRACE"))
+      std::fprintf(stderr, "mis d=%u hit inst %d tri %d t %.9g p (%.9g %.9g %.9g) wi (%.9g %.9g %.9g) beta (%.6g %.6g %.6g) pdf %.6g delta %d L (%.6g %.6g %.6g)\n",
+                   depth, nh.instance, nh.triangle, nh.t, nv.p.x, nv.p.y, nv.p.z, bs.wi.x, bs.wi.y, bs.wi.z, beta.x,
+                   beta.y, beta.z, bs.pdf, (int)bs.delta, L.x, L.y, L.z);
     v = nv;
     m = nm;
   }
@@ -787,8 +811,9 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
                 AdjointVertexSink& sink) {
   Vec3 R = L, beta(1, 1, 1);
   PathLock lock;
+  AuxRng aux0(sampler.initial_aux_rng_seed());
   SceneHit h;
-  if (!closest(s, ray.origin, ray.direction, &h)) return;
+  if (!closest(s, ray.origin, ray.direction, &h, &aux0)) return;
   Vertex v = s.shading_vertex(h.instance, h.triangle, h.bary, ray.direction);
   const Material* m = &s.mat_of(h.instance);
   uint32_t mi = s.geo.instances[h.instance].material_index;
@@ -797,9 +822,10 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
   for (uint32_t depth = 0; depth < max_depth; ++depth) {
     VertexRandoms rnd = sampler.path_vertex_randoms(depth);
     lock.stamp(v, beta);
+    AuxRng aux(rnd.aux_rng_seed);
     if (is_pure_emitter(*m)) break;
     Vec3 wl(0, 0, 0);
-    const Vec3 c = beta * direct_light(s, *m, v, rnd, &wl);
+    const Vec3 c = beta * direct_light(s, *m, v, rnd, &wl, kDirectMis, &aux);
     R = R - c;
     // a light sample at an OpenPBR vertex (directional lights): its
     // contribution scales with f at the light direction
@@ -817,7 +843,7 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
     }
     if (m->kind == kOpenPbr && !bs.delta) sink.vertex(mi, v, bs.wi, R);
     SceneHit nh;
-    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh)) break;  // R = the escape emission
+    if (!closest(s, offset_origin(v.p, v.ng, bs.wi), bs.wi, &nh, &aux)) break;  // R = the escape emission
     Vertex nv = s.shading_vertex(nh.instance, nh.triangle, nh.bary, bs.wi);
     const Material* nm = &s.mat_of(nh.instance);
     Vec3 le;

@@ -26,6 +26,7 @@ struct Material {
   Vec3 rho;        // NormalizedLambert
   Vec3 color;      // Emissive
   float strength = 0;
+  float opacity = 1;  // NormalizedLambert / Emissive opacity (OpenPBR: geometry_opacity)
   OpenPbrDesc openpbr{};   // OpenPbr
   OpenPbrLuts luts{};      // the tables the scene installed for it (scene/mod.rs:164-185)
 };
@@ -157,8 +158,9 @@ inline bool is_pure_emitter(const Material& m) { return m.kind == kEmissive; }
 // (integrator/nee.rs:104-150), no MIS weight and the plain environment
 // distribution.  wi_out (optional): the light direction.
 enum DirectMode : int { kDirectMis = 0, kDirectBdptNonArea = 1, kDirectNee = 2 };
+// aux: the AuxRng the shadow ray's alpha tests draw from (NULL: no alpha tests).
 Vec3 direct_light(const RenderScene& s, const Material& m, const Vertex& v, const VertexRandoms& rnd,
-                  Vec3* wi_out = nullptr, int mode = kDirectMis);
+                  Vec3* wi_out = nullptr, int mode = kDirectMis, AuxRng* aux = nullptr);
 // The environment's radiance along `dir` for a ray that left the scene after a
 // BSDF sample of pdf `bsdf_pdf` (`delta`: count it in full), MIS-weighted
 // against the environment's NEE pdf; zero without an environment.

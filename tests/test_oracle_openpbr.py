@@ -245,9 +245,8 @@ def test_material_sample_consistent_with_eval_and_pdf(mi):
     assert n_ok > 150
 
 
-def test_unsupported_parameters_are_rejected():
-    with pytest.raises(ValueError):
-        orc.OpenPbrMaterial({"geometry_opacity": 0.5})
+def test_every_untextured_parameter_is_supported():
+    orc.OpenPbrMaterial({"geometry_opacity": 0.5})
     orc.OpenPbrMaterial({"emission_luminance": 2.0})
     orc.OpenPbrMaterial({"transmission_weight": 0.5})
     orc.OpenPbrMaterial({"geometry_thin_walled": 1})

@@ -41,14 +41,15 @@ cudaError_t bounce_ops(const BounceKey& k, int cur, bool last, unsigned long lon
   if (e == cudaSuccess)
     e = launch_traverse_strided(k.S.geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
                                 B.h_inst, B.h_bary, B.capacity, c0, k.err, k.num_sms, s, nullptr, nullptr,
-                                B.counts + cur, k.jobs, k.jobs ? B.q_job[cur] : nullptr);
+                                B.counts + cur, k.jobs, k.jobs ? B.q_job[cur] : nullptr, nullptr, B.q_aux,
+                                B.q_slot[cur]);
   if (e == cudaSuccess)
     e = k.jobs ? launch_wf_shade_batch(k.jobs, B, cur, s, k.shade_block, k.batch_lights != 0)
                : launch_wf_shade(k.S.geo, k.S.d, k.P, B, cur, s, nullptr, k.shade_block);
   if (e == cudaSuccess && !last)
     e = launch_traverse_strided(k.S.geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
                                 nullptr, B.capacity, c1, k.err, k.num_sms, s, nullptr, nullptr, B.counts + 2, k.jobs,
-                                k.jobs ? B.s_job : nullptr);
+                                k.jobs ? B.s_job : nullptr, nullptr, B.s_aux);
   if (e == cudaSuccess && !last) e = launch_wf_resolve(B, s);
   return e;
 }

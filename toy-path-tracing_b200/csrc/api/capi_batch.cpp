@@ -111,7 +111,9 @@ tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   if ((st = cuda_check(ctx, cudaMemcpyAsync(ctx->d_jobs, dj.data(), n_jobs * sizeof(DevJob), cudaMemcpyHostToDevice, s),
                        "upload job table")))
     return st;
-  const WfBuffers& B = ctx->wf;
+  bool alpha = false;
+  for (int j = 0; j < n_jobs; ++j) alpha = alpha || jobs[j].scene->geo.inst_alpha != nullptr;
+  const WfBuffers B = wavefront_view(ctx->wf, alpha);
   float* samples = (float*)ctx->d_scratch;
   const DevGeometry no_geo{};
   bool lights = false;

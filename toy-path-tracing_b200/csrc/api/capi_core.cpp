@@ -633,6 +633,22 @@ tpt_status tpt_traverse_device(tpt_context* ctx, const tpt_scene* scene, const f
                     "traverse kernel launch");
 }
 
+tpt_status tpt_traverse_alpha_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n,
+                                     uint32_t* aux, int32_t* prim, float* t, int32_t* instance, float* bary,
+                                     void* stream) {
+  if (!ctx || !scene) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL context or scene");
+  if (n && (!rays || !aux || !prim || !t)) return set_error(ctx, TPT_ERR_INVALID_ARG, "NULL ray, state or output buffer");
+  tpt_status st = set_device(ctx);
+  if (st) return st;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  note_device_call(ctx, "tpt_traverse_alpha_device");
+  return cuda_check(ctx,
+                    launch_traverse_strided(scene->geo, rays, n, n, TPT_CLOSEST_HIT, prim, t, instance, bary, n,
+                                            next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr, nullptr,
+                                            nullptr, nullptr, nullptr, nullptr, aux),
+                    "traverse kernel launch");
+}
+
 tpt_status tpt_traverse_stats_device(tpt_context* ctx, const tpt_scene* scene, const float* rays, uint64_t n,
                                      int mode, int32_t* prim, float* t, uint32_t* node_tests, uint32_t* tri_tests,
                                      void* stream) {

@@ -84,14 +84,26 @@ tpt_status ensure_scratch(tpt_context* ctx, size_t bytes) {
   return TPT_OK;
 }
 
+// The arena as a render sees it: without alpha tests its AuxRng planes are
+// left out (NULL), so the stages skip that bookkeeping.
+WfBuffers wavefront_view(const WfBuffers& B, bool alpha) {
+  WfBuffers v = B;
+  if (!alpha) {
+    v.q_aux = nullptr;
+    v.s_aux = nullptr;
+    v.s_aux_cont = nullptr;
+  }
+  return v;
+}
+
 // Carves the wavefront arena for `capacity` path slots.
 tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   if (ctx->wf.capacity >= capacity && ctx->d_wf) return TPT_OK;
   const size_t C = capacity;
   // float planes: beta 3, L 3, prev 7, q_ray 2*7, h_t 1, h_bary 3, s_ray 7, s_contrib 3, s_t 1, s_dist 1
   // u32 planes: prev_mat, depth, q_slot 2, h_tri, h_inst, s_slot, s_target 2, s_tri, s_inst,
-  // job, q_job 2, s_job; lock 1
-  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4 + 1;
+  // job, q_job 2, s_job; lock 1; q_aux, s_aux, s_aux_cont
+  const size_t planes = 3 + 3 + 7 + 14 + 1 + 3 + 7 + 3 + 1 + 1 + 1 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 4 + 1 + 3;
   const size_t bytes = planes * C * 4 + 256;
   if (ctx->d_wf) {
     cudaDeviceSynchronize();
@@ -117,6 +129,9 @@ tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity) {
   B.prev_mat = (uint32_t*)take(1);
   B.depth = (uint32_t*)take(1);
   B.lock = (float*)take(1);
+  B.q_aux = (uint32_t*)take(1);
+  B.s_aux = (uint32_t*)take(1);
+  B.s_aux_cont = (uint32_t*)take(1);
   B.q_slot[0] = (uint32_t*)take(1);
   B.q_slot[1] = (uint32_t*)take(1);
   B.q_ray[0] = (float*)take(7);
@@ -148,8 +163,8 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
                             uint32_t n, float* samples, cudaStream_t s, const DevAdjoint* A) {
   tpt_status st = ensure_wavefront(ctx, n);
   if (st) return st;
-  const WfBuffers& B = ctx->wf;
   const DevGeometry& geo = job->scene->geo;
+  const WfBuffers B = wavefront_view(ctx->wf, geo.inst_alpha != nullptr);
   const DevRenderData& rd = job->scene->render;
   cudaError_t e = launch_wf_generate(geo, rd, L, B, first, n, s, A ? samples : nullptr);
   // direct launches for the adjoint replay and while render statistics are on
@@ -164,12 +179,12 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
     if (e == cudaSuccess)
       e = launch_traverse_strided(geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
                                   B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
-                                  nullptr, nullptr, B.counts + cur, nullptr, nullptr, tot);
+                                  nullptr, nullptr, B.counts + cur, nullptr, nullptr, tot, B.q_aux, B.q_slot[cur]);
     if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, cur, s, A);
     if (e == cudaSuccess && b < L.max_depth)
       e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
                                   nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
-                                  nullptr, B.counts + 2, nullptr, nullptr, tot ? tot + 4 : nullptr);
+                                  nullptr, B.counts + 2, nullptr, nullptr, tot ? tot + 4 : nullptr, B.s_aux);
     if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s, A);
   }
   if (e == cudaSuccess && !A) e = launch_wf_finalize(B, n, samples, s);
@@ -238,6 +253,14 @@ tpt_status ensure_bdpt_wavefront(tpt_context* ctx, uint32_t max_vertices) {
 
 tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
                                  uint64_t n, float* samples, cudaStream_t s) {
+  // Alpha tests draw every connection's visibility test from one AuxRng per
+  // sample, in connection order (bdpt.rs:81-121): the one-kernel execution,
+  // whose lanes run their connections in that order, renders such scenes.
+  if (job->scene->geo.inst_alpha)
+    return cuda_check(ctx,
+                      launch_render(job->scene->geo, job->scene->render, L, samples, first, n, ctx->d_err,
+                                    ctx->num_sms, s, next_counter(ctx)),
+                      "render kernel launch");
   tpt_status st = ensure_bdpt_wavefront(ctx, L.max_depth);
   if (st) return st;
   const BdWfBuffers& B = ctx->bd;

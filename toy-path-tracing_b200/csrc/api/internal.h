@@ -129,7 +129,10 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t stream,
                                     uint32_t* node_tests, uint32_t* tri_tests, const uint32_t* n_dev = nullptr,
                                     const DevJob* jobs = nullptr, const uint32_t* ray_job = nullptr,
-                                    unsigned long long* totals = nullptr);
+                                    unsigned long long* totals = nullptr, uint32_t* aux = nullptr,
+                                    const uint32_t* aux_index = nullptr);
+// aux: per-ray AuxRng states for the alpha tests (NULL: no alpha tests), read
+// at aux[aux_index ? aux_index[i] : i] and advanced in place by the draws.
 
 // qbvh_build_gpu.cu: the QBVH of n primitive boxes (device, n x 6 floats) built
 // on the device, equal to build_qbvh_host's (a box face at zero may be +0.0
@@ -170,6 +173,8 @@ cudaError_t launch_render_bdpt(const DevGeometry& geo, const DevRenderData& rd, 
 
 // capi_render.cpp: validates a job and derives its launch parameters.
 tpt_status render_launch_params(tpt_context* ctx, const tpt_render_job* job, RenderLaunch* out);
+// The wavefront arena with its alpha-test planes, or without them (NULL).
+WfBuffers wavefront_view(const WfBuffers& B, bool alpha);
 // The context's per-sample scratch (grown on demand) and wavefront arena.
 tpt_status ensure_scratch(tpt_context* ctx, size_t bytes);
 tpt_status ensure_wavefront(tpt_context* ctx, uint32_t capacity);

@@ -108,6 +108,26 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   for (uint32_t i = 0; i < desc->num_instances; ++i)
     if (desc->instances[i].material_index >= desc->num_materials && desc->num_materials)
       return set_error(ctx, TPT_ERR_INVALID_ARG, "instance " + std::to_string(i) + ": material index out of range");
+  // alpha tests (Material::has_alpha_test, untextured): per instance, the
+  // clamped opacity its hits are tested against, 1 for none
+  std::vector<float> ialpha;
+  {
+    std::vector<float> malpha(desc->num_materials, 1.0f);
+    bool any = false;
+    for (uint32_t i = 0; i < desc->num_materials; ++i) {
+      const tpt_material_desc& m = desc->materials[i];
+      const float o = m.kind == TPT_MATERIAL_OPENPBR ? m.openpbr->geometry_opacity : (m.has_opacity ? m.opacity : 1.0f);
+      if (o < 1.0f) {
+        malpha[i] = o < 0.0f ? 0.0f : o;
+        any = true;
+      }
+    }
+    if (any) {
+      ialpha.resize(desc->num_instances, 1.0f);
+      for (uint32_t i = 0; i < desc->num_instances; ++i)
+        if (desc->num_materials) ialpha[i] = malpha[desc->instances[i].material_index];
+    }
+  }
 
   // vertex attributes, concatenated per mesh
   std::vector<float> pos, nrm, uv;
@@ -276,7 +296,10 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
   if (!st) st = put(s, dpoints, &R.points);
   if (!st) st = put(s, dspots, &R.spots);
   if (!st) st = put(s, ddirs, &R.dirs);
+  const float* d_alpha = nullptr;
+  if (!st && !ialpha.empty()) st = put(s, ialpha, &d_alpha);
   if (st) return st;
+  s->geo.inst_alpha = d_alpha;
   R.num_area_lights = (uint32_t)dal.size();
   R.area_light_weight_sum = al_sum;
   R.cec_e = ctx->d_cec_e;

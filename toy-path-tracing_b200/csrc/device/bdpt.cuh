@@ -209,38 +209,43 @@ static __device__ __noinline__ float bdpt_mis(const DevRender& S, const BdVertex
 // contribution c if the two vertices see each other (zero when any other test
 // already makes it zero), and the visibility ray.  The reference tests
 // visibility first; each test here returns zero on its own, so the order does
-// not change the result and the shadow ray is traced only for non-zero c.
+// not change the result and the shadow ray is traced only for non-zero c --
+// except in scenes with alpha tests, where every visibility test draws from
+// the sample's AuxRng in connection order, so every pair at a non-zero
+// distance traces its ray.  Returns 0: no ray (coincident vertices), 1: a ray
+// and zero c, 2: a ray and non-zero c.
 struct BdConnection {
   V3 c, origin, dir;
   float dist;
 };
-__device__ __forceinline__ bool bdpt_connect_prepare(const DevRender& S, const BdVertex& lv, const BdVertex& cv,
-                                                     BdConnection& out) {
+__device__ __forceinline__ int bdpt_connect_prepare(const DevRender& S, const BdVertex& lv, const BdVertex& cv,
+                                                    BdConnection& out) {
   const V3 delta = cv.v.p - lv.v.p;
   const float dist2 = length_sq(delta);
-  if (dist2 <= 0.0f) return false;
+  if (dist2 <= 0.0f) return 0;
   const float dist = sqrtf(dist2);
   const V3 w_lc = delta / dist;
   const V3 w_cl = -w_lc;
+  out.origin = offset_origin(lv.v.p, lv.v.ng, w_lc);
+  out.dir = w_lc;
+  out.dist = dist;
+  out.c = V3{0.0f, 0.0f, 0.0f};
   const DevMaterialRec cm = S.d.mats[__ldg(&S.d.inst[cv.v.inst].material)];
   const V3 f_cam = material_eval(S, cm, cv.v, w_cl, false);
-  if (length_sq(f_cam) == 0.0f) return false;
+  if (length_sq(f_cam) == 0.0f) return 1;
   V3 f_light;
   if (lv.flags & kBdLight) {
-    if (dot(lv.v.ng, w_lc) <= 0.0f) return false;
+    if (dot(lv.v.ng, w_lc) <= 0.0f) return 1;
     f_light = V3{1.0f, 1.0f, 1.0f};
   } else {
     const DevMaterialRec lm = S.d.mats[__ldg(&S.d.inst[lv.v.inst].material)];
     f_light = material_eval(S, lm, lv.v, w_lc, true);
   }
-  if (length_sq(f_light) == 0.0f) return false;
+  if (length_sq(f_light) == 0.0f) return 1;
   const float g = fabsf(dot(lv.v.ng, w_lc)) * fabsf(dot(cv.v.ng, w_cl)) / dist2;
-  if (g <= 0.0f) return false;
+  if (g <= 0.0f) return 1;
   out.c = lv.v.thr * f_light * g * f_cam * cv.v.thr;
-  out.origin = offset_origin(lv.v.p, lv.v.ng, w_lc);
-  out.dir = w_lc;
-  out.dist = dist;
-  return true;
+  return 2;
 }
 
 // The subpaths and connections below are warp-synchronous: every lane of the
@@ -344,17 +349,22 @@ __device__ __forceinline__ void camera_step(const DevRender& S, const RenderLaun
   c.count_emission = s.delta;
 }
 
+// Alpha tests (aux non-NULL): one AuxRng per sample through both subpaths,
+// each depth reseeding it before its ray (bdpt.rs:160, 335), and then through
+// the connections' visibility tests in order (bdpt.rs:81-121).
 template <class Stack>
 __device__ __forceinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stack& st, bool valid,
                                                         const RenderLaunch& P, const PathSamplerDev& ps, V3 ro, V3 rd,
-                                                        BdVertex* vs, V3& L, uint32_t* err) {
+                                                        BdVertex* vs, V3& L, uint32_t* err, uint32_t* aux = nullptr) {
   BdCamState c;
   camera_state_init(c, valid);
   for (uint32_t depth = 0; depth < P.max_depth; ++depth) {
     const unsigned live = __ballot_sync(0xffffffffu, c.alive);
     if (!live) break;
     TraceResult h;
-    if (c.alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    if (aux && c.alive) *aux = aux_from_seed(ps, (int)depth);
+    if (c.alive)
+      trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err, aux);
     bool nee = false;
     DirectPrep dp;
     if (c.alive) camera_step<Stack>(S, P, ps, depth, h, ro, rd, vs, c, L, nee, dp);
@@ -363,7 +373,7 @@ __device__ __forceinline__ uint32_t bdpt_camera_subpath(const DevRender& S, Stac
       TraceResult hs;
       if (nee)
         trace_ray_ww<0>(S.geo, st, sm, dp.so.x, dp.so.y, dp.so.z, dp.wi.x, dp.wi.y, dp.wi.z,
-                        __int_as_float(0x7f800000), hs, err);
+                        __int_as_float(0x7f800000), hs, err, aux);
       if (nee && shadow_visible(hs.tri, hs.inst, hs.t, dp.inst, dp.tri, dp.dist)) L = L + dp.contrib;
     }
   }
@@ -483,7 +493,7 @@ __device__ __forceinline__ void light_step(const DevRender& S, const PathSampler
 template <class Stack>
 __device__ __forceinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack& st, bool valid,
                                                        const RenderLaunch& P, const PathSamplerDev& ps, BdVertex* vs,
-                                                       uint32_t* err) {
+                                                       uint32_t* err, uint32_t* aux = nullptr) {
   V3 ro, rd;
   BdLightState l;
   l.pending_pdf = 0.0f;
@@ -494,7 +504,9 @@ __device__ __forceinline__ uint32_t bdpt_light_subpath(const DevRender& S, Stack
     const unsigned live = __ballot_sync(0xffffffffu, l.alive);
     if (!live) break;
     TraceResult h;
-    if (l.alive) trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    if (aux && l.alive) *aux = aux_from_seed(ps, (int)depth);
+    if (l.alive)
+      trace_ray_ww<0>(S.geo, st, live, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err, aux);
     if (l.alive) light_step<Stack>(S, ps, depth, h, ro, rd, vs, l);
   }
   return l.n;
@@ -509,27 +521,33 @@ __device__ V3 trace_bdpt(const DevRender& S, Stack& st, bool valid, const Render
                          V3 ro, V3 rd, uint32_t* err) {
   BdVertex cam[kBdptMaxDepth], lig[kBdptMaxDepth];
   V3 L = V3{0.0f, 0.0f, 0.0f};
-  const uint32_t nc = bdpt_camera_subpath(S, st, valid, P, ps, ro, rd, cam, L, err);
-  const uint32_t nl = bdpt_light_subpath(S, st, valid, P, ps, lig, err);
+  const bool alpha = S.geo.inst_alpha != nullptr;
+  uint32_t aux_state = alpha ? aux_from_seed(ps, -1) : 0u;
+  uint32_t* aux = alpha ? &aux_state : nullptr;
+  const uint32_t nc = bdpt_camera_subpath(S, st, valid, P, ps, ro, rd, cam, L, err, aux);
+  const uint32_t nl = bdpt_light_subpath(S, st, valid, P, ps, lig, err, aux);
   const uint32_t np = valid ? nl * nc : 0u;
   const uint32_t max_np = __reduce_max_sync(0xffffffffu, np);
   for (uint32_t k = 0; k < max_np; ++k) {
     bool want = false;
+    int prep = 0;
     BdConnection cn;
     uint32_t li = 0, ci = 0;
     if (k < np) {
       li = k / nc;
       ci = k - li * nc;
-      if ((lig[li].flags & kBdConnectible) && (cam[ci].flags & kBdConnectible))
-        want = bdpt_connect_prepare(S, lig[li], cam[ci], cn);
+      if ((lig[li].flags & kBdConnectible) && (cam[ci].flags & kBdConnectible)) {
+        prep = bdpt_connect_prepare(S, lig[li], cam[ci], cn);
+        want = prep == 2 || (alpha && prep == 1);
+      }
     }
     const unsigned tm = __ballot_sync(0xffffffffu, want);
     if (!tm) continue;
     TraceResult h;
     if (want)
       trace_ray_ww<0>(S.geo, st, tm, cn.origin.x, cn.origin.y, cn.origin.z, cn.dir.x, cn.dir.y, cn.dir.z,
-                      __int_as_float(0x7f800000), h, err);
-    if (!want) continue;
+                      __int_as_float(0x7f800000), h, err, aux);
+    if (!want || prep != 2) continue;
     // visible_between (bdpt.rs:577-602)
     if (h.tri >= 0) {
       const bool target = (uint32_t)h.inst == cam[ci].v.inst && (uint32_t)h.tri == cam[ci].v.tri;

@@ -56,6 +56,9 @@ struct DevGeometry {
   uint32_t tlas_root_word;
   uint32_t num_instances;
   uint32_t pad;
+  // per instance: the opacity its material's alpha test compares an AuxRng
+  // draw with (1: no alpha test); NULL when no instance has one
+  const float* inst_alpha;
 };
 
 // Device-side error word (bit flags), read back by the host after each call.

@@ -211,6 +211,12 @@ static __device__ __noinline__ bool openpbr_sample(const DevRenderData& d, uint3
   return true;
 }
 
+// AuxRng::from_seed (aux_rng.rs:15-19) of the vertex's seed (path_sampler.rs:
+// offset 14) or, for `depth` < 0, of initial_aux_rng_seed (dimension 0x80000000)
+__device__ __forceinline__ uint32_t aux_from_seed(const PathSamplerDev& ps, int depth) {
+  return pcg_state_transition(ps.aux_rng_seed(depth < 0 ? 0x80000000u : vertex_dim((uint32_t)depth, kOffAuxSeed)));
+}
+
 // MaterialSampleRandoms::u_extra0..3 (offsets 9-12), drawn only for a
 // dispersive material (the only reader); zeros otherwise.
 __device__ __forceinline__ void extra_randoms(const DevRenderData& d, const DevMaterialRec& m,

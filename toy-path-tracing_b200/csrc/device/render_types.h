@@ -297,6 +297,12 @@ struct WfBuffers {
   uint32_t* prev_mat; // previous vertex material index, bit 31 = delta sample
   uint32_t* depth;    // vertices processed
   float* lock;        // the path's wavelength lock (< 0: none)
+  // alpha tests (NULL in renders without them): the AuxRng state each path's
+  // next bounce ray starts from (per slot), each shadow ray's, and whether a
+  // shadow ray's final state carries on to its path's bounce ray (MIS)
+  uint32_t* q_aux;
+  uint32_t* s_aux;
+  uint32_t* s_aux_cont;
   uint32_t* q_slot[2];
   float* q_ray[2];    // 7 planes each: o, d, tmax
   int32_t* h_tri;

@@ -13,7 +13,11 @@
 //    ray (glam Mat4::transform_point3/_vector3 order) and traverses its BLAS
 //    with the shared running t_max (scene/mod.rs:340-395, 686-723);
 //  - pbrt-v4 watertight triangle test with the f64 fallback (math/ray.rs:107-209);
-//    ties on t keep the later-tested triangle.
+//    ties on t keep the later-tested triangle;
+//  - closest_mesh_hit_with_filter's alpha test (scene/mod.rs:360-377, 686-723):
+//    when the caller passes an AuxRng state, a candidate hit on an instance
+//    whose material has an alpha test draws u from it (aux_rng.rs:21-28) and
+//    is kept iff u < the material's opacity, in the candidates' test order.
 // The library is compiled with -fmad=false so that no multiply-add is fused
 // unless written as fmaf (the reference's `mul_add`).
 #pragma once
@@ -190,13 +194,27 @@ struct TravState {
   uint32_t next;
   int sp, floor_sp;
   bool in_blas;
+  bool alpha_on;                       // an AuxRng state was given and the scene has alpha tests
   uint32_t node_base, tri_base, inst_id;
+  float alpha;                         // the current instance's opacity (1: no test)
+  uint32_t aux;                        // AuxRng state
 };
+
+// AuxRng::next_f32 (aux_rng.rs:21-28)
+__device__ __forceinline__ float aux_next_f32(uint32_t& state) {
+  state = state * 747796405u + 2891336453u;
+  uint32_t s = state;
+  s ^= s >> (4u + (s >> 28));
+  s *= 277803737u;
+  s ^= s >> 22;
+  return (float)(s >> 8) * (1.0f / 16777216.0f);
+}
 
 // Enter instance `id`'s BLAS with the ray transformed by world_to_local
 // (glam Mat4::transform_point3 / transform_vector3 order), scene/mod.rs:357.
 __device__ __forceinline__ void enter_instance(const DevGeometry& G, TravState& s, uint32_t id) {
   s.inst_id = id;
+  s.alpha = s.alpha_on ? __ldg(G.inst_alpha + id) : 1.0f;
   const DevInstance* I = G.instances + id;
   const float4 m0 = __ldg(&I->m0), m1 = __ldg(&I->m1), m2 = __ldg(&I->m2);
   const uint4 meta = __ldg(reinterpret_cast<const uint4*>(&I->node_base));
@@ -230,8 +248,12 @@ __device__ __forceinline__ void trav_pop(TravState& s, Stack& st) {
   s.next = st.get(--s.sp);
 }
 
+// aux: the ray's AuxRng state (NULL: no alpha tests), advanced by the draws
 __device__ __forceinline__ void trav_init(const DevGeometry& G, TravState& s, float ox, float oy, float oz, float dx,
-                                          float dy, float dz, float t_max) {
+                                          float dy, float dz, float t_max, const uint32_t* aux = nullptr) {
+  s.alpha_on = aux != nullptr && G.inst_alpha != nullptr;
+  s.aux = aux ? *aux : 0u;
+  s.alpha = 1.0f;
   s.wox = ox; s.woy = oy; s.woz = oz; s.wdx = dx; s.wdy = dy; s.wdz = dz;
   s.closest = t_max;
   s.res.t = __int_as_float(0x7f800000);
@@ -337,6 +359,8 @@ __device__ __forceinline__ void leaf_step(const DevGeometry& G, TravState& s, St
       if (STATS) cnt.tris++;
       float t, b0, b1, b2;
       if (tri_test(s.r, s.closest, tri, t, b0, b1, b2)) {
+        // any_hit of an alpha-tested material: keep the hit iff u < opacity
+        if (s.alpha < 1.0f && !(aux_next_f32(s.aux) < s.alpha)) continue;
         s.closest = t;
         s.res.t = t;
         s.res.tri = __float_as_int(tri.v0.w);
@@ -369,15 +393,16 @@ __device__ __forceinline__ void leaf_step(const DevGeometry& G, TravState& s, St
 template <int MODE, bool STATS, class Stack>
 __device__ __forceinline__ void trace_ray(const DevGeometry& G, Stack& st, float ox, float oy, float oz, float dx,
                                           float dy, float dz, float t_max, TraceResult& res, TraceCounters& cnt,
-                                          uint32_t* err) {
+                                          uint32_t* err, uint32_t* aux = nullptr) {
   TravState s;
-  trav_init(G, s, ox, oy, oz, dx, dy, dz, t_max);
+  trav_init(G, s, ox, oy, oz, dx, dy, dz, t_max, aux);
   if (STATS) { cnt.nodes = 0; cnt.tris = 0; }
   while (s.next != kNone) {
     if (!(s.next & kLeafBit)) node_step<STATS>(G, s, st, cnt, err);
     else leaf_step<MODE, STATS>(G, s, st, cnt, err);
   }
   res = s.res;
+  if (aux) *aux = s.aux;
 }
 
 // trace_ray for lanes that trace together: the lanes in `act` (all of which
@@ -387,10 +412,10 @@ __device__ __forceinline__ void trace_ray(const DevGeometry& G, Stack& st, float
 template <int MODE, class Stack>
 __device__ __forceinline__ void trace_ray_ww(const DevGeometry& G, Stack& st, unsigned act, float ox, float oy,
                                              float oz, float dx, float dy, float dz, float t_max, TraceResult& res,
-                                             uint32_t* err) {
+                                             uint32_t* err, uint32_t* aux = nullptr) {
   TravState s;
   TraceCounters c;
-  trav_init(G, s, ox, oy, oz, dx, dy, dz, t_max);
+  trav_init(G, s, ox, oy, oz, dx, dy, dz, t_max, aux);
   for (;;) {
     for (;;) {
       const bool want = !(s.next & kLeafBit);
@@ -401,6 +426,7 @@ __device__ __forceinline__ void trace_ray_ww(const DevGeometry& G, Stack& st, un
     if (!__any_sync(act, s.next != kNone)) break;
   }
   res = s.res;
+  if (aux) *aux = s.aux;
 }
 
 }  // namespace tpt

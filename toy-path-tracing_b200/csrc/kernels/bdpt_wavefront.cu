@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_connect(const __grid_constant__
   const BdVertex& cv = cam[ci];
   BdConnection cn;
   bool want = false;
-  if ((lv.flags & kBdConnectible) && (cv.flags & kBdConnectible)) want = bdpt_connect_prepare(S, lv, cv, cn);
+  if ((lv.flags & kBdConnectible) && (cv.flags & kBdConnectible)) want = bdpt_connect_prepare(S, lv, cv, cn) == 2;
   B.contrib[3 * (size_t)j] = 0.0f;
   B.contrib[3 * (size_t)j + 1] = 0.0f;
   B.contrib[3 * (size_t)j + 2] = 0.0f;

@@ -13,6 +13,12 @@
 // accumulated in the reference's order (emission of vertex d, its NEE, then
 // emission of vertex d + 1), so results equal the wavefront execution's bit
 // for bit.
+//
+// Alpha tests draw from the path's AuxRng in the order of the integrator
+// (mis.rs: the camera ray from the initial seed, then per vertex its seed for
+// the light sample's shadow ray and the bounce ray after it; nee.rs / pt.rs:
+// each depth's seed for the ray arriving there and, NEE, the light sample of
+// that vertex).
 #include "../api/internal.h"
 #include "../device/render.cuh"
 
@@ -52,6 +58,8 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
   float prev_pdf = 0.0f;
   uint32_t prev_mat = 0;       // material index, bit 31: delta sample
   float lock = -1.0f;          // the path's wavelength lock (< 0: none)
+  uint32_t aux = 0, bounce_aux = 0;  // AuxRng state; the state the pending bounce ray starts from (NEE, PT)
+  const bool alpha = S.geo.inst_alpha != nullptr;
   PathSamplerDev ps;
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, k == -1);
@@ -80,6 +88,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
           L = V3{0.0f, 0.0f, 0.0f};
           beta = V3{1.0f, 1.0f, 1.0f};
           lock = -1.0f;
+          if (alpha) aux = aux_from_seed(ps, P.integrator == kIntegMis ? -1 : 0);
           bounce_pending = false;
         } else {
           k = -2;
@@ -90,7 +99,8 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
     const unsigned act = __ballot_sync(0xffffffffu, k >= 0);
     if (k < 0) continue;
     TraceResult h;
-    trace_ray_ww<0>(S.geo, st, act, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err);
+    trace_ray_ww<0>(S.geo, st, act, ro.x, ro.y, ro.z, rd.x, rd.y, rd.z, __int_as_float(0x7f800000), h, err,
+                    alpha ? &aux : nullptr);
     bool done = false;
     if (kind == kRayShadow) {
       // unoccluded_ray (integrator/mod.rs:239-265)
@@ -98,6 +108,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
       if (bounce_pending) {
         ro = bo;
         rd = bd;
+        if (alpha && P.integrator != kIntegMis) aux = bounce_aux;  // MIS continues after the shadow ray
         kind = kRayBounce;
         bounce_pending = false;
       } else {
@@ -135,6 +146,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
       if (depth >= P.max_depth || m.kind == kDevEmissive) {
         done = true;  // pure emitter: no NEE, and sample() is None
       } else {
+        if (alpha && P.integrator == kIntegMis) aux = aux_from_seed(ps, (int)depth);
         float us0, us1;
         ps.sample_2d(vertex_dim(depth, kOffSurface), us0, us1);
         const float u_tree = ps.sample_1d(vertex_dim(depth, kOffTree));
@@ -167,6 +179,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
             prev_pdf = s.pdf;
             prev_mat = mi | (s.delta ? 0x80000000u : 0u);
             depth = depth + 1;
+            if (alpha && P.integrator != kIntegMis) bounce_aux = aux_from_seed(ps, (int)depth);
           }
         }
         if (nee) {
@@ -178,6 +191,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
           ro = bo;
           rd = bd;
           kind = kRayBounce;
+          if (alpha && P.integrator != kIntegMis) aux = bounce_aux;
         } else {
           done = true;
         }

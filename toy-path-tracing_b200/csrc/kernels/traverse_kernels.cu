@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
                     float* __restrict__ bary, uint32_t* __restrict__ node_tests, uint32_t* __restrict__ tri_tests,
                     unsigned long long* __restrict__ counter, const uint32_t* __restrict__ n_dev, uint32_t* err,
                     const DevJob* __restrict__ jobs, const uint32_t* __restrict__ ray_job,
-                    unsigned long long* __restrict__ totals) {
+                    unsigned long long* __restrict__ totals, uint32_t* __restrict__ aux,
+                    const uint32_t* __restrict__ aux_index) {
   if (n_dev) n = *n_dev;  // queue length produced on the device (wavefront stages)
   DevGeometry lane_geo;  // BATCH: the scene of this lane's ray
   const DevGeometry& G = BATCH ? lane_geo : geo;
@@ -71,7 +72,7 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
           const float dx = __ldcs(rays + 3 * rs + i), dy = __ldcs(rays + 4 * rs + i), dz = __ldcs(rays + 5 * rs + i);
           const float tmax = MODE == 0 ? __int_as_float(0x7f800000) : __ldcs(rays + 6 * rs + i);
           if (BATCH) lane_geo = jobs[__ldg(ray_job + i)].render.geo;
-          trav_init(G, s, ox, oy, oz, dx, dy, dz, tmax);
+          trav_init(G, s, ox, oy, oz, dx, dy, dz, tmax, aux ? aux + (aux_index ? aux_index[i] : i) : nullptr);
           if (STATS) { c.nodes = 0; c.tris = 0; }
         } else {
           ray = -2;
@@ -102,6 +103,7 @@ __global__ void __launch_bounds__(kBlock, TPT_TRAV_MINB)
       const uint64_t i = (uint64_t)ray;
       __stcs(prim + i, s.res.tri);
       __stcs(tout + i, s.res.t);
+      if (aux) aux[aux_index ? aux_index[i] : i] = s.aux;
       if (inst) __stcs(inst + i, s.res.inst);
       if (BARY) {
         __stcs(bary + i, s.res.b0);
@@ -151,7 +153,8 @@ template <int MODE, bool STATS, bool BARY, bool BATCH>
 static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t rs, uint64_t n, uint64_t bs,
                             int32_t* prim, float* t, int32_t* inst, float* bary, uint32_t* nt, uint32_t* tt,
                             unsigned long long* counter, const uint32_t* n_dev, uint32_t* err, int num_sms,
-                            cudaStream_t s, const DevJob* jobs, const uint32_t* ray_job, unsigned long long* totals) {
+                            cudaStream_t s, const DevJob* jobs, const uint32_t* ray_job, unsigned long long* totals,
+                            uint32_t* aux, const uint32_t* aux_index) {
   if (n == 0) return cudaSuccess;
   static int blocks_per_sm = 0;
   if (blocks_per_sm == 0) {
@@ -165,7 +168,7 @@ static cudaError_t launch_t(const DevGeometry& geo, const float* rays, uint64_t 
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   traverse_kernel<MODE, STATS, BARY, BATCH><<<(unsigned)blocks, kBlock, 0, s>>>(
-      geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, jobs, ray_job, totals);
+      geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, jobs, ray_job, totals, aux, aux_index);
   return cudaGetLastError();
 }
 
@@ -173,12 +176,13 @@ cudaError_t launch_traverse_strided(const DevGeometry& geo, const float* rays, u
                                     int32_t* prim, float* t, int32_t* inst, float* bary, uint64_t bs,
                                     unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
                                     uint32_t* nt, uint32_t* tt, const uint32_t* n_dev, const DevJob* jobs,
-                                    const uint32_t* ray_job, unsigned long long* totals) {
+                                    const uint32_t* ray_job, unsigned long long* totals, uint32_t* aux,
+                                    const uint32_t* aux_index) {
   const bool stats = nt != nullptr || totals != nullptr;
   const bool b = bary != nullptr;
 #define TPT_L(M, S, B, J) \
   launch_t<M, S, B, J>(geo, rays, rs, n, bs, prim, t, inst, bary, nt, tt, counter, n_dev, err, num_sms, s, jobs, \
-                       ray_job, totals)
+                       ray_job, totals, aux, aux_index)
   if (jobs) {  // batched wavefront: closest hit, with or without barycentrics
     if (mode != 0 || stats) return cudaErrorInvalidValue;
     if (b) return TPT_L(0, false, true, true);

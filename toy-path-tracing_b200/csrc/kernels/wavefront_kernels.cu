@@ -118,6 +118,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(const __grid_constant__ 
   }
   B.depth[i] = 0;
   B.lock[i] = -1.0f;
+  // alpha tests: the camera ray's AuxRng (mis.rs: the initial seed; nee.rs /
+  // pt.rs: depth 0's seed)
+  if (B.q_aux && (BATCH ? jobs[jb].render.geo.inst_alpha : S0.geo.inst_alpha) != nullptr)
+    B.q_aux[i] = aux_from_seed(ps, P.integrator == kIntegMis ? -1 : 0);
 }
 
 // One vertex per queue entry of queue `cur`; appends to queue `cur ^ 1` and the shadow queue.
@@ -147,6 +151,11 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
   DirectPrep dp;
   V3 beta = V3{B.beta[slot], B.beta[C + slot], B.beta[2 * C + slot]};
   V3 L = V3{B.L[slot], B.L[C + slot], B.L[2 * C + slot]};
+  // alpha tests (integrator order, see render_kernels.cu): the shadow ray's
+  // AuxRng start, the bounce ray's, and whether the bounce continues from the
+  // shadow ray's final state (MIS; the resolve stage copies it over)
+  const bool alpha = B.q_aux != nullptr && S.geo.inst_alpha != nullptr;
+  uint32_t sh_aux = 0, nx_aux = 0, aux_cont = 0;
   const int32_t tri = B.h_tri[j];
   if (tri >= 0) {
     TraceResult h;
@@ -192,6 +201,15 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
       const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
       PathSamplerDev ps;
       ps.init(pixel % P.width, pixel / P.width, sample, P.log2_spp, P.n_base4_digits);
+      if (alpha) {
+        if (P.integrator == kIntegMis) {
+          sh_aux = nx_aux = aux_from_seed(ps, (int)d);
+          aux_cont = 1u;
+        } else {
+          sh_aux = B.q_aux[slot];  // NEE: after the arriving ray's draws
+          nx_aux = aux_from_seed(ps, (int)d + 1);
+        }
+      }
       float us0, us1;
       ps.sample_2d(vertex_dim(d, kOffSurface), us0, us1);
       const float u_tree = ps.sample_1d(vertex_dim(d, kOffTree));
@@ -288,6 +306,7 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
     q[6 * C + qn] = __int_as_float(0x7f800000);
     B.q_slot[nxt][qn] = slot;
     if (BATCH) B.q_job[nxt][qn] = jb;
+    if (alpha) B.q_aux[slot] = nx_aux;
   }
   if (push_shadow) {
     float* q = B.s_ray;
@@ -300,6 +319,12 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
     q[6 * C + qs] = __int_as_float(0x7f800000);
     B.s_slot[qs] = slot;
     if (BATCH) B.s_job[qs] = jb;
+    if (alpha) {
+      B.s_aux[qs] = sh_aux;
+      B.s_aux_cont[qs] = aux_cont;
+    } else if (B.s_aux_cont) {
+      B.s_aux_cont[qs] = 0u;  // a batch mixes scenes with and without alpha tests
+    }
     B.s_target[qs] = dp.inst;
     B.s_target[C + qs] = dp.tri;
     if (LIGHTS) B.s_dist[qs] = dp.dist;
@@ -326,6 +351,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_resolve(WfBuffers B, const __grid
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= B.counts[2]) return;
   const uint32_t C = B.capacity;
+  // MIS with alpha tests: the bounce ray continues the shadow ray's AuxRng
+  if (B.s_aux_cont && B.s_aux_cont[j]) B.q_aux[B.s_slot[j]] = B.s_aux[j];
   const uint32_t tgt_inst = B.s_target[j];
   // the distance plane is written for delta-light shadow rays only
   const bool visible = shadow_visible(B.s_tri[j], B.s_inst[j], B.s_t[j], tgt_inst, B.s_target[C + j],

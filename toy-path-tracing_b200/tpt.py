@@ -119,6 +119,8 @@ class MaterialDesc(C.Structure):
         ("color", C.c_float * 3),
         ("strength", C.c_float),
         ("openpbr", C.c_void_p),
+        ("has_opacity", C.c_uint32),
+        ("opacity", C.c_float),
     ]
 
 
@@ -270,6 +272,7 @@ EXPORTED_SYMBOLS = [
     "tpt_traverse",
     "tpt_traverse_device",
     "tpt_traverse_stats_device",
+    "tpt_traverse_alpha_device",
     "tpt_scene_light_tree",
     "tpt_render",
     "tpt_render_device",
@@ -321,6 +324,7 @@ def _declare(L):
         "tpt_traverse": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp]),
         "tpt_traverse_device": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp, vp]),
         "tpt_traverse_stats_device": (i32, [vp, vp, vp, u64, i32, vp, vp, vp, vp, vp]),
+        "tpt_traverse_alpha_device": (i32, [vp, vp, vp, u64, vp, vp, vp, vp, vp, vp]),
         "tpt_scene_light_tree": (i32, [vp, C.POINTER(LightTreeView)]),
         "tpt_render": (i32, [vp, C.POINTER(RenderJob), i32, C.POINTER(C.c_void_p)]),
         "tpt_render_device": (i32, [vp, C.POINTER(RenderJob), vp, vp]),
@@ -559,6 +563,9 @@ def scene_desc(meshes, instances, tlas=None, materials=None, light_tree=None, li
         d.rho[:] = list(np.asarray(m.get("rho", (0, 0, 0)), np.float32))
         d.color[:] = list(np.asarray(m.get("color", (0, 0, 0)), np.float32))
         d.strength = float(np.float32(m.get("strength", 0.0)))
+        if "opacity" in m:
+            d.has_opacity = 1
+            d.opacity = float(np.float32(m["opacity"]))
         if d.kind == OPENPBR:
             od = openpbr_desc(m)
             keep.append(od)
@@ -754,6 +761,19 @@ class Scene:
         if want_bary:
             out["bary"] = bary
         return out
+
+    def traverse_alpha_device(self, rays_ptr: int, n: int, aux_ptr: int, prim_ptr: int, t_ptr: int, inst_ptr=None,
+                              bary_ptr=None, stream=None):
+        """`tpt_traverse_alpha_device`: closest hit with the materials' alpha tests,
+        drawing from (and advancing) the per-ray AuxRng states at aux_ptr."""
+        _check(
+            lib().tpt_traverse_alpha_device(
+                self.ctx.h, self.h, C.c_void_p(rays_ptr), n, C.c_void_p(aux_ptr), C.c_void_p(prim_ptr),
+                C.c_void_p(t_ptr), C.c_void_p(inst_ptr) if inst_ptr else None,
+                C.c_void_p(bary_ptr) if bary_ptr else None, _stream(stream),
+            ),
+            self.ctx,
+        )
 
     def traverse_device(self, rays_ptr: int, n: int, mode: int, prim_ptr: int, t_ptr: int, inst_ptr=None,
                         bary_ptr=None, stream=None):
