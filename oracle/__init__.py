@@ -117,7 +117,6 @@ def _declare(L):
         "orc_openpbr_params_eval_batch": (None, [vp, i32, f32, f32, vp, vp, u64, i32, vp, vp]),
         "orc_eon_eval_batch": (None, [vp, f32, vp, vp, u64, vp, vp]),
         "orc_eon_sample": (i32, [vp, f32, vp, f32, f32, vp]),
-        "orc_openpbr_unsupported": (C.c_char_p, [vp]),
         "orc_openpbr_eval": (None, [vp, i32, vp, vp, i32, vp]),
         "orc_openpbr_pdf": (f32, [vp, i32, vp, vp]),
         "orc_openpbr_sample": (i32, [vp, i32, vp, f32, f32, f32, i32, vp]),
@@ -705,9 +704,6 @@ class OpenPbrMaterial:
 
     def __init__(self, m: dict):
         self.rec = pack_openpbr(m)
-        why = lib().orc_openpbr_unsupported(_p(self.rec))
-        if why:
-            raise ValueError(why.decode())
 
     def eval(self, wo, wi, front=True, mode=0, throughput=1.0, lock=None):
         out = np.zeros(3, np.float32)

@@ -213,7 +213,6 @@ int orc_eon_sample(const float* rho, float r, const float* wo, float u0, float u
 }
 
 // Material-level queries: make_bsdf of an untextured material for a local wo.
-const char* orc_openpbr_unsupported(const void* desc) { return openpbr_unsupported(*(const OpenPbrDesc*)desc); }
 void orc_openpbr_eval(const void* desc, int front, const float* wo, const float* wi, int mode, float* out3) {
   OpenPbrBsdf b = bsdf_from_desc((const OpenPbrDesc*)desc, front, wo);
   put3(out3, b.eval(Vec3(wo[0], wo[1], wo[2]), Vec3(wi[0], wi[1], wi[2]), (TransportMode)mode));
@@ -286,8 +285,6 @@ void orc_camera_rgb_basis_at(float lambda_nm, float* out3) { put3(out3, camera_r
 const char* orc_render_scene_set_openpbr(void* h, uint32_t index, const void* desc) {
   auto* s = (RenderScene*)h;
   const OpenPbrDesc& d = *(const OpenPbrDesc*)desc;
-  const char* why = openpbr_unsupported(d);
-  if (*why) return why;
   s->materials[index].openpbr = d;
   s->materials[index].luts = openpbr_luts_for(d, threads_or_default(0));
   return "";

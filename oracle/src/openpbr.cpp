@@ -1209,8 +1209,6 @@ float openpbr_specular_eta(const OpenPbrDesc& m) {
   return modulated_eta(fmax_num(m.specular_ior, 1.0e-4f), fmax_num(m.specular_weight, 0.0f));
 }
 
-const char* openpbr_unsupported(const OpenPbrDesc&) { return ""; }
-
 // OpenPbrMaterial::make_bsdf (material/open_pbr.rs:393-487) and its helpers
 // (effective roughness 749-783, coat darkening 823-858) without textures.
 OpenPbrParams make_openpbr_params(const OpenPbrDesc& m, bool front_face, Vec3 wo_local) {

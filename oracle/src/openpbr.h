@@ -179,7 +179,5 @@ OpenPbrParams make_openpbr_params(const OpenPbrDesc& m, bool front_face, Vec3 wo
 // The dielectric eta whose albedo table the specular lobe reads
 // (OpenPbrMaterial::requires_specular_eta, material/open_pbr.rs:293-298).
 float openpbr_specular_eta(const OpenPbrDesc& m);
-// Empty string when the oracle covers every parameter of `m`.
-const char* openpbr_unsupported(const OpenPbrDesc& m);
 
 }  // namespace orc

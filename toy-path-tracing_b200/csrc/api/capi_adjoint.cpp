@@ -106,8 +106,6 @@ tpt_status tpt_scene_set_openpbr(tpt_context* ctx, tpt_scene* scene, uint32_t co
     const uint32_t m = material_ids[k];
     if (m >= scene->opbr_of_material.size() || scene->opbr_of_material[m] == kInvalidNode)
       return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(m) + " is not an OpenPBR material");
-    const std::string why = openpbr_unsupported(descs[k]);
-    if (!why.empty()) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(m) + ": " + why);
     // the light tree and the material record were built from the uploaded emission
     const tpt_openpbr_desc& old = scene->opbr_desc[scene->opbr_of_material[m]];
     if (descs[k].emission_luminance != old.emission_luminance ||

@@ -84,8 +84,6 @@ tpt_status upload_render_data(tpt_scene* s, const tpt_scene_desc* desc) {
     uint32_t opbr_index = 0;
     if (m.kind == TPT_MATERIAL_OPENPBR) {
       if (!m.openpbr) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": openpbr is NULL");
-      const std::string why = openpbr_unsupported(*m.openpbr);
-      if (!why.empty()) return set_error(ctx, TPT_ERR_INVALID_ARG, "material " + std::to_string(i) + ": " + why);
       DevOpenPbr rec;
       tpt_status st = lower_openpbr_material(ctx, *m.openpbr, &rec);
       if (st) return st;

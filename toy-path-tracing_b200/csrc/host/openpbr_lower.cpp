@@ -205,8 +205,6 @@ float radical_inverse_base3(uint32_t n) {
 }
 }  // namespace
 
-std::string openpbr_unsupported(const tpt_openpbr_desc&) { return ""; }
-
 float openpbr_spec_table_eta(const tpt_openpbr_desc& m) {
   return sanitize_eta(modulated_eta(std::fmax(m.specular_ior, 1.0e-4f), std::fmax(m.specular_weight, 0.0f)));
 }

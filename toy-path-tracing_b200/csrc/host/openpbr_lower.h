@@ -15,8 +15,6 @@ constexpr int kDaLen = 64 * 16 * 64 * 16;
 constexpr int kCecLen = 64 * 64, kCecAvgLen = 64;
 constexpr int kDecLen = 32 * 32 * 32, kDecAvgLen = 32 * 32;
 
-// Empty when the device path covers every parameter of `m`.
-std::string openpbr_unsupported(const tpt_openpbr_desc& m);
 // The eta of the specular albedo table (OpenPbrMaterial::requires_specular_eta)
 // and of the coat table (requires_coat_eta), sanitized as the table cache does.
 float openpbr_spec_table_eta(const tpt_openpbr_desc& m);

@@ -209,6 +209,12 @@ def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPEN
     (Abbe number 20 at scale 1).  The walls keep their diffuse materials
     (OpenPBR, or NormalizedLambert)."""
     sc = cornell_box(seed, material)
+    # the glass boxes float 2 mm above the floor: a box bottom coplanar with
+    # the floor, reached from inside the glass, is a tie between two
+    # instances whose winner a last-bit difference in the ray decides
+    a1, a2 = sc["angles"]
+    sc["instances"][5] = instance_matrix(5, 5, _trs((-0.55, 0.002, -0.45), a1, (0.9, 1.8, 0.9)))
+    sc["instances"][6] = instance_matrix(5, 6, _trs((0.6, 0.002, 0.5), -a2, (0.9, 0.9, 0.9)))
     thin = 1 if thin_walled else 0
     sc["materials"][5] = {"kind": OPENPBR, "base_color": np.array([0.8, 0.8, 0.8], np.float32),
                           "specular_roughness": 0.25, "transmission_weight": 1.0, "geometry_thin_walled": thin}
