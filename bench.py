@@ -684,9 +684,10 @@ def adjoint_block(ctx, args, cpu=True):
     losses = []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.adjoint_steps):
+    for step in range(args.adjoint_steps):
         opt.zero_grad()
-        im = RenderFunction.apply(params, scene, job, list(range(64)), tpt_scenes.patch_material, mask)
+        sjob = scene.job(sc["camera"], W, W, spp, depth, seed=step + 1)  # fresh sample streams every step
+        im = RenderFunction.apply(params, scene, sjob, list(range(64)), tpt_scenes.patch_material, mask)
         loss = ((im - target) ** 2).sum()
         loss.backward()
         opt.step()
@@ -702,7 +703,8 @@ def adjoint_block(ctx, args, cpu=True):
     true = sc["params"]
     out["inverse_rendering"] = {"steps": args.adjoint_steps, "lr": 0.003, "loss_first": losses[0],
                                 "loss_last": losses[-1], "seconds": adam_s,
-                                "backward": "decorrelated: the adjoint replays the job at spp + 1",
+                                "sample_streams": "seed = step + 1 per forward; the backward replays the "
+                                                  "forward seed + ADJOINT_SEED_STEP (independent paths)",
                                 "image_loss_256spp_start": clean_start, "image_loss_256spp_end": clean_loss(p_end),
                                 "param_mae_start": float(np.abs(start - true).mean()),
                                 "param_mae_end": float(np.abs(p_end - true).mean()),

@@ -426,6 +426,13 @@ typedef struct tpt_render_job {
   uint32_t max_depth; /* --depth */
   uint32_t integrator;
   uint32_t execution; /* tpt_execution; both give the same image bit for bit */
+  /* Scramble seed of the per-pixel sample streams (no counterpart in the
+   * reference, whose PathSampler scrambles with the constant 0,
+   * path_sampler.rs:77): 0 gives the reference's streams and images; any other
+   * value gives statistically independent streams of the same sampler (for
+   * independent replicas, and for an adjoint whose paths are not the forward
+   * image's). */
+  uint32_t seed;
 } tpt_render_job;
 
 /* Path slots of the wavefront pipeline's queues: a render is processed in

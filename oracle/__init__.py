@@ -87,9 +87,9 @@ def _declare(L):
         "orc_render_scene_free": (None, [vp]),
         "orc_render_scene_set_materials": (None, [vp, vp, vp, vp, vp, u32]),
         "orc_render_scene_set_light_tree": (None, [vp, vp, u64, u32]),
-        "orc_render_pixels": (None, [vp, vp, u32, u32, u32, u32, u32, u32, u32, vp, i32]),
-        "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u32, u64, u64, vp, i32]),
-        "orc_render_adjoint": (None, [vp, vp, u32, u32, u32, u32, vp, u32, C.c_float, vp, i32]),
+        "orc_render_pixels": (None, [vp, vp, u32, u32, u32, u32, u32, u32, u32, vp, i32, u32]),
+        "orc_render_samples": (None, [vp, vp, u32, u32, u32, u32, u32, u64, u64, vp, i32, u32]),
+        "orc_render_adjoint": (None, [vp, vp, u32, u32, u32, u32, vp, u32, C.c_float, vp, i32, u32]),
         "orc_geometry_step_sequence": (None, [vp, vp, u64, vp, u32, i32]),
         "orc_render_direct_light": (None, [vp, i32, i32, vp, vp, f32, f32, f32, f32, vp, i32]),
         "orc_render_env_escape": (None, [vp, vp, vp, f32, i32, vp]),
@@ -457,27 +457,28 @@ class RenderScene:
         if integrator not in (0, 1, 2, 3):
             raise ValueError("integrator: 0 MIS, 1 BDPT, 2 NEE, 3 PT")
 
-    def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0):
+    def render(self, camera, width, height, spp, max_depth, pixels=None, nthreads=None, integrator=0, seed=0):
         """Image rows [p0, p1) of pixels (flattened y*width+x); returns float32 [n, 3].
         integrator: 0 MIS (integrator/mis.rs), 1 BDPT (integrator/bdpt.rs), 2 NEE
-        (integrator/nee.rs), 3 PT (integrator/pt.rs)."""
+        (integrator/nee.rs), 3 PT (integrator/pt.rs).  seed: the sample streams'
+        scramble seed (0: the reference's)."""
         self._check_integrator(integrator)
         p0, p1 = pixels if pixels is not None else (0, width * height)
         out = np.empty((p1 - p0, 3), np.float32)
         cam = self._cam(camera)
         lib().orc_render_pixels(self.h, _p(cam), width, height, spp, max_depth, integrator, p0, p1, _p(out),
-                                nthreads or os.cpu_count() or 1)
+                                nthreads or os.cpu_count() or 1, seed)
         return out
 
-    def samples(self, camera, width, height, spp, max_depth, first, count, nthreads=None, integrator=0):
+    def samples(self, camera, width, height, spp, max_depth, first, count, nthreads=None, integrator=0, seed=0):
         self._check_integrator(integrator)
         out = np.empty((count, 3), np.float32)
         cam = self._cam(camera)
         lib().orc_render_samples(self.h, _p(cam), width, height, spp, max_depth, integrator, first, count, _p(out),
-                                 nthreads or os.cpu_count() or 1)
+                                 nthreads or os.cpu_count() or 1, seed)
         return out
 
-    def adjoint(self, camera, width, height, spp, max_depth, d_image, mask=31, step=1e-3, nthreads=None):
+    def adjoint(self, camera, width, height, spp, max_depth, d_image, mask=31, step=1e-3, nthreads=None, seed=0):
         """Path-replay adjoint (MIS): dLoss/d(OpenPBR parameters) per material,
         float64 [n_materials, 7] = base_color rgb, specular_roughness,
         base_metalness, specular_ior, coat_weight; d_image = dLoss/dimage."""
@@ -486,7 +487,7 @@ class RenderScene:
         out = np.zeros((self.n_materials, 7), np.float64)
         cam = self._cam(camera)
         lib().orc_render_adjoint(self.h, _p(cam), width, height, spp, max_depth, _p(d), mask, float(step), _p(out),
-                                 nthreads or os.cpu_count() or 1)
+                                 nthreads or os.cpu_count() or 1, seed)
         return out
 
     # -- unit-level queries (reference integrator unit tests) -------------------

@@ -167,7 +167,7 @@ void render_adjoint(const RenderScene& s, const RenderJob& job, const float* d_i
       sink.delta = Vec3(d_image[3 * pixel], d_image[3 * pixel + 1], d_image[3 * pixel + 2]) * scale;
       const uint32_t px = pixel % job.width, py = pixel / job.width;
       for (uint32_t i = 0; i < job.spp; ++i) {
-        PathSampler ps(px, py, i, job.spp, job.width, job.height);
+        PathSampler ps(px, py, i, job.spp, job.width, job.height, job.seed);
         Vec2 us = ps.camera_sample();
         Ray r = job.cam.generate_ray_differential(job.width, job.height, px, py, us, job.spp);
         const Vec3 L = trace_mis(s, r, ps, job.max_depth);
@@ -190,7 +190,8 @@ extern "C" {
 // cam11: eye(3) look_at(3) up(3) fov_y exposure.  mask bits: 1 base colour,
 // 2 specular roughness, 4 metalness, 8 specular ior, 16 coat weight.
 void orc_render_adjoint(void* h, const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth,
-                        const float* d_image, uint32_t mask, float step, double* grad, int nthreads) {
+                        const float* d_image, uint32_t mask, float step, double* grad, int nthreads,
+                        uint32_t seed) {
   using namespace orc;
   RenderJob j;
   j.cam = Camera::make(Vec3(cam11[0], cam11[1], cam11[2]), Vec3(cam11[3], cam11[4], cam11[5]),
@@ -200,6 +201,7 @@ void orc_render_adjoint(void* h, const float* cam11, uint32_t w, uint32_t hgt, u
   j.spp = spp;
   j.max_depth = depth;
   j.integrator = 0;
+  j.seed = seed;
   render_adjoint(*(const RenderScene*)h, j, d_image, mask, step, grad, nthreads);
 }
 

@@ -98,7 +98,7 @@ void orc_render_scene_set_light_tree(void* h, const void* nodes, uint64_t n, uin
 }
 
 static RenderJob make_job(const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth,
-                          uint32_t integrator) {
+                          uint32_t integrator, uint32_t seed) {
   RenderJob j;
   j.cam = Camera::make(Vec3(cam11[0], cam11[1], cam11[2]), Vec3(cam11[3], cam11[4], cam11[5]),
                        Vec3(cam11[6], cam11[7], cam11[8]), cam11[9], cam11[10]);
@@ -107,18 +107,21 @@ static RenderJob make_job(const float* cam11, uint32_t w, uint32_t hgt, uint32_t
   j.spp = spp;
   j.max_depth = depth;
   j.integrator = integrator;
+  j.seed = seed;
   return j;
 }
 
 // cam11: eye(3) look_at(3) up(3) fov_y exposure
 void orc_render_pixels(void* h, const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth,
-                       uint32_t integrator, uint32_t p0, uint32_t p1, float* out, int nthreads) {
-  render_pixels(*(RenderScene*)h, make_job(cam11, w, hgt, spp, depth, integrator), p0, p1, out, nthreads);
+                       uint32_t integrator, uint32_t p0, uint32_t p1, float* out, int nthreads, uint32_t seed) {
+  render_pixels(*(RenderScene*)h, make_job(cam11, w, hgt, spp, depth, integrator, seed), p0, p1, out, nthreads);
 }
 
 void orc_render_samples(void* h, const float* cam11, uint32_t w, uint32_t hgt, uint32_t spp, uint32_t depth,
-                        uint32_t integrator, uint64_t first, uint64_t count, float* out, int nthreads) {
-  render_samples(*(RenderScene*)h, make_job(cam11, w, hgt, spp, depth, integrator), first, count, out, nthreads);
+                        uint32_t integrator, uint64_t first, uint64_t count, float* out, int nthreads,
+                        uint32_t seed) {
+  render_samples(*(RenderScene*)h, make_job(cam11, w, hgt, spp, depth, integrator, seed), first, count, out,
+                 nthreads);
 }
 
 }  // extern "C"

@@ -860,7 +860,7 @@ void replay_mis(const RenderScene& s, const Ray& ray, const PathSampler& sampler
 namespace {
 Vec3 one_sample(const RenderScene& s, const RenderJob& job, uint32_t pixel, uint32_t sample) {
   uint32_t px = pixel % job.width, py = pixel / job.width;
-  PathSampler ps(px, py, sample, job.spp, job.width, job.height);
+  PathSampler ps(px, py, sample, job.spp, job.width, job.height, job.seed);
   Vec2 us = ps.camera_sample();
   Ray r = job.cam.generate_ray_differential(job.width, job.height, px, py, us, job.spp);
   switch (job.integrator) {

@@ -127,6 +127,7 @@ struct RenderJob {
   Camera cam;
   uint32_t width, height, spp, max_depth;
   uint32_t integrator = 0;  // 0 MIS, 1 BDPT, 2 NEE, 3 PT
+  uint32_t seed = 0;        // the sample streams' scramble seed
 };
 
 // Material interface (material/mod.rs:251-502) for the kinds in scope, with

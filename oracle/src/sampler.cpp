@@ -82,7 +82,7 @@ uint64_t IndexSampler::permuted_index(uint64_t morton, uint32_t dimension) const
 
 float PathSampler::sample_1d(uint32_t dim) const {
   uint32_t index = fold_u64(idx.sample_index(px, py, sample, dim));
-  uint32_t seed = fold_u64(mix_bits((uint64_t)dim));
+  uint32_t seed = fold_u64(mix_bits(((uint64_t)this->seed << 32) | (uint64_t)dim));  // seed_for_dimension
   uint32_t v[1];
   shuffled_scrambled_sobol(index, seed, 1, v);
   return uint_to_float(v[0]);
@@ -90,7 +90,7 @@ float PathSampler::sample_1d(uint32_t dim) const {
 
 Vec2 PathSampler::sample_2d(uint32_t dim) const {
   uint32_t index = fold_u64(idx.sample_index(px, py, sample, dim));
-  uint32_t seed = fold_u64(mix_bits((uint64_t)dim));
+  uint32_t seed = fold_u64(mix_bits(((uint64_t)this->seed << 32) | (uint64_t)dim));  // seed_for_dimension
   uint32_t v[2];
   shuffled_scrambled_sobol(index, seed, 2, v);
   return Vec2(uint_to_float(v[0]), uint_to_float(v[1]));
@@ -98,7 +98,7 @@ Vec2 PathSampler::sample_2d(uint32_t dim) const {
 
 uint32_t PathSampler::aux_rng_seed(uint32_t dim) const {
   uint64_t index = idx.sample_index(px, py, sample, dim);
-  uint64_t bits = mix_bits(index ^ ((uint64_t)dim << 32));
+  uint64_t bits = mix_bits(index ^ ((uint64_t)dim << 32) ^ (uint64_t)seed);
   return pcg_hash(fold_u64(bits));
 }
 

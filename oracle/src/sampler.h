@@ -90,8 +90,12 @@ struct VertexRandoms { LightRandoms light; MaterialRandoms material; float u_rr;
 struct PathSampler {
   IndexSampler idx;
   uint32_t px, py, sample;
-  PathSampler(uint32_t px_, uint32_t py_, uint32_t sample_, uint32_t spp, uint32_t rx, uint32_t ry)
-      : idx(spp, rx, ry), px(px_), py(py_), sample(sample_) {}
+  // Scramble seed: 0 is the reference's SCRAMBLE_SEED (path_sampler.rs:77); other
+  // values give independent streams (tpt_render_job.seed).
+  uint32_t seed;
+  PathSampler(uint32_t px_, uint32_t py_, uint32_t sample_, uint32_t spp, uint32_t rx, uint32_t ry,
+              uint32_t seed_ = 0)
+      : idx(spp, rx, ry), px(px_), py(py_), sample(sample_), seed(seed_) {}
   Vec2 camera_sample() const { return sample_2d(0); }
   uint32_t initial_aux_rng_seed() const { return aux_rng_seed(0x80000000u); }
   VertexRandoms path_vertex_randoms(uint32_t depth) const;

@@ -53,10 +53,10 @@ def render(scene, sc, W, spp, depth=6):
     return img.double().cpu().numpy()
 
 
-def adjoint(scene, sc, W, spp, d_image, depth=6, mask=0, step=0.0):
+def adjoint(scene, sc, W, spp, d_image, depth=6, mask=0, step=0.0, seed=0):
     import torch
 
-    job = scene.job(sc["camera"], W, W, spp, depth)
+    job = scene.job(sc["camera"], W, W, spp, depth, seed=seed)
     d = torch.from_numpy(np.ascontiguousarray(d_image, np.float32)).cuda()
     g = torch.zeros(scene.n_materials * tpt.GRAD_PARAMS, dtype=torch.float64, device="cuda")
     scene.adjoint_device(job, d.data_ptr(), g.data_ptr(), mask, step, _stream())
@@ -79,6 +79,12 @@ def test_adjoint_matches_oracle(patches):
     # host-buffer entry point: the same computation
     gh = scene.adjoint(scene.job(sc["camera"], W, W, spp, 6), d_image)
     assert np.linalg.norm(gh - gd) / np.linalg.norm(gd) <= 1e-12
+    # another sample-stream seed: the oracle's gradient of that seed
+    seed = tpt.ADJOINT_SEED_STEP
+    gs = adjoint(scene, sc, W, spp, d_image, seed=seed)
+    gso = orc.RenderScene(sc, scene.light_tree()).adjoint(sc["camera"], W, W, spp, 6, d_image, seed=seed)
+    assert np.linalg.norm(gs - gso) / np.linalg.norm(gso) <= PARITY_TOL
+    assert np.linalg.norm(gs - gd) / np.linalg.norm(gd) > 1e-3
 
 
 def test_linear_base_color_identity(ctx):
@@ -175,11 +181,12 @@ def visible_patches(scene, sc, W, min_frac=0.01):
 
 def test_inverse_rendering_lowers_loss(ctx):
     """200 Adam steps (lr 0.003) on the 64 patch materials from a perturbed
-    start, 128x128 at 16 spp forward and adjoint (the backward pass replays the
-    job at 17 spp, so its paths are independent of the forward image's): the
-    image loss measured at 256 spp against the 1024-spp target must fall below
-    0.6 of its start, and the base-colour error of the patches the camera sees
-    (at least 1 % of the pixels each) must fall.  Roughness and metalness are
+    start, 128x128 at 16 spp forward and adjoint, every step with fresh sample
+    streams (seed = step + 1; the backward pass replays another seed's paths,
+    so they are independent of the forward image's): the image loss measured
+    at 256 spp against the 1024-spp target must fall below 0.6 of its start,
+    and the base-colour error of the patches the camera sees (at least 1 % of
+    the pixels each) must fall.  Roughness and metalness are
     printed, not checked: they trade off against each other and against base
     colour in the image."""
     import torch
@@ -201,14 +208,14 @@ def test_inverse_rendering_lowers_loss(ctx):
 
     loss0 = clean_loss(start)
     RenderFunction = tpt.render_function()
-    job = scene.job(sc["camera"], W, W, spp, depth)
     params = torch.tensor(start, requires_grad=True)
     opt = torch.optim.Adam([params], lr=0.003)
     lo = torch.tensor([0.02, 0.02, 0.02, 0.05, 0.0])
     hi = torch.tensor([0.98, 0.98, 0.98, 1.0, 1.0])
     mask = tpt.GRAD_MASK_BASE_COLOR | tpt.GRAD_MASK_ROUGHNESS | tpt.GRAD_MASK_METALNESS
-    for _ in range(200):
+    for step in range(200):
         opt.zero_grad()
+        job = scene.job(sc["camera"], W, W, spp, depth, seed=step + 1)
         img = RenderFunction.apply(params, scene, job, list(range(64)), tpt_scenes.patch_material, mask)
         loss = ((img - target) ** 2).sum()
         loss.backward()

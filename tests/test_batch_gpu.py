@@ -115,7 +115,7 @@ def test_autotune_applies_a_setting_that_renders_the_same(ctx, mixed):
         assert r["pilot_paths"] == sum(j.width * j.height * j.spp for j in mixed)  # small: the whole workload
         # every reported time is from the one (here: first) pilot, the other shade block included
         assert r["stage"] == 1 and r["candidates"] >= 3 and r["shade_block"] in (128, 256)
-        auto = [tpt.RenderJob(j.scene, j.camera, j.width, j.height, j.spp, j.max_depth, j.integrator, tpt.EXEC_AUTO)
+        auto = [tpt.RenderJob(j.scene, j.camera, j.width, j.height, j.spp, j.max_depth, j.integrator, tpt.EXEC_AUTO, j.seed)
                 for j in mixed]
         got = _render_each(ctx, auto)
         for a, b in zip(got, ref):

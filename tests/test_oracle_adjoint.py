@@ -91,3 +91,42 @@ def test_linear_in_d_image(patches):
     assert np.abs(g1).max() > 0
     np.testing.assert_allclose(g12, g1 + g2, rtol=1e-5, atol=1e-6 * np.abs(g1).max())
     assert np.all(R.adjoint(sc["camera"], W, W, spp, 6, np.zeros(W * W * 3, np.float32)) == 0)
+
+
+def test_seeded_streams_are_independent_and_unbiased(patches):
+    """Sample-stream seeds: seed 0 is the default image; another seed gives a
+    different image of the same expectation (the two images' pixel-mean
+    difference is within noise)."""
+    sc, R = patches
+    W, spp = 24, 16
+    a = R.render(sc["camera"], W, W, spp, 4)
+    assert np.array_equal(a, R.render(sc["camera"], W, W, spp, 4, seed=0))
+    imgs = np.stack([R.render(sc["camera"], W, W, spp, 4, seed=s) for s in range(1, 17)])
+    assert not np.array_equal(imgs[0], a)
+    means = imgs.reshape(16, -1).mean(1)
+    se = means.std(ddof=1) / np.sqrt(len(means))
+    assert abs(float(a.mean()) - float(means.mean())) < 4.0 * se * np.sqrt(17.0)
+
+
+def test_backward_with_another_seed_is_unbiased_at_the_truth(patches):
+    """At the true parameters the gradient of an L2 loss against an
+    independent target has zero mean when the backward pass replays paths of
+    another seed than the forward image's (the default of tpt.render_function);
+    replaying the forward's own paths biases it by the covariance of the image
+    noise with the path derivatives."""
+    sc, R = patches
+    W, spp, depth, reps = 16, 8, 4, 48
+    totals = {False: [], True: []}
+    for k in range(reps):
+        target = R.render(sc["camera"], W, W, 64, depth, seed=1000 + k).reshape(-1)
+        fs = 2 * k + 1
+        d = 2.0 * (R.render(sc["camera"], W, W, spp, depth, seed=fs).reshape(-1) - target)
+        for same in (False, True):
+            seed = fs if same else (fs + tpt.ADJOINT_SEED_STEP) & 0xFFFFFFFF
+            g = R.adjoint(sc["camera"], W, W, spp, depth, d.astype(np.float32), mask=tpt.GRAD_MASK_BASE_COLOR,
+                          seed=seed)
+            totals[same].append(g[:64, :3].sum())
+    z = {s: np.mean(t) / (np.std(t, ddof=1) / np.sqrt(reps)) for s, t in totals.items()}
+    print("z of the summed gradient: other seed", z[False], "same paths", z[True])
+    assert abs(z[False]) < 3.5
+    assert z[True] > 5.0

@@ -59,6 +59,7 @@ tpt_status make_launch(tpt_context* ctx, const tpt_render_job* job, RenderLaunch
   L->spp = job->spp;
   L->max_depth = job->max_depth;
   L->integrator = job->integrator;
+  L->seed = job->seed;
   // IndexSampler::new (sampler/zsobol.rs:213-224)
   L->log2_spp = log2_int(round_up_pow2(job->spp));
   const uint32_t res = round_up_pow2(std::max(job->width, job->height));

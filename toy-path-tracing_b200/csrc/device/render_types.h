@@ -223,7 +223,7 @@ struct RenderLaunch {
   uint32_t width, height, spp, max_depth;
   uint32_t log2_spp, n_base4_digits;
   uint32_t integrator;  // tpt_integrator: 0 MIS, 1 BDPT, 2 NEE, 3 PT
-  uint32_t pad;
+  uint32_t seed;        // the sample streams' scramble seed (tpt_render_job.seed)
 };
 constexpr uint32_t kIntegMis = 0, kIntegBdpt = 1, kIntegNee = 2, kIntegPt = 3;
 

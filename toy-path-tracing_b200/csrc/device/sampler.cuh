@@ -83,10 +83,13 @@ struct PathSamplerDev {
   uint64_t morton;  // (encode_morton_2(px, py) << log2_spp) | sample
   uint32_t log2_spp;
   uint32_t n_base4_digits;
+  uint32_t seed;  // the scramble seed: 0 is the reference's SCRAMBLE_SEED (path_sampler.rs:77)
 
-  __device__ __forceinline__ void init(uint32_t px, uint32_t py, uint32_t sample, uint32_t log2spp, uint32_t ndig) {
+  __device__ __forceinline__ void init(uint32_t px, uint32_t py, uint32_t sample, uint32_t log2spp, uint32_t ndig,
+                                       uint32_t scramble = 0u) {
     log2_spp = log2spp;
     n_base4_digits = ndig;
+    seed = scramble;
     morton = (((left_shift_2(py) << 1) | left_shift_2(px)) << log2spp) | (uint64_t)sample;
   }
 
@@ -109,7 +112,7 @@ struct PathSamplerDev {
   __device__ __noinline__ void sobol(uint32_t dimension, int depth, float* out) const {
     const uint64_t si = sample_index(dimension);
     const uint32_t index = (uint32_t)si ^ (uint32_t)(si >> 32);
-    const uint64_t sb = mix_bits((uint64_t)dimension);
+    const uint64_t sb = mix_bits(((uint64_t)this->seed << 32) | (uint64_t)dimension);  // seed_for_dimension
     const uint32_t seed = (uint32_t)sb ^ (uint32_t)(sb >> 32);
     const uint32_t idx = lk_permutation(__brev(index), seed);
     for (int d = 0; d < depth; ++d) {
@@ -132,7 +135,7 @@ struct PathSamplerDev {
   }
   __device__ __forceinline__ uint32_t aux_rng_seed(uint32_t dim) const {
     const uint64_t si = sample_index(dim);
-    const uint64_t bits = mix_bits(si ^ ((uint64_t)dim << 32));
+    const uint64_t bits = mix_bits(si ^ ((uint64_t)dim << 32) ^ (uint64_t)seed);
     return pcg_hash((uint32_t)bits ^ (uint32_t)(bits >> 32));
   }
 };

@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(kBdptBlock) render_bdpt_kernel(const __grid_co
     const uint32_t sample = (uint32_t)(path % P.spp);
     const uint32_t px = pixel % P.width, py = pixel / P.width;
     PathSamplerDev ps;
-    ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+    ps.init(px, py, sample, P.log2_spp, P.n_base4_digits, P.seed);
     float c0, c1;
     ps.sample_2d(kDimCamera, c0, c1);
     const float fx = ((float)px + 0.5f) + 0.5f * tent(c0);

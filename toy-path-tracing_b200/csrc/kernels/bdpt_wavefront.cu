@@ -76,7 +76,7 @@ __device__ __forceinline__ PathSamplerDev sampler_of(const RenderLaunch& P, uint
   px = pixel % P.width;
   py = pixel / P.width;
   PathSamplerDev ps;
-  ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+  ps.init(px, py, sample, P.log2_spp, P.n_base4_digits, P.seed);
   return ps;
 }
 

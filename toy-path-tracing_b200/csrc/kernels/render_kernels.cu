@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kRenderBlock, TPT_MK_MINB) render_mis_kernel(c
           const uint64_t path = first_path + i;
           const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
           const uint32_t px = pixel % P.width, py = pixel / P.width;
-          ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+          ps.init(px, py, sample, P.log2_spp, P.n_base4_digits, P.seed);
           float c0, c1;
           ps.sample_2d(kDimCamera, c0, c1);
           // PinholeCamera::generate_ray_differential (camera.rs:48-73), primary direction only

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(const __grid_constant__ 
   const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
   const uint32_t px = pixel % P.width, py = pixel / P.width;
   PathSamplerDev ps;
-  ps.init(px, py, sample, P.log2_spp, P.n_base4_digits);
+  ps.init(px, py, sample, P.log2_spp, P.n_base4_digits, P.seed);
   float c0, c1;
   ps.sample_2d(kDimCamera, c0, c1);
   const float fx = ((float)px + 0.5f) + 0.5f * tent(c0);
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(BS, shade_min_blocks<ADJ, BS>()) wf_shade(cons
       }
       const uint32_t pixel = (uint32_t)(path / P.spp), sample = (uint32_t)(path % P.spp);
       PathSamplerDev ps;
-      ps.init(pixel % P.width, pixel / P.width, sample, P.log2_spp, P.n_base4_digits);
+      ps.init(pixel % P.width, pixel / P.width, sample, P.log2_spp, P.n_base4_digits, P.seed);
       if (alpha) {
         if (P.integrator == kIntegMis) {
           sh_aux = nx_aux = aux_from_seed(ps, (int)d);

@@ -211,7 +211,7 @@ class CameraDesc(C.Structure):
 class RenderJob(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("camera", CameraDesc), ("width", C.c_uint32), ("height", C.c_uint32),
                 ("spp", C.c_uint32), ("max_depth", C.c_uint32), ("integrator", C.c_uint32),
-                ("execution", C.c_uint32)]
+                ("execution", C.c_uint32), ("seed", C.c_uint32)]
 
 
 class AdjointDesc(C.Structure):
@@ -225,6 +225,8 @@ GRAD_NAMES = ["base_color_r", "base_color_g", "base_color_b", "specular_roughnes
               "specular_ior", "coat_weight"]
 GRAD_MASK_BASE_COLOR, GRAD_MASK_ROUGHNESS, GRAD_MASK_METALNESS, GRAD_MASK_IOR, GRAD_MASK_COAT = 1, 2, 4, 8, 16
 GRAD_ALL = 31
+# render_function's default backward job: the forward job's seed plus this
+ADJOINT_SEED_STEP = 0x9E3779B9
 
 class TuneResult(C.Structure):
     _fields_ = [("execution", C.c_uint32), ("wavefront_capacity", C.c_uint32), ("graphs", C.c_uint32),
@@ -635,19 +637,21 @@ class Scene:
         return nodes, v.root
 
     def job(self, camera: dict, width: int, height: int, spp: int, max_depth: int, integrator: int = 0,
-            execution: int = EXEC_WAVEFRONT):
+            execution: int = EXEC_WAVEFRONT, seed: int = 0):
+        """A `tpt_render_job`; seed 0 gives the reference's sample streams, any
+        other value independent ones."""
         cam = CameraDesc()
         cam.eye[:] = [float(np.float32(x)) for x in camera["eye"]]
         cam.look_at[:] = [float(np.float32(x)) for x in camera["look_at"]]
         cam.up[:] = [float(np.float32(x)) for x in camera["up"]]
         cam.fov_y = float(np.float32(camera["fov_y"]))
         cam.exposure = float(np.float32(camera.get("exposure", 1.0)))
-        return RenderJob(self.h.value, cam, width, height, spp, max_depth, integrator, execution)
+        return RenderJob(self.h.value, cam, width, height, spp, max_depth, integrator, execution, seed)
 
     def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int, integrator: int = 0,
-               execution: int = EXEC_WAVEFRONT):
+               execution: int = EXEC_WAVEFRONT, seed: int = 0):
         """`tpt_render`: returns float32 [height, width, 3] (host)."""
-        j = self.job(camera, width, height, spp, max_depth, integrator, execution)
+        j = self.job(camera, width, height, spp, max_depth, integrator, execution, seed)
         out = np.empty((height, width, 3), np.float32)
         ptrs = (C.c_void_p * 1)(out.ctypes.data)
         _check(lib().tpt_render(self.ctx.h, C.byref(j), 1, ptrs), self.ctx)
@@ -812,10 +816,10 @@ def render_function():
     metalness, specular_ior, coat_weight), so params rows must follow that
     order up to k.  adjoint_job
     (optional): the job the backward pass replays.  By default it is the
-    forward job at spp + 1 samples per pixel: its sample indices, and so its
-    paths, differ from the forward image's, so the gradient of an L2 loss is
-    not correlated with that image's noise (a same-sample backward is biased).
-    Pass the forward job itself to replay its very paths."""
+    forward job with another sample-stream seed (ADJOINT_SEED_STEP added), so
+    its paths are independent of the forward image's and the gradient of an L2
+    loss is not correlated with that image's noise (a same-sample backward is
+    biased).  Pass the forward job itself to replay its very paths."""
     import torch
 
     class RenderFunction(torch.autograd.Function):
@@ -829,7 +833,7 @@ def render_function():
             fctx.scene, fctx.ids, fctx.mask, fctx.step = scene, material_ids, mask, fd_step
             if adjoint_job is None:
                 adjoint_job = RenderJob.from_buffer_copy(job)
-                adjoint_job.spp = job.spp + 1
+                adjoint_job.seed = (job.seed + ADJOINT_SEED_STEP) & 0xFFFFFFFF
             fctx.job = adjoint_job
             fctx.k = params.shape[1]
             fctx.device, fctx.dtype = params.device, params.dtype
