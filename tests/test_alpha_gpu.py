@@ -21,8 +21,10 @@ pytestmark = pytest.mark.gpu
 
 def cutout_cornell(seed=2):
     """The Cornell box with a 40 %-opaque Lambert short box and a 60 %-opaque
-    OpenPBR tall box (both walls' colours, cut-outs by the alpha test)."""
-    sc = tpt_scenes.cornell_box(seed, tpt_scenes.LAMBERT)
+    OpenPBR tall box (both walls' colours, cut-outs by the alpha test), lifted
+    off the floor: rays inside a box would otherwise meet its bottom and the
+    floor in one plane, whose tie decides the number of AuxRng draws."""
+    sc = tpt_scenes.lift_boxes(tpt_scenes.cornell_box(seed, tpt_scenes.LAMBERT))
     sc["materials"][5] = {"kind": tpt.OPENPBR, "base_color": np.array([0.7, 0.6, 0.5], np.float32),
                           "specular_roughness": 0.4, "geometry_opacity": 0.6}
     sc["materials"][6] = dict(sc["materials"][6], opacity=0.4)

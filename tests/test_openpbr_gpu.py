@@ -216,7 +216,7 @@ def test_every_openpbr_parameter_reaches_the_device(ctx):
     """Nothing of an untextured OpenPBR material is refused any more: a tall box
     combining a cut-out (geometry_opacity), emission, dispersive transmission,
     coat, fuzz and thin film renders on the device as in the oracle."""
-    sc = tpt_scenes.cornell_box(6, tpt_scenes.OPENPBR)
+    sc = tpt_scenes.lift_boxes(tpt_scenes.cornell_box(6, tpt_scenes.OPENPBR))  # no floor/box-bottom ties
     sc["materials"][5] = {"kind": tpt.OPENPBR, "base_color": np.array([0.7, 0.6, 0.5], np.float32),
                           "specular_roughness": 0.3, "transmission_weight": 0.6,
                           "transmission_dispersion_scale": 1.0, "coat_weight": 0.4, "coat_roughness": 0.2,

@@ -201,6 +201,18 @@ def cornell_box(seed: int = 1, material: int = OPENPBR, light_strength: float = 
             "angles": (float(a1), float(a2)), "seed": seed}
 
 
+def lift_boxes(sc: dict, dy: float = 0.002) -> dict:
+    """The Cornell box with its two boxes floating dy above the floor.  Where
+    rays reach the inside of a box (glass, cut-outs), a box bottom coplanar
+    with the floor is a tie between two instances whose winner, and with alpha
+    tests the number of AuxRng draws, a last-bit difference in the ray decides;
+    lifted boxes make the geometry free of such ties."""
+    a1, a2 = sc["angles"]
+    sc["instances"][5] = instance_matrix(5, 5, _trs((-0.55, dy, -0.45), a1, (0.9, 1.8, 0.9)))
+    sc["instances"][6] = instance_matrix(5, 6, _trs((0.6, dy, 0.5), -a2, (0.9, 0.9, 0.9)))
+    return sc
+
+
 def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPENPBR, dispersion: float = 0.0):
     """The Cornell box with transmissive boxes: the tall box rough (specular
     roughness 0.25) and the short box smooth, both fully transmissive OpenPBR
@@ -208,13 +220,7 @@ def cornell_glass(seed: int = 1, thin_walled: bool = False, material: int = OPEN
     dispersion > 0 gives both glasses that transmission_dispersion_scale
     (Abbe number 20 at scale 1).  The walls keep their diffuse materials
     (OpenPBR, or NormalizedLambert)."""
-    sc = cornell_box(seed, material)
-    # the glass boxes float 2 mm above the floor: a box bottom coplanar with
-    # the floor, reached from inside the glass, is a tie between two
-    # instances whose winner a last-bit difference in the ray decides
-    a1, a2 = sc["angles"]
-    sc["instances"][5] = instance_matrix(5, 5, _trs((-0.55, 0.002, -0.45), a1, (0.9, 1.8, 0.9)))
-    sc["instances"][6] = instance_matrix(5, 6, _trs((0.6, 0.002, 0.5), -a2, (0.9, 0.9, 0.9)))
+    sc = lift_boxes(cornell_box(seed, material))
     thin = 1 if thin_walled else 0
     sc["materials"][5] = {"kind": OPENPBR, "base_color": np.array([0.8, 0.8, 0.8], np.float32),
                           "specular_roughness": 0.25, "transmission_weight": 1.0, "geometry_thin_walled": thin}
