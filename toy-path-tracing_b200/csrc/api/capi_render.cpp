@@ -192,14 +192,22 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
   return cuda_check(ctx, e, "wavefront launch");
 }
 
-// BDPT wavefront arena for `max_vertices` vertices per subpath: as many samples
-// as keep the connection queue at 2^24 slots (each sample has at most
-// max_vertices^2 connections).
-tpt_status ensure_bdpt_wavefront(tpt_context* ctx, uint32_t max_vertices) {
+// BDPT wavefront arena for `max_vertices` vertices per subpath and a job of
+// `n` samples: a chunk holds all of them, or as many as keep the connection
+// queue at 2^TPT_BD_PAIRS_LOG2 slots (each sample has at most max_vertices^2
+// connections; 2^27 slots are about 14 GB at 10 vertices, which large chunks
+// repay: the late subpath steps, with few rays left, run once per chunk), a
+// multiple of 128 so that no warp of bd_step straddles the camera and light
+// halves of a ray queue.  The arena only grows.
+#ifndef TPT_BD_PAIRS_LOG2
+#define TPT_BD_PAIRS_LOG2 27
+#endif
+tpt_status ensure_bdpt_wavefront(tpt_context* ctx, uint32_t max_vertices, uint64_t n) {
   const uint32_t mv = std::max<uint32_t>(1, max_vertices);
-  const uint64_t samples = std::max<uint64_t>(1024, (1ull << 24) / ((uint64_t)mv * mv));
+  const uint64_t cap = std::max<uint64_t>(1024, ((1ull << TPT_BD_PAIRS_LOG2) / ((uint64_t)mv * mv)) & ~(uint64_t)127);
+  const uint64_t samples = std::min<uint64_t>(cap, std::max<uint64_t>(1024, (n + 127) & ~(uint64_t)127));
   const uint64_t pairs = samples * mv * mv;
-  if (ctx->d_bd && ctx->bd.max_vertices == mv) return TPT_OK;
+  if (ctx->d_bd && ctx->bd.max_vertices == mv && ctx->bd.sample_capacity >= samples) return TPT_OK;
   const uint64_t q = 2 * samples;  // subpath ray queue slots (camera + light per sample)
   const size_t bytes = samples * 2 * mv * (size_t)kBdVertexBytes + samples * (3 * 4 + 3 * 4) +
                        pairs * (4 + 12 + 12 + 4) + pairs * (7 * 4 + 4 + 4 + 4 + 4) +
@@ -262,7 +270,7 @@ tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, co
                       launch_render(job->scene->geo, job->scene->render, L, samples, first, n, ctx->d_err,
                                     ctx->num_sms, s, next_counter(ctx)),
                       "render kernel launch");
-  tpt_status st = ensure_bdpt_wavefront(ctx, L.max_depth);
+  tpt_status st = ensure_bdpt_wavefront(ctx, L.max_depth, n);
   if (st) return st;
   const BdWfBuffers& B = ctx->bd;
   for (uint64_t b = 0; b < n; b += B.sample_capacity) {

@@ -283,7 +283,8 @@ struct BdWfBuffers {
   int32_t* s_tri;
   int32_t* s_inst;
   float* s_t;
-  uint32_t* counts;      // [0] connections, [1] visibility rays, [2], [3] subpath ray queues
+  uint32_t* counts;      // [0] connections, [1] visibility rays, [2], [3] camera and [4], [5] light
+                         // halves of the subpath ray queues
 };
 
 // Wavefront state: per path slot of a chunk (capacity slots), two ray queues,

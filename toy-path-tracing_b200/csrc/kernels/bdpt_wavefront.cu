@@ -6,7 +6,11 @@
 //                  one iteration of the camera loop (depth = step) or of the
 //                  light loop (depth = step + 1) per queued ray, vertices into
 //                  HBM, camera-side emission into L0, next rays into the other
-//                  queue (the same step functions the one-kernel BDPT runs);
+//                  queue (the same step functions the one-kernel BDPT runs).
+//                  A queue holds the camera rays in its first half and the
+//                  light rays in its second (sample_capacity slots each, own
+//                  counters), so every warp of bd_step runs one of the two
+//                  loops and the two halves are traversed as two launches;
 //                  in scenes with point, spot, directional or environment
 //                  lights, the camera vertices' light samples queue a shadow
 //                  ray, traversed after the step, and bd_nee_resolve adds the
@@ -31,6 +35,12 @@
 namespace tpt {
 
 constexpr int kBdWfBlock = 128;
+#ifndef TPT_BD_STEP_MINB
+// bd_step's minimum resident blocks per SM: 4 caps it at 128 registers (from
+// 168, a few hundred bytes of spills), 16 warps per SM instead of 12: 6 % less
+// BDPT time on the large scene
+#define TPT_BD_STEP_MINB 4
+#endif
 
 // Warp-exclusive prefix sum of `v` (all lanes call); returns the lane's offset
 // and the warp total in `total`.
@@ -57,6 +67,8 @@ __device__ __forceinline__ uint32_t warp_append1(uint32_t* counter, bool pred) {
   return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
+// Queue halves: camera rays at [0, sample_capacity) counted in counts[2 + q],
+// light rays at [sample_capacity, 2 * sample_capacity) in counts[4 + q].
 __device__ __forceinline__ void push_ray(const BdWfBuffers& B, int q, uint32_t slot, V3 o, V3 d, uint32_t tag) {
   const uint32_t Q = 2 * B.sample_capacity;
   float* r = B.q_ray[q];
@@ -115,18 +127,18 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_init(const __grid_constant__ De
   const bool light_ray = l.alive && P.max_depth > 1;
   const uint32_t qc = warp_append1(&B.counts[2], cam_ray);
   if (cam_ray) push_ray(B, 0, qc, o, d, i);
-  const uint32_t ql = warp_append1(&B.counts[2], light_ray);
-  if (light_ray) push_ray(B, 0, ql, lo, ld, i | kLightTag);
+  const uint32_t ql = warp_append1(&B.counts[4], light_ray);
+  if (light_ray) push_ray(B, 0, B.sample_capacity + ql, lo, ld, i | kLightTag);
 }
 
 // Step `step` of both loops: camera rays of depth `step`, light rays of depth
 // step + 1, traced into the hit arrays; the next rays into queue cur ^ 1.
-__global__ void __launch_bounds__(kBdWfBlock) bd_step(const __grid_constant__ DevRender S,
+__global__ void __launch_bounds__(kBdWfBlock, TPT_BD_STEP_MINB) bd_step(const __grid_constant__ DevRender S,
                                                   const __grid_constant__ RenderLaunch P, BdWfBuffers B,
                                                       uint64_t first_path, uint32_t step, int cur) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= B.counts[2 + cur]) return;
-  const uint32_t Q = 2 * B.sample_capacity;
+  const uint32_t S_cap = B.sample_capacity, Q = 2 * S_cap;
+  if (j < S_cap ? j >= B.counts[2 + cur] : j - S_cap >= B.counts[4 + cur]) return;
   const uint32_t tag = B.q_tag[cur][j];
   const uint32_t i = tag & ~kLightTag;
   const bool light = (tag & kLightTag) != 0;
@@ -161,8 +173,8 @@ __global__ void __launch_bounds__(kBdWfBlock) bd_step(const __grid_constant__ De
     B.light_state[i] = l;
     next = l.alive && step + 2 < P.max_depth;
   }
-  const uint32_t q = warp_append1(&B.counts[2 + (cur ^ 1)], next);
-  if (next) push_ray(B, cur ^ 1, q, ro, rd, tag);
+  const uint32_t q = warp_append1(&B.counts[(light ? 4 : 2) + (cur ^ 1)], next);
+  if (next) push_ray(B, cur ^ 1, light ? S_cap + q : q, ro, rd, tag);
   // a camera vertex's light sample: its shadow ray into the visibility queue
   // (free until the connection stage), contribution and light distance beside it
   const uint32_t qs = warp_append1(&B.counts[1], nee);
@@ -300,19 +312,24 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
                                   unsigned long long* totals) {
   if (n == 0) return cudaSuccess;
   DevRender S{geo, rd};
-  cudaError_t e = cudaMemsetAsync(B.counts, 0, 2 * sizeof(uint32_t), s);
+  cudaError_t e = cudaMemsetAsync(B.counts, 0, 6 * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  const uint32_t Q = 2 * B.sample_capacity;
-  if ((e = cudaMemsetAsync(B.counts + 2, 0, 2 * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  const uint32_t S_cap = B.sample_capacity, Q = 2 * S_cap;
   bd_init<<<grid_of(n), kBdWfBlock, 0, s>>>(S, P, B, first_path, n);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const bool lights = rd.num_extra_lights > 0;
   for (uint32_t step = 0; step < P.max_depth; ++step) {
     const int cur = (int)(step & 1u);
     if ((e = cudaMemsetAsync(B.counts + 2 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
-    e = launch_traverse_strided(geo, B.q_ray[cur], Q, Q, TPT_CLOSEST_HIT, B.h_tri, B.h_t, B.h_inst, B.h_bary, Q,
+    if ((e = cudaMemsetAsync(B.counts + 4 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
+    // the camera half, then the light half of the queue (hits at the rays' slots)
+    e = launch_traverse_strided(geo, B.q_ray[cur], Q, S_cap, TPT_CLOSEST_HIT, B.h_tri, B.h_t, B.h_inst, B.h_bary, Q,
                                 counter, err, num_sms, s, nullptr, nullptr, B.counts + 2 + cur, nullptr, nullptr,
                                 totals);
+    if (e != cudaSuccess) return e;
+    e = launch_traverse_strided(geo, B.q_ray[cur] + S_cap, Q, S_cap, TPT_CLOSEST_HIT, B.h_tri + S_cap,
+                                B.h_t + S_cap, B.h_inst + S_cap, B.h_bary + S_cap, Q, counter, err, num_sms, s,
+                                nullptr, nullptr, B.counts + 4 + cur, nullptr, nullptr, totals);
     if (e != cudaSuccess) return e;
     bd_step<<<grid_of(Q), kBdWfBlock, 0, s>>>(S, P, B, first_path, step, cur);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
