@@ -436,7 +436,7 @@ typedef struct tpt_render_job {
 } tpt_render_job;
 
 /* Path slots of the wavefront pipeline's queues: a render is processed in
- * chunks of at most this many paths (0 = the default 2^22; otherwise
+ * chunks of at most this many paths (0 = the default 2^24; otherwise
  * [1024, 2^24]).  Larger chunks fill the GPU better, smaller ones hold less
  * device memory (about 250 bytes per slot).  tpt_autotune picks it per
  * workload.  Results do not depend on it. */
@@ -514,7 +514,7 @@ typedef struct tpt_tune_result {
   uint32_t shade_block;        /* threads per block of the wavefront shade stage */
   float ms;                    /* last-pilot time of the chosen settings */
   float ms_megakernel;         /* last-pilot time of the megakernel */
-  float ms_wavefront_default;  /* last-pilot time of the wavefront at 2^22 slots, graphs, the context's block */
+  float ms_wavefront_default;  /* last-pilot time of the wavefront at 2^24 slots, graphs, the context's block */
   uint64_t pilot_paths;        /* paths of the last pilot (about) */
   uint32_t stage;              /* which pilot the times come from: 1 (at most 2^24 paths) or 2 (at most 2^26) */
   uint32_t candidates;         /* settings timed */

@@ -14,7 +14,7 @@
 // the result reports comes from that last pilot, so they compare directly.
 // Each timing is one warm-up (graph capture, arena growth) and the median of
 // three runs, CUDA events on the context's stream.  A candidate replaces the
-// default wavefront settings (2^22 slots, graphs, the context's block size)
+// default wavefront settings (kDefaultWavefrontSlots slots, graphs, the context's block size)
 // only when it is more than 3 % faster.  Results do not depend on any of the
 // tuned settings (the tests check this), only the time does.
 #include <algorithm>
@@ -124,9 +124,9 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   tpt_status st = make_pilot(kPilotPaths, p1);
   std::vector<Cand> cands;
   cands.push_back(Cand{TPT_EXEC_MEGAKERNEL, 0, 0, 256, 0.0f});
-  const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23};
+  const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22, 1u << 23, 1u << 24};
   for (uint32_t cap : caps) {
-    if (cap > 2 * std::max<uint64_t>(p1.paths, 1u << 18) && cap != (1u << 22)) continue;  // queues beyond the work
+    if (cap > 2 * std::max<uint64_t>(p1.paths, 1u << 18) && cap != kDefaultWavefrontSlots) continue;  // queues beyond the work
     for (uint32_t g : {1u, 0u}) cands.push_back(Cand{TPT_EXEC_WAVEFRONT, cap, g, saved_block, 0.0f});
   }
   for (Cand& c : cands) {
@@ -145,7 +145,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     st = make_pilot(4 * kPilotPaths, p2);
     for (Cand& c : cands) {
       if (st) break;
-      const bool is_default = c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs;
+      const bool is_default = c.exec == TPT_EXEC_WAVEFRONT && c.cap == kDefaultWavefrontSlots && c.graphs;
       if (c.ms <= 1.05f * best1 || is_default || c.exec == TPT_EXEC_MEGAKERNEL) st = run(p2, c, &c.ms);
       else c.ms = 1e30f;
     }
@@ -175,7 +175,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   best.ms = 1e30f;
   float ms_default = 0.0f;
   for (const Cand& c : cands) {
-    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == (1u << 22) && c.graphs && c.block == saved_block) ms_default = c.ms;
+    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == kDefaultWavefrontSlots && c.graphs && c.block == saved_block) ms_default = c.ms;
     if (c.ms < best.ms) {
       best.ms = c.ms;
       best.execution = c.exec;
@@ -188,7 +188,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   // them by 3 %: the pilots are scaled-down workloads and carry noise
   if (best.execution == TPT_EXEC_WAVEFRONT && ms_default > 0.0f && best.ms > 0.97f * ms_default) {
     best.ms = ms_default;
-    best.wavefront_capacity = 1u << 22;
+    best.wavefront_capacity = kDefaultWavefrontSlots;
     best.graphs = 1;
     best.shade_block = saved_block;
   }

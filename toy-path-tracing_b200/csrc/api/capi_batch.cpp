@@ -99,7 +99,7 @@ tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     pixels += (uint64_t)L[j].width * L[j].height;
   }
   if (n_jobs == 0) return TPT_OK;
-  if (capacity == 0) capacity = 1u << 22;
+  if (capacity == 0) capacity = kDefaultWavefrontSlots;
   uint32_t max_spp = 0;
   for (auto& l : L) max_spp = std::max(max_spp, l.spp);
   if (max_spp > capacity)

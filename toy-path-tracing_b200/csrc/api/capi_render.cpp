@@ -283,9 +283,9 @@ tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, co
 }
 
 // Pixels per chunk: the per-sample buffer stays below 1 GiB and a chunk has at
-// most `capacity` paths (the wavefront arena's slot count; 0 = 2^22).
+// most `capacity` paths (the wavefront arena's slot count; 0 = the default).
 uint32_t chunk_pixels(const RenderLaunch& L, uint32_t capacity) {
-  if (capacity == 0) capacity = 1u << 22;
+  if (capacity == 0) capacity = kDefaultWavefrontSlots;
   const uint64_t per_pixel = 12ull * L.spp;
   uint64_t n = std::min<uint64_t>((1ull << 30) / per_pixel, std::max<uint64_t>(1, (uint64_t)capacity / L.spp));
   const uint64_t total = (uint64_t)L.width * L.height;
@@ -328,7 +328,7 @@ tpt_status tpt_context_set_graphs(tpt_context* ctx, int enable) {
 }
 
 uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx) {
-  return ctx ? (ctx->batch_capacity ? ctx->batch_capacity : (1u << 22)) : 0u;
+  return ctx ? (ctx->batch_capacity ? ctx->batch_capacity : kDefaultWavefrontSlots) : 0u;
 }
 
 tpt_status tpt_render_device(tpt_context* ctx, const tpt_render_job* job, float* out_rgb, void* stream) {
