@@ -604,7 +604,10 @@ def batch_block(ctx, args):
     tune = ctx.autotune(jw)
     out["autotune"] = dict(tune, seconds=time.perf_counter() - t0)
     ms = _time_ms(lambda: ctx.render_batch_device(jw, ptrs, st))
-    out["batched_wavefront"] = {"value": total / ms / 1e3, "ms": ms}
+    # tpt_render_batch_device after tpt_autotune: one batched launch sequence, or
+    # the jobs one after another when the pilot found that faster
+    out["batched_wavefront"] = {"value": total / ms / 1e3, "ms": ms,
+                                "mode": "batched" if tune.get("batched", 1) else "job by job (autotuned)"}
     ctx.wavefront_capacity = 0  # the job-by-job comparisons run the default settings
     ctx.set_graphs(True)
     ctx.set_shade_block(256)

@@ -439,7 +439,8 @@ typedef struct tpt_render_job {
  * chunks of at most this many paths (0 = the default 2^24; otherwise
  * [1024, 2^24]).  Larger chunks fill the GPU better, smaller ones hold less
  * device memory (about 250 bytes per slot).  tpt_autotune picks it per
- * workload.  Results do not depend on it. */
+ * workload.  Setting it also makes tpt_render_batch_device batch again after
+ * tpt_autotune chose job-by-job rendering.  Results do not depend on it. */
 tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots);
 uint32_t tpt_context_wavefront_capacity(const tpt_context* ctx);
 /* Wavefront bounces are replayed from captured CUDA graphs (one per bounce
@@ -518,6 +519,9 @@ typedef struct tpt_tune_result {
   uint64_t pilot_paths;        /* paths of the last pilot (about) */
   uint32_t stage;              /* which pilot the times come from: 1 (at most 2^24 paths) or 2 (at most 2^26) */
   uint32_t candidates;         /* settings timed */
+  uint32_t batched;            /* 1: tpt_render_batch_device runs the jobs through one launch
+                                  sequence; 0: one job after another, each its own wavefront
+                                  (chosen when that was faster on the pilot) */
 } tpt_tune_result;
 tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs, tpt_tune_result* out);
 

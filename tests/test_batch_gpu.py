@@ -120,6 +120,13 @@ def test_autotune_applies_a_setting_that_renders_the_same(ctx, mixed):
         got = _render_each(ctx, auto)
         for a, b in zip(got, ref):
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        # the batch entry point under the tuned choice (one launch sequence or job by job)
+        assert r["batched"] in (0, 1)
+        outs = [torch.empty(j.width * j.height * 3, dtype=torch.float32, device="cuda") for j in mixed]
+        ctx.render_batch_device(mixed, [o.data_ptr() for o in outs], torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        for o, b in zip(outs, ref):
+            assert np.array_equal(o.cpu().numpy().view(np.uint32), np.asarray(b).reshape(-1).view(np.uint32))
     finally:
         ctx.wavefront_capacity = 0
         ctx.set_graphs(True)

@@ -86,6 +86,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   struct Cand {
     uint32_t exec, cap, graphs, block;
     float ms;
+    bool per_job = false;  // several jobs: wavefront job by job instead of one batch
   };
   const uint32_t saved_cap = ctx->batch_capacity;
   const bool saved_graphs = ctx->use_graphs;
@@ -100,7 +101,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     for (int rep = 0; rep < 4; ++rep) {
       cudaEventRecord(T.a, ctx->stream);
       tpt_status s2 = TPT_OK;
-      if (c.exec == TPT_EXEC_WAVEFRONT && n_jobs > 1) {
+      if (c.exec == TPT_EXEC_WAVEFRONT && n_jobs > 1 && !c.per_job) {
         s2 = render_batch(ctx, p.jobs.data(), n_jobs, p.imgs.data(), ctx->stream, c.cap);
       } else {
         for (int j = 0; j < n_jobs && !s2; ++j) {
@@ -129,6 +130,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
     if (cap > 2 * std::max<uint64_t>(p1.paths, 1u << 18) && cap != kDefaultWavefrontSlots) continue;  // queues beyond the work
     for (uint32_t g : {1u, 0u}) cands.push_back(Cand{TPT_EXEC_WAVEFRONT, cap, g, saved_block, 0.0f});
   }
+  if (n_jobs > 1) cands.push_back(Cand{TPT_EXEC_WAVEFRONT, kDefaultWavefrontSlots, 1u, saved_block, 0.0f, true});
   for (Cand& c : cands) {
     if (st) break;
     st = run(p1, c, &c.ms);
@@ -175,9 +177,12 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   best.ms = 1e30f;
   float ms_default = 0.0f;
   for (const Cand& c : cands) {
-    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == kDefaultWavefrontSlots && c.graphs && c.block == saved_block) ms_default = c.ms;
+    if (c.exec == TPT_EXEC_WAVEFRONT && c.cap == kDefaultWavefrontSlots && c.graphs && c.block == saved_block &&
+        !c.per_job)
+      ms_default = c.ms;
     if (c.ms < best.ms) {
       best.ms = c.ms;
+      best.batched = c.per_job ? 0u : 1u;
       best.execution = c.exec;
       best.wavefront_capacity = c.exec == TPT_EXEC_WAVEFRONT ? c.cap : saved_cap;
       best.graphs = c.exec == TPT_EXEC_WAVEFRONT ? c.graphs : (saved_graphs ? 1u : 0u);
@@ -188,6 +193,7 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   // them by 3 %: the pilots are scaled-down workloads and carry noise
   if (best.execution == TPT_EXEC_WAVEFRONT && ms_default > 0.0f && best.ms > 0.97f * ms_default) {
     best.ms = ms_default;
+    best.batched = 1;
     best.wavefront_capacity = kDefaultWavefrontSlots;
     best.graphs = 1;
     best.shade_block = saved_block;
@@ -198,7 +204,9 @@ tpt_status tpt_autotune(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   best.stage = stage;
   best.candidates = (uint32_t)cands.size();
   // apply
+  if (n_jobs <= 1) best.batched = 1;
   ctx->tuned_execution = best.execution;
+  ctx->batch_per_job = best.execution == TPT_EXEC_WAVEFRONT && best.batched == 0;
   if (best.execution == TPT_EXEC_WAVEFRONT) {
     ctx->batch_capacity = best.wavefront_capacity;
     ctx->use_graphs = best.graphs != 0;

@@ -145,6 +145,11 @@ tpt_status tpt_render_batch_device(tpt_context* ctx, const tpt_render_job* jobs,
   if (tpt_status st = set_device(ctx)) return st;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   note_device_call(ctx, "tpt_render_batch_device");
+  if (ctx->batch_per_job) {  // tpt_autotune found the jobs faster one after another
+    for (int j = 0; j < n_jobs; ++j)
+      if (tpt_status st = tpt_render_device(ctx, &jobs[j], out_rgb[j], (void*)s)) return st;
+    return TPT_OK;
+  }
   return render_batch(ctx, jobs, n_jobs, out_rgb, s, ctx->batch_capacity);
 }
 

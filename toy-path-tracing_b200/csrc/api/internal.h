@@ -65,6 +65,7 @@ struct tpt_context {
   // per-bounce CUDA graphs of the wavefront (bounce_graphs.cpp)
   bool use_graphs = true;
   uint32_t tuned_execution = 0;  // what TPT_EXEC_AUTO means (tpt_autotune)
+  bool batch_per_job = false;    // tpt_render_batch_device renders job by job (tpt_autotune)
   uint32_t shade_block = 256;    // threads per block of the wavefront shade stage (128 or 256)
   // tpt_context_set_render_stats: device counters the wavefront traversals add
   // to (queue rays at [0..3], shadow/visibility rays at [4..7]); NULL = off

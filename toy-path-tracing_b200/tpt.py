@@ -231,7 +231,8 @@ ADJOINT_SEED_STEP = 0x9E3779B9
 class TuneResult(C.Structure):
     _fields_ = [("execution", C.c_uint32), ("wavefront_capacity", C.c_uint32), ("graphs", C.c_uint32),
                 ("shade_block", C.c_uint32), ("ms", C.c_float), ("ms_megakernel", C.c_float), ("ms_wavefront_default", C.c_float),
-                ("pilot_paths", C.c_uint64), ("stage", C.c_uint32), ("candidates", C.c_uint32)]
+                ("pilot_paths", C.c_uint64), ("stage", C.c_uint32), ("candidates", C.c_uint32),
+                ("batched", C.c_uint32)]
 
 
 INTEGRATOR_MIS = 0
