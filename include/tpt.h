@@ -437,7 +437,7 @@ typedef struct tpt_render_job {
 
 /* Path slots of the wavefront pipeline's queues: a render is processed in
  * chunks of at most this many paths (0 = the default 2^24; otherwise
- * [1024, 2^24]).  Larger chunks fill the GPU better, smaller ones hold less
+ * [1024, 2^26]).  Larger chunks fill the GPU better, smaller ones hold less
  * device memory (about 250 bytes per slot).  tpt_autotune picks it per
  * workload.  Setting it also makes tpt_render_batch_device batch again after
  * tpt_autotune chose job-by-job rendering.  Results do not depend on it. */

@@ -302,8 +302,8 @@ extern "C" {
 
 tpt_status tpt_context_set_wavefront_capacity(tpt_context* ctx, uint32_t slots) {
   if (!ctx) return set_error(nullptr, TPT_ERR_INVALID_ARG, "NULL context");
-  if (slots != 0 && (slots < 1024 || slots > (1u << 24)))
-    return set_error(ctx, TPT_ERR_INVALID_ARG, "wavefront capacity must be 0 or in [1024, 2^24]");
+  if (slots != 0 && (slots < 1024 || slots > (1u << 26)))
+    return set_error(ctx, TPT_ERR_INVALID_ARG, "wavefront capacity must be 0 or in [1024, 2^26]");
   ctx->batch_capacity = slots;
   ctx->batch_per_job = false;  // a capacity set by hand is for batched launches
   return TPT_OK;
