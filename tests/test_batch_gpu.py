@@ -144,3 +144,17 @@ def test_host_render_of_several_jobs_is_batched_and_equal(ctx, mixed):
     assert tpt.lib().tpt_render(ctx.h, arr, len(mixed), ptrs) == 0
     for a, b in zip(outs, ref):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_seeded_jobs_in_a_batch_equal_their_single_renders(ctx, mixed):
+    """Sample-stream seeds travel with each batched job: a batch mixing seeds
+    gives every job its own seeded single render, and a seed changes the image."""
+    seeded = [tpt.RenderJob(j.scene, j.camera, j.width, j.height, j.spp, j.max_depth, j.integrator, j.execution,
+                            (7919 * (k + 1)) if k % 2 == 0 else 0) for k, j in enumerate(mixed)]
+    ctx.wavefront_capacity = 0
+    ref = _render_each(ctx, seeded)
+    plain = _render_each(ctx, mixed)
+    got = _render_batch(ctx, seeded)
+    for k, (a, b, p) in enumerate(zip(got, ref, plain)):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+        assert np.array_equal(b, p) == (k % 2 == 1)
