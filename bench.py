@@ -61,8 +61,8 @@ def parse_args():
     p.add_argument("--no-batch", action="store_true", help="skip the batched-render block")
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-render block")
     p.add_argument("--large-spp", type=int, default=256, help="MIS spp timed on the large scene (configured: 256)")
-    p.add_argument("--large-bdpt-spp", type=int, default=16,
-                   help="BDPT spp timed on the large scene (configured: 256; 16 keeps the block to seconds)")
+    p.add_argument("--large-bdpt-spp", type=int, default=256,
+                   help="BDPT spp timed on the large scene (configured: 256; one image takes ~14 s)")
     p.add_argument("--adjoint-steps", type=int, default=200, help="Adam steps of the inverse-rendering run")
     p.add_argument("--batch-spp-scale", type=float, default=1.0, help="spp scale of the batched workload")
     return p.parse_args()
@@ -486,11 +486,11 @@ def lights_block(ctx, args):
 def large_block(ctx, args, cpu=True):
     """The plain large render: ~2.1M triangles (1024 instanced spheres, boxes and
     tori + ground), 256 OpenPBR materials, 10,000 emissive triangles, 1920x1080,
-    depth 16 (MIS) and path length 10 (BDPT).  MIS is timed at the configured
-    256 spp (--large-spp); BDPT at --large-bdpt-spp (16: 256 would hold the GPU
-    for tens of seconds per image) and its one-kernel variant at 1 spp, both
-    labelled `reduced_spp` (per-sample cost does not depend on spp).  Each run is
-    warmed up by the same render at 1 spp."""
+    depth 16 (MIS) and path length 10 (BDPT).  MIS (--large-spp) and the BDPT
+    wavefront (--large-bdpt-spp) are timed at the configured 256 spp; the
+    one-kernel BDPT at 1 spp, labelled `reduced_spp` (256 spp would hold the GPU
+    for minutes; per-sample cost does not depend on spp).  Each run is warmed up
+    by the same render at 1 spp."""
     import torch
 
     import tpt
