@@ -121,8 +121,8 @@ tpt_status render_batch(tpt_context* ctx, const tpt_render_job* jobs, int n_jobs
   for (const Chunk& c : plan_chunks(L, path_base, capacity)) {
     cudaError_t e = launch_wf_generate_batch(ctx->d_jobs, (uint32_t)n_jobs, B, c.first_path, c.n_paths, s);
     for (uint32_t b = 0; e == cudaSuccess && b <= c.max_depth; ++b)
-      e = enqueue_bounce(ctx, s, no_geo, DevRenderData{}, RenderLaunch{}, B, ctx->d_jobs, (int)(b & 1u),
-                         b == c.max_depth, lights);
+      e = enqueue_bounce(ctx, s, no_geo, DevRenderData{}, RenderLaunch{}, B, ctx->d_jobs, (int)(b & 1u), b > 0,
+                         lights);
     if (e == cudaSuccess) e = launch_wf_finalize(B, c.n_paths, samples, s);
     for (const Segment& g : c.segs) {
       if (e != cudaSuccess) break;

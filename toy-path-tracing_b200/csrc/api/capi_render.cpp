@@ -172,7 +172,7 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
   const bool direct = A || ctx->render_stats;
   unsigned long long* tot = ctx->render_stats;
   for (uint32_t b = 0; !direct && e == cudaSuccess && b <= L.max_depth; ++b)
-    e = enqueue_bounce(ctx, s, geo, rd, L, B, nullptr, (int)(b & 1u), b == L.max_depth);
+    e = enqueue_bounce(ctx, s, geo, rd, L, B, nullptr, (int)(b & 1u), b > 0);
   for (uint32_t b = 0; direct && e == cudaSuccess && b <= L.max_depth; ++b) {
     const int cur = (int)(b & 1u);
     e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
@@ -275,8 +275,11 @@ tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, co
   const BdWfBuffers& B = ctx->bd;
   for (uint64_t b = 0; b < n; b += B.sample_capacity) {
     const uint32_t m = (uint32_t)std::min<uint64_t>(B.sample_capacity, n - b);
+    const bool branch = ensure_branch(ctx);
     cudaError_t e = launch_bdpt_wavefront(job->scene->geo, job->scene->render, L, B, first + b, m, samples + 3 * b,
-                                          next_counter(ctx), ctx->d_err, ctx->num_sms, s, ctx->render_stats);
+                                          next_counter(ctx), ctx->d_err, ctx->num_sms, s, ctx->render_stats,
+                                          next_counter(ctx), branch ? ctx->cap_side : nullptr, ctx->cap_fork,
+                                          ctx->cap_join);
     if ((st = cuda_check(ctx, e, "BDPT wavefront launch"))) return st;
   }
   return TPT_OK;

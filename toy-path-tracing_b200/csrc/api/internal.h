@@ -77,6 +77,12 @@ struct tpt_context {
   std::vector<tpt::BounceGraphSet*> graphs;
   uint64_t graph_clock = 0;
   cudaStream_t cap_stream = nullptr;
+  // second stream and fork/join events of two-branch launch sequences
+  // (created on first use by ensure_branch): the shadow stage of a bounce
+  // beside the next bounce's traversal in the captured bounce graphs, and the
+  // light half of the BDPT subpath queue beside its camera half
+  cudaStream_t cap_side = nullptr;
+  cudaEvent_t cap_fork = nullptr, cap_join = nullptr;
   // OpenPBR tables (built on the GPU on first use, kept until destroy)
   std::map<uint32_t, float*> da_tables;  // directional albedo per eta (bit pattern)
   float* d_cec_e = nullptr;              // conductor E (64 x 64)
@@ -169,7 +175,12 @@ cudaError_t launch_accumulate(const float* samples, uint32_t spp, uint32_t first
 cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                                   const BdWfBuffers& B, uint64_t first_path, uint32_t n, float* samples,
                                   unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
-                                  unsigned long long* totals = nullptr);
+                                  unsigned long long* totals = nullptr, unsigned long long* counter2 = nullptr,
+                                  cudaStream_t side = nullptr, cudaEvent_t fork = nullptr,
+                                  cudaEvent_t join = nullptr);
+// With `side` (and its own work counter2) the light half of each subpath step's
+// traversal runs on `side` beside the camera half (fork/join events around it).
+
 // capi_render.cpp: BDPT paths [first, first + n) through the wavefront, in chunks.
 tpt_status render_bdpt_wavefront(tpt_context* ctx, const tpt_render_job* job, const RenderLaunch& L, uint64_t first,
                                  uint64_t n, float* samples, cudaStream_t s);
@@ -210,13 +221,19 @@ cudaError_t launch_wf_shade_batch(const DevJob* jobs, const WfBuffers& B, int cu
                                   bool lights);
 cudaError_t launch_wf_finalize(const WfBuffers& B, uint32_t n_paths, float* samples, cudaStream_t s);
 
-// bounce_graphs.cpp: one wavefront bounce (single job when jobs == nullptr,
-// else batched) on `s`, replayed from a cached CUDA graph when possible.
+// bounce_graphs.cpp: step b of the wavefront loop b = 0 .. max_depth (single
+// job when jobs == nullptr, else batched) on `s`, replayed from a cached CUDA
+// graph when possible: the shadow stage of bounce b - 1 when prev_shadow
+// (b > 0), then bounce b's closest-hit traversal and shade.  The last bounce's
+// shadow rays are never traced, as in the sequential order.
 // batch_lights: some job of the batch `jobs` has point, spot or directional lights
 cudaError_t enqueue_bounce(tpt_context* ctx, cudaStream_t s, const DevGeometry& geo, const DevRenderData& rd,
-                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool last,
+                           const RenderLaunch& P, const WfBuffers& B, const DevJob* jobs, int cur, bool prev_shadow,
                            bool batch_lights = false);
 void destroy_bounce_graphs(tpt_context* ctx);
+// Creates ctx->cap_side / cap_fork / cap_join when missing; false when they
+// cannot be created (the caller then launches its branches in sequence).
+bool ensure_branch(tpt_context* ctx);
 
 // capi_batch.cpp: jobs (MIS) through one wavefront launch sequence; out_rgb are
 // device images; capacity = path slots per chunk (0 = kDefaultWavefrontSlots).

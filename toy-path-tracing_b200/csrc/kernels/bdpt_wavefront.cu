@@ -309,8 +309,10 @@ static inline unsigned grid_of(uint64_t n) { return (unsigned)((n + kBdWfBlock -
 cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& rd, const RenderLaunch& P,
                                   const BdWfBuffers& B, uint64_t first_path, uint32_t n, float* samples,
                                   unsigned long long* counter, uint32_t* err, int num_sms, cudaStream_t s,
-                                  unsigned long long* totals) {
+                                  unsigned long long* totals, unsigned long long* counter2, cudaStream_t side,
+                                  cudaEvent_t fork, cudaEvent_t join) {
   if (n == 0) return cudaSuccess;
+  if (!counter2 || !fork || !join) side = nullptr;
   DevRender S{geo, rd};
   cudaError_t e = cudaMemsetAsync(B.counts, 0, 6 * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
@@ -322,14 +324,27 @@ cudaError_t launch_bdpt_wavefront(const DevGeometry& geo, const DevRenderData& r
     const int cur = (int)(step & 1u);
     if ((e = cudaMemsetAsync(B.counts + 2 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(B.counts + 4 + (cur ^ 1), 0, sizeof(uint32_t), s)) != cudaSuccess) return e;
-    // the camera half, then the light half of the queue (hits at the rays' slots)
+    // the camera half and the light half of the queue (hits at the rays' slots,
+    // disjoint halves): with a side stream the light half runs beside the
+    // camera half, which matters in late steps, where each launch lasts as long
+    // as its longest ray's chain of node loads however few rays it holds
+    if (side) {
+      if ((e = cudaEventRecord(fork, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(side, fork, 0)) != cudaSuccess) return e;
+    }
     e = launch_traverse_strided(geo, B.q_ray[cur], Q, S_cap, TPT_CLOSEST_HIT, B.h_tri, B.h_t, B.h_inst, B.h_bary, Q,
                                 counter, err, num_sms, s, nullptr, nullptr, B.counts + 2 + cur, nullptr, nullptr,
                                 totals);
-    if (e != cudaSuccess) return e;
-    e = launch_traverse_strided(geo, B.q_ray[cur] + S_cap, Q, S_cap, TPT_CLOSEST_HIT, B.h_tri + S_cap,
-                                B.h_t + S_cap, B.h_inst + S_cap, B.h_bary + S_cap, Q, counter, err, num_sms, s,
-                                nullptr, nullptr, B.counts + 4 + cur, nullptr, nullptr, totals);
+    if (e == cudaSuccess)
+      e = launch_traverse_strided(geo, B.q_ray[cur] + S_cap, Q, S_cap, TPT_CLOSEST_HIT, B.h_tri + S_cap,
+                                  B.h_t + S_cap, B.h_inst + S_cap, B.h_bary + S_cap, Q, side ? counter2 : counter, err,
+                                  num_sms, side ? side : s, nullptr, nullptr, B.counts + 4 + cur, nullptr, nullptr,
+                                  totals);
+    if (side) {  // join even after an error: no branch is left open on the caller's stream
+      const cudaError_t ej = cudaEventRecord(join, side);
+      const cudaError_t ew = ej == cudaSuccess ? cudaStreamWaitEvent(s, join, 0) : ej;
+      if (e == cudaSuccess) e = ew;
+    }
     if (e != cudaSuccess) return e;
     bd_step<<<grid_of(Q), kBdWfBlock, 0, s>>>(S, P, B, first_path, step, cur);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
