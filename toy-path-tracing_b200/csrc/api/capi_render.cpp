@@ -173,20 +173,35 @@ tpt_status render_wavefront(tpt_context* ctx, const tpt_render_job* job, const R
   unsigned long long* tot = ctx->render_stats;
   for (uint32_t b = 0; !direct && e == cudaSuccess && b <= L.max_depth; ++b)
     e = enqueue_bounce(ctx, s, geo, rd, L, B, nullptr, (int)(b & 1u), b > 0);
+  // the step order of the bounce graphs: step b runs the shadow stage of
+  // bounce b - 1 on the side stream beside bounce b's path traversal (joined
+  // before shade; in sequence with alpha tests or without a side stream)
+  const bool branch = direct && !B.q_aux && !B.s_aux && ensure_branch(ctx);
   for (uint32_t b = 0; direct && e == cudaSuccess && b <= L.max_depth; ++b) {
     const int cur = (int)(b & 1u);
-    e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
+    const bool split = branch && b > 0;
+    if (split) {
+      e = cudaEventRecord(ctx->cap_fork, s);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->cap_side, ctx->cap_fork, 0);
+    }
+    const cudaStream_t ss = split ? ctx->cap_side : s;
+    if (e == cudaSuccess && b > 0)
+      e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
+                                  nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, ss, nullptr,
+                                  nullptr, B.counts + 2, nullptr, nullptr, tot ? tot + 4 : nullptr, B.s_aux);
+    if (e == cudaSuccess && b > 0) e = launch_wf_resolve(B, ss, A);
+    if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + (cur ^ 1), 0, 4, s);
     if (e == cudaSuccess)
       e = launch_traverse_strided(geo, B.q_ray[cur], B.capacity, B.capacity, TPT_CLOSEST_HIT, B.h_tri, B.h_t,
                                   B.h_inst, B.h_bary, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s,
                                   nullptr, nullptr, B.counts + cur, nullptr, nullptr, tot, B.q_aux, B.q_slot[cur]);
+    if (split) {  // join even after an error: no branch is left open on the caller's stream
+      const cudaError_t ej = cudaEventRecord(ctx->cap_join, ctx->cap_side);
+      const cudaError_t ew = ej == cudaSuccess ? cudaStreamWaitEvent(s, ctx->cap_join, 0) : ej;
+      if (e == cudaSuccess) e = ew;
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(B.counts + 2, 0, 4, s);
     if (e == cudaSuccess) e = launch_wf_shade(geo, rd, L, B, cur, s, A);
-    if (e == cudaSuccess && b < L.max_depth)
-      e = launch_traverse_strided(geo, B.s_ray, B.capacity, B.capacity, TPT_CLOSEST_HIT, B.s_tri, B.s_t, B.s_inst,
-                                  nullptr, B.capacity, next_counter(ctx), ctx->d_err, ctx->num_sms, s, nullptr,
-                                  nullptr, B.counts + 2, nullptr, nullptr, tot ? tot + 4 : nullptr, B.s_aux);
-    if (e == cudaSuccess && b < L.max_depth) e = launch_wf_resolve(B, s, A);
   }
   if (e == cudaSuccess && !A) e = launch_wf_finalize(B, n, samples, s);
   return cuda_check(ctx, e, "wavefront launch");
